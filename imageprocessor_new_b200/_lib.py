@@ -1,0 +1,94 @@
+"""ctypes binding of libsubpx_b200.so, the package's only compute backend.
+
+There is no CPU fallback: importing the binding on a machine without the built library or without a
+CUDA device raises immediately, with the reason.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_double, c_int, c_size_t, c_void_p, POINTER
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libsubpx_b200.so"
+
+# Pixel dtype codes (include/subpx_b200.h).
+DTYPES = {np.dtype(np.uint8): 0, np.dtype(np.uint16): 1, np.dtype(np.float32): 2, np.dtype(np.float64): 3}
+
+REFINE_CODES = {"none": 0, "weighted": 1, "logquad": 2, "logquadratic": 2, "edge_gradmoment": 3,
+                "edge_moment": 3, "edges_centered": 3, "auto": 4}
+
+STATUS_NAMES = ("ok", "no_signal", "insufficient_cell_pixels", "insufficient_fit_pixels", "singular_fit",
+                "non_gaussian_fit", "contour_outside_cell", "incomplete_rays", "fit_diverged",
+                "center_outside_cell")
+
+_P = c_void_p
+_I = c_int
+_D = c_double
+_S = c_size_t
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "spx_last_error": (ctypes.c_char_p, []),
+    "spx_version": (_I, []),
+    "spx_device_info": (_I, [POINTER(c_int), POINTER(c_int)]),
+    "spx_otsu_workspace_bytes": (_S, [_I]),
+    "spx_otsu": (_I, [_P, _I, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_triangle": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_ccl_workspace_bytes": (_S, [_I, _I]),
+    "spx_ccl_label": (_I, [_P, _I, _I, _I, _P, _D, _I, _I, _P, _P, _P, _S, _P]),
+    "spx_ccl_finish": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _S, _P]),
+    "spx_select_workspace_bytes": (_S, [_I]),
+    "spx_select_components": (_I, [_P, _I, _I, _I, _I, _D, _P, _P, _P, _P, _S, _P]),
+    "spx_refine_centers": (_I, [_P, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P]),
+    "spx_voronoi_workspace_bytes": (_S, [_I, _I, _I]),
+    "spx_voronoi_labels": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
+}
+
+
+class LibraryError(RuntimeError):
+    """A libsubpx_b200 entry point returned an error status."""
+
+
+def load_library(path: Path | str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the shared library and declares every exported entry point (no GPU needed)."""
+    path = Path(path)
+    if not path.exists():
+        raise RuntimeError(f"{path.name} is not built; run `python -m imageprocessor_new_b200.build`")
+    lib = ctypes.CDLL(str(path))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_LIB: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library, after checking that a CUDA device is usable."""
+    global _LIB
+    if _LIB is None:
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("imageprocessor_new_b200 needs a CUDA device (B200, sm_100a); none is visible")
+        _LIB = load_library()
+    return _LIB
+
+
+def call(name: str, *args) -> int:
+    """Calls an entry point and raises LibraryError with spx_last_error() on a non-zero status."""
+    fn = getattr(lib(), name)
+    status = fn(*args)
+    if status != 0:
+        msg = lib().spx_last_error().decode(errors="replace")
+        raise LibraryError(f"{name}: {msg} (status {status})")
+    return status
+
+
+def size(name: str, *args) -> int:
+    return int(getattr(lib(), name)(*args))

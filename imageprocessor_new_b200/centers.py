@@ -1,0 +1,204 @@
+"""Centre detection on the device: threshold -> connected components -> per-blob refinement.
+
+Drop-in for ``detect_centers(..., backend="gpu")`` of subpx/centers.py:130-220 and
+``detect_centers_tiled`` (subpx/legacy.py:93-95). Semantics follow the reference CPU estimators
+(subpx/_cpu/centers.py); see the module docstrings of csrc/refine.cu for the rules.
+"""
+
+from __future__ import annotations
+
+import warnings
+
+import numpy as np
+import torch
+
+from . import _device as dev
+from . import _lib
+from . import segment
+from .types import CenterResult
+
+_SUPPORTED_REFINE = ("none", "weighted", "logquad", "logquadratic", "edge_gradmoment", "edge_moment",
+                     "edges_centered", "auto")
+_VORONOI_METHODS = {"radial_symmetry", "isophote_curvature"}
+
+
+def choose_refine_method_for_bbox(width: float, height: float, *, small_feature_max: float = 12.0) -> str:
+    """logquad for features up to ``small_feature_max`` px, else edge_gradmoment (subpx/_cpu/centers.py:22-30)."""
+    size = float(max(width, height))
+    return "logquad" if size <= float(small_feature_max) else "edge_gradmoment"
+
+
+def recommend_refine_method(width_px: float, height_px: float, *, small_feature_max: float = 12.0) -> str:
+    return choose_refine_method_for_bbox(width_px, height_px, small_feature_max=small_feature_max)
+
+
+def _check_backend(backend: str) -> None:
+    if backend not in ("auto", "gpu"):
+        raise ValueError("imageprocessor_new_b200 is the GPU backend: backend must be 'gpu' or 'auto'")
+
+
+def _as_image(image) -> np.ndarray:
+    img = image.detach().cpu().numpy() if isinstance(image, torch.Tensor) else np.asarray(image)
+    if img.ndim != 2:
+        raise ValueError("Expected 2D grayscale image.")
+    return img
+
+
+def _device_image(img: np.ndarray) -> torch.Tensor:
+    if img.dtype not in _lib.DTYPES:
+        raise ValueError(f"unsupported image dtype {img.dtype}; use uint8, uint16, float32 or float64")
+    return dev.upload(img)
+
+
+def _morphology(binary_src: torch.Tensor, threshold, fixed, invert, morph_open, morph_close):
+    if morph_open or morph_close:
+        raise NotImplementedError("morph_open / morph_close are not implemented on the GPU path")
+
+
+def _centers_on_device(img_d: torch.Tensor, *, threshold_dev: torch.Tensor | None, fixed_threshold: float,
+                       invert: bool, area_min: int, area_max: int, pad: int, refine: str,
+                       connectivity: int, small_feature_max: float) -> torch.Tensor:
+    """Refined centres (n, 2) on the device, NaN rows for failed refinements, in label order."""
+    comp = segment.label(img_d, threshold=threshold_dev, fixed_threshold=fixed_threshold, invert=invert,
+                         connectivity=connectivity)
+    k = comp.count
+    h, w = img_d.shape
+    rows = dev.empty((max(k, 1), 5), torch.int32)
+    methods = dev.empty((max(k, 1),), torch.uint8)
+    kept = dev.empty((1,), torch.int32)
+    ws = dev.workspace(_lib.size("spx_select_workspace_bytes", k))
+    _lib.call("spx_select_components", comp.stats.data_ptr(), k, int(area_min), int(area_max),
+              _lib.REFINE_CODES[refine], float(small_feature_max), rows.data_ptr(), methods.data_ptr(),
+              kept.data_ptr(), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+    n = dev.read_int(kept)
+    centers = dev.empty((max(n, 1), 2), torch.float64)
+    _lib.call("spx_refine_centers", img_d.data_ptr(), dev.dtype_code(img_d), h, w, comp.labels.data_ptr(),
+              rows.data_ptr(), methods.data_ptr(), n, int(pad), centers.data_ptr(), dev.stream_ptr())
+    return centers[:n]
+
+
+def _finite(centers: torch.Tensor) -> np.ndarray:
+    c = centers.cpu().numpy().reshape(-1, 2)
+    return c[np.isfinite(c).all(axis=1)].astype(np.float64, copy=False)
+
+
+def detect_centers(
+    image: np.ndarray,
+    *,
+    backend: str = "auto",
+    threshold: str = "triangle",
+    invert: bool = False,
+    area_min: int = 1,
+    area_max: int = 50,
+    morph_open: int = 0,
+    morph_close: int = 0,
+    pad: int = 3,
+    refine: str = "logquad",
+    connectivity: int = 8,
+    gpu_batch: int = 4096,
+    device: int = 0,
+    use_float64: bool = True,
+    components_backend: str = "cpu",
+    small_feature_max: float = 12.0,
+    upsample_factor: int = 4,
+    tile_h: int | None = None,
+    overlap: int = 128,
+    threshold_mode: str = "auto",
+    otsu_downsample: int = 4,
+    thr_scale: float = 0.8,
+    dedupe_eps: float = 1.5,
+    background: str | None = None,
+    deblend_iterations: int = 30,
+) -> CenterResult:
+    """Detect and refine centres (subpx/centers.py:130-220), on the GPU.
+
+    Centres are returned in component label order (the reference CPU order; the reference GPU
+    path groups them by refine method). ``gpu_batch``, ``use_float64``, ``components_backend`` and
+    ``upsample_factor`` are accepted for signature compatibility: every method runs in FP64 in one
+    launch and components are always labelled on the GPU.
+    """
+    _check_backend(backend)
+    if refine in _VORONOI_METHODS:
+        raise NotImplementedError(f"refine='{refine}' is outside this package's hot path")
+    if refine not in _SUPPORTED_REFINE:
+        raise ValueError(f"Unsupported refine method: {refine}")
+    if background not in (None, "model"):
+        raise ValueError("background must be None or 'model'")
+    if background == "model":
+        raise NotImplementedError("background='model' centre re-refinement is not part of this package yet")
+    if connectivity not in (4, 8):
+        raise ValueError("connectivity must be 4 or 8")
+    img = _as_image(image)
+    _morphology(None, None, None, invert, morph_open, morph_close)
+    with dev.on_device(device):
+        if tile_h is not None:
+            return _detect_tiled(img, threshold=threshold, invert=invert, area_min=area_min, area_max=area_max,
+                                 pad=pad, refine=refine, connectivity=connectivity,
+                                 small_feature_max=small_feature_max, tile_h=int(tile_h), overlap=int(overlap),
+                                 threshold_mode=threshold_mode, otsu_downsample=otsu_downsample,
+                                 thr_scale=thr_scale, dedupe_eps=dedupe_eps, device=device)
+        img_d = _device_image(img)
+        thr = segment.binarize_threshold(img_d, threshold, invert)
+        centers = _centers_on_device(img_d, threshold_dev=thr, fixed_threshold=0.0, invert=invert,
+                                     area_min=area_min, area_max=area_max, pad=pad, refine=refine,
+                                     connectivity=connectivity, small_feature_max=small_feature_max)
+        arr = _finite(centers)
+    meta = {
+        "invert": bool(invert), "area_min": int(area_min), "area_max": int(area_max),
+        "morph_open": int(morph_open), "morph_close": int(morph_close), "pad": int(pad),
+        "connectivity": int(connectivity), "gpu_batch": int(gpu_batch), "device": int(device),
+        "use_float64": bool(use_float64), "components_backend": str(components_backend),
+        "small_feature_max": float(small_feature_max),
+    }
+    return CenterResult(centers_xy=arr, method=f"threshold={threshold}, refine={refine}", backend="gpu", meta=meta)
+
+
+def _detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, connectivity, small_feature_max,
+                  tile_h, overlap, threshold_mode, otsu_downsample, thr_scale, dedupe_eps, device) -> CenterResult:
+    """Row bands of ``tile_h`` with an ``overlap`` halo, keep-band rule, dedupe
+    (subpx/_gpu/centers.py:1778-1862), with the image resident on the device."""
+    from . import tiled
+
+    return tiled.detect_tiled(img, threshold=threshold, invert=invert, area_min=area_min, area_max=area_max,
+                              pad=pad, refine=refine, connectivity=connectivity,
+                              small_feature_max=small_feature_max, tile_h=tile_h, overlap=overlap,
+                              threshold_mode=threshold_mode, otsu_downsample=otsu_downsample,
+                              thr_scale=thr_scale, dedupe_eps=dedupe_eps, device=device)
+
+
+def detect_centers_tiled(image, *, tile_h=8192, **kwargs) -> CenterResult:
+    """Deprecated alias of ``detect_centers(image, tile_h=...)`` (subpx/legacy.py:93-95)."""
+    warnings.warn("detect_centers_tiled is deprecated; use detect_centers(image, tile_h=...)",
+                  DeprecationWarning, stacklevel=2)
+    kwargs.setdefault("backend", "gpu")
+    return detect_centers(image, tile_h=tile_h, **kwargs)
+
+
+def detect_centers_tiled_global_otsu(image, *, tile_h=8192, threshold_mode="global", **kwargs) -> CenterResult:
+    warnings.warn("detect_centers_tiled_global_otsu is deprecated; use detect_centers(image, tile_h=..., "
+                  "threshold_mode='global')", DeprecationWarning, stacklevel=2)
+    kwargs.setdefault("backend", "gpu")
+    return detect_centers(image, tile_h=tile_h, threshold_mode=threshold_mode, **kwargs)
+
+
+def detect_centers_batch(frames, /, *args, progress: bool = False, **kwargs):
+    """detect_centers over frames (subpx/batch.py:22-24)."""
+    out = []
+    for i, frame in enumerate(frames):
+        out.append(detect_centers(frame, *args, **kwargs))
+        if progress and (i + 1) % 50 == 0:
+            print(f"processed {i + 1} frames")
+    return out
+
+
+def filter_centers(centers_xy, image_shape_hw, *, margin: float = 5.0) -> np.ndarray:
+    """Centres at least ``margin`` px inside the image (subpx/centers.py:317-332)."""
+    centers = np.asarray(centers_xy, dtype=np.float64)
+    if centers.size == 0:
+        return centers.reshape(0, 2)
+    shape = tuple(image_shape_hw)
+    h, w = int(shape[0]), int(shape[1])
+    m = float(margin)
+    x, y = centers[:, 0], centers[:, 1]
+    keep = (x >= m) & (x < (w - m)) & (y >= m) & (y < (h - m))
+    return centers[keep]

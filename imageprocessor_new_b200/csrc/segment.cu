@@ -1,0 +1,767 @@
+// Segmentation: Otsu threshold, binarisation and connected-component labelling with stats.
+//
+// Replaces, for the subpx hot path:
+//   cv2.threshold(..., THRESH_OTSU)            subpx/_cpu/centers.py:247-266, subpx/_gpu/centers.py:1789-1796
+//   cv2.connectedComponentsWithStats           subpx/_cpu/components.py:18-32
+//
+// Otsu: a shared-memory histogram over the occupied value range, then OpenCV's published Otsu scan
+// (between-class variance q1*q2*(mu1-mu2)^2, first maximum, bins skipped while min(q1,q2) <
+// FLT_EPSILON). The scan's running sums are rounded sequentially by one thread so that the chosen
+// bin is the one OpenCV chooses.
+//
+// CCL: union-find in two levels. Parents live in a canonical-order array: for 8-connectivity the
+// pixels of each 2x2 block are contiguous and blocks follow the row-pair scan, for 4-connectivity
+// canonical order is raster order. Unions always link the larger id under the smaller, so the root
+// of a component is its first pixel in that order, and OpenCV's label numbering is the rank of the
+// root among all roots: a bitmap of roots plus a prefix count of its words.
+//   k_local_ccl     one CTA per 32x64 tile: binarise, union-find in shared memory, write parents
+//   k_border_merge  unions across tile borders in global memory (lock-free atomicMin linking)
+//   scan            popcount prefix of the root bitmap -> component count K
+//   k_finish        final raster labels (rank of the root) + stats by warp run-length aggregation
+
+#include "common.cuh"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+namespace spx {
+
+static thread_local char g_error[1024];
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+}
+
+int check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("%s launch failed: %s", what, cudaGetErrorString(e));
+        return SPX_ERR_CUDA;
+    }
+    return SPX_OK;
+}
+
+namespace {
+
+constexpr int kHistSmemBins = 16384;  // value ranges up to this use a shared-memory histogram
+constexpr int kTileH = 32;            // CCL tile (even height keeps 2x2 blocks inside one tile)
+constexpr int kTileW = 64;
+constexpr int kTilePx = kTileH * kTileW;
+
+// ------------------------------------------------------------------------------------------ Otsu
+
+__device__ __forceinline__ unsigned int px_u(const void* img, int dtype, long long i) {
+    return dtype == SPX_U8 ? (unsigned int)static_cast<const uint8_t*>(img)[i]
+                           : (unsigned int)static_cast<const uint16_t*>(img)[i];
+}
+
+// range[0] = min, range[1] = max of the sampled pixels (range must be preset to {~0u, 0}).
+__global__ void k_minmax(const void* img, int dtype, int height, int width, int step,
+                         unsigned int* range) {
+    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const long long n = (long long)hs * ws;
+    unsigned int lo = 0xffffffffu, hi = 0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long y = k / ws, x = k % ws;
+        const unsigned int v = px_u(img, dtype, y * step * (long long)width + x * step);
+        lo = min(lo, v);
+        hi = max(hi, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&range[0], lo);
+        atomicMax(&range[1], hi);
+    }
+}
+
+// Histogram of the sampled pixels into hist[65536] (pre-zeroed, u32).
+__global__ void k_histogram(const void* img, int dtype, int height, int width, int step,
+                            int dense, const unsigned int* range, unsigned int* hist) {
+    extern __shared__ unsigned int sh[];
+    const unsigned int lo = range[0], hi = range[1];
+    const unsigned int nb = hi >= lo ? hi - lo + 1 : 0;
+    const bool in_smem = nb <= (unsigned int)kHistSmemBins;
+    if (in_smem) {
+        for (unsigned int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0;
+        __syncthreads();
+    }
+    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const long long n = (long long)hs * ws;
+    if (dense) {
+        // 16-byte loads of 8 pixels, then the ragged tail.
+        const uint4* v4 = static_cast<const uint4*>(img);
+        const long long n8 = n / 8;
+        for (long long k = n8 * 8 + blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+             k += (long long)gridDim.x * blockDim.x) {
+            const unsigned int v = static_cast<const uint16_t*>(img)[k];
+            if (in_smem) atomicAdd(&sh[v - lo], 1u);
+            else atomicAdd(&hist[v], 1u);
+        }
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n8;
+             k += (long long)gridDim.x * blockDim.x) {
+            const uint4 q = __ldg(v4 + k);
+            const unsigned int w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const unsigned int a = w[j] & 0xffffu, b = w[j] >> 16;
+                if (in_smem) {
+                    atomicAdd(&sh[a - lo], 1u);
+                    atomicAdd(&sh[b - lo], 1u);
+                } else {
+                    atomicAdd(&hist[a], 1u);
+                    atomicAdd(&hist[b], 1u);
+                }
+            }
+        }
+    } else {
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+             k += (long long)gridDim.x * blockDim.x) {
+            const long long y = k / ws, x = k % ws;
+            const unsigned int v = px_u(img, dtype, y * step * (long long)width + x * step);
+            if (in_smem) atomicAdd(&sh[v - lo], 1u);
+            else atomicAdd(&hist[v], 1u);
+        }
+    }
+    if (in_smem) {
+        __syncthreads();
+        for (unsigned int i = threadIdx.x; i < nb; i += blockDim.x)
+            if (sh[i]) atomicAdd(&hist[lo + i], sh[i]);
+    }
+}
+
+// OpenCV's Otsu scan (getThreshVal_Otsu) over bins [0, N), by one block in four phases:
+//   A  p_i = h[i] * scale (parallel), then q1_i = q1_{i-1} + p_i by one thread (additions only);
+//   B  y_i = RN(1 / q1_i) (parallel);
+//   C  the mu1 recurrence by one thread: mu1 <- mu1 * q1_{i-1}; unless bin i is skipped,
+//      mu1 <- RN((mu1 + i p_i) / q1_i), the quotient by Markstein's correction
+//      (q = RN(a y); r = a - q q1 exactly by FMA; RN(q + r y) = RN(a / q1) when y = RN(1 / q1));
+//   D  sigma_i = q1 q2 (mu1 - mu2)^2 for every unskipped bin and the first maximum (parallel).
+// Every value is rounded exactly as OpenCV's sequential loop rounds it, so the chosen bin is OpenCV's.
+__global__ void __launch_bounds__(1024) k_otsu_scan(const unsigned int* hist, int nbins,
+                                                    const unsigned int* range, long long total,
+                                                    double* p_buf, double* q1_buf, double* y_buf,
+                                                    double* mu1_buf, double* threshold) {
+    __shared__ unsigned long long s_mu[32];
+    __shared__ double s_best[32];
+    __shared__ int s_arg[32];
+    unsigned long long mu_part = 0;
+    for (int i = threadIdx.x; i < nbins; i += blockDim.x) mu_part += (unsigned long long)i * hist[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mu_part += __shfl_xor_sync(0xffffffffu, mu_part, o);
+    if ((threadIdx.x & 31) == 0) s_mu[threadIdx.x >> 5] = mu_part;
+    const double scale = 1.0 / (double)total;
+    int first = (int)range[0], last = (int)range[1];
+    if (first < 0) first = 0;
+    if (last > nbins - 1) last = nbins - 1;
+    const int n = last - first + 1;
+    // Bins below the first occupied one leave mu1 = q1 = 0 and are all skipped; bins above the last
+    // occupied one have q2 < FLT_EPSILON and are skipped as well.
+    for (int k = threadIdx.x; k < n; k += blockDim.x) p_buf[k] = __dmul_rn((double)hist[first + k], scale);
+    __syncthreads();
+    unsigned long long mu_int = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mu_int += s_mu[w];
+    // The reference sums i*h[i] sequentially in double: every partial sum is an integer below 2^53,
+    // hence exact, and equal to this integer sum.
+    const double mu = __dmul_rn((double)mu_int, scale);
+    if (threadIdx.x == 0) {
+        double q1 = 0.0;
+        for (int k = 0; k < n; ++k) {
+            q1 = __dadd_rn(q1, p_buf[k]);
+            q1_buf[k] = q1;
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < n; k += blockDim.x) y_buf[k] = __drcp_rn(q1_buf[k]);
+    __syncthreads();
+    const double eps = (double)1.1920928955078125e-07f;
+    const double one_minus_eps = __dsub_rn(1.0, eps);
+    if (threadIdx.x == 0) {
+        double mu1 = 0.0, q1_prev = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double q1 = q1_buf[k], p_i = p_buf[k];
+            mu1 = __dmul_rn(mu1, q1_prev);
+            q1_prev = q1;
+            const double q2 = __dsub_rn(1.0, q1);
+            if (fmin(q1, q2) < eps || fmax(q1, q2) > one_minus_eps) {
+                mu1_buf[k] = dnan();
+                continue;
+            }
+            const double a = __dadd_rn(mu1, __dmul_rn((double)(first + k), p_i));
+            const double y = y_buf[k];
+            const double q = __dmul_rn(a, y);
+            const double r = __fma_rn(-q, q1, a);
+            mu1 = __fma_rn(r, y, q);
+            mu1_buf[k] = mu1;
+        }
+    }
+    __syncthreads();
+    double best = 0.0;
+    int arg = 0x7fffffff;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const double mu1 = mu1_buf[k];
+        if (isnan(mu1)) continue;
+        const double q1 = q1_buf[k], q2 = __dsub_rn(1.0, q1);
+        const double mu2 = __ddiv_rn(__dsub_rn(mu, __dmul_rn(q1, mu1)), q2);
+        const double d = __dsub_rn(mu1, mu2);
+        const double sigma = __dmul_rn(__dmul_rn(__dmul_rn(q1, q2), d), d);
+        // First maximum strictly above 0 (OpenCV starts from max_sigma = 0, bin 0).
+        if (sigma > best) { best = sigma; arg = k; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oa = __shfl_xor_sync(0xffffffffu, arg, o);
+        if (ob > best || (ob == best && oa < arg)) { best = ob; arg = oa; }
+    }
+    if ((threadIdx.x & 31) == 0) { s_best[threadIdx.x >> 5] = best; s_arg[threadIdx.x >> 5] = arg; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        int a = 0x7fffffff;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            if (s_best[w] > b || (s_best[w] == b && s_arg[w] < a)) { b = s_best[w]; a = s_arg[w]; }
+        *threshold = (b > 0.0 && a != 0x7fffffff) ? (double)(first + a) : 0.0;
+    }
+}
+
+// OpenCV's triangle threshold (getThreshVal_Triangle_8u) over a 256-bin histogram: the bin of
+// maximum distance to the line from the histogram peak to the far end of the occupied range.
+__global__ void k_triangle_scan(const unsigned int* hist, double* threshold) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int N = 256;
+    long long h[256];
+    for (int i = 0; i < N; ++i) h[i] = hist[i];
+    int left = 0, right = 0, max_ind = 0;
+    long long mx = 0;
+    for (int i = 0; i < N; ++i)
+        if (h[i] > 0) { left = i; break; }
+    if (left > 0) left--;
+    for (int i = N - 1; i > 0; --i)
+        if (h[i] > 0) { right = i; break; }
+    if (right < N - 1) right++;
+    for (int i = 0; i < N; ++i)
+        if (h[i] > mx) { mx = h[i]; max_ind = i; }
+    bool flipped = false;
+    if (max_ind - left < right - max_ind) {
+        flipped = true;
+        for (int i = 0, j = N - 1; i < j; ++i, --j) { const long long t = h[i]; h[i] = h[j]; h[j] = t; }
+        left = N - 1 - right;
+        max_ind = N - 1 - max_ind;
+    }
+    double thresh = left, dist = 0.0;
+    const double a = (double)mx, b = (double)(left - max_ind);
+    for (int i = left + 1; i <= max_ind; ++i) {
+        const double d = __dadd_rn(__dmul_rn(a, (double)i), __dmul_rn(b, (double)h[i]));
+        if (d > dist) { dist = d; thresh = i; }
+    }
+    thresh -= 1.0;
+    if (flipped) thresh = (N - 1) - thresh;
+    *threshold = thresh;
+}
+
+// -------------------------------------------------------------------------------------------- CCL
+
+struct Geo {
+    int H, W, Wb;   // image size; blocks per row pair (8-connectivity)
+    int conn;       // 8 or 4
+    __device__ __forceinline__ int canon(int y, int x) const {
+        return conn == 8 ? ((((y >> 1) * Wb + (x >> 1)) << 2) | ((y & 1) << 1) | (x & 1)) : y * W + x;
+    }
+};
+
+__device__ __forceinline__ bool is_fg(double v, double t, int invert) { return invert ? v <= t : v > t; }
+
+// Root of a, halving the path on the way (each visited node is re-pointed to its grandparent, an
+// ancestor, so concurrent finds and unions stay valid).
+__device__ __forceinline__ int find_root_volatile(volatile int* p, int a) {
+    while (true) {
+        const int b = p[a];
+        if (b == a) return a;
+        const int c = p[b];
+        if (c == b) return b;
+        p[a] = c;
+        a = c;
+    }
+}
+
+// Lock-free union (link the larger root under the smaller with atomicMin; retry from the value
+// that was there when another thread won the race). Clears the root bit of a root that gets linked.
+__device__ void unite(int* p, int a, int b, unsigned int* roots) {
+    while (true) {
+        a = find_root_volatile(p, a);
+        b = find_root_volatile(p, b);
+        if (a == b) return;
+        if (a < b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        const int old = atomicMin(&p[a], b);
+        if (old == a) {
+            if (roots) atomicAnd(&roots[a >> 5], ~(1u << (a & 31)));
+            return;
+        }
+        a = old;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_local_ccl(const void* img, int dtype, Geo g,
+                                                   const double* thr_dev, double thr_fixed,
+                                                   int invert, int* parents, unsigned int* roots) {
+    __shared__ int par[kTilePx];
+    __shared__ unsigned char fg[kTilePx];  // indexed by raster position inside the tile
+    const int tx0 = blockIdx.x * kTileW, ty0 = blockIdx.y * kTileH;
+    const double t = thr_dev ? *thr_dev : thr_fixed;
+    // Local index: canonical order restricted to the tile (keeps the global order of ids).
+    auto lidx = [&](int yl, int xl) {
+        return g.conn == 8 ? ((((yl >> 1) * (kTileW / 2) + (xl >> 1)) << 2) | ((yl & 1) << 1) | (xl & 1))
+                           : yl * kTileW + xl;
+    };
+    for (int k = threadIdx.x; k < kTilePx; k += blockDim.x) {
+        const int yl = k / kTileW, xl = k % kTileW, y = ty0 + yl, x = tx0 + xl;
+        bool f = false;
+        if (y < g.H && x < g.W) f = is_fg(load_px(img, dtype, (long long)y * g.W + x), t, invert);
+        fg[k] = f;
+        const int l = lidx(yl, xl);
+        par[l] = f ? l : -1;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kTilePx; k += blockDim.x) {
+        if (!fg[k]) continue;
+        const int yl = k / kTileW, xl = k % kTileW, l = lidx(yl, xl);
+        if (xl > 0 && fg[k - 1]) unite(par, l, lidx(yl, xl - 1), nullptr);
+        if (yl > 0) {
+            if (fg[k - kTileW]) unite(par, l, lidx(yl - 1, xl), nullptr);
+            if (g.conn == 8) {
+                if (xl > 0 && fg[k - kTileW - 1]) unite(par, l, lidx(yl - 1, xl - 1), nullptr);
+                if (xl + 1 < kTileW && fg[k - kTileW + 1]) unite(par, l, lidx(yl - 1, xl + 1), nullptr);
+            }
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kTilePx; k += blockDim.x) {
+        const int yl = k / kTileW, xl = k % kTileW, y = ty0 + yl, x = tx0 + xl;
+        if (y >= g.H || x >= g.W) continue;
+        const int gid = g.canon(y, x);
+        if (!fg[k]) {
+            parents[gid] = -1;
+            continue;
+        }
+        const int l = lidx(yl, xl);
+        const int r = find_root_volatile(par, l);
+        // Global id of the local root.
+        int ry, rx;
+        if (g.conn == 8) {
+            const int b = r >> 2;
+            ry = (b / (kTileW / 2)) * 2 + ((r >> 1) & 1);
+            rx = (b % (kTileW / 2)) * 2 + (r & 1);
+        } else {
+            ry = r / kTileW;
+            rx = r % kTileW;
+        }
+        const int rg = g.canon(ty0 + ry, tx0 + rx);
+        parents[gid] = rg;
+        if (r == l) atomicOr(&roots[gid >> 5], 1u << (gid & 31));
+    }
+}
+
+// Unions across tile borders. One thread per border pixel of a tile: top row (neighbours above),
+// left column (neighbours to the left), right column (the up-right neighbour in the next tile).
+__global__ void k_border_merge(Geo g, int* parents, unsigned int* roots, int tiles_x, int tiles_y) {
+    const int per_tile = kTileW + 2 * kTileH;
+    const long long total = (long long)tiles_x * tiles_y * per_tile;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int tile = (int)(k / per_tile), e = (int)(k % per_tile);
+        const int tx0 = (tile % tiles_x) * kTileW, ty0 = (tile / tiles_x) * kTileH;
+        int y, x;
+        if (e < kTileW) { y = ty0; x = tx0 + e; }
+        else if (e < kTileW + kTileH) { y = ty0 + (e - kTileW); x = tx0; }
+        else { y = ty0 + (e - kTileW - kTileH); x = tx0 + kTileW - 1; }
+        if (y >= g.H || x >= g.W) continue;
+        const int me = g.canon(y, x);
+        if (parents[me] < 0) continue;
+        auto link = [&](int yy, int xx) {
+            if (yy < 0 || xx < 0 || xx >= g.W) return;
+            // Only neighbours in another tile.
+            if (yy >= ty0 && xx >= tx0 && xx < tx0 + kTileW) return;
+            const int other = g.canon(yy, xx);
+            if (parents[other] < 0) return;
+            unite(parents, me, other, roots);
+        };
+        if (e < kTileW) {  // top row: (y-1, x) and, for 8-connectivity, (y-1, x-1), (y-1, x+1)
+            link(y - 1, x);
+            if (g.conn == 8) { link(y - 1, x - 1); link(y - 1, x + 1); }
+        } else if (e < kTileW + kTileH) {  // left column: (y, x-1) and (y-1, x-1)
+            link(y, x - 1);
+            if (g.conn == 8) link(y - 1, x - 1);
+        } else {  // right column: (y-1, x+1) lies in the tile to the right (or up-right)
+            if (g.conn == 8) link(y - 1, x + 1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------- prefix of popcounts
+
+__global__ void k_popc_block_sums(const unsigned int* words, long long n, int per_block,
+                                  int* block_sums) {
+    __shared__ int s[32];
+    const long long start = (long long)blockIdx.x * per_block;
+    int acc = 0;
+    for (int i = threadIdx.x; i < per_block; i += blockDim.x) {
+        const long long w = start + i;
+        if (w < n) acc += __popc(words[w]);
+    }
+    acc = warp_sum_i(acc);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        int v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0;
+        v = warp_sum_i(v);
+        if (threadIdx.x == 0) block_sums[blockIdx.x] = v;
+    }
+}
+
+// Exclusive scan of block_sums in place by one block; writes the total to *total.
+__global__ void k_scan_small(int* block_sums, int n, int* total) {
+    __shared__ int s[1024];
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int b0 = threadIdx.x * per;
+    int acc = 0;
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < n) acc += block_sums[b0 + i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        const int v = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+        __syncthreads();
+        s[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = s[threadIdx.x] - acc;  // exclusive prefix of this thread's chunk
+    for (int i = 0; i < per; ++i)
+        if (b0 + i < n) {
+            const int v = block_sums[b0 + i];
+            block_sums[b0 + i] = run;
+            run += v;
+        }
+    if (threadIdx.x == blockDim.x - 1) *total = s[threadIdx.x];
+}
+
+// prefix[w] = number of set bits in words[0..w).
+__global__ void k_popc_prefix(const unsigned int* words, long long n, int per_block,
+                              const int* block_offsets, int* prefix) {
+    __shared__ int s[1024];
+    const long long start = (long long)blockIdx.x * per_block;
+    const int per = per_block / blockDim.x;  // words per thread (per_block is a multiple)
+    const long long w0 = start + (long long)threadIdx.x * per;
+    int acc = 0;
+    for (int i = 0; i < per; ++i)
+        if (w0 + i < n) acc += __popc(words[w0 + i]);
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        const int v = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+        __syncthreads();
+        s[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = block_offsets[blockIdx.x] + s[threadIdx.x] - acc;
+    for (int i = 0; i < per; ++i)
+        if (w0 + i < n) {
+            prefix[w0 + i] = run;
+            run += __popc(words[w0 + i]);
+        }
+}
+
+// --------------------------------------------------------------------------------------- finish
+
+__global__ void k_stats_init(int* stats, unsigned long long* sums, int k1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k1; i += gridDim.x * blockDim.x) {
+        stats[i * 5 + 0] = 0x7fffffff;  // min x
+        stats[i * 5 + 1] = 0x7fffffff;  // min y
+        stats[i * 5 + 2] = -1;          // max x (turned into width)
+        stats[i * 5 + 3] = -1;          // max y (turned into height)
+        stats[i * 5 + 4] = 0;           // area
+        sums[2 * i] = 0;
+        sums[2 * i + 1] = 0;
+    }
+}
+
+// Final labels and stats. Each warp covers 32 consecutive pixels of one row, so equal labels form
+// runs of lanes; a run's head lane adds the run's bbox, area and coordinate sums with one set of
+// atomics. Background runs are reduced per block first.
+__global__ void __launch_bounds__(256) k_finish(Geo g, const int* parents, const unsigned int* roots,
+                                                const int* prefix, int* labels, int* stats,
+                                                unsigned long long* sums) {
+    __shared__ long long s_bg[7];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = blockIdx.x * 32 + lane;
+    const int y = blockIdx.y * 8 + warp;
+    const bool inside = x < g.W && y < g.H;
+    int lab = -1;  // -1 outside the image
+    if (inside) {
+        int p = parents[g.canon(y, x)];
+        if (p < 0) {
+            lab = 0;
+        } else {
+            int q = parents[p];
+            while (q != p) {
+                p = q;
+                q = parents[p];
+            }
+            lab = prefix[p >> 5] + __popc(roots[p >> 5] & ((1u << (p & 31)) - 1u)) + 1;
+        }
+        labels[(long long)y * g.W + x] = lab;
+    }
+    const int prev = __shfl_up_sync(0xffffffffu, lab, 1);
+    const bool head = lab >= 0 && (lane == 0 || prev != lab);
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const unsigned valid = __ballot_sync(0xffffffffu, lab >= 0);
+    // Run end: lane before the next head (or the last valid lane).
+    const unsigned later = heads & ~((2u << lane) - 1u);
+    int next = later ? __ffs(later) - 1 : 32;
+    const int last_valid = 31 - __clz(valid | 1u);
+    int tail = min(next - 1, last_valid);
+    if (head && lab > 0) {
+        const int x0 = x, x1 = x + (tail - lane);
+        const long long len = x1 - x0 + 1;
+        const long long sx = (long long)(x0 + x1) * len / 2;
+        int* st = stats + (long long)lab * 5;
+        atomicMin(&st[0], x0);
+        atomicMin(&st[1], y);
+        atomicMax(&st[2], x1);
+        atomicMax(&st[3], y);
+        atomicAdd(&st[4], (int)len);
+        atomicAdd(&sums[2LL * lab], (unsigned long long)sx);
+        atomicAdd(&sums[2LL * lab + 1], (unsigned long long)((long long)y * len));
+    }
+    // Background (label 0): one ballot per warp row, block totals in shared memory.
+    const unsigned bgm = __ballot_sync(0xffffffffu, lab == 0);
+    const int bx = lab == 0 ? x : 0;
+    const int bsum = warp_sum_i(bx);
+    if (threadIdx.x == 0) {
+        s_bg[0] = 0x7fffffff; s_bg[1] = 0x7fffffff; s_bg[2] = -1; s_bg[3] = -1; s_bg[4] = 0; s_bg[5] = 0; s_bg[6] = 0;
+    }
+    __syncthreads();
+    if (lane == 0 && bgm) {
+        const int x0 = blockIdx.x * 32;
+        atomicMin(&s_bg[0], (long long)(x0 + __ffs(bgm) - 1));
+        atomicMin(&s_bg[1], (long long)y);
+        atomicMax(&s_bg[2], (long long)(x0 + 31 - __clz(bgm)));
+        atomicMax(&s_bg[3], (long long)y);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[4]), (unsigned long long)__popc(bgm));
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[5]), (unsigned long long)bsum);
+        atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[6]), (unsigned long long)((long long)y * __popc(bgm)));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_bg[4] > 0) {
+        atomicMin(&stats[0], (int)s_bg[0]);
+        atomicMin(&stats[1], (int)s_bg[1]);
+        atomicMax(&stats[2], (int)s_bg[2]);
+        atomicMax(&stats[3], (int)s_bg[3]);
+        atomicAdd(&stats[4], (int)s_bg[4]);
+        atomicAdd(&sums[0], (unsigned long long)s_bg[5]);
+        atomicAdd(&sums[1], (unsigned long long)s_bg[6]);
+    }
+}
+
+// bbox max -> width/height; centroid = exact integer sum / area (as OpenCV).
+__global__ void k_stats_final(int* stats, const unsigned long long* sums, double* centroids, int k1) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k1; i += gridDim.x * blockDim.x) {
+        int* st = stats + (long long)i * 5;
+        const int area = st[4];
+        const unsigned long long sx = sums[2 * i], sy = sums[2 * i + 1];
+        if (area > 0) {
+            st[2] = st[2] - st[0] + 1;
+            st[3] = st[3] - st[1] + 1;
+            centroids[2 * i] = (double)sx / (double)area;
+            centroids[2 * i + 1] = (double)sy / (double)area;
+        } else {
+            st[0] = st[1] = st[2] = st[3] = 0;
+            centroids[2 * i] = dnan();
+            centroids[2 * i + 1] = dnan();
+        }
+    }
+}
+
+struct CclLayout {
+    long long canon_n;   // entries of the canonical parents array
+    long long words;     // root bitmap words
+    int scan_blocks;     // blocks of the popcount prefix
+    int* parents;
+    unsigned int* roots;
+    int* prefix;
+    int* block_sums;
+    int* scratch_count;
+};
+constexpr int kScanPerBlock = 4096;  // bitmap words per prefix block (1024 threads x 4)
+
+CclLayout ccl_layout(void* ws, int H, int W, size_t* bytes) {
+    CclLayout L;
+    const long long Hb = (H + 1) / 2, Wb = (W + 1) / 2;
+    L.canon_n = Hb * Wb * 4;  // >= H*W; also covers raster order for 4-connectivity
+    L.words = (L.canon_n + 31) / 32;
+    L.scan_blocks = (int)((L.words + kScanPerBlock - 1) / kScanPerBlock);
+    Arena a(ws);
+    L.parents = a.take<int>(L.canon_n);
+    L.roots = a.take<unsigned int>(L.words);
+    L.prefix = a.take<int>(L.words);
+    L.block_sums = a.take<int>(L.scan_blocks + 1);
+    L.scratch_count = a.take<int>(4);
+    if (bytes) *bytes = a.used;
+    return L;
+}
+
+}  // namespace
+}  // namespace spx
+
+using namespace spx;
+
+extern "C" {
+
+const char* spx_last_error(void) { return spx::g_error; }
+
+int spx_version(void) { return 1; }
+
+int spx_device_info(int* sm_count, int* is_sm100) {
+    int dev = 0;
+    SPX_CUDA(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    SPX_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (sm_count) *sm_count = prop.multiProcessorCount;
+    if (is_sm100) *is_sm100 = prop.major == 10 ? 1 : 0;
+    return SPX_OK;
+}
+
+size_t spx_otsu_workspace_bytes(int dtype) {
+    (void)dtype;
+    Arena a(nullptr);
+    a.take<unsigned int>(65536);
+    a.take<unsigned int>(2);
+    a.take<double>(4 * 65536);
+    return a.used;
+}
+
+int spx_otsu(const void* img, int dtype, int height, int width, int step, double* threshold,
+             void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(dtype == SPX_U8 || dtype == SPX_U16, "Otsu thresholding needs a uint8 or uint16 image");
+    SPX_REQUIRE(height > 0 && width > 0 && step >= 1, "bad image size or step");
+    SPX_REQUIRE(img && threshold && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_otsu_workspace_bytes(dtype), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Arena a(workspace);
+    unsigned int* hist = a.take<unsigned int>(65536);
+    unsigned int* range = a.take<unsigned int>(2);
+    const int nbins = dtype == SPX_U8 ? 256 : 65536;
+    SPX_CUDA(cudaMemsetAsync(hist, 0, 65536 * sizeof(unsigned int), s));
+    const unsigned int init[2] = {0xffffffffu, 0u};
+    SPX_CUDA(cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const long long n = (long long)hs * ws;
+    k_minmax<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(img, dtype, height, width, step, range);
+    if (int e = check_launch("k_minmax")) return e;
+    const size_t smem = kHistSmemBins * sizeof(unsigned int);
+    SPX_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int dense = step == 1 && dtype == SPX_U16 && (reinterpret_cast<uintptr_t>(img) % 16) == 0;
+    k_histogram<<<grid_for(n / 8 + 1, 512, 148 * 3), 512, smem, s>>>(img, dtype, height, width, step,
+                                                                     dense, range, hist);
+    if (int e = check_launch("k_histogram")) return e;
+    double* bufs = a.take<double>(4 * 65536);
+    k_otsu_scan<<<1, 1024, 0, s>>>(hist, nbins, range, n, bufs, bufs + 65536, bufs + 2 * 65536,
+                                   bufs + 3 * 65536, threshold);
+    return check_launch("k_otsu_scan");
+}
+
+int spx_triangle(const void* img, int dtype, int height, int width, double* threshold,
+                 void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(dtype == SPX_U8, "the triangle threshold needs a uint8 image");
+    SPX_REQUIRE(height > 0 && width > 0, "bad image size");
+    SPX_REQUIRE(img && threshold && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_otsu_workspace_bytes(dtype), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Arena a(workspace);
+    unsigned int* hist = a.take<unsigned int>(65536);
+    unsigned int* range = a.take<unsigned int>(2);
+    SPX_CUDA(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned int), s));
+    const unsigned int init[2] = {0u, 255u};
+    SPX_CUDA(cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const long long n = (long long)height * width;
+    const size_t smem = kHistSmemBins * sizeof(unsigned int);
+    SPX_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_histogram<<<grid_for(n, 512, 148 * 3), 512, smem, s>>>(img, dtype, height, width, 1, 0, range, hist);
+    if (int e = check_launch("k_histogram")) return e;
+    k_triangle_scan<<<1, 32, 0, s>>>(hist, threshold);
+    return check_launch("k_triangle_scan");
+}
+
+size_t spx_ccl_workspace_bytes(int height, int width) {
+    size_t b = 0;
+    ccl_layout(nullptr, height, width, &b);
+    return b;
+}
+
+int spx_ccl_label(const void* img, int dtype, int height, int width, const double* threshold_dev,
+                  double fixed_threshold, int invert, int connectivity, int* labels, int* count,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+    (void)labels;
+    SPX_REQUIRE(height > 0 && width > 0, "bad image size");
+    SPX_REQUIRE((long long)((height + 1) / 2) * ((width + 1) / 2) * 4 < 0x7fffffffLL,
+                "image too large for 32-bit labels");
+    SPX_REQUIRE(connectivity == 8 || connectivity == 4, "connectivity must be 4 or 8");
+    SPX_REQUIRE(dtype >= SPX_U8 && dtype <= SPX_F64, "bad dtype");
+    SPX_REQUIRE(img && count && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_ccl_workspace_bytes(height, width), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CclLayout L = ccl_layout(workspace, height, width, nullptr);
+    Geo g{height, width, (width + 1) / 2, connectivity};
+    SPX_CUDA(cudaMemsetAsync(L.roots, 0, L.words * sizeof(unsigned int), s));
+    if (connectivity == 8 && ((height & 1) || (width & 1)))  // padding entries of odd sizes
+        SPX_CUDA(cudaMemsetAsync(L.parents, 0xff, L.canon_n * sizeof(int), s));
+    const int tiles_x = (width + kTileW - 1) / kTileW, tiles_y = (height + kTileH - 1) / kTileH;
+    k_local_ccl<<<dim3(tiles_x, tiles_y), 256, 0, s>>>(img, dtype, g, threshold_dev, fixed_threshold,
+                                                       invert, L.parents, L.roots);
+    if (int e = check_launch("k_local_ccl")) return e;
+    const long long border = (long long)tiles_x * tiles_y * (kTileW + 2 * kTileH);
+    k_border_merge<<<grid_for(border, 256), 256, 0, s>>>(g, L.parents, L.roots, tiles_x, tiles_y);
+    if (int e = check_launch("k_border_merge")) return e;
+    SPX_REQUIRE(L.scan_blocks <= 1024 * 64, "image too large for the label prefix");
+    k_popc_block_sums<<<L.scan_blocks, 1024, 0, s>>>(L.roots, L.words, kScanPerBlock, L.block_sums);
+    if (int e = check_launch("k_popc_block_sums")) return e;
+    k_scan_small<<<1, 1024, 0, s>>>(L.block_sums, L.scan_blocks, count);
+    if (int e = check_launch("k_scan_small")) return e;
+    k_popc_prefix<<<L.scan_blocks, 1024, 0, s>>>(L.roots, L.words, kScanPerBlock, L.block_sums, L.prefix);
+    return check_launch("k_popc_prefix");
+}
+
+int spx_ccl_finish(int* labels, int height, int width, int connectivity, int num_components,
+                   int* stats, double* centroids, void* workspace, size_t workspace_bytes,
+                   void* stream) {
+    SPX_REQUIRE(labels && stats && centroids && workspace, "null pointer");
+    SPX_REQUIRE(num_components >= 0, "bad component count");
+    SPX_REQUIRE(workspace_bytes >= spx_ccl_workspace_bytes(height, width), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    CclLayout L = ccl_layout(workspace, height, width, nullptr);
+    Geo g{height, width, (width + 1) / 2, connectivity};
+    const int k1 = num_components + 1;
+    // The u64 coordinate sums live in the centroid array until the last kernel converts them.
+    unsigned long long* sums = reinterpret_cast<unsigned long long*>(centroids);
+    k_stats_init<<<grid_for(k1, 256), 256, 0, s>>>(stats, sums, k1);
+    if (int e = check_launch("k_stats_init")) return e;
+    k_finish<<<dim3((width + 31) / 32, (height + 7) / 8), 256, 0, s>>>(g, L.parents, L.roots, L.prefix,
+                                                                       labels, stats, sums);
+    if (int e = check_launch("k_finish")) return e;
+    k_stats_final<<<grid_for(k1, 256), 256, 0, s>>>(stats, sums, centroids, k1);
+    return check_launch("k_stats_final");
+}
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+"""detect_centers through the CUDA path against the reference CPU golden outputs and the oracle."""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import centers as oc
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = {"page": dict(threshold="otsu", area_max=400), "dots": dict(threshold="otsu", area_max=50),
+          "small": dict(threshold="otsu", area_max=200), "dots_tri": dict(threshold="triangle", area_max=50)}
+
+
+@pytest.mark.parametrize("refine", ["weighted", "logquad", "edge_gradmoment", "none", "auto"])
+def test_detect_centers_matches_reference_cpu(refine):
+    from imageprocessor_new_b200 import detect_centers
+
+    z = np.load(GOLDEN / "centers.npz")
+    for name in z["names"]:
+        img = z[f"{name}_img"]
+        got = detect_centers(img, backend="gpu", refine=refine, **PARAMS[str(name)])
+        want = z[f"{name}_{refine}"]
+        assert got.backend == "gpu"
+        assert got.centers_xy.shape == want.shape, (name, refine)
+        # weighted / none are exact on integer images; logquad solves normal equations and the edge
+        # moments use pow(d, 8), whose last bit may differ from the host libm.
+        tol = 1e-9 if refine in ("logquad", "auto", "edge_gradmoment") else 0.0
+        np.testing.assert_allclose(got.centers_xy, want, rtol=0, atol=tol, err_msg=f"{name} {refine}")
+
+
+@pytest.mark.parametrize("refine", ["weighted", "logquad", "edge_gradmoment"])
+def test_detect_centers_page_against_oracle(refine):
+    from imageprocessor_new_b200 import detect_centers, synthetic
+
+    page = synthetic.page_square(3).image
+    got = detect_centers(page, backend="gpu", threshold="otsu", refine=refine, area_max=400).centers_xy
+    want = oc.detect_centers(page, threshold="otsu", refine_method=refine, area_max=400)
+    assert got.shape == want.shape
+    np.testing.assert_allclose(got, want, rtol=0, atol=0.0 if refine == "weighted" else 1e-9)
+
+
+def test_detect_centers_invert_and_edges():
+    from imageprocessor_new_b200 import detect_centers, synthetic
+
+    page = synthetic.page_square(4).image
+    dark = (np.iinfo(np.uint16).max - page).astype(np.uint16)
+    got = detect_centers(dark, backend="gpu", threshold="otsu", invert=True, refine="weighted", area_max=400)
+    want = oc.detect_centers(dark, threshold="otsu", invert=True, refine_method="weighted", area_max=400)
+    assert got.centers_xy.shape == want.shape
+    np.testing.assert_array_equal(got.centers_xy, want)
+    # A blob cut by the image border.
+    crop = np.ascontiguousarray(page[5:300, 9:333])
+    for refine in ("weighted", "edge_gradmoment", "logquad"):
+        got = detect_centers(crop, backend="gpu", threshold="otsu", refine=refine, area_max=400).centers_xy
+        want = oc.detect_centers(crop, threshold="otsu", refine_method=refine, area_max=400)
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-9)
+
+
+def test_empty_image_has_no_centers():
+    from imageprocessor_new_b200 import detect_centers
+
+    img = np.zeros((64, 80), np.uint16)
+    res = detect_centers(img, backend="gpu", threshold="otsu")
+    assert res.centers_xy.shape == (0, 2)
+
+
+def test_bad_arguments_raise():
+    from imageprocessor_new_b200 import detect_centers
+
+    img = np.zeros((16, 16), np.uint16)
+    with pytest.raises(ValueError):
+        detect_centers(img, backend="gpu", refine="bogus")
+    with pytest.raises(ValueError):
+        detect_centers(img, backend="cpu")
+    with pytest.raises(ValueError):
+        detect_centers(np.zeros((4, 4, 3), np.uint8), backend="gpu")

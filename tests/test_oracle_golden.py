@@ -1,0 +1,67 @@
+"""The CPU oracle against the golden fixtures produced by the reference's own CPU path."""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import centers as oc
+from oracle import segment as osg
+from oracle import voronoi as ov
+
+
+def _load(name):
+    return np.load(GOLDEN / f"{name}.npz", allow_pickle=False)
+
+
+def test_otsu_and_triangle_match_opencv():
+    z = _load("thresholds")
+    for i in range(int(z["n"])):
+        img = z[f"img{i}"]
+        assert osg.otsu_threshold(img) == z["otsu"][i], i
+        if img.dtype == np.uint8:
+            assert osg.triangle_threshold(img) == z["triangle"][i], i
+
+
+@pytest.mark.parametrize("conn", [8, 4])
+def test_ccl_numbering_and_stats_match_opencv(conn):
+    z = _load("ccl")
+    for i in range(int(z["n"])):
+        shape = tuple(z[f"shape{i}"])
+        mask = np.unpackbits(z[f"mask{i}"])[: shape[0] * shape[1]].reshape(shape).astype(bool)
+        num, labels, stats, cents = osg.label_components(mask, conn)
+        np.testing.assert_array_equal(labels, z[f"labels{i}_{conn}"])
+        np.testing.assert_array_equal(stats[1:], z[f"stats{i}_{conn}"][1:])
+        np.testing.assert_array_equal(cents[1:], z[f"cent{i}_{conn}"][1:])
+        # Background row: area and bbox as OpenCV.
+        np.testing.assert_array_equal(stats[0], z[f"stats{i}_{conn}"][0])
+
+
+def test_detect_centers_match_reference_cpu():
+    z = _load("centers")
+    params = {"page": dict(threshold="otsu", area_max=400), "dots": dict(threshold="otsu", area_max=50),
+              "small": dict(threshold="otsu", area_max=200), "dots_tri": dict(threshold="triangle", area_max=50)}
+    for name in z["names"]:
+        img = z[f"{name}_img"]
+        for refine in ("weighted", "logquad", "edge_gradmoment", "none", "auto"):
+            got = oc.detect_centers(img, refine_method=refine, **params[str(name)])
+            want = z[f"{name}_{refine}"]
+            assert got.shape == want.shape, (name, refine)
+            tol = 1e-9 if refine in ("logquad", "auto") else 0.0
+            np.testing.assert_allclose(got, want, rtol=0, atol=tol, err_msg=f"{name} {refine}")
+
+
+def test_voronoi_labels_match_reference():
+    z = _load("voronoi")
+    for name in z["names"]:
+        seeds, shape = z[f"{name}_seeds"], tuple(z[f"{name}_shape"])
+        np.testing.assert_array_equal(ov.voronoi_labels(seeds, shape), z[f"{name}_labels"], err_msg=str(name))
+
+
+def test_tiled_rules_match_reference():
+    z = _load("tiled")
+    got = oc.detect_tiled(z["img"], tile_h=int(z["tile_h"]), overlap=int(z["overlap"]), area_max=200,
+                          refine_method="logquad")
+    want = z["centers"]
+    assert got.shape == want.shape
+    key = lambda a: a[np.lexsort((a[:, 1], a[:, 0]))]
+    np.testing.assert_allclose(key(got), key(want), rtol=0, atol=1e-9)
