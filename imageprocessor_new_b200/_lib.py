@@ -29,6 +29,24 @@ _I = c_int
 _D = c_double
 _S = c_size_t
 
+class BgMap(ctypes.Structure):
+    """spx_bgmap (include/subpx_b200.h)."""
+
+    _fields_ = [("rows", c_void_p), ("j1", c_void_p), ("t", c_void_p), ("ny", c_int), ("width", c_int),
+                ("fixed", c_double), ("mode", c_int)]
+
+
+class MethodOut(ctypes.Structure):
+    """spx_method_out (include/subpx_b200.h)."""
+
+    _fields_ = [("centers", c_void_p), ("contours", c_void_p), ("status", c_void_p), ("metrics", c_void_p),
+                ("center_local", c_void_p), ("edge_px", c_void_p), ("eigenvalues", c_void_p), ("axes", c_void_p),
+                ("n_metrics", c_int)]
+
+
+_BG = POINTER(BgMap)
+_MO = POINTER(MethodOut)
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "spx_last_error": (ctypes.c_char_p, []),
@@ -45,7 +63,32 @@ SIGNATURES = {
     "spx_refine_centers": (_I, [_P, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P]),
     "spx_voronoi_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_voronoi_labels": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_seed_distance_map": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_nearest_distances": (_I, [_P, _I, _P, _I, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_cells_setup": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "spx_fit_workspace_bytes": (_S, [_I]),
+    "spx_deblend_initial": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _D, _I, _I, _P, _P, _P, _P,
+                                 _S, _P]),
+    "spx_deblend_iteration": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _I, _I, _I, _BG, _P, _I, _P, _D, _I, _P,
+                                   _P, _P, _P, _P, _S, _P]),
+    "spx_render_workspace_bytes": (_S, [_I, _I, _I]),
+    "spx_render_model": (_I, [_P, _P, _I, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_clean_cells": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _BG, _P, _P, _I, _I, _I, _P, _P]),
+    "spx_tile_medians": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _D, _D, _I, _P, _P, _P]),
+    "spx_background_rows": (_I, [_P, _I, _I, _I, _I, _P, _P]),
+    "spx_residual": (_I, [_P, _I, _D, _I, _I, _BG, _P, _P, _P]),
+    "spx_gaussian_filter": (_I, [_P, _I, _I, _P, _I, _P, _P, _P]),
+    "spx_maximum_filter": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "spx_find_peaks": (_I, [_P, _P, _P, _I, _I, _D, _P, _I, _P, _P]),
+    "spx_label_mask": (_I, [_P, _P, _I, _I, _I, _P, _P, _P]),
+    "spx_gaussian_method": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _MO, _P]),
+    "spx_logquad_cd": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _MO, _P]),
+    "spx_radial_workspace_bytes": (_S, [_I, _I]),
+    "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _MO, _MO, _P, _S, _P]),
 }
+
+BG_MAP, BG_FIXED = 0, 1
+TILE_FREE, TILE_USABLE, TILE_ALL = 0, 1, 2
 
 
 class LibraryError(RuntimeError):

@@ -1,0 +1,496 @@
+"""measure_cds on the device: cells, deblending and CD measurements (drop-in for
+``subpx.measure_cds(..., backend="gpu")``, subpx/cd.py:44-380 and _measure_cds 424-784).
+
+Scope: ``background="model"`` with ``seeds="threshold"`` and the methods gaussian (deblended
+Gaussian FWHM), logquad, gradient and halfmax — the hot path. Every per-pixel and per-cell step
+runs in libsubpx_b200; the host keeps the reference's orchestration (validation, the seed revision
+bookkeeping, result assembly).
+"""
+
+from __future__ import annotations
+
+import time
+
+import numpy as np
+import torch
+
+from . import _device as dev
+from . import _lib
+from . import segment
+from .deblend import FWHM_K, STATUS, Deblender, build_cells, sigma_major
+from .types import CDMethodResult, CDResult, CDSummary
+
+METHOD_LABELS = {
+    "gaussian": "Deblended Gaussian FWHM",
+    "logquad": "Gaussian FWHM",
+    "gradient": "Maximum radial gradient",
+    "halfmax": "Half-height contour",
+}
+SUPPORTED = tuple(METHOD_LABELS)
+# Methods of the reference that are outside this package (invariant, local, outline families).
+OTHER_METHODS = ("disk", "flux_ratio", "projection", "half_area", "half_area_min", "half_area_min_avg",
+                 "tail_area", "tail_area_norm", "edge_area", "foot_area", "foot_area_ratio", "local_projection",
+                 "local_half_area", "local_half_area_min_avg", "local_tail_area", "outline_fit", "outline_fit_fast")
+
+GEOMETRY_METRICS = ("area_px2", "cd_equivalent_px", "cd_x_px", "cd_y_px", "perimeter_px")
+FIT_METRICS = ("sigma_major_px", "sigma_minor_px", "fwhm_major_px", "fwhm_minor_px", "angle_deg", "log_fit_rmse")
+# Device metric columns (include/subpx_b200.h): 0-4 geometry, 5 background, 6 peak_signal, 7.. method.
+_COLS = GEOMETRY_METRICS + ("background", "peak_signal")
+
+
+def _metric_names(method: str) -> tuple[str, ...]:
+    if method == "logquad":
+        return _COLS + FIT_METRICS
+    if method == "gaussian":
+        return _COLS + FIT_METRICS[:-1] + ("fit_rmse",)
+    return _COLS + ("ray_coverage",)
+
+
+def _validate(img, *, methods, background, seeds, threshold, area_min, area_max, pad, n_angles, radial_step,
+              smooth_sigma, fit_fraction, deblend_iterations, deblend_tolerance, pixel_size, unit, metrics_only,
+              summary_only, peak_min_distance, background_tile, background_level):
+    """The reference's argument checks (subpx/cd.py:286-365), same messages."""
+    if img.ndim != 2 or img.size == 0 or not np.issubdtype(img.dtype, np.number):
+        raise ValueError("image must be a nonempty 2D real grayscale array")
+    if np.iscomplexobj(img) or not np.isfinite(img).all():
+        raise ValueError("image must contain finite real intensities")
+    if background not in {"model", "border"}:
+        raise ValueError("background must be 'model' or 'border'")
+    if seeds not in {"threshold", "peaks"}:
+        raise ValueError("seeds must be 'threshold' or 'peaks'")
+    if seeds == "peaks" and background == "border":
+        raise ValueError("seeds='peaks' requires background='model'")
+    if methods is None:
+        methods = ("gaussian", "logquad", "gradient", "halfmax") if background == "model" else (
+            "logquad", "gradient", "halfmax")
+    if isinstance(methods, str):
+        methods = (methods,)
+    methods = tuple(methods)
+    known = SUPPORTED + OTHER_METHODS
+    if not methods or len(set(methods)) != len(methods) or any(m not in known for m in methods):
+        raise ValueError("methods must be unique choices from " + ", ".join(known))
+    if "gaussian" in methods and background != "model":
+        raise ValueError("method 'gaussian' requires background='model'")
+    for name, value in (("metrics_only", metrics_only), ("summary_only", summary_only)):
+        if not isinstance(value, (bool, np.bool_)):
+            raise ValueError(f"{name} must be True or False")
+    if not np.isfinite(deblend_tolerance) or deblend_tolerance <= 0:
+        raise ValueError("deblend_tolerance must be positive")
+    for name, value, lower in (("area_min", area_min, 1), ("area_max", area_max, area_min), ("pad", pad, 0),
+                               ("n_angles", n_angles, 16), ("deblend_iterations", deblend_iterations, 1)):
+        if not np.isfinite(value) or int(value) != value or value < lower:
+            raise ValueError(f"{name} must be an integer >= {lower}")
+    if not np.isfinite([radial_step, smooth_sigma, fit_fraction, pixel_size]).all():
+        raise ValueError("measurement parameters must be finite")
+    if not 0 < radial_step <= 1 or smooth_sigma < 0 or not 0 < fit_fraction < 1 or pixel_size <= 0:
+        raise ValueError("require 0 < radial_step <= 1, smooth_sigma >= 0, 0 < fit_fraction < 1, pixel_size > 0")
+    for name, value, lower in (("peak_min_distance", peak_min_distance, 1.0), ("background_tile", background_tile, 4)):
+        if value is not None and (not np.isfinite(value) or value < lower):
+            raise ValueError(f"{name} must be >= {lower}")
+    if background_level is not None and not np.isfinite(background_level):
+        raise ValueError("background_level must be finite")
+    if not isinstance(unit, str) or not unit.strip():
+        raise ValueError("unit must be a nonempty length-unit label")
+    if unit == "px" and pixel_size != 1:
+        raise ValueError("supply a physical unit when pixel_size differs from 1")
+    return methods
+
+
+def measure_cds(
+    image: np.ndarray,
+    *,
+    methods: tuple[str, ...] | None = None,
+    background: str = "model",
+    seeds: str = "threshold",
+    threshold: str = "otsu",
+    invert: bool = False,
+    area_min: int = 3,
+    area_max: int = 50,
+    pad: int = 3,
+    n_angles: int = 128,
+    radial_step: float = 0.1,
+    smooth_sigma: float = 0.0,
+    fit_fraction: float = 0.2,
+    peak_min_distance: float | None = None,
+    background_level: float | None = None,
+    background_tile: int | None = None,
+    deblend_iterations: int = 30,
+    deblend_tolerance: float = 1e-3,
+    pixel_size: float = 1.0,
+    unit: str = "px",
+    backend: str = "gpu",
+    cell_backend: str | None = None,
+    device: int = 0,
+    metrics_only: bool = False,
+    summary_only: bool = False,
+    **other,
+) -> CDResult | CDSummary:
+    """Voronoi cells and their CDs (subpx/cd.py:44-380) on the GPU.
+
+    Cells, background map, Gaussian deblending and the gaussian / logquad / gradient / halfmax
+    measurements follow the reference CPU path operation for operation (FP64). Parameters of the
+    reference's other method families (``nominal_cd``, ``psf_fwhm``, ``half_area_level``, ...) are
+    accepted in ``other`` and must keep their defaults.
+    """
+    img = np.asarray(image.detach().cpu().numpy() if isinstance(image, torch.Tensor) else image)
+    methods = _validate(img, methods=methods, background=background, seeds=seeds, threshold=threshold,
+                        area_min=area_min, area_max=area_max, pad=pad, n_angles=n_angles, radial_step=radial_step,
+                        smooth_sigma=smooth_sigma, fit_fraction=fit_fraction, deblend_iterations=deblend_iterations,
+                        deblend_tolerance=deblend_tolerance, pixel_size=pixel_size, unit=unit,
+                        metrics_only=metrics_only, summary_only=summary_only, peak_min_distance=peak_min_distance,
+                        background_tile=background_tile, background_level=background_level)
+    if backend not in {"cpu", "gpu", "auto"}:
+        raise ValueError("backend must be 'cpu', 'gpu' or 'auto'")
+    if cell_backend not in {None, "cpu", "gpu"}:
+        raise ValueError("cell_backend must be 'cpu' or 'gpu'")
+    if backend == "cpu" or cell_backend == "cpu":
+        raise ValueError("imageprocessor_new_b200 is the GPU backend: use backend='gpu' (or 'auto')")
+    if background != "model":
+        raise ValueError("backend='gpu' requires background='model'; border mode runs on the CPU")
+    if seeds != "threshold":
+        raise NotImplementedError("seeds='peaks' is not part of this package yet")
+    unsupported = [m for m in methods if m not in SUPPORTED]
+    if unsupported:
+        raise NotImplementedError("methods outside the hot path: " + ", ".join(unsupported))
+    if smooth_sigma > 0:
+        raise NotImplementedError("smooth_sigma > 0 is not part of this package yet")
+    metrics_only = bool(metrics_only) or bool(summary_only)
+    with dev.on_device(device):
+        return _measure_cds(img, methods=methods, threshold=threshold, invert=bool(invert), area_min=int(area_min),
+                            area_max=int(area_max), pad=int(pad), n_angles=int(n_angles),
+                            radial_step=float(radial_step), fit_fraction=float(fit_fraction),
+                            background_level=background_level, background_tile=background_tile,
+                            deblend_iterations=int(deblend_iterations), deblend_tolerance=float(deblend_tolerance),
+                            pixel_size=float(pixel_size), unit=unit, device=int(device), metrics_only=metrics_only,
+                            summary_only=bool(summary_only))
+
+
+def _segment(img: np.ndarray, img_d: torch.Tensor, threshold: str, invert: bool):
+    """Binary components of the reference's segmentation (subpx/cd.py:472-481): uint8 and uint16 +
+    Otsu images are thresholded as they are, others are scaled to uint8 first."""
+    rescaled = img.dtype != np.uint8 and not (img.dtype == np.uint16 and threshold == "otsu")
+    seg = img_d
+    if rescaled:
+        gray = img_d.to(torch.float64)
+        lo, hi = float(gray.min()), float(gray.max())
+        span = hi - lo
+        if span:
+            seg = torch.round((gray - lo) * (255 / span)).to(torch.uint8)
+        else:
+            seg = torch.zeros(img.shape, dtype=torch.uint8, device="cuda")
+    thr = segment.binarize_threshold(seg, threshold, invert)
+    comp = segment.label(seg, threshold=thr, invert=invert, connectivity=8)
+    return comp, rescaled
+
+
+def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
+    names = _metric_names(method)
+    b = {
+        "centers": dev.empty((max(n, 1), 2), torch.float64),
+        "contours": dev.empty((max(n, 1), n_angles + 1, 2), torch.float64) if contours else None,
+        "status": dev.empty((max(n, 1),), torch.uint8),
+        "metrics": dev.empty((max(n, 1), max(len(names), 13)), torch.float64),
+        "center_local": dev.empty((max(n, 1), 2), torch.float64),
+        "edge_px": dev.empty((max(n, 1), n_angles), torch.float64) if method in ("gradient", "halfmax") else None,
+        "eigenvalues": dev.empty((max(n, 1), 2), torch.float64) if method in ("logquad", "gaussian") else None,
+        "axes": dev.empty((max(n, 1), 2, 2), torch.float64) if method in ("logquad", "gaussian") else None,
+    }
+    struct = _lib.MethodOut(*(None if b[k] is None else b[k].data_ptr() for k in
+                              ("centers", "contours", "status", "metrics", "center_local", "edge_px", "eigenvalues",
+                               "axes")), b["metrics"].shape[1])
+    return b, struct
+
+
+def _to_result(method: str, n: int, b: dict, metrics_only: bool, n_angles: int) -> CDMethodResult:
+    names = _metric_names(method)
+    m = b["metrics"][:n].cpu().numpy()
+    status = STATUS[b["status"][:n].cpu().numpy()]
+    metrics = {name: np.ascontiguousarray(m[:, k]) for k, name in enumerate(names)}
+    if b["contours"] is not None:
+        contours = b["contours"][:n].cpu().numpy()
+    else:
+        contours = np.empty((n, 0 if metrics_only else n_angles + 1, 2))
+    geometry = {}
+    if method == "logquad":
+        geometry = {"center_local": b["center_local"][:n].cpu().numpy(),
+                    "eigenvalues": b["eigenvalues"][:n].cpu().numpy(), "axes": b["axes"][:n].cpu().numpy()}
+    elif method in ("gradient", "halfmax"):
+        geometry = {"center_local": b["center_local"][:n].cpu().numpy(), "edge_px": b["edge_px"][:n].cpu().numpy()}
+    elif not metrics_only:
+        geometry = {"eigenvalues": b["eigenvalues"][:n].cpu().numpy(), "axes": b["axes"][:n].cpu().numpy()}
+    return CDMethodResult(method=method, centers_xy=b["centers"][:n].cpu().numpy(), contours_xy=contours,
+                          valid=status == "ok", status=status, metrics=metrics, geometry=geometry)
+
+
+def _revise_seeds(dbl: Deblender, state, seeds_xy, pitch, oversized_d, *, drop_fraction=0.3, add_fraction=0.5):
+    """Seeds to drop and holes to add after one deblending pass (subpx/_cpu/deblend.py:525-567)."""
+    p = state.params
+    finite = np.isfinite(p).all(axis=1)
+    good = finite & (state.status_codes == 0) & (p[:, 0] > 0)
+    if not good.any():
+        return np.zeros(len(p), bool), np.zeros((0, 2))
+    reference = float(np.median(p[good, 0]))
+    drop = ~finite | (p[:, 0] < drop_fraction * reference)
+    h, w = dbl.shape
+    resid = dev.empty((h, w), torch.float64)
+    _lib.call("spx_residual", dbl.img.data_ptr(), dbl.dtype, dbl.sign, h, w, state.background.struct(),
+              state.model.data_ptr(), resid.data_ptr(), dev.stream_ptr())
+    sigma = max(0.5, 0.1 * pitch)
+    radius_g = int(4.0 * sigma + 0.5)
+    x = np.arange(-radius_g, radius_g + 1)
+    phi = np.exp(-0.5 / (sigma * sigma) * x ** 2)
+    weights = dev.upload(phi / phi.sum())
+    tmp = dev.empty((h, w), torch.float64)
+    smooth = dev.empty((h, w), torch.float64)
+    _lib.call("spx_gaussian_filter", resid.data_ptr(), h, w, weights.data_ptr(), radius_g, tmp.data_ptr(),
+              smooth.data_ptr(), dev.stream_ptr())
+    radius = max(1, int(np.floor(0.5 * pitch)))
+    maxf = resid  # reuse
+    _lib.call("spx_maximum_filter", smooth.data_ptr(), h, w, radius, tmp.data_ptr(), maxf.data_ptr(),
+              dev.stream_ptr())
+    count = dev.empty((1,), torch.int32)
+    cap = 1 << 16
+    peaks = dev.empty((cap, 2), torch.int32)
+    _lib.call("spx_find_peaks", smooth.data_ptr(), maxf.data_ptr(), dev.ptr(oversized_d), h, w,
+              float(add_fraction * reference), peaks.data_ptr(), cap, count.data_ptr(), dev.stream_ptr())
+    k = dev.read_int(count)
+    if k > cap:
+        peaks = dev.empty((k, 2), torch.int32)
+        _lib.call("spx_find_peaks", smooth.data_ptr(), maxf.data_ptr(), dev.ptr(oversized_d), h, w,
+                  float(add_fraction * reference), peaks.data_ptr(), k, count.data_ptr(), dev.stream_ptr())
+    yx = peaks[:k].cpu().numpy().astype(np.int64)
+    order = np.lexsort((yx[:, 1], yx[:, 0]))  # np.nonzero order: row-major
+    yx = yx[order]
+    new = np.column_stack((yx[:, 1], yx[:, 0])).astype(float)
+    kept = np.asarray(seeds_xy, float)[~drop]
+    if len(new) and len(kept):
+        kd = dev.upload(np.ascontiguousarray(kept))
+        qd = dev.upload(np.ascontiguousarray(new))
+        dist = dev.empty((len(new),), torch.float64)
+        ws = dev.workspace(_lib.size("spx_voronoi_workspace_bytes", len(kept), h, w))
+        _lib.call("spx_nearest_distances", kd.data_ptr(), len(kept), qd.data_ptr(), len(new), 0, h, w,
+                  dist.data_ptr(), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+        new = new[dist.cpu().numpy() > 0.5 * pitch]
+    return drop, new
+
+
+def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_angles, radial_step, fit_fraction,
+                 background_level, background_tile, deblend_iterations, deblend_tolerance, pixel_size, unit, device,
+                 metrics_only, summary_only):
+    started = time.perf_counter()
+    seconds = {}
+    height, width = img.shape
+    sign = -1.0 if invert else 1.0
+    img_d = dev.upload(img if img.dtype in _lib.DTYPES else img.astype(np.float64))
+    comp, rescaled = _segment(img, img_d, threshold, invert)
+    stats = comp.stats.cpu().numpy()
+    cents = comp.centroids.cpu().numpy()
+    k = comp.count
+    components_before_filter = k
+    x, y, w, h, area = stats[1:k + 1].astype(np.int64).T
+    keep = (area >= area_min) & (area <= area_max)
+    oversized_flags = np.zeros(k + 1, np.uint8)
+    oversized_flags[1:][area > area_max] = 1
+    inside = ~((x <= 0) | (y <= 0) | (x + w >= width) | (y + h >= height))
+    rows = np.column_stack((x, y, w, h, cents[1:k + 1])).astype(np.float64)[keep]
+    component_ids = (np.flatnonzero(keep) + 1).astype(np.int32)
+    interior = inside[keep]
+    labels_d = comp.labels
+    tmp8 = dev.empty((height, width), torch.uint8)
+    oversized_d = None
+    if oversized_flags.any():
+        oversized_d = dev.empty((height, width), torch.uint8)
+        _lib.call("spx_label_mask", labels_d.data_ptr(), dev.upload(oversized_flags).data_ptr(), height, width, 0,
+                  oversized_d.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
+
+    def exclude_for(ids):
+        flags = np.ones(k + 1, np.uint8)
+        flags[0] = 0
+        ids = ids[(ids >= 0) & (ids <= k)]
+        flags[ids] = 0
+        out = dev.empty((height, width), torch.uint8)
+        _lib.call("spx_label_mask", labels_d.data_ptr(), dev.upload(flags).data_ptr(), height, width, 2,
+                  out.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
+        return out
+
+    cells = build_cells(rows, img.shape, pad)
+    seconds["segmentation"] = time.perf_counter() - started
+    meta = {
+        "background": "model", "seeds": "threshold", "threshold": threshold, "invert": bool(invert),
+        "area_min": int(area_min), "area_max": int(area_max), "pad": int(pad), "n_angles": int(n_angles),
+        "radial_step": float(radial_step), "smooth_sigma": 0.0, "fit_fraction": float(fit_fraction),
+        "cell_backend": "gpu", "measurement_backend": "gpu", "device": int(device),
+        "metrics_only": bool(metrics_only), "summary_only": bool(summary_only),
+        "deblend_tolerance": float(deblend_tolerance), "segmentation_rescaled": bool(rescaled),
+        "components_before_filter": int(components_before_filter),
+        "coordinates": "global [x, y] pixels; images indexed [y, x]", "seconds": seconds,
+    }
+    start = time.perf_counter()
+    by_reach = np.zeros(len(rows), bool)
+    level = None if background_level is None else sign * float(background_level)
+
+    def make_deblender(cells_, tile):
+        return Deblender(img_d, sign, cells_, exclude_d=exclude_for(component_ids), tile=tile,
+                         background_level=level, tolerance=deblend_tolerance)
+
+    from .deblend import auto_tile
+
+    tile_px, pitch = auto_tile(cells.seeds_d, cells.n, img.shape)
+    tiled_seeds = cells
+
+    def tile_for(cells_):
+        if background_tile is not None or cells_ is not tiled_seeds:
+            return background_tile
+        return tile_px
+
+    passes = []
+    added = dropped = 0
+    state = dbl = None
+    for revision in range(3):
+        final = revision == 2 or not np.isfinite(pitch)
+        dbl = make_deblender(cells, tile_for(cells))
+        state = dbl.run(iterations=deblend_iterations if final else min(10, deblend_iterations))
+        passes.append(int(state.iterations))
+        if final:
+            break
+        drop, new = _revise_seeds(dbl, state, cells.seeds, pitch, oversized_d)
+        if not drop.any() and not len(new):
+            if state.converged or state.iterations >= deblend_iterations:
+                break
+            state = dbl.run(iterations=deblend_iterations - state.iterations, init=state.params)
+            passes.append(int(state.iterations))
+            break
+        keep_s = ~drop
+        half = int(np.ceil(0.6 * pitch))
+        rows = np.concatenate((rows[keep_s], np.array([[px - half, py - half, 2 * half + 1, 2 * half + 1, px, py]
+                                                       for px, py in new], dtype=np.float64).reshape(-1, 6)))
+        component_ids = np.concatenate((component_ids[keep_s], np.full(len(new), -1, np.int32)))
+        interior = np.concatenate((interior[keep_s], np.ones(len(new), bool)))
+        by_reach = np.concatenate((by_reach[keep_s], np.ones(len(new), bool)))
+        added, dropped = added + len(new), dropped + int(drop.sum())
+        cells = build_cells(rows, img.shape, pad)
+    if by_reach.any():
+        params = state.params[by_reach]
+        centers = params[:, 1:3] + cells.origins[by_reach]
+        reach = np.where(np.isfinite(params).all(axis=1), 2 * FWHM_K * sigma_major(params), np.inf)
+        interior[by_reach] = ((centers[:, 0] - reach > 0) & (centers[:, 0] + reach < width - 1)
+                              & (centers[:, 1] - reach > 0) & (centers[:, 1] + reach < height - 1))
+    report = np.flatnonzero(interior).astype(np.int32)
+    nr = len(report)
+    cleaned = dbl.cleaned(state, report)
+    report_d = dev.upload(report) if nr else None
+    seconds["deblend"], start = time.perf_counter() - start, time.perf_counter()
+    found = {}
+    stream = dev.stream_ptr()
+    c = cells
+    radial = [m for m in methods if m in ("gradient", "halfmax")]
+    bufs = {}
+    if radial and nr:
+        hb = _method_buffers(nr, n_angles, "halfmax", not metrics_only) if "halfmax" in radial else (None, None)
+        gb = _method_buffers(nr, n_angles, "gradient", not metrics_only) if "gradient" in radial else (None, None)
+        ws = dev.workspace(_lib.size("spx_radial_workspace_bytes", c.hm, c.wm))
+        _lib.call("spx_radial_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(),
+                  nr, c.hm, c.wm, width, n_angles, radial_step,
+                  None if hb[1] is None else hb[1], None if gb[1] is None else gb[1], ws.data_ptr(), ws.numel(),
+                  stream)
+        if hb[0] is not None:
+            bufs["halfmax"] = hb[0]
+        if gb[0] is not None:
+            bufs["gradient"] = gb[0]
+    if "logquad" in methods and nr:
+        lb = _method_buffers(nr, n_angles, "logquad", not metrics_only)
+        _lib.call("spx_logquad_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(),
+                  c.seeds_d.data_ptr(), nr, c.hm, c.wm, width, n_angles, fit_fraction, lb[1], stream)
+        bufs["logquad"] = lb[0]
+    seconds["radial"], start = time.perf_counter() - start, time.perf_counter()
+    if "gaussian" in methods and nr:
+        gb2 = _method_buffers(nr, n_angles, "gaussian", not metrics_only)
+        _lib.call("spx_gaussian_method", state.params_d.data_ptr(), state.status_d.data_ptr(), cleaned.data_ptr(),
+                  c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(), nr, c.hm, c.wm, width, n_angles,
+                  gb2[1], stream)
+        bufs["gaussian"] = gb2[0]
+    for name in methods:
+        if nr:
+            found[name] = _to_result(name, nr, bufs[name], metrics_only, n_angles)
+        else:
+            found[name] = _empty_result(name, n_angles, metrics_only)
+    seconds["gaussian"], start = time.perf_counter() - start, time.perf_counter()
+    local_background = sign * state.background.at_points(c.seeds[report]) if nr else np.zeros(0)
+    measurements = {}
+    for name in methods:
+        found[name].metrics["background"][:] = local_background
+        measurements[name] = found[name]
+    statuses, counts = np.unique(state.status[report], return_counts=True)
+    info = state.background_info
+    meta.update(
+        background_definition=("Smooth map fitted jointly with one 2-D Gaussian per hole; measured cells have the map "
+                               "and all other holes' models removed"),
+        background_source=info.get("source"), background_tiles=info.get("tiles"),
+        background_measured_tiles=info.get("measured_tiles"), background_tile_px=int(state.tile_px),
+        background_level=background_level, deblend_iterations=int(deblend_iterations),
+        deblend_iterations_used=sum(passes), deblend_passes=len(passes), deblend_pass_iterations=passes,
+        deblend_converged=bool(state.converged),
+        deblend_status_counts=dict(zip(statuses.tolist(), counts.tolist())), modelled_holes=int(len(rows)),
+        seeds_added_from_residual=int(added), seeds_dropped_as_insignificant=int(dropped),
+        pitch_px=float(pitch) if np.isfinite(pitch) else None,
+        cell_stack_shape=[int(c.hm), int(c.wm)],
+    )
+    if summary_only:
+        result = CDSummary(seeds_xy=c.seeds[report], measurements=measurements, pixel_size=float(pixel_size),
+                           unit=unit, meta=meta)
+        seconds["result"] = time.perf_counter() - start
+        seconds["total"] = time.perf_counter() - started
+        return result
+    vor = c.voronoi.cpu().numpy()
+    remap = np.full(len(rows) + 1, -1, dtype=np.int32)
+    remap[report] = np.arange(nr, dtype=np.int32)
+    cell_labels = remap[vor]
+    params_global = state.params.copy()
+    params_global[:, 1:3] += c.origins
+    deblend_model = {"params": params_global, "report": report.astype(np.int64), "tile_px": int(state.tile_px)}
+    if "tile_medians" in info:
+        deblend_model["tile_medians"] = info["tile_medians"]
+    if metrics_only:
+        rois, masks = np.empty((nr, 0, 0)), np.empty((nr, 0, 0), bool)
+    else:
+        rois = cleaned.cpu().numpy()
+        masks = _mask_stack(c, report)
+    result = CDResult(
+        image=img.copy(), binary=comp.labels.cpu().numpy() > 0, component_labels=comp.labels.cpu().numpy(),
+        component_ids=np.asarray(component_ids, dtype=np.int32)[report],
+        boxes_xywh=rows[report, :4].astype(np.int32), seeds_xy=c.seeds[report], cell_labels=cell_labels,
+        cell_areas_px2=np.bincount(cell_labels[cell_labels >= 0], minlength=nr), origins_xy=c.origins[report],
+        rois=rois, masks=masks, measurements=measurements, pixel_size=float(pixel_size), unit=unit,
+        background_map=sign * state.background.host_map(), deblend_model=deblend_model, meta=meta,
+    )
+    seconds["result"] = time.perf_counter() - start
+    seconds["total"] = time.perf_counter() - started
+    return result
+
+
+def _mask_stack(c, report) -> np.ndarray:
+    """(n, hm, wm) masks: label == j inside each cell's box (subpx/_gpu/cells.py:31-36)."""
+    h, w = c.voronoi.shape
+    rep = torch.as_tensor(report, dtype=torch.int64, device="cuda")
+    boxes = c.boxes.to(torch.int64)[rep]
+    r = torch.arange(c.hm, device="cuda")
+    col = torch.arange(c.wm, device="cuda")
+    inside = (r[None] < boxes[:, 3:4])[:, :, None] & (col[None] < boxes[:, 2:3])[:, None, :]
+    ys = torch.clamp(boxes[:, 1:2] + r[None], 0, h - 1)[:, :, None]
+    xs = torch.clamp(boxes[:, 0:1] + col[None], 0, w - 1)[:, None, :]
+    return (inside & (c.voronoi.to(torch.int64)[ys, xs] == rep[:, None, None])).cpu().numpy()
+
+
+def _empty_result(method, n_angles, metrics_only) -> CDMethodResult:
+    names = _metric_names(method)
+    geometry = {}
+    if method == "logquad":
+        geometry = {"center_local": np.zeros((0, 2)), "eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}
+    elif method in ("gradient", "halfmax"):
+        geometry = {"center_local": np.zeros((0, 2)), "edge_px": np.zeros((0, n_angles))}
+    elif not metrics_only:
+        geometry = {"eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}
+    return CDMethodResult(method=method, centers_xy=np.zeros((0, 2)),
+                          contours_xy=np.zeros((0, 0 if metrics_only else n_angles + 1, 2)),
+                          valid=np.zeros(0, bool), status=np.zeros(0, "U32"),
+                          metrics={name: np.zeros(0) for name in names}, geometry=geometry)

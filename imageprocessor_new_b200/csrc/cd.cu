@@ -1,0 +1,833 @@
+// CD measurements of deblended cells, one warp per cell (every per-cell step on the device).
+//
+// Reference: subpx/_cpu/cd.py — _inside (19-25), _geometry (35-47), _logquad (50-89),
+// _half_max_ellipse (92-107), _ellipse_geometry (131-141), gaussian_method (144-192),
+// _radial_profiles (195-217), _radial_contour (220-264), measure_cells (267-322); the GPU
+// reference's ray kernel subpx/_gpu/cd.py:31-131 for the streaming form of the ray rules.
+//
+// The symmetric 2x2 eigen-decomposition follows LAPACK's published dsyevd path for n = 2 (dsteqr:
+// the deflation tests, then dlaev2, then ascending order), so eigenvector signs, and with them the
+// contour vertex order and angle_deg, agree with numpy.linalg.eigh. The cubic B-spline profiles
+// use Unser's recursive prefilter (pole sqrt(3) - 2) over the cell padded by 12 edge pixels, as
+// scipy.ndimage.map_coordinates(order=3, mode="nearest") does, and scipy's cubic weights.
+
+#include "common.cuh"
+#include "lm.cuh"
+
+namespace spx {
+namespace {
+
+constexpr double kFwhmK = 1.1774100225154747;  // sqrt(2 ln 2)
+constexpr double kPi = 3.141592653589793;
+constexpr int kPad = 12;
+
+// ------------------------------------------------------------------------------ 2x2 eigh
+
+struct Eig2 {
+    double w0, w1;          // ascending eigenvalues
+    double v00, v10;        // eigenvector of w0 (column 0: axes[0][0], axes[1][0])
+    double v01, v11;        // eigenvector of w1
+};
+
+// dlaev2(a, b, c): rt1 (larger in absolute value), rt2 and (cs1, sn1), the unit eigenvector of rt1.
+__device__ void dlaev2(double a, double b, double c, double* rt1, double* rt2, double* cs1, double* sn1) {
+    const double sm = __dadd_rn(a, c), df = __dsub_rn(a, c), adf = fabs(df);
+    const double tb = __dadd_rn(b, b), ab = fabs(tb);
+    double acmx, acmn;
+    if (fabs(a) > fabs(c)) { acmx = a; acmn = c; } else { acmx = c; acmn = a; }
+    double rt;
+    if (adf > ab) { const double q = __ddiv_rn(ab, adf); rt = __dmul_rn(adf, sqrt(__dadd_rn(1.0, __dmul_rn(q, q)))); }
+    else if (adf < ab) { const double q = __ddiv_rn(adf, ab); rt = __dmul_rn(ab, sqrt(__dadd_rn(1.0, __dmul_rn(q, q)))); }
+    else rt = __dmul_rn(ab, sqrt(2.0));
+    int sgn1;
+    if (sm < 0.0) {
+        *rt1 = __dmul_rn(0.5, __dsub_rn(sm, rt));
+        sgn1 = -1;
+        *rt2 = __dsub_rn(__dmul_rn(__ddiv_rn(acmx, *rt1), acmn), __dmul_rn(__ddiv_rn(b, *rt1), b));
+    } else if (sm > 0.0) {
+        *rt1 = __dmul_rn(0.5, __dadd_rn(sm, rt));
+        sgn1 = 1;
+        *rt2 = __dsub_rn(__dmul_rn(__ddiv_rn(acmx, *rt1), acmn), __dmul_rn(__ddiv_rn(b, *rt1), b));
+    } else {
+        *rt1 = __dmul_rn(0.5, rt);
+        *rt2 = __dmul_rn(-0.5, rt);
+        sgn1 = 1;
+    }
+    int sgn2;
+    double cs;
+    if (df >= 0.0) { cs = __dadd_rn(df, rt); sgn2 = 1; } else { cs = __dsub_rn(df, rt); sgn2 = -1; }
+    const double acs = fabs(cs);
+    if (acs > ab) {
+        const double ct = __ddiv_rn(-tb, cs);
+        *sn1 = __ddiv_rn(1.0, sqrt(__dadd_rn(1.0, __dmul_rn(ct, ct))));
+        *cs1 = __dmul_rn(ct, *sn1);
+    } else if (ab == 0.0) {
+        *cs1 = 1.0;
+        *sn1 = 0.0;
+    } else {
+        const double tn = __ddiv_rn(-cs, tb);
+        *cs1 = __ddiv_rn(1.0, sqrt(__dadd_rn(1.0, __dmul_rn(tn, tn))));
+        *sn1 = __dmul_rn(tn, *cs1);
+    }
+    if (sgn1 == sgn2) {
+        const double tn = *cs1;
+        *cs1 = -*sn1;
+        *sn1 = tn;
+    }
+}
+
+// numpy.linalg.eigh of [[a, b], [b, c]] (dsyevd, lower): eigenvalues ascending, columns of V.
+__device__ Eig2 eigh2(double a, double b, double c) {
+    const double eps = 1.1102230246251565e-16;      // dlamch('E')
+    const double safmin = 2.2250738585072014e-308;  // dlamch('S')
+    double d0 = a, d1 = c;
+    double z00 = 1.0, z01 = 0.0, z10 = 0.0, z11 = 1.0;
+    const double e = b;
+    // Initial splitting test of dsteqr.
+    bool split = e == 0.0 || fabs(e) <= __dmul_rn(__dmul_rn(sqrt(fabs(d0)), sqrt(fabs(d1))), eps);
+    if (!split) {
+        // QL when |d1| >= |d0|, QR otherwise; both test e^2 <= eps^2 |d_m| |d_m+1| + safmin and else
+        // rotate the 2x2 block with dlaev2 into (rt1, rt2) with vectors (cs, sn), (-sn, cs).
+        const double tst = __dmul_rn(fabs(e), fabs(e));
+        const double bound = (fabs(d1) < fabs(d0))
+                                 ? __dadd_rn(__dmul_rn(__dmul_rn(eps * eps, fabs(d1)), fabs(d0)), safmin)
+                                 : __dadd_rn(__dmul_rn(__dmul_rn(eps * eps, fabs(d0)), fabs(d1)), safmin);
+        if (!(tst <= bound)) {
+            double rt1, rt2, cs, sn;
+            dlaev2(d0, e, d1, &rt1, &rt2, &cs, &sn);
+            d0 = rt1;
+            d1 = rt2;
+            z00 = cs; z10 = sn;    // column 0
+            z01 = -sn; z11 = cs;   // column 1
+        }
+    }
+    Eig2 r;
+    if (d1 < d0) {  // selection sort: ascending, columns swapped with their values
+        r.w0 = d1; r.w1 = d0;
+        r.v00 = z01; r.v10 = z11; r.v01 = z00; r.v11 = z10;
+    } else {
+        r.w0 = d0; r.w1 = d1;
+        r.v00 = z00; r.v10 = z10; r.v01 = z01; r.v11 = z11;
+    }
+    return r;
+}
+
+// ---------------------------------------------------------------------------- shared pieces
+
+struct CellView {
+    const double* roi;  // hm x wm cleaned cell (zero outside its mask)
+    const int* vor;
+    int4 box;
+    int j;              // cell index in the Voronoi labels
+    int W, hm, wm;
+    __device__ __forceinline__ bool mask(int yy, int xx) const {
+        return yy >= 0 && xx >= 0 && yy < box.w && xx < box.z && yy < hm && xx < wm &&
+               vor[(long long)(box.y + yy) * W + (box.x + xx)] == j;
+    }
+};
+
+// Output slots of one method (per cell arrays; null pointers are skipped).
+struct MethodOut {
+    double* centers;     // n x 2 global
+    double* contours;    // n x (n_angles + 1) x 2 global, or null (metrics_only)
+    uint8_t* status;     // n
+    double* metrics;     // n x n_metrics, NaN where not measured
+    double* center_local;  // n x 2 (radial, logquad)
+    double* edge_px;     // n x n_angles (radial)
+    double* eigenvalues; // n x 2 (ellipse methods)
+    double* axes;        // n x 2 x 2 (ellipse methods)
+    int n_metrics;
+};
+
+// Metric columns (same order as the Python side).
+enum {
+    M_AREA = 0, M_CD_EQ = 1, M_CD_X = 2, M_CD_Y = 3, M_PERIM = 4, M_BACKGROUND = 5, M_PEAK = 6,
+    // ellipse methods
+    M_SIG_MAJ = 7, M_SIG_MIN = 8, M_FWHM_MAJ = 9, M_FWHM_MIN = 10, M_ANGLE = 11, M_RMSE = 12,
+    // radial methods
+    M_COVERAGE = 7
+};
+
+// Half-maximum ellipse: contour vertex k of center + (cos t_k, sin t_k) * (K sigma) @ axes^T.
+__device__ __forceinline__ void ellipse_vertex(double cx, double cy, const Eig2& e, double s0, double s1, double ang,
+                                               double* px, double* py) {
+    const double u = __dmul_rn(cos(ang), __dmul_rn(kFwhmK, s0));
+    const double v = __dmul_rn(sin(ang), __dmul_rn(kFwhmK, s1));
+    // (u, v) @ axes^T: x = u axes[0][0] + v axes[0][1]; y = u axes[1][0] + v axes[1][1]
+    *px = __dadd_rn(cx, __dadd_rn(__dmul_rn(u, e.v00), __dmul_rn(v, e.v01)));
+    *py = __dadd_rn(cy, __dadd_rn(__dmul_rn(u, e.v10), __dmul_rn(v, e.v11)));
+}
+
+// Warp-wide polygon geometry of the closed contour (n_angles + 1 vertices): shoelace area about
+// the first vertex, perimeter, x and y extents. Vertices come from `vertex(k, &x, &y)`.
+template <typename V>
+__device__ void polygon_geometry(int nv, V vertex, int lane, double* area, double* perim, double* ptpx,
+                                 double* ptpy) {
+    double x0, y0;
+    vertex(0, &x0, &y0);
+    double s = 0.0, p = 0.0, xmn = dinf(), xmx = -dinf(), ymn = dinf(), ymx = -dinf();
+    for (int k = lane; k < nv - 1; k += 32) {
+        double xa, ya, xb, yb;
+        vertex(k, &xa, &ya);
+        vertex(k + 1, &xb, &yb);
+        const double ax = xa - x0, ay = ya - y0, bx = xb - x0, by = yb - y0;
+        s += ax * by - bx * ay;
+        p += sqrt((xb - xa) * (xb - xa) + (yb - ya) * (yb - ya));
+        xmn = fmin(xmn, xa); xmx = fmax(xmx, xa); ymn = fmin(ymn, ya); ymx = fmax(ymx, ya);
+    }
+    if (lane == 0) {  // the closing vertex
+        double xa, ya;
+        vertex(nv - 1, &xa, &ya);
+        xmn = fmin(xmn, xa); xmx = fmax(xmx, xa); ymn = fmin(ymn, ya); ymx = fmax(ymx, ya);
+    }
+    s = warp_sum(s);
+    p = warp_sum(p);
+    *area = fabs(s) / 2.0;
+    *perim = p;
+    *ptpx = warp_max(xmx) - warp_min(xmn);
+    *ptpy = warp_max(ymx) - warp_min(ymn);
+}
+
+// map_coordinates(mask, order=1, mode='constant') >= 1 - 1e-8 (_inside).
+__device__ __forceinline__ bool inside_bilinear(const CellView& c, bool eroded, double y, double x) {
+    const double h1 = (double)(c.hm - 1), w1 = (double)(c.wm - 1);
+    if (!(y >= 0.0 && y <= h1 && x >= 0.0 && x <= w1)) return false;
+    const double fy = floor(y), fx = floor(x);
+    const int y0 = (int)fy, x0 = (int)fx;
+    const int ny = (y == fy) ? 1 : 2, nx = (x == fx) ? 1 : 2;
+    double v = 0.0;
+    for (int a = 0; a < ny; ++a) {
+        const double wy = a == 0 ? (fy + 1.0) - y : y - fy;
+        for (int b = 0; b < nx; ++b) {
+            const double wx = b == 0 ? (fx + 1.0) - x : x - fx;
+            bool m;
+            const int yy = y0 + a, xx = x0 + b;
+            if (eroded) {  // binary_erosion with the cross structure, border 0
+                m = c.mask(yy, xx) && yy > 0 && xx > 0 && yy < c.hm - 1 && xx < c.wm - 1 && c.mask(yy - 1, xx) &&
+                    c.mask(yy + 1, xx) && c.mask(yy, xx - 1) && c.mask(yy, xx + 1);
+            } else {
+                m = c.mask(yy, xx);
+            }
+            v += (m ? 1.0 : 0.0) * (wy * wx);
+        }
+    }
+    return v >= 1.0 - 1e-8;
+}
+
+// ---------------------------------------------------------------------- gaussian method
+
+// gaussian_method: params ROI-local; status in/out (non_gaussian_fit for eig0 <= 1e-10).
+__global__ void k_gaussian_method(const double* params, const uint8_t* status_in, const double* cleaned,
+                                  const int* vor, const int4* boxes, const int* which, int n, int hm, int wm,
+                                  int W, int n_angles, MethodOut out) {
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
+        const int j = which ? which[i] : i;
+        const double* p = params + 6LL * j;
+        const CellView c{cleaned + (long long)i * hm * wm, vor, boxes[j], j, W, hm, wm};
+        // fit_rmse over the mask, untruncated model.
+        const double e1 = exp(p[3]), e3 = exp(p[5]);
+        double ss = 0.0;
+        int cnt = 0;
+        for (int k = lane; k < hm * wm; k += 32) {
+            const int yy = k / wm, xx = k % wm;
+            if (!c.mask(yy, xx)) continue;
+            const GaussEval g = gauss_eval(p, e1, e3, (double)xx - p[1], (double)yy - p[2]);
+            const double r = c.roi[k] - p[0] * g.shape;
+            ss += r * r;
+            ++cnt;
+        }
+        ss = warp_sum(ss);
+        cnt = warp_sum_i(cnt);
+        double* m = out.metrics + (long long)i * out.n_metrics;
+        uint8_t st = status_in[j];
+        bool finite = true;
+        for (int q = 0; q < 6; ++q) finite = finite && isfinite(p[q]);
+        const int nv = n_angles + 1;
+        if (lane == 0) {
+            for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
+            m[M_PEAK] = p[0];
+            m[M_RMSE] = sqrt(ss / (double)max(cnt, 1));
+            out.centers[2LL * i] = out.centers[2LL * i + 1] = dnan();
+            if (out.eigenvalues) {
+                out.eigenvalues[2LL * i] = out.eigenvalues[2LL * i + 1] = dnan();
+                for (int q = 0; q < 4; ++q) out.axes[4LL * i + q] = dnan();
+            }
+        }
+        if (out.contours)
+            for (int k = lane; k < 2 * nv; k += 32) out.contours[(long long)i * 2 * nv + k] = dnan();
+        if (!finite) {
+            if (lane == 0) out.status[i] = st;
+            continue;
+        }
+        const double cx = p[1] + c.box.x, cy = p[2] + c.box.y;
+        // precision = L L^T.
+        const double pa = e1 * e1, pb = e1 * p[4], pc = p[4] * p[4] + e3 * e3;
+        const Eig2 e = eigh2(pa, pb, pc);
+        if (lane == 0) { out.centers[2LL * i] = cx; out.centers[2LL * i + 1] = cy; }
+        if (e.w0 <= 1e-10) {
+            if (lane == 0) out.status[i] = SPX_ST_NON_GAUSSIAN_FIT;
+            continue;
+        }
+        const double s0 = 1.0 / sqrt(e.w0), s1 = 1.0 / sqrt(e.w1);
+        const double step = 2.0 * kPi / n_angles;
+        auto vertex = [&](int k, double* x, double* y) {
+            ellipse_vertex(cx, cy, e, s0, s1, (double)(k % n_angles) * step, x, y);
+        };
+        if (out.contours)
+            for (int k = lane; k < nv; k += 32) {
+                double x, y;
+                vertex(k, &x, &y);
+                out.contours[(long long)i * 2 * nv + 2 * k] = x;
+                out.contours[(long long)i * 2 * nv + 2 * k + 1] = y;
+            }
+        double area = 0, perim = 0, px = 0, py = 0;
+        if (out.contours) polygon_geometry(nv, vertex, lane, &area, &perim, &px, &py);
+        if (lane == 0) {
+            if (out.eigenvalues) {
+                out.eigenvalues[2LL * i] = e.w0;
+                out.eigenvalues[2LL * i + 1] = e.w1;
+                out.axes[4LL * i + 0] = e.v00; out.axes[4LL * i + 1] = e.v01;
+                out.axes[4LL * i + 2] = e.v10; out.axes[4LL * i + 3] = e.v11;
+            }
+            m[M_SIG_MAJ] = s0;
+            m[M_SIG_MIN] = s1;
+            m[M_FWHM_MAJ] = 2.0 * kFwhmK * s0;
+            m[M_FWHM_MIN] = 2.0 * kFwhmK * s1;
+            double ang = atan2(e.v10, e.v00) * (180.0 / kPi);
+            ang = fmod(ang, 180.0);
+            if (ang < 0) ang += 180.0;
+            m[M_ANGLE] = ang;
+            if (st == SPX_ST_OK) {
+                const double ar = kPi * kFwhmK * kFwhmK * (s0 * s1);
+                m[M_AREA] = ar;
+                m[M_CD_EQ] = 2.0 * sqrt(ar / kPi);
+                // covariance = axes diag(sigma^2) axes^T
+                const double c00 = e.v00 * e.v00 * s0 * s0 + e.v01 * e.v01 * s1 * s1;
+                const double c11 = e.v10 * e.v10 * s0 * s0 + e.v11 * e.v11 * s1 * s1;
+                m[M_CD_X] = 2.0 * kFwhmK * sqrt(c00);
+                m[M_CD_Y] = 2.0 * kFwhmK * sqrt(c11);
+                m[M_PERIM] = out.contours ? perim : dnan();
+            }
+            out.status[i] = st;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ logquad CD
+
+__global__ void k_logquad_cd(const double* cleaned, const int* vor, const int4* boxes, const int* which,
+                             const double* seeds, int n, int hm, int wm, int W, int n_angles, double fit_fraction,
+                             MethodOut out) {
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    const double scale = 0.5 * (double)max(hm, wm), inv = 1.0 / scale;
+    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
+        const int j = which ? which[i] : i;
+        const CellView c{cleaned + (long long)i * hm * wm, vor, boxes[j], j, W, hm, wm};
+        const double sx = seeds[2LL * j] - c.box.x, sy = seeds[2LL * j + 1] - c.box.y;
+        const int nv = n_angles + 1;
+        double* m = out.metrics + (long long)i * out.n_metrics;
+        // Defaults: no_signal, seed centre, NaN geometry.
+        if (lane == 0) {
+            for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
+            out.status[i] = SPX_ST_NO_SIGNAL;
+            out.centers[2LL * i] = out.centers[2LL * i + 1] = dnan();
+            out.center_local[2LL * i] = out.center_local[2LL * i + 1] = dnan();
+            out.eigenvalues[2LL * i] = out.eigenvalues[2LL * i + 1] = dnan();
+            for (int q = 0; q < 4; ++q) out.axes[4LL * i + q] = dnan();
+        }
+        if (out.contours)
+            for (int k = lane; k < 2 * nv; k += 32) out.contours[(long long)i * 2 * nv + k] = dnan();
+        int cnt = 0;
+        double peak = -dinf();
+        for (int k = lane; k < hm * wm; k += 32) {
+            if (!c.mask(k / wm, k % wm)) continue;
+            ++cnt;
+            peak = fmax(peak, c.roi[k]);
+        }
+        cnt = warp_sum_i(cnt);
+        peak = warp_max(peak);
+        if (cnt < 6) {
+            if (lane == 0) out.status[i] = SPX_ST_INSUFFICIENT_CELL_PIXELS;
+            continue;
+        }
+        if (!(peak > 0.0)) continue;  // measure_cells skips cells with no signal above the background
+        if (lane == 0) {
+            m[M_BACKGROUND] = 0.0;
+            m[M_PEAK] = peak;
+            out.center_local[2LL * i] = sx;
+            out.center_local[2LL * i + 1] = sy;
+            out.centers[2LL * i] = sx + c.box.x;
+            out.centers[2LL * i + 1] = sy + c.box.y;
+        }
+        // Weighted sums of the log-quadratic least squares in seed-centred coordinates / scale.
+        double acc[28];
+#pragma unroll
+        for (int q = 0; q < 28; ++q) acc[q] = 0.0;
+        for (int k = lane; k < hm * wm; k += 32) {
+            const int yy = k / wm, xx = k % wm;
+            const double s = c.roi[k];
+            if (!c.mask(yy, xx) || !(s > fit_fraction * peak)) continue;
+            const double wt = s / peak, w2 = wt * wt, z = log(s);
+            const double u = ((double)xx - sx) * inv, v = ((double)yy - sy) * inv;
+            const double d[6] = {u * u, v * v, u * v, u, v, 1.0};
+            int q = 1;
+#pragma unroll
+            for (int a = 0; a < 6; ++a)
+#pragma unroll
+                for (int b = a; b < 6; ++b) acc[q++] += w2 * d[a] * d[b];
+#pragma unroll
+            for (int a = 0; a < 6; ++a) acc[22 + a] += w2 * d[a] * z;
+            acc[0] += 1.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 28; ++q) acc[q] = warp_sum(acc[q]);
+        if (acc[0] < 6.0) {
+            if (lane == 0) out.status[i] = SPX_ST_INSUFFICIENT_FIT_PIXELS;
+            continue;
+        }
+        // Cholesky of the normal matrix; a pivot below 1e-12 of the largest diagonal is rank
+        // deficiency (lstsq rank < 6).
+        double A[6][6], b[6];
+        {
+            int q = 1;
+            for (int a = 0; a < 6; ++a)
+                for (int bb = a; bb < 6; ++bb) { A[a][bb] = A[bb][a] = acc[q++]; }
+            for (int a = 0; a < 6; ++a) b[a] = acc[22 + a];
+        }
+        double dmax = 0.0;
+        for (int a = 0; a < 6; ++a) dmax = fmax(dmax, A[a][a]);
+        bool singular = false;
+        double L[6][6];
+        for (int r = 0; r < 6; ++r)
+            for (int col = 0; col <= r; ++col) {
+                double v = A[r][col];
+                for (int k = 0; k < col; ++k) v -= L[r][k] * L[col][k];
+                if (r == col) {
+                    if (!(v > 1e-12 * dmax)) singular = true;
+                    L[r][r] = sqrt(fmax(v, 1e-300));
+                } else {
+                    L[r][col] = v / L[col][col];
+                }
+            }
+        if (singular) {
+            if (lane == 0) out.status[i] = SPX_ST_SINGULAR_FIT;
+            continue;
+        }
+        double yv[6], cf[6];
+        for (int r = 0; r < 6; ++r) {
+            double v = b[r];
+            for (int k = 0; k < r; ++k) v -= L[r][k] * yv[k];
+            yv[r] = v / L[r][r];
+        }
+        for (int r = 5; r >= 0; --r) {
+            double v = yv[r];
+            for (int k = r + 1; k < 6; ++k) v -= L[k][r] * cf[k];
+            cf[r] = v / L[r][r];
+        }
+        // Back to pixel units.
+        const double ca = cf[0] / (scale * scale), cb = cf[1] / (scale * scale), cc = cf[2] / (scale * scale);
+        const double cd = cf[3] / scale, ce = cf[4] / scale;
+        const double pa = -2.0 * ca, pb = -cc, pc = -2.0 * cb;  // precision = -[[2a, c], [c, 2b]]
+        const Eig2 e = eigh2(pa, pb, pc);
+        if (e.w0 <= 1e-10 || e.w1 / e.w0 > 1e8) {
+            if (lane == 0) out.status[i] = SPX_ST_NON_GAUSSIAN_FIT;
+            continue;
+        }
+        // offset = solve(precision, [d, e]).
+        const double det = pa * pc - pb * pb;
+        const double ox = (cd * pc - pb * ce) / det, oy = (pa * ce - pb * cd) / det;
+        const double lx = sx + ox, ly = sy + oy;
+        const double gx = lx + c.box.x, gy = ly + c.box.y;
+        const double s0 = 1.0 / sqrt(e.w0), s1 = 1.0 / sqrt(e.w1);
+        const double step = 2.0 * kPi / n_angles;
+        auto lvertex = [&](int k, double* x, double* y) {
+            ellipse_vertex(lx, ly, e, s0, s1, (double)(k % n_angles) * step, x, y);
+        };
+        // log_fit_rmse (weights w^2) of the solved fit.
+        double rr = 0.0, ww = 0.0;
+        for (int k = lane; k < hm * wm; k += 32) {
+            const int yy = k / wm, xx = k % wm;
+            const double s = c.roi[k];
+            if (!c.mask(yy, xx) || !(s > fit_fraction * peak)) continue;
+            const double wt = s / peak, w2 = wt * wt;
+            const double u = ((double)xx - sx) * inv, v = ((double)yy - sy) * inv;
+            const double fit = cf[0] * u * u + cf[1] * v * v + cf[2] * u * v + cf[3] * u + cf[4] * v + cf[5];
+            const double d = fit - log(s);
+            rr += w2 * d * d;
+            ww += w2;
+        }
+        rr = warp_sum(rr);
+        ww = warp_sum(ww);
+        // Centre and contour inside the cell mask.
+        bool inside = true;
+        for (int k = lane; k < nv; k += 32) {
+            double x, y;
+            lvertex(k, &x, &y);
+            inside = inside && inside_bilinear(c, false, y, x);
+        }
+        inside = __all_sync(0xffffffffu, inside) && inside_bilinear(c, false, ly, lx);
+        if (out.contours)
+            for (int k = lane; k < nv; k += 32) {
+                double x, y;
+                lvertex(k, &x, &y);
+                out.contours[(long long)i * 2 * nv + 2 * k] = x + c.box.x;
+                out.contours[(long long)i * 2 * nv + 2 * k + 1] = y + c.box.y;
+            }
+        double area = 0, perim = 0, px = 0, py = 0;
+        polygon_geometry(nv, lvertex, lane, &area, &perim, &px, &py);
+        if (lane == 0) {
+            out.center_local[2LL * i] = lx;
+            out.center_local[2LL * i + 1] = ly;
+            out.centers[2LL * i] = gx;
+            out.centers[2LL * i + 1] = gy;
+            out.eigenvalues[2LL * i] = e.w0;
+            out.eigenvalues[2LL * i + 1] = e.w1;
+            out.axes[4LL * i + 0] = e.v00; out.axes[4LL * i + 1] = e.v01;
+            out.axes[4LL * i + 2] = e.v10; out.axes[4LL * i + 3] = e.v11;
+            m[M_SIG_MAJ] = s0;
+            m[M_SIG_MIN] = s1;
+            m[M_FWHM_MAJ] = 2.0 * kFwhmK * s0;
+            m[M_FWHM_MIN] = 2.0 * kFwhmK * s1;
+            double ang = atan2(e.v10, e.v00) * (180.0 / kPi);
+            ang = fmod(ang, 180.0);
+            if (ang < 0) ang += 180.0;
+            m[M_ANGLE] = ang;
+            m[M_RMSE] = sqrt(rr / ww);
+            if (!inside) {
+                out.status[i] = SPX_ST_CONTOUR_OUTSIDE_CELL;
+            } else {
+                const double ar = kPi * kFwhmK * kFwhmK * (s0 * s1);
+                m[M_AREA] = ar;
+                m[M_CD_EQ] = 2.0 * sqrt(ar / kPi);
+                const double c00 = e.v00 * e.v00 * s0 * s0 + e.v01 * e.v01 * s1 * s1;
+                const double c11 = e.v10 * e.v10 * s0 * s0 + e.v11 * e.v11 * s1 * s1;
+                m[M_CD_X] = 2.0 * kFwhmK * sqrt(c00);
+                m[M_CD_Y] = 2.0 * kFwhmK * sqrt(c11);
+                m[M_PERIM] = perim;
+                out.status[i] = SPX_ST_OK;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ radial CD
+
+// Unser's causal/anticausal recursion for the cubic B-spline (pole z = sqrt(3) - 2) over one line
+// of n values with stride, the gain applied first, half-sample-symmetric initial conditions.
+__device__ void spline_line(double* c, int n, int stride) {
+    const double z = -0.2679491924311228;  // sqrt(3) - 2
+    const double gain = (1.0 - z) * (1.0 - 1.0 / z);
+    for (int i = 0; i < n; ++i) c[i * stride] *= gain;
+    if (n == 1) return;
+    // causal init
+    {
+        double zi = z;
+        const double zn = pow(z, (double)n);
+        const double c0 = c[0];
+        double acc = c[0] + zn * c[(n - 1) * stride];
+        for (int i = 1; i < n; ++i) {
+            acc += zi * (c[i * stride] + zn * c[(n - 1 - i) * stride]);
+            zi *= z;
+        }
+        acc *= z / (1.0 - zn * zn);
+        c[0] = acc + c0;
+    }
+    for (int i = 1; i < n; ++i) c[i * stride] += z * c[(i - 1) * stride];
+    c[(n - 1) * stride] *= z / (z - 1.0);
+    for (int i = n - 2; i >= 0; --i) c[i * stride] = z * (c[(i + 1) * stride] - c[i * stride]);
+}
+
+// scipy's order-3 interpolation weights and clamped ("nearest") indices at coordinate v.
+__device__ __forceinline__ void cubic_weights(double v, int n, double* w, int* idx) {
+    const double f = floor(v), t = v - f, s = 1.0 - t;
+    w[1] = (t * t * (t - 2.0) * 3.0 + 4.0) / 6.0;
+    w[2] = (s * s * (s - 2.0) * 3.0 + 4.0) / 6.0;
+    w[0] = s * s * s / 6.0;
+    w[3] = 1.0 - w[0] - w[1] - w[2];
+    for (int k = 0; k < 4; ++k) idx[k] = min(max((int)f - 1 + k, 0), n - 1);
+}
+
+__device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, double y, double x) {
+    double wy[4], wx[4];
+    int iy[4], ix[4];
+    cubic_weights(y, hp, wy, iy);
+    cubic_weights(x, wp, wx, ix);
+    double out = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out += coef[iy[a] * wp + ix[b]] * wy[a] * wx[b];
+    return out;
+}
+
+// Radial profiles of each cell: weighted centroid of the pixels above 0.1 x max, cubic-spline
+// samples every radial_step along n_angles rays until the eroded cell ends, first half-height
+// crossing and the parabolic maximum of the outward decrease (halfmax / gradient methods).
+__global__ void k_radial_cd(const double* cleaned, const int* vor, const int4* boxes, const int* which, int n,
+                            int hm, int wm, int W, int n_angles, double radial_step, int n_radii,
+                            double* coef_scratch, MethodOut half_out, MethodOut grad_out) {
+    extern __shared__ double sm[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    const int hp = hm + 2 * kPad, wp = wm + 2 * kPad;
+    double* coef = coef_scratch ? coef_scratch + (long long)(blockIdx.x * warps + warp) * hp * wp
+                                : sm + (long long)warp * hp * wp;
+    const double thr = fmax(0.35, 2.0 * radial_step);
+    const int nv = n_angles + 1;
+    for (int i = blockIdx.x * warps + warp; i < n; i += gridDim.x * warps) {
+        const int j = which ? which[i] : i;
+        const CellView c{cleaned + (long long)i * hm * wm, vor, boxes[j], j, W, hm, wm};
+        MethodOut outs[2] = {half_out, grad_out};
+        for (int o = 0; o < 2; ++o) {
+            const MethodOut& out = outs[o];
+            if (!out.status) continue;
+            double* m = out.metrics + (long long)i * out.n_metrics;
+            if (lane == 0) {
+                for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
+                out.status[i] = SPX_ST_NO_SIGNAL;
+                out.centers[2LL * i] = out.centers[2LL * i + 1] = dnan();
+                out.center_local[2LL * i] = out.center_local[2LL * i + 1] = dnan();
+            }
+            for (int k = lane; k < n_angles; k += 32) out.edge_px[(long long)i * n_angles + k] = dnan();
+            if (out.contours)
+                for (int k = lane; k < 2 * nv; k += 32) out.contours[(long long)i * 2 * nv + k] = dnan();
+        }
+        int cnt = 0;
+        double top = 0.0;  // max of the signal array (zeros outside the mask)
+        for (int k = lane; k < hm * wm; k += 32) {
+            if (c.mask(k / wm, k % wm)) ++cnt;
+            top = fmax(top, c.roi[k]);
+        }
+        cnt = warp_sum_i(cnt);
+        top = warp_max(top);
+        if (cnt < 6) {
+            if (lane == 0)
+                for (int o = 0; o < 2; ++o)
+                    if (outs[o].status) outs[o].status[i] = SPX_ST_INSUFFICIENT_CELL_PIXELS;
+            continue;
+        }
+        if (!(top > 0.0)) continue;
+        // Weighted centroid of pixels above 0.1 x max.
+        double sw = 0.0, swx = 0.0, swy = 0.0;
+        for (int k = lane; k < hm * wm; k += 32) {
+            const int yy = k / wm, xx = k % wm;
+            const double s = c.mask(yy, xx) ? c.roi[k] : 0.0;
+            if (c.mask(yy, xx) && s > 0.1 * top) {
+                sw += s;
+                swx += s * xx;
+                swy += s * yy;
+            }
+        }
+        sw = warp_sum(sw);
+        const double cx = warp_sum(swx) / sw, cy = warp_sum(swy) / sw;
+        // Spline coefficients: the cell padded by 12 edge pixels, filtered along y then x.
+        for (int k = lane; k < hp * wp; k += 32) {
+            const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
+            coef[k] = c.mask(yy, xx) ? c.roi[yy * wm + xx] : 0.0;
+        }
+        __syncwarp();
+        for (int col = lane; col < wp; col += 32) spline_line(coef + col, hp, wp);
+        __syncwarp();
+        for (int row = lane; row < hp; row += 32) spline_line(coef + (long long)row * wp, wp, 1);
+        __syncwarp();
+        const double peak = cubic_at(coef, hp, wp, cy + kPad, cx + kPad);
+        const double half = peak / 2.0;
+        const double inv2s = 1.0 / (2.0 * radial_step);
+        int found_h = 0, found_g = 0;
+        for (int ray = lane; ray < ((n_angles + 31) / 32) * 32; ray += 32) {
+            double edge_h = dnan(), edge_g = dnan();
+            if (ray < n_angles && peak > 0.0) {
+                const double ang = (double)ray * (2.0 * kPi / n_angles);
+                const double ux = cos(ang), uy = sin(ang);
+                double h1 = 0, h2 = 0, h3 = 0, h4 = 0;  // p[k-1] .. p[k-4]
+                bool crossed = false;
+                double best = -dinf(), gl = 0, gm = 0, gr = 0;
+                int best_j = -1, first_invalid = n_radii;
+                for (int k = 0; k < n_radii; ++k) {
+                    const double r = (double)k * radial_step;
+                    const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
+                    if (!inside_bilinear(c, true, y, x)) { first_invalid = k; break; }
+                    const double p = k == 0 ? peak : cubic_at(coef, hp, wp, y + kPad, x + kPad);
+                    if (k >= 1 && !crossed && h1 >= half && p < half) {
+                        edge_h = (double)(k - 1) * radial_step + ((h1 - half) / (h1 - p)) * radial_step;
+                        crossed = true;
+                    }
+                    // Sample k valid makes j = k - 2 a candidate (valid[j - 2] and valid[j + 2]).
+                    const int jj = k - 2;
+                    if (jj >= 2 && jj <= n_radii - 3 && (double)jj * radial_step >= thr) {
+                        const double g = -((h1 - h3) * inv2s);  // -(p[j+1] - p[j-1]) / (2 step)
+                        if (g > best) {
+                            best = g;
+                            best_j = jj;
+                            gm = g;
+                            gl = -((h2 - h4) * inv2s);  // g[j-1]
+                            gr = -((p - h2) * inv2s);   // g[j+1]
+                        }
+                    }
+                    h4 = h3;
+                    h3 = h2;
+                    h2 = h1;
+                    h1 = p;
+                }
+                if (best_j >= 0) {
+                    const int jj = best_j;
+                    const bool left_ok = jj - 1 >= 2 && (double)(jj - 1) * radial_step >= thr;
+                    const bool right_ok = jj + 1 <= n_radii - 3 && jj + 3 < first_invalid &&
+                                          (double)(jj + 1) * radial_step >= thr;
+                    const double curv = gl - 2.0 * gm + gr;
+                    if (left_ok && right_ok && gm >= gl && gm >= gr && gm > 0.01 * peak && curv < -1e-12) {
+                        double delta = 0.5 * (gl - gr) / curv;
+                        delta = delta < -0.5 ? -0.5 : (delta > 0.5 ? 0.5 : delta);
+                        edge_g = (double)jj * radial_step + delta * radial_step;
+                    }
+                }
+            }
+            if (ray < n_angles) {
+                if (half_out.status) half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
+                if (grad_out.status) grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
+                found_h += isfinite(edge_h);
+                found_g += isfinite(edge_g);
+            }
+        }
+        found_h = warp_sum_i(found_h);
+        found_g = warp_sum_i(found_g);
+        __syncwarp();
+        for (int o = 0; o < 2; ++o) {
+            const MethodOut& out = outs[o];
+            if (!out.status) continue;
+            const int found = o == 0 ? found_h : found_g;
+            const double* edge = out.edge_px + (long long)i * n_angles;
+            const double step = 2.0 * kPi / n_angles;
+            auto vertex = [&](int k, double* x, double* y) {
+                const int a = k % n_angles;
+                const double ang = (double)a * step;
+                *x = cx + edge[a] * cos(ang);
+                *y = cy + edge[a] * sin(ang);
+            };
+            if (out.contours)
+                for (int k = lane; k < nv; k += 32) {
+                    double x, y;
+                    vertex(k, &x, &y);
+                    out.contours[(long long)i * 2 * nv + 2 * k] = x + c.box.x;
+                    out.contours[(long long)i * 2 * nv + 2 * k + 1] = y + c.box.y;
+                }
+            double area = 0, perim = 0, px = 0, py = 0;
+            if (found == n_angles) polygon_geometry(nv, vertex, lane, &area, &perim, &px, &py);
+            if (lane == 0) {
+                double* m = out.metrics + (long long)i * out.n_metrics;
+                out.center_local[2LL * i] = cx;
+                out.center_local[2LL * i + 1] = cy;
+                out.centers[2LL * i] = cx + c.box.x;
+                out.centers[2LL * i + 1] = cy + c.box.y;
+                m[M_BACKGROUND] = 0.0;
+                m[M_PEAK] = peak;
+                m[M_COVERAGE] = (double)found / n_angles;
+                if (found == n_angles) {
+                    m[M_AREA] = area;
+                    m[M_CD_EQ] = 2.0 * sqrt(area / kPi);
+                    m[M_CD_X] = px;
+                    m[M_CD_Y] = py;
+                    m[M_PERIM] = perim;
+                    out.status[i] = SPX_ST_OK;
+                } else {
+                    out.status[i] = SPX_ST_INCOMPLETE_RAYS;
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+MethodOut method_out(const spx_method_out* o) {
+    MethodOut m;
+    if (!o) {
+        m = MethodOut{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+        return m;
+    }
+    m.centers = o->centers;
+    m.contours = o->contours;
+    m.status = o->status;
+    m.metrics = o->metrics;
+    m.center_local = o->center_local;
+    m.edge_px = o->edge_px;
+    m.eigenvalues = o->eigenvalues;
+    m.axes = o->axes;
+    m.n_metrics = o->n_metrics;
+    return m;
+}
+
+}  // namespace
+}  // namespace spx
+
+using namespace spx;
+
+extern "C" {
+
+int spx_gaussian_method(const double* params, const uint8_t* status_in, const double* cleaned, const int* voronoi,
+                        const int* boxes, const int* which, int n, int hm, int wm, int width, int n_angles,
+                        const spx_method_out* out, void* stream) {
+    SPX_REQUIRE(n >= 0 && n_angles >= 1, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(params && status_in && cleaned && voronoi && boxes && out && out->centers && out->status &&
+                    out->metrics && out->n_metrics >= 13,
+                "null pointer or too few metric columns");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_gaussian_method<<<grid_for(n, 8, 148 * 32), 256, 0, s>>>(params, status_in, cleaned, voronoi,
+                                                              reinterpret_cast<const int4*>(boxes), which, n, hm,
+                                                              wm, width, n_angles, method_out(out));
+    return check_launch("k_gaussian_method");
+}
+
+int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, const double* seeds,
+                   int n, int hm, int wm, int width, int n_angles, double fit_fraction, const spx_method_out* out,
+                   void* stream) {
+    SPX_REQUIRE(n >= 0 && n_angles >= 1, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(cleaned && voronoi && boxes && seeds && out && out->centers && out->status && out->metrics &&
+                    out->center_local && out->eigenvalues && out->axes && out->n_metrics >= 13,
+                "null pointer or too few metric columns");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_logquad_cd<<<grid_for(n, 8, 148 * 32), 256, 0, s>>>(cleaned, voronoi, reinterpret_cast<const int4*>(boxes),
+                                                         which, seeds, n, hm, wm, width, n_angles, fit_fraction,
+                                                         method_out(out));
+    return check_launch("k_logquad_cd");
+}
+
+size_t spx_radial_workspace_bytes(int hm, int wm) {
+    const size_t per = (size_t)(hm + 2 * kPad) * (wm + 2 * kPad) * sizeof(double);
+    return 4 * per <= 200 * 1024 ? 256 : (size_t)148 * 8 * 4 * per + 256;
+}
+
+int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
+                  int wm, int width, int n_angles, double radial_step, const spx_method_out* halfmax,
+                  const spx_method_out* gradient, void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(n >= 0 && n_angles >= 1 && radial_step > 0, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(cleaned && voronoi && boxes && (halfmax || gradient), "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_radial_workspace_bytes(hm, wm), "workspace too small");
+    for (const spx_method_out* o : {halfmax, gradient})
+        if (o) SPX_REQUIRE(o->centers && o->status && o->metrics && o->center_local && o->edge_px && o->n_metrics >= 8,
+                           "null pointer or too few metric columns");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // radii = np.arange(0, hypot(hm, wm) + step, step)
+    const double stop = hypot((double)hm, (double)wm) + radial_step;
+    const int n_radii = (int)ceil(stop / radial_step);
+    const size_t per = (size_t)(hm + 2 * kPad) * (wm + 2 * kPad) * sizeof(double);
+    const int warps = 4;
+    size_t smem = warps * per;
+    double* scratch = nullptr;
+    int blocks = grid_for(n, warps, 148 * 8);
+    if (smem > 200 * 1024) {
+        smem = 0;
+        scratch = static_cast<double*>(workspace);
+        blocks = min(blocks, 148 * 8);
+    } else if (smem > 48 * 1024) {
+        SPX_CUDA(cudaFuncSetAttribute(k_radial_cd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    k_radial_cd<<<blocks, warps * 32, smem, s>>>(cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm,
+                                                  wm, width, n_angles, radial_step, n_radii, scratch,
+                                                  method_out(halfmax), method_out(gradient));
+    return check_launch("k_radial_cd");
+}
+
+}  // extern "C"

@@ -1,0 +1,838 @@
+// Joint deblending on the device: background map + one 2-D Gaussian per hole.
+//
+// Reference: subpx/_cpu/deblend.py (deblend 421-522, fit_gaussians_batch 174-254, initial_params
+// 152-171, fit_status 262-277, clean_cells 136-149, render_models 87-107, _tile_medians 280-291,
+// _upsample_rows / _upsample_tiles / _tile_centers 294-320) and subpx/_gpu/cells.py:11-38 (cell
+// boxes and masks). Host code (Python) drives the outer iteration and the tile interpolation; every
+// per-pixel and per-cell step is a kernel here.
+//
+// Cells are implicit: cell j is box j (origin, size) intersected with Voronoi label j, so no mask
+// stack is stored. A fit kernel stages each cell's cleaned pixels (image - background - (model -
+// own model)) once into the warp's shared-memory slice and runs the whole LM loop there; a work
+// queue hands cells to persistent warps. The model image is gathered, not scattered: each 16x16
+// tile sums the truncated Gaussians that reach it in increasing cell order (NumPy's bincount order),
+// so it is deterministic without atomics.
+
+#include "bins.cuh"
+#include "lm.cuh"
+
+namespace spx {
+namespace {
+
+constexpr int kFitWarps = 4;  // warps (cells in flight) per block of the fit kernels
+
+// Background map: bg(y, x) = (1 - t[y]) rows[j1[y]-1][x] + t[y] rows[j1[y]][x] (ny > 1),
+// rows[0][x] (ny == 1), or a constant.
+__device__ __forceinline__ double bg_at(const spx_bgmap& m, int y, int x) {
+    if (m.mode == SPX_BG_FIXED) return m.fixed;
+    if (m.ny == 1) return m.rows[x];
+    const int j = m.j1[y];
+    const double t = m.t[y];
+    return __dadd_rn(__dmul_rn(__dsub_rn(1.0, t), m.rows[(long long)(j - 1) * m.width + x]),
+                     __dmul_rn(t, m.rows[(long long)j * m.width + x]));
+}
+
+struct Image {
+    const void* data;
+    int dtype;
+    double sign;
+    int H, W;
+    __device__ __forceinline__ double at(int y, int x) const {
+        const double v = load_px(data, dtype, (long long)y * W + x);
+        return sign < 0 ? -v : v;
+    }
+};
+
+__device__ __forceinline__ int render_radius(const double* p, int cap) {
+    double r = ceil(4.0 * sigma_major(p));
+    if (!(r >= 2.0)) r = 2.0;  // NaN -> 2, as np.clip(nan) would not, but NaN params are never rendered
+    if (r > (double)cap) r = (double)cap;
+    return (int)r;
+}
+
+// ------------------------------------------------------------------------------- cell geometry
+
+__global__ void k_cells_setup(const double* rows, int n, int pad, int H, int W, const int* vor,
+                              int4* boxes, int* counts, double* caps) {
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int j = blockIdx.x * warps + (threadIdx.x >> 5); j < n; j += gridDim.x * warps) {
+        const double* r = rows + 6LL * j;
+        // int() truncates toward zero, as astype(np.int32).
+        const int x0 = max(0, (int)r[0] - pad), y0 = max(0, (int)r[1] - pad);
+        const int x1 = min(W, (int)(r[0] + r[2]) + pad), y1 = min(H, (int)(r[1] + r[3]) + pad);
+        const int bw = max(0, x1 - x0), bh = max(0, y1 - y0);
+        int c = 0;
+        for (int k = lane; k < bw * bh; k += 32) {
+            const int yy = y0 + k / bw, xx = x0 + k % bw;
+            c += vor[(long long)yy * W + xx] == j;
+        }
+        c = warp_sum_i(c);
+        if (lane == 0) {
+            boxes[j] = make_int4(x0, y0, bw, bh);
+            counts[j] = c;
+            caps[j] = fmax(1.0, sqrt((double)c / 3.141592653589793));
+        }
+    }
+}
+
+// --------------------------------------------------------------------------------- fit status
+
+// fit_status (subpx/_cpu/deblend.py:262-277) of ROI-local params p of cell j.
+__device__ int fit_status_of(const double* p, double cap, int j, int4 box, int hm, int wm, const int* vor, int W) {
+    for (int i = 0; i < 6; ++i)
+        if (!isfinite(p[i])) return SPX_ST_FIT_DIVERGED;
+    int st = SPX_ST_OK;
+    const double sig = sigma_major(p);
+    if (p[0] <= 0.0 || sig >= 0.999 * cap) st = SPX_ST_NON_GAUSSIAN_FIT;
+    // np.round (half to even) of the centre, clipped to the stack.
+    int cy = (int)rint(p[2]), cx = (int)rint(p[1]);
+    cy = min(max(cy, 0), hm - 1);
+    cx = min(max(cx, 0), wm - 1);
+    bool inside = p[1] >= -0.5 && p[1] <= wm - 0.5 && p[2] >= -0.5 && p[2] <= hm - 0.5;
+    inside = inside && cx < box.z && cy < box.w && vor[(long long)(box.y + cy) * W + (box.x + cx)] == j;
+    if (st == SPX_ST_OK && !inside) st = SPX_ST_CENTER_OUTSIDE_CELL;
+    return st;
+}
+
+// ---------------------------------------------------------------------------------- staging
+
+// Compacts cell j's mask pixels: v[slot] = value(yy, xx) (box-local coords), xy[slot] packed.
+// Returns the pixel count (same on all lanes).
+template <typename F>
+__device__ int stage_cell(int4 box, int j, const int* vor, int W, double* v, int* xy, int lane, F value) {
+    int base = 0;
+    const int P = box.z * box.w;
+    for (int k0 = 0; k0 < P; k0 += 32) {
+        const int k = k0 + lane;
+        bool in = false;
+        int yy = 0, xx = 0;
+        if (k < P) {
+            yy = k / box.z;
+            xx = k - yy * box.z;
+            in = vor[(long long)(box.y + yy) * W + (box.x + xx)] == j;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const int slot = base + __popc(m & ((1u << lane) - 1u));
+            v[slot] = value(yy, xx);
+            xy[slot] = xx | (yy << 16);
+        }
+        base += __popc(m);
+    }
+    __syncwarp();
+    return base;
+}
+
+// --------------------------------------------------------------------------------- kernels
+
+struct FitArgs {
+    Image img;
+    const int* vor;
+    const int4* boxes;
+    const double* caps;
+    int n, hm, wm;
+    int cap_px;       // per-warp pixel capacity of the staging buffers
+    int max_iter;
+    int* queue;       // work counter (reset by the host before the launch)
+    double* gbuf_v;   // global staging when shared memory is too small (else null)
+    int* gbuf_xy;
+};
+
+// Initial fit: 10th-percentile cell-border background, initial_params, LM, status.
+__global__ void k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
+                              double* params, uint8_t* status, int* iters) {
+    extern __shared__ unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* v;
+    int* xy;
+    if (a.gbuf_v) {
+        const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+        v = a.gbuf_v + w * a.cap_px;
+        xy = a.gbuf_xy + w * a.cap_px;
+    } else {
+        v = reinterpret_cast<double*>(smem) + (long long)warp * a.cap_px;
+        xy = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + (long long)(blockDim.x >> 5) * a.cap_px) +
+             (long long)warp * a.cap_px;
+    }
+    while (true) {
+        int j = 0;
+        if (lane == 0) j = atomicAdd(a.queue, 1);
+        j = __shfl_sync(0xffffffffu, j, 0);
+        if (j >= a.n) break;
+        const int4 box = a.boxes[j];
+        // Border pixels: mask pixels with an 8-neighbour outside the mask or the box.
+        auto in_cell = [&](int yy, int xx) {
+            return yy >= 0 && xx >= 0 && yy < box.w && xx < box.z &&
+                   a.vor[(long long)(box.y + yy) * a.img.W + (box.x + xx)] == j;
+        };
+        double bg0;
+        if (has_level) {
+            bg0 = background_level;
+        } else {
+            // Stage border values into v (sorted below), then take the 10th percentile.
+            int base = 0;
+            const int P = box.z * box.w;
+            for (int k0 = 0; k0 < P; k0 += 32) {
+                const int k = k0 + lane;
+                bool border = false;
+                int yy = 0, xx = 0;
+                if (k < P) {
+                    yy = k / box.z;
+                    xx = k - yy * box.z;
+                    if (in_cell(yy, xx)) {
+                        for (int dy = -1; dy <= 1 && !border; ++dy)
+                            for (int dx = -1; dx <= 1; ++dx)
+                                if (!in_cell(yy + dy, xx + dx)) { border = true; break; }
+                    }
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, border);
+                if (border) v[base + __popc(m & ((1u << lane) - 1u))] = a.img.at(box.y + yy, box.x + xx);
+                base += __popc(m);
+            }
+            __syncwarp();
+            int m2 = 1;
+            while (m2 < base) m2 <<= 1;
+            for (int i = base + lane; i < m2; i += 32) v[i] = dinf();
+            __syncwarp();
+            warp_bitonic_sort(v, m2, lane);
+            bg0 = base > 0 ? sorted_percentile(v, base, 0.1) : 0.0;
+            __syncwarp();
+        }
+        const int n = stage_cell(box, j, a.vor, a.img.W, v, xy, lane, [&](int yy, int xx) {
+            return a.img.at(box.y + yy, box.x + xx) - bg0;
+        });
+        // initial_params: amplitude = peak, centre = seed, sigma from the core's second moment.
+        double peak = -dinf();
+        for (int k = lane; k < n; k += 32) peak = fmax(peak, v[k]);
+        peak = warp_max(peak);
+        const double sx = seeds[2LL * j] - box.x, sy = seeds[2LL * j + 1] - box.y;
+        double tot = 0.0, mom = 0.0, amax = 0.0;
+        for (int k = lane; k < n; k += 32) {
+            const double d = v[k];
+            amax = fmax(amax, fabs(d));
+            if (d > 0.2 * peak) {
+                const double dx = (double)(xy[k] & 0xffff) - sx, dy = (double)(xy[k] >> 16) - sy;
+                tot += d;
+                mom += d * (dx * dx + dy * dy);
+            }
+        }
+        tot = warp_sum(tot);
+        mom = warp_sum(mom);
+        amax = warp_max(amax);
+        const double var = (mom / fmax(tot, 1e-300)) / 2.0;
+        const double sigma = sqrt(fmax(var, 0.25));
+        double p[6] = {fmax(peak, 1e-12), sx, sy, -log(sigma), 0.0, -log(sigma)};
+        const double cap = a.caps[j];
+        const int it = warp_lm_fit(p, v, xy, n, cap, 3.0 * fmax(amax, 1e-12), a.max_iter, lane);
+        if (lane == 0) {
+            for (int i = 0; i < 6; ++i) params[6LL * j + i] = p[i];
+            status[j] = (uint8_t)fit_status_of(p, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
+            if (iters) iters[j] = it;
+        }
+        __syncwarp();
+    }
+}
+
+// One deblending iteration for every cell: clean (image - background - (model - own)), LM from the
+// current params, relaxation p + relax * (fitted - p) (non-finite components step 0), status of
+// the relaxed params, and max |step[1:]| (NaN unless the cell is "ok" with a finite fit).
+__global__ void k_fit_iteration(FitArgs a, spx_bgmap bg, const double* model, int radius_cap,
+                                const double* params, double relaxation, double* params_out,
+                                uint8_t* status_out, double* maxstep, int* iters) {
+    extern __shared__ unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* v;
+    int* xy;
+    if (a.gbuf_v) {
+        const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+        v = a.gbuf_v + w * a.cap_px;
+        xy = a.gbuf_xy + w * a.cap_px;
+    } else {
+        v = reinterpret_cast<double*>(smem) + (long long)warp * a.cap_px;
+        xy = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + (long long)(blockDim.x >> 5) * a.cap_px) +
+             (long long)warp * a.cap_px;
+    }
+    while (true) {
+        int j = 0;
+        if (lane == 0) j = atomicAdd(a.queue, 1);
+        j = __shfl_sync(0xffffffffu, j, 0);
+        if (j >= a.n) break;
+        const int4 box = a.boxes[j];
+        double p0[6];
+        for (int i = 0; i < 6; ++i) p0[i] = params[6LL * j + i];
+        const double gx0 = p0[1] + box.x, gy0 = p0[2] + box.y;
+        const int r = render_radius(p0, radius_cap);
+        const double e1 = exp(p0[3]), e3 = exp(p0[5]);
+        const int n = stage_cell(box, j, a.vor, a.img.W, v, xy, lane, [&](int yy, int xx) {
+            const int y = box.y + yy, x = box.x + xx;
+            const double dx = (double)x - gx0, dy = (double)y - gy0;
+            double own = 0.0;
+            if (fabs(dx) <= r && fabs(dy) <= r) {
+                const double aa = e1 * dx + p0[4] * dy, bb = e3 * dy;
+                own = p0[0] * exp(-0.5 * (aa * aa + bb * bb));
+            }
+            const double raw = a.img.at(y, x);
+            return (raw - bg_at(bg, y, x)) - (model[(long long)y * a.img.W + x] - own);
+        });
+        double amax = 0.0;
+        for (int k = lane; k < n; k += 32) amax = fmax(amax, fabs(v[k]));
+        amax = warp_max(amax);
+        double p[6];
+        for (int i = 0; i < 6; ++i) p[i] = p0[i];
+        const double cap = a.caps[j];
+        const int it = warp_lm_fit(p, v, xy, n, cap, 3.0 * fmax(amax, 1e-12), a.max_iter, lane);
+        if (lane == 0) {
+            double q[6];
+            bool finite = true;
+            double ms = 0.0;
+            for (int i = 0; i < 6; ++i) {
+                finite = finite && isfinite(p[i]);
+                const double step = isfinite(p[i]) ? p[i] - p0[i] : 0.0;
+                q[i] = p0[i] + relaxation * step;
+                if (i >= 1) ms = fmax(ms, fabs(step));
+            }
+            const int st = fit_status_of(q, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
+            for (int i = 0; i < 6; ++i) params_out[6LL * j + i] = q[i];
+            status_out[j] = (uint8_t)st;
+            maxstep[j] = (st == SPX_ST_OK && finite) ? ms : dnan();
+            if (iters) iters[j] = it;
+        }
+        __syncwarp();
+    }
+}
+
+// Global centres and render radii of all cells (for the render's bin grid).
+__global__ void k_render_prep(const double* params, const int4* boxes, int n, int radius_cap,
+                              double* centres, int* radius, uint8_t* valid, int* rmax) {
+    int local = 0;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const double* p = params + 6LL * j;
+        bool ok = true;
+        for (int i = 0; i < 6; ++i) ok = ok && isfinite(p[i]);
+        const int4 b = boxes[j];
+        centres[2LL * j] = p[1] + b.x;
+        centres[2LL * j + 1] = p[2] + b.y;
+        const int r = ok ? render_radius(p, radius_cap) : 0;
+        radius[j] = r;
+        valid[j] = ok;
+        local = max(local, r);
+    }
+    for (int o = 16; o > 0; o >>= 1) local = max(local, __shfl_xor_sync(0xffffffffu, local, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(rmax, local);
+}
+
+constexpr int kRenderTile = 16;
+constexpr int kRenderCap = 2048;
+
+// model(y, x) = sum over cells (increasing index) whose truncated square covers the pixel, each
+// term A exp(-(a^2 + b^2) / 2) for |x - X0| <= r and |y - Y0| <= r (render_models).
+__global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const double* params,
+                                               const double* centres, const int* radius,
+                                               const int* rmax_dev, double* model, int* overflow) {
+    __shared__ int cand[kRenderCap];
+    __shared__ int s_n;
+    const int tx0 = blockIdx.x * kRenderTile, ty0 = blockIdx.y * kRenderTile;
+    const int tx1 = min(tx0 + kRenderTile, W) - 1, ty1 = min(ty0 + kRenderTile, H) - 1;
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    const int rmax = *rmax_dev;
+    const int gx0 = bin_index((double)(tx0 - rmax - 1), g.cell, g.gw);
+    const int gx1 = bin_index((double)(tx1 + rmax + 1), g.cell, g.gw);
+    const int gy0 = bin_index((double)(ty0 - rmax - 1), g.cell, g.gh);
+    const int gy1 = bin_index((double)(ty1 + rmax + 1), g.cell, g.gh);
+    for (int gy = gy0; gy <= gy1; ++gy) {
+        const int j0 = g.start[gy * g.gw + gx0], j1 = g.start[gy * g.gw + gx1 + 1];
+        for (int k = j0 + threadIdx.x; k < j1; k += blockDim.x) {
+            const int id = g.id[k];
+            const double2 c = g.xy[k];
+            const double r = (double)radius[id];
+            if (c.x + r >= tx0 && c.x - r <= tx1 && c.y + r >= ty0 && c.y - r <= ty1) {
+                const int slot = atomicAdd(&s_n, 1);
+                if (slot < kRenderCap) cand[slot] = id;
+            }
+        }
+    }
+    __syncthreads();
+    const int m = s_n;
+    if (m > kRenderCap) {
+        if (threadIdx.x == 0) atomicExch(overflow, 1);
+        return;
+    }
+    int m2 = 1;
+    while (m2 < m) m2 <<= 1;
+    for (int i = m + threadIdx.x; i < m2; i += blockDim.x) cand[i] = 0x7fffffff;
+    __syncthreads();
+    for (int len = 2; len <= m2; len <<= 1)
+        for (int stride = len >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < m2; i += blockDim.x) {
+                const int jx = i ^ stride;
+                if (jx > i) {
+                    const bool up = (i & len) == 0;
+                    const int u = cand[i], w = cand[jx];
+                    if (up ? u > w : u < w) { cand[i] = w; cand[jx] = u; }
+                }
+            }
+            __syncthreads();
+        }
+    const int x = tx0 + (threadIdx.x % kRenderTile), y = ty0 + (threadIdx.x / kRenderTile);
+    if (x >= W || y >= H) return;
+    double acc = 0.0;
+    for (int k = 0; k < m; ++k) {
+        const int id = cand[k];
+        const double r = (double)radius[id];
+        const double dx = (double)x - centres[2LL * id], dy = (double)y - centres[2LL * id + 1];
+        if (fabs(dx) > r || fabs(dy) > r) continue;
+        const double* p = params + 6LL * id;
+        const double aa = exp(p[3]) * dx + p[4] * dy, bb = exp(p[5]) * dy;
+        const double val = p[0] * exp(-0.5 * (aa * aa + bb * bb));
+        if (val != 0.0) acc += val;
+    }
+    model[(long long)y * W + x] = acc;
+}
+
+// Cleaned cells (image - background - (model - own)) of the cells in `which` (all when null) as
+// an (n_out, hm, wm) stack, zero outside each cell (DeblendState.cleaned).
+__global__ void k_clean_stack(Image img, const int* vor, const int4* boxes, const double* params,
+                              int radius_cap, spx_bgmap bg, const double* model, const int* which,
+                              int n_out, int hm, int wm, double* out) {
+    const long long total = (long long)n_out * hm * wm;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(t / ((long long)hm * wm));
+        const int k = (int)(t % ((long long)hm * wm));
+        const int yy = k / wm, xx = k % wm;
+        const int j = which ? which[c] : c;
+        const int4 b = boxes[j];
+        double v = 0.0;
+        if (yy < b.w && xx < b.z) {
+            const int y = b.y + yy, x = b.x + xx;
+            if (vor[(long long)y * img.W + x] == j) {
+                const double* p = params + 6LL * j;
+                const double dx = (double)x - (p[1] + b.x), dy = (double)y - (p[2] + b.y);
+                const int r = render_radius(p, radius_cap);
+                double own = 0.0;
+                if (fabs(dx) <= r && fabs(dy) <= r) {
+                    const double aa = exp(p[3]) * dx + p[4] * dy, bb = exp(p[5]) * dy;
+                    own = p[0] * exp(-0.5 * (aa * aa + bb * bb));
+                }
+                v = (img.at(y, x) - bg_at(bg, y, x)) - (model[(long long)y * img.W + x] - own);
+            }
+        }
+        out[t] = v;
+    }
+}
+
+// ------------------------------------------------------------------------------ tile medians
+
+constexpr int kTileThreads = 512;
+constexpr int kTileSmemKeys = 24576;  // keys held in shared memory (192 KiB)
+
+__device__ __forceinline__ unsigned long long order_key(double v) {
+    const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double key_value(unsigned long long k) {
+    const unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)u);
+}
+
+struct TileSel {
+    Image img;
+    const double* model;      // null: residual = image
+    const unsigned int* d2;   // distance map (free mode)
+    const uint8_t* usable;    // null: all usable
+    int mode;                 // SPX_TILE_FREE: model < thr_model & dist >= thr_dist; SPX_TILE_USABLE; SPX_TILE_ALL
+    double thr_model, thr_dist;
+    __device__ __forceinline__ bool select(long long i, double* value) const {
+        const double m = model ? model[i] : 0.0;
+        if (mode != SPX_TILE_ALL) {
+            if (usable && !usable[i]) return false;
+            if (mode == SPX_TILE_FREE) {
+                if (!(m < thr_model)) return false;
+                if (!(sqrt((double)d2[i]) >= thr_dist)) return false;
+            }
+        }
+        const int y = (int)(i / img.W), x = (int)(i % img.W);
+        *value = img.at(y, x) - m;
+        return true;
+    }
+};
+
+// Median (mean of the two middle values, NaN when empty) and count of the selected residuals of
+// each tile, by an 8-pass radix select on order-preserving 64-bit keys.
+__global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int tile, int nx, int smem_keys,
+                                                              double* medians, long long* counts) {
+    extern __shared__ unsigned long long keys[];
+    __shared__ int hist[256];
+    __shared__ int s_count, s_digit, s_k;
+    __shared__ unsigned long long s_min;
+    __shared__ int s_le;
+    const int ty = blockIdx.x / nx, tx = blockIdx.x % nx;
+    const int y0 = ty * tile, x0 = tx * tile;
+    const int th = min(tile, sel.img.H - y0), tw = min(tile, sel.img.W - x0);
+    const long long P = (long long)th * tw;
+    if (threadIdx.x == 0) s_count = 0;
+    __syncthreads();
+    // Pass 0: count and (when they fit) stage the keys.
+    for (long long k = threadIdx.x; k < P; k += blockDim.x) {
+        const long long i = (long long)(y0 + k / tw) * sel.img.W + (x0 + k % tw);
+        double v;
+        if (sel.select(i, &v)) {
+            const int slot = atomicAdd(&s_count, 1);
+            if (slot < smem_keys) keys[slot] = order_key(v);
+        }
+    }
+    __syncthreads();
+    const int c = s_count;
+    const bool in_smem = c <= smem_keys;
+    auto for_keys = [&](auto&& fn) {
+        if (in_smem) {
+            for (int i = threadIdx.x; i < c; i += blockDim.x) fn(keys[i]);
+        } else {
+            for (long long k = threadIdx.x; k < P; k += blockDim.x) {
+                const long long i = (long long)(y0 + k / tw) * sel.img.W + (x0 + k % tw);
+                double v;
+                if (sel.select(i, &v)) fn(order_key(v));
+            }
+        }
+    };
+    if (c == 0) {
+        if (threadIdx.x == 0) {
+            medians[blockIdx.x] = dnan();
+            counts[blockIdx.x] = 0;
+        }
+        return;
+    }
+    // k-th smallest key (k = (c - 1) / 2).
+    unsigned long long prefix = 0, mask = 0;
+    if (threadIdx.x == 0) s_k = (c - 1) / 2;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        for_keys([&](unsigned long long key) {
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1);
+        });
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int k = s_k, d = 0;
+            for (; d < 255; ++d) {
+                if (k < hist[d]) break;
+                k -= hist[d];
+            }
+            s_digit = d;
+            s_k = k;
+        }
+        __syncthreads();
+        prefix |= (unsigned long long)s_digit << shift;
+        mask |= 0xffull << shift;
+        __syncthreads();
+    }
+    const unsigned long long k1 = prefix;
+    double v2;
+    if ((c & 1) == 0) {
+        // The next order statistic: k1 again when it repeats, else the smallest key above it.
+        if (threadIdx.x == 0) { s_le = 0; s_min = ~0ull; }
+        __syncthreads();
+        int le = 0;
+        unsigned long long mn = ~0ull;
+        for_keys([&](unsigned long long key) {
+            if (key <= k1) ++le;
+            else if (key < mn) mn = key;
+        });
+        atomicAdd(&s_le, le);
+        atomicMin(&s_min, mn);
+        __syncthreads();
+        v2 = s_le > c / 2 ? key_value(k1) : key_value(s_min);
+    } else {
+        v2 = key_value(k1);
+    }
+    if (threadIdx.x == 0) {
+        const double v1 = key_value(k1);
+        medians[blockIdx.x] = __ddiv_rn(__dadd_rn(v1, v2), 2.0);
+        counts[blockIdx.x] = c;
+    }
+}
+
+// rows[j][x] = np.interp(x, xc, medians[j]) with xc the tile-centre columns.
+__global__ void k_bg_rows(const double* medians, int ny, int nx, int tile, int W, double* rows) {
+    const long long total = (long long)ny * W;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(t / W), x = (int)(t % W);
+        const double* fp = medians + (long long)j * nx;
+        auto xc = [&](int i) { return (double)(i * tile + min((i + 1) * tile, W) - 1) / 2.0; };
+        const double xv = (double)x;
+        double res;
+        if (nx == 1) {
+            res = fp[0];
+        } else if (xv < xc(0)) {
+            res = fp[0];
+        } else if (xv > xc(nx - 1)) {
+            res = fp[nx - 1];
+        } else {
+            // xc(i) <= x < xc(i+1); tiles are `tile` wide so the interval is x / tile or one below.
+            int i = min(max(x / tile, 0), nx - 1);
+            while (i > 0 && xc(i) > xv) --i;
+            while (i < nx - 1 && xc(i + 1) <= xv) ++i;
+            if (i == nx - 1 || xc(i) == xv) {
+                res = fp[i];
+            } else {
+                const double slope = __ddiv_rn(__dsub_rn(fp[i + 1], fp[i]), __dsub_rn(xc(i + 1), xc(i)));
+                res = __dadd_rn(__dmul_rn(slope, __dsub_rn(xv, xc(i))), fp[i]);
+                if (isnan(res)) {
+                    res = __dadd_rn(__dmul_rn(slope, __dsub_rn(xv, xc(i + 1))), fp[i + 1]);
+                    if (isnan(res) && fp[i] == fp[i + 1]) res = fp[i];
+                }
+            }
+        }
+        rows[t] = res;
+    }
+}
+
+// residual = image - background - model at every pixel (revise_seeds' input).
+__global__ void k_residual(Image img, spx_bgmap bg, const double* model, double* out) {
+    const long long total = (long long)img.H * img.W;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / img.W), x = (int)(i % img.W);
+        out[i] = (img.at(y, x) - bg_at(bg, y, x)) - model[i];
+    }
+}
+
+struct FitLayout {
+    int* queue;
+    double* gbuf_v;
+    int* gbuf_xy;
+};
+
+int fit_blocks() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * 8;
+}
+
+// Shared memory per block for cap_px pixels per warp; 0 when it does not fit (global staging).
+size_t fit_smem(int cap_px) {
+    const size_t bytes = (size_t)kFitWarps * cap_px * (sizeof(double) + sizeof(int));
+    return bytes <= 200 * 1024 ? bytes : 0;
+}
+
+FitLayout fit_layout(void* ws, int cap_px, size_t* bytes) {
+    Arena a(ws);
+    FitLayout L;
+    L.queue = a.take<int>(4);
+    const bool global = fit_smem(cap_px) == 0;
+    const long long warps = global ? (long long)fit_blocks() * kFitWarps : 0;
+    L.gbuf_v = global ? a.take<double>(warps * cap_px) : nullptr;
+    L.gbuf_xy = global ? a.take<int>(warps * cap_px) : nullptr;
+    if (!global) { a.take<double>(1); a.take<int>(1); }
+    if (bytes) *bytes = a.used;
+    return L;
+}
+
+}  // namespace
+}  // namespace spx
+
+using namespace spx;
+
+namespace {
+
+int pow2_at_least(int n) {
+    int m = 1;
+    while (m < n) m <<= 1;
+    return m;
+}
+
+template <typename Launch>
+int launch_fit(const FitArgs& a0, FitLayout L, cudaStream_t s, Launch&& launch) {
+    FitArgs a = a0;
+    a.queue = L.queue;
+    a.gbuf_v = L.gbuf_v;
+    a.gbuf_xy = L.gbuf_xy;
+    SPX_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(int), s));
+    const size_t smem = a.gbuf_v ? 0 : fit_smem(a.cap_px);
+    return launch(a, smem);
+}
+
+struct RenderLayout {
+    BinStorage bins;
+    double* centres;
+    int* radius;
+    uint8_t* valid;
+    int* rmax;
+    int* overflow;
+};
+
+RenderLayout render_layout(void* ws, int n, int H, int W, size_t* bytes) {
+    Arena a(ws);
+    RenderLayout L;
+    L.bins = bin_layout(a, n, H, W, bin_cell_size(n, H, W, 1.0, 8.0));
+    L.centres = a.take<double>(2 * (size_t)(n > 0 ? n : 1));
+    L.radius = a.take<int>(n > 0 ? n : 1);
+    L.valid = a.take<uint8_t>(n > 0 ? n : 1);
+    L.rmax = a.take<int>(1);
+    L.overflow = a.take<int>(1);
+    if (bytes) *bytes = a.used;
+    return L;
+}
+
+}  // namespace
+
+extern "C" {
+
+int spx_cells_setup(const double* rows, int n, int pad, int height, int width, const int* voronoi,
+                    int* boxes, int* counts, double* caps, void* stream) {
+    SPX_REQUIRE(n >= 0 && pad >= 0 && height > 0 && width > 0, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(rows && voronoi && boxes && counts && caps, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_cells_setup<<<grid_for(n, 8, 148 * 16), 256, 0, s>>>(rows, n, pad, height, width, voronoi,
+                                                           reinterpret_cast<int4*>(boxes), counts, caps);
+    return check_launch("k_cells_setup");
+}
+
+size_t spx_fit_workspace_bytes(int max_cell_pixels) {
+    size_t b = 0;
+    fit_layout(nullptr, pow2_at_least(max_cell_pixels > 0 ? max_cell_pixels : 1), &b);
+    return b;
+}
+
+int spx_deblend_initial(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                        const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
+                        int max_cell_pixels, double background_level, int has_level, int max_iter,
+                        double* params, uint8_t* status, int* iterations, void* workspace,
+                        size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(img && voronoi && boxes && caps && seeds && params && status && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_fit_workspace_bytes(max_cell_pixels), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int cap_px = pow2_at_least(max_cell_pixels > 0 ? max_cell_pixels : 1);
+    FitLayout L = fit_layout(workspace, cap_px, nullptr);
+    FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
+              hm, wm, cap_px, max_iter, nullptr, nullptr, nullptr};
+    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem) -> int {
+        if (smem > 48 * 1024)
+            SPX_CUDA(cudaFuncSetAttribute(k_fit_initial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_fit_initial<<<fit_blocks(), kFitWarps * 32, smem, s>>>(fa, seeds, background_level, has_level, params,
+                                                                  status, iterations);
+        return check_launch("k_fit_initial");
+    });
+}
+
+int spx_deblend_iteration(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                          const int* boxes, const double* caps, int n, int hm, int wm, int max_cell_pixels,
+                          const spx_bgmap* background, const double* model, int radius_cap,
+                          const double* params, double relaxation, int max_iter, double* params_out,
+                          uint8_t* status_out, double* maxstep, int* iterations, void* workspace,
+                          size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(img && voronoi && boxes && caps && background && model && params && params_out && status_out &&
+                    maxstep && workspace,
+                "null pointer");
+    SPX_REQUIRE(params != params_out, "params_out must not alias params");
+    SPX_REQUIRE(workspace_bytes >= spx_fit_workspace_bytes(max_cell_pixels), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int cap_px = pow2_at_least(max_cell_pixels > 0 ? max_cell_pixels : 1);
+    FitLayout L = fit_layout(workspace, cap_px, nullptr);
+    FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
+              hm, wm, cap_px, max_iter, nullptr, nullptr, nullptr};
+    const spx_bgmap bg = *background;
+    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem) -> int {
+        if (smem > 48 * 1024)
+            SPX_CUDA(cudaFuncSetAttribute(k_fit_iteration, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_fit_iteration<<<fit_blocks(), kFitWarps * 32, smem, s>>>(fa, bg, model, radius_cap, params, relaxation,
+                                                                    params_out, status_out, maxstep, iterations);
+        return check_launch("k_fit_iteration");
+    });
+}
+
+size_t spx_render_workspace_bytes(int n, int height, int width) {
+    size_t b = 0;
+    render_layout(nullptr, n, height, width, &b);
+    return b;
+}
+
+int spx_render_model(const double* params, const int* boxes, int n, int height, int width, int radius_cap,
+                     double* model, void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && radius_cap >= 2, "bad arguments");
+    SPX_REQUIRE(model && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_render_workspace_bytes(n, height, width), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    RenderLayout L = render_layout(workspace, n, height, width, nullptr);
+    SPX_CUDA(cudaMemsetAsync(L.rmax, 0, sizeof(int), s));
+    SPX_CUDA(cudaMemsetAsync(L.overflow, 0, sizeof(int), s));
+    if (n > 0) {
+        SPX_REQUIRE(params && boxes, "null pointer");
+        k_render_prep<<<grid_for(n, 256), 256, 0, s>>>(params, reinterpret_cast<const int4*>(boxes), n, radius_cap,
+                                                       L.centres, L.radius, L.valid, L.rmax);
+        if (int e = check_launch("k_render_prep")) return e;
+    }
+    if (int e = bin_build(L.bins, L.centres, 2, nullptr, L.valid, n, s)) return e;
+    const dim3 grid((width + kRenderTile - 1) / kRenderTile, (height + kRenderTile - 1) / kRenderTile);
+    k_render<<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
+                                  L.overflow);
+    if (int e = check_launch("k_render")) return e;
+    int overflow = 0;
+    SPX_CUDA(cudaMemcpyAsync(&overflow, L.overflow, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPX_CUDA(cudaStreamSynchronize(s));
+    if (overflow) {
+        set_error("render: more than %d truncated Gaussians reach one 16x16 tile", kRenderCap);
+        return SPX_ERR_CAPACITY;
+    }
+    return SPX_OK;
+}
+
+int spx_clean_cells(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                    const int* boxes, const double* params, int radius_cap, const spx_bgmap* background,
+                    const double* model, const int* which, int n_out, int hm, int wm, double* out, void* stream) {
+    SPX_REQUIRE(n_out >= 0 && hm >= 0 && wm >= 0, "bad arguments");
+    if (n_out == 0 || hm == 0 || wm == 0) return SPX_OK;
+    SPX_REQUIRE(img && voronoi && boxes && params && background && model && out, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long total = (long long)n_out * hm * wm;
+    k_clean_stack<<<grid_for(total, 256), 256, 0, s>>>(Image{img, dtype, sign, height, width}, voronoi,
+                                                       reinterpret_cast<const int4*>(boxes), params, radius_cap,
+                                                       *background, model, which, n_out, hm, wm, out);
+    return check_launch("k_clean_stack");
+}
+
+int spx_tile_medians(const void* img, int dtype, double sign, int height, int width, const double* model,
+                     const unsigned int* dist2, const uint8_t* usable, int mode, double thr_model, double thr_dist,
+                     int tile, double* medians, long long* counts, void* stream) {
+    SPX_REQUIRE(height > 0 && width > 0 && tile >= 1, "bad arguments");
+    SPX_REQUIRE(mode == SPX_TILE_FREE || mode == SPX_TILE_USABLE || mode == SPX_TILE_ALL, "bad mode");
+    SPX_REQUIRE(img && medians && counts && (mode != SPX_TILE_FREE || dist2), "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int ny = (height + tile - 1) / tile, nx = (width + tile - 1) / tile;
+    const long long t2 = (long long)tile * tile;
+    const int smem_keys = (int)(t2 < kTileSmemKeys ? t2 : kTileSmemKeys);
+    const size_t smem = (size_t)smem_keys * sizeof(unsigned long long);
+    SPX_CUDA(cudaFuncSetAttribute(k_tile_median, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TileSel sel{Image{img, dtype, sign, height, width}, model, dist2, usable, mode, thr_model, thr_dist};
+    k_tile_median<<<ny * nx, kTileThreads, smem, s>>>(sel, tile, nx, smem_keys, medians, counts);
+    return check_launch("k_tile_median");
+}
+
+int spx_background_rows(const double* medians, int ny, int nx, int tile, int width, double* rows, void* stream) {
+    SPX_REQUIRE(ny >= 1 && nx >= 1 && tile >= 1 && width > 0, "bad arguments");
+    SPX_REQUIRE(medians && rows, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long total = (long long)ny * width;
+    k_bg_rows<<<grid_for(total, 256), 256, 0, s>>>(medians, ny, nx, tile, width, rows);
+    return check_launch("k_bg_rows");
+}
+
+int spx_residual(const void* img, int dtype, double sign, int height, int width, const spx_bgmap* background,
+                 const double* model, double* out, void* stream) {
+    SPX_REQUIRE(height > 0 && width > 0, "bad arguments");
+    SPX_REQUIRE(img && background && model && out, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_residual<<<grid_for((long long)height * width, 256), 256, 0, s>>>(Image{img, dtype, sign, height, width},
+                                                                        *background, model, out);
+    return check_launch("k_residual");
+}
+
+}  // extern "C"

@@ -1,0 +1,177 @@
+// One warp fits one 2-D Gaussian to one cell by Levenberg-Marquardt.
+//
+// Model (subpx/_cpu/deblend.py:9-12, 48-71): params [A, x0, y0, u1, u2, u3], precision L L^T with
+// L = [[e^u1, 0], [u2, e^u3]]; value A exp(-(a^2 + b^2) / 2), a = e^u1 dx + u2 dy, b = e^u3 dy.
+// Iteration (fit_gaussians_batch, subpx/_cpu/deblend.py:174-254): normal equations J^T J and J^T r
+// over the cell's mask pixels, damping lam * diag + 1e-12, trial clipped to A in [0, 3 max|d|] and
+// u1, u3 in [-log(cap), -log(0.5)], accepted when the cost does not rise (lam / 3, else lam * 4);
+// stop when the relative cost drop is <= 1e-12, max |step| < 1e-7, lam > 1e12 or after max_iter.
+//
+// Layout: the cell's mask pixels are compacted into (value, packed local x | y << 16) arrays; lanes
+// stride over them, the 27 sums are butterfly-reduced so every lane holds identical totals, and
+// every lane solves the damped 6x6 system (Cholesky, fully unrolled in registers) and takes the
+// same decisions, so the warp never diverges on control flow. Arithmetic is FP64.
+#pragma once
+
+#include "common.cuh"
+
+namespace spx {
+
+constexpr double kSigmaMin = 0.5;  // _SIGMA_MIN
+
+struct GaussEval {
+    double shape, a, b;
+};
+
+__device__ __forceinline__ GaussEval gauss_eval(const double* p, double e1, double e3, double dx, double dy) {
+    GaussEval g;
+    g.a = e1 * dx + p[4] * dy;
+    g.b = e3 * dy;
+    g.shape = exp(-0.5 * (g.a * g.a + g.b * g.b));
+    return g;
+}
+
+__device__ __forceinline__ double warp_cost(const double* p, const double* v, const int* xy, int n, int lane) {
+    const double e1 = exp(p[3]), e3 = exp(p[5]);
+    double acc = 0.0;
+    for (int k = lane; k < n; k += 32) {
+        const int c = xy[k];
+        const double dx = (double)(c & 0xffff) - p[1], dy = (double)(c >> 16) - p[2];
+        const GaussEval g = gauss_eval(p, e1, e3, dx, dy);
+        const double r = v[k] - p[0] * g.shape;
+        acc += r * r;
+    }
+    return warp_sum(acc);
+}
+
+// Solves (N + diag(lam * N_ii + 1e-12)) s = g for the symmetric 6x6 N given by its upper triangle
+// (21 values, row-major) by Cholesky; NaN propagates into s when the matrix is not positive.
+__device__ __forceinline__ void damped_solve(const double* nu, const double* g, double lam, double* s) {
+    double L[21];
+    double y[6];
+    int q = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i)
+#pragma unroll
+        for (int j = i; j < 6; ++j) {
+            double v = nu[q];
+            if (i == j) v = v + (lam * v + 1e-12);
+            L[q] = v;
+            ++q;
+        }
+    // In-place Cholesky of the upper triangle: U^T U = M (row-major upper storage).
+    auto at = [](int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); };
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double d = L[at(i, i)];
+#pragma unroll
+        for (int k = 0; k < i; ++k) d -= L[at(k, i)] * L[at(k, i)];
+        d = sqrt(d);  // NaN when not positive definite
+        L[at(i, i)] = d;
+        const double inv = 1.0 / d;
+#pragma unroll
+        for (int j = i + 1; j < 6; ++j) {
+            double v = L[at(i, j)];
+#pragma unroll
+            for (int k = 0; k < i; ++k) v -= L[at(k, i)] * L[at(k, j)];
+            L[at(i, j)] = v * inv;
+        }
+    }
+    // U^T y = g, then U s = y.
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double v = g[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) v -= L[at(k, i)] * y[k];
+        y[i] = v / L[at(i, i)];
+    }
+#pragma unroll
+    for (int i = 5; i >= 0; --i) {
+        double v = y[i];
+#pragma unroll
+        for (int k = i + 1; k < 6; ++k) v -= L[at(i, k)] * s[k];
+        s[i] = v / L[at(i, i)];
+    }
+}
+
+// Fits p (ROI-local, identical on all lanes) to the n compacted pixels. Returns the number of
+// iterations run. `cap` is the cell's sigma cap, `amp_cap` 3 * max(max|v|, 1e-12).
+__device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int n, double cap, double amp_cap,
+                           int max_iter, int lane) {
+    double cost = warp_cost(p, v, xy, n, lane);
+    if (!isfinite(cost)) return 0;
+    double lam = 1e-3;
+    const double lo = -log(cap), hi = -log(kSigmaMin);
+    int it = 0;
+    for (; it < max_iter; ++it) {
+        double s[27];
+#pragma unroll
+        for (int i = 0; i < 27; ++i) s[i] = 0.0;
+        const double e1 = exp(p[3]), e3 = exp(p[5]);
+        for (int k = lane; k < n; k += 32) {
+            const int c = xy[k];
+            const double dx = (double)(c & 0xffff) - p[1], dy = (double)(c >> 16) - p[2];
+            const GaussEval g = gauss_eval(p, e1, e3, dx, dy);
+            const double model = p[0] * g.shape;
+            const double r = v[k] - model;
+            double J[6];
+            J[0] = g.shape;
+            J[1] = model * (g.a * e1);
+            J[2] = model * (g.a * p[4] + g.b * e3);
+            J[3] = -model * (g.a * e1 * dx);
+            J[4] = -model * (g.a * dy);
+            J[5] = -model * (g.b * e3 * dy);
+            int q = 0;
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+#pragma unroll
+                for (int j = i; j < 6; ++j) s[q++] += J[i] * J[j];
+#pragma unroll
+            for (int i = 0; i < 6; ++i) s[21 + i] += J[i] * r;
+        }
+#pragma unroll
+        for (int i = 0; i < 27; ++i) s[i] = warp_sum(s[i]);
+        double step[6];
+        damped_solve(s, s + 21, lam, step);
+        double trial[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) trial[i] = p[i] + step[i];
+        // np.clip semantics: NaN passes through.
+        trial[0] = trial[0] < 0.0 ? 0.0 : (trial[0] > amp_cap ? amp_cap : trial[0]);
+        trial[3] = trial[3] < lo ? lo : (trial[3] > hi ? hi : trial[3]);
+        trial[5] = trial[5] < lo ? lo : (trial[5] > hi ? hi : trial[5]);
+        const double new_cost = warp_cost(trial, v, xy, n, lane);
+        const bool better = isfinite(new_cost) && new_cost <= cost;
+        double smax = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) smax = fmax(smax, fabs(step[i]));
+        // fmax ignores NaN; a NaN step is not "small" (np.abs(nan) < 1e-7 is False).
+        bool small = smax < 1e-7;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) small = small && !isnan(step[i]);
+        const bool done = (better && (cost - new_cost <= 1e-12 * fmax(cost, 1e-300))) || small;
+        if (better) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) p[i] = trial[i];
+            lam /= 3.0;
+            cost = new_cost;
+        } else {
+            lam *= 4.0;
+        }
+        if (done || lam > 1e12) { ++it; break; }
+    }
+    return it;
+}
+
+// sigma_major of the Cholesky parameters in closed form: the precision L L^T has determinant
+// (e1 e3)^2, so its smaller eigenvalue is that over the larger one.
+__device__ __forceinline__ double sigma_major(const double* p) {
+    const double e1 = exp(p[3]), u2 = p[4], e3 = exp(p[5]);
+    const double a = e1 * e1, b = e1 * u2, c = u2 * u2 + e3 * e3;
+    const double half = (a - c) / 2;
+    const double larger = (a + c) / 2 + sqrt(half * half + b * b);
+    const double smaller = larger > 0 ? (e1 * e3) * (e1 * e3) / larger : 0.0;
+    return 1.0 / sqrt(fmax(smaller, 1e-300));
+}
+
+}  // namespace spx

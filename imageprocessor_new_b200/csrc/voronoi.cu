@@ -1,8 +1,10 @@
-// Voronoi partition: label of the nearest seed for every pixel.
+// Voronoi partition, distance-to-nearest-seed-pixel map and nearest-point queries.
 //
 // Reference: subpx/_cpu/cells.py:8-33 (cKDTree k=2 query, exact ties resolved by the lowest seed
 // index on recomputed squared distances) and subpx/_gpu/voronoi.py (same rule). The rule is
 // argmin over seeds of (d2, index) with d2 = (px-sx)*(px-sx) + (py-sy)*(py-sy) rounded without FMA.
+// The distance map replaces scipy.ndimage.distance_transform_edt of the seed-pixel mask
+// (subpx/_cpu/deblend.py:452-457): squared distance to the nearest rint()-ed seed pixel.
 //
 // B200 layout: seeds are counting-sorted into a grid of square bins (about one seed per bin). One
 // CTA labels a 16x16 pixel tile: warp 0 bounds the distance from the tile centre to its nearest
@@ -10,69 +12,160 @@
 // (contiguous runs of the bin-sorted array, one run per bin row) are staged through shared memory
 // in chunks and each thread keeps its own (d2, index) minimum. Writes are 4 B/px, coalesced.
 
-#include "common.cuh"
-#include "scan.cuh"
+#include "bins.cuh"
 
 namespace spx {
+
+__global__ void k_bin_count(const double* pts, int stride, const int* origin, const uint8_t* valid,
+                            long long n, int gw, int gh, double cell, int* counts) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (valid && !valid[i]) continue;
+        double x = pts[i * stride], y = pts[i * stride + 1];
+        if (origin) { x += origin[2 * i]; y += origin[2 * i + 1]; }
+        atomicAdd(&counts[bin_index(y, cell, gh) * gw + bin_index(x, cell, gw)], 1);
+    }
+}
+
+__global__ void k_bin_fill(const double* pts, int stride, const int* origin, const uint8_t* valid,
+                           long long n, int gw, int gh, double cell, const int* start, int* fill,
+                           double2* xy, int* id) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (valid && !valid[i]) continue;
+        double x = pts[i * stride], y = pts[i * stride + 1];
+        if (origin) { x += origin[2 * i]; y += origin[2 * i + 1]; }
+        const int b = bin_index(y, cell, gh) * gw + bin_index(x, cell, gw);
+        const int slot = start[b] + atomicAdd(&fill[b], 1);
+        xy[slot] = make_double2(x, y);
+        id[slot] = (int)i;
+    }
+}
+
+int bin_build(BinStorage& b, const double* pts, int stride, const int* origin, const uint8_t* valid,
+              long long n, cudaStream_t s) {
+    const long long bins = (long long)b.gw * b.gh;
+    SPX_CUDA(cudaMemsetAsync(b.counts, 0, (bins + 1) * sizeof(int), s));
+    SPX_CUDA(cudaMemsetAsync(b.fill, 0, (bins + 1) * sizeof(int), s));
+    if (n > 0) {
+        k_bin_count<<<grid_for(n, 256), 256, 0, s>>>(pts, stride, origin, valid, n, b.gw, b.gh, b.cell, b.counts);
+        if (int e = check_launch("k_bin_count")) return e;
+    }
+    if (int e = exclusive_scan(b.counts, bins + 1, b.start, nullptr, b.scratch, s)) return e;
+    if (n > 0) {
+        k_bin_fill<<<grid_for(n, 256), 256, 0, s>>>(pts, stride, origin, valid, n, b.gw, b.gh, b.cell, b.start,
+                                                    b.fill, b.xy, b.id);
+        if (int e = check_launch("k_bin_fill")) return e;
+    }
+    return SPX_OK;
+}
+
 namespace {
 
 constexpr int kTile = 16;
 constexpr int kThreads = kTile * kTile;
-
-struct Grid {
-    int gw, gh;
-    double cell;
-};
-
-__device__ __forceinline__ int bin_of(double v, double cell, int n) {
-    long long b = (long long)floor(v / cell);
-    if (b < 0) b = 0;
-    if (b > n - 1) b = n - 1;
-    return (int)b;
-}
-
-__global__ void k_bin_count(const double* seeds, int n, Grid g, int* counts) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int bx = bin_of(seeds[2 * i], g.cell, g.gw), by = bin_of(seeds[2 * i + 1], g.cell, g.gh);
-        atomicAdd(&counts[by * g.gw + bx], 1);
-    }
-}
-
-// Scatter seeds into bin order; within a bin the order is arbitrary (ties compare indices).
-__global__ void k_bin_fill(const double* seeds, int n, Grid g, const int* start, int* fill,
-                           double2* sorted_xy, int* sorted_id) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int bx = bin_of(seeds[2 * i], g.cell, g.gw), by = bin_of(seeds[2 * i + 1], g.cell, g.gh);
-        const int b = by * g.gw + bx;
-        const int slot = start[b] + atomicAdd(&fill[b], 1);
-        sorted_xy[slot] = make_double2(seeds[2 * i], seeds[2 * i + 1]);
-        sorted_id[slot] = i;
-    }
-}
 
 __device__ __forceinline__ double dist2(double px, double py, double sx, double sy) {
     const double dx = __dsub_rn(px, sx), dy = __dsub_rn(py, sy);
     return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
 }
 
-__global__ void __launch_bounds__(kThreads) k_voronoi(int H, int W, Grid g, const int* start,
-                                                       const double2* sxy, const int* sid, int n,
-                                                       int* labels) {
+// Smallest squared distance from (cx, cy) to any point, by rings of bins until one holds a point,
+// plus one more ring (called by one full warp; the result is the same on every lane).
+__device__ double warp_nearest_bound(const BinGrid& g, double cx, double cy, int lane) {
+    const int bx = bin_index(cx, g.cell, g.gw), by = bin_index(cy, g.cell, g.gh);
+    double best = dinf();
+    int found_ring = -1;
+    const int max_ring = max(g.gw, g.gh);
+    for (int R = 0; R <= max_ring; ++R) {
+        const int side = 2 * R + 1;
+        const int count = R == 0 ? 1 : 4 * (side - 1);
+        for (int k = lane; k < count; k += 32) {
+            int gx, gy;
+            if (R == 0) { gx = bx; gy = by; }
+            else if (k < side) { gx = bx - R + k; gy = by - R; }
+            else if (k < 2 * side) { gx = bx - R + (k - side); gy = by + R; }
+            else if (k < 2 * side + (side - 2)) { gx = bx - R; gy = by - R + 1 + (k - 2 * side); }
+            else { gx = bx + R; gy = by - R + 1 + (k - 2 * side - (side - 2)); }
+            if (gx < 0 || gy < 0 || gx >= g.gw || gy >= g.gh) continue;
+            const int b = gy * g.gw + gx;
+            for (int j = g.start[b]; j < g.start[b + 1]; ++j) {
+                const double2 s = g.xy[j];
+                best = fmin(best, dist2(cx, cy, s.x, s.y));
+            }
+        }
+        best = warp_min(best);
+        if (best < dinf() && found_ring < 0) found_ring = R;
+        if (found_ring >= 0 && R >= found_ring + 1) break;
+    }
+    return best;
+}
+
+// labels != null: nearest-seed index; d2 != null: squared distance to the nearest seed.
+__global__ void __launch_bounds__(kThreads) k_voronoi(int H, int W, BinGrid g, int* labels,
+                                                       unsigned int* d2out) {
     __shared__ double2 c_xy[kThreads];
     __shared__ int c_id[kThreads];
     __shared__ double s_bound;
     const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
     const int lane = threadIdx.x & 31;
-    // Tile centre, clipped to the image part of the tile.
-    const double cx = 0.5 * (tx0 + min(tx0 + kTile, W) - 1), cy = 0.5 * (ty0 + min(ty0 + kTile, H) - 1);
-    const double half_diag = 0.5 * sqrt((double)(min(kTile, W - tx0) - 1) * (min(kTile, W - tx0) - 1) +
-                                        (double)(min(kTile, H - ty0) - 1) * (min(kTile, H - ty0) - 1));
+    const int ex = min(kTile, W - tx0), ey = min(kTile, H - ty0);
+    const double cx = 0.5 * (tx0 + tx0 + ex - 1), cy = 0.5 * (ty0 + ty0 + ey - 1);
+    const double half_diag = 0.5 * sqrt((double)(ex - 1) * (ex - 1) + (double)(ey - 1) * (ey - 1));
     if (threadIdx.x < 32) {
-        // Nearest-seed distance bound of the centre: rings of bins until one holds a seed, plus
-        // one more ring.
-        const int bx = bin_of(cx, g.cell, g.gw), by = bin_of(cy, g.cell, g.gh);
+        const double best = warp_nearest_bound(g, cx, cy, lane);
+        if (lane == 0) s_bound = sqrt(best) + 2.0 * half_diag + 1.0;
+    }
+    __syncthreads();
+    const double R = s_bound;
+    int gx0, gx1, gy0, gy1;
+    if (isfinite(R)) {
+        gx0 = bin_index(cx - R, g.cell, g.gw);
+        gx1 = bin_index(cx + R, g.cell, g.gw);
+        gy0 = bin_index(cy - R, g.cell, g.gh);
+        gy1 = bin_index(cy + R, g.cell, g.gh);
+    } else {
+        gx0 = gy0 = 0;
+        gx1 = g.gw - 1;
+        gy1 = g.gh - 1;
+    }
+    const int x = tx0 + (threadIdx.x % kTile), y = ty0 + (threadIdx.x / kTile);
+    const double px = (double)x, py = (double)y;
+    double best = dinf();
+    int label = 0x7fffffff;
+    for (int gy = gy0; gy <= gy1; ++gy) {
+        const int j0 = g.start[gy * g.gw + gx0], j1 = g.start[gy * g.gw + gx1 + 1];
+        for (int base = j0; base < j1; base += kThreads) {
+            const int m = min(kThreads, j1 - base);
+            __syncthreads();
+            if ((int)threadIdx.x < m) {
+                c_xy[threadIdx.x] = g.xy[base + threadIdx.x];
+                c_id[threadIdx.x] = g.id[base + threadIdx.x];
+            }
+            __syncthreads();
+            for (int k = 0; k < m; ++k) {
+                const double2 s = c_xy[k];
+                const double d2 = dist2(px, py, s.x, s.y);
+                const int id = c_id[k];
+                if (d2 < best || (d2 == best && id < label)) { best = d2; label = id; }
+            }
+        }
+    }
+    if (x < W && y < H) {
+        if (labels) labels[(long long)y * W + x] = label;
+        if (d2out) d2out[(long long)y * W + x] = best < 4294967295.0 ? (unsigned int)best : 0xffffffffu;
+    }
+}
+
+// Nearest point of the grid to each query point (excluding the point with the same index when
+// exclude_self): distance (not squared) to out_dist.
+__global__ void k_nearest_query(BinGrid g, const double* q, int nq, int exclude_self, double* out_dist) {
+    const int lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5;
+    for (int i = blockIdx.x * warps + (threadIdx.x >> 5); i < nq; i += gridDim.x * warps) {
+        const double qx = q[2 * i], qy = q[2 * i + 1];
+        const int bx = bin_index(qx, g.cell, g.gw), by = bin_index(qy, g.cell, g.gh);
         double best = dinf();
-        int found_ring = -1;
         const int max_ring = max(g.gw, g.gh);
         for (int R = 0; R <= max_ring; ++R) {
             const int side = 2 * R + 1;
@@ -86,44 +179,20 @@ __global__ void __launch_bounds__(kThreads) k_voronoi(int H, int W, Grid g, cons
                 else { gx = bx + R; gy = by - R + 1 + (k - 2 * side - (side - 2)); }
                 if (gx < 0 || gy < 0 || gx >= g.gw || gy >= g.gh) continue;
                 const int b = gy * g.gw + gx;
-                for (int j = start[b]; j < start[b + 1]; ++j) {
-                    const double2 s = sxy[j];
-                    best = fmin(best, dist2(cx, cy, s.x, s.y));
+                for (int j = g.start[b]; j < g.start[b + 1]; ++j) {
+                    if (exclude_self && g.id[j] == i) continue;
+                    const double2 s = g.xy[j];
+                    best = fmin(best, dist2(qx, qy, s.x, s.y));
                 }
             }
             best = warp_min(best);
-            if (best < dinf() && found_ring < 0) found_ring = R;
-            if (found_ring >= 0 && R >= found_ring + 1) break;
+            // Points beyond ring R are at least R * cell away (from inside the query's bin); stop
+            // once that exceeds the best distance found.
+            const double reach = (double)R * g.cell;
+            if (best < dinf() && reach * reach > best) break;
         }
-        if (lane == 0) s_bound = sqrt(best) + 2.0 * half_diag + 1.0;
+        if (lane == 0) out_dist[i] = sqrt(best);
     }
-    __syncthreads();
-    const double R = s_bound;
-    const int gx0 = bin_of(cx - R, g.cell, g.gw), gx1 = bin_of(cx + R, g.cell, g.gw);
-    const int gy0 = bin_of(cy - R, g.cell, g.gh), gy1 = bin_of(cy + R, g.cell, g.gh);
-    const int x = tx0 + (threadIdx.x % kTile), y = ty0 + (threadIdx.x / kTile);
-    const double px = (double)x, py = (double)y;
-    double best = dinf();
-    int label = 0x7fffffff;
-    for (int gy = gy0; gy <= gy1; ++gy) {
-        const int j0 = start[gy * g.gw + gx0], j1 = start[gy * g.gw + gx1 + 1];
-        for (int base = j0; base < j1; base += kThreads) {
-            const int m = min(kThreads, j1 - base);
-            __syncthreads();
-            if ((int)threadIdx.x < m) {
-                c_xy[threadIdx.x] = sxy[base + threadIdx.x];
-                c_id[threadIdx.x] = sid[base + threadIdx.x];
-            }
-            __syncthreads();
-            for (int k = 0; k < m; ++k) {
-                const double2 s = c_xy[k];
-                const double d2 = dist2(px, py, s.x, s.y);
-                const int id = c_id[k];
-                if (d2 < best || (d2 == best && id < label)) { best = d2; label = id; }
-            }
-        }
-    }
-    if (x < W && y < H) labels[(long long)y * W + x] = label;
 }
 
 __global__ void k_fill(int* labels, long long n, int v) {
@@ -132,46 +201,37 @@ __global__ void k_fill(int* labels, long long n, int v) {
         labels[i] = v;
 }
 
-Grid make_grid(int n, int H, int W) {
-    Grid g;
-    double cell = floor(sqrt((double)H * (double)W / (double)(n > 0 ? n : 1)));
-    if (cell < 1.0) cell = 1.0;
-    g.cell = cell;
-    g.gw = (int)ceil(W / cell);
-    g.gh = (int)ceil(H / cell);
-    if (g.gw < 1) g.gw = 1;
-    if (g.gh < 1) g.gh = 1;
-    return g;
-}
-
-struct VorLayout {
-    int* counts;
-    int* start;
-    int* fill;
-    double2* sorted_xy;
-    int* sorted_id;
-    int* scratch;
-};
-
-VorLayout vor_layout(void* ws, int n, int H, int W, size_t* bytes) {
-    const Grid g = make_grid(n, H, W);
-    const long long bins = (long long)g.gw * g.gh;
-    Arena a(ws);
-    VorLayout L;
-    L.counts = a.take<int>(bins + 1);
-    L.start = a.take<int>(bins + 1);
-    L.fill = a.take<int>(bins + 1);
-    L.sorted_xy = a.take<double2>(n > 0 ? n : 1);
-    L.sorted_id = a.take<int>(n > 0 ? n : 1);
-    L.scratch = a.take<int>(scan_scratch_ints(bins + 1));
-    if (bytes) *bytes = a.used;
-    return L;
+__global__ void k_seed_pixels(const double* seeds, int n, int H, int W, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double x = fmin(fmax(rint(seeds[2 * i]), 0.0), (double)(W - 1));
+        const double y = fmin(fmax(rint(seeds[2 * i + 1]), 0.0), (double)(H - 1));
+        out[2 * i] = x;
+        out[2 * i + 1] = y;
+    }
 }
 
 }  // namespace
 }  // namespace spx
 
 using namespace spx;
+
+namespace {
+
+struct VorWs {
+    BinStorage bins;
+    double* seed_px;
+};
+
+VorWs vor_layout(void* ws, int n, int H, int W, size_t* bytes) {
+    Arena a(ws);
+    VorWs v;
+    v.bins = bin_layout(a, n, H, W, bin_cell_size(n, H, W));
+    v.seed_px = a.take<double>(2 * (size_t)(n > 0 ? n : 1));
+    if (bytes) *bytes = a.used;
+    return v;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -193,20 +253,40 @@ int spx_voronoi_labels(const double* seeds, int n, int height, int width, int* l
     }
     SPX_REQUIRE(seeds && workspace, "null pointer");
     SPX_REQUIRE(workspace_bytes >= spx_voronoi_workspace_bytes(n, height, width), "workspace too small");
-    const Grid g = make_grid(n, height, width);
-    const long long bins = (long long)g.gw * g.gh;
-    VorLayout L = vor_layout(workspace, n, height, width, nullptr);
-    SPX_CUDA(cudaMemsetAsync(L.counts, 0, (bins + 1) * sizeof(int), s));
-    SPX_CUDA(cudaMemsetAsync(L.fill, 0, (bins + 1) * sizeof(int), s));
-    k_bin_count<<<grid_for(n, 256), 256, 0, s>>>(seeds, n, g, L.counts);
-    if (int e = check_launch("k_bin_count")) return e;
-    // start[b] = seeds in bins before b; start[bins] = n (the extra zero count).
-    if (int e = exclusive_scan(L.counts, bins + 1, L.start, nullptr, L.scratch, s)) return e;
-    k_bin_fill<<<grid_for(n, 256), 256, 0, s>>>(seeds, n, g, L.start, L.fill, L.sorted_xy, L.sorted_id);
-    if (int e = check_launch("k_bin_fill")) return e;
+    VorWs L = vor_layout(workspace, n, height, width, nullptr);
+    if (int e = bin_build(L.bins, seeds, 2, nullptr, nullptr, n, s)) return e;
     const dim3 grid((width + kTile - 1) / kTile, (height + kTile - 1) / kTile);
-    k_voronoi<<<grid, kThreads, 0, s>>>(height, width, g, L.start, L.sorted_xy, L.sorted_id, n, labels);
+    k_voronoi<<<grid, kThreads, 0, s>>>(height, width, bin_view(L.bins), labels, nullptr);
     return check_launch("k_voronoi");
+}
+
+int spx_seed_distance_map(const double* seeds, int n, int height, int width, unsigned int* d2,
+                          void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(height > 0 && width > 0 && n >= 1, "bad arguments");
+    SPX_REQUIRE(seeds && d2 && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_voronoi_workspace_bytes(n, height, width), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    VorWs L = vor_layout(workspace, n, height, width, nullptr);
+    k_seed_pixels<<<grid_for(n, 256), 256, 0, s>>>(seeds, n, height, width, L.seed_px);
+    if (int e = check_launch("k_seed_pixels")) return e;
+    if (int e = bin_build(L.bins, L.seed_px, 2, nullptr, nullptr, n, s)) return e;
+    const dim3 grid((width + kTile - 1) / kTile, (height + kTile - 1) / kTile);
+    k_voronoi<<<grid, kThreads, 0, s>>>(height, width, bin_view(L.bins), nullptr, d2);
+    return check_launch("k_voronoi");
+}
+
+int spx_nearest_distances(const double* points, int n, const double* queries, int nq, int exclude_self,
+                          int height, int width, double* out, void* workspace, size_t workspace_bytes,
+                          void* stream) {
+    SPX_REQUIRE(n >= 1 && nq >= 0, "bad arguments");
+    SPX_REQUIRE(points && out && workspace && (queries || nq == 0), "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_voronoi_workspace_bytes(n, height, width), "workspace too small");
+    if (nq == 0) return SPX_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    VorWs L = vor_layout(workspace, n, height, width, nullptr);
+    if (int e = bin_build(L.bins, points, 2, nullptr, nullptr, n, s)) return e;
+    k_nearest_query<<<grid_for(nq, 8, 148 * 32), 256, 0, s>>>(bin_view(L.bins), queries, nq, exclude_self, out);
+    return check_launch("k_nearest_query");
 }
 
 }  // extern "C"

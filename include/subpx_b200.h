@@ -124,6 +124,148 @@ size_t spx_voronoi_workspace_bytes(int n, int height, int width);
 int spx_voronoi_labels(const double* seeds, int n, int height, int width, int* labels,
                        void* workspace, size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------------------------------------
+ * Deblending: smooth background map + one 2-D Gaussian per hole, fitted by Levenberg-Marquardt.
+ * Replaces subpx/_cpu/deblend.py:421-522 (deblend) with subpx/_gpu/deblend.py:453-585 as the
+ * reference GPU driver: fit_gaussians_batch (:174-254) / lm_fit, initial_params (:152-171),
+ * fit_status (:262-277), clean_cells (:136-149), render_models (:87-107) / render_fixed,
+ * _tile_medians (:280-291) / tile_medians, _upsample_tiles (:294-320). Cells are the Voronoi cells
+ * of subpx/_gpu/cells.py:11-38 (box = bbox +- pad clipped; mask = box & labels == j), stored as
+ * boxes (int4 x0, y0, w, h) over the label image instead of a mask stack. Params are ROI-local
+ * [A, x0, y0, u1, u2, u3] as double[6] per cell.
+ * ---------------------------------------------------------------------------------------------- */
+
+enum { SPX_BG_MAP = 0, SPX_BG_FIXED = 1 };
+/* Background map: bg(y, x) = (1 - t[y]) rows[j1[y]-1][x] + t[y] rows[j1[y]][x] (ny > 1),
+ * rows[0][x] (ny == 1), or `fixed` (mode SPX_BG_FIXED). rows: ny x width; j1, t: one per image row. */
+typedef struct spx_bgmap {
+    const double* rows;
+    const int* j1;
+    const double* t;
+    int ny;
+    int width;
+    double fixed;
+    int mode;
+} spx_bgmap;
+
+/* Cell boxes, mask pixel counts and sigma caps max(1, sqrt(count / pi)) from rows (n x 6 double
+ * [x, y, w, h, cx, cy]) and the Voronoi labels. */
+int spx_cells_setup(const double* rows, int n, int pad, int height, int width, const int* voronoi,
+                    int* boxes, int* counts, double* caps, void* stream);
+
+size_t spx_fit_workspace_bytes(int max_cell_pixels);
+/* Initial fits: 10th-percentile cell-border background (or background_level when has_level),
+ * initial_params, LM (max_iter), fit_status. `sign` is -1 for inverted images. */
+int spx_deblend_initial(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                        const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
+                        int max_cell_pixels, double background_level, int has_level, int max_iter,
+                        double* params, uint8_t* status, int* iterations, void* workspace,
+                        size_t workspace_bytes, void* stream);
+/* One outer iteration: clean every cell against `model` and `background`, LM from `params`,
+ * params_out = params + relaxation * (fitted - params), status of params_out, and maxstep =
+ * max |step[1:]| (NaN unless the cell is ok with a finite fit). */
+int spx_deblend_iteration(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                          const int* boxes, const double* caps, int n, int hm, int wm, int max_cell_pixels,
+                          const spx_bgmap* background, const double* model, int radius_cap,
+                          const double* params, double relaxation, int max_iter, double* params_out,
+                          uint8_t* status_out, double* maxstep, int* iterations, void* workspace,
+                          size_t workspace_bytes, void* stream);
+
+size_t spx_render_workspace_bytes(int n, int height, int width);
+/* Sum of every cell's truncated Gaussian (radius clip(ceil(4 sigma_major), 2, radius_cap)) into
+ * model (H x W double), in increasing cell order per pixel. Synchronises the stream. */
+int spx_render_model(const double* params, const int* boxes, int n, int height, int width, int radius_cap,
+                     double* model, void* workspace, size_t workspace_bytes, void* stream);
+/* Cleaned cells of `which` (n_out indices; all cells when null) as an (n_out, hm, wm) stack. */
+int spx_clean_cells(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                    const int* boxes, const double* params, int radius_cap, const spx_bgmap* background,
+                    const double* model, const int* which, int n_out, int hm, int wm, double* out, void* stream);
+
+enum { SPX_TILE_FREE = 0, SPX_TILE_USABLE = 1, SPX_TILE_ALL = 2 };
+/* Per tile (ny x nx, row-major): median (mean of the middle pair; NaN if none) and count of the
+ * residual sign*img - model over the selected pixels: SPX_TILE_FREE = usable & model < thr_model &
+ * sqrt(dist2) >= thr_dist; SPX_TILE_USABLE = usable; SPX_TILE_ALL = every pixel. usable may be null. */
+int spx_tile_medians(const void* img, int dtype, double sign, int height, int width, const double* model,
+                     const unsigned int* dist2, const uint8_t* usable, int mode, double thr_model, double thr_dist,
+                     int tile, double* medians, long long* counts, void* stream);
+/* rows[j][x] = np.interp(x, tile-centre columns, medians[j]) (ny x width). */
+int spx_background_rows(const double* medians, int ny, int nx, int tile, int width, double* rows, void* stream);
+/* out = sign*img - background - model (H x W double). */
+int spx_residual(const void* img, int dtype, double sign, int height, int width, const spx_bgmap* background,
+                 const double* model, double* out, void* stream);
+
+/* Squared distance (uint32) from every pixel to the nearest rint()-ed, clipped seed pixel, as
+ * scipy.ndimage.distance_transform_edt of the seed-pixel mask squared (subpx/_cpu/deblend.py:452-457).
+ * Uses the Voronoi workspace. */
+int spx_seed_distance_map(const double* seeds, int n, int height, int width, unsigned int* dist2,
+                          void* workspace, size_t workspace_bytes, void* stream);
+/* Distance from each query point to the nearest of `points` (excluding the same index when
+ * exclude_self), as cKDTree.query (auto_tile's pitch, subpx/_cpu/deblend.py:396-403, and the
+ * new-seed spacing test of revise_seeds, :564-566). Uses the Voronoi workspace sized for n points. */
+int spx_nearest_distances(const double* points, int n, const double* queries, int nq, int exclude_self,
+                          int height, int width, double* out, void* workspace, size_t workspace_bytes,
+                          void* stream);
+
+/* ------------------------------------------------------------------------------------------------
+ * Seed revision and feature masks. Replaces the SciPy filters of revise_seeds
+ * (subpx/_cpu/deblend.py:555-558: gaussian_filter / maximum_filter, mode "nearest"; the CuPy
+ * variants in the reference GPU path), _unmodelled_features (subpx/cd.py:411-421) and the oversized
+ * exclusion (subpx/cd.py:489-491).
+ * ---------------------------------------------------------------------------------------------- */
+
+/* Separable Gaussian filter (weights of length 2 radius + 1, symmetric), axis 0 then axis 1,
+ * nearest edges; tmp is an H x W scratch image distinct from in and out. */
+int spx_gaussian_filter(const double* in, int height, int width, const double* weights, int radius, double* tmp,
+                        double* out, void* stream);
+/* Separable maximum filter of size 2 radius + 1, nearest edges. */
+int spx_maximum_filter(const double* in, int height, int width, int radius, double* tmp, double* out, void* stream);
+/* Pixels where smooth == maxf, smooth > level and not exclude[i] (exclude may be null), appended as
+ * (y, x) int pairs in any order; *count (device) receives the total (may exceed capacity). */
+int spx_find_peaks(const double* smooth, const double* maxf, const uint8_t* exclude, int height, int width,
+                   double level, int* out_yx, int capacity, int* count, void* stream);
+/* out[i] = flags[labels[i]] for labels > 0 (else 0), then `dilations` dilations with the 3x3 cross
+ * (zero outside the image); tmp is an H x W byte scratch. */
+int spx_label_mask(const int* labels, const uint8_t* flags, int height, int width, int dilations, uint8_t* out,
+                   uint8_t* tmp, void* stream);
+
+/* ------------------------------------------------------------------------------------------------
+ * CD measurements of cleaned cells (an (n, hm, wm) stack, zero outside each cell; cell i is cell
+ * which[i] of the Voronoi labels / boxes, or i when which is null). Replaces subpx/_cpu/cd.py
+ * measure_cells (:267-322: logquad, gradient, halfmax) and gaussian_method (:144-192), with the GPU
+ * reference subpx/_gpu/cd.py (:31-131 rays, :147-207 logquad sums, :465-522 gaussian) as the
+ * batched counterpart. Metric columns: 0 area_px2, 1 cd_equivalent_px, 2 cd_x_px, 3 cd_y_px,
+ * 4 perimeter_px, 5 background, 6 peak_signal, then for the ellipse methods 7 sigma_major_px,
+ * 8 sigma_minor_px, 9 fwhm_major_px, 10 fwhm_minor_px, 11 angle_deg, 12 log_fit_rmse (logquad) or
+ * fit_rmse (gaussian); for the radial methods 7 ray_coverage.
+ * ---------------------------------------------------------------------------------------------- */
+
+typedef struct spx_method_out {
+    double* centers;       /* n x 2 global [x, y] */
+    double* contours;      /* n x (n_angles + 1) x 2 global, or null (metrics only) */
+    uint8_t* status;       /* n status codes */
+    double* metrics;       /* n x n_metrics */
+    double* center_local;  /* n x 2 (radial, logquad) */
+    double* edge_px;       /* n x n_angles (radial) */
+    double* eigenvalues;   /* n x 2 (ellipse methods) */
+    double* axes;          /* n x 2 x 2 (ellipse methods) */
+    int n_metrics;
+} spx_method_out;
+
+/* Half-maximum ellipses of the deblended Gaussian fits (params of cells `which`, ROI-local). */
+int spx_gaussian_method(const double* params, const uint8_t* status_in, const double* cleaned, const int* voronoi,
+                        const int* boxes, const int* which, int n, int hm, int wm, int width, int n_angles,
+                        const spx_method_out* out, void* stream);
+/* Weighted log-quadratic fit of log(signal) over pixels above fit_fraction x peak (background 0). */
+int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, const double* seeds,
+                   int n, int hm, int wm, int width, int n_angles, double fit_fraction, const spx_method_out* out,
+                   void* stream);
+size_t spx_radial_workspace_bytes(int hm, int wm);
+/* Cubic-spline radial profiles; half-height crossings (halfmax) and gradient maxima (gradient).
+ * Either output may be null. */
+int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
+                  int wm, int width, int n_angles, double radial_step, const spx_method_out* halfmax,
+                  const spx_method_out* gradient, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -198,8 +198,57 @@ def make_tiled(out: Path, ref):
                         tile_h=tile_h, overlap=overlap)
 
 
+def cd_cases():
+    from imageprocessor_new_b200 import synthetic as S
+
+    lat2, _ = S.gaussian_lattice(2.0, shape=(120, 240))
+    lat14, _ = S.gaussian_lattice(1.4, shape=(120, 240), seed=1)
+    page = np.ascontiguousarray(S.page_square(0).image[:256, :320])
+    rng = np.random.default_rng(11)
+    cen = S.staggered_grid((192, 256), 24.0, rng)
+    stag = S.add_noise(S.render((192, 256), cen, 12.0 * (1 + rng.uniform(-0.05, 0.05, len(cen))), 1.2,
+                                amplitude=3000.0, background=1000.0), rng, read_noise=100.0, poisson=False)
+    return {
+        "lattice2": (lat2, dict(area_max=400)),
+        "lattice14": (lat14, dict(area_max=400, methods=("gaussian", "halfmax"))),
+        "page": (page, dict(area_max=400)),
+        "staggered": (stag, dict(area_max=400)),
+        "page_invert": ((65535 - page).astype(np.uint16), dict(area_max=400, invert=True,
+                                                               methods=("gaussian", "logquad"))),
+    }
+
+
+def make_cd(out: Path, ref):
+    from subpx import measure_cds
+
+    arrays = {}
+    names = []
+    for name, (img, kw) in cd_cases().items():
+        res = measure_cds(img, backend="cpu", **kw)
+        arrays[f"{name}_img"] = img
+        arrays[f"{name}_seeds"] = res.seeds_xy
+        arrays[f"{name}_cell_labels"] = res.cell_labels
+        arrays[f"{name}_params"] = res.deblend_model["params"]
+        arrays[f"{name}_report"] = res.deblend_model["report"]
+        arrays[f"{name}_bgmap"] = res.background_map.astype(np.float32)
+        arrays[f"{name}_meta"] = np.array([res.meta["deblend_iterations_used"], res.meta["deblend_passes"],
+                                           res.meta["seeds_added_from_residual"],
+                                           res.meta["seeds_dropped_as_insignificant"]])
+        arrays[f"{name}_source"] = np.array(res.meta["background_source"])
+        meths = list(res.measurements)
+        arrays[f"{name}_methods"] = np.array(meths)
+        for m, r in res.measurements.items():
+            arrays[f"{name}_{m}_status"] = r.status
+            arrays[f"{name}_{m}_centers"] = r.centers_xy
+            arrays[f"{name}_{m}_contours"] = r.contours_xy
+            for metric, v in r.metrics.items():
+                arrays[f"{name}_{m}_m_{metric}"] = v
+        names.append(name)
+    np.savez_compressed(out / "cd.npz", names=np.array(names), **arrays)
+
+
 MAKERS = {"thresholds": make_thresholds, "ccl": make_ccl, "centers": make_centers, "voronoi": make_voronoi,
-          "tiled": make_tiled}
+          "tiled": make_tiled, "cd": make_cd}
 
 
 def main():
