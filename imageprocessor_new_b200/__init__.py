@@ -16,13 +16,15 @@ from .centers import (
     filter_centers,
     recommend_refine_method,
 )
+from .cd import METHOD_LABELS, measure_cds
 from .segment import connected_components_stats
 from .voronoi import compute_voronoi_labels, compute_voronoi_labels_gpu
 
 __version__ = "0.1.0"
 
 __all__ = [
-    "CDMethodResult", "CDResult", "CDSummary", "CenterResult", "ComponentStatsResult",
+    "CDMethodResult", "CDResult", "CDSummary", "CenterResult", "ComponentStatsResult", "METHOD_LABELS",
+    "measure_cds",
     "choose_refine_method_for_bbox", "compute_voronoi_labels", "compute_voronoi_labels_gpu",
     "connected_components_stats", "detect_centers", "detect_centers_batch", "detect_centers_tiled",
     "detect_centers_tiled_global_otsu", "filter_centers", "recommend_refine_method",

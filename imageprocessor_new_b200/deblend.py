@@ -282,7 +282,9 @@ class Deblender:
             _lib.call("spx_seed_distance_map", cells.seeds_d.data_ptr(), self.n, h, w, self.dist2.data_ptr(),
                       ws.data_ptr(), ws.numel(), dev.stream_ptr())
         else:
-            self.dist2 = None
+            # No seeds: every pixel is "far" (the reference's distance map is +inf; the FWHM threshold
+            # is then 0, which any distance meets).
+            self.dist2 = torch.zeros((h, w), dtype=torch.int32, device="cuda")
         self.bg = Background(self.shape, self.tile)
 
     # ---------------------------------------------------------------------------- pieces

@@ -41,7 +41,9 @@ def test_measure_cds_matches_reference_cpu(golden, name):
         method = str(method)
         got = res.measurements[method]
         status = z[f"{name}_{method}_status"]
-        assert np.mean(got.status == status) >= 0.999, method
+        assert got.status.shape == status.shape, method
+        if len(status):
+            assert np.mean(got.status == status) >= 0.999, method
         both = got.valid & (status == "ok")
         cd = z[f"{name}_{method}_m_cd_equivalent_px"]
         delta = np.abs(got.metrics["cd_equivalent_px"][both] - cd[both])
