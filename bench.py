@@ -1,0 +1,274 @@
+"""Benchmark of the subpixel-metrology hot path on B200 (one JSON line on rank 0).
+
+Workload (one step): the 8192 x 8192 uint16 staggered contact-hole page (pitch 24, d 12 +- 5 %,
+sigma 1.2, ~116k holes incl. border-clipped), synthetic and seeded: detect_centers with the three
+refiners (weighted, logquad, edge_gradmoment) and measure_cds (model background, LM Gaussian-FWHM,
+radial-gradient and half-height CDs, summary_only), all through the public API.
+
+  value  cells/s with the page already in HBM (a CUDA tensor passed to the API)
+  e2e    cells/s through the same API with a host (NumPy) page: host->device copy of the page and
+         device->host copy of the results inside the timed region
+
+Cells = Voronoi cells reported and measured by the LM Gaussian method. The page (134 MB) is larger
+than the 126 MB L2, so consecutive steps do not run from cache.
+
+``--impl reference`` times the CPU path (the oracle restatement of the reference algorithm, NumPy /
+SciPy on the host cores) on a crop of the same page; under torchrun only rank 0 runs it.
+Multi-GPU: one process per GPU, each measuring its own page (weak scaling, no collective on the
+data path); the step time is the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cells/s on 1 B200 at ≤1e-3 px vs FP64: NN-warm-started LM vs plain LM"
+UNIT = "cells/s"
+WORKLOAD = "page_staggered_8192x8192_u16_pitch24_d12_3refiners_3cd"
+METHODS = ("gaussian", "gradient", "halfmax")
+REFINERS = ("weighted", "logquad", "edge_gradmoment")
+CD_KW = dict(area_max=400, summary_only=True)
+CENTER_KW = dict(threshold="otsu", area_max=400)
+
+
+def _dist():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def _peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def make_page(rank: int):
+    from imageprocessor_new_b200 import synthetic
+
+    return synthetic.page_staggered(seed=rank).image
+
+
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    from imageprocessor_new_b200 import _lib, deblend, detect_centers, measure_cds
+
+    rank, world, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    page = make_page(rank)
+    page_d = torch.from_numpy(page).cuda()
+    lib = _lib.lib()
+
+    # Dominant-kernel timing: CUDA events around every LM deblending iteration (one k_fit_iteration
+    # launch each) on the launching stream, inside the timed region.
+    fit_times = []
+    fit_cells = []
+    orig_iteration = deblend.Deblender.iteration
+
+    def timed_iteration(self, params_d, model, bg):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        out = orig_iteration(self, params_d, model, bg)
+        e.record()
+        fit_times.append((s, e))
+        fit_cells.append(self.n)
+        return out
+
+    deblend.Deblender.iteration = timed_iteration
+
+    def step(image):
+        for refine in REFINERS:
+            detect_centers(image, backend="gpu", refine=refine, **CENTER_KW)
+        return measure_cds(image, backend="gpu", methods=METHODS, **CD_KW)
+
+    def run(image, k):
+        fit_times.clear()
+        fit_cells.clear()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = lib.spx_launch_count()
+        s.record()
+        cells = 0
+        for _ in range(k):
+            res = step(image)
+            cells += len(res.seeds_xy)
+        e.record()
+        torch.cuda.synchronize()
+        launches = lib.spx_launch_count() - n0
+        ms = s.elapsed_time(e)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return ms, cells, launches
+
+    for _ in range(args.warmup):
+        step(page_d)
+    with ClockSampler(local) as clocks:
+        ms, cells, launches = run(page_d, args.steps)
+    fit_ms = [a.elapsed_time(b) for a, b in fit_times]
+    fit_avg_ms = float(np.mean(fit_ms)) if fit_ms else float("nan")
+    fit_n = float(np.mean(fit_cells)) if fit_cells else 0.0
+    # End to end: host page, copies inside the region.
+    step(page)
+    ms_e2e, cells_e2e, _ = run(page, args.steps)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    per_step_cells = cells / args.steps
+    value = world * per_step_cells / (ms / 1e3 / args.steps)
+    e2e = world * (cells_e2e / args.steps) / (ms_e2e / 1e3 / args.steps)
+    peaks, which = _peaks()
+    # Roofline of the dominant kernel (the LM deblending iteration, FP64, compute-bound): its
+    # algorithmic HBM bytes per launch are the cells' pixels read (image 2 B + labels 4 B + model 8 B
+    # + background rows 8 B) plus 6 params in / 6 out + status; its FP64 rate is reported beside.
+    px_per_cell = 24 * 24
+    bytes_per_cell = px_per_cell * (2 + 4 + 8 + 8) + 13 * 8
+    achieved = fit_n * bytes_per_cell / (fit_avg_ms / 1e3) / 1e9 if fit_ms else None
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded render + noise)",
+        "config": {"workload": WORKLOAD, "image": "8192x8192 uint16", "cells_per_step": per_step_cells,
+                   "methods": list(METHODS), "refiners": list(REFINERS), "l2": "inputs larger than L2 (134 MB page)",
+                   "warm_start": "plain LM (no network)"},
+        "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(page.nbytes) * (len(REFINERS) + 1),
+                "d2h_bytes_per_step": int(per_step_cells * 8 * 13 * len(METHODS))},
+        "roofline": {"bound": "hbm", "kernel": "k_fit_iteration", "achieved": None if achieved is None else round(achieved, 1),
+                     "peak": peaks.get("hbm_gbs"), "peak_source": which, "unit": "GB/s",
+                     "frac": None if achieved is None else round(achieved / peaks["hbm_gbs"], 4),
+                     "traffic": None, "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if args.cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(page, args.cpu_sample)
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(page, size):
+    """The oracle (CPU restatement of the reference path) on a crop of the page, all host cores."""
+    from oracle import cd as ocd
+    from oracle import centers as oc
+
+    crop = np.ascontiguousarray(page[:size, :size])
+    t0 = time.perf_counter()
+    for refine in REFINERS:
+        oc.detect_centers(crop, threshold="otsu", refine_method=refine, area_max=400)
+    res = ocd.measure_cds(crop, methods=METHODS, area_max=400)
+    dt = time.perf_counter() - t0
+    n = len(res["seeds"])
+    return {"value": round(n / dt, 2), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{size}x{size} crop of the page ({n} cells), same step", "seconds": round(dt, 2)}
+
+
+def reference_arm(args):
+    rank, world, _ = _dist()
+    if rank != 0:
+        return
+    page = make_page(0)
+    size = args.cpu_sample
+    for _ in range(max(0, min(args.warmup, 1))):
+        pass
+    vals, secs, cells = [], [], 0
+    for _ in range(args.steps):
+        r = cpu_baseline(page, size)
+        vals.append(r["value"])
+        secs.append(r["seconds"])
+    value = float(np.median(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * float(np.mean(secs)), 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded render + noise)",
+            "config": {"workload": WORKLOAD, "sample": f"{size}x{size} crop"}, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{size}x{size} crop of the page, same step"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=("gpu", "reference"))
+    ap.add_argument("--cpu-sample", type=int, default=768)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

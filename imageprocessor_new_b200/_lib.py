@@ -51,6 +51,7 @@ _MO = POINTER(MethodOut)
 SIGNATURES = {
     "spx_last_error": (ctypes.c_char_p, []),
     "spx_version": (_I, []),
+    "spx_launch_count": (ctypes.c_ulonglong, []),
     "spx_device_info": (_I, [POINTER(c_int), POINTER(c_int)]),
     "spx_otsu_workspace_bytes": (_S, [_I]),
     "spx_otsu": (_I, [_P, _I, _I, _I, _I, _P, _P, _S, _P]),

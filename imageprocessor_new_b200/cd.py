@@ -50,10 +50,16 @@ def _validate(img, *, methods, background, seeds, threshold, area_min, area_max,
               smooth_sigma, fit_fraction, deblend_iterations, deblend_tolerance, pixel_size, unit, metrics_only,
               summary_only, peak_min_distance, background_tile, background_level):
     """The reference's argument checks (subpx/cd.py:286-365), same messages."""
-    if img.ndim != 2 or img.size == 0 or not np.issubdtype(img.dtype, np.number):
-        raise ValueError("image must be a nonempty 2D real grayscale array")
-    if np.iscomplexobj(img) or not np.isfinite(img).all():
-        raise ValueError("image must contain finite real intensities")
+    if isinstance(img, torch.Tensor):
+        if img.ndim != 2 or img.numel() == 0 or img.dtype not in dev.TORCH_DTYPES.values():
+            raise ValueError("image must be a nonempty 2D real grayscale array")
+        if img.dtype.is_floating_point and not bool(torch.isfinite(img).all()):
+            raise ValueError("image must contain finite real intensities")
+    else:
+        if img.ndim != 2 or img.size == 0 or not np.issubdtype(img.dtype, np.number):
+            raise ValueError("image must be a nonempty 2D real grayscale array")
+        if np.iscomplexobj(img) or not np.isfinite(img).all():
+            raise ValueError("image must contain finite real intensities")
     if background not in {"model", "border"}:
         raise ValueError("background must be 'model' or 'border'")
     if seeds not in {"threshold", "peaks"}:
@@ -132,7 +138,9 @@ def measure_cds(
     reference's other method families (``nominal_cd``, ``psf_fwhm``, ``half_area_level``, ...) are
     accepted in ``other`` and must keep their defaults.
     """
-    img = np.asarray(image.detach().cpu().numpy() if isinstance(image, torch.Tensor) else image)
+    on_device = isinstance(image, torch.Tensor) and image.is_cuda
+    img = image if on_device else np.asarray(image.detach().cpu().numpy() if isinstance(image, torch.Tensor)
+                                             else image)
     methods = _validate(img, methods=methods, background=background, seeds=seeds, threshold=threshold,
                         area_min=area_min, area_max=area_max, pad=pad, n_angles=n_angles, radial_step=radial_step,
                         smooth_sigma=smooth_sigma, fit_fraction=fit_fraction, deblend_iterations=deblend_iterations,
@@ -165,10 +173,10 @@ def measure_cds(
                             summary_only=bool(summary_only))
 
 
-def _segment(img: np.ndarray, img_d: torch.Tensor, threshold: str, invert: bool):
+def _segment(img_d: torch.Tensor, threshold: str, invert: bool):
     """Binary components of the reference's segmentation (subpx/cd.py:472-481): uint8 and uint16 +
     Otsu images are thresholded as they are, others are scaled to uint8 first."""
-    rescaled = img.dtype != np.uint8 and not (img.dtype == np.uint16 and threshold == "otsu")
+    rescaled = img_d.dtype != torch.uint8 and not (img_d.dtype == torch.uint16 and threshold == "otsu")
     seg = img_d
     if rescaled:
         gray = img_d.to(torch.float64)
@@ -177,7 +185,7 @@ def _segment(img: np.ndarray, img_d: torch.Tensor, threshold: str, invert: bool)
         if span:
             seg = torch.round((gray - lo) * (255 / span)).to(torch.uint8)
         else:
-            seg = torch.zeros(img.shape, dtype=torch.uint8, device="cuda")
+            seg = torch.zeros(img_d.shape, dtype=torch.uint8, device="cuda")
     thr = segment.binarize_threshold(seg, threshold, invert)
     comp = segment.label(seg, threshold=thr, invert=invert, connectivity=8)
     return comp, rescaled
@@ -279,10 +287,13 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
                  metrics_only, summary_only):
     started = time.perf_counter()
     seconds = {}
-    height, width = img.shape
+    height, width = tuple(img.shape)
     sign = -1.0 if invert else 1.0
-    img_d = dev.upload(img if img.dtype in _lib.DTYPES else img.astype(np.float64))
-    comp, rescaled = _segment(img, img_d, threshold, invert)
+    if isinstance(img, torch.Tensor):
+        img_d = img.contiguous()
+    else:
+        img_d = dev.upload(img if img.dtype in _lib.DTYPES else img.astype(np.float64))
+    comp, rescaled = _segment(img_d, threshold, invert)
     stats = comp.stats.cpu().numpy()
     cents = comp.centroids.cpu().numpy()
     k = comp.count
@@ -313,7 +324,8 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
                   out.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
         return out
 
-    cells = build_cells(rows, img.shape, pad)
+    shape = tuple(img_d.shape)
+    cells = build_cells(rows, shape, pad)
     seconds["segmentation"] = time.perf_counter() - started
     meta = {
         "background": "model", "seeds": "threshold", "threshold": threshold, "invert": bool(invert),
@@ -335,7 +347,7 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
 
     from .deblend import auto_tile
 
-    tile_px, pitch = auto_tile(cells.seeds_d, cells.n, img.shape)
+    tile_px, pitch = auto_tile(cells.seeds_d, cells.n, shape)
     tiled_seeds = cells
 
     def tile_for(cells_):
@@ -368,7 +380,7 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         interior = np.concatenate((interior[keep_s], np.ones(len(new), bool)))
         by_reach = np.concatenate((by_reach[keep_s], np.ones(len(new), bool)))
         added, dropped = added + len(new), dropped + int(drop.sum())
-        cells = build_cells(rows, img.shape, pad)
+        cells = build_cells(rows, shape, pad)
     if by_reach.any():
         params = state.params[by_reach]
         centers = params[:, 1:3] + cells.origins[by_reach]
@@ -456,7 +468,7 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         rois = cleaned.cpu().numpy()
         masks = _mask_stack(c, report)
     result = CDResult(
-        image=img.copy(), binary=comp.labels.cpu().numpy() > 0, component_labels=comp.labels.cpu().numpy(),
+        image=img_d.cpu().numpy() if isinstance(img, torch.Tensor) else img.copy(), binary=comp.labels.cpu().numpy() > 0, component_labels=comp.labels.cpu().numpy(),
         component_ids=np.asarray(component_ids, dtype=np.int32)[report],
         boxes_xywh=rows[report, :4].astype(np.int32), seeds_xy=c.seeds[report], cell_labels=cell_labels,
         cell_areas_px2=np.bincount(cell_labels[cell_labels >= 0], minlength=nr), origins_xy=c.origins[report],

@@ -37,14 +37,22 @@ def _check_backend(backend: str) -> None:
         raise ValueError("imageprocessor_new_b200 is the GPU backend: backend must be 'gpu' or 'auto'")
 
 
-def _as_image(image) -> np.ndarray:
-    img = image.detach().cpu().numpy() if isinstance(image, torch.Tensor) else np.asarray(image)
+def _as_image(image):
+    """NumPy array, or a CUDA tensor kept on the device."""
+    if isinstance(image, torch.Tensor) and image.is_cuda:
+        img = image
+    else:
+        img = image.detach().cpu().numpy() if isinstance(image, torch.Tensor) else np.asarray(image)
     if img.ndim != 2:
         raise ValueError("Expected 2D grayscale image.")
     return img
 
 
-def _device_image(img: np.ndarray) -> torch.Tensor:
+def _device_image(img) -> torch.Tensor:
+    if isinstance(img, torch.Tensor):
+        if img.dtype not in dev.TORCH_DTYPES.values():
+            raise ValueError(f"unsupported image dtype {img.dtype}; use uint8, uint16, float32 or float64")
+        return img.contiguous()
     if img.dtype not in _lib.DTYPES:
         raise ValueError(f"unsupported image dtype {img.dtype}; use uint8, uint16, float32 or float64")
     return dev.upload(img)

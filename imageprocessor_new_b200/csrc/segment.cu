@@ -28,6 +28,7 @@
 namespace spx {
 
 static thread_local char g_error[1024];
+static unsigned long long g_launches = 0;  // kernel launches issued by this library (all threads)
 
 void set_error(const char* fmt, ...) {
     va_list ap;
@@ -37,6 +38,7 @@ void set_error(const char* fmt, ...) {
 }
 
 int check_launch(const char* what) {
+    __atomic_add_fetch(&g_launches, 1ull, __ATOMIC_RELAXED);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("%s launch failed: %s", what, cudaGetErrorString(e));
@@ -632,6 +634,8 @@ extern "C" {
 const char* spx_last_error(void) { return spx::g_error; }
 
 int spx_version(void) { return 1; }
+
+unsigned long long spx_launch_count(void) { return __atomic_load_n(&spx::g_launches, __ATOMIC_RELAXED); }
 
 int spx_device_info(int* sm_count, int* is_sm100) {
     int dev = 0;

@@ -54,6 +54,8 @@ enum {
 
 const char* spx_last_error(void);
 int spx_version(void);
+/* Number of kernel launches this library has issued in the process (for launch accounting). */
+unsigned long long spx_launch_count(void);
 /* Number of SMs of the current device, and whether it is an sm_100 part (1) or not (0). */
 int spx_device_info(int* sm_count, int* is_sm100);
 

@@ -65,3 +65,32 @@ def test_tiled_rules_match_reference():
     assert got.shape == want.shape
     key = lambda a: a[np.lexsort((a[:, 1], a[:, 0]))]
     np.testing.assert_allclose(key(got), key(want), rtol=0, atol=1e-9)
+
+
+CD_CASES = {
+    "lattice2": dict(area_max=400),
+    "lattice14": dict(area_max=400, methods=("gaussian", "halfmax")),
+    "page": dict(area_max=400),
+    "staggered": dict(area_max=400),
+    "page_invert": dict(area_max=400, invert=True, methods=("gaussian", "logquad")),
+}
+
+
+@pytest.mark.parametrize("name", ["lattice2", "page", "page_invert"])
+def test_measure_cds_oracle_matches_reference(name):
+    from oracle import cd as ocd
+
+    z = _load("cd")
+    kw = dict(CD_CASES[name])
+    got = ocd.measure_cds(z[f"{name}_img"], **kw)
+    np.testing.assert_array_equal(got["seeds"], z[f"{name}_seeds"])
+    np.testing.assert_array_equal(got["cell_labels"], z[f"{name}_cell_labels"])
+    assert got["iterations_used"] == z[f"{name}_meta"][0]
+    np.testing.assert_allclose(got["params"], z[f"{name}_params"], rtol=0, atol=1e-9)
+    for method in z[f"{name}_methods"]:
+        method = str(method)
+        r = got["measurements"][method]
+        np.testing.assert_array_equal(r["status"], z[f"{name}_{method}_status"])
+        np.testing.assert_allclose(r["metrics"]["cd_equivalent_px"], z[f"{name}_{method}_m_cd_equivalent_px"],
+                                   rtol=0, atol=1e-9, equal_nan=True)
+        np.testing.assert_allclose(r["contours"], z[f"{name}_{method}_contours"], rtol=0, atol=1e-9, equal_nan=True)
