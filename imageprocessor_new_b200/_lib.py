@@ -55,6 +55,7 @@ SIGNATURES = {
     "spx_device_info": (_I, [POINTER(c_int), POINTER(c_int)]),
     "spx_otsu_workspace_bytes": (_S, [_I]),
     "spx_otsu": (_I, [_P, _I, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_otsu_static": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "spx_triangle": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
     "spx_ccl_label": (_I, [_P, _I, _I, _I, _P, _D, _I, _I, _P, _P, _P, _S, _P]),

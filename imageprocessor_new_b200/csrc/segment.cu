@@ -24,6 +24,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 namespace spx {
 
@@ -624,6 +625,49 @@ CclLayout ccl_layout(void* ws, int H, int W, size_t* bytes) {
     return L;
 }
 
+// ---------------------------------------------------------------------- allocation-free Otsu
+
+// Scratch of spx_otsu_static: the same pieces as the Otsu workspace (histogram, value range, four
+// per-bin arrays of the scan), in one file-scope device array. Every GPU that loads this library
+// holds it (2.3 MiB) until the process exits.
+constexpr size_t kOtsuStaticBytes = 65536 * sizeof(unsigned int) + 256 + 4 * 65536 * sizeof(double) + 256;
+__device__ __align__(256) unsigned char g_otsu_static[kOtsuStaticBytes];
+
+__global__ void k_range_init(unsigned int* range) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        range[0] = 0xffffffffu;
+        range[1] = 0u;
+    }
+}
+
+__global__ void k_zero_u32(unsigned int* p, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0u;
+}
+
+// Device address of g_otsu_static for the current device, looked up once per device.
+int otsu_static_scratch(void** out) {
+    static std::mutex mu;
+    static void* cache[128] = {};
+    int dev = 0;
+    SPX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) {
+        set_error("device index %d out of range", dev);
+        return SPX_ERR_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cache[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_otsu_static);
+        if (e != cudaSuccess || !p) {
+            set_error("cudaGetSymbolAddress(g_otsu_static) failed: %s", cudaGetErrorString(e));
+            return SPX_ERR_CUDA;
+        }
+        cache[dev] = p;
+    }
+    *out = cache[dev];
+    return SPX_OK;
+}
+
 }  // namespace
 }  // namespace spx
 
@@ -683,6 +727,42 @@ int spx_otsu(const void* img, int dtype, int height, int width, int step, double
     double* bufs = a.take<double>(4 * 65536);
     k_otsu_scan<<<1, 1024, 0, s>>>(hist, nbins, range, n, bufs, bufs + 65536, bufs + 2 * 65536,
                                    bufs + 3 * 65536, threshold);
+    return check_launch("k_otsu_scan");
+}
+
+int spx_otsu_static(const void* img, int dtype, int height, int width, int step, double* threshold, void* stream) {
+    SPX_REQUIRE(dtype == SPX_U8 || dtype == SPX_U16, "Otsu thresholding needs a uint8 or uint16 image");
+    SPX_REQUIRE(height > 0 && width > 0 && step >= 1, "bad image size or step");
+    const long long hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    SPX_REQUIRE(hs * ws <= 0xffffffffLL,
+                "spx_otsu_static: %lld sampled pixels exceed the maximum of 4294967295 (32-bit histogram counts)",
+                hs * ws);
+    SPX_REQUIRE(img && threshold, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    void* scratch = nullptr;
+    if (int e = otsu_static_scratch(&scratch)) return e;
+    Arena a(scratch);
+    unsigned int* hist = a.take<unsigned int>(65536);
+    unsigned int* range = a.take<unsigned int>(2);
+    double* bufs = a.take<double>(4 * 65536);
+    SPX_REQUIRE(a.used <= kOtsuStaticBytes, "static Otsu scratch too small");
+    const int nbins = dtype == SPX_U8 ? 256 : 65536;
+    const long long n = hs * ws;
+    // The array keeps the previous call's contents: clear the histogram and reset the range first.
+    k_zero_u32<<<64, 256, 0, s>>>(hist, 65536);
+    if (int e = check_launch("k_zero_u32")) return e;
+    k_range_init<<<1, 32, 0, s>>>(range);
+    if (int e = check_launch("k_range_init")) return e;
+    k_minmax<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(img, dtype, height, width, step, range);
+    if (int e = check_launch("k_minmax")) return e;
+    const size_t smem = kHistSmemBins * sizeof(unsigned int);
+    SPX_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int dense = step == 1 && dtype == SPX_U16 && (reinterpret_cast<uintptr_t>(img) % 16) == 0;
+    k_histogram<<<grid_for(n / 8 + 1, 512, 148 * 3), 512, smem, s>>>(img, dtype, height, width, step, dense, range,
+                                                                     hist);
+    if (int e = check_launch("k_histogram")) return e;
+    k_otsu_scan<<<1, 1024, 0, s>>>(hist, nbins, range, n, bufs, bufs + 65536, bufs + 2 * 65536, bufs + 3 * 65536,
+                                   threshold);
     return check_launch("k_otsu_scan");
 }
 

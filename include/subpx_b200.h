@@ -72,6 +72,19 @@ size_t spx_otsu_workspace_bytes(int dtype);
 int spx_otsu(const void* img, int dtype, int height, int width, int step, double* threshold,
              void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free Otsu threshold, for callers that cannot allocate device memory or pass a
+ * workspace: code running inside CUDA stream capture or a real-time acquisition loop, where
+ * cudaMalloc would synchronise the device or fail under a fixed memory budget, and hosts whose own
+ * allocator owns every device byte. No counterpart in the reference: it is spx_otsu with its scratch
+ * in a 2.3 MiB file-scope device array that every GPU loading the library holds until exit.
+ * Limit: at most 4294967295 sampled pixels (ceil(H/step) * ceil(W/step)), the range of the 32-bit
+ * histogram counts; larger images are rejected with SPX_ERR_ARGUMENT. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make it before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller. Allocates nothing (no cudaMalloc, cudaFree or
+ * allocating library call). */
+int spx_otsu_static(const void* img, int dtype, int height, int width, int step, double* threshold, void* stream);
+
 /* Triangle threshold of a uint8 image, as OpenCV's THRESH_TRIANGLE (uses the Otsu workspace). */
 int spx_triangle(const void* img, int dtype, int height, int width, double* threshold,
                  void* workspace, size_t workspace_bytes, void* stream);
