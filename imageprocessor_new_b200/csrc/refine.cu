@@ -246,6 +246,56 @@ __device__ bool solve_lu(double (&A)[N][N], double (&b)[N]) {
     return true;
 }
 
+// Eigen-decomposition of a symmetric 6x6 matrix by cyclic Jacobi rotations: A is destroyed, its
+// diagonal ends up holding the eigenvalues, the columns of V the eigenvectors.
+__device__ void jacobi6(double (&A)[6][6], double (&V)[6][6]) {
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) V[i][j] = i == j ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 30; ++sweep) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < 6; ++i) {
+            diag += A[i][i] * A[i][i];
+            for (int j = i + 1; j < 6; ++j) off += A[i][j] * A[i][j];
+        }
+        if (off == 0.0 || off <= 1e-36 * diag) break;
+        for (int p = 0; p < 5; ++p)
+            for (int q = p + 1; q < 6; ++q) {
+                const double apq = A[p][q];
+                if (apq == 0.0) continue;
+                const double theta = (A[q][q] - A[p][p]) / (2.0 * apq);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < 6; ++k) {
+                    const double akp = A[k][p], akq = A[k][q];
+                    A[k][p] = c * akp - sn * akq;
+                    A[k][q] = sn * akp + c * akq;
+                }
+                for (int k = 0; k < 6; ++k) {
+                    const double apk = A[p][k], aqk = A[q][k];
+                    A[p][k] = c * apk - sn * aqk;
+                    A[q][k] = sn * apk + c * aqk;
+                }
+                for (int k = 0; k < 6; ++k) {
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - sn * vkq;
+                    V[k][q] = sn * vkp + c * vkq;
+                }
+            }
+    }
+}
+
+// Coefficients in ROI pixel coordinates from coefficients in u = (x - xm) / s, v = (y - ym) / s
+// (design [x^2, y^2, xy, x, y, 1] in both).
+__device__ void unscale_coef(const double* c, double xm, double ym, double s, double* out) {
+    const double s2 = s * s;
+    out[0] = c[0] / s2;
+    out[1] = c[1] / s2;
+    out[2] = c[2] / s2;
+    out[3] = (-2.0 * c[0] * xm - c[2] * ym) / s2 + c[3] / s;
+    out[4] = (-2.0 * c[1] * ym - c[2] * xm) / s2 + c[4] / s;
+    out[5] = (c[0] * xm * xm + c[1] * ym * ym + c[2] * xm * ym) / s2 - (c[3] * xm + c[4] * ym) / s + c[5];
+}
+
 __device__ void refine_logquad(const void* img, int dtype, const int* labels, int W, const Roi& r,
                                double* keys, int lane, double* cx, double* cy) {
     *cx = *cy = dnan();
@@ -285,13 +335,67 @@ __device__ void refine_logquad(const void* img, int dtype, const int* labels, in
     for (int a = 0; a < 6; ++a)
         for (int c = a; c < 6; ++c) { A[a][c] = A[c][a] = acc[q++]; }
     for (int a = 0; a < 6; ++a) b[a] = acc[21 + a];
-    if (!solve_lu<6>(A, b)) return;
-    const double ca = b[0], cb = b[1], cc = b[2], cd = b[3], ce = b[4], cf = b[5];
-    // A flat blob (log-values constant over the mask) has zero curvature: the reference's SVD
-    // least squares then returns rounding noise for a..e and no meaningful stationary point. Treat
-    // curvature below 1e-9 of the fitted level (in ROI-scaled units) as no fit.
-    const double level = fmax(1.0, fabs(cf));
-    if (fmax(fmax(fabs(ca), fabs(cb)), fabs(cc)) <= 1e-9 * level) return;
+    double ca, cb, cc, cd, ce;
+    const bool degenerate = (ms.xmax - ms.xmin) <= 1 || (ms.ymax - ms.ymin) <= 1;
+    if (!degenerate) {
+        if (!solve_lu<6>(A, b)) return;
+        const double cf = b[5];
+        ca = b[0]; cb = b[1]; cc = b[2]; cd = b[3]; ce = b[4];
+        // A flat blob (log-values constant over the mask) has zero curvature: the reference's SVD
+        // least squares then returns rounding noise for a..e and no meaningful stationary point.
+        // Treat curvature below 1e-9 of the fitted level (in ROI-scaled units) as no fit.
+        const double level = fmax(1.0, fabs(cf));
+        if (fmax(fmax(fabs(ca), fabs(cb)), fabs(cc)) <= 1e-9 * level) return;
+    } else {
+        // Blobs one or two pixels thick: the design is rank-deficient (for two rows y1, y2,
+        // y^2 - (y1 + y2) y + y1 y2 = 0 on every pixel). lstsq returns the minimum-norm solution in
+        // pixel coordinates; build it from the scaled problem: pseudo-inverse solution there, mapped
+        // to pixel coordinates, minus its component along the (mapped) null space.
+        double V[6][6];
+        jacobi6(A, V);
+        double lmax = 0.0;
+        for (int k = 0; k < 6; ++k) lmax = fmax(lmax, A[k][k]);
+        double cs[6] = {0, 0, 0, 0, 0, 0};
+        double nul[6][6];
+        int nn = 0;
+        for (int k = 0; k < 6; ++k) {
+            const double lam = A[k][k];
+            if (lam > 1e-11 * lmax) {
+                double dot = 0.0;
+                for (int r2 = 0; r2 < 6; ++r2) dot += V[r2][k] * b[r2];
+                for (int r2 = 0; r2 < 6; ++r2) cs[r2] += V[r2][k] * (dot / lam);
+            } else {
+                double col[6];
+                for (int r2 = 0; r2 < 6; ++r2) col[r2] = V[r2][k];
+                unscale_coef(col, xm, ym, sc, nul[nn]);
+                ++nn;
+            }
+        }
+        double cp[6];
+        unscale_coef(cs, xm, ym, sc, cp);
+        // Orthonormalise the null directions (Gram-Schmidt) and project them out of cp.
+        for (int k = 0; k < nn; ++k) {
+            for (int j = 0; j < k; ++j) {
+                double d = 0.0;
+                for (int r2 = 0; r2 < 6; ++r2) d += nul[k][r2] * nul[j][r2];
+                for (int r2 = 0; r2 < 6; ++r2) nul[k][r2] -= d * nul[j][r2];
+            }
+            double nrm = 0.0;
+            for (int r2 = 0; r2 < 6; ++r2) nrm += nul[k][r2] * nul[k][r2];
+            nrm = sqrt(nrm);
+            if (!(nrm > 0.0)) continue;
+            for (int r2 = 0; r2 < 6; ++r2) nul[k][r2] /= nrm;
+            double d = 0.0;
+            for (int r2 = 0; r2 < 6; ++r2) d += nul[k][r2] * cp[r2];
+            for (int r2 = 0; r2 < 6; ++r2) cp[r2] -= d * nul[k][r2];
+        }
+        // Back to the scaled units of the code below (its cond test and centre map undo them).
+        ca = cp[0] * sc * sc;
+        cb = cp[1] * sc * sc;
+        cc = cp[2] * sc * sc;
+        cd = (cp[3] + 2.0 * cp[0] * xm + cp[2] * ym) * sc;
+        ce = (cp[4] + 2.0 * cp[1] * ym + cp[2] * xm) * sc;
+    }
     // H = [[2a, c], [c, 2b]] (in scaled units); cond(H) by its eigenvalues (symmetric).
     const double h00 = 2.0 * ca, h01 = cc, h11 = 2.0 * cb;
     const double mean = 0.5 * (h00 + h11), half = 0.5 * (h00 - h11);

@@ -130,6 +130,23 @@ int spx_refine_centers(const void* img, int dtype, int height, int width, const 
                        double* centers_out, void* stream);
 
 /* ------------------------------------------------------------------------------------------------
+ * Tiled detection (detect_centers(tile_h=...), subpx/_gpu/centers.py:1778-1862 and
+ * subpx/legacy.py:93-95): band keep rule and dedupe_centers (subpx/centers.py:335-378).
+ * ---------------------------------------------------------------------------------------------- */
+
+size_t spx_keep_band_workspace_bytes(int n);
+/* Appends the finite centres of one band (band-local y) whose global y = y + y_offset lies in
+ * [keep_lo, keep_hi) to out at the device counter *count (zero it before the first band), in order. */
+int spx_keep_band(const double* centers, int n, double y_offset, double keep_lo, double keep_hi, double* out,
+                  int* count, int capacity, void* workspace, size_t workspace_bytes, void* stream);
+size_t spx_dedupe_workspace_bytes(int n, double xmin, double ymin, double xmax, double ymax, double eps);
+/* Clusters of centres linked by squared distance <= eps^2 (union-find), each replaced by the mean
+ * of its members summed in index order; clusters ordered by their smallest member; *count (device)
+ * = number of clusters. out needs n rows. [xmin, xmax] x [ymin, ymax] bounds the centres. */
+int spx_dedupe_centers(const double* centers, int n, double xmin, double ymin, double xmax, double ymax, double eps,
+                       double* out, int* count, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------------------------------
  * Voronoi partition. Replaces subpx/_cpu/cells.py:8-33 (compute_voronoi_labels_cpu, cKDTree) and
  * subpx/_gpu/voronoi.py:124-151 (_labels_device): nearest seed by FP64 squared distance
  * dx*dx + dy*dy (no FMA), exact ties to the lowest seed index; -1 everywhere without seeds.

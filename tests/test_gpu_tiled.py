@@ -1,0 +1,54 @@
+"""detect_centers(tile_h=...) on the GPU against the reference's tiled rules (golden) and dedupe."""
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from oracle import centers as oc
+
+pytestmark = pytest.mark.gpu
+
+
+def _sorted(a):
+    return a[np.lexsort((a[:, 1], a[:, 0]))]
+
+
+def test_tiled_matches_reference_rules():
+    from imageprocessor_new_b200 import detect_centers_tiled
+
+    z = np.load(GOLDEN / "tiled.npz")
+    with pytest.warns(DeprecationWarning):
+        res = detect_centers_tiled(z["img"], tile_h=int(z["tile_h"]), overlap=int(z["overlap"]), backend="gpu",
+                                   threshold="otsu", area_max=200, refine="logquad")
+    want = z["centers"]
+    assert res.centers_xy.shape == want.shape
+    np.testing.assert_allclose(_sorted(res.centers_xy), _sorted(want), rtol=0, atol=1e-9)
+
+
+@pytest.mark.parametrize("n, eps", [(0, 1.5), (1, 1.5), (500, 1.5), (20000, 1.5), (3000, 0.0), (4000, 6.0)])
+def test_dedupe_matches_oracle(n, eps):
+    from imageprocessor_new_b200.tiled import dedupe_centers
+
+    rng = np.random.default_rng(n)
+    base = rng.uniform(0, 2000, (n, 2))
+    # Near duplicates, exact duplicates and chains.
+    dup = base[: n // 3] + rng.normal(0, 0.5, (n // 3, 2))
+    pts = np.concatenate([base, dup, base[: n // 10]]) if n else np.zeros((0, 2))
+    pts = pts[rng.permutation(len(pts))]
+    got = dedupe_centers(pts, eps=eps)
+    want = oc.dedupe(pts, eps)
+    assert got.shape == want.shape
+    np.testing.assert_array_equal(got, want)
+
+
+def test_tiled_per_tile_threshold_and_bad_overlap():
+    from imageprocessor_new_b200 import detect_centers, synthetic
+
+    page = synthetic.page_square(2).image
+    res = detect_centers(page, backend="gpu", tile_h=300, overlap=40, threshold="otsu", threshold_mode="per_tile",
+                         area_max=400, refine="weighted")
+    full = detect_centers(page, backend="gpu", threshold="otsu", area_max=400, refine="weighted").centers_xy
+    # Bands of 300 rows see whole holes (pitch 32) in their keep zones: the same centres.
+    assert abs(len(res.centers_xy) - len(full)) <= 2
+    with pytest.raises(ValueError):
+        detect_centers(page, backend="gpu", tile_h=100, overlap=100)
