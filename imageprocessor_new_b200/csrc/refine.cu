@@ -247,8 +247,10 @@ __device__ bool solve_lu(double (&A)[N][N], double (&b)[N]) {
 }
 
 // Eigen-decomposition of a symmetric 6x6 matrix by cyclic Jacobi rotations: A is destroyed, its
-// diagonal ends up holding the eigenvalues, the columns of V the eigenvectors.
-__device__ void jacobi6(double (&A)[6][6], double (&V)[6][6]) {
+// diagonal ends up holding the eigenvalues, the columns of V the eigenvectors. Kept out of line:
+// inlined into k_refine (nvcc 12.9, sm_100a) the rotations stopped being similarity transforms
+// (the trace was not preserved), while the out-of-line copy and the same code on the host agree.
+__device__ __noinline__ void jacobi6(double (&A)[6][6], double (&V)[6][6]) {
     for (int i = 0; i < 6; ++i)
         for (int j = 0; j < 6; ++j) V[i][j] = i == j ? 1.0 : 0.0;
     for (int sweep = 0; sweep < 30; ++sweep) {
