@@ -79,6 +79,10 @@ SIGNATURES = {
                                    _P, _P, _P, _P, _S, _P]),
     "spx_render_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_render_model": (_I, [_P, _P, _I, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_render_overflow": (_I, [_P, _I, _I, _I, POINTER(c_int), _I, _P]),
+    "spx_quantiles": (_I, [_P, _I, _P, _P]),
+    "spx_cell_stats": (_I, [_P, _P, _I, _P, _P, _P]),
+    "spx_background_at": (_I, [_BG, _I, _I, _P, _I, _D, _P, _P]),
     "spx_clean_cells": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _BG, _P, _P, _I, _I, _I, _P, _P]),
     "spx_tile_medians": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _D, _D, _I, _P, _P, _P]),
     "spx_background_rows": (_I, [_P, _I, _I, _I, _I, _P, _P]),
@@ -92,6 +96,13 @@ SIGNATURES = {
     "spx_radial_workspace_bytes": (_S, [_I, _I]),
     "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _MO, _MO, _P, _S, _P]),
 }
+
+class QuantileReq(ctypes.Structure):
+    """The request struct of spx_quantiles."""
+
+    _fields_ = [("values", c_void_p), ("stride", c_int), ("mask", c_void_p), ("finite_only", c_int), ("n", c_int),
+                ("mode", c_int), ("q", c_double)]
+
 
 BG_MAP, BG_FIXED = 0, 1
 TILE_FREE, TILE_USABLE, TILE_ALL = 0, 1, 2

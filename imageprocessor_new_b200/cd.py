@@ -427,7 +427,8 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         else:
             found[name] = _empty_result(name, n_angles, metrics_only)
     seconds["gaussian"], start = time.perf_counter() - start, time.perf_counter()
-    local_background = sign * state.background.at_points(c.seeds[report]) if nr else np.zeros(0)
+    local_background = (state.background.at_points(c.seeds_d[dev.upload(report.astype(np.int64))], sign)
+                        if nr else np.zeros(0))
     measurements = {}
     for name in methods:
         found[name].metrics["background"][:] = local_background

@@ -214,6 +214,23 @@ __device__ __forceinline__ bool inside_bilinear(const CellView& c, bool eroded, 
     return v >= 1.0 - 1e-8;
 }
 
+// The same test on a byte mask staged in shared memory (hm x wm).
+__device__ __forceinline__ bool inside_bytes(const uint8_t* m, int hm, int wm, double y, double x) {
+    if (!(y >= 0.0 && y <= (double)(hm - 1) && x >= 0.0 && x <= (double)(wm - 1))) return false;
+    const double fy = floor(y), fx = floor(x);
+    const int y0 = (int)fy, x0 = (int)fx;
+    const int ny = (y == fy) ? 1 : 2, nx = (x == fx) ? 1 : 2;
+    double v = 0.0;
+    for (int a = 0; a < ny; ++a) {
+        const double wy = a == 0 ? (fy + 1.0) - y : y - fy;
+        for (int b = 0; b < nx; ++b) {
+            const double wx = b == 0 ? (fx + 1.0) - x : x - fx;
+            v += (m[(y0 + a) * wm + x0 + b] ? 1.0 : 0.0) * (wy * wx);
+        }
+    }
+    return v >= 1.0 - 1e-8;
+}
+
 // ---------------------------------------------------------------------- gaussian method
 
 // gaussian_method: params ROI-local; status in/out (non_gaussian_fit for eig0 <= 1e-10).
@@ -570,8 +587,10 @@ __global__ void k_radial_cd(const double* cleaned, const int* vor, const int4* b
     extern __shared__ double sm[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     const int hp = hm + 2 * kPad, wp = wm + 2 * kPad;
-    double* coef = coef_scratch ? coef_scratch + (long long)(blockIdx.x * warps + warp) * hp * wp
-                                : sm + (long long)warp * hp * wp;
+    const long long per = (long long)hp * wp + (hm * wm + 7) / 8;  // doubles per warp: coefficients + mask bytes
+    double* coef = coef_scratch ? coef_scratch + (long long)(blockIdx.x * warps + warp) * per
+                                : sm + (long long)warp * per;
+    uint8_t* emask = reinterpret_cast<uint8_t*>(coef + (long long)hp * wp);
     const double thr = fmax(0.35, 2.0 * radial_step);
     const int nv = n_angles + 1;
     for (int i = blockIdx.x * warps + warp; i < n; i += gridDim.x * warps) {
@@ -625,6 +644,12 @@ __global__ void k_radial_cd(const double* cleaned, const int* vor, const int4* b
             const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
             coef[k] = c.mask(yy, xx) ? c.roi[yy * wm + xx] : 0.0;
         }
+        // Eroded cell (cross structure, zero outside the stack): where ray samples stay valid.
+        for (int k = lane; k < hm * wm; k += 32) {
+            const int yy = k / wm, xx = k % wm;
+            emask[k] = c.mask(yy, xx) && yy > 0 && xx > 0 && yy < hm - 1 && xx < wm - 1 && c.mask(yy - 1, xx) &&
+                       c.mask(yy + 1, xx) && c.mask(yy, xx - 1) && c.mask(yy, xx + 1);
+        }
         __syncwarp();
         for (int col = lane; col < wp; col += 32) spline_line(coef + col, hp, wp);
         __syncwarp();
@@ -646,7 +671,7 @@ __global__ void k_radial_cd(const double* cleaned, const int* vor, const int4* b
                 for (int k = 0; k < n_radii; ++k) {
                     const double r = (double)k * radial_step;
                     const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
-                    if (!inside_bilinear(c, true, y, x)) { first_invalid = k; break; }
+                    if (!inside_bytes(emask, hm, wm, y, x)) { first_invalid = k; break; }
                     const double p = k == 0 ? peak : cubic_at(coef, hp, wp, y + kPad, x + kPad);
                     if (k >= 1 && !crossed && h1 >= half && p < half) {
                         edge_h = (double)(k - 1) * radial_step + ((h1 - half) / (h1 - p)) * radial_step;
@@ -794,7 +819,7 @@ int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, 
 }
 
 size_t spx_radial_workspace_bytes(int hm, int wm) {
-    const size_t per = (size_t)(hm + 2 * kPad) * (wm + 2 * kPad) * sizeof(double);
+    const size_t per = ((size_t)(hm + 2 * kPad) * (wm + 2 * kPad) + (hm * wm + 7) / 8) * sizeof(double);
     return 4 * per <= 200 * 1024 ? 256 : (size_t)148 * 8 * 4 * per + 256;
 }
 
@@ -812,7 +837,7 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
     // radii = np.arange(0, hypot(hm, wm) + step, step)
     const double stop = hypot((double)hm, (double)wm) + radial_step;
     const int n_radii = (int)ceil(stop / radial_step);
-    const size_t per = (size_t)(hm + 2 * kPad) * (wm + 2 * kPad) * sizeof(double);
+    const size_t per = ((size_t)(hm + 2 * kPad) * (wm + 2 * kPad) + (hm * wm + 7) / 8) * sizeof(double);
     const int warps = 4;
     size_t smem = warps * per;
     double* scratch = nullptr;

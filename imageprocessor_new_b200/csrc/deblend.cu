@@ -599,6 +599,132 @@ __global__ void k_residual(Image img, spx_bgmap bg, const double* model, double*
     }
 }
 
+// ------------------------------------------------------------------------ order statistics
+
+// Selected values of one request: values[i * stride] where the selection holds (mask[i] != 0 when
+// mask is given; finite values only when finite_only).
+struct QuantileReq {
+    const double* values;
+    int stride;
+    const uint8_t* mask;
+    int finite_only;
+    int n;
+    int mode;     // 0: np.median; 1: np.percentile(q) with linear interpolation
+    double q;
+};
+
+__device__ __forceinline__ bool q_select(const QuantileReq& r, int i, double* v) {
+    if (r.mask && !r.mask[i]) return false;
+    const double x = r.values[(long long)i * r.stride];
+    if (r.finite_only && !isfinite(x)) return false;
+    *v = x;
+    return true;
+}
+
+// k-th smallest selected value (0-based) by an 8-pass radix select over the global array.
+__device__ double block_kth(const QuantileReq& r, int k, int* hist, int* s_digit, int* s_k) {
+    unsigned long long prefix = 0, mask = 0;
+    if (threadIdx.x == 0) *s_k = k;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < r.n; i += blockDim.x) {
+            double v;
+            if (!q_select(r, i, &v)) continue;
+            const unsigned long long key = order_key(v);
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int kk = *s_k, d = 0;
+            for (; d < 255; ++d) {
+                if (kk < hist[d]) break;
+                kk -= hist[d];
+            }
+            *s_digit = d;
+            *s_k = kk;
+        }
+        __syncthreads();
+        prefix |= (unsigned long long)(*s_digit) << shift;
+        mask |= 0xffull << shift;
+        __syncthreads();
+    }
+    return key_value(prefix);
+}
+
+// One block per request: out[2 * b] = result (NaN when nothing is selected), out[2 * b + 1] = count.
+__global__ void __launch_bounds__(1024) k_quantiles(const QuantileReq* reqs, double* out) {
+    __shared__ int hist[256];
+    __shared__ int s_digit, s_k, s_count;
+    const QuantileReq r = reqs[blockIdx.x];
+    __shared__ int s_nan;
+    if (threadIdx.x == 0) s_count = s_nan = 0;
+    __syncthreads();
+    int c = 0, nan = 0;
+    for (int i = threadIdx.x; i < r.n; i += blockDim.x) {
+        double v;
+        if (q_select(r, i, &v)) {
+            ++c;
+            nan += isnan(v);
+        }
+    }
+    atomicAdd(&s_count, c);
+    atomicAdd(&s_nan, nan);
+    __syncthreads();
+    const int n = s_count;
+    double res = dnan();
+    if (n > 0 && s_nan == 0) {  // numpy: a NaN among the values makes the median / percentile NaN
+        if (r.mode == 0) {
+            const double a = block_kth(r, (n - 1) / 2, hist, &s_digit, &s_k);
+            const double b = (n & 1) ? a : block_kth(r, n / 2, hist, &s_digit, &s_k);
+            res = __ddiv_rn(__dadd_rn(a, b), 2.0);
+        } else {
+            // numpy 'linear': virtual index (n - 1) q, _lerp of the neighbours.
+            const double virt = __dmul_rn((double)(n - 1), r.q);
+            const double below = floor(virt);
+            const int lo = min(max((int)below, 0), n - 1), hi = min(lo + 1, n - 1);
+            const double a = block_kth(r, lo, hist, &s_digit, &s_k);
+            const double b = hi == lo ? a : block_kth(r, hi, hist, &s_digit, &s_k);
+            if (virt >= (double)(n - 1)) {
+                res = b;
+            } else {
+                const double g = __dsub_rn(virt, below), diff = __dsub_rn(b, a);
+                res = g >= 0.5 ? __dsub_rn(b, __dmul_rn(diff, __dsub_rn(1.0, g))) : __dadd_rn(a, __dmul_rn(diff, g));
+            }
+        }
+    }
+    if (threadIdx.x == 0) {
+        out[2 * blockIdx.x] = res;
+        out[2 * blockIdx.x + 1] = (double)n;
+    }
+}
+
+// Per-cell amplitude, 2 sqrt(2 ln 2) sigma_major and the "good" flag (status ok and A > 0).
+__global__ void k_cell_stats(const double* params, const uint8_t* status, int n, double* fwhm, uint8_t* good) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const double* p = params + 6LL * j;
+        good[j] = status[j] == SPX_ST_OK && p[0] > 0.0;
+        fwhm[j] = 2.0 * 1.1774100225154747 * sigma_major(p);
+    }
+}
+
+// map_coordinates(background map, [y, x], order=1, mode="nearest") at points [x, y].
+__global__ void k_background_at(spx_bgmap bg, int H, int W, const double* pts, int n, double sign, double* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double x = pts[2 * i], y = pts[2 * i + 1];
+        const double fy = floor(y), fx = floor(x);
+        const double ty = y - fy, tx = x - fx;
+        const int y0 = min(max((int)fy, 0), H - 1), y1 = min(max((int)fy + 1, 0), H - 1);
+        const int x0 = min(max((int)fx, 0), W - 1), x1 = min(max((int)fx + 1, 0), W - 1);
+        double acc = 0.0;
+        acc += bg_at(bg, y0, x0) * (1.0 - ty) * (1.0 - tx);
+        acc += bg_at(bg, y0, x1) * (1.0 - ty) * tx;
+        acc += bg_at(bg, y1, x0) * ty * (1.0 - tx);
+        acc += bg_at(bg, y1, x1) * ty * tx;
+        out[i] = sign * acc;
+    }
+}
+
 struct FitLayout {
     int* queue;
     double* gbuf_v;
@@ -749,6 +875,19 @@ int spx_deblend_iteration(const void* img, int dtype, double sign, int height, i
     });
 }
 
+int spx_render_overflow(void* workspace, int n, int height, int width, int* flag_out, int reset, void* stream) {
+    SPX_REQUIRE(workspace && flag_out, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    RenderLayout L = render_layout(workspace, n, height, width, nullptr);
+    if (reset) {
+        SPX_CUDA(cudaMemsetAsync(L.overflow, 0, sizeof(int), s));
+        return SPX_OK;
+    }
+    SPX_CUDA(cudaMemcpyAsync(flag_out, L.overflow, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SPX_CUDA(cudaStreamSynchronize(s));
+    return SPX_OK;
+}
+
 size_t spx_render_workspace_bytes(int n, int height, int width) {
     size_t b = 0;
     render_layout(nullptr, n, height, width, &b);
@@ -763,7 +902,6 @@ int spx_render_model(const double* params, const int* boxes, int n, int height, 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     RenderLayout L = render_layout(workspace, n, height, width, nullptr);
     SPX_CUDA(cudaMemsetAsync(L.rmax, 0, sizeof(int), s));
-    SPX_CUDA(cudaMemsetAsync(L.overflow, 0, sizeof(int), s));
     if (n > 0) {
         SPX_REQUIRE(params && boxes, "null pointer");
         k_render_prep<<<grid_for(n, 256), 256, 0, s>>>(params, reinterpret_cast<const int4*>(boxes), n, radius_cap,
@@ -774,15 +912,7 @@ int spx_render_model(const double* params, const int* boxes, int n, int height, 
     const dim3 grid((width + kRenderTile - 1) / kRenderTile, (height + kRenderTile - 1) / kRenderTile);
     k_render<<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
                                   L.overflow);
-    if (int e = check_launch("k_render")) return e;
-    int overflow = 0;
-    SPX_CUDA(cudaMemcpyAsync(&overflow, L.overflow, sizeof(int), cudaMemcpyDeviceToHost, s));
-    SPX_CUDA(cudaStreamSynchronize(s));
-    if (overflow) {
-        set_error("render: more than %d truncated Gaussians reach one 16x16 tile", kRenderCap);
-        return SPX_ERR_CAPACITY;
-    }
-    return SPX_OK;
+    return check_launch("k_render");
 }
 
 int spx_clean_cells(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
@@ -823,6 +953,33 @@ int spx_background_rows(const double* medians, int ny, int nx, int tile, int wid
     const long long total = (long long)ny * width;
     k_bg_rows<<<grid_for(total, 256), 256, 0, s>>>(medians, ny, nx, tile, width, rows);
     return check_launch("k_bg_rows");
+}
+
+int spx_quantiles(const void* requests, int n_requests, double* out, void* stream) {
+    SPX_REQUIRE(n_requests >= 1 && n_requests <= 64, "between 1 and 64 requests");
+    SPX_REQUIRE(requests && out, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_quantiles<<<n_requests, 1024, 0, s>>>(static_cast<const QuantileReq*>(requests), out);
+    return check_launch("k_quantiles");
+}
+
+int spx_cell_stats(const double* params, const uint8_t* status, int n, double* fwhm, uint8_t* good, void* stream) {
+    SPX_REQUIRE(n >= 0, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(params && status && fwhm && good, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_cell_stats<<<grid_for(n, 256), 256, 0, s>>>(params, status, n, fwhm, good);
+    return check_launch("k_cell_stats");
+}
+
+int spx_background_at(const spx_bgmap* background, int height, int width, const double* points, int n,
+                      double sign, double* out, void* stream) {
+    SPX_REQUIRE(n >= 0 && height > 0 && width > 0, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(background && points && out, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_background_at<<<grid_for(n, 256), 256, 0, s>>>(*background, height, width, points, n, sign, out);
+    return check_launch("k_background_at");
 }
 
 int spx_residual(const void* img, int dtype, double sign, int height, int width, const spx_bgmap* background,

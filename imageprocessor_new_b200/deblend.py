@@ -12,6 +12,7 @@ subpx/_cpu/deblend.py:346-393 does — on the host, with SciPy, as the reference
 
 from __future__ import annotations
 
+import ctypes
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -85,6 +86,15 @@ def auto_tile(seeds_d: torch.Tensor, n: int, shape) -> tuple[int, float]:
               ws.data_ptr(), ws.numel(), dev.stream_ptr())
     pitch = float(np.median(out.cpu().numpy()))
     return int(np.clip(round(4 * pitch), 16, max(shape))), pitch
+
+
+def quantiles(reqs) -> np.ndarray:
+    """Run spx_quantiles on a list of _lib.QuantileReq; (len, 2) array of (value, count)."""
+    arr = (_lib.QuantileReq * len(reqs))(*reqs)
+    raw = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to("cuda")
+    out = dev.empty((len(reqs), 2), torch.float64)
+    _lib.call("spx_quantiles", raw.data_ptr(), len(reqs), out.data_ptr(), dev.stream_ptr())
+    return out.cpu().numpy()
 
 
 def sigma_major(params: np.ndarray) -> np.ndarray:
@@ -192,40 +202,15 @@ class Background:
                   dev.stream_ptr())
         return -out.cpu().numpy()
 
-    def at_points(self, xy: np.ndarray) -> np.ndarray:
-        """map_coordinates(map, [y, x], order=1, mode="nearest") at points (N, 2) [x, y], from the
-        tile medians (the same interpolation as the device map)."""
-        xy = np.asarray(xy, dtype=np.float64).reshape(-1, 2)
-        if len(xy) == 0:
+    def at_points(self, xy_d: torch.Tensor, sign: float = 1.0) -> np.ndarray:
+        """sign * map_coordinates(map, [y, x], order=1, mode="nearest") at device points (N, 2) [x, y]."""
+        n = int(xy_d.shape[0])
+        if n == 0:
             return np.zeros(0)
-        if self.fixed is not None:
-            return np.full(len(xy), self.fixed)
-        h, w = self.shape
-        _, xc = tile_centers(self.tile, self.shape)
-        yc, _ = tile_centers(self.tile, self.shape)
-
-        def value(iy, ix):
-            rows = np.stack([np.interp(ix.astype(float), xc, self.medians[j]) for j in range(self.ny)])
-            if self.ny == 1:
-                return rows[0]
-            y = iy.astype(float)
-            j1 = np.clip(np.searchsorted(yc, y), 1, self.ny - 1)
-            t = np.clip((y - yc[j1 - 1]) / (yc[j1] - yc[j1 - 1]), 0, 1)
-            k = np.arange(len(ix))
-            return (1 - t) * rows[j1 - 1, k] + t * rows[j1, k]
-
-        y, x = xy[:, 1], xy[:, 0]
-        y0, x0 = np.floor(y), np.floor(x)
-        ty, tx = y - y0, x - x0
-        iy0 = np.clip(y0.astype(np.int64), 0, h - 1)
-        iy1 = np.clip(y0.astype(np.int64) + 1, 0, h - 1)
-        ix0 = np.clip(x0.astype(np.int64), 0, w - 1)
-        ix1 = np.clip(x0.astype(np.int64) + 1, 0, w - 1)
-        out = np.zeros(len(xy))
-        for iy, wy in ((iy0, 1 - ty), (iy1, ty)):
-            for ix, wx in ((ix0, 1 - tx), (ix1, tx)):
-                out += (value(iy, ix) * wy) * wx
-        return out
+        out = dev.empty((n,), torch.float64)
+        _lib.call("spx_background_at", self.struct(), self.shape[0], self.shape[1],
+                  xy_d.contiguous().data_ptr(), n, float(sign), out.data_ptr(), dev.stream_ptr())
+        return out.cpu().numpy()
 
 
 @dataclass
@@ -277,6 +262,9 @@ class Deblender:
         self.fit_ws = dev.workspace(_lib.size("spx_fit_workspace_bytes", cells.max_px))
         self.render_ws = dev.workspace(_lib.size("spx_render_workspace_bytes", self.n, h, w))
         if self.n:
+            _lib.call("spx_render_overflow", self.render_ws.data_ptr(), self.n, h, w, ctypes.byref(ctypes.c_int(0)), 1,
+                      dev.stream_ptr())
+        if self.n:
             self.dist2 = dev.empty((h, w), torch.int32)
             ws = dev.workspace(_lib.size("spx_voronoi_workspace_bytes", self.n, h, w))
             _lib.call("spx_seed_distance_map", cells.seeds_d.data_ptr(), self.n, h, w, self.dist2.data_ptr(),
@@ -307,13 +295,34 @@ class Deblender:
                   med.data_ptr(), cnt.data_ptr(), dev.stream_ptr())
         return med.cpu().numpy().reshape(ny, nx), cnt.cpu().numpy().reshape(ny, nx)
 
-    def background_of(self, model, params, status_codes):
-        """Background map and info (subpx/_cpu/deblend.py:459-466 background_of, 323-393)."""
+    def stats(self, params_d, status_d, maxstep_d=None):
+        """Median amplitude and FWHM of the good cells (subpx/_cpu/deblend.py:463-464) and, given the
+        steps, the 99th percentile of the finite ones (:517), computed on the device; one download.
+        Returns (amplitude, fwhm, p99, n_finite)."""
+        n = self.n
+        if n == 0:
+            return 1.0, 0.0, np.nan, 0
+        fwhm = dev.empty((n,), torch.float64)
+        good = dev.empty((n,), torch.uint8)
+        _lib.call("spx_cell_stats", params_d.data_ptr(), status_d.data_ptr(), n, fwhm.data_ptr(), good.data_ptr(),
+                  dev.stream_ptr())
+        reqs = [_lib.QuantileReq(params_d.data_ptr(), 6, good.data_ptr(), 0, n, 0, 0.0),
+                _lib.QuantileReq(fwhm.data_ptr(), 1, good.data_ptr(), 0, n, 0, 0.0)]
+        if maxstep_d is not None:
+            reqs.append(_lib.QuantileReq(maxstep_d.data_ptr(), 1, None, 1, n, 1, 99 / 100))
+        res = quantiles(reqs)
+        amplitude = float(res[0, 0]) if res[0, 1] > 0 else 1.0
+        width = float(res[1, 0]) if res[1, 1] > 0 else 0.0
+        if maxstep_d is None:
+            return amplitude, width, np.nan, 0
+        return amplitude, width, float(res[2, 0]), int(res[2, 1])
+
+    def background_of(self, model, stats):
+        """Background map and info (subpx/_cpu/deblend.py:459-466 background_of, 323-393); stats =
+        (median amplitude, median FWHM) of the good cells."""
         if self.background_level is not None:
             return self.bg.set_fixed(self.background_level), {"source": "fixed"}
-        good = (status_codes == OK) & (params[:, 0] > 0)
-        amplitude = float(np.median(params[good, 0])) if good.any() else 1.0
-        fwhm = float(np.median(2 * FWHM_K * sigma_major(params[good]))) if good.any() else 0.0
+        amplitude, fwhm = stats[0], stats[1]
         tile = self.tile
         free_med, free_count = self._tile_medians(model, _lib.TILE_FREE, self.free_fraction * amplitude,
                                                   self.free_distance_fwhm * fwhm)
@@ -381,7 +390,7 @@ class Deblender:
         """deblend() of subpx/_cpu/deblend.py:421-522."""
         if self.n == 0:
             model = torch.zeros(self.shape, dtype=torch.float64, device="cuda")
-            bg, info = self.background_of(model, np.zeros((0, 6)), np.zeros(0, np.uint8))
+            bg, info = self.background_of(model, (1.0, 0.0))
             return DeblendState(bg, model, np.zeros((0, 6)), dev.empty((0, 6), torch.float64),
                                 np.zeros(0, np.uint8), dev.empty((0,), torch.uint8), self.tile, 0, info, False)
         fit_iters = []
@@ -392,27 +401,35 @@ class Deblender:
             init = np.asarray(init, dtype=np.float64)
             params_d = dev.upload(init)
             status_d = self._status_of(params_d)
-        params = params_d.cpu().numpy()
-        status = status_d.cpu().numpy()
+        stats = self.stats(params_d, status_d)
         model = self.render(params_d)
         used, converged = 0, False
         for used in range(1, int(iterations) + 1):
-            bg, info = self.background_of(model, params, status)
+            bg, info = self.background_of(model, stats)
             params_d, status_d, maxstep_d, it = self.iteration(params_d, model, bg)
             fit_iters.append(it)
             model = self.render(params_d)
-            params = params_d.cpu().numpy()
-            status = status_d.cpu().numpy()
-            maxstep = maxstep_d.cpu().numpy()
-            ok = np.isfinite(maxstep)
-            if not ok.any():
+            stats = self.stats(params_d, status_d, maxstep_d)
+            if stats[3] == 0:
                 break
-            if np.percentile(maxstep[ok], 99) < self.tolerance:
+            if stats[2] < self.tolerance:
                 converged = True
                 break
-        bg, info = self.background_of(model, params, status)
-        return DeblendState(bg, model, params, params_d, status, status_d, self.tile, used, info, converged,
-                            fit_iters)
+        bg, info = self.background_of(model, stats)
+        self.check_render()
+        return DeblendState(bg, model, params_d.cpu().numpy(), params_d, status_d.cpu().numpy(), status_d, self.tile,
+                            used, info, converged, fit_iters)
+
+    def check_render(self):
+        """Raise if a render since the last check overflowed a tile's Gaussian list."""
+        if not self.n:
+            return
+        h, w = self.shape
+        flag = ctypes.c_int(0)
+        _lib.call("spx_render_overflow", self.render_ws.data_ptr(), self.n, h, w, ctypes.byref(flag), 0,
+                  dev.stream_ptr())
+        if flag.value:
+            raise RuntimeError("render: more than 2048 truncated Gaussians reach one 16x16 tile")
 
     def _status_of(self, params_d):
         """fit_status of given params: an iteration pass with relaxation 0 returns the params unchanged

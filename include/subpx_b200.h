@@ -205,9 +205,13 @@ int spx_deblend_iteration(const void* img, int dtype, double sign, int height, i
 
 size_t spx_render_workspace_bytes(int n, int height, int width);
 /* Sum of every cell's truncated Gaussian (radius clip(ceil(4 sigma_major), 2, radius_cap)) into
- * model (H x W double), in increasing cell order per pixel. Synchronises the stream. */
+ * model (H x W double), in increasing cell order per pixel (see spx_render_overflow). */
 int spx_render_model(const double* params, const int* boxes, int n, int height, int width, int radius_cap,
                      double* model, void* workspace, size_t workspace_bytes, void* stream);
+/* Render overflow flag kept in the render workspace (more than 2048 truncated Gaussians reaching
+ * one 16x16 tile leaves that tile unrendered): reset = 1 clears it, reset = 0 copies it to the host
+ * int *flag_out and synchronises the stream. */
+int spx_render_overflow(void* workspace, int n, int height, int width, int* flag_out, int reset, void* stream);
 /* Cleaned cells of `which` (n_out indices; all cells when null) as an (n_out, hm, wm) stack. */
 int spx_clean_cells(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                     const int* boxes, const double* params, int radius_cap, const spx_bgmap* background,
@@ -222,6 +226,18 @@ int spx_tile_medians(const void* img, int dtype, double sign, int height, int wi
                      int tile, double* medians, long long* counts, void* stream);
 /* rows[j][x] = np.interp(x, tile-centre columns, medians[j]) (ny x width). */
 int spx_background_rows(const double* medians, int ny, int nx, int tile, int width, double* rows, void* stream);
+/* Order statistics on the device (np.median / np.percentile 'linear' of a selection), one request
+ * per block: requests is a device array of n_requests structs {const double* values; int stride;
+ * const uint8_t* mask; int finite_only; int n; int mode (0 median, 1 percentile); double q} laid
+ * out as in C; out[2 b] = value (NaN if none selected), out[2 b + 1] = count. Replaces the host
+ * medians and percentile of deblend (subpx/_cpu/deblend.py:463-464, 517). */
+int spx_quantiles(const void* requests, int n_requests, double* out, void* stream);
+/* fwhm[j] = 2 sqrt(2 ln 2) sigma_major(params[j]); good[j] = status ok and A > 0. */
+int spx_cell_stats(const double* params, const uint8_t* status, int n, double* fwhm, uint8_t* good, void* stream);
+/* sign * map_coordinates(background, [y, x], order=1, mode="nearest") at n points [x, y]
+ * (the per-hole "background" metric, subpx/cd.py:719-721). */
+int spx_background_at(const spx_bgmap* background, int height, int width, const double* points, int n,
+                      double sign, double* out, void* stream);
 /* out = sign*img - background - model (H x W double). */
 int spx_residual(const void* img, int dtype, double sign, int height, int width, const spx_bgmap* background,
                  const double* model, double* out, void* stream);
