@@ -41,6 +41,9 @@ METHODS = ("gaussian", "gradient", "halfmax")
 REFINERS = ("weighted", "logquad", "edge_gradmoment")
 CD_KW = dict(area_max=400, summary_only=True)
 CENTER_KW = dict(threshold="otsu", area_max=400)
+# DRAM bytes (read + write) per cell of one k_fit_iteration launch, from an ncu capture of one
+# launch on the 4096x4096 page (29,241 cells, 195.0 MB); traffic scales with the cells processed.
+FIT_TRAFFIC_PER_CELL = 6668.0
 
 
 def _dist():
@@ -58,12 +61,21 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms; started before the warm-up (its
+    start-up takes driver locks that would stall the timed steps) and summarised over the samples
+    taken between mark_start() and mark_end()."""
 
     def __init__(self, index: int):
         self.index = index
         self.samples = []
         self.proc = None
+        self.window = (None, None)
+
+    def mark_start(self):
+        self.window = (time.monotonic(), None)
+
+    def mark_end(self):
+        self.window = (self.window[0], time.monotonic())
 
     def __enter__(self):
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -83,7 +95,7 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.samples.append(parts)
+                self.samples.append((time.monotonic(), parts))
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -94,20 +106,22 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.samples:
+        t0, t1 = self.window
+        inside = [p for t, p in self.samples if (t0 is None or t >= t0) and (t1 is None or t <= t1)]
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        sm = [float(s[1]) for s in inside if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in inside if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[5 + k].lower() == "active"})
+        reasons = sorted({names[k] for s in inside for k in range(4) if s[5 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(inside)}
 
 
-def make_page(rank: int):
+def make_page(rank: int, size: int = 8192):
     from imageprocessor_new_b200 import synthetic
 
-    return synthetic.page_staggered(seed=rank).image
+    return synthetic.page_staggered(seed=rank, shape=(size, size)).image
 
 
 def gpu_arm(args):
@@ -120,7 +134,7 @@ def gpu_arm(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
-    page = make_page(rank)
+    page = make_page(rank, args.page)
     page_d = torch.from_numpy(page).cuda()
     lib = _lib.lib()
 
@@ -170,10 +184,12 @@ def gpu_arm(args):
             dist.barrier()
         return ms, cells, launches
 
-    for _ in range(args.warmup):
-        step(page_d)
     with ClockSampler(local) as clocks:
+        for _ in range(args.warmup):
+            step(page_d)
+        clocks.mark_start()
         ms, cells, launches = run(page_d, args.steps)
+        clocks.mark_end()
     fit_ms = [a.elapsed_time(b) for a, b in fit_times]
     fit_avg_ms = float(np.mean(fit_ms)) if fit_ms else float("nan")
     fit_n = float(np.mean(fit_cells)) if fit_cells else 0.0
@@ -188,6 +204,7 @@ def gpu_arm(args):
     value = world * per_step_cells / (ms / 1e3 / args.steps)
     e2e = world * (cells_e2e / args.steps) / (ms_e2e / 1e3 / args.steps)
     peaks, which = _peaks()
+    d2h = _d2h_bytes(int(per_step_cells))
     # Roofline of the dominant kernel (the LM deblending iteration, FP64, compute-bound): its
     # algorithmic HBM bytes per launch are the cells' pixels read (image 2 B + labels 4 B + model 8 B
     # + background rows 8 B) plus 6 params in / 6 out + status; its FP64 rate is reported beside.
@@ -198,21 +215,39 @@ def gpu_arm(args):
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded render + noise)",
-        "config": {"workload": WORKLOAD, "image": "8192x8192 uint16", "cells_per_step": per_step_cells,
+        "config": {"workload": _workload(args.page), "image": f"{args.page}x{args.page} uint16",
+                   "cells_per_step": per_step_cells,
                    "methods": list(METHODS), "refiners": list(REFINERS), "l2": "inputs larger than L2 (134 MB page)",
                    "warm_start": "plain LM (no network)"},
         "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(page.nbytes) * (len(REFINERS) + 1),
-                "d2h_bytes_per_step": int(per_step_cells * 8 * 13 * len(METHODS))},
+                "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "kernel": "k_fit_iteration", "achieved": None if achieved is None else round(achieved, 1),
                      "peak": peaks.get("hbm_gbs"), "peak_source": which, "unit": "GB/s",
                      "frac": None if achieved is None else round(achieved / peaks["hbm_gbs"], 4),
-                     "traffic": None, "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n},
+                     "traffic": round(FIT_TRAFFIC_PER_CELL * fit_n / 1e9, 4), "traffic_unit": "GB per launch",
+                     "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
     if args.cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(page, args.cpu_sample)
     print(json.dumps(line), flush=True)
+
+
+def _workload(size: int) -> str:
+    return WORKLOAD if size == 8192 else WORKLOAD.replace("8192x8192", f"{size}x{size}")
+
+
+def _d2h_bytes(cells: int) -> int:
+    """Result bytes copied to the host per step: each CD method's output buffer (one copy per method)
+    and the three refiners' centre arrays."""
+    from imageprocessor_new_b200 import cd
+
+    total = 0
+    for method in METHODS:
+        b, _ = cd._method_buffers(cells, 128, method, False)
+        total += b["_flat"].numel() * 8
+    return total + len(REFINERS) * cells * 16
 
 
 def cpu_baseline(page, size):
@@ -258,10 +293,11 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gpu", choices=("gpu", "reference"))
     ap.add_argument("--cpu-sample", type=int, default=768)
+    ap.add_argument("--page", type=int, default=8192, help="page side in pixels (8192 = the benchmark page)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     args = ap.parse_args()
     if args.impl == "reference":

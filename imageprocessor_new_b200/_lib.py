@@ -58,6 +58,8 @@ SIGNATURES = {
     "spx_otsu_static": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "spx_triangle": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
+    "spx_binarize": (_I, [_P, _I, _I, _I, _P, _D, _I, _P, _P]),
+    "spx_morphology": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "spx_ccl_label": (_I, [_P, _I, _I, _I, _P, _D, _I, _I, _P, _P, _P, _S, _P]),
     "spx_ccl_finish": (_I, [_P, _I, _I, _I, _I, _P, _P, _P, _S, _P]),
     "spx_select_workspace_bytes": (_S, [_I]),

@@ -192,41 +192,70 @@ def _segment(img_d: torch.Tensor, threshold: str, invert: bool):
 
 
 def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
+    """Every output of one method carved from ONE device buffer (256-byte aligned regions), so the
+    result comes back in a single copy."""
     names = _metric_names(method)
-    b = {
-        "centers": dev.empty((max(n, 1), 2), torch.float64),
-        "contours": dev.empty((max(n, 1), n_angles + 1, 2), torch.float64) if contours else None,
-        "status": dev.empty((max(n, 1),), torch.uint8),
-        "metrics": dev.empty((max(n, 1), max(len(names), 13)), torch.float64),
-        "center_local": dev.empty((max(n, 1), 2), torch.float64),
-        "edge_px": dev.empty((max(n, 1), n_angles), torch.float64) if method in ("gradient", "halfmax") else None,
-        "eigenvalues": dev.empty((max(n, 1), 2), torch.float64) if method in ("logquad", "gaussian") else None,
-        "axes": dev.empty((max(n, 1), 2, 2), torch.float64) if method in ("logquad", "gaussian") else None,
+    m = max(n, 1)
+    shapes = {
+        "centers": (m, 2),
+        "contours": (m, n_angles + 1, 2) if contours else None,
+        "metrics": (m, max(len(names), 13)),
+        "center_local": (m, 2),
+        "edge_px": (m, n_angles) if method in ("gradient", "halfmax") else None,
+        "eigenvalues": (m, 2) if method in ("logquad", "gaussian") else None,
+        "axes": (m, 2, 2) if method in ("logquad", "gaussian") else None,
+        "status": ((m + 7) // 8,),  # bytes, viewed as uint8
     }
+    offsets, total = {}, 0
+    for key, shape in shapes.items():
+        if shape is not None:
+            offsets[key] = total
+            total += -(-int(np.prod(shape)) // 32) * 32
+    flat = dev.empty((total,), torch.float64)
+    b = {"_flat": flat, "_layout": (shapes, offsets)}
+    for key, shape in shapes.items():
+        b[key] = None if shape is None else flat[offsets[key]:offsets[key] + int(np.prod(shape))].view(shape)
+    b["status"] = b["status"].view(torch.uint8)[:m]
     struct = _lib.MethodOut(*(None if b[k] is None else b[k].data_ptr() for k in
                               ("centers", "contours", "status", "metrics", "center_local", "edge_px", "eigenvalues",
                                "axes")), b["metrics"].shape[1])
     return b, struct
 
 
-def _to_result(method: str, n: int, b: dict, metrics_only: bool, n_angles: int) -> CDMethodResult:
+def _download(bufs: dict) -> dict:
+    """Copy every method's buffer into pinned host memory with one copy each and one synchronise."""
+    host = {}
+    for name, b in bufs.items():
+        h = torch.empty(b["_flat"].shape, dtype=torch.float64, pin_memory=True)
+        h.copy_(b["_flat"], non_blocking=True)
+        host[name] = h
+    torch.cuda.current_stream().synchronize()
+    return {name: h.numpy() for name, h in host.items()}
+
+
+def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: bool, n_angles: int) -> CDMethodResult:
     names = _metric_names(method)
-    m = b["metrics"][:n].cpu().numpy()
-    status = STATUS[b["status"][:n].cpu().numpy()]
+    shapes, offsets = b["_layout"]
+
+    def part(key):
+        shape = shapes[key]
+        return host[offsets[key]:offsets[key] + int(np.prod(shape))].reshape(shape)[:n]
+
+    m = part("metrics")
+    status = STATUS[host[offsets["status"]:].view(np.uint8)[:n]]
     metrics = {name: np.ascontiguousarray(m[:, k]) for k, name in enumerate(names)}
-    if b["contours"] is not None:
-        contours = b["contours"][:n].cpu().numpy()
+    if shapes["contours"] is not None:
+        contours = part("contours")
     else:
         contours = np.empty((n, 0 if metrics_only else n_angles + 1, 2))
     geometry = {}
     if method == "logquad":
-        geometry = {"center_local": b["center_local"][:n].cpu().numpy(),
-                    "eigenvalues": b["eigenvalues"][:n].cpu().numpy(), "axes": b["axes"][:n].cpu().numpy()}
+        geometry = {"center_local": part("center_local"), "eigenvalues": part("eigenvalues"), "axes": part("axes")}
     elif method in ("gradient", "halfmax"):
-        geometry = {"center_local": b["center_local"][:n].cpu().numpy(), "edge_px": b["edge_px"][:n].cpu().numpy()}
+        geometry = {"center_local": part("center_local"), "edge_px": part("edge_px")}
     elif not metrics_only:
-        geometry = {"eigenvalues": b["eigenvalues"][:n].cpu().numpy(), "axes": b["axes"][:n].cpu().numpy()}
-    return CDMethodResult(method=method, centers_xy=b["centers"][:n].cpu().numpy(), contours_xy=contours,
+        geometry = {"eigenvalues": part("eigenvalues"), "axes": part("axes")}
+    return CDMethodResult(method=method, centers_xy=part("centers"), contours_xy=contours,
                           valid=status == "ok", status=status, metrics=metrics, geometry=geometry)
 
 
@@ -421,9 +450,10 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
                   c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(), nr, c.hm, c.wm, width, n_angles,
                   gb2[1], stream)
         bufs["gaussian"] = gb2[0]
+    host = _download(bufs) if nr else {}
     for name in methods:
         if nr:
-            found[name] = _to_result(name, nr, bufs[name], metrics_only, n_angles)
+            found[name] = _to_result(name, nr, bufs[name], host[name], metrics_only, n_angles)
         else:
             found[name] = _empty_result(name, n_angles, metrics_only)
     seconds["gaussian"], start = time.perf_counter() - start, time.perf_counter()
@@ -433,7 +463,9 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
     for name in methods:
         found[name].metrics["background"][:] = local_background
         measurements[name] = found[name]
-    statuses, counts = np.unique(state.status[report], return_counts=True)
+    code_counts = np.bincount(state.status_codes[report], minlength=len(STATUS))
+    present = sorted((str(STATUS[code]), int(cnt)) for code, cnt in enumerate(code_counts) if cnt)
+    statuses, counts = np.array([name for name, _ in present]), np.array([cnt for _, cnt in present])
     info = state.background_info
     meta.update(
         background_definition=("Smooth map fitted jointly with one 2-D Gaussian per hole; measured cells have the map "

@@ -58,17 +58,30 @@ def _device_image(img) -> torch.Tensor:
     return dev.upload(img)
 
 
-def _morphology(binary_src: torch.Tensor, threshold, fixed, invert, morph_open, morph_close):
-    if morph_open or morph_close:
-        raise NotImplementedError("morph_open / morph_close are not implemented on the GPU path")
+def _segmentation_source(img_d: torch.Tensor, threshold_dev, fixed_threshold: float, invert: bool, morph_open: int,
+                         morph_close: int):
+    """What segment.label binarises: the image itself, or (with morphology) the 0/255 image after
+    cv2.morphologyEx OPEN / CLOSE with the 3x3 elliptic element (subpx/_cpu/centers.py:257-265)."""
+    if not (morph_open or morph_close):
+        return img_d, threshold_dev, fixed_threshold, invert
+    h, w = img_d.shape
+    bw = dev.empty((h, w), torch.uint8)
+    tmp = dev.empty((h, w), torch.uint8)
+    _lib.call("spx_binarize", img_d.data_ptr(), dev.dtype_code(img_d), h, w, dev.ptr(threshold_dev),
+              float(fixed_threshold), int(bool(invert)), bw.data_ptr(), dev.stream_ptr())
+    _lib.call("spx_morphology", bw.data_ptr(), h, w, int(morph_open), int(morph_close), tmp.data_ptr(),
+              dev.stream_ptr())
+    return bw, None, 0.0, False
 
 
 def _centers_on_device(img_d: torch.Tensor, *, threshold_dev: torch.Tensor | None, fixed_threshold: float,
                        invert: bool, area_min: int, area_max: int, pad: int, refine: str,
-                       connectivity: int, small_feature_max: float) -> torch.Tensor:
+                       connectivity: int, small_feature_max: float, morph_open: int = 0,
+                       morph_close: int = 0) -> torch.Tensor:
     """Refined centres (n, 2) on the device, NaN rows for failed refinements, in label order."""
-    comp = segment.label(img_d, threshold=threshold_dev, fixed_threshold=fixed_threshold, invert=invert,
-                         connectivity=connectivity)
+    src, thr, fixed, inv = _segmentation_source(img_d, threshold_dev, fixed_threshold, invert, morph_open,
+                                                morph_close)
+    comp = segment.label(src, threshold=thr, fixed_threshold=fixed, invert=inv, connectivity=connectivity)
     k = comp.count
     h, w = img_d.shape
     rows = dev.empty((max(k, 1), 5), torch.int32)
@@ -136,20 +149,23 @@ def detect_centers(
         raise NotImplementedError("background='model' centre re-refinement is not part of this package yet")
     if connectivity not in (4, 8):
         raise ValueError("connectivity must be 4 or 8")
+    if int(morph_open) < 0 or int(morph_close) < 0:
+        raise ValueError("morph_open and morph_close must be >= 0")
     img = _as_image(image)
-    _morphology(None, None, None, invert, morph_open, morph_close)
     with dev.on_device(device):
         if tile_h is not None:
             return _detect_tiled(img, threshold=threshold, invert=invert, area_min=area_min, area_max=area_max,
                                  pad=pad, refine=refine, connectivity=connectivity,
                                  small_feature_max=small_feature_max, tile_h=int(tile_h), overlap=int(overlap),
                                  threshold_mode=threshold_mode, otsu_downsample=otsu_downsample,
-                                 thr_scale=thr_scale, dedupe_eps=dedupe_eps, device=device)
+                                 thr_scale=thr_scale, dedupe_eps=dedupe_eps, device=device,
+                                 morph_open=int(morph_open), morph_close=int(morph_close))
         img_d = _device_image(img)
         thr = segment.binarize_threshold(img_d, threshold, invert)
         centers = _centers_on_device(img_d, threshold_dev=thr, fixed_threshold=0.0, invert=invert,
                                      area_min=area_min, area_max=area_max, pad=pad, refine=refine,
-                                     connectivity=connectivity, small_feature_max=small_feature_max)
+                                     connectivity=connectivity, small_feature_max=small_feature_max,
+                                     morph_open=int(morph_open), morph_close=int(morph_close))
         arr = _finite(centers)
     meta = {
         "invert": bool(invert), "area_min": int(area_min), "area_max": int(area_max),
@@ -162,7 +178,8 @@ def detect_centers(
 
 
 def _detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, connectivity, small_feature_max,
-                  tile_h, overlap, threshold_mode, otsu_downsample, thr_scale, dedupe_eps, device) -> CenterResult:
+                  tile_h, overlap, threshold_mode, otsu_downsample, thr_scale, dedupe_eps, device, morph_open=0,
+                  morph_close=0) -> CenterResult:
     """Row bands of ``tile_h`` with an ``overlap`` halo, keep-band rule, dedupe
     (subpx/_gpu/centers.py:1778-1862), with the image resident on the device."""
     from . import tiled
@@ -171,7 +188,8 @@ def _detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, co
                               pad=pad, refine=refine, connectivity=connectivity,
                               small_feature_max=small_feature_max, tile_h=tile_h, overlap=overlap,
                               threshold_mode=threshold_mode, otsu_downsample=otsu_downsample,
-                              thr_scale=thr_scale, dedupe_eps=dedupe_eps, device=device)
+                              thr_scale=thr_scale, dedupe_eps=dedupe_eps, device=device, morph_open=morph_open,
+                              morph_close=morph_close)
 
 
 def detect_centers_tiled(image, *, tile_h=8192, **kwargs) -> CenterResult:

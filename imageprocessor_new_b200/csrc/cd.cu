@@ -11,6 +11,7 @@
 // use Unser's recursive prefilter (pole sqrt(3) - 2) over the cell padded by 12 edge pixels, as
 // scipy.ndimage.map_coordinates(order=3, mode="nearest") does, and scipy's cubic weights.
 
+#include <algorithm>
 #include "common.cuh"
 #include "lm.cuh"
 
@@ -578,90 +579,165 @@ __device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, d
     return out;
 }
 
+constexpr int kRadialThreads = 128;
+
+// Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients, a reduction
+// area, then the cell mask and the eroded mask as bytes.
+__host__ __device__ inline long long radial_cta_doubles(int hm, int wm) {
+    return (long long)(hm + 2 * kPad) * (wm + 2 * kPad) + 32 + (2LL * hm * wm + 7) / 8;
+}
+
+// Sum over the CTA's 4 warps in a fixed order (the same value on every thread). Slots of `red`
+// must not be reused before the next __syncthreads that follows every read.
+__device__ __forceinline__ double cta_sum(double v, double* red) {
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    return ((red[0] + red[1]) + red[2]) + red[3];
+}
+
+__device__ __forceinline__ double cta_max(double v, double* red) {
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    return fmax(fmax(red[0], red[1]), fmax(red[2], red[3]));
+}
+
+// NaN / no_signal defaults of one cell's radial outputs (the CTA's threads share the stores).
+__device__ void radial_clear(const MethodOut out, int i, int n_angles) {
+    if (!out.status) return;
+    const int nv = n_angles + 1;
+    if (threadIdx.x == 0) {
+        double* m = out.metrics + (long long)i * out.n_metrics;
+        for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
+        out.status[i] = SPX_ST_NO_SIGNAL;
+        out.centers[2LL * i] = out.centers[2LL * i + 1] = dnan();
+        out.center_local[2LL * i] = out.center_local[2LL * i + 1] = dnan();
+    }
+    for (int k = threadIdx.x; k < n_angles; k += blockDim.x) out.edge_px[(long long)i * n_angles + k] = dnan();
+    if (out.contours)
+        for (int k = threadIdx.x; k < 2 * nv; k += blockDim.x) out.contours[(long long)i * 2 * nv + k] = dnan();
+}
+
+// Contour, polygon geometry and metrics of one method from its edge radii (one warp).
+__device__ __noinline__ void radial_finish(const MethodOut out, int found, int i, int n_angles, double cx, double cy,
+                                           double peak, int4 box) {
+    if (!out.status) return;
+    const int lane = threadIdx.x & 31, nv = n_angles + 1;
+    const double* edge = out.edge_px + (long long)i * n_angles;
+    const double step = 2.0 * kPi / n_angles;
+    auto vertex = [&](int k, double* x, double* y) {
+        const int a = k % n_angles;
+        const double ang = (double)a * step;
+        *x = cx + edge[a] * cos(ang);
+        *y = cy + edge[a] * sin(ang);
+    };
+    if (out.contours)
+        for (int k = lane; k < nv; k += 32) {
+            double x, y;
+            vertex(k, &x, &y);
+            out.contours[(long long)i * 2 * nv + 2 * k] = x + box.x;
+            out.contours[(long long)i * 2 * nv + 2 * k + 1] = y + box.y;
+        }
+    double area = 0, perim = 0, px = 0, py = 0;
+    if (found == n_angles) polygon_geometry(nv, vertex, lane, &area, &perim, &px, &py);
+    if (lane == 0) {
+        double* m = out.metrics + (long long)i * out.n_metrics;
+        out.center_local[2LL * i] = cx;
+        out.center_local[2LL * i + 1] = cy;
+        out.centers[2LL * i] = cx + box.x;
+        out.centers[2LL * i + 1] = cy + box.y;
+        m[M_BACKGROUND] = 0.0;
+        m[M_PEAK] = peak;
+        m[M_COVERAGE] = (double)found / n_angles;
+        if (found == n_angles) {
+            m[M_AREA] = area;
+            m[M_CD_EQ] = 2.0 * sqrt(area / kPi);
+            m[M_CD_X] = px;
+            m[M_CD_Y] = py;
+            m[M_PERIM] = perim;
+            out.status[i] = SPX_ST_OK;
+        } else {
+            out.status[i] = SPX_ST_INCOMPLETE_RAYS;
+        }
+    }
+}
+
 // Radial profiles of each cell: weighted centroid of the pixels above 0.1 x max, cubic-spline
 // samples every radial_step along n_angles rays until the eroded cell ends, first half-height
 // crossing and the parabolic maximum of the outward decrease (halfmax / gradient methods).
-__global__ void k_radial_cd(const double* cleaned, const int* vor, const int4* boxes, const int* which, int n,
-                            int hm, int wm, int W, int n_angles, double radial_step, int n_radii,
-                            double* coef_scratch, MethodOut half_out, MethodOut grad_out) {
+// One 128-thread CTA per cell: the cell's masks and spline coefficients are staged once in
+// shared memory and each thread walks its own rays.
+__global__ void __launch_bounds__(kRadialThreads, 5) k_radial_cd(
+    const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
+    int n_angles, double radial_step, int n_radii, double* coef_scratch, MethodOut half_out, MethodOut grad_out) {
     extern __shared__ double sm[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-    const int hp = hm + 2 * kPad, wp = wm + 2 * kPad;
-    const long long per = (long long)hp * wp + (hm * wm + 7) / 8;  // doubles per warp: coefficients + mask bytes
-    double* coef = coef_scratch ? coef_scratch + (long long)(blockIdx.x * warps + warp) * per
-                                : sm + (long long)warp * per;
-    uint8_t* emask = reinterpret_cast<uint8_t*>(coef + (long long)hp * wp);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int hp = hm + 2 * kPad, wp = wm + 2 * kPad, area_px = hm * wm;
+    double* coef = coef_scratch ? coef_scratch + (long long)blockIdx.x * radial_cta_doubles(hm, wm) : sm;
+    double* red = coef + (long long)hp * wp;  // 32 doubles: 8 slots of 4
+    uint8_t* mask = reinterpret_cast<uint8_t*>(red + 32);
+    uint8_t* emask = mask + area_px;
     const double thr = fmax(0.35, 2.0 * radial_step);
-    const int nv = n_angles + 1;
-    for (int i = blockIdx.x * warps + warp; i < n; i += gridDim.x * warps) {
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
         const int j = which ? which[i] : i;
-        const CellView c{cleaned + (long long)i * hm * wm, vor, boxes[j], j, W, hm, wm};
-        MethodOut outs[2] = {half_out, grad_out};
-        for (int o = 0; o < 2; ++o) {
-            const MethodOut& out = outs[o];
-            if (!out.status) continue;
-            double* m = out.metrics + (long long)i * out.n_metrics;
-            if (lane == 0) {
-                for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
-                out.status[i] = SPX_ST_NO_SIGNAL;
-                out.centers[2LL * i] = out.centers[2LL * i + 1] = dnan();
-                out.center_local[2LL * i] = out.center_local[2LL * i + 1] = dnan();
-            }
-            for (int k = lane; k < n_angles; k += 32) out.edge_px[(long long)i * n_angles + k] = dnan();
-            if (out.contours)
-                for (int k = lane; k < 2 * nv; k += 32) out.contours[(long long)i * 2 * nv + k] = dnan();
-        }
+        const CellView c{cleaned + (long long)i * area_px, vor, boxes[j], j, W, hm, wm};
+        __syncthreads();  // the previous cell's shared-memory reads are done
+        radial_clear(half_out, i, n_angles);
+        radial_clear(grad_out, i, n_angles);
         int cnt = 0;
         double top = 0.0;  // max of the signal array (zeros outside the mask)
-        for (int k = lane; k < hm * wm; k += 32) {
-            if (c.mask(k / wm, k % wm)) ++cnt;
+        for (int k = tid; k < area_px; k += kRadialThreads) {
+            const bool m = c.mask(k / wm, k % wm);
+            mask[k] = m;
+            cnt += m;
             top = fmax(top, c.roi[k]);
         }
-        cnt = warp_sum_i(cnt);
-        top = warp_max(top);
-        if (cnt < 6) {
-            if (lane == 0)
-                for (int o = 0; o < 2; ++o)
-                    if (outs[o].status) outs[o].status[i] = SPX_ST_INSUFFICIENT_CELL_PIXELS;
+        const int total = (int)cta_sum((double)cnt, red);
+        top = cta_max(top, red + 4);
+        if (total < 6) {
+            if (tid == 0) {
+                if (half_out.status) half_out.status[i] = SPX_ST_INSUFFICIENT_CELL_PIXELS;
+                if (grad_out.status) grad_out.status[i] = SPX_ST_INSUFFICIENT_CELL_PIXELS;
+            }
             continue;
         }
         if (!(top > 0.0)) continue;
         // Weighted centroid of pixels above 0.1 x max.
         double sw = 0.0, swx = 0.0, swy = 0.0;
-        for (int k = lane; k < hm * wm; k += 32) {
-            const int yy = k / wm, xx = k % wm;
-            const double s = c.mask(yy, xx) ? c.roi[k] : 0.0;
-            if (c.mask(yy, xx) && s > 0.1 * top) {
+        for (int k = tid; k < area_px; k += kRadialThreads) {
+            const double s = mask[k] ? c.roi[k] : 0.0;
+            if (mask[k] && s > 0.1 * top) {
                 sw += s;
-                swx += s * xx;
-                swy += s * yy;
+                swx += s * (k % wm);
+                swy += s * (k / wm);
             }
         }
-        sw = warp_sum(sw);
-        const double cx = warp_sum(swx) / sw, cy = warp_sum(swy) / sw;
-        // Spline coefficients: the cell padded by 12 edge pixels, filtered along y then x.
-        for (int k = lane; k < hp * wp; k += 32) {
+        sw = cta_sum(sw, red + 8);
+        const double cx = cta_sum(swx, red + 12) / sw, cy = cta_sum(swy, red + 16) / sw;
+        // Spline coefficients (the cell padded by 12 edge pixels) and the eroded cell (cross
+        // structure, zero outside the stack), where ray samples stay valid.
+        for (int k = tid; k < hp * wp; k += kRadialThreads) {
             const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
-            coef[k] = c.mask(yy, xx) ? c.roi[yy * wm + xx] : 0.0;
+            coef[k] = mask[yy * wm + xx] ? c.roi[yy * wm + xx] : 0.0;
         }
-        // Eroded cell (cross structure, zero outside the stack): where ray samples stay valid.
-        for (int k = lane; k < hm * wm; k += 32) {
+        for (int k = tid; k < area_px; k += kRadialThreads) {
             const int yy = k / wm, xx = k % wm;
-            emask[k] = c.mask(yy, xx) && yy > 0 && xx > 0 && yy < hm - 1 && xx < wm - 1 && c.mask(yy - 1, xx) &&
-                       c.mask(yy + 1, xx) && c.mask(yy, xx - 1) && c.mask(yy, xx + 1);
+            emask[k] = mask[k] && yy > 0 && xx > 0 && yy < hm - 1 && xx < wm - 1 && mask[k - wm] && mask[k + wm] &&
+                       mask[k - 1] && mask[k + 1];
         }
-        __syncwarp();
-        for (int col = lane; col < wp; col += 32) spline_line(coef + col, hp, wp);
-        __syncwarp();
-        for (int row = lane; row < hp; row += 32) spline_line(coef + (long long)row * wp, wp, 1);
-        __syncwarp();
+        __syncthreads();
+        for (int col = tid; col < wp; col += kRadialThreads) spline_line(coef + col, hp, wp);
+        __syncthreads();
+        for (int row = tid; row < hp; row += kRadialThreads) spline_line(coef + (long long)row * wp, wp, 1);
+        __syncthreads();
         const double peak = cubic_at(coef, hp, wp, cy + kPad, cx + kPad);
         const double half = peak / 2.0;
         const double inv2s = 1.0 / (2.0 * radial_step);
         int found_h = 0, found_g = 0;
-        for (int ray = lane; ray < ((n_angles + 31) / 32) * 32; ray += 32) {
+        for (int ray = tid; ray < n_angles; ray += kRadialThreads) {
             double edge_h = dnan(), edge_g = dnan();
-            if (ray < n_angles && peak > 0.0) {
+            if (peak > 0.0) {
                 const double ang = (double)ray * (2.0 * kPi / n_angles);
                 const double ux = cos(ang), uy = sin(ang);
                 double h1 = 0, h2 = 0, h3 = 0, h4 = 0;  // p[k-1] .. p[k-4]
@@ -707,59 +783,15 @@ __global__ void k_radial_cd(const double* cleaned, const int* vor, const int4* b
                     }
                 }
             }
-            if (ray < n_angles) {
-                if (half_out.status) half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
-                if (grad_out.status) grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
-                found_h += isfinite(edge_h);
-                found_g += isfinite(edge_g);
-            }
+            if (half_out.status) half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
+            if (grad_out.status) grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
+            found_h += isfinite(edge_h);
+            found_g += isfinite(edge_g);
         }
-        found_h = warp_sum_i(found_h);
-        found_g = warp_sum_i(found_g);
-        __syncwarp();
-        for (int o = 0; o < 2; ++o) {
-            const MethodOut& out = outs[o];
-            if (!out.status) continue;
-            const int found = o == 0 ? found_h : found_g;
-            const double* edge = out.edge_px + (long long)i * n_angles;
-            const double step = 2.0 * kPi / n_angles;
-            auto vertex = [&](int k, double* x, double* y) {
-                const int a = k % n_angles;
-                const double ang = (double)a * step;
-                *x = cx + edge[a] * cos(ang);
-                *y = cy + edge[a] * sin(ang);
-            };
-            if (out.contours)
-                for (int k = lane; k < nv; k += 32) {
-                    double x, y;
-                    vertex(k, &x, &y);
-                    out.contours[(long long)i * 2 * nv + 2 * k] = x + c.box.x;
-                    out.contours[(long long)i * 2 * nv + 2 * k + 1] = y + c.box.y;
-                }
-            double area = 0, perim = 0, px = 0, py = 0;
-            if (found == n_angles) polygon_geometry(nv, vertex, lane, &area, &perim, &px, &py);
-            if (lane == 0) {
-                double* m = out.metrics + (long long)i * out.n_metrics;
-                out.center_local[2LL * i] = cx;
-                out.center_local[2LL * i + 1] = cy;
-                out.centers[2LL * i] = cx + c.box.x;
-                out.centers[2LL * i + 1] = cy + c.box.y;
-                m[M_BACKGROUND] = 0.0;
-                m[M_PEAK] = peak;
-                m[M_COVERAGE] = (double)found / n_angles;
-                if (found == n_angles) {
-                    m[M_AREA] = area;
-                    m[M_CD_EQ] = 2.0 * sqrt(area / kPi);
-                    m[M_CD_X] = px;
-                    m[M_CD_Y] = py;
-                    m[M_PERIM] = perim;
-                    out.status[i] = SPX_ST_OK;
-                } else {
-                    out.status[i] = SPX_ST_INCOMPLETE_RAYS;
-                }
-            }
-        }
-        __syncwarp();
+        const int all_h = (int)cta_sum((double)found_h, red + 20);
+        const int all_g = (int)cta_sum((double)found_g, red + 24);  // also orders the edge writes
+        if (warp < 2)  // warp 0: halfmax, warp 1: gradient
+            radial_finish(warp == 0 ? half_out : grad_out, warp == 0 ? all_h : all_g, i, n_angles, cx, cy, peak, c.box);
     }
 }
 
@@ -818,9 +850,17 @@ int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, 
     return check_launch("k_logquad_cd");
 }
 
+// Shared memory of one radial CTA, or 0 when it does not fit and the CTAs use global scratch.
+static size_t radial_smem(int hm, int wm) {
+    const size_t bytes = (size_t)radial_cta_doubles(hm, wm) * sizeof(double);
+    return bytes <= 220 * 1024 ? bytes : 0;
+}
+
+constexpr int kRadialScratchCtas = 148 * 4;
+
 size_t spx_radial_workspace_bytes(int hm, int wm) {
-    const size_t per = ((size_t)(hm + 2 * kPad) * (wm + 2 * kPad) + (hm * wm + 7) / 8) * sizeof(double);
-    return 4 * per <= 200 * 1024 ? 256 : (size_t)148 * 8 * 4 * per + 256;
+    if (radial_smem(hm, wm)) return 256;
+    return (size_t)kRadialScratchCtas * radial_cta_doubles(hm, wm) * sizeof(double) + 256;
 }
 
 int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
@@ -837,21 +877,22 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
     // radii = np.arange(0, hypot(hm, wm) + step, step)
     const double stop = hypot((double)hm, (double)wm) + radial_step;
     const int n_radii = (int)ceil(stop / radial_step);
-    const size_t per = ((size_t)(hm + 2 * kPad) * (wm + 2 * kPad) + (hm * wm + 7) / 8) * sizeof(double);
-    const int warps = 4;
-    size_t smem = warps * per;
+    const size_t smem = radial_smem(hm, wm);
     double* scratch = nullptr;
-    int blocks = grid_for(n, warps, 148 * 8);
-    if (smem > 200 * 1024) {
-        smem = 0;
+    int blocks;
+    if (smem) {
+        if (smem > 48 * 1024)
+            SPX_CUDA(cudaFuncSetAttribute(k_radial_cd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd, kRadialThreads, smem));
+        blocks = (int)std::min<long long>(n, 148LL * std::max(per_sm, 1));
+    } else {
         scratch = static_cast<double*>(workspace);
-        blocks = min(blocks, 148 * 8);
-    } else if (smem > 48 * 1024) {
-        SPX_CUDA(cudaFuncSetAttribute(k_radial_cd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        blocks = std::min(n, kRadialScratchCtas);
     }
-    k_radial_cd<<<blocks, warps * 32, smem, s>>>(cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm,
-                                                  wm, width, n_angles, radial_step, n_radii, scratch,
-                                                  method_out(halfmax), method_out(gradient));
+    k_radial_cd<<<blocks, kRadialThreads, smem, s>>>(cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n,
+                                                      hm, wm, width, n_angles, radial_step, n_radii, scratch,
+                                                      method_out(halfmax), method_out(gradient));
     return check_launch("k_radial_cd");
 }
 

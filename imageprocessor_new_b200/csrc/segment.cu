@@ -668,6 +668,42 @@ int otsu_static_scratch(void** out) {
     return SPX_OK;
 }
 
+
+// ------------------------------------------------------------------------------ morphology
+
+// bw = 255 where the pixel is foreground (img > t, or img <= t with invert), else 0: the 0/255
+// image of cv2.threshold(THRESH_BINARY[_INV]).
+__global__ void k_binarize(const void* img, int dtype, long long n, const double* t_dev, double t_fixed, int invert,
+                           uint8_t* bw) {
+    const double t = t_dev ? *t_dev : t_fixed;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        bw[i] = is_fg(load_px(img, dtype, i), t, invert) ? 255 : 0;
+}
+
+// One erosion (dilate = 0: minimum) or dilation (maximum) of a 0/255 image with the 3x3 cross
+// (cv2.getStructuringElement(MORPH_ELLIPSE, (3, 3))); neighbours outside the image are ignored, as
+// OpenCV's default morphology border does.
+__global__ void k_morph_cross(const uint8_t* in, int H, int W, int dilate, uint8_t* out) {
+    const long long total = (long long)H * W;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / W), x = (int)(i % W);
+        unsigned v = in[i];
+        if (dilate) {
+            if (y > 0) v = max(v, (unsigned)in[i - W]);
+            if (y < H - 1) v = max(v, (unsigned)in[i + W]);
+            if (x > 0) v = max(v, (unsigned)in[i - 1]);
+            if (x < W - 1) v = max(v, (unsigned)in[i + 1]);
+        } else {
+            if (y > 0) v = min(v, (unsigned)in[i - W]);
+            if (y < H - 1) v = min(v, (unsigned)in[i + W]);
+            if (x > 0) v = min(v, (unsigned)in[i - 1]);
+            if (x < W - 1) v = min(v, (unsigned)in[i + 1]);
+        }
+        out[i] = (uint8_t)v;
+    }
+}
+
 }  // namespace
 }  // namespace spx
 
@@ -792,6 +828,42 @@ size_t spx_ccl_workspace_bytes(int height, int width) {
     size_t b = 0;
     ccl_layout(nullptr, height, width, &b);
     return b;
+}
+
+int spx_binarize(const void* img, int dtype, int height, int width, const double* threshold_dev,
+                 double fixed_threshold, int invert, uint8_t* out, void* stream) {
+    SPX_REQUIRE(height > 0 && width > 0 && dtype >= SPX_U8 && dtype <= SPX_F64, "bad arguments");
+    SPX_REQUIRE(img && out, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long n = (long long)height * width;
+    k_binarize<<<grid_for(n, 256), 256, 0, s>>>(img, dtype, n, threshold_dev, fixed_threshold, invert, out);
+    return check_launch("k_binarize");
+}
+
+int spx_morphology(uint8_t* bw, int height, int width, int open_iterations, int close_iterations, uint8_t* tmp,
+                   void* stream) {
+    SPX_REQUIRE(height > 0 && width > 0 && open_iterations >= 0 && close_iterations >= 0, "bad arguments");
+    SPX_REQUIRE(bw && tmp && bw != tmp, "null or aliased pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long n = (long long)height * width;
+    // MORPH_OPEN: erode then dilate, `open` times each; MORPH_CLOSE: dilate then erode. The number
+    // of passes is even, so the result ends in bw.
+    uint8_t* cur = bw;
+    uint8_t* nxt = tmp;
+    auto pass = [&](int dilate, int times) -> int {
+        for (int k = 0; k < times; ++k) {
+            k_morph_cross<<<grid_for(n, 256), 256, 0, s>>>(cur, height, width, dilate, nxt);
+            if (int e = check_launch("k_morph_cross")) return e;
+            uint8_t* t = cur;
+            cur = nxt;
+            nxt = t;
+        }
+        return SPX_OK;
+    };
+    if (int e = pass(0, open_iterations)) return e;
+    if (int e = pass(1, open_iterations)) return e;
+    if (int e = pass(1, close_iterations)) return e;
+    return pass(0, close_iterations);
 }
 
 int spx_ccl_label(const void* img, int dtype, int height, int width, const double* threshold_dev,

@@ -37,7 +37,8 @@ def _dedupe_device(pts_d: torch.Tensor, n: int, eps: float) -> torch.Tensor:
 
 
 def detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, connectivity, small_feature_max,
-                 tile_h, overlap, threshold_mode, otsu_downsample, thr_scale, dedupe_eps, device) -> CenterResult:
+                 tile_h, overlap, threshold_mode, otsu_downsample, thr_scale, dedupe_eps, device, morph_open=0,
+                 morph_close=0) -> CenterResult:
     from .centers import _centers_on_device, _device_image
 
     if overlap >= tile_h:
@@ -59,7 +60,8 @@ def detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, con
         thr = segment.binarize_threshold(band, threshold, invert) if pre is None else None
         c = _centers_on_device(band, threshold_dev=thr, fixed_threshold=pre if pre is not None else 0.0,
                                invert=invert, area_min=area_min, area_max=area_max, pad=pad, refine=refine,
-                               connectivity=connectivity, small_feature_max=small_feature_max)
+                               connectivity=connectivity, small_feature_max=small_feature_max,
+                               morph_open=morph_open, morph_close=morph_close)
         half = overlap // 2
         lo = y0 if y0 == 0 else y0 + half
         hi = y1 if y1 == height else y1 - half

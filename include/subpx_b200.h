@@ -89,6 +89,18 @@ int spx_otsu_static(const void* img, int dtype, int height, int width, int step,
 int spx_triangle(const void* img, int dtype, int height, int width, double* threshold,
                  void* workspace, size_t workspace_bytes, void* stream);
 
+/* bw (H x W uint8) = 255 where img > t (img <= t with invert), else 0, t = *threshold_dev or
+ * fixed_threshold when threshold_dev is null: cv2.threshold(THRESH_BINARY[_INV]) as
+ * subpx/_cpu/centers.py:257-258 and subpx/_gpu/centers.py:1515-1516 use it before morphology. */
+int spx_binarize(const void* img, int dtype, int height, int width, const double* threshold_dev,
+                 double fixed_threshold, int invert, uint8_t* out, void* stream);
+/* In place on the 0/255 image bw: open_iterations x (erode) then open_iterations x (dilate)
+ * (MORPH_OPEN), then close_iterations x (dilate) and close_iterations x (erode) (MORPH_CLOSE), each
+ * with the 3x3 cross and image-border pixels ignored; tmp is an H x W scratch image.
+ * subpx/_cpu/centers.py:260-265 (cv2.morphologyEx with MORPH_ELLIPSE (3, 3)). */
+int spx_morphology(uint8_t* bw, int height, int width, int open_iterations, int close_iterations, uint8_t* tmp,
+                   void* stream);
+
 size_t spx_ccl_workspace_bytes(int height, int width);
 /* Binarise (img > t, or img <= t with invert; t = *threshold_dev when threshold_dev is non-null,
  * else fixed_threshold) and label the foreground with `connectivity` 8 or 4. Writes provisional

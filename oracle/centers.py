@@ -178,13 +178,16 @@ def centers_from_components(g, labels, stats, num, *, area_min, area_max, pad, r
 
 
 def detect_centers(image, *, threshold="otsu", invert=False, area_min=1, area_max=50, pad=3,
-                   refine_method="logquad", connectivity=8, small_feature_max=12.0, fixed_threshold=None):
+                   refine_method="logquad", connectivity=8, small_feature_max=12.0, fixed_threshold=None,
+                   morph_open=0, morph_close=0):
     g = np.asarray(image)
     if fixed_threshold is None:
         t = segment.otsu_threshold(g) if threshold == "otsu" else segment.triangle_threshold(g)
     else:
         t = fixed_threshold
     fg = segment.binarize(g, t, invert)
+    if morph_open or morph_close:
+        fg = segment.morphology(fg, morph_open, morph_close)
     num, labels, stats, _ = segment.label_components(fg, connectivity)
     return centers_from_components(g, labels, stats, num, area_min=area_min, area_max=area_max, pad=pad,
                                    refine_method=refine_method, small_feature_max=small_feature_max)

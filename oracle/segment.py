@@ -93,6 +93,35 @@ def binarize(img: np.ndarray, t: float, invert: bool = False) -> np.ndarray:
     return (v <= t) if invert else (v > t)
 
 
+def morphology(fg: np.ndarray, morph_open: int = 0, morph_close: int = 0) -> np.ndarray:
+    """cv2.morphologyEx(bw, MORPH_OPEN, k, iterations=morph_open) then MORPH_CLOSE with
+    k = getStructuringElement(MORPH_ELLIPSE, (3, 3)) -- the 3x3 cross -- on a boolean mask
+    (subpx/_cpu/centers.py:260-265). OPEN is `n` erosions then `n` dilations, CLOSE the reverse;
+    pixels outside the image never change a minimum or a maximum (OpenCV's default border)."""
+    m = np.asarray(fg, dtype=bool).copy()
+
+    def erode(a):
+        out = a.copy()
+        out[1:, :] &= a[:-1, :]
+        out[:-1, :] &= a[1:, :]
+        out[:, 1:] &= a[:, :-1]
+        out[:, :-1] &= a[:, 1:]
+        return out
+
+    def dilate(a):
+        out = a.copy()
+        out[1:, :] |= a[:-1, :]
+        out[:-1, :] |= a[1:, :]
+        out[:, 1:] |= a[:, :-1]
+        out[:, :-1] |= a[:, 1:]
+        return out
+
+    for op, times in ((erode, morph_open), (dilate, morph_open), (dilate, morph_close), (erode, morph_close)):
+        for _ in range(int(times)):
+            m = op(m)
+    return m
+
+
 def label_components(fg: np.ndarray, connectivity: int = 8):
     """(num_labels, labels int32, stats (K+1, 5) int32, centroids (K+1, 2) f64) numbered as OpenCV:
     components ordered by their first 2x2 block in row-pair scan order (8-connectivity) or their

@@ -105,6 +105,9 @@ def center_images():
         "dots": (dots, dict(threshold="otsu", area_max=50)),
         "small": (small, dict(threshold="otsu", area_max=200)),
         "dots_tri": (dots, dict(threshold="triangle", area_max=50)),
+        "small_morph": (small, dict(threshold="otsu", area_max=200, morph_open=1, morph_close=1)),
+        "page_morph": (np.ascontiguousarray(page[:256, :384]), dict(threshold="otsu", area_max=400, morph_open=2,
+                                                                    morph_close=1)),
     }
 
 

@@ -9,7 +9,9 @@ from oracle import centers as oc
 pytestmark = pytest.mark.gpu
 
 PARAMS = {"page": dict(threshold="otsu", area_max=400), "dots": dict(threshold="otsu", area_max=50),
-          "small": dict(threshold="otsu", area_max=200), "dots_tri": dict(threshold="triangle", area_max=50)}
+          "small": dict(threshold="otsu", area_max=200), "dots_tri": dict(threshold="triangle", area_max=50),
+          "small_morph": dict(threshold="otsu", area_max=200, morph_open=1, morph_close=1),
+          "page_morph": dict(threshold="otsu", area_max=400, morph_open=2, morph_close=1)}
 
 
 @pytest.mark.parametrize("refine", ["weighted", "logquad", "edge_gradmoment", "none", "auto"])
@@ -75,3 +77,38 @@ def test_bad_arguments_raise():
         detect_centers(img, backend="cpu")
     with pytest.raises(ValueError):
         detect_centers(np.zeros((4, 4, 3), np.uint8), backend="gpu")
+
+
+def test_morphology_masks_match_oracle():
+    import torch
+
+    from imageprocessor_new_b200 import _lib, synthetic
+
+    page = synthetic.page_square(2).image[:300, :417]
+    thr = 2200.0
+    fg = page > thr
+    img_d = torch.from_numpy(np.ascontiguousarray(page)).cuda()
+    h, w = page.shape
+    stream = torch.cuda.current_stream().cuda_stream
+    for o, c in ((1, 0), (0, 2), (2, 1), (3, 3)):
+        bw = torch.empty((h, w), dtype=torch.uint8, device="cuda")
+        tmp = torch.empty_like(bw)
+        _lib.call("spx_binarize", img_d.data_ptr(), 1, h, w, None, thr, 0, bw.data_ptr(), stream)
+        _lib.call("spx_morphology", bw.data_ptr(), h, w, o, c, tmp.data_ptr(), stream)
+        from oracle import segment as osg
+
+        want = osg.morphology(fg, o, c).astype(np.uint8) * 255
+        np.testing.assert_array_equal(bw.cpu().numpy(), want, err_msg=f"open {o} close {c}")
+
+
+def test_tiled_with_morphology_matches_untiled_rules():
+    from imageprocessor_new_b200 import detect_centers, synthetic
+
+    page = synthetic.page_square(1).image
+    kw = dict(backend="gpu", threshold="otsu", refine="weighted", area_max=400, morph_open=1, morph_close=1)
+    whole = detect_centers(page, tile_h=page.shape[0], overlap=0, **kw).centers_xy
+    tiled = detect_centers(page, tile_h=300, overlap=64, **kw).centers_xy
+    # Bands see the same global threshold; holes away from band edges are found identically.
+    d = np.sqrt(((whole[:, None, :] - tiled[None, :, :]) ** 2).sum(-1)).min(axis=1)
+    assert len(tiled) == len(whole)
+    assert np.median(d) == 0.0

@@ -39,7 +39,9 @@ def test_ccl_numbering_and_stats_match_opencv(conn):
 def test_detect_centers_match_reference_cpu():
     z = _load("centers")
     params = {"page": dict(threshold="otsu", area_max=400), "dots": dict(threshold="otsu", area_max=50),
-              "small": dict(threshold="otsu", area_max=200), "dots_tri": dict(threshold="triangle", area_max=50)}
+              "small": dict(threshold="otsu", area_max=200), "dots_tri": dict(threshold="triangle", area_max=50),
+              "small_morph": dict(threshold="otsu", area_max=200, morph_open=1, morph_close=1),
+              "page_morph": dict(threshold="otsu", area_max=400, morph_open=2, morph_close=1)}
     for name in z["names"]:
         img = z[f"{name}_img"]
         for refine in ("weighted", "logquad", "edge_gradmoment", "none", "auto"):
@@ -94,3 +96,21 @@ def test_measure_cds_oracle_matches_reference(name):
         np.testing.assert_allclose(r["metrics"]["cd_equivalent_px"], z[f"{name}_{method}_m_cd_equivalent_px"],
                                    rtol=0, atol=1e-9, equal_nan=True)
         np.testing.assert_allclose(r["contours"], z[f"{name}_{method}_contours"], rtol=0, atol=1e-9, equal_nan=True)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_morphology_matches_opencv(seed):
+    cv2 = pytest.importorskip("cv2")
+    rng = np.random.default_rng(seed)
+    fg = rng.random((61, 83)) < (0.35 + 0.2 * seed)
+    fg[0, :] = True        # borders: pixels outside must not erode or dilate anything
+    fg[:, -1] = seed % 2 == 0
+    bw = fg.astype(np.uint8) * 255
+    k = cv2.getStructuringElement(cv2.MORPH_ELLIPSE, (3, 3))
+    for o, c in ((1, 0), (0, 1), (2, 1), (1, 3)):
+        want = bw
+        if o:
+            want = cv2.morphologyEx(want, cv2.MORPH_OPEN, k, iterations=o)
+        if c:
+            want = cv2.morphologyEx(want, cv2.MORPH_CLOSE, k, iterations=c)
+        np.testing.assert_array_equal(osg.morphology(fg, o, c), want > 0, err_msg=f"open {o} close {c}")
