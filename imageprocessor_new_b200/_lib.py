@@ -7,7 +7,7 @@ CUDA device raises immediately, with the reason.
 from __future__ import annotations
 
 import ctypes
-from ctypes import c_double, c_int, c_size_t, c_void_p, POINTER
+from ctypes import POINTER, c_double, c_int, c_longlong, c_size_t, c_void_p
 from pathlib import Path
 
 import numpy as np
@@ -58,6 +58,8 @@ SIGNATURES = {
     "spx_otsu_static": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "spx_triangle": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
+    "spx_histogram": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
+    "spx_otsu_from_histogram": (_I, [_P, _I, _P, c_longlong, _P, _P, _S, _P]),
     "spx_binarize": (_I, [_P, _I, _I, _I, _P, _D, _I, _P, _P]),
     "spx_morphology": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "spx_ccl_label": (_I, [_P, _I, _I, _I, _P, _D, _I, _I, _P, _P, _P, _S, _P]),

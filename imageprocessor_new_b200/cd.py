@@ -242,7 +242,8 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
         return host[offsets[key]:offsets[key] + int(np.prod(shape))].reshape(shape)[:n]
 
     m = part("metrics")
-    status = STATUS[host[offsets["status"]:].view(np.uint8)[:n]]
+    codes = host[offsets["status"]:].view(np.uint8)[:n]
+    status = STATUS[codes]
     metrics = {name: np.ascontiguousarray(m[:, k]) for k, name in enumerate(names)}
     if shapes["contours"] is not None:
         contours = part("contours")
@@ -256,7 +257,7 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
     elif not metrics_only:
         geometry = {"eigenvalues": part("eigenvalues"), "axes": part("axes")}
     return CDMethodResult(method=method, centers_xy=part("centers"), contours_xy=contours,
-                          valid=status == "ok", status=status, metrics=metrics, geometry=geometry)
+                          valid=codes == 0, status=status, metrics=metrics, geometry=geometry)
 
 
 def _revise_seeds(dbl: Deblender, state, seeds_xy, pitch, oversized_d, *, drop_fraction=0.3, add_fraction=0.5):

@@ -556,13 +556,27 @@ __device__ void spline_line(double* c, int n, int stride) {
     for (int i = n - 2; i >= 0; --i) c[i * stride] = z * (c[(i + 1) * stride] - c[i * stride]);
 }
 
+// x / 6, correctly rounded, by Markstein's correction of x * RN(1/6) with one FMA (checked against
+// exact rational division on 600k operands spanning the double range).
+__device__ __forceinline__ double div6(double x) {
+    const double c = 0.16666666666666666;  // RN(1/6)
+    const double q = __dmul_rn(x, c);
+    return __fma_rn(__fma_rn(-q, 6.0, x), c, q);
+}
+
+// scipy's order-3 interpolation weights at fractional offset t = v - floor(v).
+__device__ __forceinline__ void cubic_weights_t(double t, double* w) {
+    const double s = 1.0 - t;
+    w[1] = div6(t * t * (t - 2.0) * 3.0 + 4.0);
+    w[2] = div6(s * s * (s - 2.0) * 3.0 + 4.0);
+    w[0] = div6(s * s * s);
+    w[3] = 1.0 - w[0] - w[1] - w[2];
+}
+
 // scipy's order-3 interpolation weights and clamped ("nearest") indices at coordinate v.
 __device__ __forceinline__ void cubic_weights(double v, int n, double* w, int* idx) {
-    const double f = floor(v), t = v - f, s = 1.0 - t;
-    w[1] = (t * t * (t - 2.0) * 3.0 + 4.0) / 6.0;
-    w[2] = (s * s * (s - 2.0) * 3.0 + 4.0) / 6.0;
-    w[0] = s * s * s / 6.0;
-    w[3] = 1.0 - w[0] - w[1] - w[2];
+    const double f = floor(v);
+    cubic_weights_t(v - f, w);
     for (int k = 0; k < 4; ++k) idx[k] = min(max((int)f - 1 + k, 0), n - 1);
 }
 
@@ -577,6 +591,48 @@ __device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, d
 #pragma unroll
         for (int b = 0; b < 4; ++b) out += coef[iy[a] * wp + ix[b]] * wy[a] * wx[b];
     return out;
+}
+
+// The 4x4 coefficient window around the last sample of a ray, kept in registers and reloaded
+// only when the ray enters another integer cell (about every 10 samples at 0.1 px steps). The
+// sum runs in the same order as cubic_at.
+struct SplineWindow {
+    int fy = -1 << 30, fx = -1 << 30;
+    double c[16];
+    __device__ __forceinline__ double at(const double* coef, int hp, int wp, double y, double x) {
+        const double fyd = floor(y), fxd = floor(x);
+        const int iy = (int)fyd, ix = (int)fxd;
+        if (iy != fy || ix != fx) {
+            fy = iy;
+            fx = ix;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int ya = min(max(iy - 1 + a, 0), hp - 1);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) c[a * 4 + b] = coef[ya * wp + min(max(ix - 1 + b, 0), wp - 1)];
+            }
+        }
+        double wy[4], wx[4];
+        cubic_weights_t(y - fyd, wy);
+        cubic_weights_t(x - fxd, wx);
+        double out = 0.0;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) out += c[a * 4 + b] * wy[a] * wx[b];
+        return out;
+    }
+};
+
+// inside_bytes with a shortcut: when every mask byte the bilinear weights touch is set, the
+// weights sum to 1 within rounding and the sample is inside.
+__device__ __forceinline__ bool inside_fast(const uint8_t* m, int hm, int wm, double y, double x) {
+    if (!(y >= 0.0 && y <= (double)(hm - 1) && x >= 0.0 && x <= (double)(wm - 1))) return false;
+    const double fy = floor(y), fx = floor(x);
+    const bool ey = y == fy, ex = x == fx;
+    const uint8_t* r = m + (int)fy * wm + (int)fx;
+    if (r[0] && (ex || r[1]) && (ey || (r[wm] && (ex || r[wm + 1])))) return true;
+    return inside_bytes(m, hm, wm, y, x);
 }
 
 constexpr int kRadialThreads = 128;
@@ -668,7 +724,7 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
 // crossing and the parabolic maximum of the outward decrease (halfmax / gradient methods).
 // One 128-thread CTA per cell: the cell's masks and spline coefficients are staged once in
 // shared memory and each thread walks its own rays.
-__global__ void __launch_bounds__(kRadialThreads, 5) k_radial_cd(
+__global__ void __launch_bounds__(kRadialThreads, 4) k_radial_cd(
     const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
     int n_angles, double radial_step, int n_radii, double* coef_scratch, MethodOut half_out, MethodOut grad_out) {
     extern __shared__ double sm[];
@@ -744,11 +800,12 @@ __global__ void __launch_bounds__(kRadialThreads, 5) k_radial_cd(
                 bool crossed = false;
                 double best = -dinf(), gl = 0, gm = 0, gr = 0;
                 int best_j = -1, first_invalid = n_radii;
+                SplineWindow win;
                 for (int k = 0; k < n_radii; ++k) {
                     const double r = (double)k * radial_step;
                     const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
-                    if (!inside_bytes(emask, hm, wm, y, x)) { first_invalid = k; break; }
-                    const double p = k == 0 ? peak : cubic_at(coef, hp, wp, y + kPad, x + kPad);
+                    if (!inside_fast(emask, hm, wm, y, x)) { first_invalid = k; break; }
+                    const double p = k == 0 ? peak : win.at(coef, hp, wp, y + kPad, x + kPad);
                     if (k >= 1 && !crossed && h1 >= half && p < half) {
                         edge_h = (double)(k - 1) * radial_step + ((h1 - half) / (h1 - p)) * radial_step;
                         crossed = true;

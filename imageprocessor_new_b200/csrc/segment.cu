@@ -766,6 +766,43 @@ int spx_otsu(const void* img, int dtype, int height, int width, int step, double
     return check_launch("k_otsu_scan");
 }
 
+int spx_histogram(const void* img, int dtype, int height, int width, int step, unsigned int* hist,
+                  unsigned int* range, void* stream) {
+    SPX_REQUIRE(dtype == SPX_U8 || dtype == SPX_U16, "histograms need a uint8 or uint16 image");
+    SPX_REQUIRE(height > 0 && width > 0 && step >= 1, "bad image size or step");
+    SPX_REQUIRE(img && hist && range, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    SPX_CUDA(cudaMemsetAsync(hist, 0, 65536 * sizeof(unsigned int), s));
+    const unsigned int init[2] = {0xffffffffu, 0u};
+    SPX_CUDA(cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const long long n = (long long)hs * ws;
+    k_minmax<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(img, dtype, height, width, step, range);
+    if (int e = check_launch("k_minmax")) return e;
+    const size_t smem = kHistSmemBins * sizeof(unsigned int);
+    SPX_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int dense = step == 1 && dtype == SPX_U16 && (reinterpret_cast<uintptr_t>(img) % 16) == 0;
+    k_histogram<<<grid_for(n / 8 + 1, 512, 148 * 3), 512, smem, s>>>(img, dtype, height, width, step, dense, range,
+                                                                     hist);
+    return check_launch("k_histogram");
+}
+
+int spx_otsu_from_histogram(const unsigned int* hist, int dtype, const unsigned int* range, long long total,
+                            double* threshold, void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(dtype == SPX_U8 || dtype == SPX_U16, "Otsu thresholding needs a uint8 or uint16 histogram");
+    SPX_REQUIRE(total > 0, "empty histogram");
+    SPX_REQUIRE(hist && range && threshold && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_otsu_workspace_bytes(dtype), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Arena a(workspace);
+    a.take<unsigned int>(65536);
+    a.take<unsigned int>(2);
+    double* bufs = a.take<double>(4 * 65536);
+    k_otsu_scan<<<1, 1024, 0, s>>>(hist, dtype == SPX_U8 ? 256 : 65536, range, total, bufs, bufs + 65536,
+                                   bufs + 2 * 65536, bufs + 3 * 65536, threshold);
+    return check_launch("k_otsu_scan");
+}
+
 int spx_otsu_static(const void* img, int dtype, int height, int width, int step, double* threshold, void* stream) {
     SPX_REQUIRE(dtype == SPX_U8 || dtype == SPX_U16, "Otsu thresholding needs a uint8 or uint16 image");
     SPX_REQUIRE(height > 0 && width > 0 && step >= 1, "bad image size or step");

@@ -85,6 +85,17 @@ int spx_otsu(const void* img, int dtype, int height, int width, int step, double
  * allocating library call). */
 int spx_otsu_static(const void* img, int dtype, int height, int width, int step, double* threshold, void* stream);
 
+/* Histogram of img[::step, ::step] into hist (65536 uint32 counts, absolute grey levels) and its
+ * [min, max] into range[2]. With spx_otsu_from_histogram this splits spx_otsu so that row shards of
+ * one page on several GPUs can sum their histograms (and min / max their ranges) before the global
+ * Otsu of subpx/_gpu/centers.py:1789-1796. */
+int spx_histogram(const void* img, int dtype, int height, int width, int step, unsigned int* hist,
+                  unsigned int* range, void* stream);
+/* Otsu threshold (OpenCV THRESH_OTSU) of a histogram of `total` pixels with value range `range`;
+ * the workspace is spx_otsu_workspace_bytes(dtype). */
+int spx_otsu_from_histogram(const unsigned int* hist, int dtype, const unsigned int* range, long long total,
+                            double* threshold, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Triangle threshold of a uint8 image, as OpenCV's THRESH_TRIANGLE (uses the Otsu workspace). */
 int spx_triangle(const void* img, int dtype, int height, int width, double* threshold,
                  void* workspace, size_t workspace_bytes, void* stream);

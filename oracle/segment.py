@@ -27,8 +27,14 @@ def otsu_threshold(img: np.ndarray) -> float:
     img = np.asarray(img)
     if img.dtype not in (np.uint8, np.uint16):
         raise ValueError("Otsu needs uint8 or uint16")
-    h = histogram(img)
-    scale = 1.0 / img.size
+    return otsu_from_histogram(histogram(img), img.size)
+
+
+def otsu_from_histogram(h: np.ndarray, total: int) -> float:
+    """The Otsu scan of otsu_threshold on a histogram of `total` pixels (a sum of histograms of row
+    shards gives the whole image's threshold)."""
+    h = np.asarray(h, dtype=np.int64)
+    scale = 1.0 / total
     mu = float(np.dot(np.arange(len(h), dtype=np.int64), h)) * scale  # exact integer sum
     nz = np.flatnonzero(h)
     if len(nz) == 0:

@@ -52,3 +52,49 @@ def test_tiled_per_tile_threshold_and_bad_overlap():
     assert abs(len(res.centers_xy) - len(full)) <= 2
     with pytest.raises(ValueError):
         detect_centers(page, backend="gpu", tile_h=100, overlap=100)
+
+
+def test_histogram_shards_give_the_global_otsu():
+    import torch
+
+    from imageprocessor_new_b200 import segment, shard, synthetic
+
+    page = synthetic.page_staggered(2, shape=(1500, 1300)).image
+    ops = shard.GpuBandOps()
+    ds = 4
+    hist = torch.zeros(shard.NBINS, dtype=torch.int64, device="cuda")
+    lo, hi, total = None, None, 0
+    for rank in range(3):
+        r0, r1 = shard.sampled_rows_of_rank(page.shape[0], ds, rank, 3)
+        h, rng, n = ops.histogram(page[r0:r1], ds)
+        hist += h
+        lo = int(rng[0]) if lo is None else min(lo, int(rng[0]))
+        hi = int(rng[1]) if hi is None else max(hi, int(rng[1]))
+        total += n
+    got = ops.otsu(hist, torch.tensor([lo, hi], dtype=torch.int64, device="cuda"), total, page.dtype)
+    want = float(segment.otsu(torch.from_numpy(page).cuda(), step=ds).item())
+    assert got == want
+
+
+def test_sharded_tiled_detection_on_one_rank_matches_detect_centers():
+    import os
+    import socket
+
+    import torch.distributed as dist
+
+    from imageprocessor_new_b200 import detect_centers, shard, synthetic
+
+    page = synthetic.page_square(5).image
+    kw = dict(threshold="otsu", invert=False, area_min=1, area_max=400, pad=3, refine="logquad", connectivity=8,
+              small_feature_max=12.0)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        got = shard.detect_tiled_sharded(page, tile_h=300, overlap=64, ops=shard.GpuBandOps(**kw))
+    finally:
+        dist.destroy_process_group()
+    want = detect_centers(page, backend="gpu", tile_h=300, overlap=64, **kw).centers_xy
+    np.testing.assert_array_equal(got, want)
