@@ -41,7 +41,7 @@ class MethodOut(ctypes.Structure):
 
     _fields_ = [("centers", c_void_p), ("contours", c_void_p), ("status", c_void_p), ("metrics", c_void_p),
                 ("center_local", c_void_p), ("edge_px", c_void_p), ("eigenvalues", c_void_p), ("axes", c_void_p),
-                ("n_metrics", c_int)]
+                ("n_metrics", c_int), ("metric_col_stride", c_longlong)]
 
 
 _BG = POINTER(BgMap)

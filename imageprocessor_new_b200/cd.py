@@ -199,7 +199,7 @@ def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
     shapes = {
         "centers": (m, 2),
         "contours": (m, n_angles + 1, 2) if contours else None,
-        "metrics": (m, max(len(names), 13)),
+        "metrics": (max(len(names), 13), m),  # column-major: one contiguous column per metric
         "center_local": (m, 2),
         "edge_px": (m, n_angles) if method in ("gradient", "halfmax") else None,
         "eigenvalues": (m, 2) if method in ("logquad", "gaussian") else None,
@@ -218,19 +218,31 @@ def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
     b["status"] = b["status"].view(torch.uint8)[:m]
     struct = _lib.MethodOut(*(None if b[k] is None else b[k].data_ptr() for k in
                               ("centers", "contours", "status", "metrics", "center_local", "edge_px", "eigenvalues",
-                               "axes")), b["metrics"].shape[1])
+                               "axes")), b["metrics"].shape[0], m)
     return b, struct
 
 
-def _download(bufs: dict) -> dict:
-    """Copy every method's buffer into pinned host memory with one copy each and one synchronise."""
-    host = {}
-    for name, b in bufs.items():
+_COPY_STREAMS: dict = {}
+
+
+def _copy_stream() -> torch.cuda.Stream:
+    dev_index = torch.cuda.current_device()
+    if dev_index not in _COPY_STREAMS:
+        _COPY_STREAMS[dev_index] = torch.cuda.Stream()
+    return _COPY_STREAMS[dev_index]
+
+
+def _start_download(b: dict, after: torch.cuda.Event):
+    """Copies one method's buffer to pinned host memory on a side stream once `after` has fired;
+    returns (host tensor, completion event)."""
+    side = _copy_stream()
+    side.wait_event(after)
+    with torch.cuda.stream(side):
         h = torch.empty(b["_flat"].shape, dtype=torch.float64, pin_memory=True)
         h.copy_(b["_flat"], non_blocking=True)
-        host[name] = h
-    torch.cuda.current_stream().synchronize()
-    return {name: h.numpy() for name, h in host.items()}
+        done = torch.cuda.Event()
+        done.record(side)
+    return h, done
 
 
 def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: bool, n_angles: int) -> CDMethodResult:
@@ -241,10 +253,11 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
         shape = shapes[key]
         return host[offsets[key]:offsets[key] + int(np.prod(shape))].reshape(shape)[:n]
 
-    m = part("metrics")
+    shape = shapes["metrics"]
+    m = host[offsets["metrics"]:offsets["metrics"] + int(np.prod(shape))].reshape(shape)
     codes = host[offsets["status"]:].view(np.uint8)[:n]
     status = STATUS[codes]
-    metrics = {name: np.ascontiguousarray(m[:, k]) for k, name in enumerate(names)}
+    metrics = {name: m[k, :n] for k, name in enumerate(names)}
     if shapes["contours"] is not None:
         contours = part("contours")
     else:
@@ -426,7 +439,31 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
     stream = dev.stream_ptr()
     c = cells
     radial = [m for m in methods if m in ("gradient", "halfmax")]
-    bufs = {}
+    bufs, pending = {}, []  # pending: (method names, host copies and their completion events)
+    main = torch.cuda.current_stream()
+
+    def launched(names):
+        # Each method's results go to pinned host memory on a side stream as soon as its kernel is
+        # done, so the host converts one method while the GPU still runs the next.
+        ev = torch.cuda.Event()
+        ev.record(main)
+        pending.append((names, [_start_download(bufs[name], ev) for name in names]))
+
+    t_gauss = time.perf_counter()
+    if "gaussian" in methods and nr:
+        gb2 = _method_buffers(nr, n_angles, "gaussian", not metrics_only)
+        _lib.call("spx_gaussian_method", state.params_d.data_ptr(), state.status_d.data_ptr(), cleaned.data_ptr(),
+                  c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(), nr, c.hm, c.wm, width, n_angles,
+                  gb2[1], stream)
+        bufs["gaussian"] = gb2[0]
+        launched(["gaussian"])
+    t_gauss = time.perf_counter() - t_gauss
+    if "logquad" in methods and nr:
+        lb = _method_buffers(nr, n_angles, "logquad", not metrics_only)
+        _lib.call("spx_logquad_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(),
+                  c.seeds_d.data_ptr(), nr, c.hm, c.wm, width, n_angles, fit_fraction, lb[1], stream)
+        bufs["logquad"] = lb[0]
+        launched(["logquad"])
     if radial and nr:
         hb = _method_buffers(nr, n_angles, "halfmax", not metrics_only) if "halfmax" in radial else (None, None)
         gb = _method_buffers(nr, n_angles, "gradient", not metrics_only) if "gradient" in radial else (None, None)
@@ -439,25 +476,21 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
             bufs["halfmax"] = hb[0]
         if gb[0] is not None:
             bufs["gradient"] = gb[0]
-    if "logquad" in methods and nr:
-        lb = _method_buffers(nr, n_angles, "logquad", not metrics_only)
-        _lib.call("spx_logquad_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(),
-                  c.seeds_d.data_ptr(), nr, c.hm, c.wm, width, n_angles, fit_fraction, lb[1], stream)
-        bufs["logquad"] = lb[0]
-    seconds["radial"], start = time.perf_counter() - start, time.perf_counter()
-    if "gaussian" in methods and nr:
-        gb2 = _method_buffers(nr, n_angles, "gaussian", not metrics_only)
-        _lib.call("spx_gaussian_method", state.params_d.data_ptr(), state.status_d.data_ptr(), cleaned.data_ptr(),
-                  c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(), nr, c.hm, c.wm, width, n_angles,
-                  gb2[1], stream)
-        bufs["gaussian"] = gb2[0]
-    host = _download(bufs) if nr else {}
+        launched([m for m in ("halfmax", "gradient") if m in bufs])
+    seconds["radial"] = time.perf_counter() - start - t_gauss
+    for names, copies in pending:
+        t0 = time.perf_counter()
+        for name, (host, done) in zip(names, copies):
+            done.synchronize()
+            found[name] = _to_result(name, nr, bufs[name], host.numpy(), metrics_only, n_angles)
+        key = "gaussian" if names == ["gaussian"] else "radial"
+        seconds[key] = seconds.get(key, 0.0) + time.perf_counter() - t0
+    seconds["gaussian"] = seconds.get("gaussian", 0.0) + t_gauss
     for name in methods:
-        if nr:
-            found[name] = _to_result(name, nr, bufs[name], host[name], metrics_only, n_angles)
-        else:
+        if not nr:
             found[name] = _empty_result(name, n_angles, metrics_only)
-    seconds["gaussian"], start = time.perf_counter() - start, time.perf_counter()
+    found = {name: found[name] for name in methods}
+    start = time.perf_counter()
     local_background = (state.background.at_points(c.seeds_d[dev.upload(report.astype(np.int64))], sign)
                         if nr else np.zeros(0))
     measurements = {}

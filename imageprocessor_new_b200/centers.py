@@ -99,8 +99,13 @@ def _centers_on_device(img_d: torch.Tensor, *, threshold_dev: torch.Tensor | Non
 
 
 def _finite(centers: torch.Tensor) -> np.ndarray:
-    c = centers.cpu().numpy().reshape(-1, 2)
-    return c[np.isfinite(c).all(axis=1)].astype(np.float64, copy=False)
+    """The finite rows of the device centres, through pinned host memory."""
+    host = torch.empty(centers.shape, dtype=centers.dtype, pin_memory=True)
+    host.copy_(centers, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    c = host.numpy().reshape(-1, 2)
+    ok = np.isfinite(c[:, 0]) & np.isfinite(c[:, 1])
+    return c if ok.all() else c[ok]
 
 
 def detect_centers(

@@ -138,7 +138,20 @@ struct MethodOut {
     double* eigenvalues; // n x 2 (ellipse methods)
     double* axes;        // n x 2 x 2 (ellipse methods)
     int n_metrics;
+    long long col_stride;  // 0: row-major metrics; else metric q of cell i at metrics[i + q * col_stride]
+    __device__ __forceinline__ struct MetricRow row(long long i) const;
 };
+
+// One cell's metrics, row-major or column-major.
+struct MetricRow {
+    double* p;
+    long long step;
+    __device__ __forceinline__ double& operator[](int q) const { return p[q * step]; }
+};
+
+__device__ __forceinline__ MetricRow MethodOut::row(long long i) const {
+    return col_stride ? MetricRow{metrics + i, col_stride} : MetricRow{metrics + i * n_metrics, 1};
+}
 
 // Metric columns (same order as the Python side).
 enum {
@@ -257,7 +270,7 @@ __global__ void k_gaussian_method(const double* params, const uint8_t* status_in
         }
         ss = warp_sum(ss);
         cnt = warp_sum_i(cnt);
-        double* m = out.metrics + (long long)i * out.n_metrics;
+        const MetricRow m = out.row(i);
         uint8_t st = status_in[j];
         bool finite = true;
         for (int q = 0; q < 6; ++q) finite = finite && isfinite(p[q]);
@@ -344,7 +357,7 @@ __global__ void k_logquad_cd(const double* cleaned, const int* vor, const int4* 
         const CellView c{cleaned + (long long)i * hm * wm, vor, boxes[j], j, W, hm, wm};
         const double sx = seeds[2LL * j] - c.box.x, sy = seeds[2LL * j + 1] - c.box.y;
         const int nv = n_angles + 1;
-        double* m = out.metrics + (long long)i * out.n_metrics;
+        const MetricRow m = out.row(i);
         // Defaults: no_signal, seed centre, NaN geometry.
         if (lane == 0) {
             for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
@@ -664,7 +677,7 @@ __device__ void radial_clear(const MethodOut out, int i, int n_angles) {
     if (!out.status) return;
     const int nv = n_angles + 1;
     if (threadIdx.x == 0) {
-        double* m = out.metrics + (long long)i * out.n_metrics;
+        const MetricRow m = out.row(i);
         for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
         out.status[i] = SPX_ST_NO_SIGNAL;
         out.centers[2LL * i] = out.centers[2LL * i + 1] = dnan();
@@ -698,7 +711,7 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
     double area = 0, perim = 0, px = 0, py = 0;
     if (found == n_angles) polygon_geometry(nv, vertex, lane, &area, &perim, &px, &py);
     if (lane == 0) {
-        double* m = out.metrics + (long long)i * out.n_metrics;
+        const MetricRow m = out.row(i);
         out.center_local[2LL * i] = cx;
         out.center_local[2LL * i + 1] = cy;
         out.centers[2LL * i] = cx + box.x;
@@ -855,7 +868,7 @@ __global__ void __launch_bounds__(kRadialThreads, 4) k_radial_cd(
 MethodOut method_out(const spx_method_out* o) {
     MethodOut m;
     if (!o) {
-        m = MethodOut{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+        m = MethodOut{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0};
         return m;
     }
     m.centers = o->centers;
@@ -867,6 +880,7 @@ MethodOut method_out(const spx_method_out* o) {
     m.eigenvalues = o->eigenvalues;
     m.axes = o->axes;
     m.n_metrics = o->n_metrics;
+    m.col_stride = o->metric_col_stride;
     return m;
 }
 

@@ -78,7 +78,7 @@ __global__ void k_cells_setup(const double* rows, int n, int pad, int H, int W, 
 // --------------------------------------------------------------------------------- fit status
 
 // fit_status (subpx/_cpu/deblend.py:262-277) of ROI-local params p of cell j.
-__device__ int fit_status_of(const double* p, double cap, int j, int4 box, int hm, int wm, const int* vor, int W) {
+__device__ __forceinline__ int fit_status_of(const double* p, double cap, int j, int4 box, int hm, int wm, const int* vor, int W) {
     for (int i = 0; i < 6; ++i)
         if (!isfinite(p[i])) return SPX_ST_FIT_DIVERGED;
     int st = SPX_ST_OK;

@@ -8,7 +8,7 @@
 // stop when the relative cost drop is <= 1e-12, max |step| < 1e-7, lam > 1e12 or after max_iter.
 //
 // Layout: the cell's mask pixels are compacted into (value, packed local x | y << 16) arrays; lanes
-// stride over them, the 27 sums are butterfly-reduced so every lane holds identical totals, and
+// stride over them, the 27 sums are all-reduced so every lane holds identical totals, and
 // every lane solves the damped 6x6 system (Cholesky, fully unrolled in registers) and takes the
 // same decisions, so the warp never diverges on control flow. Arithmetic is FP64.
 #pragma once
@@ -31,106 +31,133 @@ __device__ __forceinline__ GaussEval gauss_eval(const double* p, double e1, doub
     return g;
 }
 
-__device__ __forceinline__ double warp_cost(const double* p, const double* v, const int* xy, int n, int lane) {
-    const double e1 = exp(p[3]), e3 = exp(p[5]);
-    double acc = 0.0;
-    for (int k = lane; k < n; k += 32) {
-        const int c = xy[k];
-        const double dx = (double)(c & 0xffff) - p[1], dy = (double)(c >> 16) - p[2];
-        const GaussEval g = gauss_eval(p, e1, e3, dx, dy);
-        const double r = v[k] - p[0] * g.shape;
-        acc += r * r;
-    }
-    return warp_sum(acc);
-}
-
 // Solves (N + diag(lam * N_ii + 1e-12)) s = g for the symmetric 6x6 N given by its upper triangle
 // (21 values, row-major) by Cholesky; NaN propagates into s when the matrix is not positive.
 __device__ __forceinline__ void damped_solve(const double* nu, const double* g, double lam, double* s) {
-    double L[21];
-    double y[6];
+    // Dense 6x6 storage with compile-time indices only, so the factor stays in registers.
+    double U[6][6];
     int q = 0;
 #pragma unroll
     for (int i = 0; i < 6; ++i)
 #pragma unroll
-        for (int j = i; j < 6; ++j) {
-            double v = nu[q];
-            if (i == j) v = v + (lam * v + 1e-12);
-            L[q] = v;
-            ++q;
-        }
-    // In-place Cholesky of the upper triangle: U^T U = M (row-major upper storage).
-    auto at = [](int i, int j) { return i * 6 - (i * (i - 1)) / 2 + (j - i); };
+        for (int j = 0; j < 6; ++j)
+            if (j >= i) {
+                double v = nu[q++];
+                if (i == j) v = v + (lam * v + 1e-12);
+                U[i][j] = v;
+            }
+    // In-place Cholesky of the upper triangle: U^T U = M.
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        double d = L[at(i, i)];
+        double d = U[i][i];
 #pragma unroll
-        for (int k = 0; k < i; ++k) d -= L[at(k, i)] * L[at(k, i)];
+        for (int k = 0; k < 6; ++k)
+            if (k < i) d -= U[k][i] * U[k][i];
         d = sqrt(d);  // NaN when not positive definite
-        L[at(i, i)] = d;
+        U[i][i] = d;
         const double inv = 1.0 / d;
 #pragma unroll
-        for (int j = i + 1; j < 6; ++j) {
-            double v = L[at(i, j)];
+        for (int j = 0; j < 6; ++j)
+            if (j > i) {
+                double v = U[i][j];
 #pragma unroll
-            for (int k = 0; k < i; ++k) v -= L[at(k, i)] * L[at(k, j)];
-            L[at(i, j)] = v * inv;
-        }
+                for (int k = 0; k < 6; ++k)
+                    if (k < i) v -= U[k][i] * U[k][j];
+                U[i][j] = v * inv;
+            }
     }
     // U^T y = g, then U s = y.
+    double y[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         double v = g[i];
 #pragma unroll
-        for (int k = 0; k < i; ++k) v -= L[at(k, i)] * y[k];
-        y[i] = v / L[at(i, i)];
+        for (int k = 0; k < 6; ++k)
+            if (k < i) v -= U[k][i] * y[k];
+        y[i] = v / U[i][i];
     }
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
         double v = y[i];
 #pragma unroll
-        for (int k = i + 1; k < 6; ++k) v -= L[at(i, k)] * s[k];
-        s[i] = v / L[at(i, i)];
+        for (int k = 0; k < 6; ++k)
+            if (k > i) v -= U[i][k] * s[k];
+        s[i] = v / U[i][i];
     }
+}
+
+// Warp totals of the 27 sums on every lane with the additions of a butterfly all-reduce (the same
+// partial sums meet at every level, so the totals are identical to 27 separate butterflies) but as a
+// reduce-scatter: at each level a lane keeps half of its slots, adding its partner's copy of them,
+// so 31 additions and shuffles replace 135; lane i then holds total i and broadcasts it.
+__device__ __forceinline__ void warp_allreduce27(double* s, int lane) {
+    double a[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) a[i] = i < 27 ? s[i] : 0.0;
+#pragma unroll
+    for (int half = 16; half >= 1; half >>= 1) {
+        const bool upper = (lane & half) != 0;
+#pragma unroll
+        for (int j = 0; j < half; ++j) {
+            const double send = upper ? a[j] : a[j + half];
+            const double keep = upper ? a[j + half] : a[j];
+            a[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 27; ++i) s[i] = __shfl_sync(0xffffffffu, a[0], i);
+}
+
+// One pass over the pixels at params q: the 21 upper-triangle entries of J^T J and the 6 of J^T r
+// into s[0..26] and the cost sum of r^2 with r = v - A shape (numpy's model-then-residual order),
+// as warp totals identical on all lanes.
+__device__ __forceinline__ double warp_normal_pass(const double* q, const double* v, const int* xy, int n, int lane,
+                                                   double* s) {
+#pragma unroll
+    for (int i = 0; i < 27; ++i) s[i] = 0.0;
+    double acc = 0.0;
+    const double e1 = exp(q[3]), e3 = exp(q[5]);
+    for (int k = lane; k < n; k += 32) {
+        const int c = xy[k];
+        const double dx = (double)(c & 0xffff) - q[1], dy = (double)(c >> 16) - q[2];
+        const GaussEval g = gauss_eval(q, e1, e3, dx, dy);
+        const double model = q[0] * g.shape;
+        const double r = v[k] - model;
+        acc += r * r;
+        double J[6];
+        J[0] = g.shape;
+        J[1] = model * (g.a * e1);
+        J[2] = model * (g.a * q[4] + g.b * e3);
+        J[3] = -model * (g.a * e1 * dx);
+        J[4] = -model * (g.a * dy);
+        J[5] = -model * (g.b * e3 * dy);
+        int t = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int j = i; j < 6; ++j) s[t++] += J[i] * J[j];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s[21 + i] += J[i] * r;
+    }
+    warp_allreduce27(s, lane);
+    return warp_sum(acc);
 }
 
 // Fits p (ROI-local, identical on all lanes) to the n compacted pixels. Returns the number of
 // iterations run. `cap` is the cell's sigma cap, `amp_cap` 3 * max(max|v|, 1e-12).
+//
+// Each trial's cost is evaluated in the same pass as its normal equations: an accepted trial (the
+// usual case) hands its sums to the next iteration, a rejected one recomputes the sums at the kept
+// params. The arithmetic of every sum is that of separate Jacobian and cost passes.
 __device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int n, double cap, double amp_cap,
                            int max_iter, int lane) {
-    double cost = warp_cost(p, v, xy, n, lane);
+    double s[27];
+    double cost = warp_normal_pass(p, v, xy, n, lane, s);
     if (!isfinite(cost)) return 0;
     double lam = 1e-3;
     const double lo = -log(cap), hi = -log(kSigmaMin);
     int it = 0;
     for (; it < max_iter; ++it) {
-        double s[27];
-#pragma unroll
-        for (int i = 0; i < 27; ++i) s[i] = 0.0;
-        const double e1 = exp(p[3]), e3 = exp(p[5]);
-        for (int k = lane; k < n; k += 32) {
-            const int c = xy[k];
-            const double dx = (double)(c & 0xffff) - p[1], dy = (double)(c >> 16) - p[2];
-            const GaussEval g = gauss_eval(p, e1, e3, dx, dy);
-            const double model = p[0] * g.shape;
-            const double r = v[k] - model;
-            double J[6];
-            J[0] = g.shape;
-            J[1] = model * (g.a * e1);
-            J[2] = model * (g.a * p[4] + g.b * e3);
-            J[3] = -model * (g.a * e1 * dx);
-            J[4] = -model * (g.a * dy);
-            J[5] = -model * (g.b * e3 * dy);
-            int q = 0;
-#pragma unroll
-            for (int i = 0; i < 6; ++i)
-#pragma unroll
-                for (int j = i; j < 6; ++j) s[q++] += J[i] * J[j];
-#pragma unroll
-            for (int i = 0; i < 6; ++i) s[21 + i] += J[i] * r;
-        }
-#pragma unroll
-        for (int i = 0; i < 27; ++i) s[i] = warp_sum(s[i]);
         double step[6];
         damped_solve(s, s + 21, lam, step);
         double trial[6];
@@ -140,8 +167,6 @@ __device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int
         trial[0] = trial[0] < 0.0 ? 0.0 : (trial[0] > amp_cap ? amp_cap : trial[0]);
         trial[3] = trial[3] < lo ? lo : (trial[3] > hi ? hi : trial[3]);
         trial[5] = trial[5] < lo ? lo : (trial[5] > hi ? hi : trial[5]);
-        const double new_cost = warp_cost(trial, v, xy, n, lane);
-        const bool better = isfinite(new_cost) && new_cost <= cost;
         double smax = 0.0;
 #pragma unroll
         for (int i = 0; i < 6; ++i) smax = fmax(smax, fabs(step[i]));
@@ -149,6 +174,8 @@ __device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int
         bool small = smax < 1e-7;
 #pragma unroll
         for (int i = 0; i < 6; ++i) small = small && !isnan(step[i]);
+        const double new_cost = warp_normal_pass(trial, v, xy, n, lane, s);
+        const bool better = isfinite(new_cost) && new_cost <= cost;
         const bool done = (better && (cost - new_cost <= 1e-12 * fmax(cost, 1e-300))) || small;
         if (better) {
 #pragma unroll
@@ -159,6 +186,7 @@ __device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int
             lam *= 4.0;
         }
         if (done || lam > 1e12) { ++it; break; }
+        if (!better && it + 1 < max_iter) warp_normal_pass(p, v, xy, n, lane, s);
     }
     return it;
 }

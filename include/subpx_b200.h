@@ -314,12 +314,13 @@ typedef struct spx_method_out {
     double* centers;       /* n x 2 global [x, y] */
     double* contours;      /* n x (n_angles + 1) x 2 global, or null (metrics only) */
     uint8_t* status;       /* n status codes */
-    double* metrics;       /* n x n_metrics */
+    double* metrics;       /* n x n_metrics (row-major), or n_metrics columns of n (metric_col_stride) */
     double* center_local;  /* n x 2 (radial, logquad) */
     double* edge_px;       /* n x n_angles (radial) */
     double* eigenvalues;   /* n x 2 (ellipse methods) */
     double* axes;          /* n x 2 x 2 (ellipse methods) */
     int n_metrics;
+    long long metric_col_stride;  /* 0: row-major; else metric q of cell i at metrics[i + q * stride] */
 } spx_method_out;
 
 /* Half-maximum ellipses of the deblended Gaussian fits (params of cells `which`, ROI-local). */
