@@ -276,12 +276,11 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
 def _revise_seeds(dbl: Deblender, state, seeds_xy, pitch, oversized_d, *, drop_fraction=0.3, add_fraction=0.5):
     """Seeds to drop and holes to add after one deblending pass (subpx/_cpu/deblend.py:525-567)."""
     p = state.params
-    finite = np.isfinite(p).all(axis=1)
-    good = finite & (state.status_codes == 0) & (p[:, 0] > 0)
-    if not good.any():
+    # The median amplitude of the "ok" cells with A > 0 was taken on the device at the end of the
+    # pass ("ok" implies finite params).
+    reference = state.amplitude_median
+    if not np.isfinite(reference):
         return np.zeros(len(p), bool), np.zeros((0, 2))
-    reference = float(np.median(p[good, 0]))
-    drop = ~finite | (p[:, 0] < drop_fraction * reference)
     h, w = dbl.shape
     resid = dev.empty((h, w), torch.float64)
     _lib.call("spx_residual", dbl.img.data_ptr(), dbl.dtype, dbl.sign, h, w, state.background.struct(),
@@ -299,6 +298,9 @@ def _revise_seeds(dbl: Deblender, state, seeds_xy, pitch, oversized_d, *, drop_f
     maxf = resid  # reuse
     _lib.call("spx_maximum_filter", smooth.data_ptr(), h, w, radius, tmp.data_ptr(), maxf.data_ptr(),
               dev.stream_ptr())
+    # Host work while the filters run.
+    finite = np.isfinite(p).all(axis=1)
+    drop = ~finite | (p[:, 0] < drop_fraction * reference)
     count = dev.empty((1,), torch.int32)
     cap = 1 << 16
     peaks = dev.empty((cap, 2), torch.int32)

@@ -374,20 +374,36 @@ __global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const d
             }
             __syncthreads();
         }
+    // Each candidate's centre, radius, amplitude and precision factors are staged once per tile
+    // (chunks of 256), so a pixel term costs one exp.
+    __shared__ double s_cx[256], s_cy[256], s_r[256], s_a[256], s_e1[256], s_u2[256], s_e3[256];
     const int x = tx0 + (threadIdx.x % kRenderTile), y = ty0 + (threadIdx.x / kRenderTile);
-    if (x >= W || y >= H) return;
     double acc = 0.0;
-    for (int k = 0; k < m; ++k) {
-        const int id = cand[k];
-        const double r = (double)radius[id];
-        const double dx = (double)x - centres[2LL * id], dy = (double)y - centres[2LL * id + 1];
-        if (fabs(dx) > r || fabs(dy) > r) continue;
-        const double* p = params + 6LL * id;
-        const double aa = exp(p[3]) * dx + p[4] * dy, bb = exp(p[5]) * dy;
-        const double val = p[0] * exp(-0.5 * (aa * aa + bb * bb));
-        if (val != 0.0) acc += val;
+    for (int c0 = 0; c0 < m; c0 += 256) {
+        const int cn = min(256, m - c0);
+        if ((int)threadIdx.x < cn) {
+            const int id = cand[c0 + threadIdx.x];
+            const double* p = params + 6LL * id;
+            s_cx[threadIdx.x] = centres[2LL * id];
+            s_cy[threadIdx.x] = centres[2LL * id + 1];
+            s_r[threadIdx.x] = (double)radius[id];
+            s_a[threadIdx.x] = p[0];
+            s_e1[threadIdx.x] = exp(p[3]);
+            s_u2[threadIdx.x] = p[4];
+            s_e3[threadIdx.x] = exp(p[5]);
+        }
+        __syncthreads();
+        for (int k = 0; k < cn; ++k) {
+            const double r = s_r[k];
+            const double dx = (double)x - s_cx[k], dy = (double)y - s_cy[k];
+            if (fabs(dx) > r || fabs(dy) > r) continue;
+            const double aa = s_e1[k] * dx + s_u2[k] * dy, bb = s_e3[k] * dy;
+            const double val = s_a[k] * exp(-0.5 * (aa * aa + bb * bb));
+            if (val != 0.0) acc += val;
+        }
+        __syncthreads();
     }
-    model[(long long)y * W + x] = acc;
+    if (x < W && y < H) model[(long long)y * W + x] = acc;
 }
 
 // Cleaned cells (image - background - (model - own)) of the cells in `which` (all when null) as

@@ -84,7 +84,8 @@ def auto_tile(seeds_d: torch.Tensor, n: int, shape) -> tuple[int, float]:
     ws = dev.workspace(_lib.size("spx_voronoi_workspace_bytes", n, h, w))
     _lib.call("spx_nearest_distances", seeds_d.data_ptr(), n, seeds_d.data_ptr(), n, 1, h, w, out.data_ptr(),
               ws.data_ptr(), ws.numel(), dev.stream_ptr())
-    pitch = float(np.median(out.cpu().numpy()))
+    res = quantiles([_lib.QuantileReq(out.data_ptr(), 1, None, 0, n, 0, 0.0)])
+    pitch = float(res[0, 0])
     return int(np.clip(round(4 * pitch), 16, max(shape))), pitch
 
 
@@ -228,6 +229,7 @@ class DeblendState:
     background_info: dict
     converged: bool = False
     fit_iterations: list = field(default_factory=list)  # LM iterations per pass (device, int32)
+    amplitude_median: float = float("nan")  # median A of the "ok" cells with A > 0 (NaN if none)
 
     @property
     def status(self) -> np.ndarray:
@@ -298,10 +300,10 @@ class Deblender:
     def stats(self, params_d, status_d, maxstep_d=None):
         """Median amplitude and FWHM of the good cells (subpx/_cpu/deblend.py:463-464) and, given the
         steps, the 99th percentile of the finite ones (:517), computed on the device; one download.
-        Returns (amplitude, fwhm, p99, n_finite)."""
+        Returns (amplitude, fwhm, p99, n_finite, n_good)."""
         n = self.n
         if n == 0:
-            return 1.0, 0.0, np.nan, 0
+            return 1.0, 0.0, np.nan, 0, 0
         fwhm = dev.empty((n,), torch.float64)
         good = dev.empty((n,), torch.uint8)
         _lib.call("spx_cell_stats", params_d.data_ptr(), status_d.data_ptr(), n, fwhm.data_ptr(), good.data_ptr(),
@@ -314,8 +316,8 @@ class Deblender:
         amplitude = float(res[0, 0]) if res[0, 1] > 0 else 1.0
         width = float(res[1, 0]) if res[1, 1] > 0 else 0.0
         if maxstep_d is None:
-            return amplitude, width, np.nan, 0
-        return amplitude, width, float(res[2, 0]), int(res[2, 1])
+            return amplitude, width, np.nan, 0, int(res[0, 1])
+        return amplitude, width, float(res[2, 0]), int(res[2, 1]), int(res[0, 1])
 
     def background_of(self, model, stats):
         """Background map and info (subpx/_cpu/deblend.py:459-466 background_of, 323-393); stats =
@@ -418,7 +420,7 @@ class Deblender:
         bg, info = self.background_of(model, stats)
         self.check_render()
         return DeblendState(bg, model, params_d.cpu().numpy(), params_d, status_d.cpu().numpy(), status_d, self.tile,
-                            used, info, converged, fit_iters)
+                            used, info, converged, fit_iters, stats[0] if stats[4] else float("nan"))
 
     def check_render(self):
         """Raise if a render since the last check overflowed a tile's Gaussian list."""
