@@ -637,17 +637,6 @@ struct SplineWindow {
     }
 };
 
-// inside_bytes with a shortcut: when every mask byte the bilinear weights touch is set, the
-// weights sum to 1 within rounding and the sample is inside.
-__device__ __forceinline__ bool inside_fast(const uint8_t* m, int hm, int wm, double y, double x) {
-    if (!(y >= 0.0 && y <= (double)(hm - 1) && x >= 0.0 && x <= (double)(wm - 1))) return false;
-    const double fy = floor(y), fx = floor(x);
-    const bool ey = y == fy, ex = x == fx;
-    const uint8_t* r = m + (int)fy * wm + (int)fx;
-    if (r[0] && (ex || r[1]) && (ey || (r[wm] && (ex || r[wm + 1])))) return true;
-    return inside_bytes(m, hm, wm, y, x);
-}
-
 constexpr int kRadialThreads = 128;
 
 // Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients, a reduction
@@ -814,10 +803,23 @@ __global__ void __launch_bounds__(kRadialThreads, 4) k_radial_cd(
                 double best = -dinf(), gl = 0, gm = 0, gr = 0;
                 int best_j = -1, first_invalid = n_radii;
                 SplineWindow win;
+                int mfy = -1 << 30, mfx = -1 << 30;  // mask cell of the last sample and whether all
+                bool mfull = false;                   // four of its corners are in the eroded cell
                 for (int k = 0; k < n_radii; ++k) {
                     const double r = (double)k * radial_step;
                     const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
-                    if (!inside_fast(emask, hm, wm, y, x)) { first_invalid = k; break; }
+                    bool valid = y >= 0.0 && y <= (double)(hm - 1) && x >= 0.0 && x <= (double)(wm - 1);
+                    if (valid) {
+                        const int iy = (int)floor(y), ix = (int)floor(x);
+                        if (iy != mfy || ix != mfx) {
+                            mfy = iy;
+                            mfx = ix;
+                            const uint8_t* q = emask + iy * wm + ix;
+                            mfull = iy + 1 < hm && ix + 1 < wm && q[0] && q[1] && q[wm] && q[wm + 1];
+                        }
+                        valid = mfull || inside_bytes(emask, hm, wm, y, x);
+                    }
+                    if (!valid) { first_invalid = k; break; }
                     const double p = k == 0 ? peak : win.at(coef, hp, wp, y + kPad, x + kPad);
                     if (k >= 1 && !crossed && h1 >= half && p < half) {
                         edge_h = (double)(k - 1) * radial_step + ((h1 - half) / (h1 - p)) * radial_step;

@@ -321,7 +321,7 @@ __global__ void k_render_prep(const double* params, const int4* boxes, int n, in
     if ((threadIdx.x & 31) == 0) atomicMax(rmax, local);
 }
 
-constexpr int kRenderTile = 16;
+constexpr int kRenderTile = 32;  // 32x32 pixels per 256-thread block, four rows per thread
 constexpr int kRenderCap = 2048;
 
 // model(y, x) = sum over cells (increasing index) whose truncated square covers the pixel, each
@@ -358,31 +358,28 @@ __global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const d
         if (threadIdx.x == 0) atomicExch(overflow, 1);
         return;
     }
-    int m2 = 1;
-    while (m2 < m) m2 <<= 1;
-    for (int i = m + threadIdx.x; i < m2; i += blockDim.x) cand[i] = 0x7fffffff;
+    // Increasing cell order by rank: ids are distinct, so each candidate's slot is the number of
+    // smaller ids (one barrier instead of a bitonic network's log^2 m).
+    __shared__ int sorted[kRenderCap];
+    for (int t = threadIdx.x; t < m; t += blockDim.x) {
+        const int id = cand[t];
+        int rank = 0;
+        for (int q = 0; q < m; ++q) rank += cand[q] < id;
+        sorted[rank] = id;
+    }
     __syncthreads();
-    for (int len = 2; len <= m2; len <<= 1)
-        for (int stride = len >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < m2; i += blockDim.x) {
-                const int jx = i ^ stride;
-                if (jx > i) {
-                    const bool up = (i & len) == 0;
-                    const int u = cand[i], w = cand[jx];
-                    if (up ? u > w : u < w) { cand[i] = w; cand[jx] = u; }
-                }
-            }
-            __syncthreads();
-        }
     // Each candidate's centre, radius, amplitude and precision factors are staged once per tile
     // (chunks of 256), so a pixel term costs one exp.
     __shared__ double s_cx[256], s_cy[256], s_r[256], s_a[256], s_e1[256], s_u2[256], s_e3[256];
-    const int x = tx0 + (threadIdx.x % kRenderTile), y = ty0 + (threadIdx.x / kRenderTile);
-    double acc = 0.0;
+    constexpr int kRows = kRenderTile * kRenderTile / 256;
+    const int x = tx0 + (threadIdx.x % kRenderTile), yb = ty0 + (threadIdx.x / kRenderTile);
+    double acc[kRows];
+#pragma unroll
+    for (int q = 0; q < kRows; ++q) acc[q] = 0.0;
     for (int c0 = 0; c0 < m; c0 += 256) {
         const int cn = min(256, m - c0);
         if ((int)threadIdx.x < cn) {
-            const int id = cand[c0 + threadIdx.x];
+            const int id = sorted[c0 + threadIdx.x];
             const double* p = params + 6LL * id;
             s_cx[threadIdx.x] = centres[2LL * id];
             s_cy[threadIdx.x] = centres[2LL * id + 1];
@@ -395,15 +392,25 @@ __global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const d
         __syncthreads();
         for (int k = 0; k < cn; ++k) {
             const double r = s_r[k];
-            const double dx = (double)x - s_cx[k], dy = (double)y - s_cy[k];
-            if (fabs(dx) > r || fabs(dy) > r) continue;
-            const double aa = s_e1[k] * dx + s_u2[k] * dy, bb = s_e3[k] * dy;
-            const double val = s_a[k] * exp(-0.5 * (aa * aa + bb * bb));
-            if (val != 0.0) acc += val;
+            const double dx = (double)x - s_cx[k];
+            if (fabs(dx) > r) continue;
+#pragma unroll
+            for (int q = 0; q < kRows; ++q) {
+                const double dy = (double)(yb + q * (256 / kRenderTile)) - s_cy[k];
+                if (fabs(dy) > r) continue;
+                const double aa = s_e1[k] * dx + s_u2[k] * dy, bb = s_e3[k] * dy;
+                const double val = s_a[k] * exp(-0.5 * (aa * aa + bb * bb));
+                if (val != 0.0) acc[q] += val;
+            }
         }
         __syncthreads();
     }
-    if (x < W && y < H) model[(long long)y * W + x] = acc;
+    if (x < W)
+#pragma unroll
+        for (int q = 0; q < kRows; ++q) {
+            const int y = yb + q * (256 / kRenderTile);
+            if (y < H) model[(long long)y * W + x] = acc[q];
+        }
 }
 
 // Cleaned cells (image - background - (model - own)) of the cells in `which` (all when null) as
@@ -637,47 +644,106 @@ __device__ __forceinline__ bool q_select(const QuantileReq& r, int i, double* v)
     return true;
 }
 
-// k-th smallest selected value (0-based) by an 8-pass radix select over the global array.
-__device__ double block_kth(const QuantileReq& r, int k, int* hist, int* s_digit, int* s_k) {
-    unsigned long long prefix = 0, mask = 0;
-    if (threadIdx.x == 0) *s_k = k;
-    for (int shift = 56; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+constexpr int kQuantThreads = 1024;
+
+// Inclusive scan over the CTA's 1024 threads (the same totals on every call site).
+__device__ __forceinline__ int cta_incl_scan(int v, int* warp_tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_tot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        int w = warp_tot[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        warp_tot[lane] = w;
+    }
+    __syncthreads();
+    const int r = v + (warp ? warp_tot[warp - 1] : 0);
+    __syncthreads();
+    return r;
+}
+
+// Order key of the k-th smallest selected value (0-based): a radix select over 64-bit keys with
+// 11-bit digits (six passes over the values), each digit found by a CTA-wide prefix sum.
+__device__ unsigned long long cta_kth_key(const QuantileReq& r, int k, int* hist, int* warp_tot, int* s_pick) {
+    unsigned long long prefix = 0, pmask = 0;
+    int kk = k, shift = 64;
+    for (int pass = 0; pass < 6; ++pass) {
+        const int bits = pass < 5 ? 11 : 9, nb = 1 << bits;
+        shift -= bits;
+        for (int i = threadIdx.x; i < nb; i += kQuantThreads) hist[i] = 0;
         __syncthreads();
-        for (int i = threadIdx.x; i < r.n; i += blockDim.x) {
+        for (int i = threadIdx.x; i < r.n; i += kQuantThreads) {
             double v;
             if (!q_select(r, i, &v)) continue;
             const unsigned long long key = order_key(v);
-            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1);
+            if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int kk = *s_k, d = 0;
-            for (; d < 255; ++d) {
-                if (kk < hist[d]) break;
-                kk -= hist[d];
-            }
-            *s_digit = d;
-            *s_k = kk;
+        const int b0 = 2 * threadIdx.x;
+        const int c0 = b0 < nb ? hist[b0] : 0, c1 = b0 + 1 < nb ? hist[b0 + 1] : 0;
+        const int incl = cta_incl_scan(c0 + c1, warp_tot);
+        const int excl = incl - c0 - c1;
+        if (excl <= kk && kk < incl) {
+            const bool first = kk < excl + c0;
+            s_pick[0] = first ? b0 : b0 + 1;
+            s_pick[1] = first ? kk - excl : kk - excl - c0;
         }
         __syncthreads();
-        prefix |= (unsigned long long)(*s_digit) << shift;
-        mask |= 0xffull << shift;
+        prefix |= (unsigned long long)s_pick[0] << shift;
+        pmask |= (unsigned long long)(nb - 1) << shift;
+        kk = s_pick[1];
         __syncthreads();
     }
-    return key_value(prefix);
+    return prefix;
 }
 
-// One block per request: out[2 * b] = result (NaN when nothing is selected), out[2 * b + 1] = count.
-__global__ void __launch_bounds__(1024) k_quantiles(const QuantileReq* reqs, double* out) {
-    __shared__ int hist[256];
-    __shared__ int s_digit, s_k, s_count;
+// The key of the (k+1)-th smallest given the k-th's key: itself when at least k + 2 selected keys
+// are <= it, else the smallest key above it (one pass).
+__device__ unsigned long long cta_next_key(const QuantileReq& r, int k, unsigned long long key_k, int* s_cnt,
+                                           unsigned long long* s_min) {
+    if (threadIdx.x == 0) {
+        *s_cnt = 0;
+        *s_min = ~0ull;
+    }
+    __syncthreads();
+    int cnt = 0;
+    unsigned long long mn = ~0ull;
+    for (int i = threadIdx.x; i < r.n; i += kQuantThreads) {
+        double v;
+        if (!q_select(r, i, &v)) continue;
+        const unsigned long long key = order_key(v);
+        if (key <= key_k) ++cnt;
+        else mn = min(mn, key);
+    }
+    atomicAdd(s_cnt, cnt);
+    atomicMin(s_min, mn);
+    __syncthreads();
+    const unsigned long long out = *s_cnt >= k + 2 ? key_k : *s_min;
+    __syncthreads();
+    return out;
+}
+
+// One CTA per request: out[2 * b] = result (NaN when nothing is selected), out[2 * b + 1] = count.
+__global__ void __launch_bounds__(kQuantThreads) k_quantiles(const QuantileReq* reqs, double* out) {
+    __shared__ int hist[2048];
+    __shared__ int warp_tot[32];
+    __shared__ int s_pick[2];
+    __shared__ int s_count, s_nan;
+    __shared__ unsigned long long s_min;
     const QuantileReq r = reqs[blockIdx.x];
-    __shared__ int s_nan;
     if (threadIdx.x == 0) s_count = s_nan = 0;
     __syncthreads();
     int c = 0, nan = 0;
-    for (int i = threadIdx.x; i < r.n; i += blockDim.x) {
+    for (int i = threadIdx.x; i < r.n; i += kQuantThreads) {
         double v;
         if (q_select(r, i, &v)) {
             ++c;
@@ -688,19 +754,24 @@ __global__ void __launch_bounds__(1024) k_quantiles(const QuantileReq* reqs, dou
     atomicAdd(&s_nan, nan);
     __syncthreads();
     const int n = s_count;
+    const bool any_nan = s_nan != 0;
+    __syncthreads();
     double res = dnan();
-    if (n > 0 && s_nan == 0) {  // numpy: a NaN among the values makes the median / percentile NaN
+    if (n > 0 && !any_nan) {  // numpy: a NaN among the values makes the median / percentile NaN
         if (r.mode == 0) {
-            const double a = block_kth(r, (n - 1) / 2, hist, &s_digit, &s_k);
-            const double b = (n & 1) ? a : block_kth(r, n / 2, hist, &s_digit, &s_k);
+            const int k = (n - 1) / 2;
+            const unsigned long long ka = cta_kth_key(r, k, hist, warp_tot, s_pick);
+            const double a = key_value(ka);
+            const double b = (n & 1) ? a : key_value(cta_next_key(r, k, ka, &s_count, &s_min));
             res = __ddiv_rn(__dadd_rn(a, b), 2.0);
         } else {
             // numpy 'linear': virtual index (n - 1) q, _lerp of the neighbours.
             const double virt = __dmul_rn((double)(n - 1), r.q);
             const double below = floor(virt);
             const int lo = min(max((int)below, 0), n - 1), hi = min(lo + 1, n - 1);
-            const double a = block_kth(r, lo, hist, &s_digit, &s_k);
-            const double b = hi == lo ? a : block_kth(r, hi, hist, &s_digit, &s_k);
+            const unsigned long long ka = cta_kth_key(r, lo, hist, warp_tot, s_pick);
+            const double a = key_value(ka);
+            const double b = hi == lo ? a : key_value(cta_next_key(r, lo, ka, &s_count, &s_min));
             if (virt >= (double)(n - 1)) {
                 res = b;
             } else {
@@ -975,7 +1046,7 @@ int spx_quantiles(const void* requests, int n_requests, double* out, void* strea
     SPX_REQUIRE(n_requests >= 1 && n_requests <= 64, "between 1 and 64 requests");
     SPX_REQUIRE(requests && out, "null pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_quantiles<<<n_requests, 1024, 0, s>>>(static_cast<const QuantileReq*>(requests), out);
+    k_quantiles<<<n_requests, kQuantThreads, 0, s>>>(static_cast<const QuantileReq*>(requests), out);
     return check_launch("k_quantiles");
 }
 

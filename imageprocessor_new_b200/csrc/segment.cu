@@ -86,6 +86,39 @@ __global__ void k_minmax(const void* img, int dtype, int height, int width, int 
     }
 }
 
+// k_minmax for a contiguous, 16-byte aligned uint16 image: eight pixels per 16-byte load.
+__global__ void k_minmax_dense(const uint16_t* img, long long n, unsigned int* range) {
+    unsigned int lo = 0xffffffffu, hi = 0;
+    const uint4* v4 = reinterpret_cast<const uint4*>(img);
+    const long long n8 = n / 8;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n8;
+         k += (long long)gridDim.x * blockDim.x) {
+        const uint4 q = __ldg(v4 + k);
+        const unsigned int w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const unsigned int a = w[j] & 0xffffu, b = w[j] >> 16;
+            lo = min(lo, min(a, b));
+            hi = max(hi, max(a, b));
+        }
+    }
+    for (long long k = n8 * 8 + blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
+         k += (long long)gridDim.x * blockDim.x) {
+        const unsigned int v = img[k];
+        lo = min(lo, v);
+        hi = max(hi, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&range[0], lo);
+        atomicMax(&range[1], hi);
+    }
+}
+
 // Histogram of the sampled pixels into hist[65536] (pre-zeroed, u32).
 __global__ void k_histogram(const void* img, int dtype, int height, int width, int step,
                             int dense, const unsigned int* range, unsigned int* hist) {
@@ -175,11 +208,20 @@ __global__ void __launch_bounds__(1024) k_otsu_scan(const unsigned int* hist, in
     // The reference sums i*h[i] sequentially in double: every partial sum is an integer below 2^53,
     // hence exact, and equal to this integer sum.
     const double mu = __dmul_rn((double)mu_int, scale);
+    // The sequential loops below load eight bins ahead, so the loads are not on the recurrence's
+    // critical path.
+    constexpr int kAhead = 8;
     if (threadIdx.x == 0) {
         double q1 = 0.0;
-        for (int k = 0; k < n; ++k) {
-            q1 = __dadd_rn(q1, p_buf[k]);
-            q1_buf[k] = q1;
+        for (int k0 = 0; k0 < n; k0 += kAhead) {
+            double pb[kAhead];
+#pragma unroll
+            for (int j = 0; j < kAhead; ++j) pb[j] = k0 + j < n ? p_buf[k0 + j] : 0.0;
+#pragma unroll
+            for (int j = 0; j < kAhead; ++j) {
+                q1 = __dadd_rn(q1, pb[j]);
+                if (k0 + j < n) q1_buf[k0 + j] = q1;
+            }
         }
     }
     __syncthreads();
@@ -189,21 +231,34 @@ __global__ void __launch_bounds__(1024) k_otsu_scan(const unsigned int* hist, in
     const double one_minus_eps = __dsub_rn(1.0, eps);
     if (threadIdx.x == 0) {
         double mu1 = 0.0, q1_prev = 0.0;
-        for (int k = 0; k < n; ++k) {
-            const double q1 = q1_buf[k], p_i = p_buf[k];
-            mu1 = __dmul_rn(mu1, q1_prev);
-            q1_prev = q1;
-            const double q2 = __dsub_rn(1.0, q1);
-            if (fmin(q1, q2) < eps || fmax(q1, q2) > one_minus_eps) {
-                mu1_buf[k] = dnan();
-                continue;
+        for (int k0 = 0; k0 < n; k0 += kAhead) {
+            double qb[kAhead], pb[kAhead], yb[kAhead];
+#pragma unroll
+            for (int j = 0; j < kAhead; ++j) {
+                const bool in = k0 + j < n;
+                qb[j] = in ? q1_buf[k0 + j] : 0.0;
+                pb[j] = in ? p_buf[k0 + j] : 0.0;
+                yb[j] = in ? y_buf[k0 + j] : 0.0;
             }
-            const double a = __dadd_rn(mu1, __dmul_rn((double)(first + k), p_i));
-            const double y = y_buf[k];
-            const double q = __dmul_rn(a, y);
-            const double r = __fma_rn(-q, q1, a);
-            mu1 = __fma_rn(r, y, q);
-            mu1_buf[k] = mu1;
+#pragma unroll
+            for (int j = 0; j < kAhead; ++j) {
+                const int k = k0 + j;
+                if (k >= n) break;
+                const double q1 = qb[j], p_i = pb[j];
+                mu1 = __dmul_rn(mu1, q1_prev);
+                q1_prev = q1;
+                const double q2 = __dsub_rn(1.0, q1);
+                if (fmin(q1, q2) < eps || fmax(q1, q2) > one_minus_eps) {
+                    mu1_buf[k] = dnan();
+                    continue;
+                }
+                const double a = __dadd_rn(mu1, __dmul_rn((double)(first + k), p_i));
+                const double y = yb[j];
+                const double q = __dmul_rn(a, y);
+                const double r = __fma_rn(-q, q1, a);
+                mu1 = __fma_rn(r, y, q);
+                mu1_buf[k] = mu1;
+            }
         }
     }
     __syncthreads();
@@ -736,6 +791,16 @@ size_t spx_otsu_workspace_bytes(int dtype) {
     return a.used;
 }
 
+static int launch_minmax(const void* img, int dtype, int height, int width, int step, long long n, unsigned int* range,
+                         cudaStream_t s) {
+    if (step == 1 && dtype == SPX_U16 && (reinterpret_cast<uintptr_t>(img) % 16) == 0) {
+        k_minmax_dense<<<grid_for(n / 8 + 1, 256, 148 * 8), 256, 0, s>>>(static_cast<const uint16_t*>(img), n, range);
+        return check_launch("k_minmax_dense");
+    }
+    k_minmax<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(img, dtype, height, width, step, range);
+    return check_launch("k_minmax");
+}
+
 int spx_otsu(const void* img, int dtype, int height, int width, int step, double* threshold,
              void* workspace, size_t workspace_bytes, void* stream) {
     SPX_REQUIRE(dtype == SPX_U8 || dtype == SPX_U16, "Otsu thresholding needs a uint8 or uint16 image");
@@ -752,8 +817,7 @@ int spx_otsu(const void* img, int dtype, int height, int width, int step, double
     SPX_CUDA(cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, s));
     const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
     const long long n = (long long)hs * ws;
-    k_minmax<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(img, dtype, height, width, step, range);
-    if (int e = check_launch("k_minmax")) return e;
+    if (int e = launch_minmax(img, dtype, height, width, step, n, range, s)) return e;
     const size_t smem = kHistSmemBins * sizeof(unsigned int);
     SPX_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int dense = step == 1 && dtype == SPX_U16 && (reinterpret_cast<uintptr_t>(img) % 16) == 0;
@@ -777,8 +841,7 @@ int spx_histogram(const void* img, int dtype, int height, int width, int step, u
     SPX_CUDA(cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, s));
     const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
     const long long n = (long long)hs * ws;
-    k_minmax<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(img, dtype, height, width, step, range);
-    if (int e = check_launch("k_minmax")) return e;
+    if (int e = launch_minmax(img, dtype, height, width, step, n, range, s)) return e;
     const size_t smem = kHistSmemBins * sizeof(unsigned int);
     SPX_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int dense = step == 1 && dtype == SPX_U16 && (reinterpret_cast<uintptr_t>(img) % 16) == 0;
@@ -826,8 +889,7 @@ int spx_otsu_static(const void* img, int dtype, int height, int width, int step,
     if (int e = check_launch("k_zero_u32")) return e;
     k_range_init<<<1, 32, 0, s>>>(range);
     if (int e = check_launch("k_range_init")) return e;
-    k_minmax<<<grid_for(n, 256, 148 * 8), 256, 0, s>>>(img, dtype, height, width, step, range);
-    if (int e = check_launch("k_minmax")) return e;
+    if (int e = launch_minmax(img, dtype, height, width, step, n, range, s)) return e;
     const size_t smem = kHistSmemBins * sizeof(unsigned int);
     SPX_CUDA(cudaFuncSetAttribute(k_histogram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int dense = step == 1 && dtype == SPX_U16 && (reinterpret_cast<uintptr_t>(img) % 16) == 0;
