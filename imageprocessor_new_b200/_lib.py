@@ -44,6 +44,14 @@ class MethodOut(ctypes.Structure):
                 ("n_metrics", c_int), ("metric_col_stride", c_longlong)]
 
 
+class GemmEpilogue(ctypes.Structure):
+    """spx_gemm_epilogue."""
+
+    _fields_ = [("scale", ctypes.c_float), ("bias", c_void_p), ("relu", c_int), ("mask_act", c_void_p),
+                ("ld_mask", c_int), ("out_f32", c_void_p), ("ld_f32", c_int), ("accumulate", c_int),
+                ("out_bf16", c_void_p), ("ld_bf16", c_int), ("out_bf16_t", c_void_p), ("ld_t", c_int)]
+
+
 _BG = POINTER(BgMap)
 _MO = POINTER(MethodOut)
 
@@ -58,6 +66,7 @@ SIGNATURES = {
     "spx_otsu_static": (_I, [_P, _I, _I, _I, _I, _P, _P]),
     "spx_triangle": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
+    "spx_gemm_bf16": (_I, [_P, _I, _P, _I, _I, _I, _I, POINTER(GemmEpilogue), _P, _P]),
     "spx_histogram": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
     "spx_otsu_from_histogram": (_I, [_P, _I, _P, c_longlong, _P, _P, _S, _P]),
     "spx_binarize": (_I, [_P, _I, _I, _I, _P, _D, _I, _P, _P]),

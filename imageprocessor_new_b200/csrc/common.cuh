@@ -74,6 +74,20 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 
+// (i / d, i % d) of a non-negative pixel index: 32-bit division when the index fits in 31 bits
+// (every image up to 2^31 pixels), 64-bit otherwise.
+__device__ __forceinline__ void divmod_idx(long long i, int d, int* q, int* r) {
+    if (i <= 0x7fffffffLL) {
+        const int ii = (int)i, qq = ii / d;
+        *q = qq;
+        *r = ii - qq * d;
+    } else {
+        const long long qq = i / d;
+        *q = (int)qq;
+        *r = (int)(i - qq * d);
+    }
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -421,8 +421,8 @@ __global__ void k_clean_stack(Image img, const int* vor, const int4* boxes, cons
     const long long total = (long long)n_out * hm * wm;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t / ((long long)hm * wm));
-        const int k = (int)(t % ((long long)hm * wm));
+        int c, k;
+        divmod_idx(t, hm * wm, &c, &k);
         const int yy = k / wm, xx = k % wm;
         const int j = which ? which[c] : c;
         const int4 b = boxes[j];
@@ -466,7 +466,8 @@ struct TileSel {
     const uint8_t* usable;    // null: all usable
     int mode;                 // SPX_TILE_FREE: model < thr_model & dist >= thr_dist; SPX_TILE_USABLE; SPX_TILE_ALL
     double thr_model, thr_dist;
-    __device__ __forceinline__ bool select(long long i, double* value) const {
+    __device__ __forceinline__ bool select(int y, int x, double* value) const {
+        const long long i = (long long)y * img.W + x;
         const double m = model ? model[i] : 0.0;
         if (mode != SPX_TILE_ALL) {
             if (usable && !usable[i]) return false;
@@ -475,19 +476,75 @@ struct TileSel {
                 if (!(sqrt((double)d2[i]) >= thr_dist)) return false;
             }
         }
-        const int y = (int)(i / img.W), x = (int)(i % img.W);
         *value = img.at(y, x) - m;
         return true;
     }
 };
+
+// Inclusive scan of one int per thread over a CTA of NT threads (NT / 32 <= 32 warps).
+template <int NT>
+__device__ __forceinline__ int cta_incl_scan(int v, int* warp_tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_tot[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < NT / 32 ? warp_tot[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        if (lane < NT / 32) warp_tot[lane] = w;
+    }
+    __syncthreads();
+    const int r = v + (warp ? warp_tot[warp - 1] : 0);
+    __syncthreads();
+    return r;
+}
+
+// One radix pass of a CTA-wide select: hist[2048] holds the counts of the current 11-bit (last: 9-bit)
+// digit among the keys that match the prefix so far; finds the digit holding the kk-th key and
+// the rank inside it. NT threads, each owning 2048 / NT consecutive bins.
+template <int NT>
+__device__ __forceinline__ void cta_pick_digit(const int* hist, int nb, int kk, int* warp_tot, int* s_pick) {
+    constexpr int per = 2048 / NT;
+    const int b0 = per * threadIdx.x;
+    int c[per];
+    int mine = 0;
+#pragma unroll
+    for (int j = 0; j < per; ++j) {
+        c[j] = b0 + j < nb ? hist[b0 + j] : 0;
+        mine += c[j];
+    }
+    const int incl = cta_incl_scan<NT>(mine, warp_tot);
+    int excl = incl - mine;
+    if (excl <= kk && kk < incl) {
+#pragma unroll
+        for (int j = 0; j < per; ++j) {
+            if (kk < excl + c[j]) {
+                s_pick[0] = b0 + j;
+                s_pick[1] = kk - excl;
+                break;
+            }
+            excl += c[j];
+        }
+    }
+    __syncthreads();
+}
 
 // Median (mean of the two middle values, NaN when empty) and count of the selected residuals of
 // each tile, by an 8-pass radix select on order-preserving 64-bit keys.
 __global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int tile, int nx, int smem_keys,
                                                               double* medians, long long* counts) {
     extern __shared__ unsigned long long keys[];
-    __shared__ int hist[256];
-    __shared__ int s_count, s_digit, s_k;
+    __shared__ int hist[2048];
+    __shared__ int warp_tot[32], s_pick[2];
+    __shared__ int s_count;
     __shared__ unsigned long long s_min;
     __shared__ int s_le;
     const int ty = blockIdx.x / nx, tx = blockIdx.x % nx;
@@ -497,10 +554,10 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int t
     if (threadIdx.x == 0) s_count = 0;
     __syncthreads();
     // Pass 0: count and (when they fit) stage the keys.
-    for (long long k = threadIdx.x; k < P; k += blockDim.x) {
-        const long long i = (long long)(y0 + k / tw) * sel.img.W + (x0 + k % tw);
+    for (int k = threadIdx.x; k < (int)P; k += blockDim.x) {
+        const int yy = k / tw, xx = k - yy * tw;
         double v;
-        if (sel.select(i, &v)) {
+        if (sel.select(y0 + yy, x0 + xx, &v)) {
             const int slot = atomicAdd(&s_count, 1);
             if (slot < smem_keys) keys[slot] = order_key(v);
         }
@@ -512,10 +569,10 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int t
         if (in_smem) {
             for (int i = threadIdx.x; i < c; i += blockDim.x) fn(keys[i]);
         } else {
-            for (long long k = threadIdx.x; k < P; k += blockDim.x) {
-                const long long i = (long long)(y0 + k / tw) * sel.img.W + (x0 + k % tw);
+            for (int k = threadIdx.x; k < (int)P; k += blockDim.x) {
+                const int yy = k / tw, xx = k - yy * tw;
                 double v;
-                if (sel.select(i, &v)) fn(order_key(v));
+                if (sel.select(y0 + yy, x0 + xx, &v)) fn(order_key(v));
             }
         }
     };
@@ -526,28 +583,22 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int t
         }
         return;
     }
-    // k-th smallest key (k = (c - 1) / 2).
+    // k-th smallest key (k = (c - 1) / 2): radix select with 11-bit digits (six passes).
     unsigned long long prefix = 0, mask = 0;
-    if (threadIdx.x == 0) s_k = (c - 1) / 2;
-    for (int shift = 56; shift >= 0; shift -= 8) {
-        for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+    int kk = (c - 1) / 2, shift = 64;
+    for (int pass = 0; pass < 6; ++pass) {
+        const int bits = pass < 5 ? 11 : 9, nb = 1 << bits;
+        shift -= bits;
+        for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
         __syncthreads();
         for_keys([&](unsigned long long key) {
-            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1);
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
         });
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int k = s_k, d = 0;
-            for (; d < 255; ++d) {
-                if (k < hist[d]) break;
-                k -= hist[d];
-            }
-            s_digit = d;
-            s_k = k;
-        }
-        __syncthreads();
-        prefix |= (unsigned long long)s_digit << shift;
-        mask |= 0xffull << shift;
+        cta_pick_digit<kTileThreads>(hist, nb, kk, warp_tot, s_pick);
+        prefix |= (unsigned long long)s_pick[0] << shift;
+        mask |= (unsigned long long)(nb - 1) << shift;
+        kk = s_pick[1];
         __syncthreads();
     }
     const unsigned long long k1 = prefix;
@@ -581,7 +632,8 @@ __global__ void k_bg_rows(const double* medians, int ny, int nx, int tile, int W
     const long long total = (long long)ny * W;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(t / W), x = (int)(t % W);
+        int j, x;
+        divmod_idx(t, W, &j, &x);
         const double* fp = medians + (long long)j * nx;
         auto xc = [&](int i) { return (double)(i * tile + min((i + 1) * tile, W) - 1) / 2.0; };
         const double xv = (double)x;
@@ -617,7 +669,8 @@ __global__ void k_residual(Image img, spx_bgmap bg, const double* model, double*
     const long long total = (long long)img.H * img.W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / img.W), x = (int)(i % img.W);
+        int y, x;
+        divmod_idx(i, img.W, &y, &x);
         out[i] = (img.at(y, x) - bg_at(bg, y, x)) - model[i];
     }
 }
@@ -646,31 +699,6 @@ __device__ __forceinline__ bool q_select(const QuantileReq& r, int i, double* v)
 
 constexpr int kQuantThreads = 1024;
 
-// Inclusive scan over the CTA's 1024 threads (the same totals on every call site).
-__device__ __forceinline__ int cta_incl_scan(int v, int* warp_tot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += u;
-    }
-    if (lane == 31) warp_tot[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        int w = warp_tot[lane];
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += u;
-        }
-        warp_tot[lane] = w;
-    }
-    __syncthreads();
-    const int r = v + (warp ? warp_tot[warp - 1] : 0);
-    __syncthreads();
-    return r;
-}
-
 // Order key of the k-th smallest selected value (0-based): a radix select over 64-bit keys with
 // 11-bit digits (six passes over the values), each digit found by a CTA-wide prefix sum.
 __device__ unsigned long long cta_kth_key(const QuantileReq& r, int k, int* hist, int* warp_tot, int* s_pick) {
@@ -688,16 +716,7 @@ __device__ unsigned long long cta_kth_key(const QuantileReq& r, int k, int* hist
             if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
         }
         __syncthreads();
-        const int b0 = 2 * threadIdx.x;
-        const int c0 = b0 < nb ? hist[b0] : 0, c1 = b0 + 1 < nb ? hist[b0 + 1] : 0;
-        const int incl = cta_incl_scan(c0 + c1, warp_tot);
-        const int excl = incl - c0 - c1;
-        if (excl <= kk && kk < incl) {
-            const bool first = kk < excl + c0;
-            s_pick[0] = first ? b0 : b0 + 1;
-            s_pick[1] = first ? kk - excl : kk - excl - c0;
-        }
-        __syncthreads();
+        cta_pick_digit<kQuantThreads>(hist, nb, kk, warp_tot, s_pick);
         prefix |= (unsigned long long)s_pick[0] << shift;
         pmask |= (unsigned long long)(nb - 1) << shift;
         kk = s_pick[1];

@@ -74,7 +74,8 @@ __global__ void k_gauss_1d(const double* in, int H, int W, const double* w, int 
     const long long total = (long long)H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / W), x = (int)(i % W);
+        int y, x;
+        divmod_idx(i, W, &y, &x);
         auto at = [&](int o) {
             if (along_y) return in[(long long)min(max(y + o, 0), H - 1) * W + x];
             return in[(long long)y * W + min(max(x + o, 0), W - 1)];
@@ -89,7 +90,8 @@ __global__ void k_max_1d(const double* in, int H, int W, int r, int along_y, dou
     const long long total = (long long)H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / W), x = (int)(i % W);
+        int y, x;
+        divmod_idx(i, W, &y, &x);
         double m = -dinf();
         for (int o = -r; o <= r; ++o) {
             const double v = along_y ? in[(long long)min(max(y + o, 0), H - 1) * W + x]
@@ -124,8 +126,10 @@ __global__ void k_peaks(const double* smooth, const double* maxf, const uint8_t*
         if (s == maxf[i] && s > level && !(exclude && exclude[i])) {
             const int slot = atomicAdd(count, 1);
             if (slot < capacity) {
-                out[2 * slot] = (int)(i / W);
-                out[2 * slot + 1] = (int)(i % W);
+                int y, x;
+                divmod_idx(i, W, &y, &x);
+                out[2 * slot] = y;
+                out[2 * slot + 1] = x;
             }
         }
     }
@@ -147,7 +151,8 @@ __global__ void k_dilate_cross4(const uint32_t* in, int H, int W4, uint32_t* out
     const long long total = (long long)H * W4;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / W4), xw = (int)(i % W4);
+        int y, xw;
+        divmod_idx(i, W4, &y, &xw);
         const uint32_t v = in[i];
         uint32_t d = v | (v << 8) | (v >> 8);
         if (y > 0) d |= in[i - W4];
@@ -163,7 +168,8 @@ __global__ void k_dilate_cross(const uint8_t* in, int H, int W, uint8_t* out) {
     const long long total = (long long)H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / W), x = (int)(i % W);
+        int y, x;
+        divmod_idx(i, W, &y, &x);
         uint8_t v = in[i];
         if (!v) v = (y > 0 && in[i - W]) || (y < H - 1 && in[i + W]) || (x > 0 && in[i - 1]) || (x < W - 1 && in[i + 1]);
         out[i] = v;

@@ -1,0 +1,194 @@
+// The learned warm start of the LM fits: a 1024 -> 256 -> 256 -> 7 MLP on 32x32 cell patches.
+//
+// GEMMs run on the 5th-generation tensor cores: one CTA of 128 threads computes a 128 x BN tile of
+// C = A B^T (A: M x K, B: N x K, both bf16 and K-contiguous) with the accumulator in TMEM. Operand
+// tiles of 64 K are copied into a two-stage ring of 128-byte-swizzled shared-memory tiles with
+// cp.async; thread 0 issues four tcgen05.mma (K = 16 each) per stage and commits them to the
+// stage's mbarrier, which gates the reuse of that stage. The epilogue reads TMEM with tcgen05.ld
+// (warp w owns rows 32w..32w+31) and applies scale, bias, ReLU or the ReLU derivative of a forward
+// activation, and writes f32 and/or bf16 outputs, row-major or transposed (the transposed copies
+// feed the weight-gradient GEMMs, whose reduction runs over the batch).
+//
+// Every wait on an mbarrier is bounded; a wait that runs out sets the error flag and the kernel
+// still frees its TMEM.
+
+#include <cuda_bf16.h>
+
+#include "umma.cuh"
+
+namespace spx {
+namespace {
+
+constexpr int kGemmThreads = 128;
+constexpr int kGemmBM = 128;
+constexpr int kGemmBK = 64;
+constexpr long long kWaitLimit = 1ll << 24;
+
+struct GemmEpi {
+    float scale;
+    const float* bias;
+    int relu;
+    const __nv_bfloat16* mask_act;
+    int ld_mask;
+    float* out_f32;
+    int ld_f32;
+    int accumulate;
+    __nv_bfloat16* out_bf16;
+    int ld_bf16;
+    __nv_bfloat16* out_bf16_t;
+    int ld_t;
+};
+
+// Copies rows [r0, r0 + rows) x K-block kb of a K-contiguous bf16 matrix into a swizzled tile,
+// zero past `valid_rows` and past K.
+__device__ __forceinline__ void load_tile(uint8_t* tile, const __nv_bfloat16* src, int ld, int r0, int rows,
+                                          int valid_rows, int kb, int K) {
+    const int chunks = rows * 8;
+    for (int c = threadIdx.x; c < chunks; c += kGemmThreads) {
+        const int r = c >> 3, ch = c & 7;
+        const int k = kb * kGemmBK + ch * 8;
+        const int row = r0 + r;
+        int bytes = 0;
+        const __nv_bfloat16* p = src;
+        if (row < valid_rows && k < K) {
+            bytes = min(16, (K - k) * 2);
+            p = src + (long long)row * ld + k;
+        }
+        cp_async16(tile + r * 128 + ((ch ^ (r & 7)) << 4), p, bytes);
+    }
+}
+
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
+                                                            int ldb, int M, int N, int K, int BN, uint32_t tmem_cols,
+                                                            GemmEpi ep, int* err) {
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte aligned stages: [A0 | B0 | A1 | B1], then two mbarriers and the TMEM address.
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int a_bytes = kGemmBM * 128, b_bytes = BN * 128;
+    uint8_t* stage_a[2] = {base, base + a_bytes + b_bytes};
+    uint8_t* stage_b[2] = {base + a_bytes, base + 2 * a_bytes + b_bytes};
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+    const int warp = threadIdx.x >> 5;
+    const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
+
+    if (warp == 0) tmem_alloc(tmem_slot, tmem_cols);
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t idesc = umma_idesc_bf16(kGemmBM, BN);
+    const int nk = (K + kGemmBK - 1) / kGemmBK;
+    bool ok = true;
+
+    load_tile(stage_a[0], A, lda, m0, kGemmBM, M, 0, K);
+    load_tile(stage_b[0], B, ldb, n0, BN, N, 0, K);
+    cp_async_commit();
+    for (int kb = 0; kb < nk; ++kb) {
+        const int s = kb & 1;
+        if (kb + 1 < nk) {
+            const int s2 = (kb + 1) & 1;
+            if (kb + 1 >= 2) ok = ok && mbar_wait(&mbar[s2], ((kb - 1) >> 1) & 1, kWaitLimit);
+            load_tile(stage_a[s2], A, lda, m0, kGemmBM, M, kb + 1, K);
+            load_tile(stage_b[s2], B, ldb, n0, BN, N, kb + 1, K);
+            cp_async_commit();
+            asm volatile("cp.async.wait_group 1;\n" : : : "memory");
+        } else {
+            cp_async_wait_all();
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint64_t ad = umma_desc_sw128(smem_u32(stage_a[s]));
+            const uint64_t bd = umma_desc_sw128(smem_u32(stage_b[s]));
+#pragma unroll
+            for (int k = 0; k < kGemmBK / 16; ++k)
+                umma_bf16(tmem, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
+                          (kb > 0 || k > 0) ? 1u : 0u);
+            umma_commit(&mbar[s]);
+        }
+    }
+    // The last commit covers every MMA of the tile.
+    ok = mbar_wait(&mbar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, kWaitLimit) && ok;
+    tc_fence_after();
+    if (!ok && threadIdx.x == 0) atomicExch(err, 1);
+
+    if (ok) {
+        const int m = m0 + warp * 32 + (threadIdx.x & 31);
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float v[16];
+            tmem_ld16(lane_addr + (uint32_t)c0, v);
+            if (m >= M) continue;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const int n = n0 + c0 + i;
+                if (n >= N) break;
+                float x = v[i] * ep.scale;
+                if (ep.bias) x += ep.bias[n];
+                if (ep.mask_act && !(__bfloat162float(ep.mask_act[(long long)m * ep.ld_mask + n]) > 0.0f)) x = 0.0f;
+                if (ep.relu) x = fmaxf(x, 0.0f);
+                if (ep.out_f32) {
+                    float* o = ep.out_f32 + (long long)m * ep.ld_f32 + n;
+                    *o = ep.accumulate ? *o + x : x;
+                }
+                if (ep.out_bf16) ep.out_bf16[(long long)m * ep.ld_bf16 + n] = __float2bfloat16_rn(x);
+                if (ep.out_bf16_t) ep.out_bf16_t[(long long)n * ep.ld_t + m] = __float2bfloat16_rn(x);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, tmem_cols);
+}
+
+size_t gemm_smem(int BN) { return 2 * (size_t)(kGemmBM * 128 + BN * 128) + 64 + 1024; }
+
+}  // namespace
+}  // namespace spx
+
+using namespace spx;
+
+extern "C" {
+
+int spx_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int N, int K, const spx_gemm_epilogue* epi,
+                  int* error_flag, void* stream) {
+    SPX_REQUIRE(M > 0 && N > 0 && K > 0 && lda >= K && ldb >= K, "bad GEMM shape");
+    SPX_REQUIRE(lda % 8 == 0 && ldb % 8 == 0, "lda and ldb must be multiples of 8 (16-byte rows)");
+    SPX_REQUIRE(A && B && epi && error_flag, "null pointer");
+    SPX_REQUIRE(reinterpret_cast<uintptr_t>(A) % 16 == 0 && reinterpret_cast<uintptr_t>(B) % 16 == 0,
+                "operands must be 16-byte aligned");
+    SPX_REQUIRE(epi->out_f32 || epi->out_bf16 || epi->out_bf16_t, "no output");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // Column tile: all of N up to 256 (a multiple of 16), else 256-wide tiles.
+    const int BN = N >= 256 ? 256 : ((N + 15) / 16) * 16;
+    uint32_t cols = 32;
+    while ((int)cols < BN) cols <<= 1;
+    const size_t smem = gemm_smem(BN);
+    SPX_CUDA(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GemmEpi ep{epi->scale,
+               epi->bias,
+               epi->relu,
+               static_cast<const __nv_bfloat16*>(epi->mask_act),
+               epi->ld_mask,
+               epi->out_f32,
+               epi->ld_f32,
+               epi->accumulate,
+               static_cast<__nv_bfloat16*>(epi->out_bf16),
+               epi->ld_bf16,
+               static_cast<__nv_bfloat16*>(epi->out_bf16_t),
+               epi->ld_t};
+    const dim3 grid((M + kGemmBM - 1) / kGemmBM, (N + BN - 1) / BN);
+    k_gemm_bf16<<<grid, kGemmThreads, smem, s>>>(static_cast<const __nv_bfloat16*>(A), lda,
+                                                 static_cast<const __nv_bfloat16*>(B), ldb, M, N, K, BN, cols, ep,
+                                                 error_flag);
+    return check_launch("k_gemm_bf16");
+}
+
+}  // extern "C"

@@ -70,7 +70,9 @@ __global__ void k_minmax(const void* img, int dtype, int height, int width, int 
     unsigned int lo = 0xffffffffu, hi = 0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
          k += (long long)gridDim.x * blockDim.x) {
-        const long long y = k / ws, x = k % ws;
+        int yi, xi;
+        divmod_idx(k, ws, &yi, &xi);
+        const long long y = yi, x = xi;
         const unsigned int v = px_u(img, dtype, y * step * (long long)width + x * step);
         lo = min(lo, v);
         hi = max(hi, v);
@@ -161,7 +163,9 @@ __global__ void k_histogram(const void* img, int dtype, int height, int width, i
     } else {
         for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
              k += (long long)gridDim.x * blockDim.x) {
-            const long long y = k / ws, x = k % ws;
+            int yi, xi;
+        divmod_idx(k, ws, &yi, &xi);
+        const long long y = yi, x = xi;
             const unsigned int v = px_u(img, dtype, y * step * (long long)width + x * step);
             if (in_smem) atomicAdd(&sh[v - lo], 1u);
             else atomicAdd(&hist[v], 1u);
@@ -439,7 +443,8 @@ __global__ void k_border_merge(Geo g, int* parents, unsigned int* roots, int til
     const long long total = (long long)tiles_x * tiles_y * per_tile;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
          k += (long long)gridDim.x * blockDim.x) {
-        const int tile = (int)(k / per_tile), e = (int)(k % per_tile);
+        int tile, e;
+        divmod_idx(k, per_tile, &tile, &e);
         const int tx0 = (tile % tiles_x) * kTileW, ty0 = (tile / tiles_x) * kTileH;
         int y, x;
         if (e < kTileW) { y = ty0; x = tx0 + e; }
@@ -742,7 +747,8 @@ __global__ void k_morph_cross(const uint8_t* in, int H, int W, int dilate, uint8
     const long long total = (long long)H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int y = (int)(i / W), x = (int)(i % W);
+        int y, x;
+        divmod_idx(i, W, &y, &x);
         unsigned v = in[i];
         if (dilate) {
             if (y > 0) v = max(v, (unsigned)in[i - W]);

@@ -338,6 +338,35 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
                   int wm, int width, int n_angles, double radial_step, const spx_method_out* halfmax,
                   const spx_method_out* gradient, void* workspace, size_t workspace_bytes, void* stream);
 
+
+/* ------------------------------------------------------------------ learned warm start (MLP) */
+
+/* Epilogue of spx_gemm_bf16: x = scale * acc (+ bias[n]); x = 0 where mask_act[m, n] <= 0 (the
+ * ReLU derivative of a forward activation, bf16, row stride ld_mask) when mask_act is set;
+ * x = max(x, 0) when relu; then any of: out_f32[m, n] (= or += with accumulate), out_bf16[m, n],
+ * out_bf16_t[n, m] (transposed). */
+typedef struct spx_gemm_epilogue {
+    float scale;
+    const float* bias;
+    int relu;
+    const void* mask_act;
+    int ld_mask;
+    float* out_f32;
+    int ld_f32;
+    int accumulate;
+    void* out_bf16;
+    int ld_bf16;
+    void* out_bf16_t;
+    int ld_t;
+} spx_gemm_epilogue;
+
+/* C (M x N) = A (M x K) B^T (B: N x K), bf16 operands with K contiguous (row strides lda, ldb,
+ * multiples of 8 elements, 16-byte aligned), f32 accumulation in TMEM by tcgen05.mma, then the
+ * epilogue. *error_flag (device int) is set to 1 if a completion wait gave up. No reference
+ * counterpart: this and the MLP entry points below implement the learned warm start of the LM fits. */
+int spx_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int N, int K, const spx_gemm_epilogue* epi,
+                  int* error_flag, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
