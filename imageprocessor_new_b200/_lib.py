@@ -67,6 +67,17 @@ SIGNATURES = {
     "spx_triangle": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
     "spx_gemm_bf16": (_I, [_P, _I, _P, _I, _I, _I, _I, POINTER(GemmEpilogue), _P, _P]),
+    "spx_deblend_initial_warm": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _D, _I, _I, _P, _P, _P, _P,
+                                      _P, _P, _P, _P, _S, _P]),
+    "spx_mlp_loss_grad": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _P, _P]),
+    "spx_rowsum_bf16": (_I, [_P, _I, _I, _P, _P]),
+    "spx_adamw": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                       ctypes.c_float, _P, _I, _P, _I, _P]),
+    "spx_transpose_bf16": (_I, [_P, _I, _I, _P, _P]),
+    "spx_mlp_outputs_to_params": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
+    "spx_extract_patches": (_I, [_P, _I, _D, _I, _I, _P, _I, _P, _P, _P]),
+    "spx_hole_coverage": (_I, [_I, _I, _P, _P, _P, _I, _I, _D, _I, _P, _P]),
+    "spx_page_finish": (_I, [_P, c_longlong, _D, _D, _D, ctypes.c_ulonglong, _P, _P]),
     "spx_histogram": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
     "spx_otsu_from_histogram": (_I, [_P, _I, _P, c_longlong, _P, _P, _S, _P]),
     "spx_binarize": (_I, [_P, _I, _I, _I, _P, _D, _I, _P, _P]),

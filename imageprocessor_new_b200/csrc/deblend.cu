@@ -139,8 +139,17 @@ struct FitArgs {
 };
 
 // Initial fit: 10th-percentile cell-border background, initial_params, LM, status.
+// Optional warm start of the initial fits: per-cell starting params (ROI-local) with a validity
+// flag; the border background and whether the plain start had to be used are reported.
+struct WarmStart {
+    const double* params;
+    const uint8_t* ok;
+    double* background;
+    uint8_t* fallback;
+};
+
 __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
-                              double* params, uint8_t* status, int* iters) {
+                              double* params, uint8_t* status, int* iters, WarmStart warm) {
     extern __shared__ unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double* v;
@@ -223,11 +232,38 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
         const double sigma = sqrt(fmax(var, 0.25));
         double p[6] = {fmax(peak, 1e-12), sx, sy, -log(sigma), 0.0, -log(sigma)};
         const double cap = a.caps[j];
-        const int it = warp_lm_fit(p, v, xy, n, cap, 3.0 * fmax(amax, 1e-12), a.max_iter, lane);
+        const double amp_cap = 3.0 * fmax(amax, 1e-12);
+        int it = 0, st = 0;
+        bool fell_back = false, done = false;
+        if (warm.params && (!warm.ok || warm.ok[j])) {
+            // Warm start: LM from the predicted params; kept when it meets the stop rule within
+            // max_iter and ends "ok", else the plain start below runs as well.
+            double q[6];
+            bool finite = true;
+            for (int i = 0; i < 6; ++i) {
+                q[i] = warm.params[6LL * j + i];
+                finite = finite && isfinite(q[i]);
+            }
+            if (finite && q[0] > 0.0) {
+                it = warp_lm_fit(q, v, xy, n, cap, amp_cap, a.max_iter, lane);
+                st = fit_status_of(q, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
+                if (it < a.max_iter && st == SPX_ST_OK) {
+                    for (int i = 0; i < 6; ++i) p[i] = q[i];
+                    done = true;
+                }
+            }
+            fell_back = !done;
+        }
+        if (!done) {
+            it += warp_lm_fit(p, v, xy, n, cap, amp_cap, a.max_iter, lane);
+            st = fit_status_of(p, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
+        }
         if (lane == 0) {
             for (int i = 0; i < 6; ++i) params[6LL * j + i] = p[i];
-            status[j] = (uint8_t)fit_status_of(p, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
+            status[j] = (uint8_t)st;
             if (iters) iters[j] = it;
+            if (warm.background) warm.background[j] = bg0;
+            if (warm.fallback) warm.fallback[j] = fell_back;
         }
         __syncwarp();
     }
@@ -935,6 +971,17 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
                         int max_cell_pixels, double background_level, int has_level, int max_iter,
                         double* params, uint8_t* status, int* iterations, void* workspace,
                         size_t workspace_bytes, void* stream) {
+    return spx_deblend_initial_warm(img, dtype, sign, height, width, voronoi, boxes, caps, seeds, n, hm, wm,
+                                    max_cell_pixels, background_level, has_level, max_iter, nullptr, nullptr,
+                                    params, status, iterations, nullptr, nullptr, workspace, workspace_bytes, stream);
+}
+
+int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                             const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
+                             int max_cell_pixels, double background_level, int has_level, int max_iter,
+                             const double* init_params, const uint8_t* init_ok, double* params, uint8_t* status,
+                             int* iterations, double* background_out, uint8_t* fallback_out, void* workspace,
+                             size_t workspace_bytes, void* stream) {
     SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && voronoi && boxes && caps && seeds && params && status && workspace, "null pointer");
@@ -947,8 +994,9 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
     return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem) -> int {
         if (smem > 48 * 1024)
             SPX_CUDA(cudaFuncSetAttribute(k_fit_initial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fit_initial<<<fit_blocks(), kFitWarps * 32, smem, s>>>(fa, seeds, background_level, has_level, params,
-                                                                  status, iterations);
+        k_fit_initial<<<fit_blocks(), kFitWarps * 32, smem, s>>>(
+            fa, seeds, background_level, has_level, params, status, iterations,
+            WarmStart{init_params, init_ok, background_out, fallback_out});
         return check_launch("k_fit_initial");
     });
 }

@@ -148,6 +148,111 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
     if (warp == 0) tmem_dealloc(tmem, tmem_cols);
 }
 
+// Weighted MSE gradient: dy = 2 w_j (y - t) / B as bf16, row-major (B x ldd, zero in the padding
+// columns) and transposed (ldd x B); loss += sum w_j (y - t)^2 / B (f64 atomics per block).
+__global__ void k_mse_grad(const float* y, const float* t, const float* w, int B, int nout, int ldd,
+                           __nv_bfloat16* dy, __nv_bfloat16* dy_t, double* loss) {
+    __shared__ double s_part[32];
+    double part = 0.0;
+    const long long total = (long long)B * ldd;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        int b, j;
+        divmod_idx(i, ldd, &b, &j);
+        float g = 0.0f;
+        if (j < nout) {
+            const float d = y[(long long)b * nout + j] - t[(long long)b * nout + j];
+            part += (double)w[j] * d * d;
+            g = 2.0f * w[j] * d / (float)B;
+        }
+        const __nv_bfloat16 gb = __float2bfloat16_rn(g);
+        dy[i] = gb;
+        dy_t[(long long)j * B + b] = gb;
+    }
+    part = warp_sum(part);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) acc += s_part[i];
+        atomicAdd(loss, acc / (double)B);
+    }
+}
+
+// out[r] = sum over the row r of a bf16 matrix (R x C), f32 accumulation, one warp per row.
+__global__ void k_rowsum_bf16(const __nv_bfloat16* src, int R, int C, float* out) {
+    const int lane = threadIdx.x & 31;
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < R; r += gridDim.x * (blockDim.x >> 5)) {
+        float acc = 0.0f;
+        for (int c = lane; c < C; c += 32) acc += __bfloat162float(src[(long long)r * C + c]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[r] = acc;
+    }
+}
+
+// AdamW on f32 parameters (rows x cols): m, v moments, bias-corrected step, decoupled decay; then
+// the bf16 copy (row-major, padded to out_rows rows of zeros) and/or its transpose (cols x ld_t).
+__global__ void k_adamw(float* p, const float* g, float* m, float* v, int rows, int cols, float lr, float beta1,
+                        float beta2, float eps, float wd, float c1, float c2, __nv_bfloat16* out, int out_rows,
+                        __nv_bfloat16* out_t, int ld_t) {
+    const long long total = (long long)max(rows, out_rows) * cols;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        int r, c;
+        divmod_idx(i, cols, &r, &c);
+        float w = 0.0f;
+        if (r < rows) {
+            const float gi = g[i];
+            const float mi = beta1 * m[i] + (1.0f - beta1) * gi;
+            const float vi = beta2 * v[i] + (1.0f - beta2) * gi * gi;
+            m[i] = mi;
+            v[i] = vi;
+            const float mh = mi / c1, vh = vi / c2;
+            w = p[i] - lr * (mh / (sqrtf(vh) + eps) + wd * p[i]);
+            p[i] = w;
+        }
+        if (out && r < out_rows) out[i] = __float2bfloat16_rn(w);
+        if (out_t && r < rows) out_t[(long long)c * ld_t + r] = __float2bfloat16_rn(w);
+    }
+}
+
+// dst (C x R) = src (R x C)^T for bf16, through 32 x 32 shared-memory tiles.
+__global__ void k_transpose_bf16(const __nv_bfloat16* src, int R, int C, __nv_bfloat16* dst) {
+    __shared__ __nv_bfloat16 tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = r0 + i, c = c0 + threadIdx.x;
+        if (r < R && c < C) tile[i][threadIdx.x] = src[(long long)r * C + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, r = r0 + threadIdx.x;
+        if (r < R && c < C) dst[(long long)c * R + r] = tile[threadIdx.x][i];
+    }
+}
+
+// Standardised MLP outputs -> ROI-local LM starting params: A = t0 amp, x0 = ox + 16 + t1 - box.x,
+// y0 = oy + 16 + t2 - box.y, u = t3..t5 (t = y * std + mean); ok = finite and A > 0.
+__global__ void k_outputs_to_params(const float* y, const double* mean, const double* stdv, const double* norm,
+                                    const int4* boxes, int n, double* params, uint8_t* ok) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double t[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) t[j] = (double)y[7LL * i + j] * stdv[j] + mean[j];
+        const double* nm = norm + 4LL * i;
+        const int4 b = boxes[i];
+        const double p[6] = {t[0] * nm[3], nm[0] + 16.0 + t[1] - b.x, nm[1] + 16.0 + t[2] - b.y, t[3], t[4], t[5]};
+        bool good = p[0] > 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            good = good && isfinite(p[j]);
+            params[6LL * i + j] = p[j];
+        }
+        ok[i] = good;
+    }
+}
+
 size_t gemm_smem(int BN) { return 2 * (size_t)(kGemmBM * 128 + BN * 128) + 64 + 1024; }
 
 }  // namespace
@@ -189,6 +294,57 @@ int spx_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int N, 
                                                  static_cast<const __nv_bfloat16*>(B), ldb, M, N, K, BN, cols, ep,
                                                  error_flag);
     return check_launch("k_gemm_bf16");
+}
+
+int spx_mlp_loss_grad(const float* y, const float* t, const float* weights, int batch, int n_out, int ld_grad,
+                      void* dy, void* dy_t, double* loss, void* stream) {
+    SPX_REQUIRE(batch > 0 && n_out > 0 && ld_grad >= n_out, "bad arguments");
+    SPX_REQUIRE(y && t && weights && dy && dy_t && loss, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_mse_grad<<<grid_for((long long)batch * ld_grad, 256, 148 * 4), 256, 0, s>>>(
+        y, t, weights, batch, n_out, ld_grad, static_cast<__nv_bfloat16*>(dy), static_cast<__nv_bfloat16*>(dy_t), loss);
+    return check_launch("k_mse_grad");
+}
+
+int spx_rowsum_bf16(const void* src, int rows, int cols, float* out, void* stream) {
+    SPX_REQUIRE(rows > 0 && cols > 0 && src && out, "bad arguments");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_rowsum_bf16<<<grid_for(rows, 8, 148 * 8), 256, 0, s>>>(static_cast<const __nv_bfloat16*>(src), rows, cols, out);
+    return check_launch("k_rowsum_bf16");
+}
+
+int spx_adamw(float* param, const float* grad, float* m, float* v, int rows, int cols, int step, float lr, float beta1,
+              float beta2, float eps, float weight_decay, void* out_bf16, int out_rows, void* out_bf16_t, int ld_t,
+              void* stream) {
+    SPX_REQUIRE(rows > 0 && cols > 0 && step >= 1 && out_rows >= 0 && (!out_bf16_t || ld_t >= rows),
+                "bad arguments");
+    SPX_REQUIRE(param && grad && m && v, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const float c1 = 1.0f - powf(beta1, (float)step), c2 = 1.0f - powf(beta2, (float)step);
+    k_adamw<<<grid_for((long long)max(rows, out_rows) * cols, 256), 256, 0, s>>>(
+        param, grad, m, v, rows, cols, lr, beta1, beta2, eps, weight_decay, c1, c2,
+        static_cast<__nv_bfloat16*>(out_bf16), out_rows, static_cast<__nv_bfloat16*>(out_bf16_t), ld_t);
+    return check_launch("k_adamw");
+}
+
+int spx_transpose_bf16(const void* src, int rows, int cols, void* dst, void* stream) {
+    SPX_REQUIRE(rows > 0 && cols > 0 && src && dst && src != dst, "bad arguments");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const dim3 grid((cols + 31) / 32, (rows + 31) / 32);
+    k_transpose_bf16<<<grid, dim3(32, 8), 0, s>>>(static_cast<const __nv_bfloat16*>(src), rows, cols,
+                                                 static_cast<__nv_bfloat16*>(dst));
+    return check_launch("k_transpose_bf16");
+}
+
+int spx_mlp_outputs_to_params(const float* y, const double* out_mean, const double* out_std, const double* norm,
+                              const int* boxes, int n, double* params, uint8_t* ok, void* stream) {
+    SPX_REQUIRE(n >= 0, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(y && out_mean && out_std && norm && boxes && params && ok, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_outputs_to_params<<<grid_for(n, 256), 256, 0, s>>>(y, out_mean, out_std, norm,
+                                                        reinterpret_cast<const int4*>(boxes), n, params, ok);
+    return check_launch("k_outputs_to_params");
 }
 
 }  // extern "C"

@@ -344,18 +344,25 @@ class Deblender:
         info["tile_medians"] = medians
         return self.bg.set_medians(medians), info
 
-    def initial(self, max_iter):
+    def initial(self, max_iter, warm_params=None, warm_ok=None, extras=False):
+        """Initial fits (subpx/_cpu/deblend.py:152-171 + LM). With warm_params (n x 6, ROI-local,
+        device) the LM starts there and falls back to the plain start per cell (learned warm
+        start); extras=True also returns the cell-border backgrounds and the fallback flags."""
         h, w = self.shape
         c = self.cells
         params = dev.empty((self.n, 6), torch.float64)
         status = dev.empty((self.n,), torch.uint8)
         iters = dev.empty((self.n,), torch.int32)
+        bg0 = dev.empty((self.n,), torch.float64) if extras else None
+        fell = dev.empty((self.n,), torch.uint8) if extras else None
         has = self.background_level is not None
-        _lib.call("spx_deblend_initial", self.img.data_ptr(), self.dtype, self.sign, h, w, c.voronoi.data_ptr(),
+        _lib.call("spx_deblend_initial_warm", self.img.data_ptr(), self.dtype, self.sign, h, w, c.voronoi.data_ptr(),
                   c.boxes.data_ptr(), c.caps.data_ptr(), c.seeds_d.data_ptr(), self.n, c.hm, c.wm, c.max_px,
-                  float(self.background_level) if has else 0.0, int(has), int(max_iter), params.data_ptr(),
-                  status.data_ptr(), iters.data_ptr(), self.fit_ws.data_ptr(), self.fit_ws.numel(),
-                  dev.stream_ptr())
+                  float(self.background_level) if has else 0.0, int(has), int(max_iter), _ptr(warm_params),
+                  _ptr(warm_ok), params.data_ptr(), status.data_ptr(), iters.data_ptr(), _ptr(bg0), _ptr(fell),
+                  self.fit_ws.data_ptr(), self.fit_ws.numel(), dev.stream_ptr())
+        if extras:
+            return params, status, iters, bg0, fell
         return params, status, iters
 
     def iteration(self, params_d, model, bg: Background):
@@ -397,7 +404,15 @@ class Deblender:
                                 np.zeros(0, np.uint8), dev.empty((0,), torch.uint8), self.tile, 0, info, False)
         fit_iters = []
         if init is None:
-            params_d, status_d, it = self.initial(self.max_iter)
+            from . import warmstart
+
+            net = warmstart.active()
+            if net is not None and self.n:
+                p0, ok = warmstart.predict_init(net, self.img, self.sign, self.cells.seeds_d, self.cells.boxes,
+                                                self.n)
+                params_d, status_d, it = self.initial(self.max_iter, warm_params=p0, warm_ok=ok)
+            else:
+                params_d, status_d, it = self.initial(self.max_iter)
             fit_iters.append(it)
         else:
             init = np.asarray(init, dtype=np.float64)

@@ -216,6 +216,17 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
                         int max_cell_pixels, double background_level, int has_level, int max_iter,
                         double* params, uint8_t* status, int* iterations, void* workspace,
                         size_t workspace_bytes, void* stream);
+/* spx_deblend_initial with a warm start: where init_params (n x 6, ROI-local) is given and
+ * init_ok[j] is set (or init_ok is null), cell j's LM starts from init_params[j]; that fit is kept
+ * when it meets the LM stop rule within max_iter and ends "ok", otherwise the plain start runs as
+ * well (fallback_out[j] = 1; iterations counts both). background_out[j] receives the cell-border
+ * background the fit subtracted. No reference counterpart (learned warm start). */
+int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
+                             const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
+                             int max_cell_pixels, double background_level, int has_level, int max_iter,
+                             const double* init_params, const uint8_t* init_ok, double* params, uint8_t* status,
+                             int* iterations, double* background_out, uint8_t* fallback_out, void* workspace,
+                             size_t workspace_bytes, void* stream);
 /* One outer iteration: clean every cell against `model` and `background`, LM from `params`,
  * params_out = params + relaxation * (fitted - params), status of params_out, and maxstep =
  * max |step[1:]| (NaN unless the cell is ok with a finite fit). */
@@ -366,6 +377,43 @@ typedef struct spx_gemm_epilogue {
  * counterpart: this and the MLP entry points below implement the learned warm start of the LM fits. */
 int spx_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int N, int K, const spx_gemm_epilogue* epi,
                   int* error_flag, void* stream);
+
+
+/* Weighted MSE gradient of the MLP outputs y (batch x n_out f32) against t: dy (batch x ld_grad
+ * bf16, zero padding columns) and its transpose (ld_grad x batch); *loss (device double) +=
+ * mean_b sum_j w_j (y - t)^2. */
+int spx_mlp_loss_grad(const float* y, const float* t, const float* weights, int batch, int n_out, int ld_grad,
+                      void* dy, void* dy_t, double* loss, void* stream);
+/* out[r] = sum of row r of a bf16 rows x cols matrix (f32): bias gradients from transposed
+ * activation gradients. */
+int spx_rowsum_bf16(const void* src, int rows, int cols, float* out, void* stream);
+/* AdamW (decoupled weight decay, bias-corrected moments, step >= 1) on f32 params (rows x cols),
+ * then optional bf16 copies: row-major with rows padded by zeros to out_rows, and transposed
+ * (cols x ld_t, ld_t >= rows). */
+int spx_adamw(float* param, const float* grad, float* m, float* v, int rows, int cols, int step, float lr, float beta1,
+              float beta2, float eps, float weight_decay, void* out_bf16, int out_rows, void* out_bf16_t, int ld_t,
+              void* stream);
+/* dst (cols x rows) = src (rows x cols)^T, bf16. */
+int spx_transpose_bf16(const void* src, int rows, int cols, void* dst, void* stream);
+/* Standardised MLP outputs y (n x 7 f32) -> ROI-local LM starting params (n x 6): t = y * std +
+ * mean; A = t0 amp, x0 = origin x + 16 + t1 - box x, y0 = origin y + 16 + t2 - box y, u = t3..t5,
+ * with norm rows [origin x, origin y, bg, amp] of spx_extract_patches; ok = finite and A > 0. */
+int spx_mlp_outputs_to_params(const float* y, const double* out_mean, const double* out_std, const double* norm,
+                              const int* boxes, int n, double* params, uint8_t* ok, void* stream);
+/* 32 x 32 signal patches (sign x image) centred on the rounded seeds [x, y], edges replicated,
+ * normalised to (v - bg) / amp with bg the 10th percentile of the 2-pixel border ring and
+ * amp = max - bg, as bf16 (n x 1024); norm (n x 4 doubles) = [origin x, origin y, bg, amp]. */
+int spx_extract_patches(const void* img, int dtype, double sign, int height, int width, const double* seeds, int n,
+                        void* out, double* norm, void* stream);
+/* Training pages: coverage (H x W doubles) of rotated superellipse holes (rows of [cx, cy, a, b,
+ * theta, exponent]) sampled on samples x samples points per pixel, holes found through a CSR grid
+ * of cell size `cell` (grid_start: grid_w * grid_h + 1 offsets into grid_ids). */
+int spx_hole_coverage(int height, int width, const double* holes, const int* grid_start, const int* grid_ids,
+                      int grid_w, int grid_h, double cell, int samples, double* coverage, void* stream);
+/* page = clip(rint(background + amplitude x coverage + noise x N(0, 1)), 0, 65535) as uint16, the
+ * normal deviates from a counter-based hash of (seed, pixel). */
+int spx_page_finish(const double* coverage, long long n, double background, double amplitude, double noise,
+                    unsigned long long seed, uint16_t* page, void* stream);
 
 #ifdef __cplusplus
 }

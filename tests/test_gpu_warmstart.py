@@ -1,0 +1,141 @@
+"""The learned warm start: MLP gradients and AdamW against the FP64 oracle, patch extraction against
+NumPy, and what a trained network gains over the plain initial fit at the same accuracy.
+
+The oracle comparisons emulate the GPU's bf16 roundings (inputs, weights, activations and
+activation gradients are bf16, accumulation is f32), so the remaining differences are f32
+summation order only.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import mlp as om
+
+pytestmark = pytest.mark.gpu
+
+
+def _net_and_batch(b=512, seed=3):
+    import torch
+
+    from imageprocessor_new_b200.warmstart import WarmStartNet
+
+    net = WarmStartNet(seed=seed)
+    rng = np.random.default_rng(seed)
+    x = torch.from_numpy(rng.normal(0, 0.5, (b, 1024)).astype(np.float32)).cuda().to(torch.bfloat16)
+    t = torch.from_numpy(rng.normal(0, 1, (b, 7)).astype(np.float32)).cuda()
+    return net, x, t
+
+
+def test_mlp_gradients_match_oracle():
+    import torch
+
+    from imageprocessor_new_b200 import _lib
+    from imageprocessor_new_b200.warmstart import IN
+
+    net, x, t = _net_and_batch()
+    b = x.shape[0]
+    w = {k: q.w.cpu().numpy().astype(np.float64) for k, q in net.p.items()}
+    xt = torch.empty((IN, b), dtype=torch.bfloat16, device="cuda")
+    _lib.call("spx_transpose_bf16", x.data_ptr(), b, IN, xt.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    weights = torch.tensor([1, 2, 2, 1, 1, 1, 0.5], dtype=torch.float32, device="cuda")
+    loss = net.train_step(x, xt, t, weights, lr=0.0, weight_decay=0.0)  # lr 0: gradients only
+    torch.cuda.synchronize()
+    net.check_errors()
+    # Oracle with the GPU's roundings.
+    xs = x.float().cpu().numpy().astype(np.float64)
+    tt = t.cpu().numpy().astype(np.float64)
+    wv = weights.cpu().numpy().astype(np.float64)
+    w1, w2, w3 = om.bf16(w["w1"]), om.bf16(w["w2"]), om.bf16(w["w3"])
+    h1 = om.bf16(np.maximum(xs @ w1.T + w["b1"], 0))
+    h2 = om.bf16(np.maximum(h1 @ w2.T + w["b2"], 0))
+    y = h2 @ w3.T + w["b3"]
+    ref_loss, dy = om.loss_and_grad_output(y, tt, wv)
+    dy = om.bf16(dy)
+    want = {"w3": dy.T @ h2, "b3": dy.sum(0)}
+    dh2 = om.bf16((dy @ w3) * (h2 > 0))
+    want.update(w2=dh2.T @ h1, b2=dh2.sum(0))
+    dh1 = om.bf16((dh2 @ w2) * (h1 > 0))
+    want.update(w1=dh1.T @ xs, b1=dh1.sum(0))
+    assert abs(float(loss.item()) - ref_loss) <= 1e-4 * ref_loss
+    for k, ref in want.items():
+        got = net.p[k].g.cpu().numpy().astype(np.float64)
+        err = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-30)
+        assert err < 2e-3, (k, err)
+    # And the unrounded FP64 oracle agrees to bf16 precision.
+    h1_64, h2_64, y64 = om.forward(xs, w["w1"], w["b1"], w["w2"], w["b2"], w["w3"], w["b3"])
+    _, dy64 = om.loss_and_grad_output(y64, tt, wv)
+    g64 = om.backward(xs, h1_64, h2_64, dy64, w["w2"], w["w3"])
+    for k, ref in zip(("w1", "b1", "w2", "b2", "w3", "b3"), g64):
+        got = net.p[k].g.cpu().numpy().astype(np.float64)
+        assert np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-30) < 5e-2, k
+
+
+def test_adamw_matches_oracle():
+    import ctypes
+
+    import torch
+
+    from imageprocessor_new_b200 import _lib
+
+    rng = np.random.default_rng(1)
+    rows, cols = 7, 256
+    w0 = rng.normal(0, 1, (rows, cols)).astype(np.float32)
+    w = torch.from_numpy(w0.copy()).cuda()
+    m = torch.zeros_like(w)
+    v = torch.zeros_like(w)
+    out = torch.zeros((16, cols), dtype=torch.bfloat16, device="cuda")
+    out_t = torch.zeros((cols, 16), dtype=torch.bfloat16, device="cuda")
+    wr, mr, vr = w0.astype(np.float64), np.zeros((rows, cols)), np.zeros((rows, cols))
+    for step in range(1, 4):
+        g0 = rng.normal(0, 1, (rows, cols)).astype(np.float32)
+        g = torch.from_numpy(g0).cuda()
+        _lib.call("spx_adamw", w.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), rows, cols, step,
+                  ctypes.c_float(1e-2), ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8),
+                  ctypes.c_float(0.01), out.data_ptr(), 16, out_t.data_ptr(), 16,
+                  torch.cuda.current_stream().cuda_stream)
+        wr, mr, vr = om.adamw(wr, g0.astype(np.float64), mr, vr, step, lr=1e-2, weight_decay=0.01)
+    np.testing.assert_allclose(w.cpu().numpy(), wr, rtol=0, atol=2e-6)
+    assert torch.equal(out[:rows], w.to(torch.bfloat16))
+    assert not out[rows:].any()
+    assert torch.equal(out_t[:, :rows], w.t().to(torch.bfloat16))
+
+
+def test_patches_match_numpy():
+    import torch
+
+    from imageprocessor_new_b200 import synthetic
+    from imageprocessor_new_b200.warmstart import patches
+
+    page = synthetic.page_square(2).image[:300, :400]
+    seeds = np.array([[200.3, 150.7], [3.0, 4.4], [398.6, 299.2], [15.5, 16.5]])
+    x, norm = patches(torch.from_numpy(np.ascontiguousarray(page)).cuda(), 1.0,
+                      torch.from_numpy(seeds).cuda(), len(seeds))
+    x, norm = x.float().cpu().numpy(), norm.cpu().numpy()
+    for i, (sx, sy) in enumerate(seeds):
+        ox, oy = int(np.rint(sx)) - 16, int(np.rint(sy)) - 16
+        ys = np.clip(np.arange(oy, oy + 32), 0, page.shape[0] - 1)
+        xs = np.clip(np.arange(ox, ox + 32), 0, page.shape[1] - 1)
+        p = page[np.ix_(ys, xs)].astype(np.float64)
+        ring = np.concatenate([p[:2].ravel(), p[-2:].ravel(), p[2:-2, :2].ravel(), p[2:-2, -2:].ravel()])
+        bg = np.percentile(ring, 10)
+        amp = p.max() - bg
+        assert norm[i, 0] == ox and norm[i, 1] == oy
+        assert norm[i, 2] == bg and norm[i, 3] == amp
+        want = ((p - bg) / amp).astype(np.float32)
+        np.testing.assert_allclose(x[i].reshape(32, 32), want, rtol=2 ** -8, atol=2 ** -9)
+
+
+def test_trained_network_gains_over_the_plain_start():
+    """A network trained here on synthetic pages needs fewer LM iterations than the plain initialiser
+    and ends at the plain fit's optimum (centres within 1e-3 px)."""
+    from imageprocessor_new_b200 import warmstart as ws
+
+    x, t = ws.training_set(12, size=1536, seed=11)
+    net = ws.WarmStartNet(seed=11)
+    hist = ws.train(net, x, t, epochs=12, batch=2048, lr=2e-3, seed=11)
+    assert hist[-1] < 0.5 * hist[0]
+    r = ws.evaluate(net, pages=1, size=1536, seed=5, repeats=1)
+    assert r["cells"] > 1000
+    assert r["warm_iterations_mean"] < r["plain_iterations_mean"]
+    assert r["fallback_fraction"] < 0.2
+    assert r["within_1e-3_px"] >= 0.99
