@@ -21,6 +21,7 @@ data path); the step time is the max over ranks.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import subprocess
@@ -184,18 +185,36 @@ def gpu_arm(args):
             dist.barrier()
         return ms, cells, launches
 
-    with ClockSampler(local) as clocks:
-        for _ in range(args.warmup):
-            step(page_d)
-        clocks.mark_start()
-        ms, cells, launches = run(page_d, args.steps)
-        clocks.mark_end()
-    fit_ms = [a.elapsed_time(b) for a, b in fit_times]
-    fit_avg_ms = float(np.mean(fit_ms)) if fit_ms else float("nan")
-    fit_n = float(np.mean(fit_cells)) if fit_cells else 0.0
-    # End to end: host page, copies inside the region.
-    step(page)
-    ms_e2e, cells_e2e, _ = run(page, args.steps)
+    # Variants: the NN-warm-started pipeline (when a trained model is present) and the plain one.
+    from imageprocessor_new_b200 import warmstart
+
+    model_path = Path(args.model) if args.model else warmstart.DEFAULT_MODEL
+    net = warmstart.WarmStartNet.load(model_path) if (args.warm_start and model_path.exists()) else None
+    timings, results = {}, {}
+    for variant in (["warm"] if net is not None else []) + ["plain"]:
+        warmstart.use(net if variant == "warm" else None)
+        headline = variant == ("warm" if net is not None else "plain")
+        with (ClockSampler(local) if headline else contextlib.nullcontext()) as clocks:
+            for _ in range(args.warmup):
+                step(page_d)
+            if headline:
+                clocks.mark_start()
+            ms_v, cells_v, launches_v = run(page_d, args.steps)
+            if headline:
+                clocks.mark_end()
+                clock_summary = clocks.summary()
+        timings[variant] = (ms_v, cells_v, launches_v)
+        if headline:
+            ms, cells, launches = ms_v, cells_v, launches_v
+            fit_ms = [a.elapsed_time(b) for a, b in fit_times]
+            fit_avg_ms = float(np.mean(fit_ms)) if fit_ms else float("nan")
+            fit_n = float(np.mean(fit_cells)) if fit_cells else 0.0
+            # End to end: host page, copies inside the region.
+            step(page)
+            ms_e2e, cells_e2e, _ = run(page, args.steps)
+        results[variant] = step(page_d)
+    lm_stage = warmstart.compare_on_page(net, page_d) if (net is not None and world == 1) else None
+    warmstart.use(None)
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -227,11 +246,35 @@ def gpu_arm(args):
                      "traffic": round(FIT_TRAFFIC_PER_CELL * fit_n / 1e9, 4), "traffic_unit": "GB per launch",
                      "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n},
         "gpu_launches": int(launches),
-        "clocks": clocks.summary(),
+        "clocks": clock_summary,
     }
+    if net is not None:
+        ms_p, cells_p, _ = timings["plain"]
+        line["config"]["warm_start"] = f"MLP 1024-256-256-7 ({model_path.name}), plain-start fallback"
+        line["plain_lm"] = {"value": round(world * (cells_p / args.steps) / (ms_p / 1e3 / args.steps), 1),
+                            "unit": UNIT, "ms_per_step": round(ms_p / args.steps, 3)}
+        line["accuracy_vs_plain"] = _accuracy(results["warm"], results["plain"])
+        if lm_stage is not None:
+            line["lm_stage"] = {k: (round(v, 6) if isinstance(v, float) else v) for k, v in lm_stage.items()}
     if args.cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(page, args.cpu_sample)
     print(json.dumps(line), flush=True)
+
+
+def _accuracy(warm, plain) -> dict:
+    """Largest differences of the warm-started pipeline's results from the plain pipeline's (same
+    cells): centres and equivalent CDs of every method, in pixels, over cells valid in both."""
+    out = {"same_cells": bool(np.array_equal(warm.seeds_xy, plain.seeds_xy))}
+    if not out["same_cells"]:
+        return out
+    for name in METHODS:
+        a, b = warm.measurements[name], plain.measurements[name]
+        both = a.valid & b.valid
+        dc = float(np.abs(a.centers_xy[both] - b.centers_xy[both]).max()) if both.any() else 0.0
+        dcd = (float(np.abs(a.metrics["cd_equivalent_px"][both] - b.metrics["cd_equivalent_px"][both]).max())
+               if both.any() else 0.0)
+        out[name] = {"centre_max_px": dc, "cd_max_px": dcd, "same_validity": float((a.valid == b.valid).mean())}
+    return out
 
 
 def _workload(size: int) -> str:
@@ -298,6 +341,8 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=("gpu", "reference"))
     ap.add_argument("--cpu-sample", type=int, default=768)
     ap.add_argument("--page", type=int, default=8192, help="page side in pixels (8192 = the benchmark page)")
+    ap.add_argument("--model", default=None, help="warm-start MLP (default: the packaged model)")
+    ap.add_argument("--no-warm-start", dest="warm_start", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     args = ap.parse_args()
     if args.impl == "reference":

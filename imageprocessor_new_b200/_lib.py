@@ -67,8 +67,8 @@ SIGNATURES = {
     "spx_triangle": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
     "spx_gemm_bf16": (_I, [_P, _I, _P, _I, _I, _I, _I, POINTER(GemmEpilogue), _P, _P]),
-    "spx_deblend_initial_warm": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _D, _I, _I, _P, _P, _P, _P,
-                                      _P, _P, _P, _P, _S, _P]),
+    "spx_deblend_initial_warm": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _D, _I, _I, _P, _P, _D, _P,
+                                      _P, _P, _P, _P, _P, _S, _P]),
     "spx_mlp_loss_grad": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _P, _P]),
     "spx_rowsum_bf16": (_I, [_P, _I, _I, _P, _P]),
     "spx_adamw": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,

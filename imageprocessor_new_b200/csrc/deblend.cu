@@ -146,6 +146,7 @@ struct WarmStart {
     const uint8_t* ok;
     double* background;
     uint8_t* fallback;
+    double cost_tol;  // relative cost drop that ends a warm-started fit
 };
 
 __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
@@ -245,7 +246,7 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
                 finite = finite && isfinite(q[i]);
             }
             if (finite && q[0] > 0.0) {
-                it = warp_lm_fit(q, v, xy, n, cap, amp_cap, a.max_iter, lane);
+                it = warp_lm_fit(q, v, xy, n, cap, amp_cap, a.max_iter, lane, warm.cost_tol);
                 st = fit_status_of(q, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
                 if (it < a.max_iter && st == SPX_ST_OK) {
                     for (int i = 0; i < 6; ++i) p[i] = q[i];
@@ -972,16 +973,17 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
                         double* params, uint8_t* status, int* iterations, void* workspace,
                         size_t workspace_bytes, void* stream) {
     return spx_deblend_initial_warm(img, dtype, sign, height, width, voronoi, boxes, caps, seeds, n, hm, wm,
-                                    max_cell_pixels, background_level, has_level, max_iter, nullptr, nullptr,
+                                    max_cell_pixels, background_level, has_level, max_iter, nullptr, nullptr, 1e-12,
                                     params, status, iterations, nullptr, nullptr, workspace, workspace_bytes, stream);
 }
 
 int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                              const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
                              int max_cell_pixels, double background_level, int has_level, int max_iter,
-                             const double* init_params, const uint8_t* init_ok, double* params, uint8_t* status,
-                             int* iterations, double* background_out, uint8_t* fallback_out, void* workspace,
-                             size_t workspace_bytes, void* stream) {
+                             const double* init_params, const uint8_t* init_ok, double warm_cost_tol,
+                             double* params, uint8_t* status, int* iterations, double* background_out,
+                             uint8_t* fallback_out, void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(warm_cost_tol > 0.0, "warm_cost_tol must be positive");
     SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && voronoi && boxes && caps && seeds && params && status && workspace, "null pointer");
@@ -996,7 +998,7 @@ int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height
             SPX_CUDA(cudaFuncSetAttribute(k_fit_initial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_fit_initial<<<fit_blocks(), kFitWarps * 32, smem, s>>>(
             fa, seeds, background_level, has_level, params, status, iterations,
-            WarmStart{init_params, init_ok, background_out, fallback_out});
+            WarmStart{init_params, init_ok, background_out, fallback_out, warm_cost_tol});
         return check_launch("k_fit_initial");
     });
 }

@@ -149,8 +149,10 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const double
 // Each trial's cost is evaluated in the same pass as its normal equations: an accepted trial (the
 // usual case) hands its sums to the next iteration, a rejected one recomputes the sums at the kept
 // params. The arithmetic of every sum is that of separate Jacobian and cost passes.
+// `cost_tol` is the relative cost drop at or below which an accepted step ends the fit (1e-12, the
+// reference's rule, by default).
 __device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int n, double cap, double amp_cap,
-                           int max_iter, int lane) {
+                           int max_iter, int lane, double cost_tol = 1e-12) {
     double s[27];
     double cost = warp_normal_pass(p, v, xy, n, lane, s);
     if (!isfinite(cost)) return 0;
@@ -176,7 +178,7 @@ __device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int
         for (int i = 0; i < 6; ++i) small = small && !isnan(step[i]);
         const double new_cost = warp_normal_pass(trial, v, xy, n, lane, s);
         const bool better = isfinite(new_cost) && new_cost <= cost;
-        const bool done = (better && (cost - new_cost <= 1e-12 * fmax(cost, 1e-300))) || small;
+        const bool done = (better && (cost - new_cost <= cost_tol * fmax(cost, 1e-300))) || small;
         if (better) {
 #pragma unroll
             for (int i = 0; i < 6; ++i) p[i] = trial[i];

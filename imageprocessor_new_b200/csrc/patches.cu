@@ -2,8 +2,9 @@
 //
 // A patch is the 32 x 32 window of the signal (image x sign) whose centre pixel (16, 16) is the
 // cell seed rounded to the nearest pixel, edges replicated. It is normalised by its own level and
-// scale: bg = 10th percentile (numpy 'linear') of the 2-pixel border ring, amp = max - bg, and
-// x = (v - bg) / amp, stored as bf16. One warp per patch.
+// scale: bg = the smallest mean of the 60 2 x 2 blocks along its border (robust to single noisy
+// pixels), amp = max - bg, and x = (v - bg) / amp, stored as bf16. One warp per patch, lane c
+// holding column c in registers, so the window is read once.
 //
 // Training pages are rendered here so that the training set comes from the same detection and
 // plain-fit pipeline the warm start serves: every hole is a rotated superellipse
@@ -19,58 +20,48 @@ namespace spx {
 namespace {
 
 constexpr int kPatch = 32;
-constexpr int kRing = 2 * kPatch * 2 + 2 * (kPatch - 4) * 2;  // 2-pixel border ring: 240 pixels
-
 __global__ void k_extract_patches(const void* img, int dtype, double sign, int H, int W, const double* seeds, int n,
                                   __nv_bfloat16* out, double* norm) {
-    __shared__ double ring_s[8][256];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double* ring = ring_s[wib];
-    for (int i = blockIdx.x * (blockDim.x >> 5) + wib; i < n; i += gridDim.x * (blockDim.x >> 5)) {
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const int ox = (int)rint(seeds[2LL * i]) - kPatch / 2, oy = (int)rint(seeds[2LL * i + 1]) - kPatch / 2;
-        auto at = [&](int r, int c) {
-            const int y = min(max(oy + r, 0), H - 1), x = min(max(ox + c, 0), W - 1);
-            return sign * load_px(img, dtype, (long long)y * W + x);
-        };
-        // Border ring into shared memory (padded to 256 with +inf), sorted.
-        for (int k = lane; k < 256; k += 32) {
-            double v = dinf();
-            if (k < kRing) {
-                int r, c;
-                if (k < 2 * kPatch) {                      // top two rows
-                    r = k / kPatch;
-                    c = k % kPatch;
-                } else if (k < 4 * kPatch) {               // bottom two rows
-                    r = kPatch - 2 + (k - 2 * kPatch) / kPatch;
-                    c = (k - 2 * kPatch) % kPatch;
-                } else {                                   // two columns on each side, rows 2..29
-                    const int j = k - 4 * kPatch, q = j & 3;
-                    r = 2 + (j >> 2);
-                    c = q < 2 ? q : kPatch - 4 + q;
-                }
-                v = at(r, c);
-            }
-            ring[k] = v;
-        }
-        __syncwarp();
-        warp_bitonic_sort(ring, 256, lane);
-        const double bg = sorted_percentile(ring, kRing, 0.1);
-        __syncwarp();
+        const int x = min(max(ox + lane, 0), W - 1);
+        double col[kPatch];
         double mx = -dinf();
-        for (int k = lane; k < kPatch * kPatch; k += 32) mx = fmax(mx, at(k / kPatch, k % kPatch));
+#pragma unroll
+        for (int r = 0; r < kPatch; ++r) {
+            const int y = min(max(oy + r, 0), H - 1);
+            col[r] = sign * load_px(img, dtype, (long long)y * W + x);
+            mx = fmax(mx, col[r]);
+        }
         mx = warp_max(mx);
+        // 2 x 2 block sums along the border: this lane's column pair (lane, lane ^ 1) for the top and
+        // bottom block rows, and the block rows in between for the outer column pairs.
+        double lo = dinf();
+        auto pair = [&](int r) { return col[r] + col[r + 1]; };
+        const double top = pair(0), bottom = pair(kPatch - 2);
+        const double top_b = top + __shfl_xor_sync(0xffffffffu, top, 1);
+        const double bottom_b = bottom + __shfl_xor_sync(0xffffffffu, bottom, 1);
+        lo = fmin(top_b, bottom_b);
+#pragma unroll
+        for (int br = 1; br < kPatch / 2 - 1; ++br) {
+            const double v = pair(2 * br);
+            const double blk = v + __shfl_xor_sync(0xffffffffu, v, 1);
+            if (lane < 2 || lane >= kPatch - 2) lo = fmin(lo, blk);
+        }
+        const double bg = warp_min(lo) / 4.0;
         const double amp = fmax(mx - bg, 1e-12);
         const double inv = 1.0 / amp;
-        for (int k = lane; k < kPatch * kPatch; k += 32)
-            out[(long long)i * kPatch * kPatch + k] =
-                __float2bfloat16_rn((float)((at(k / kPatch, k % kPatch) - bg) * inv));
+        __nv_bfloat16* o = out + (long long)i * kPatch * kPatch + lane;
+#pragma unroll
+        for (int r = 0; r < kPatch; ++r) o[r * kPatch] = __float2bfloat16_rn((float)((col[r] - bg) * inv));
         if (lane == 0) {
             norm[4LL * i] = ox;
             norm[4LL * i + 1] = oy;
             norm[4LL * i + 2] = bg;
             norm[4LL * i + 3] = amp;
         }
-        __syncwarp();
     }
 }
 
@@ -137,7 +128,7 @@ int spx_extract_patches(const void* img, int dtype, double sign, int height, int
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && seeds && out && norm, "null pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_extract_patches<<<grid_for(n, 8, 148 * 16), 256, 0, s>>>(img, dtype, sign, height, width, seeds, n,
+    k_extract_patches<<<grid_for(n, 8, 148 * 32), 256, 0, s>>>(img, dtype, sign, height, width, seeds, n,
                                                                static_cast<__nv_bfloat16*>(out), norm);
     return check_launch("k_extract_patches");
 }

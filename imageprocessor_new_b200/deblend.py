@@ -344,7 +344,7 @@ class Deblender:
         info["tile_medians"] = medians
         return self.bg.set_medians(medians), info
 
-    def initial(self, max_iter, warm_params=None, warm_ok=None, extras=False):
+    def initial(self, max_iter, warm_params=None, warm_ok=None, extras=False, warm_cost_tol=1e-12):
         """Initial fits (subpx/_cpu/deblend.py:152-171 + LM). With warm_params (n x 6, ROI-local,
         device) the LM starts there and falls back to the plain start per cell (learned warm
         start); extras=True also returns the cell-border backgrounds and the fallback flags."""
@@ -359,7 +359,8 @@ class Deblender:
         _lib.call("spx_deblend_initial_warm", self.img.data_ptr(), self.dtype, self.sign, h, w, c.voronoi.data_ptr(),
                   c.boxes.data_ptr(), c.caps.data_ptr(), c.seeds_d.data_ptr(), self.n, c.hm, c.wm, c.max_px,
                   float(self.background_level) if has else 0.0, int(has), int(max_iter), _ptr(warm_params),
-                  _ptr(warm_ok), params.data_ptr(), status.data_ptr(), iters.data_ptr(), _ptr(bg0), _ptr(fell),
+                  _ptr(warm_ok), float(warm_cost_tol), params.data_ptr(), status.data_ptr(), iters.data_ptr(),
+                  _ptr(bg0), _ptr(fell),
                   self.fit_ws.data_ptr(), self.fit_ws.numel(), dev.stream_ptr())
         if extras:
             return params, status, iters, bg0, fell
@@ -410,7 +411,8 @@ class Deblender:
             if net is not None and self.n:
                 p0, ok = warmstart.predict_init(net, self.img, self.sign, self.cells.seeds_d, self.cells.boxes,
                                                 self.n)
-                params_d, status_d, it = self.initial(self.max_iter, warm_params=p0, warm_ok=ok)
+                params_d, status_d, it = self.initial(self.max_iter, warm_params=p0, warm_ok=ok,
+                                                      warm_cost_tol=net.cost_tol)
             else:
                 params_d, status_d, it = self.initial(self.max_iter)
             fit_iters.append(it)

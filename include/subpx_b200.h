@@ -217,16 +217,18 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
                         double* params, uint8_t* status, int* iterations, void* workspace,
                         size_t workspace_bytes, void* stream);
 /* spx_deblend_initial with a warm start: where init_params (n x 6, ROI-local) is given and
- * init_ok[j] is set (or init_ok is null), cell j's LM starts from init_params[j]; that fit is kept
- * when it meets the LM stop rule within max_iter and ends "ok", otherwise the plain start runs as
- * well (fallback_out[j] = 1; iterations counts both). background_out[j] receives the cell-border
- * background the fit subtracted. No reference counterpart (learned warm start). */
+ * init_ok[j] is set (or init_ok is null), cell j's LM starts from init_params[j] and stops when
+ * an accepted step lowers the cost by at most warm_cost_tol relative (1e-12 is the plain rule),
+ * max |step| < 1e-7 or the damping exceeds 1e12; that fit is kept when it stops within max_iter and ends "ok", otherwise
+ * the plain start runs as well (fallback_out[j] = 1; iterations counts both). background_out[j]
+ * receives the cell-border background the fit subtracted. No reference counterpart (learned warm
+ * start). */
 int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                              const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
                              int max_cell_pixels, double background_level, int has_level, int max_iter,
-                             const double* init_params, const uint8_t* init_ok, double* params, uint8_t* status,
-                             int* iterations, double* background_out, uint8_t* fallback_out, void* workspace,
-                             size_t workspace_bytes, void* stream);
+                             const double* init_params, const uint8_t* init_ok, double warm_cost_tol,
+                             double* params, uint8_t* status, int* iterations, double* background_out,
+                             uint8_t* fallback_out, void* workspace, size_t workspace_bytes, void* stream);
 /* One outer iteration: clean every cell against `model` and `background`, LM from `params`,
  * params_out = params + relaxation * (fitted - params), status of params_out, and maxstep =
  * max |step[1:]| (NaN unless the cell is ok with a finite fit). */
@@ -401,7 +403,7 @@ int spx_transpose_bf16(const void* src, int rows, int cols, void* dst, void* str
 int spx_mlp_outputs_to_params(const float* y, const double* out_mean, const double* out_std, const double* norm,
                               const int* boxes, int n, double* params, uint8_t* ok, void* stream);
 /* 32 x 32 signal patches (sign x image) centred on the rounded seeds [x, y], edges replicated,
- * normalised to (v - bg) / amp with bg the 10th percentile of the 2-pixel border ring and
+ * normalised to (v - bg) / amp with bg the smallest mean of the 2 x 2 blocks along the border and
  * amp = max - bg, as bf16 (n x 1024); norm (n x 4 doubles) = [origin x, origin y, bg, amp]. */
 int spx_extract_patches(const void* img, int dtype, double sign, int height, int width, const double* seeds, int n,
                         void* out, double* norm, void* stream);
