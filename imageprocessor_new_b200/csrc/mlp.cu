@@ -2,10 +2,10 @@
 //
 // GEMMs run on the 5th-generation tensor cores: one CTA of 128 threads computes a 128 x BN tile of
 // C = A B^T (A: M x K, B: N x K, both bf16 and K-contiguous) with the accumulator in TMEM. Operand
-// tiles of 64 K are copied into a two-stage ring of 128-byte-swizzled shared-memory tiles with
-// cp.async; thread 0 issues four tcgen05.mma (K = 16 each) per stage and commits them to the
-// stage's mbarrier, which gates the reuse of that stage. The epilogue reads TMEM with tcgen05.ld
-// (warp w owns rows 32w..32w+31) and applies scale, bias, ReLU or the ReLU derivative of a forward
+// tiles of 64 K are copied with cp.async into a four-stage ring of 128-byte-swizzled shared-memory
+// tiles, three K-blocks ahead; thread 0 issues four tcgen05.mma (K = 16 each) per stage and commits
+// them to the stage's mbarrier, which gates the reuse of that stage. The epilogue reads TMEM with
+// tcgen05.ld (warp w owns rows 32w..32w+31) and applies scale, bias, ReLU or the ReLU derivative of a forward
 // activation, and writes f32 and/or bf16 outputs, row-major or transposed (the transposed copies
 // feed the weight-gradient GEMMs, whose reduction runs over the batch).
 //
@@ -22,6 +22,7 @@ namespace {
 constexpr int kGemmThreads = 128;
 constexpr int kGemmBM = 128;
 constexpr int kGemmBK = 64;
+constexpr int kGemmStages = 4;  // shared-memory ring of K-blocks
 constexpr long long kWaitLimit = 1ll << 24;
 
 struct GemmEpi {
@@ -62,21 +63,19 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
                                                             int ldb, int M, int N, int K, int BN, uint32_t tmem_cols,
                                                             GemmEpi ep, int* err) {
     extern __shared__ uint8_t smem_raw[];
-    // 1024-byte aligned stages: [A0 | B0 | A1 | B1], then two mbarriers and the TMEM address.
+    // kGemmStages 1024-byte aligned stages [A | B], then one mbarrier per stage and the TMEM address.
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    const int a_bytes = kGemmBM * 128, b_bytes = BN * 128;
-    uint8_t* stage_a[2] = {base, base + a_bytes + b_bytes};
-    uint8_t* stage_b[2] = {base + a_bytes, base + 2 * a_bytes + b_bytes};
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(base + 2 * (a_bytes + b_bytes));
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+    const int a_bytes = kGemmBM * 128, b_bytes = BN * 128, stage_bytes = a_bytes + b_bytes;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(base + kGemmStages * stage_bytes);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + kGemmStages);
     const int warp = threadIdx.x >> 5;
     const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
+    auto stage_a = [&](int s) { return base + s * stage_bytes; };
+    auto stage_b = [&](int s) { return base + s * stage_bytes + a_bytes; };
 
     if (warp == 0) tmem_alloc(tmem_slot, tmem_cols);
-    if (threadIdx.x == 0) {
-        mbar_init(&mbar[0], 1);
-        mbar_init(&mbar[1], 1);
-    }
+    if (threadIdx.x == 0)
+        for (int s = 0; s < kGemmStages; ++s) mbar_init(&mbar[s], 1);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -86,27 +85,32 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
     const int nk = (K + kGemmBK - 1) / kGemmBK;
     bool ok = true;
 
-    load_tile(stage_a[0], A, lda, m0, kGemmBM, M, 0, K);
-    load_tile(stage_b[0], B, ldb, n0, BN, N, 0, K);
-    cp_async_commit();
-    for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb & 1;
-        if (kb + 1 < nk) {
-            const int s2 = (kb + 1) & 1;
-            if (kb + 1 >= 2) ok = ok && mbar_wait(&mbar[s2], ((kb - 1) >> 1) & 1, kWaitLimit);
-            load_tile(stage_a[s2], A, lda, m0, kGemmBM, M, kb + 1, K);
-            load_tile(stage_b[s2], B, ldb, n0, BN, N, kb + 1, K);
-            cp_async_commit();
-            asm volatile("cp.async.wait_group 1;\n" : : : "memory");
-        } else {
-            cp_async_wait_all();
+    // Prologue: the first kGemmStages - 1 K-blocks in flight (one cp.async group each, empty
+    // groups past the end keep the group count uniform).
+    for (int kb = 0; kb < kGemmStages - 1; ++kb) {
+        if (kb < nk) {
+            load_tile(stage_a(kb), A, lda, m0, kGemmBM, M, kb, K);
+            load_tile(stage_b(kb), B, ldb, n0, BN, N, kb, K);
         }
+        cp_async_commit();
+    }
+    for (int kb = 0; kb < nk; ++kb) {
+        const int s = kb % kGemmStages;
+        const int kn = kb + kGemmStages - 1;  // block to fetch now, into the stage block kb - 1 used
+        if (kn < nk) {
+            const int sn = kn % kGemmStages;
+            if (kb >= 1) ok = ok && mbar_wait(&mbar[sn], ((kb - 1) / kGemmStages) & 1, kWaitLimit);
+            load_tile(stage_a(sn), A, lda, m0, kGemmBM, M, kn, K);
+            load_tile(stage_b(sn), B, ldb, n0, BN, N, kn, K);
+        }
+        cp_async_commit();
+        asm volatile("cp.async.wait_group %0;\n" : : "n"(kGemmStages - 1) : "memory");
         fence_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
             tc_fence_after();
-            const uint64_t ad = umma_desc_sw128(smem_u32(stage_a[s]));
-            const uint64_t bd = umma_desc_sw128(smem_u32(stage_b[s]));
+            const uint64_t ad = umma_desc_sw128(smem_u32(stage_a(s)));
+            const uint64_t bd = umma_desc_sw128(smem_u32(stage_b(s)));
 #pragma unroll
             for (int k = 0; k < kGemmBK / 16; ++k)
                 umma_bf16(tmem, ad + (uint64_t)((k * 32) >> 4), bd + (uint64_t)((k * 32) >> 4), idesc,
@@ -115,7 +119,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
         }
     }
     // The last commit covers every MMA of the tile.
-    ok = mbar_wait(&mbar[(nk - 1) & 1], ((nk - 1) >> 1) & 1, kWaitLimit) && ok;
+    ok = mbar_wait(&mbar[(nk - 1) % kGemmStages], ((nk - 1) / kGemmStages) & 1, kWaitLimit) && ok;
     tc_fence_after();
     if (!ok && threadIdx.x == 0) atomicExch(err, 1);
 
@@ -126,21 +130,63 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
             float v[16];
             tmem_ld16(lane_addr + (uint32_t)c0, v);
             if (m >= M) continue;
+            const int nb = n0 + c0;
+            const int cnt = min(16, N - nb);
+            if (cnt <= 0) continue;
+            float x[16];
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
-                const int n = n0 + c0 + i;
-                if (n >= N) break;
-                float x = v[i] * ep.scale;
-                if (ep.bias) x += ep.bias[n];
-                if (ep.mask_act && !(__bfloat162float(ep.mask_act[(long long)m * ep.ld_mask + n]) > 0.0f)) x = 0.0f;
-                if (ep.relu) x = fmaxf(x, 0.0f);
-                if (ep.out_f32) {
-                    float* o = ep.out_f32 + (long long)m * ep.ld_f32 + n;
-                    *o = ep.accumulate ? *o + x : x;
+                const int n = nb + i;
+                float t = v[i] * ep.scale;
+                if (i < cnt) {
+                    if (ep.bias) t += ep.bias[n];
+                    if (ep.mask_act && !(__bfloat162float(ep.mask_act[(long long)m * ep.ld_mask + n]) > 0.0f)) t = 0.0f;
                 }
-                if (ep.out_bf16) ep.out_bf16[(long long)m * ep.ld_bf16 + n] = __float2bfloat16_rn(x);
-                if (ep.out_bf16_t) ep.out_bf16_t[(long long)n * ep.ld_t + m] = __float2bfloat16_rn(x);
+                if (ep.relu) t = fmaxf(t, 0.0f);
+                x[i] = t;
             }
+            // Row-major outputs: 16-byte vector stores for a full, aligned chunk of 16 columns.
+            if (ep.out_f32) {
+                float* o = ep.out_f32 + (long long)m * ep.ld_f32 + nb;
+                if (cnt == 16 && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+                    float4* o4 = reinterpret_cast<float4*>(o);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float4 w = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+                        if (ep.accumulate) {
+                            const float4 u = o4[q];
+                            w.x += u.x; w.y += u.y; w.z += u.z; w.w += u.w;
+                        }
+                        o4[q] = w;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        if (i < cnt) o[i] = ep.accumulate ? o[i] + x[i] : x[i];
+                }
+            }
+            if (ep.out_bf16) {
+                __nv_bfloat16* o = ep.out_bf16 + (long long)m * ep.ld_bf16 + nb;
+                if (cnt == 16 && (reinterpret_cast<uintptr_t>(o) & 15) == 0) {
+                    uint4 pk[2];
+                    uint32_t* w = reinterpret_cast<uint32_t*>(pk);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const __nv_bfloat162 h = __floats2bfloat162_rn(x[2 * q], x[2 * q + 1]);
+                        w[q] = *reinterpret_cast<const uint32_t*>(&h);
+                    }
+                    reinterpret_cast<uint4*>(o)[0] = pk[0];
+                    reinterpret_cast<uint4*>(o)[1] = pk[1];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        if (i < cnt) o[i] = __float2bfloat16_rn(x[i]);
+                }
+            }
+            if (ep.out_bf16_t)  // consecutive rows on consecutive lanes: coalesced per column
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    if (i < cnt) ep.out_bf16_t[(long long)(nb + i) * ep.ld_t + m] = __float2bfloat16_rn(x[i]);
         }
     }
     tc_fence_before();
@@ -253,7 +299,7 @@ __global__ void k_outputs_to_params(const float* y, const double* mean, const do
     }
 }
 
-size_t gemm_smem(int BN) { return 2 * (size_t)(kGemmBM * 128 + BN * 128) + 64 + 1024; }
+size_t gemm_smem(int BN) { return kGemmStages * (size_t)(kGemmBM * 128 + BN * 128) + 8 * kGemmStages + 16 + 1024; }
 
 }  // namespace
 }  // namespace spx
