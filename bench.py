@@ -191,7 +191,7 @@ def gpu_arm(args):
     model_path = Path(args.model) if args.model else warmstart.DEFAULT_MODEL
     net = warmstart.WarmStartNet.load(model_path) if (args.warm_start and model_path.exists()) else None
     timings, results = {}, {}
-    for variant in (["warm"] if net is not None else []) + ["plain"]:
+    for variant in ["plain"] + (["warm"] if net is not None else []):
         warmstart.use(net if variant == "warm" else None)
         headline = variant == ("warm" if net is not None else "plain")
         with (ClockSampler(local) if headline else contextlib.nullcontext()) as clocks:

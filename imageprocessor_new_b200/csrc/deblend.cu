@@ -179,34 +179,9 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
         if (has_level) {
             bg0 = background_level;
         } else {
-            // Stage border values into v (sorted below), then take the 10th percentile. The cell's
-            // membership bits (one word per 32 box pixels) go into the xy buffer first, so the
-            // 8-neighbour tests read shared memory instead of the label image; a box with more
-            // words than the buffer holds tests the labels directly.
+            // Stage border values into v (sorted below), then take the 10th percentile.
             int base = 0;
             const int P = box.z * box.w;
-            const int words = (P + 31) >> 5;
-            const bool use_bits = words <= a.cap_px;
-            unsigned* bits = reinterpret_cast<unsigned*>(xy);
-            if (use_bits) {
-                for (int w = 0; w < words; ++w) {
-                    const int k = (w << 5) + lane;
-                    bool in = false;
-                    if (k < P) {
-                        const int yy = k / box.z;
-                        in = in_cell(yy, k - yy * box.z);
-                    }
-                    const unsigned b = __ballot_sync(0xffffffffu, in);
-                    if (lane == 0) bits[w] = b;
-                }
-                __syncwarp();
-            }
-            auto member = [&](int yy, int xx) -> bool {
-                if (!use_bits) return in_cell(yy, xx);
-                if (yy < 0 || xx < 0 || yy >= box.w || xx >= box.z) return false;
-                const int k = yy * box.z + xx;
-                return (bits[k >> 5] >> (k & 31)) & 1u;
-            };
             for (int k0 = 0; k0 < P; k0 += 32) {
                 const int k = k0 + lane;
                 bool border = false;
@@ -214,10 +189,10 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
                 if (k < P) {
                     yy = k / box.z;
                     xx = k - yy * box.z;
-                    if (member(yy, xx)) {
+                    if (in_cell(yy, xx)) {
                         for (int dy = -1; dy <= 1 && !border; ++dy)
                             for (int dx = -1; dx <= 1; ++dx)
-                                if (!member(yy + dy, xx + dx)) { border = true; break; }
+                                if (!in_cell(yy + dy, xx + dx)) { border = true; break; }
                     }
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, border);
