@@ -637,6 +637,48 @@ struct SplineWindow {
     }
 };
 
+// The same window evaluated in FP32 (weights, products and sums), the sampling precision the ray
+// profiles use: sample positions stay FP64 and only their fractional offsets inside the window are
+// rounded to FP32, so a sample differs from the FP64 evaluation by ~1e-7 relative.
+struct SplineWindowF {
+    int fy = -1 << 30, fx = -1 << 30;
+    float c[16];
+    __device__ __forceinline__ static void weights(float t, float* w) {
+        const float s = 1.0f - t;
+        const float k = 1.0f / 6.0f;
+        w[1] = (t * t * (t - 2.0f) * 3.0f + 4.0f) * k;
+        w[2] = (s * s * (s - 2.0f) * 3.0f + 4.0f) * k;
+        w[0] = s * s * s * k;
+        w[3] = 1.0f - w[0] - w[1] - w[2];
+    }
+    __device__ __forceinline__ double at(const double* coef, int hp, int wp, double y, double x) {
+        const double fyd = floor(y), fxd = floor(x);
+        const int iy = (int)fyd, ix = (int)fxd;
+        if (iy != fy || ix != fx) {
+            fy = iy;
+            fx = ix;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int ya = min(max(iy - 1 + a, 0), hp - 1);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) c[a * 4 + b] = (float)coef[ya * wp + min(max(ix - 1 + b, 0), wp - 1)];
+            }
+        }
+        float wy[4], wx[4];
+        weights((float)(y - fyd), wy);
+        weights((float)(x - fxd), wx);
+        float out = 0.0f;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            float row = 0.0f;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) row = fmaf(c[a * 4 + b], wx[b], row);
+            out = fmaf(row, wy[a], out);
+        }
+        return (double)out;
+    }
+};
+
 constexpr int kRadialThreads = 128;
 
 // Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients, a reduction
@@ -726,7 +768,7 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
 // crossing and the parabolic maximum of the outward decrease (halfmax / gradient methods).
 // One 128-thread CTA per cell: the cell's masks and spline coefficients are staged once in
 // shared memory and each thread walks its own rays.
-__global__ void __launch_bounds__(kRadialThreads, 4) k_radial_cd(
+__global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
     int n_angles, double radial_step, int n_radii, double* coef_scratch, MethodOut half_out, MethodOut grad_out) {
     extern __shared__ double sm[];
@@ -792,17 +834,22 @@ __global__ void __launch_bounds__(kRadialThreads, 4) k_radial_cd(
         const double peak = cubic_at(coef, hp, wp, cy + kPad, cx + kPad);
         const double half = peak / 2.0;
         const double inv2s = 1.0 / (2.0 * radial_step);
+        int j_min = 2;  // first gradient candidate: j >= 2 and j * step >= thr
+        while ((double)j_min * radial_step < thr) ++j_min;
         int found_h = 0, found_g = 0;
         for (int ray = tid; ray < n_angles; ray += kRadialThreads) {
             double edge_h = dnan(), edge_g = dnan();
             if (peak > 0.0) {
                 const double ang = (double)ray * (2.0 * kPi / n_angles);
                 const double ux = cos(ang), uy = sin(ang);
-                double h1 = 0, h2 = 0, h3 = 0, h4 = 0;  // p[k-1] .. p[k-4]
+                // Samples are FP32 (SplineWindowF); the profile bookkeeping follows in FP32 and the
+                // edge positions are computed in FP64 from the kept samples.
+                float h1 = 0, h2 = 0, h3 = 0, h4 = 0;  // p[k-1] .. p[k-4]
                 bool crossed = false;
-                double best = -dinf(), gl = 0, gm = 0, gr = 0;
+                float best = -INFINITY, dl = 0, dm = 0, dr = 0;  // p[j-1] - p[j+1] at the best j, j-1, j+1
                 int best_j = -1, first_invalid = n_radii;
-                SplineWindow win;
+                const float halff = (float)half;
+                SplineWindowF win;
                 int mfy = -1 << 30, mfx = -1 << 30;  // mask cell of the last sample and whether all
                 bool mfull = false;                   // four of its corners are in the eroded cell
                 for (int k = 0; k < n_radii; ++k) {
@@ -820,21 +867,23 @@ __global__ void __launch_bounds__(kRadialThreads, 4) k_radial_cd(
                         valid = mfull || inside_bytes(emask, hm, wm, y, x);
                     }
                     if (!valid) { first_invalid = k; break; }
-                    const double p = k == 0 ? peak : win.at(coef, hp, wp, y + kPad, x + kPad);
-                    if (k >= 1 && !crossed && h1 >= half && p < half) {
-                        edge_h = (double)(k - 1) * radial_step + ((h1 - half) / (h1 - p)) * radial_step;
+                    const float p = k == 0 ? (float)peak : (float)win.at(coef, hp, wp, y + kPad, x + kPad);
+                    if (k >= 1 && !crossed && h1 >= halff && p < halff) {
+                        edge_h = (double)(k - 1) * radial_step +
+                                 (((double)h1 - half) / ((double)h1 - (double)p)) * radial_step;
                         crossed = true;
                     }
-                    // Sample k valid makes j = k - 2 a candidate (valid[j - 2] and valid[j + 2]).
+                    // Sample k valid makes j = k - 2 a candidate (valid[j - 2] and valid[j + 2]); its
+                    // outward decrease is (p[j-1] - p[j+1]) / (2 step).
                     const int jj = k - 2;
-                    if (jj >= 2 && jj <= n_radii - 3 && (double)jj * radial_step >= thr) {
-                        const double g = -((h1 - h3) * inv2s);  // -(p[j+1] - p[j-1]) / (2 step)
-                        if (g > best) {
-                            best = g;
+                    if (jj >= j_min && jj <= n_radii - 3) {
+                        const float d = h3 - h1;
+                        if (d > best) {
+                            best = d;
                             best_j = jj;
-                            gm = g;
-                            gl = -((h2 - h4) * inv2s);  // g[j-1]
-                            gr = -((p - h2) * inv2s);   // g[j+1]
+                            dm = d;
+                            dl = h4 - h2;  // j - 1
+                            dr = h2 - p;   // j + 1
                         }
                     }
                     h4 = h3;
@@ -844,9 +893,9 @@ __global__ void __launch_bounds__(kRadialThreads, 4) k_radial_cd(
                 }
                 if (best_j >= 0) {
                     const int jj = best_j;
-                    const bool left_ok = jj - 1 >= 2 && (double)(jj - 1) * radial_step >= thr;
-                    const bool right_ok = jj + 1 <= n_radii - 3 && jj + 3 < first_invalid &&
-                                          (double)(jj + 1) * radial_step >= thr;
+                    const double gm = (double)dm * inv2s, gl = (double)dl * inv2s, gr = (double)dr * inv2s;
+                    const bool left_ok = jj - 1 >= j_min;
+                    const bool right_ok = jj + 1 <= n_radii - 3 && jj + 3 < first_invalid;
                     const double curv = gl - 2.0 * gm + gr;
                     if (left_ok && right_ok && gm >= gl && gm >= gr && gm > 0.01 * peak && curv < -1e-12) {
                         double delta = 0.5 * (gl - gr) / curv;
