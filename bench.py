@@ -185,8 +185,12 @@ def gpu_arm(args):
             dist.barrier()
         return ms, cells, launches
 
+    # Launch shapes from the autotuner (timed on this page's cells, outside the timed region).
+    from imageprocessor_new_b200 import autotune, warmstart
+
+    tuned = autotune.tune(page_d, use_cache=False)["config"] if args.autotune else autotune.current()
+
     # Variants: the NN-warm-started pipeline (when a trained model is present) and the plain one.
-    from imageprocessor_new_b200 import warmstart
 
     model_path = Path(args.model) if args.model else warmstart.DEFAULT_MODEL
     net = warmstart.WarmStartNet.load(model_path) if (args.warm_start and model_path.exists()) else None
@@ -248,6 +252,7 @@ def gpu_arm(args):
         "gpu_launches": int(launches),
         "clocks": clock_summary,
     }
+    line["config"]["launch_shapes"] = tuned
     if net is not None:
         ms_p, cells_p, _ = timings["plain"]
         line["config"]["warm_start"] = f"MLP 1024-256-256-7 ({model_path.name}), plain-start fallback"
@@ -343,6 +348,7 @@ def main():
     ap.add_argument("--page", type=int, default=8192, help="page side in pixels (8192 = the benchmark page)")
     ap.add_argument("--model", default=None, help="warm-start MLP (default: the packaged model)")
     ap.add_argument("--no-warm-start", dest="warm_start", action="store_false")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -78,6 +78,8 @@ SIGNATURES = {
     "spx_extract_patches": (_I, [_P, _I, _D, _I, _I, _P, _I, _P, _P, _P]),
     "spx_hole_coverage": (_I, [_I, _I, _P, _P, _P, _I, _I, _D, _I, _P, _P]),
     "spx_page_finish": (_I, [_P, c_longlong, _D, _D, _D, ctypes.c_ulonglong, _P, _P]),
+    "spx_tune_set": (_I, [ctypes.c_char_p, _I]),
+    "spx_tune_get": (_I, [ctypes.c_char_p, POINTER(c_int)]),
     "spx_histogram": (_I, [_P, _I, _I, _I, _I, _P, _P, _P]),
     "spx_otsu_from_histogram": (_I, [_P, _I, _P, c_longlong, _P, _P, _S, _P]),
     "spx_binarize": (_I, [_P, _I, _I, _I, _P, _D, _I, _P, _P]),

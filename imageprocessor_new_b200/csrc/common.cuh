@@ -16,6 +16,14 @@ namespace spx {
 void set_error(const char* fmt, ...);
 int check_launch(const char* what);
 
+// Launch-shape knobs the autotuner sets (process-wide; none of them changes a result).
+struct Tuning {
+    int fit_warps = 4;          // warps (cells in flight) per block of the LM fit kernels: 2, 4 or 8
+    int fit_blocks_per_sm = 8;  // persistent fit blocks per SM: 2..32
+    int render_tile = 32;       // model render tile edge: 16 or 32 pixels
+};
+Tuning& tuning();
+
 #define SPX_REQUIRE(cond, ...)                 \
     do {                                       \
         if (!(cond)) {                         \

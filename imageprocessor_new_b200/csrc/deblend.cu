@@ -19,7 +19,7 @@
 namespace spx {
 namespace {
 
-constexpr int kFitWarps = 4;  // warps (cells in flight) per block of the fit kernels
+constexpr int kFitWarpsMax = 8;  // largest tuning().fit_warps (sizes the global staging fallback)
 
 // Background map: bg(y, x) = (1 - t[y]) rows[j1[y]-1][x] + t[y] rows[j1[y]][x] (ny > 1),
 // rows[0][x] (ny == 1), or a constant.
@@ -358,11 +358,13 @@ __global__ void k_render_prep(const double* params, const int4* boxes, int n, in
     if ((threadIdx.x & 31) == 0) atomicMax(rmax, local);
 }
 
-constexpr int kRenderTile = 32;  // 32x32 pixels per 256-thread block, four rows per thread
+// Render tiles: Tile x Tile pixels per 256-thread block (16: one pixel per thread, 32: four rows
+// per thread), chosen by tuning().render_tile.
 constexpr int kRenderCap = 2048;
 
 // model(y, x) = sum over cells (increasing index) whose truncated square covers the pixel, each
 // term A exp(-(a^2 + b^2) / 2) for |x - X0| <= r and |y - Y0| <= r (render_models).
+template <int kRenderTile>
 __global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const double* params,
                                                const double* centres, const int* radius,
                                                const int* rmax_dev, double* model, int* overflow) {
@@ -874,25 +876,29 @@ struct FitLayout {
     int* gbuf_xy;
 };
 
-int fit_blocks() {
+int fit_sms() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms * 8;
+    return sms;
 }
 
+int fit_blocks() { return fit_sms() * tuning().fit_blocks_per_sm; }
+
 // Shared memory per block for cap_px pixels per warp; 0 when it does not fit (global staging).
-size_t fit_smem(int cap_px) {
-    const size_t bytes = (size_t)kFitWarps * cap_px * (sizeof(double) + sizeof(int));
+size_t fit_smem(int cap_px, int warps) {
+    const size_t bytes = (size_t)warps * cap_px * (sizeof(double) + sizeof(int));
     return bytes <= 200 * 1024 ? bytes : 0;
 }
 
+// Workspace layout: the staging fallback (cells too large for shared memory) always runs 4 blocks
+// of 8 warps per SM, so a workspace stays valid whatever the autotuner picks later.
 FitLayout fit_layout(void* ws, int cap_px, size_t* bytes) {
     Arena a(ws);
     FitLayout L;
     L.queue = a.take<int>(4);
-    const bool global = fit_smem(cap_px) == 0;
-    const long long warps = global ? (long long)fit_blocks() * kFitWarps : 0;
+    const bool global = fit_smem(cap_px, kFitWarpsMax) == 0;
+    const long long warps = global ? (long long)fit_sms() * 4 * kFitWarpsMax : 0;
     L.gbuf_v = global ? a.take<double>(warps * cap_px) : nullptr;
     L.gbuf_xy = global ? a.take<int>(warps * cap_px) : nullptr;
     if (!global) { a.take<double>(1); a.take<int>(1); }
@@ -920,8 +926,9 @@ int launch_fit(const FitArgs& a0, FitLayout L, cudaStream_t s, Launch&& launch) 
     a.gbuf_v = L.gbuf_v;
     a.gbuf_xy = L.gbuf_xy;
     SPX_CUDA(cudaMemsetAsync(L.queue, 0, sizeof(int), s));
-    const size_t smem = a.gbuf_v ? 0 : fit_smem(a.cap_px);
-    return launch(a, smem);
+    const int warps = a.gbuf_v ? kFitWarpsMax : tuning().fit_warps;
+    const size_t smem = a.gbuf_v ? 0 : fit_smem(a.cap_px, warps);
+    return launch(a, smem, warps, a.gbuf_v ? fit_sms() * 4 : fit_blocks());
 }
 
 struct RenderLayout {
@@ -993,10 +1000,10 @@ int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height
     FitLayout L = fit_layout(workspace, cap_px, nullptr);
     FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
               hm, wm, cap_px, max_iter, nullptr, nullptr, nullptr};
-    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem) -> int {
+    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
         if (smem > 48 * 1024)
             SPX_CUDA(cudaFuncSetAttribute(k_fit_initial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fit_initial<<<fit_blocks(), kFitWarps * 32, smem, s>>>(
+        k_fit_initial<<<blocks, warps * 32, smem, s>>>(
             fa, seeds, background_level, has_level, params, status, iterations,
             WarmStart{init_params, init_ok, background_out, fallback_out, warm_cost_tol});
         return check_launch("k_fit_initial");
@@ -1022,11 +1029,11 @@ int spx_deblend_iteration(const void* img, int dtype, double sign, int height, i
     FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
               hm, wm, cap_px, max_iter, nullptr, nullptr, nullptr};
     const spx_bgmap bg = *background;
-    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem) -> int {
+    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
         if (smem > 48 * 1024)
             SPX_CUDA(cudaFuncSetAttribute(k_fit_iteration, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fit_iteration<<<fit_blocks(), kFitWarps * 32, smem, s>>>(fa, bg, model, radius_cap, params, relaxation,
-                                                                    params_out, status_out, maxstep, iterations);
+        k_fit_iteration<<<blocks, warps * 32, smem, s>>>(fa, bg, model, radius_cap, params, relaxation,
+                                                          params_out, status_out, maxstep, iterations);
         return check_launch("k_fit_iteration");
     });
 }
@@ -1065,9 +1072,14 @@ int spx_render_model(const double* params, const int* boxes, int n, int height, 
         if (int e = check_launch("k_render_prep")) return e;
     }
     if (int e = bin_build(L.bins, L.centres, 2, nullptr, L.valid, n, s)) return e;
-    const dim3 grid((width + kRenderTile - 1) / kRenderTile, (height + kRenderTile - 1) / kRenderTile);
-    k_render<<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
-                                  L.overflow);
+    const int tile = tuning().render_tile;
+    const dim3 grid((width + tile - 1) / tile, (height + tile - 1) / tile);
+    if (tile == 16)
+        k_render<16><<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
+                                          L.overflow);
+    else
+        k_render<32><<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
+                                          L.overflow);
     return check_launch("k_render");
 }
 

@@ -38,6 +38,11 @@ void set_error(const char* fmt, ...) {
     va_end(ap);
 }
 
+Tuning& tuning() {
+    static Tuning t;
+    return t;
+}
+
 int check_launch(const char* what) {
     __atomic_add_fetch(&g_launches, 1ull, __ATOMIC_RELAXED);
     cudaError_t e = cudaGetLastError();
@@ -775,6 +780,38 @@ extern "C" {
 const char* spx_last_error(void) { return spx::g_error; }
 
 int spx_version(void) { return 1; }
+
+int spx_tune_set(const char* knob, int value) {
+    SPX_REQUIRE(knob, "null knob name");
+    Tuning& t = tuning();
+    if (!strcmp(knob, "fit_warps")) {
+        SPX_REQUIRE(value == 2 || value == 4 || value == 8, "fit_warps must be 2, 4 or 8");
+        t.fit_warps = value;
+    } else if (!strcmp(knob, "fit_blocks_per_sm")) {
+        SPX_REQUIRE(value >= 2 && value <= 32, "fit_blocks_per_sm must be in [2, 32]");
+        t.fit_blocks_per_sm = value;
+    } else if (!strcmp(knob, "render_tile")) {
+        SPX_REQUIRE(value == 16 || value == 32, "render_tile must be 16 or 32");
+        t.render_tile = value;
+    } else {
+        set_error("unknown tuning knob '%s'", knob);
+        return SPX_ERR_ARGUMENT;
+    }
+    return SPX_OK;
+}
+
+int spx_tune_get(const char* knob, int* value) {
+    SPX_REQUIRE(knob && value, "null pointer");
+    const Tuning& t = tuning();
+    if (!strcmp(knob, "fit_warps")) *value = t.fit_warps;
+    else if (!strcmp(knob, "fit_blocks_per_sm")) *value = t.fit_blocks_per_sm;
+    else if (!strcmp(knob, "render_tile")) *value = t.render_tile;
+    else {
+        set_error("unknown tuning knob '%s'", knob);
+        return SPX_ERR_ARGUMENT;
+    }
+    return SPX_OK;
+}
 
 unsigned long long spx_launch_count(void) { return __atomic_load_n(&spx::g_launches, __ATOMIC_RELAXED); }
 

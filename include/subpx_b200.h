@@ -56,6 +56,12 @@ const char* spx_last_error(void);
 int spx_version(void);
 /* Number of kernel launches this library has issued in the process (for launch accounting). */
 unsigned long long spx_launch_count(void);
+/* Launch-shape knobs (process-wide, chosen by the autotuner; none changes a result):
+ * "fit_warps" (2, 4, 8 cells in flight per block of the LM fit kernels), "fit_blocks_per_sm"
+ * (2..32 persistent fit blocks per SM), "render_tile" (16 or 32 pixel model-render tiles).
+ * No reference counterpart. */
+int spx_tune_set(const char* knob, int value);
+int spx_tune_get(const char* knob, int* value);
 /* Number of SMs of the current device, and whether it is an sm_100 part (1) or not (0). */
 int spx_device_info(int* sm_count, int* is_sm100);
 
