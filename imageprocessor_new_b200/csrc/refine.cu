@@ -73,6 +73,53 @@ __device__ __forceinline__ Roi make_roi(const int* row, int pad, int H, int W) {
     return r;
 }
 
+// k-th smallest (0-based) of n 16-bit values value(i) by a warp: two 8-bit radix passes over a
+// 256-bin shared-memory histogram, each digit found by a warp prefix sum of per-lane bin groups.
+template <typename F>
+__device__ int warp_select_u16(F value, int n, int k, int* hist, int lane) {
+    int prefix = 0;
+    for (int shift = 8; shift >= 0; shift -= 8) {
+        for (int b = lane; b < 256; b += 32) hist[b] = 0;
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const int v = value(i);
+            if (shift == 0 ? (v >> 8) == (prefix >> 8) : true) atomicAdd(&hist[(v >> shift) & 255], 1);
+        }
+        __syncwarp();
+        int c[8], mine = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = hist[lane * 8 + j];
+            mine += c[j];
+        }
+        int incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        const int excl = incl - mine;
+        const unsigned owner = __ballot_sync(0xffffffffu, excl <= k && k < incl);
+        const int src = __ffs(owner) - 1;
+        int digit = 0, rest = k - excl;
+        if (lane == src) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (rest < c[j]) {
+                    digit = lane * 8 + j;
+                    break;
+                }
+                rest -= c[j];
+            }
+        }
+        digit = __shfl_sync(0xffffffffu, digit, src);
+        k = __shfl_sync(0xffffffffu, rest, src);
+        prefix |= digit << shift;
+        __syncwarp();
+    }
+    return prefix;
+}
+
 // Median of the ROI's top and bottom 2 rows and left and right 2 columns (full height, so the four
 // 2x2 corners count twice), or of the whole ROI when it is too small, as _bg_from_border:
 // np.median = mean of the two middle values for an even count.
@@ -102,6 +149,14 @@ __device__ double border_median(const void* img, int dtype, int W, const Roi& r,
         }
         return load_px(img, dtype, (long long)(r.y0 + yy) * W + (r.x0 + xx));
     };
+    if (dtype == SPX_U8 || dtype == SPX_U16) {
+        // Integer images: the two middle order statistics by radix selection (exact).
+        int* hist = reinterpret_cast<int*>(keys);
+        auto iv = [&](int i) { return (int)value(i); };
+        const int a = warp_select_u16(iv, n, (n - 1) / 2, hist, lane);
+        const int b = (n & 1) ? a : warp_select_u16(iv, n, n / 2, hist, lane);
+        return __ddiv_rn(__dadd_rn((double)a, (double)b), 2.0);
+    }
     if (n <= kSortCap) {
         int m = 1;
         while (m < n) m <<= 1;

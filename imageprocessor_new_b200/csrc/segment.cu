@@ -343,6 +343,12 @@ struct Geo {
     __device__ __forceinline__ int canon(int y, int x) const {
         return conn == 8 ? ((((y >> 1) * Wb + (x >> 1)) << 2) | ((y & 1) << 1) | (x & 1)) : y * W + x;
     }
+    // Foreground bitmap: bit x & 31 of word y * words_per_row + x / 32. Only foreground pixels have
+    // an entry in the parents array; readers test the bitmap first.
+    __device__ __forceinline__ int words_per_row() const { return (W + 63) / 64 * 2; }
+    __device__ __forceinline__ bool fg(const unsigned* bits, int y, int x) const {
+        return (bits[(long long)y * words_per_row() + (x >> 5)] >> (x & 31)) & 1u;
+    }
 };
 
 __device__ __forceinline__ bool is_fg(double v, double t, int invert) { return invert ? v <= t : v > t; }
@@ -383,7 +389,8 @@ __device__ void unite(int* p, int a, int b, unsigned int* roots) {
 
 __global__ void __launch_bounds__(256) k_local_ccl(const void* img, int dtype, Geo g,
                                                    const double* thr_dev, double thr_fixed,
-                                                   int invert, int* parents, unsigned int* roots) {
+                                                   int invert, int* parents, unsigned int* roots,
+                                                   unsigned int* fgbits) {
     __shared__ int par[kTilePx];
     __shared__ unsigned char fg[kTilePx];  // indexed by raster position inside the tile
     const int tx0 = blockIdx.x * kTileW, ty0 = blockIdx.y * kTileH;
@@ -400,6 +407,9 @@ __global__ void __launch_bounds__(256) k_local_ccl(const void* img, int dtype, G
         fg[k] = f;
         const int l = lidx(yl, xl);
         par[l] = f ? l : -1;
+        // A warp holds 32 consecutive pixels of one tile row: one bitmap word.
+        const unsigned word = __ballot_sync(0xffffffffu, f);
+        if ((threadIdx.x & 31) == 0 && y < g.H) fgbits[(long long)y * g.words_per_row() + (x >> 5)] = word;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < kTilePx; k += blockDim.x) {
@@ -419,10 +429,7 @@ __global__ void __launch_bounds__(256) k_local_ccl(const void* img, int dtype, G
         const int yl = k / kTileW, xl = k % kTileW, y = ty0 + yl, x = tx0 + xl;
         if (y >= g.H || x >= g.W) continue;
         const int gid = g.canon(y, x);
-        if (!fg[k]) {
-            parents[gid] = -1;
-            continue;
-        }
+        if (!fg[k]) continue;
         const int l = lidx(yl, xl);
         const int r = find_root_volatile(par, l);
         // Global id of the local root.
@@ -443,7 +450,8 @@ __global__ void __launch_bounds__(256) k_local_ccl(const void* img, int dtype, G
 
 // Unions across tile borders. One thread per border pixel of a tile: top row (neighbours above),
 // left column (neighbours to the left), right column (the up-right neighbour in the next tile).
-__global__ void k_border_merge(Geo g, int* parents, unsigned int* roots, int tiles_x, int tiles_y) {
+__global__ void k_border_merge(Geo g, int* parents, unsigned int* roots, const unsigned int* fgbits, int tiles_x,
+                               int tiles_y) {
     const int per_tile = kTileW + 2 * kTileH;
     const long long total = (long long)tiles_x * tiles_y * per_tile;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total;
@@ -456,15 +464,14 @@ __global__ void k_border_merge(Geo g, int* parents, unsigned int* roots, int til
         else if (e < kTileW + kTileH) { y = ty0 + (e - kTileW); x = tx0; }
         else { y = ty0 + (e - kTileW - kTileH); x = tx0 + kTileW - 1; }
         if (y >= g.H || x >= g.W) continue;
+        if (!g.fg(fgbits, y, x)) continue;
         const int me = g.canon(y, x);
-        if (parents[me] < 0) continue;
         auto link = [&](int yy, int xx) {
             if (yy < 0 || xx < 0 || xx >= g.W) return;
             // Only neighbours in another tile.
             if (yy >= ty0 && xx >= tx0 && xx < tx0 + kTileW) return;
-            const int other = g.canon(yy, xx);
-            if (parents[other] < 0) return;
-            unite(parents, me, other, roots);
+            if (!g.fg(fgbits, yy, xx)) return;
+            unite(parents, me, g.canon(yy, xx), roots);
         };
         if (e < kTileW) {  // top row: (y-1, x) and, for 8-connectivity, (y-1, x-1), (y-1, x+1)
             link(y - 1, x);
@@ -569,8 +576,8 @@ __global__ void k_stats_init(int* stats, unsigned long long* sums, int k1) {
 // runs of lanes; a run's head lane adds the run's bbox, area and coordinate sums with one set of
 // atomics. Background runs are reduced per block first.
 __global__ void __launch_bounds__(256) k_finish(Geo g, const int* parents, const unsigned int* roots,
-                                                const int* prefix, int* labels, int* stats,
-                                                unsigned long long* sums) {
+                                                const int* prefix, const unsigned int* fgbits, int* labels,
+                                                int* stats, unsigned long long* sums) {
     __shared__ long long s_bg[7];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = blockIdx.x * 32 + lane;
@@ -578,10 +585,10 @@ __global__ void __launch_bounds__(256) k_finish(Geo g, const int* parents, const
     const bool inside = x < g.W && y < g.H;
     int lab = -1;  // -1 outside the image
     if (inside) {
-        int p = parents[g.canon(y, x)];
-        if (p < 0) {
+        if (!g.fg(fgbits, y, x)) {
             lab = 0;
         } else {
+            int p = parents[g.canon(y, x)];
             int q = parents[p];
             while (q != p) {
                 p = q;
@@ -671,6 +678,7 @@ struct CclLayout {
     int* prefix;
     int* block_sums;
     int* scratch_count;
+    unsigned int* fgbits;  // foreground bitmap, H x words-per-row
 };
 constexpr int kScanPerBlock = 4096;  // bitmap words per prefix block (1024 threads x 4)
 
@@ -686,6 +694,7 @@ CclLayout ccl_layout(void* ws, int H, int W, size_t* bytes) {
     L.prefix = a.take<int>(L.words);
     L.block_sums = a.take<int>(L.scan_blocks + 1);
     L.scratch_count = a.take<int>(4);
+    L.fgbits = a.take<unsigned int>((long long)H * ((W + 63) / 64 * 2));
     if (bytes) *bytes = a.used;
     return L;
 }
@@ -1027,10 +1036,10 @@ int spx_ccl_label(const void* img, int dtype, int height, int width, const doubl
         SPX_CUDA(cudaMemsetAsync(L.parents, 0xff, L.canon_n * sizeof(int), s));
     const int tiles_x = (width + kTileW - 1) / kTileW, tiles_y = (height + kTileH - 1) / kTileH;
     k_local_ccl<<<dim3(tiles_x, tiles_y), 256, 0, s>>>(img, dtype, g, threshold_dev, fixed_threshold,
-                                                       invert, L.parents, L.roots);
+                                                       invert, L.parents, L.roots, L.fgbits);
     if (int e = check_launch("k_local_ccl")) return e;
     const long long border = (long long)tiles_x * tiles_y * (kTileW + 2 * kTileH);
-    k_border_merge<<<grid_for(border, 256), 256, 0, s>>>(g, L.parents, L.roots, tiles_x, tiles_y);
+    k_border_merge<<<grid_for(border, 256), 256, 0, s>>>(g, L.parents, L.roots, L.fgbits, tiles_x, tiles_y);
     if (int e = check_launch("k_border_merge")) return e;
     SPX_REQUIRE(L.scan_blocks <= 1024 * 64, "image too large for the label prefix");
     k_popc_block_sums<<<L.scan_blocks, 1024, 0, s>>>(L.roots, L.words, kScanPerBlock, L.block_sums);
@@ -1056,7 +1065,7 @@ int spx_ccl_finish(int* labels, int height, int width, int connectivity, int num
     k_stats_init<<<grid_for(k1, 256), 256, 0, s>>>(stats, sums, k1);
     if (int e = check_launch("k_stats_init")) return e;
     k_finish<<<dim3((width + 31) / 32, (height + 7) / 8), 256, 0, s>>>(g, L.parents, L.roots, L.prefix,
-                                                                       labels, stats, sums);
+                                                                       L.fgbits, labels, stats, sums);
     if (int e = check_launch("k_finish")) return e;
     k_stats_final<<<grid_for(k1, 256), 256, 0, s>>>(stats, sums, centroids, k1);
     return check_launch("k_stats_final");
