@@ -52,7 +52,14 @@ class GemmEpilogue(ctypes.Structure):
                 ("out_bf16", c_void_p), ("ld_bf16", c_int), ("out_bf16_t", c_void_p), ("ld_t", c_int)]
 
 
+class FitOptions(ctypes.Structure):
+    """spx_fit_options: LM arithmetic (FIT_F64 / FIT_F32) and the plain fits' relative cost tolerance."""
+    _fields_ = [("precision", c_int), ("cost_tol", c_double)]
+
+
+FIT_F64, FIT_F32 = 0, 1
 _BG = POINTER(BgMap)
+_FO = POINTER(FitOptions)
 _MO = POINTER(MethodOut)
 
 # name -> (restype, argtypes)
@@ -68,7 +75,7 @@ SIGNATURES = {
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
     "spx_gemm_bf16": (_I, [_P, _I, _P, _I, _I, _I, _I, POINTER(GemmEpilogue), _P, _P]),
     "spx_deblend_initial_warm": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _D, _I, _I, _P, _P, _D, _P,
-                                      _P, _P, _P, _P, _P, _S, _P]),
+                                      _P, _P, _P, _P, _FO, _P, _S, _P]),
     "spx_mlp_loss_grad": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _P, _P]),
     "spx_rowsum_bf16": (_I, [_P, _I, _I, _P, _P]),
     "spx_adamw": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -102,7 +109,7 @@ SIGNATURES = {
     "spx_deblend_initial": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _D, _I, _I, _P, _P, _P, _P,
                                  _S, _P]),
     "spx_deblend_iteration": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _I, _I, _I, _BG, _P, _I, _P, _D, _I, _P,
-                                   _P, _P, _P, _P, _S, _P]),
+                                   _P, _P, _P, _FO, _P, _S, _P]),
     "spx_render_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_render_model": (_I, [_P, _P, _I, _I, _I, _I, _P, _P, _S, _P]),
     "spx_render_overflow": (_I, [_P, _I, _I, _I, POINTER(c_int), _I, _P]),

@@ -129,6 +129,7 @@ def measure_cds(
     device: int = 0,
     metrics_only: bool = False,
     summary_only: bool = False,
+    fit_precision: str = "fp64",
     **other,
 ) -> CDResult | CDSummary:
     """Voronoi cells and their CDs (subpx/cd.py:44-380) on the GPU.
@@ -137,6 +138,10 @@ def measure_cds(
     measurements follow the reference CPU path operation for operation (FP64). Parameters of the
     reference's other method families (``nominal_cd``, ``psf_fwhm``, ``half_area_level``, ...) are
     accepted in ``other`` and must keep their defaults.
+
+    ``fit_precision`` (no reference counterpart) sets the deblending LM's arithmetic: "fp64" is the
+    reference's; "fp32" runs the per-pixel residuals, Jacobian and sums in FP32 (compensated J^T r
+    and cost, FP64 totals) with the solve, acceptance and stop rule (relative cost drop 1e-7) in FP64.
     """
     on_device = isinstance(image, torch.Tensor) and image.is_cuda
     img = image if on_device else np.asarray(image.detach().cpu().numpy() if isinstance(image, torch.Tensor)
@@ -147,6 +152,9 @@ def measure_cds(
                         deblend_tolerance=deblend_tolerance, pixel_size=pixel_size, unit=unit,
                         metrics_only=metrics_only, summary_only=summary_only, peak_min_distance=peak_min_distance,
                         background_tile=background_tile, background_level=background_level)
+    from .deblend import fit_options
+
+    fit_options(fit_precision)  # ValueError for an unknown arithmetic
     if backend not in {"cpu", "gpu", "auto"}:
         raise ValueError("backend must be 'cpu', 'gpu' or 'auto'")
     if cell_backend not in {None, "cpu", "gpu"}:
@@ -170,7 +178,7 @@ def measure_cds(
                             background_level=background_level, background_tile=background_tile,
                             deblend_iterations=int(deblend_iterations), deblend_tolerance=float(deblend_tolerance),
                             pixel_size=float(pixel_size), unit=unit, device=int(device), metrics_only=metrics_only,
-                            summary_only=bool(summary_only))
+                            summary_only=bool(summary_only), fit_precision=fit_precision)
 
 
 def _segment(img_d: torch.Tensor, threshold: str, invert: bool):
@@ -329,7 +337,7 @@ def _revise_seeds(dbl: Deblender, state, seeds_xy, pitch, oversized_d, *, drop_f
 
 def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_angles, radial_step, fit_fraction,
                  background_level, background_tile, deblend_iterations, deblend_tolerance, pixel_size, unit, device,
-                 metrics_only, summary_only):
+                 metrics_only, summary_only, fit_precision="fp64"):
     started = time.perf_counter()
     seconds = {}
     height, width = tuple(img.shape)
@@ -378,7 +386,8 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         "radial_step": float(radial_step), "smooth_sigma": 0.0, "fit_fraction": float(fit_fraction),
         "cell_backend": "gpu", "measurement_backend": "gpu", "device": int(device),
         "metrics_only": bool(metrics_only), "summary_only": bool(summary_only),
-        "deblend_tolerance": float(deblend_tolerance), "segmentation_rescaled": bool(rescaled),
+        "deblend_tolerance": float(deblend_tolerance), "fit_precision": fit_precision,
+        "segmentation_rescaled": bool(rescaled),
         "components_before_filter": int(components_before_filter),
         "coordinates": "global [x, y] pixels; images indexed [y, x]", "seconds": seconds,
     }
@@ -388,7 +397,7 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
 
     def make_deblender(cells_, tile):
         return Deblender(img_d, sign, cells_, exclude_d=exclude_for(component_ids), tile=tile,
-                         background_level=level, tolerance=deblend_tolerance)
+                         background_level=level, tolerance=deblend_tolerance, fit_precision=fit_precision)
 
     from .deblend import auto_tile
 

@@ -98,8 +98,8 @@ __device__ __forceinline__ int fit_status_of(const double* p, double cap, int j,
 
 // Compacts cell j's mask pixels: v[slot] = value(yy, xx) (box-local coords), xy[slot] packed.
 // Returns the pixel count (same on all lanes).
-template <typename F>
-__device__ int stage_cell(int4 box, int j, const int* vor, int W, double* v, int* xy, int lane, F value) {
+template <typename T, typename F>
+__device__ int stage_cell(int4 box, int j, const int* vor, int W, T* v, int* xy, int lane, F value) {
     int base = 0;
     const int P = box.z * box.w;
     for (int k0 = 0; k0 < P; k0 += 32) {
@@ -114,7 +114,7 @@ __device__ int stage_cell(int4 box, int j, const int* vor, int W, double* v, int
         const unsigned m = __ballot_sync(0xffffffffu, in);
         if (in) {
             const int slot = base + __popc(m & ((1u << lane) - 1u));
-            v[slot] = value(yy, xx);
+            v[slot] = (T)value(yy, xx);
             xy[slot] = xx | (yy << 16);
         }
         base += __popc(m);
@@ -133,6 +133,7 @@ struct FitArgs {
     int n, hm, wm;
     int cap_px;       // per-warp pixel capacity of the staging buffers
     int max_iter;
+    double cost_tol;  // relative cost drop that ends a plain-start fit (1e-12: the reference's rule)
     int* queue;       // work counter (reset by the host before the launch)
     double* gbuf_v;   // global staging when shared memory is too small (else null)
     int* gbuf_xy;
@@ -149,21 +150,24 @@ struct WarmStart {
     double cost_tol;  // relative cost drop that ends a warm-started fit
 };
 
+// T: type of the staged cell values and of the LM's per-pixel arithmetic (double or float).
+template <typename T>
 __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
                               double* params, uint8_t* status, int* iters, WarmStart warm) {
     extern __shared__ unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double* v;
+    double* vbuf;  // the warp's staging buffer: border values (double), then the cell's values (T)
     int* xy;
     if (a.gbuf_v) {
         const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
-        v = a.gbuf_v + w * a.cap_px;
+        vbuf = a.gbuf_v + w * a.cap_px;
         xy = a.gbuf_xy + w * a.cap_px;
     } else {
-        v = reinterpret_cast<double*>(smem) + (long long)warp * a.cap_px;
+        vbuf = reinterpret_cast<double*>(smem) + (long long)warp * a.cap_px;
         xy = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + (long long)(blockDim.x >> 5) * a.cap_px) +
              (long long)warp * a.cap_px;
     }
+    T* v = reinterpret_cast<T*>(vbuf);
     while (true) {
         int j = 0;
         if (lane == 0) j = atomicAdd(a.queue, 1);
@@ -196,16 +200,16 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
                     }
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, border);
-                if (border) v[base + __popc(m & ((1u << lane) - 1u))] = a.img.at(box.y + yy, box.x + xx);
+                if (border) vbuf[base + __popc(m & ((1u << lane) - 1u))] = a.img.at(box.y + yy, box.x + xx);
                 base += __popc(m);
             }
             __syncwarp();
             int m2 = 1;
             while (m2 < base) m2 <<= 1;
-            for (int i = base + lane; i < m2; i += 32) v[i] = dinf();
+            for (int i = base + lane; i < m2; i += 32) vbuf[i] = dinf();
             __syncwarp();
-            warp_bitonic_sort(v, m2, lane);
-            bg0 = base > 0 ? sorted_percentile(v, base, 0.1) : 0.0;
+            warp_bitonic_sort(vbuf, m2, lane);
+            bg0 = base > 0 ? sorted_percentile(vbuf, base, 0.1) : 0.0;
             __syncwarp();
         }
         const int n = stage_cell(box, j, a.vor, a.img.W, v, xy, lane, [&](int yy, int xx) {
@@ -213,12 +217,12 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
         });
         // initial_params: amplitude = peak, centre = seed, sigma from the core's second moment.
         double peak = -dinf();
-        for (int k = lane; k < n; k += 32) peak = fmax(peak, v[k]);
+        for (int k = lane; k < n; k += 32) peak = fmax(peak, (double)v[k]);
         peak = warp_max(peak);
         const double sx = seeds[2LL * j] - box.x, sy = seeds[2LL * j + 1] - box.y;
         double tot = 0.0, mom = 0.0, amax = 0.0;
         for (int k = lane; k < n; k += 32) {
-            const double d = v[k];
+            const double d = (double)v[k];
             amax = fmax(amax, fabs(d));
             if (d > 0.2 * peak) {
                 const double dx = (double)(xy[k] & 0xffff) - sx, dy = (double)(xy[k] >> 16) - sy;
@@ -256,7 +260,7 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
             fell_back = !done;
         }
         if (!done) {
-            it += warp_lm_fit(p, v, xy, n, cap, amp_cap, a.max_iter, lane);
+            it += warp_lm_fit(p, v, xy, n, cap, amp_cap, a.max_iter, lane, a.cost_tol);
             st = fit_status_of(p, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
         }
         if (lane == 0) {
@@ -273,19 +277,20 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
 // One deblending iteration for every cell: clean (image - background - (model - own)), LM from the
 // current params, relaxation p + relax * (fitted - p) (non-finite components step 0), status of
 // the relaxed params, and max |step[1:]| (NaN unless the cell is "ok" with a finite fit).
+template <typename T>
 __global__ void k_fit_iteration(FitArgs a, spx_bgmap bg, const double* model, int radius_cap,
                                 const double* params, double relaxation, double* params_out,
                                 uint8_t* status_out, double* maxstep, int* iters) {
     extern __shared__ unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double* v;
+    T* v;
     int* xy;
     if (a.gbuf_v) {
         const long long w = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
-        v = a.gbuf_v + w * a.cap_px;
+        v = reinterpret_cast<T*>(a.gbuf_v + w * a.cap_px);
         xy = a.gbuf_xy + w * a.cap_px;
     } else {
-        v = reinterpret_cast<double*>(smem) + (long long)warp * a.cap_px;
+        v = reinterpret_cast<T*>(reinterpret_cast<double*>(smem) + (long long)warp * a.cap_px);
         xy = reinterpret_cast<int*>(reinterpret_cast<double*>(smem) + (long long)(blockDim.x >> 5) * a.cap_px) +
              (long long)warp * a.cap_px;
     }
@@ -312,12 +317,12 @@ __global__ void k_fit_iteration(FitArgs a, spx_bgmap bg, const double* model, in
             return (raw - bg_at(bg, y, x)) - (model[(long long)y * a.img.W + x] - own);
         });
         double amax = 0.0;
-        for (int k = lane; k < n; k += 32) amax = fmax(amax, fabs(v[k]));
+        for (int k = lane; k < n; k += 32) amax = fmax(amax, fabs((double)v[k]));
         amax = warp_max(amax);
         double p[6];
         for (int i = 0; i < 6; ++i) p[i] = p0[i];
         const double cap = a.caps[j];
-        const int it = warp_lm_fit(p, v, xy, n, cap, 3.0 * fmax(amax, 1e-12), a.max_iter, lane);
+        const int it = warp_lm_fit(p, v, xy, n, cap, 3.0 * fmax(amax, 1e-12), a.max_iter, lane, a.cost_tol);
         if (lane == 0) {
             double q[6];
             bool finite = true;
@@ -981,17 +986,64 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
                         size_t workspace_bytes, void* stream) {
     return spx_deblend_initial_warm(img, dtype, sign, height, width, voronoi, boxes, caps, seeds, n, hm, wm,
                                     max_cell_pixels, background_level, has_level, max_iter, nullptr, nullptr, 1e-12,
-                                    params, status, iterations, nullptr, nullptr, workspace, workspace_bytes, stream);
+                                    params, status, iterations, nullptr, nullptr, nullptr, workspace,
+                                    workspace_bytes, stream);
 }
+
+}  // extern "C"
+
+namespace {
+
+// The fit options with their defaults (FP64, the reference's 1e-12 stop rule) and checks.
+int read_fit_options(const spx_fit_options* o, bool* f32, double* cost_tol) {
+    *f32 = o && o->precision == SPX_FIT_F32;
+    *cost_tol = o ? o->cost_tol : 1e-12;
+    SPX_REQUIRE(!o || o->precision == SPX_FIT_F64 || o->precision == SPX_FIT_F32, "bad fit precision");
+    SPX_REQUIRE(*cost_tol > 0.0 && *cost_tol < 1.0, "fit cost_tol must be in (0, 1)");
+    return SPX_OK;
+}
+
+template <typename T>
+int launch_fit_initial(const FitArgs& a0, FitLayout L, cudaStream_t s, const double* seeds, double background_level,
+                       int has_level, double* params, uint8_t* status, int* iterations, WarmStart warm) {
+    return launch_fit(a0, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
+        if (smem > 48 * 1024)
+            SPX_CUDA(cudaFuncSetAttribute(k_fit_initial<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_fit_initial<T><<<blocks, warps * 32, smem, s>>>(fa, seeds, background_level, has_level, params, status,
+                                                           iterations, warm);
+        return check_launch("k_fit_initial");
+    });
+}
+
+template <typename T>
+int launch_fit_iteration(const FitArgs& a0, FitLayout L, cudaStream_t s, const spx_bgmap& bg, const double* model,
+                         int radius_cap, const double* params, double relaxation, double* params_out,
+                         uint8_t* status_out, double* maxstep, int* iterations) {
+    return launch_fit(a0, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
+        if (smem > 48 * 1024)
+            SPX_CUDA(cudaFuncSetAttribute(k_fit_iteration<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_fit_iteration<T><<<blocks, warps * 32, smem, s>>>(fa, bg, model, radius_cap, params, relaxation,
+                                                             params_out, status_out, maxstep, iterations);
+        return check_launch("k_fit_iteration");
+    });
+}
+
+}  // namespace
+
+extern "C" {
 
 int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                              const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
                              int max_cell_pixels, double background_level, int has_level, int max_iter,
                              const double* init_params, const uint8_t* init_ok, double warm_cost_tol,
                              double* params, uint8_t* status, int* iterations, double* background_out,
-                             uint8_t* fallback_out, void* workspace, size_t workspace_bytes, void* stream) {
+                             uint8_t* fallback_out, const spx_fit_options* options, void* workspace,
+                             size_t workspace_bytes, void* stream) {
     SPX_REQUIRE(warm_cost_tol > 0.0, "warm_cost_tol must be positive");
     SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
+    bool f32 = false;
+    double cost_tol = 1e-12;
+    if (int e = read_fit_options(options, &f32, &cost_tol)) return e;
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && voronoi && boxes && caps && seeds && params && status && workspace, "null pointer");
     SPX_REQUIRE(workspace_bytes >= spx_fit_workspace_bytes(max_cell_pixels), "workspace too small");
@@ -999,24 +1051,24 @@ int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height
     const int cap_px = pow2_at_least(max_cell_pixels > 0 ? max_cell_pixels : 1);
     FitLayout L = fit_layout(workspace, cap_px, nullptr);
     FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
-              hm, wm, cap_px, max_iter, nullptr, nullptr, nullptr};
-    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
-        if (smem > 48 * 1024)
-            SPX_CUDA(cudaFuncSetAttribute(k_fit_initial, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fit_initial<<<blocks, warps * 32, smem, s>>>(
-            fa, seeds, background_level, has_level, params, status, iterations,
-            WarmStart{init_params, init_ok, background_out, fallback_out, warm_cost_tol});
-        return check_launch("k_fit_initial");
-    });
+              hm, wm, cap_px, max_iter, cost_tol, nullptr, nullptr, nullptr};
+    const WarmStart warm{init_params, init_ok, background_out, fallback_out, warm_cost_tol};
+    return f32 ? launch_fit_initial<float>(a, L, s, seeds, background_level, has_level, params, status, iterations,
+                                           warm)
+               : launch_fit_initial<double>(a, L, s, seeds, background_level, has_level, params, status,
+                                            iterations, warm);
 }
 
 int spx_deblend_iteration(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                           const int* boxes, const double* caps, int n, int hm, int wm, int max_cell_pixels,
                           const spx_bgmap* background, const double* model, int radius_cap,
                           const double* params, double relaxation, int max_iter, double* params_out,
-                          uint8_t* status_out, double* maxstep, int* iterations, void* workspace,
-                          size_t workspace_bytes, void* stream) {
+                          uint8_t* status_out, double* maxstep, int* iterations, const spx_fit_options* options,
+                          void* workspace, size_t workspace_bytes, void* stream) {
     SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
+    bool f32 = false;
+    double cost_tol = 1e-12;
+    if (int e = read_fit_options(options, &f32, &cost_tol)) return e;
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && voronoi && boxes && caps && background && model && params && params_out && status_out &&
                     maxstep && workspace,
@@ -1027,15 +1079,11 @@ int spx_deblend_iteration(const void* img, int dtype, double sign, int height, i
     const int cap_px = pow2_at_least(max_cell_pixels > 0 ? max_cell_pixels : 1);
     FitLayout L = fit_layout(workspace, cap_px, nullptr);
     FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
-              hm, wm, cap_px, max_iter, nullptr, nullptr, nullptr};
-    const spx_bgmap bg = *background;
-    return launch_fit(a, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
-        if (smem > 48 * 1024)
-            SPX_CUDA(cudaFuncSetAttribute(k_fit_iteration, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fit_iteration<<<blocks, warps * 32, smem, s>>>(fa, bg, model, radius_cap, params, relaxation,
-                                                          params_out, status_out, maxstep, iterations);
-        return check_launch("k_fit_iteration");
-    });
+              hm, wm, cap_px, max_iter, cost_tol, nullptr, nullptr, nullptr};
+    return f32 ? launch_fit_iteration<float>(a, L, s, *background, model, radius_cap, params, relaxation, params_out,
+                                             status_out, maxstep, iterations)
+               : launch_fit_iteration<double>(a, L, s, *background, model, radius_cap, params, relaxation,
+                                              params_out, status_out, maxstep, iterations);
 }
 
 int spx_render_overflow(void* workspace, int n, int height, int width, int* flag_out, int reset, void* stream) {

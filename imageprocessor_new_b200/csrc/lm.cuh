@@ -10,7 +10,13 @@
 // Layout: the cell's mask pixels are compacted into (value, packed local x | y << 16) arrays; lanes
 // stride over them, the 27 sums are all-reduced so every lane holds identical totals, and
 // every lane solves the damped 6x6 system (Cholesky, fully unrolled in registers) and takes the
-// same decisions, so the warp never diverges on control flow. Arithmetic is FP64.
+// same decisions, so the warp never diverges on control flow.
+//
+// Two arithmetics, chosen by the type of the staged values. double: every sum in FP64 (the
+// reference's arithmetic). float: the residuals, the model, the Jacobian and the per-lane sums run
+// in FP32 -- J^T J by plain FMA (it only shapes the step), J^T r and the cost by Kahan-compensated
+// summation (they set the fixed point and the acceptance test) -- and the lane totals are added in
+// FP64; the damped solve, the clipping, the acceptance test and the stop rule stay FP64.
 #pragma once
 
 #include "common.cuh"
@@ -143,6 +149,62 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const double
     return warp_sum(acc);
 }
 
+// Kahan-compensated FP32 running sum; s - c is the total to about twice FP32 precision.
+struct KahanF {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float x) {
+        const float y = x - c;
+        const float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double total() const { return (double)s - (double)c; }
+};
+
+// Exact float of a 16-bit unsigned field: the field as the mantissa of 2^23, minus 2^23.
+__device__ __forceinline__ float u16_to_float(int u) { return __int_as_float(0x4b000000 | u) - 8388608.0f; }
+
+// The FP32 pass: as warp_normal_pass above with the per-pixel arithmetic and lane sums in FP32
+// (ROI-local coordinates keep dx, dy within a few ulp of 64) and FP64 warp totals.
+__device__ __forceinline__ double warp_normal_pass(const double* q, const float* v, const int* xy, int n, int lane,
+                                                   double* s) {
+    float jj[21];
+#pragma unroll
+    for (int i = 0; i < 21; ++i) jj[i] = 0.0f;
+    KahanF jr[6], cost;
+    const float e1 = (float)exp(q[3]), e3 = (float)exp(q[5]);
+    const float A = (float)q[0], x0 = (float)q[1], y0 = (float)q[2], u2 = (float)q[4];
+    for (int k = lane; k < n; k += 32) {
+        const int c = xy[k];
+        const float dx = u16_to_float(c & 0xffff) - x0, dy = u16_to_float(c >> 16) - y0;
+        const float a = fmaf(e1, dx, u2 * dy), b = e3 * dy;
+        const float shape = __expf(-0.5f * fmaf(a, a, b * b));
+        const float model = A * shape;
+        const float r = v[k] - model;
+        cost.add(r * r);
+        float J[6];
+        J[0] = shape;
+        J[1] = model * (a * e1);
+        J[2] = model * fmaf(a, u2, b * e3);
+        J[3] = -model * (a * e1 * dx);
+        J[4] = -model * (a * dy);
+        J[5] = -model * (b * e3 * dy);
+        int t = 0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i)
+#pragma unroll
+            for (int j = i; j < 6; ++j, ++t) jj[t] = fmaf(J[i], J[j], jj[t]);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) jr[i].add(J[i] * r);
+    }
+#pragma unroll
+    for (int i = 0; i < 21; ++i) s[i] = (double)jj[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s[21 + i] = jr[i].total();
+    warp_allreduce27(s, lane);
+    return warp_sum(cost.total());
+}
+
 // Fits p (ROI-local, identical on all lanes) to the n compacted pixels. Returns the number of
 // iterations run. `cap` is the cell's sigma cap, `amp_cap` 3 * max(max|v|, 1e-12).
 //
@@ -151,8 +213,9 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const double
 // params. The arithmetic of every sum is that of separate Jacobian and cost passes.
 // `cost_tol` is the relative cost drop at or below which an accepted step ends the fit (1e-12, the
 // reference's rule, by default).
-__device__ inline int warp_lm_fit(double* p, const double* v, const int* xy, int n, double cap, double amp_cap,
-                           int max_iter, int lane, double cost_tol = 1e-12) {
+template <typename T>
+__device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, double cap, double amp_cap,
+                                  int max_iter, int lane, double cost_tol = 1e-12) {
     double s[27];
     double cost = warp_normal_pass(p, v, xy, n, lane, s);
     if (!isfinite(cost)) return 0;

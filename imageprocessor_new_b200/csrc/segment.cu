@@ -343,8 +343,9 @@ struct Geo {
     __device__ __forceinline__ int canon(int y, int x) const {
         return conn == 8 ? ((((y >> 1) * Wb + (x >> 1)) << 2) | ((y & 1) << 1) | (x & 1)) : y * W + x;
     }
-    // Foreground bitmap: bit x & 31 of word y * words_per_row + x / 32. Only foreground pixels have
-    // an entry in the parents array; readers test the bitmap first.
+    // Foreground bitmap: bit x & 31 of word y * words_per_row + x / 32 (rows padded to 64 bits).
+    // Only local roots and foreground pixels on tile edges have an entry in the parents array;
+    // readers test the bitmap first.
     __device__ __forceinline__ int words_per_row() const { return (W + 63) / 64 * 2; }
     __device__ __forceinline__ bool fg(const unsigned* bits, int y, int x) const {
         return (bits[(long long)y * words_per_row() + (x >> 5)] >> (x & 31)) & 1u;
@@ -364,6 +365,16 @@ __device__ __forceinline__ int find_root_volatile(volatile int* p, int a) {
         p[a] = c;
         a = c;
     }
+}
+
+// Root of a without writing: safe to run while other threads overwrite entries with their roots.
+__device__ __forceinline__ int find_root_readonly(const volatile int* p, int a) {
+    int b = p[a];
+    while (b != a) {
+        a = b;
+        b = p[a];
+    }
+    return a;
 }
 
 // Lock-free union (link the larger root under the smaller with atomicMin; retry from the value
@@ -387,64 +398,145 @@ __device__ void unite(int* p, int a, int b, unsigned int* roots) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_local_ccl(const void* img, int dtype, Geo g,
-                                                   const double* thr_dev, double thr_fixed,
-                                                   int invert, int* parents, unsigned int* roots,
-                                                   unsigned int* fgbits) {
-    __shared__ int par[kTilePx];
-    __shared__ unsigned char fg[kTilePx];  // indexed by raster position inside the tile
-    const int tx0 = blockIdx.x * kTileW, ty0 = blockIdx.y * kTileH;
-    const double t = thr_dev ? *thr_dev : thr_fixed;
-    // Local index: canonical order restricted to the tile (keeps the global order of ids).
-    auto lidx = [&](int yl, int xl) {
-        return g.conn == 8 ? ((((yl >> 1) * (kTileW / 2) + (xl >> 1)) << 2) | ((yl & 1) << 1) | (xl & 1))
-                           : yl * kTileW + xl;
-    };
-    for (int k = threadIdx.x; k < kTilePx; k += blockDim.x) {
-        const int yl = k / kTileW, xl = k % kTileW, y = ty0 + yl, x = tx0 + xl;
-        bool f = false;
-        if (y < g.H && x < g.W) f = is_fg(load_px(img, dtype, (long long)y * g.W + x), t, invert);
-        fg[k] = f;
-        const int l = lidx(yl, xl);
-        par[l] = f ? l : -1;
-        // A warp holds 32 consecutive pixels of one tile row: one bitmap word.
-        const unsigned word = __ballot_sync(0xffffffffu, f);
-        if ((threadIdx.x & 31) == 0 && y < g.H) fgbits[(long long)y * g.words_per_row() + (x >> 5)] = word;
+// ---------------------------------------------------------------------- run-based tile union-find
+//
+// A 32 x 64 tile is 32 row masks (bit x of mask[r] = pixel (ty0 + r, tx0 + x) is foreground). The
+// union-find runs over the row runs: a run's node is its first pixel, which has the smallest
+// canonical id of the run (canonical order increases with x inside a row), so the root of every
+// local component is its smallest canonical id, as in a pixel-level union by minimum. Each of 32
+// threads takes one row and unites every run with the runs of the row above that touch it (their
+// columns overlap, widened by one for 8-connectivity). Both CCL kernels rebuild the same tile
+// forest from the bitmap; the result does not depend on the order of the unions.
+
+constexpr int kCclThreads = 128;
+
+__device__ __forceinline__ int tile_lidx(int conn, int yl, int xl) {
+    return conn == 8 ? ((((yl >> 1) * (kTileW / 2) + (xl >> 1)) << 2) | ((yl & 1) << 1) | (xl & 1))
+                     : yl * kTileW + xl;
+}
+
+// First column of the run of set bits of m that holds bit x.
+__device__ __forceinline__ int run_first(unsigned long long m, int x) {
+    const unsigned long long below = ~m & ((1ull << x) - 1ull);
+    return below ? 64 - __clzll((long long)below) : 0;
+}
+
+// Last column of the run of set bits of m that holds bit x.
+__device__ __forceinline__ int run_last(unsigned long long m, int x) {
+    const unsigned long long above = ~m & ~((1ull << x) - 1ull);
+    return above ? __ffsll((long long)above) - 2 : 63;
+}
+
+// Builds the tile forest in par[] (indexed by local canonical id; only run nodes are written) from
+// mask[0..31] and leaves every run node pointing at its root. Called by all threads of the block.
+__device__ void tile_forest(const unsigned long long* mask, int conn, int* par) {
+    const int r = threadIdx.x;
+    if (r < kTileH) {
+        const unsigned long long m = mask[r];
+        for (unsigned long long s = m & ~(m << 1); s; s &= s - 1) {
+            const int a = __ffsll((long long)s) - 1;
+            par[tile_lidx(conn, r, a)] = tile_lidx(conn, r, a);
+        }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < kTilePx; k += blockDim.x) {
-        if (!fg[k]) continue;
-        const int yl = k / kTileW, xl = k % kTileW, l = lidx(yl, xl);
-        if (xl > 0 && fg[k - 1]) unite(par, l, lidx(yl, xl - 1), nullptr);
-        if (yl > 0) {
-            if (fg[k - kTileW]) unite(par, l, lidx(yl - 1, xl), nullptr);
-            if (g.conn == 8) {
-                if (xl > 0 && fg[k - kTileW - 1]) unite(par, l, lidx(yl - 1, xl - 1), nullptr);
-                if (xl + 1 < kTileW && fg[k - kTileW + 1]) unite(par, l, lidx(yl - 1, xl + 1), nullptr);
+    if (r > 0 && r < kTileH) {
+        const unsigned long long m = mask[r], mp = mask[r - 1];
+        for (unsigned long long s = m & ~(m << 1); s && mp; s &= s - 1) {
+            const int a = __ffsll((long long)s) - 1, b = run_last(m, a);
+            const int lo = conn == 8 ? max(a - 1, 0) : a, hi = conn == 8 ? min(b + 1, 63) : b;
+            unsigned long long touch = mp & ((2ull << hi) - 1ull) & ~((1ull << lo) - 1ull);
+            const int me = tile_lidx(conn, r, a);
+            while (touch) {
+                const int c = __ffsll((long long)touch) - 1;
+                unite(par, me, tile_lidx(conn, r - 1, run_first(mp, c)), nullptr);
+                const int e = run_last(mp, c);
+                touch = e >= 63 ? 0ull : touch & ~((2ull << e) - 1ull);
             }
         }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < kTilePx; k += blockDim.x) {
-        const int yl = k / kTileW, xl = k % kTileW, y = ty0 + yl, x = tx0 + xl;
-        if (y >= g.H || x >= g.W) continue;
-        const int gid = g.canon(y, x);
-        if (!fg[k]) continue;
-        const int l = lidx(yl, xl);
-        const int r = find_root_volatile(par, l);
-        // Global id of the local root.
-        int ry, rx;
-        if (g.conn == 8) {
-            const int b = r >> 2;
-            ry = (b / (kTileW / 2)) * 2 + ((r >> 1) & 1);
-            rx = (b % (kTileW / 2)) * 2 + (r & 1);
-        } else {
-            ry = r / kTileW;
-            rx = r % kTileW;
+    // Point every run node at its root. The finds do not write (a path-halving find could put an
+    // intermediate node back over an entry its owner has already set to the root); each entry is
+    // written only by its own thread, with a value that is an ancestor of every value it had.
+    if (r < kTileH) {
+        const unsigned long long m = mask[r];
+        for (unsigned long long s = m & ~(m << 1); s; s &= s - 1) {
+            const int l = tile_lidx(conn, r, __ffsll((long long)s) - 1);
+            par[l] = find_root_readonly(par, l);
         }
-        const int rg = g.canon(ty0 + ry, tx0 + rx);
-        parents[gid] = rg;
-        if (r == l) atomicOr(&roots[gid >> 5], 1u << (gid & 31));
+    }
+    __syncthreads();
+}
+
+// Global canonical id of local canonical id l of the tile at (ty0, tx0).
+__device__ __forceinline__ int tile_gid(const Geo& g, int ty0, int tx0, int l) {
+    int ry, rx;
+    if (g.conn == 8) {
+        const int b = l >> 2;
+        ry = (b / (kTileW / 2)) * 2 + ((l >> 1) & 1);
+        rx = (b % (kTileW / 2)) * 2 + (l & 1);
+    } else {
+        ry = l / kTileW;
+        rx = l % kTileW;
+    }
+    return g.canon(ty0 + ry, tx0 + rx);
+}
+
+// Binarises one 32 x 64 tile into the foreground bitmap and builds its forest. Writes parents only
+// where the border merge reads them: each local root points at itself (and gets its root bit) and
+// each foreground pixel on the tile's four edges points at its local root.
+__global__ void __launch_bounds__(kCclThreads) k_local_ccl(const void* img, int dtype, Geo g,
+                                                           const double* thr_dev, double thr_fixed,
+                                                           int invert, int* parents, unsigned int* roots,
+                                                           unsigned int* fgbits) {
+    __shared__ int par[kTilePx];
+    __shared__ unsigned int words[kTileH * 2];
+    __shared__ unsigned long long mask[kTileH];
+    const int tx0 = blockIdx.x * kTileW, ty0 = blockIdx.y * kTileH;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double t = thr_dev ? *thr_dev : thr_fixed;
+    // Half-rows of 32 pixels: one warp-wide ballot each.
+    for (int hr = warp; hr < kTileH * 2; hr += kCclThreads / 32) {
+        const int y = ty0 + (hr >> 1), x = tx0 + (hr & 1) * 32 + lane;
+        bool f = false;
+        if (y < g.H && x < g.W) f = is_fg(load_px(img, dtype, (long long)y * g.W + x), t, invert);
+        const unsigned w = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) {
+            words[hr] = w;
+            if (y < g.H) fgbits[(long long)y * g.words_per_row() + (x >> 5)] = w;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < kTileH)
+        mask[threadIdx.x] = (unsigned long long)words[2 * threadIdx.x] |
+                            ((unsigned long long)words[2 * threadIdx.x + 1] << 32);
+    __syncthreads();
+    tile_forest(mask, g.conn, par);
+    if (threadIdx.x < kTileH) {
+        const int r = threadIdx.x, y = ty0 + r;
+        const unsigned long long m = mask[r];
+        for (unsigned long long s = m & ~(m << 1); s; s &= s - 1) {
+            const int l = tile_lidx(g.conn, r, __ffsll((long long)s) - 1);
+            if (par[l] == l) {
+                const int gid = tile_gid(g, ty0, tx0, l);
+                parents[gid] = gid;
+                atomicOr(&roots[gid >> 5], 1u << (gid & 31));
+            }
+        }
+        // Left and right edge pixels of this row.
+        if (m & 1ull) parents[g.canon(y, tx0)] = tile_gid(g, ty0, tx0, par[tile_lidx(g.conn, r, 0)]);
+        if (m >> 63)
+            parents[g.canon(y, tx0 + 63)] =
+                tile_gid(g, ty0, tx0, par[tile_lidx(g.conn, r, run_first(m, 63))]);
+    }
+    // Top and bottom rows: one warp each, lanes over the 64 columns.
+    if (warp < 2) {
+        const int r = warp == 0 ? 0 : kTileH - 1;
+        const unsigned long long m = mask[r];
+        for (int x = lane; x < kTileW; x += 32)
+            if ((m >> x) & 1ull)
+                parents[g.canon(ty0 + r, tx0 + x)] =
+                    tile_gid(g, ty0, tx0, par[tile_lidx(g.conn, r, run_first(m, x))]);
     }
 }
 
@@ -572,71 +664,95 @@ __global__ void k_stats_init(int* stats, unsigned long long* sums, int k1) {
     }
 }
 
-// Final labels and stats. Each warp covers 32 consecutive pixels of one row, so equal labels form
-// runs of lanes; a run's head lane adds the run's bbox, area and coordinate sums with one set of
-// atomics. Background runs are reduced per block first.
-__global__ void __launch_bounds__(256) k_finish(Geo g, const int* parents, const unsigned int* roots,
-                                                const int* prefix, const unsigned int* fgbits, int* labels,
-                                                int* stats, unsigned long long* sums) {
+// Final labels and stats of one 32 x 64 tile. The tile forest is rebuilt from the bitmap; each
+// local root follows the merged parents to its global root once, whose label is the rank of that
+// root among the roots (popcount prefix) + 1; every pixel then takes the label of its run's root.
+// Warps write 32 consecutive pixels of a row, so equal labels form runs of lanes; a run's head lane
+// adds the run's bbox, area and coordinate sums with one set of atomics. Background runs are
+// reduced per block first.
+__global__ void __launch_bounds__(kCclThreads) k_finish(Geo g, const int* parents, const unsigned int* roots,
+                                                        const int* prefix, const unsigned int* fgbits,
+                                                        int* labels, int* stats, unsigned long long* sums, int k1) {
+    __shared__ int par[kTilePx];
+    __shared__ int lab_of[kTilePx];
+    __shared__ unsigned long long mask[kTileH];
     __shared__ long long s_bg[7];
+    const int tx0 = blockIdx.x * kTileW, ty0 = blockIdx.y * kTileH;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = blockIdx.x * 32 + lane;
-    const int y = blockIdx.y * 8 + warp;
-    const bool inside = x < g.W && y < g.H;
-    int lab = -1;  // -1 outside the image
-    if (inside) {
-        if (!g.fg(fgbits, y, x)) {
-            lab = 0;
-        } else {
-            int p = parents[g.canon(y, x)];
+    if (threadIdx.x < kTileH) {
+        const int y = ty0 + threadIdx.x;
+        unsigned long long m = 0;
+        if (y < g.H) {
+            const unsigned* row = fgbits + (long long)y * g.words_per_row() + (tx0 >> 5);
+            m = (unsigned long long)row[0] | ((unsigned long long)row[1] << 32);
+        }
+        mask[threadIdx.x] = m;
+    }
+    if (threadIdx.x == 0) {
+        s_bg[0] = 0x7fffffff; s_bg[1] = 0x7fffffff; s_bg[2] = -1; s_bg[3] = -1; s_bg[4] = 0; s_bg[5] = 0; s_bg[6] = 0;
+    }
+    __syncthreads();
+    tile_forest(mask, g.conn, par);
+    if (threadIdx.x < kTileH) {
+        const unsigned long long m = mask[threadIdx.x];
+        for (unsigned long long s = m & ~(m << 1); s; s &= s - 1) {
+            const int l = tile_lidx(g.conn, threadIdx.x, __ffsll((long long)s) - 1);
+            if (par[l] != l) continue;
+            int p = tile_gid(g, ty0, tx0, l);
             int q = parents[p];
             while (q != p) {
                 p = q;
                 q = parents[p];
             }
-            lab = prefix[p >> 5] + __popc(roots[p >> 5] & ((1u << (p & 31)) - 1u)) + 1;
+            lab_of[l] = prefix[p >> 5] + __popc(roots[p >> 5] & ((1u << (p & 31)) - 1u)) + 1;
         }
-        labels[(long long)y * g.W + x] = lab;
-    }
-    const int prev = __shfl_up_sync(0xffffffffu, lab, 1);
-    const bool head = lab >= 0 && (lane == 0 || prev != lab);
-    const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const unsigned valid = __ballot_sync(0xffffffffu, lab >= 0);
-    // Run end: lane before the next head (or the last valid lane).
-    const unsigned later = heads & ~((2u << lane) - 1u);
-    int next = later ? __ffs(later) - 1 : 32;
-    const int last_valid = 31 - __clz(valid | 1u);
-    int tail = min(next - 1, last_valid);
-    if (head && lab > 0) {
-        const int x0 = x, x1 = x + (tail - lane);
-        const long long len = x1 - x0 + 1;
-        const long long sx = (long long)(x0 + x1) * len / 2;
-        int* st = stats + (long long)lab * 5;
-        atomicMin(&st[0], x0);
-        atomicMin(&st[1], y);
-        atomicMax(&st[2], x1);
-        atomicMax(&st[3], y);
-        atomicAdd(&st[4], (int)len);
-        atomicAdd(&sums[2LL * lab], (unsigned long long)sx);
-        atomicAdd(&sums[2LL * lab + 1], (unsigned long long)((long long)y * len));
-    }
-    // Background (label 0): one ballot per warp row, block totals in shared memory.
-    const unsigned bgm = __ballot_sync(0xffffffffu, lab == 0);
-    const int bx = lab == 0 ? x : 0;
-    const int bsum = warp_sum_i(bx);
-    if (threadIdx.x == 0) {
-        s_bg[0] = 0x7fffffff; s_bg[1] = 0x7fffffff; s_bg[2] = -1; s_bg[3] = -1; s_bg[4] = 0; s_bg[5] = 0; s_bg[6] = 0;
     }
     __syncthreads();
-    if (lane == 0 && bgm) {
-        const int x0 = blockIdx.x * 32;
-        atomicMin(&s_bg[0], (long long)(x0 + __ffs(bgm) - 1));
-        atomicMin(&s_bg[1], (long long)y);
-        atomicMax(&s_bg[2], (long long)(x0 + 31 - __clz(bgm)));
-        atomicMax(&s_bg[3], (long long)y);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[4]), (unsigned long long)__popc(bgm));
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[5]), (unsigned long long)bsum);
-        atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[6]), (unsigned long long)((long long)y * __popc(bgm)));
+    for (int hr = warp; hr < kTileH * 2; hr += kCclThreads / 32) {
+        const int r = hr >> 1, xl = (hr & 1) * 32 + lane;
+        const int y = ty0 + r, x = tx0 + xl;
+        const unsigned long long m = mask[r];
+        int lab = -1;  // -1 outside the image
+        if (x < g.W && y < g.H) {
+            lab = ((m >> xl) & 1ull) ? lab_of[par[tile_lidx(g.conn, r, run_first(m, xl))]] : 0;
+            labels[(long long)y * g.W + x] = lab;
+        }
+        const int prev = __shfl_up_sync(0xffffffffu, lab, 1);
+        const bool head = lab >= 0 && (lane == 0 || prev != lab);
+        const unsigned heads = __ballot_sync(0xffffffffu, head);
+        const unsigned valid = __ballot_sync(0xffffffffu, lab >= 0);
+        // Run end: lane before the next head (or the last valid lane).
+        const unsigned later = heads & ~((2u << lane) - 1u);
+        const int next = later ? __ffs(later) - 1 : 32;
+        const int last_valid = 31 - __clz(valid | 1u);
+        const int tail = min(next - 1, last_valid);
+        if (head && lab > 0 && lab < k1) {  // labels beyond the component count cannot occur
+            const int x0 = x, x1 = x + (tail - lane);
+            const long long len = x1 - x0 + 1;
+            const long long sx = (long long)(x0 + x1) * len / 2;
+            int* st = stats + (long long)lab * 5;
+            atomicMin(&st[0], x0);
+            atomicMin(&st[1], y);
+            atomicMax(&st[2], x1);
+            atomicMax(&st[3], y);
+            atomicAdd(&st[4], (int)len);
+            atomicAdd(&sums[2LL * lab], (unsigned long long)sx);
+            atomicAdd(&sums[2LL * lab + 1], (unsigned long long)((long long)y * len));
+        }
+        // Background (label 0): one ballot per warp row, block totals in shared memory.
+        const unsigned bgm = __ballot_sync(0xffffffffu, lab == 0);
+        const int bsum = warp_sum_i(lab == 0 ? x : 0);
+        if (lane == 0 && bgm) {
+            const int xs = tx0 + (hr & 1) * 32;
+            atomicMin(&s_bg[0], (long long)(xs + __ffs(bgm) - 1));
+            atomicMin(&s_bg[1], (long long)y);
+            atomicMax(&s_bg[2], (long long)(xs + 31 - __clz(bgm)));
+            atomicMax(&s_bg[3], (long long)y);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[4]), (unsigned long long)__popc(bgm));
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[5]), (unsigned long long)bsum);
+            atomicAdd(reinterpret_cast<unsigned long long*>(&s_bg[6]),
+                      (unsigned long long)((long long)y * __popc(bgm)));
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_bg[4] > 0) {
@@ -1032,10 +1148,8 @@ int spx_ccl_label(const void* img, int dtype, int height, int width, const doubl
     CclLayout L = ccl_layout(workspace, height, width, nullptr);
     Geo g{height, width, (width + 1) / 2, connectivity};
     SPX_CUDA(cudaMemsetAsync(L.roots, 0, L.words * sizeof(unsigned int), s));
-    if (connectivity == 8 && ((height & 1) || (width & 1)))  // padding entries of odd sizes
-        SPX_CUDA(cudaMemsetAsync(L.parents, 0xff, L.canon_n * sizeof(int), s));
     const int tiles_x = (width + kTileW - 1) / kTileW, tiles_y = (height + kTileH - 1) / kTileH;
-    k_local_ccl<<<dim3(tiles_x, tiles_y), 256, 0, s>>>(img, dtype, g, threshold_dev, fixed_threshold,
+    k_local_ccl<<<dim3(tiles_x, tiles_y), kCclThreads, 0, s>>>(img, dtype, g, threshold_dev, fixed_threshold,
                                                        invert, L.parents, L.roots, L.fgbits);
     if (int e = check_launch("k_local_ccl")) return e;
     const long long border = (long long)tiles_x * tiles_y * (kTileW + 2 * kTileH);
@@ -1064,8 +1178,8 @@ int spx_ccl_finish(int* labels, int height, int width, int connectivity, int num
     unsigned long long* sums = reinterpret_cast<unsigned long long*>(centroids);
     k_stats_init<<<grid_for(k1, 256), 256, 0, s>>>(stats, sums, k1);
     if (int e = check_launch("k_stats_init")) return e;
-    k_finish<<<dim3((width + 31) / 32, (height + 7) / 8), 256, 0, s>>>(g, L.parents, L.roots, L.prefix,
-                                                                       L.fgbits, labels, stats, sums);
+    k_finish<<<dim3((width + kTileW - 1) / kTileW, (height + kTileH - 1) / kTileH), kCclThreads, 0, s>>>(
+        g, L.parents, L.roots, L.prefix, L.fgbits, labels, stats, sums, k1);
     if (int e = check_launch("k_finish")) return e;
     k_stats_final<<<grid_for(k1, 256), 256, 0, s>>>(stats, sums, centroids, k1);
     return check_launch("k_stats_final");

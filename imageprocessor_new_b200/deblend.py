@@ -109,6 +109,23 @@ def sigma_major(params: np.ndarray) -> np.ndarray:
     return 1 / np.sqrt(np.maximum(smaller, 1e-300))
 
 
+FIT_PRECISIONS = ("fp64", "fp32")
+# Relative cost drop that ends an FP32 fit. FP32 residuals resolve cost changes down to a few 1e-7
+# of the cost (a tighter rule only adds rejected trials); 1e-7 keeps the fitted sigmas within about
+# 1e-3 px of the FP64 fit on holes up to 20 px.
+FP32_COST_TOL = 1e-7
+
+
+def fit_options(precision: str = "fp64", cost_tol: float | None = None) -> _lib.FitOptions:
+    """spx_fit_options for an LM arithmetic: "fp64" (the reference's, stop rule 1e-12) or "fp32"
+    (FP32 per-pixel arithmetic and lane sums, FP64 totals, solve and acceptance)."""
+    if precision not in FIT_PRECISIONS:
+        raise ValueError(f"fit_precision must be one of {FIT_PRECISIONS}, got {precision!r}")
+    if cost_tol is None:
+        cost_tol = 1e-12 if precision == "fp64" else FP32_COST_TOL
+    return _lib.FitOptions(_lib.FIT_F32 if precision == "fp32" else _lib.FIT_F64, float(cost_tol))
+
+
 def tile_centers(tile: int, shape):
     h, w = shape
     yc = np.array([(j * tile + min((j + 1) * tile, h) - 1) / 2 for j in range(-(-h // tile))])
@@ -241,8 +258,10 @@ class Deblender:
 
     def __init__(self, image_d: torch.Tensor, sign: float, cells: Cells, *, exclude_d=None, tile=None,
                  background_level=None, free_fraction=0.05, free_distance_fwhm=1.25, relaxation=0.6,
-                 tolerance=1e-3, max_iter=30):
+                 tolerance=1e-3, max_iter=30, fit_precision="fp64", fit_cost_tol=None):
         self.img = image_d
+        self.fit_precision = fit_precision
+        self.fit_options = fit_options(fit_precision, fit_cost_tol)
         self.dtype = dev.dtype_code(image_d)
         self.sign = float(sign)
         self.shape = tuple(image_d.shape)
@@ -356,11 +375,12 @@ class Deblender:
         bg0 = dev.empty((self.n,), torch.float64) if extras else None
         fell = dev.empty((self.n,), torch.uint8) if extras else None
         has = self.background_level is not None
+        warm_cost_tol = max(float(warm_cost_tol), self.fit_options.cost_tol)
         _lib.call("spx_deblend_initial_warm", self.img.data_ptr(), self.dtype, self.sign, h, w, c.voronoi.data_ptr(),
                   c.boxes.data_ptr(), c.caps.data_ptr(), c.seeds_d.data_ptr(), self.n, c.hm, c.wm, c.max_px,
                   float(self.background_level) if has else 0.0, int(has), int(max_iter), _ptr(warm_params),
                   _ptr(warm_ok), float(warm_cost_tol), params.data_ptr(), status.data_ptr(), iters.data_ptr(),
-                  _ptr(bg0), _ptr(fell),
+                  _ptr(bg0), _ptr(fell), self.fit_options,
                   self.fit_ws.data_ptr(), self.fit_ws.numel(), dev.stream_ptr())
         if extras:
             return params, status, iters, bg0, fell
@@ -377,7 +397,7 @@ class Deblender:
         _lib.call("spx_deblend_iteration", self.img.data_ptr(), self.dtype, self.sign, h, w, c.voronoi.data_ptr(),
                   c.boxes.data_ptr(), c.caps.data_ptr(), self.n, c.hm, c.wm, c.max_px, st, model.data_ptr(),
                   max(self.radius_cap, 2), params_d.data_ptr(), float(self.relaxation), self.max_iter,
-                  out.data_ptr(), status.data_ptr(), maxstep.data_ptr(), iters.data_ptr(),
+                  out.data_ptr(), status.data_ptr(), maxstep.data_ptr(), iters.data_ptr(), self.fit_options,
                   self.fit_ws.data_ptr(), self.fit_ws.numel(), dev.stream_ptr())
         return out, status, maxstep, iters
 
@@ -464,5 +484,5 @@ class Deblender:
         _lib.call("spx_deblend_iteration", self.img.data_ptr(), self.dtype, self.sign, h, w, c.voronoi.data_ptr(),
                   c.boxes.data_ptr(), c.caps.data_ptr(), self.n, c.hm, c.wm, c.max_px, st, zero_model.data_ptr(),
                   max(self.radius_cap, 2), params_d.data_ptr(), 0.0, 1, out.data_ptr(), status.data_ptr(),
-                  maxstep.data_ptr(), None, self.fit_ws.data_ptr(), self.fit_ws.numel(), dev.stream_ptr())
+                  maxstep.data_ptr(), None, None, self.fit_ws.data_ptr(), self.fit_ws.numel(), dev.stream_ptr())
         return status

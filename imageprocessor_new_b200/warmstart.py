@@ -331,9 +331,13 @@ def page_cells(page_d: torch.Tensor, *, area_min: int = 10, area_max: int = 2000
 
 
 def initial_fits(page_d: torch.Tensor, cells, *, sign: float = 1.0, max_iter: int = 30, warm=None,
-                 cost_tol: float = 1e-12):
-    """The initial LM fits of the cells (plain, or warm-started with (params, ok)): params, status,
-    iterations, cell-border backgrounds and fallback flags (device)."""
+                 cost_tol: float = 1e-12, precision: str = "fp64"):
+    """The initial LM fits of the cells (plain, or warm-started with (params, ok)) in the given LM
+    arithmetic: params, status, iterations, cell-border backgrounds and fallback flags (device)."""
+    from .deblend import fit_options
+
+    opts = fit_options(precision)
+    cost_tol = max(float(cost_tol), opts.cost_tol)
     n = cells.n
     h, w = page_d.shape
     ws = dev.workspace(_lib.size("spx_fit_workspace_bytes", cells.max_px))
@@ -348,7 +352,7 @@ def initial_fits(page_d: torch.Tensor, cells, *, sign: float = 1.0, max_iter: in
               cells.hm, cells.wm, cells.max_px, 0.0, 0, int(max_iter), None if wp is None else wp.data_ptr(),
               None if wo is None else wo.data_ptr(), float(cost_tol), params.data_ptr(), status.data_ptr(),
               iters.data_ptr(),
-              bg0.data_ptr(), fell.data_ptr(), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+              bg0.data_ptr(), fell.data_ptr(), opts, ws.data_ptr(), ws.numel(), dev.stream_ptr())
     return params[:n], status[:n], iters[:n], bg0[:n], fell[:n]
 
 
@@ -415,10 +419,10 @@ def train(net: WarmStartNet, x: torch.Tensor, t: torch.Tensor, *, epochs: int = 
 # -------------------------------------------------------------------------------- evaluation
 
 def compare_on_page(net: WarmStartNet, page_d: torch.Tensor, *, max_iter: int = 30, repeats: int = 3,
-                    cells=None) -> dict:
-    """Plain against warm-started initial fits of one page's cells: LM iterations, fallback share,
-    centre deviation of the warm fits from the plain ones ("ok" in both), and the device time of
-    the LM stage (the warm time includes the patches and the MLP)."""
+                    cells=None, precision: str = "fp64") -> dict:
+    """Plain FP64 against warm-started initial fits (in `precision`) of one page's cells: LM
+    iterations, fallback share, centre deviation of the warm fits from the plain ones ("ok" in
+    both), and the device time of the LM stage (the warm time includes the patches and the MLP)."""
     cells = page_cells(page_d) if cells is None else cells
     n = cells.n
 
@@ -427,7 +431,8 @@ def compare_on_page(net: WarmStartNet, page_d: torch.Tensor, *, max_iter: int = 
 
     def warm():
         p0, ok = predict_init(net, page_d, 1.0, cells.seeds_d, cells.boxes, n)
-        return initial_fits(page_d, cells, max_iter=max_iter, warm=(p0, ok), cost_tol=net.cost_tol)
+        return initial_fits(page_d, cells, max_iter=max_iter, warm=(p0, ok), cost_tol=net.cost_tol,
+                            precision=precision)
 
     for fn in (plain, warm):
         fn()

@@ -214,6 +214,19 @@ typedef struct spx_bgmap {
 int spx_cells_setup(const double* rows, int n, int pad, int height, int width, const int* voronoi,
                     int* boxes, int* counts, double* caps, void* stream);
 
+/* Arithmetic of the LM fits (no reference counterpart; a null options pointer means FP64 with the
+ * reference's rule). SPX_FIT_F64: every sum and the solve in FP64, as subpx/_cpu/deblend.py:174-254.
+ * SPX_FIT_F32: the staged cell values, residuals, model, Jacobian and per-lane sums in FP32 (J^T J by
+ * FMA, J^T r and the cost Kahan-compensated), lane totals added in FP64, and the damped solve, the
+ * clipping, the step acceptance and the stop rule in FP64. cost_tol: relative cost drop at or below
+ * which an accepted step ends a plain-start fit (1e-12 is the reference's rule; FP32 residuals
+ * resolve cost changes down to a few 1e-7 of the cost). */
+enum { SPX_FIT_F64 = 0, SPX_FIT_F32 = 1 };
+typedef struct spx_fit_options {
+    int precision;
+    double cost_tol;
+} spx_fit_options;
+
 size_t spx_fit_workspace_bytes(int max_cell_pixels);
 /* Initial fits: 10th-percentile cell-border background (or background_level when has_level),
  * initial_params, LM (max_iter), fit_status. `sign` is -1 for inverted images. */
@@ -227,23 +240,26 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
  * an accepted step lowers the cost by at most warm_cost_tol relative (1e-12 is the plain rule),
  * max |step| < 1e-7 or the damping exceeds 1e12; that fit is kept when it stops within max_iter and ends "ok", otherwise
  * the plain start runs as well (fallback_out[j] = 1; iterations counts both). background_out[j]
- * receives the cell-border background the fit subtracted. No reference counterpart (learned warm
- * start). */
+ * receives the cell-border background the fit subtracted. options (null: FP64, cost_tol 1e-12)
+ * sets the fits' arithmetic and the plain-start fits' stop rule. No reference counterpart (learned
+ * warm start). */
 int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                              const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
                              int max_cell_pixels, double background_level, int has_level, int max_iter,
                              const double* init_params, const uint8_t* init_ok, double warm_cost_tol,
                              double* params, uint8_t* status, int* iterations, double* background_out,
-                             uint8_t* fallback_out, void* workspace, size_t workspace_bytes, void* stream);
+                             uint8_t* fallback_out, const spx_fit_options* options, void* workspace,
+                             size_t workspace_bytes, void* stream);
 /* One outer iteration: clean every cell against `model` and `background`, LM from `params`,
  * params_out = params + relaxation * (fitted - params), status of params_out, and maxstep =
- * max |step[1:]| (NaN unless the cell is ok with a finite fit). */
+ * max |step[1:]| (NaN unless the cell is ok with a finite fit). The cleaning is FP64 in both
+ * arithmetics; options as for spx_deblend_initial_warm. */
 int spx_deblend_iteration(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                           const int* boxes, const double* caps, int n, int hm, int wm, int max_cell_pixels,
                           const spx_bgmap* background, const double* model, int radius_cap,
                           const double* params, double relaxation, int max_iter, double* params_out,
-                          uint8_t* status_out, double* maxstep, int* iterations, void* workspace,
-                          size_t workspace_bytes, void* stream);
+                          uint8_t* status_out, double* maxstep, int* iterations, const spx_fit_options* options,
+                          void* workspace, size_t workspace_bytes, void* stream);
 
 size_t spx_render_workspace_bytes(int n, int height, int width);
 /* Sum of every cell's truncated Gaussian (radius clip(ceil(4 sigma_major), 2, radius_cap)) into

@@ -37,3 +37,23 @@ def test_build_targets_sm100a_only():
     from imageprocessor_new_b200 import build
 
     assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_fit_options_are_checked_before_any_device_work():
+    """An unknown LM arithmetic or a cost tolerance outside (0, 1) is an argument error, reported
+    before the entry point touches the device (so it runs without a GPU)."""
+    import pytest
+
+    from imageprocessor_new_b200 import _lib, deblend
+
+    with pytest.raises(ValueError, match="fit_precision"):
+        deblend.fit_options("fp16")
+    assert deblend.fit_options("fp64").cost_tol == 1e-12
+    assert deblend.fit_options("fp32").precision == _lib.FIT_F32
+    lib = _lib.load_library()
+    bg = _lib.BgMap()
+    for opts in (_lib.FitOptions(7, 1e-6), _lib.FitOptions(_lib.FIT_F32, 0.0), _lib.FitOptions(_lib.FIT_F64, 1.5)):
+        rc = lib.spx_deblend_iteration(None, 1, 1.0, 8, 8, None, None, None, 0, 4, 4, 16, bg, None, 2, None, 0.6, 30,
+                                       None, None, None, None, opts, None, 0, None)
+        assert rc != 0
+        assert b"fit" in lib.spx_last_error()
