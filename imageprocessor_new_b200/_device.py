@@ -36,6 +36,14 @@ def upload(a: np.ndarray) -> torch.Tensor:
     return torch.from_numpy(a).to("cuda", non_blocking=False)
 
 
+def start_download(t: torch.Tensor) -> np.ndarray:
+    """Queues a copy of a device tensor into pinned host memory on the current stream and returns
+    the host array; its contents are valid once the stream has been synchronised."""
+    host = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+    host.copy_(t, non_blocking=True)
+    return host.numpy()
+
+
 def empty(shape, dtype) -> torch.Tensor:
     return torch.empty(shape, dtype=dtype, device="cuda")
 

@@ -347,24 +347,30 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
     else:
         img_d = dev.upload(img if img.dtype in _lib.DTYPES else img.astype(np.float64))
     comp, rescaled = _segment(img_d, threshold, invert)
-    stats = comp.stats.cpu().numpy()
-    cents = comp.centroids.cpu().numpy()
     k = comp.count
     components_before_filter = k
-    x, y, w, h, area = stats[1:k + 1].astype(np.int64).T
-    keep = (area >= area_min) & (area <= area_max)
-    oversized_flags = np.zeros(k + 1, np.uint8)
-    oversized_flags[1:][area > area_max] = 1
-    inside = ~((x <= 0) | (y <= 0) | (x + w >= width) | (y + h >= height))
-    rows = np.column_stack((x, y, w, h, cents[1:k + 1])).astype(np.float64)[keep]
-    component_ids = (np.flatnonzero(keep) + 1).astype(np.int32)
-    interior = inside[keep]
+    # Area filter, cell rows, border flags and oversized labels on the device (subpx/cd.py:485-500).
+    rows_d = dev.empty((max(k, 1), 6), torch.float64)
+    ids_d = dev.empty((max(k, 1),), torch.int32)
+    inside_d = dev.empty((max(k, 1),), torch.uint8)
+    oversized_flags_d = dev.empty((k + 1,), torch.uint8)
+    counts_d = dev.empty((2,), torch.int32)
+    ws = dev.workspace(_lib.size("spx_select_workspace_bytes", k))
+    _lib.call("spx_component_rows", comp.stats.data_ptr(), comp.centroids.data_ptr(), k, int(area_min), int(area_max),
+              width, height, rows_d.data_ptr(), ids_d.data_ptr(), inside_d.data_ptr(), oversized_flags_d.data_ptr(),
+              counts_d.data_ptr(), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+    n_keep, n_oversized = (int(v) for v in counts_d.cpu().numpy())
+    rows_d = rows_d[:n_keep]
+    # Host copies land while the Voronoi cells are built (build_cells syncs before reading them).
+    rows = dev.start_download(rows_d)
+    component_ids = dev.start_download(ids_d[:n_keep])
+    interior_u8 = dev.start_download(inside_d[:n_keep])
     labels_d = comp.labels
     tmp8 = dev.empty((height, width), torch.uint8)
     oversized_d = None
-    if oversized_flags.any():
+    if n_oversized:
         oversized_d = dev.empty((height, width), torch.uint8)
-        _lib.call("spx_label_mask", labels_d.data_ptr(), dev.upload(oversized_flags).data_ptr(), height, width, 0,
+        _lib.call("spx_label_mask", labels_d.data_ptr(), oversized_flags_d.data_ptr(), height, width, 0,
                   oversized_d.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
 
     def exclude_for(ids):
@@ -378,7 +384,10 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         return out
 
     shape = tuple(img_d.shape)
-    cells = build_cells(rows, shape, pad)
+    cells = build_cells(rows, shape, pad, rows_d=rows_d)
+    rows = cells.rows
+    component_ids = np.array(component_ids)
+    interior = interior_u8.astype(bool)
     seconds["segmentation"] = time.perf_counter() - started
     meta = {
         "background": "model", "seeds": "threshold", "threshold": threshold, "invert": bool(invert),

@@ -54,6 +54,34 @@ __global__ void k_select_rows(const int* stats, int k, int area_min, int area_ma
     }
 }
 
+// Cells of measure_cds: rows [x, y, w, h, cx, cy] (double) of the kept components in label order,
+// their labels, whether the bbox stays off the image border, and per label whether it is too large.
+__global__ void k_component_rows(const int* stats, const double* centroids, int k, int area_min, int area_max,
+                                 int width, int height, const int* offsets, double* rows, int* ids,
+                                 uint8_t* interior, uint8_t* oversized, int* n_oversized) {
+    int over = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+        const int* st = stats + (long long)(i + 1) * 5;
+        const int area = st[4];
+        oversized[i + 1] = area > area_max;
+        over += area > area_max;
+        if (!(area >= area_min && area <= area_max)) continue;
+        const int o = offsets[i];
+        double* r = rows + (long long)o * 6;
+        r[0] = st[0];
+        r[1] = st[1];
+        r[2] = st[2];
+        r[3] = st[3];
+        r[4] = centroids[2LL * (i + 1)];
+        r[5] = centroids[2LL * (i + 1) + 1];
+        ids[o] = i + 1;
+        interior[o] = !(st[0] <= 0 || st[1] <= 0 || st[0] + st[2] >= width || st[1] + st[3] >= height);
+    }
+    over = warp_sum_i(over);
+    if ((threadIdx.x & 31) == 0 && over) atomicAdd(n_oversized, over);
+    if (blockIdx.x == 0 && threadIdx.x == 0) oversized[0] = 0;
+}
+
 // ------------------------------------------------------------------------------------- refiners
 
 struct Roi {
@@ -651,6 +679,32 @@ int spx_select_components(const int* stats, int num_components, int area_min, in
     k_select_rows<<<grid_for(num_components, 256), 256, 0, s>>>(
         stats, num_components, area_min, area_max, refine, small_feature_max, flags, rows_out, methods_out);
     return check_launch("k_select_rows");
+}
+
+int spx_component_rows(const int* stats, const double* centroids, int num_components, int area_min, int area_max,
+                       int width, int height, double* rows_out, int* ids_out, uint8_t* interior_out,
+                       uint8_t* oversized_out, int* counts_out, void* workspace, size_t workspace_bytes,
+                       void* stream) {
+    SPX_REQUIRE(num_components >= 0 && width > 0 && height > 0, "bad arguments");
+    SPX_REQUIRE(counts_out && oversized_out && workspace, "null pointer");
+    SPX_REQUIRE(workspace_bytes >= spx_select_workspace_bytes(num_components), "workspace too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    SPX_CUDA(cudaMemsetAsync(counts_out, 0, 2 * sizeof(int), s));
+    if (num_components == 0) {
+        SPX_CUDA(cudaMemsetAsync(oversized_out, 0, 1, s));
+        return SPX_OK;
+    }
+    SPX_REQUIRE(stats && centroids && rows_out && ids_out && interior_out, "null pointer");
+    Arena a(workspace);
+    int* flags = a.take<int>(num_components);
+    int* scratch = a.take<int>(scan_scratch_ints(num_components));
+    k_select_flags<<<grid_for(num_components, 256), 256, 0, s>>>(stats, num_components, area_min, area_max, flags);
+    if (int e = check_launch("k_select_flags")) return e;
+    if (int e = exclusive_scan(flags, num_components, flags, counts_out, scratch, s)) return e;
+    k_component_rows<<<grid_for(num_components, 256), 256, 0, s>>>(stats, centroids, num_components, area_min,
+                                                                    area_max, width, height, flags, rows_out, ids_out,
+                                                                    interior_out, oversized_out, counts_out + 1);
+    return check_launch("k_component_rows");
 }
 
 int spx_refine_centers(const void* img, int dtype, int height, int width, const int* labels,

@@ -53,21 +53,28 @@ class Cells:
         return len(self.rows)
 
 
-def build_cells(rows, shape, pad: int) -> Cells:
-    """Voronoi labels of the row centres and the padded boxes (subpx/_gpu/cells.py:11-38)."""
+def build_cells(rows, shape, pad: int, rows_d: torch.Tensor | None = None) -> Cells:
+    """Voronoi labels of the row centres and the padded boxes (subpx/_gpu/cells.py:11-38).
+
+    With ``rows_d`` (the rows already on the device) ``rows`` may be a host array whose copy from
+    the device is still in flight on the current stream: it is read only after the stream syncs."""
     h, w = shape
-    rows = np.asarray(rows, dtype=np.float64).reshape(-1, 6)
-    n = len(rows)
-    seeds = np.ascontiguousarray(rows[:, 4:6])
-    seeds_d = dev.upload(seeds) if n else dev.empty((0, 2), torch.float64)
+    if rows_d is None:
+        rows = np.asarray(rows, dtype=np.float64).reshape(-1, 6)
+        n = len(rows)
+        rows_d = dev.upload(rows) if n else None
+    else:
+        n = rows_d.shape[0]
+    seeds_d = rows_d[:, 4:6].contiguous() if n else dev.empty((0, 2), torch.float64)
     vor = labels_device(seeds_d if n else None, shape)
     boxes = dev.empty((max(n, 1), 4), torch.int32)
     counts = dev.empty((max(n, 1),), torch.int32)
     caps = dev.empty((max(n, 1),), torch.float64)
-    rows_d = dev.upload(rows) if n else None
-    _lib.call("spx_cells_setup", _ptr(rows_d), n, int(pad), h, w, vor.data_ptr(), boxes.data_ptr(),
+    _lib.call("spx_cells_setup", _ptr(rows_d) if n else None, n, int(pad), h, w, vor.data_ptr(), boxes.data_ptr(),
               counts.data_ptr(), caps.data_ptr(), dev.stream_ptr())
     host = boxes[:n].cpu().numpy()
+    rows = np.asarray(rows, dtype=np.float64).reshape(-1, 6)
+    seeds = np.ascontiguousarray(rows[:, 4:6])
     hm = int(host[:, 3].max()) if n else 0
     wm = int(host[:, 2].max()) if n else 0
     max_px = int(counts[:n].max().item()) if n else 1

@@ -152,6 +152,16 @@ int spx_select_components(const int* stats, int num_components, int area_min, in
                           uint8_t* methods_out, int* kept, void* workspace,
                           size_t workspace_bytes, void* stream);
 
+/* measure_cds cells (subpx/cd.py:485-500): the components 1..K with area_min <= area <= area_max in
+ * label order as rows_out [x, y, w, h, cx, cy] (double), ids_out their labels, interior_out whether
+ * the bbox keeps off the image border (x > 0, y > 0, x + w < width, y + h < height); oversized_out
+ * (K + 1 bytes) flags labels with area > area_max. counts_out (device, 2 ints) = [kept, oversized].
+ * Workspace: spx_select_workspace_bytes(K). */
+int spx_component_rows(const int* stats, const double* centroids, int num_components, int area_min, int area_max,
+                       int width, int height, double* rows_out, int* ids_out, uint8_t* interior_out,
+                       uint8_t* oversized_out, int* counts_out, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
 /* One centre per row: ROI = bbox +- pad clipped to the image, mask = labels == label.
  * centers_out (n x 2 double) gets global [x, y] or NaN where the refiner fails. */
 int spx_refine_centers(const void* img, int dtype, int height, int width, const int* labels,
