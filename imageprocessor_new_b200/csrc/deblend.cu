@@ -20,6 +20,8 @@ namespace spx {
 namespace {
 
 constexpr int kFitWarpsMax = 8;  // largest tuning().fit_warps (sizes the global staging fallback)
+// Static shared memory of the fit kernels: two 27-double LM sum slots per warp.
+constexpr int kLmSlotBytes = kFitWarpsMax * 54 * (int)sizeof(double);
 
 // Background map: bg(y, x) = (1 - t[y]) rows[j1[y]-1][x] + t[y] rows[j1[y]][x] (ny > 1),
 // rows[0][x] (ny == 1), or a constant.
@@ -155,6 +157,7 @@ template <typename T>
 __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
                               double* params, uint8_t* status, int* iters, WarmStart warm) {
     extern __shared__ unsigned char smem[];
+    __shared__ double lm_slots[kFitWarpsMax][54];  // kept / trial normal-equation sums per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double* vbuf;  // the warp's staging buffer: border values (double), then the cell's values (T)
     int* xy;
@@ -250,7 +253,7 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
                 finite = finite && isfinite(q[i]);
             }
             if (finite && q[0] > 0.0) {
-                it = warp_lm_fit(q, v, xy, n, cap, amp_cap, a.max_iter, lane, warm.cost_tol);
+                it = warp_lm_fit(q, v, xy, n, cap, amp_cap, a.max_iter, lane, lm_slots[warp], warm.cost_tol);
                 st = fit_status_of(q, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
                 if (it < a.max_iter && st == SPX_ST_OK) {
                     for (int i = 0; i < 6; ++i) p[i] = q[i];
@@ -260,7 +263,7 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
             fell_back = !done;
         }
         if (!done) {
-            it += warp_lm_fit(p, v, xy, n, cap, amp_cap, a.max_iter, lane, a.cost_tol);
+            it += warp_lm_fit(p, v, xy, n, cap, amp_cap, a.max_iter, lane, lm_slots[warp], a.cost_tol);
             st = fit_status_of(p, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
         }
         if (lane == 0) {
@@ -282,6 +285,7 @@ __global__ void k_fit_iteration(FitArgs a, spx_bgmap bg, const double* model, in
                                 const double* params, double relaxation, double* params_out,
                                 uint8_t* status_out, double* maxstep, int* iters) {
     extern __shared__ unsigned char smem[];
+    __shared__ double lm_slots[kFitWarpsMax][54];  // kept / trial normal-equation sums per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     T* v;
     int* xy;
@@ -322,7 +326,8 @@ __global__ void k_fit_iteration(FitArgs a, spx_bgmap bg, const double* model, in
         double p[6];
         for (int i = 0; i < 6; ++i) p[i] = p0[i];
         const double cap = a.caps[j];
-        const int it = warp_lm_fit(p, v, xy, n, cap, 3.0 * fmax(amax, 1e-12), a.max_iter, lane, a.cost_tol);
+        const int it =
+            warp_lm_fit(p, v, xy, n, cap, 3.0 * fmax(amax, 1e-12), a.max_iter, lane, lm_slots[warp], a.cost_tol);
         if (lane == 0) {
             double q[6];
             bool finite = true;
@@ -1007,7 +1012,7 @@ template <typename T>
 int launch_fit_initial(const FitArgs& a0, FitLayout L, cudaStream_t s, const double* seeds, double background_level,
                        int has_level, double* params, uint8_t* status, int* iterations, WarmStart warm) {
     return launch_fit(a0, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
-        if (smem > 48 * 1024)
+        if (smem + kLmSlotBytes > 48 * 1024)
             SPX_CUDA(cudaFuncSetAttribute(k_fit_initial<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_fit_initial<T><<<blocks, warps * 32, smem, s>>>(fa, seeds, background_level, has_level, params, status,
                                                            iterations, warm);
@@ -1020,7 +1025,7 @@ int launch_fit_iteration(const FitArgs& a0, FitLayout L, cudaStream_t s, const s
                          int radius_cap, const double* params, double relaxation, double* params_out,
                          uint8_t* status_out, double* maxstep, int* iterations) {
     return launch_fit(a0, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
-        if (smem > 48 * 1024)
+        if (smem + kLmSlotBytes > 48 * 1024)
             SPX_CUDA(cudaFuncSetAttribute(k_fit_iteration<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_fit_iteration<T><<<blocks, warps * 32, smem, s>>>(fa, bg, model, radius_cap, params, relaxation,
                                                              params_out, status_out, maxstep, iterations);

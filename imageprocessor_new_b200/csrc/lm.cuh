@@ -96,7 +96,8 @@ __device__ __forceinline__ void damped_solve(const double* nu, const double* g, 
 // partial sums meet at every level, so the totals are identical to 27 separate butterflies) but as a
 // reduce-scatter: at each level a lane keeps half of its slots, adding its partner's copy of them,
 // so 31 additions and shuffles replace 135; lane i then holds total i and broadcasts it.
-__device__ __forceinline__ void warp_allreduce27(double* s, int lane) {
+// `slot` (shared memory, 27 doubles, or null) also receives the totals (lane i writes total i).
+__device__ __forceinline__ void warp_allreduce27(double* s, int lane, double* slot = nullptr) {
     double a[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) a[i] = i < 27 ? s[i] : 0.0;
@@ -110,6 +111,7 @@ __device__ __forceinline__ void warp_allreduce27(double* s, int lane) {
             a[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
         }
     }
+    if (slot && lane < 27) slot[lane] = a[0];
 #pragma unroll
     for (int i = 0; i < 27; ++i) s[i] = __shfl_sync(0xffffffffu, a[0], i);
 }
@@ -118,7 +120,7 @@ __device__ __forceinline__ void warp_allreduce27(double* s, int lane) {
 // into s[0..26] and the cost sum of r^2 with r = v - A shape (numpy's model-then-residual order),
 // as warp totals identical on all lanes.
 __device__ __forceinline__ double warp_normal_pass(const double* q, const double* v, const int* xy, int n, int lane,
-                                                   double* s) {
+                                                   double* s, double* slot = nullptr) {
 #pragma unroll
     for (int i = 0; i < 27; ++i) s[i] = 0.0;
     double acc = 0.0;
@@ -145,7 +147,7 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const double
 #pragma unroll
         for (int i = 0; i < 6; ++i) s[21 + i] += J[i] * r;
     }
-    warp_allreduce27(s, lane);
+    warp_allreduce27(s, lane, slot);
     return warp_sum(acc);
 }
 
@@ -167,7 +169,7 @@ __device__ __forceinline__ float u16_to_float(int u) { return __int_as_float(0x4
 // The FP32 pass: as warp_normal_pass above with the per-pixel arithmetic and lane sums in FP32
 // (ROI-local coordinates keep dx, dy within a few ulp of 64) and FP64 warp totals.
 __device__ __forceinline__ double warp_normal_pass(const double* q, const float* v, const int* xy, int n, int lane,
-                                                   double* s) {
+                                                   double* s, double* slot = nullptr) {
     float jj[21];
 #pragma unroll
     for (int i = 0; i < 21; ++i) jj[i] = 0.0f;
@@ -201,7 +203,7 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const float*
     for (int i = 0; i < 21; ++i) s[i] = (double)jj[i];
 #pragma unroll
     for (int i = 0; i < 6; ++i) s[21 + i] = jr[i].total();
-    warp_allreduce27(s, lane);
+    warp_allreduce27(s, lane, slot);
     return warp_sum(cost.total());
 }
 
@@ -209,15 +211,18 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const float*
 // iterations run. `cap` is the cell's sigma cap, `amp_cap` 3 * max(max|v|, 1e-12).
 //
 // Each trial's cost is evaluated in the same pass as its normal equations: an accepted trial (the
-// usual case) hands its sums to the next iteration, a rejected one recomputes the sums at the kept
-// params. The arithmetic of every sum is that of separate Jacobian and cost passes.
+// usual case) hands its sums to the next iteration; a rejected one restores the sums of the kept
+// params, which every pass also leaves in one of the warp's two shared-memory slots (`slots`, 54
+// doubles; the pass at the kept params wrote slot `kept`, a trial writes the other one). The
+// arithmetic of every sum is that of separate Jacobian and cost passes.
 // `cost_tol` is the relative cost drop at or below which an accepted step ends the fit (1e-12, the
 // reference's rule, by default).
 template <typename T>
 __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, double cap, double amp_cap,
-                                  int max_iter, int lane, double cost_tol = 1e-12) {
+                                  int max_iter, int lane, double* slots, double cost_tol = 1e-12) {
     double s[27];
-    double cost = warp_normal_pass(p, v, xy, n, lane, s);
+    int kept = 0;
+    double cost = warp_normal_pass(p, v, xy, n, lane, s, slots);
     if (!isfinite(cost)) return 0;
     double lam = 1e-3;
     const double lo = -log(cap), hi = -log(kSigmaMin);
@@ -239,7 +244,7 @@ __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, d
         bool small = smax < 1e-7;
 #pragma unroll
         for (int i = 0; i < 6; ++i) small = small && !isnan(step[i]);
-        const double new_cost = warp_normal_pass(trial, v, xy, n, lane, s);
+        const double new_cost = warp_normal_pass(trial, v, xy, n, lane, s, slots + 27 * (kept ^ 1));
         const bool better = isfinite(new_cost) && new_cost <= cost;
         const bool done = (better && (cost - new_cost <= cost_tol * fmax(cost, 1e-300))) || small;
         if (better) {
@@ -247,12 +252,18 @@ __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, d
             for (int i = 0; i < 6; ++i) p[i] = trial[i];
             lam /= 3.0;
             cost = new_cost;
+            kept ^= 1;
         } else {
             lam *= 4.0;
         }
         if (done || lam > 1e12) { ++it; break; }
-        if (!better && it + 1 < max_iter) warp_normal_pass(p, v, xy, n, lane, s);
+        if (!better && it + 1 < max_iter) {
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 27; ++i) s[i] = slots[27 * kept + i];
+        }
     }
+    __syncwarp();
     return it;
 }
 
