@@ -153,8 +153,10 @@ struct WarmStart {
 };
 
 // T: type of the staged cell values and of the LM's per-pixel arithmetic (double or float).
+// Launch bounds: at most 8 warps, two such blocks per SM, which caps registers at 128 (a few spilled
+// in the solve) so that 16 warps of 4-warp blocks fit per SM.
 template <typename T>
-__global__ void k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
+__global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
                               double* params, uint8_t* status, int* iters, WarmStart warm) {
     extern __shared__ unsigned char smem[];
     __shared__ double lm_slots[kFitWarpsMax][54];  // kept / trial normal-equation sums per warp
@@ -281,7 +283,7 @@ __global__ void k_fit_initial(FitArgs a, const double* seeds, double background_
 // current params, relaxation p + relax * (fitted - p) (non-finite components step 0), status of
 // the relaxed params, and max |step[1:]| (NaN unless the cell is "ok" with a finite fit).
 template <typename T>
-__global__ void k_fit_iteration(FitArgs a, spx_bgmap bg, const double* model, int radius_cap,
+__global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_iteration(FitArgs a, spx_bgmap bg, const double* model, int radius_cap,
                                 const double* params, double relaxation, double* params_out,
                                 uint8_t* status_out, double* maxstep, int* iters) {
     extern __shared__ unsigned char smem[];

@@ -38,7 +38,9 @@ __device__ __forceinline__ GaussEval gauss_eval(const double* p, double e1, doub
 }
 
 // Solves (N + diag(lam * N_ii + 1e-12)) s = g for the symmetric 6x6 N given by its upper triangle
-// (21 values, row-major) by Cholesky; NaN propagates into s when the matrix is not positive.
+// (21 values, row-major) by Cholesky; NaN propagates into s when the matrix is not positive. The
+// factor keeps the reciprocals of its diagonal (one rsqrt per pivot, multiplications instead of
+// the square roots and divisions, which sit on the fit's critical path).
 __device__ __forceinline__ void damped_solve(const double* nu, const double* g, double lam, double* s) {
     // Dense 6x6 storage with compile-time indices only, so the factor stays in registers.
     double U[6][6];
@@ -52,16 +54,15 @@ __device__ __forceinline__ void damped_solve(const double* nu, const double* g, 
                 if (i == j) v = v + (lam * v + 1e-12);
                 U[i][j] = v;
             }
-    // In-place Cholesky of the upper triangle: U^T U = M.
+    // In-place Cholesky of the upper triangle, U^T U = M, with 1 / U_ii kept on the diagonal.
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         double d = U[i][i];
 #pragma unroll
         for (int k = 0; k < 6; ++k)
             if (k < i) d -= U[k][i] * U[k][i];
-        d = sqrt(d);  // NaN when not positive definite
-        U[i][i] = d;
-        const double inv = 1.0 / d;
+        const double inv = rsqrt(d);  // NaN when not positive definite
+        U[i][i] = inv;
 #pragma unroll
         for (int j = 0; j < 6; ++j)
             if (j > i) {
@@ -80,7 +81,7 @@ __device__ __forceinline__ void damped_solve(const double* nu, const double* g, 
 #pragma unroll
         for (int k = 0; k < 6; ++k)
             if (k < i) v -= U[k][i] * y[k];
-        y[i] = v / U[i][i];
+        y[i] = v * U[i][i];
     }
 #pragma unroll
     for (int i = 5; i >= 0; --i) {
@@ -88,7 +89,7 @@ __device__ __forceinline__ void damped_solve(const double* nu, const double* g, 
 #pragma unroll
         for (int k = 0; k < 6; ++k)
             if (k > i) v -= U[i][k] * s[k];
-        s[i] = v / U[i][i];
+        s[i] = v * U[i][i];
     }
 }
 
