@@ -606,40 +606,10 @@ __device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, d
     return out;
 }
 
-// The 4x4 coefficient window around the last sample of a ray, kept in registers and reloaded
-// only when the ray enters another integer cell (about every 10 samples at 0.1 px steps). The
-// sum runs in the same order as cubic_at.
-struct SplineWindow {
-    int fy = -1 << 30, fx = -1 << 30;
-    double c[16];
-    __device__ __forceinline__ double at(const double* coef, int hp, int wp, double y, double x) {
-        const double fyd = floor(y), fxd = floor(x);
-        const int iy = (int)fyd, ix = (int)fxd;
-        if (iy != fy || ix != fx) {
-            fy = iy;
-            fx = ix;
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const int ya = min(max(iy - 1 + a, 0), hp - 1);
-#pragma unroll
-                for (int b = 0; b < 4; ++b) c[a * 4 + b] = coef[ya * wp + min(max(ix - 1 + b, 0), wp - 1)];
-            }
-        }
-        double wy[4], wx[4];
-        cubic_weights_t(y - fyd, wy);
-        cubic_weights_t(x - fxd, wx);
-        double out = 0.0;
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) out += c[a * 4 + b] * wy[a] * wx[b];
-        return out;
-    }
-};
-
 // The same window evaluated in FP32 (weights, products and sums), the sampling precision the ray
-// profiles use: sample positions stay FP64 and only their fractional offsets inside the window are
-// rounded to FP32, so a sample differs from the FP64 evaluation by ~1e-7 relative.
+// profiles use, from an FP32 copy of the coefficients: sample positions stay FP64 and only their
+// fractional offsets inside the window are rounded to FP32, so a sample differs from the FP64
+// evaluation by ~1e-7 relative. The caller passes the window's integer cell and the offsets.
 struct SplineWindowF {
     int fy = -1 << 30, fx = -1 << 30;
     float c[16];
@@ -651,22 +621,21 @@ struct SplineWindowF {
         w[0] = s * s * s * k;
         w[3] = 1.0f - w[0] - w[1] - w[2];
     }
-    __device__ __forceinline__ double at(const double* coef, int hp, int wp, double y, double x) {
-        const double fyd = floor(y), fxd = floor(x);
-        const int iy = (int)fyd, ix = (int)fxd;
+    // (iy, ix): the sample's cell in padded coordinates, at least 1 and at most hp - 3 / wp - 3 for a
+    // sample inside the cell box (the padding is wider than the 4 x 4 window), so no clamping.
+    __device__ __forceinline__ float at(const float* coef, int wp, int iy, int ix, float ty, float tx) {
         if (iy != fy || ix != fx) {
             fy = iy;
             fx = ix;
+            const float* q = coef + (iy - 1) * wp + (ix - 1);
 #pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const int ya = min(max(iy - 1 + a, 0), hp - 1);
+            for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 4; ++b) c[a * 4 + b] = (float)coef[ya * wp + min(max(ix - 1 + b, 0), wp - 1)];
-            }
+                for (int b = 0; b < 4; ++b) c[a * 4 + b] = q[a * wp + b];
         }
         float wy[4], wx[4];
-        weights((float)(y - fyd), wy);
-        weights((float)(x - fxd), wx);
+        weights(ty, wy);
+        weights(tx, wx);
         float out = 0.0f;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
@@ -675,16 +644,34 @@ struct SplineWindowF {
             for (int b = 0; b < 4; ++b) row = fmaf(c[a * 4 + b], wx[b], row);
             out = fmaf(row, wy[a], out);
         }
-        return (double)out;
+        return out;
     }
 };
 
-constexpr int kRadialThreads = 128;
+// floor(y) for 0 <= y < 2^51 as an int and as a double, with FP64 additions only (no conversion
+// instructions): y + 1.5 * 2^52 holds y rounded to an integer in its low mantissa bits, and one
+// comparison turns the rounding into a floor.
+__device__ __forceinline__ int floor_nonneg(double y, double* fl) {
+    const double magic = 6755399441055744.0;
+    const double t = __dadd_rn(y, magic);
+    double r = __dsub_rn(t, magic);
+    int n = __double2loint(t);
+    if (r > y) {
+        r -= 1.0;
+        n -= 1;
+    }
+    *fl = r;
+    return n;
+}
 
-// Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients, a reduction
-// area, then the cell mask and the eroded mask as bytes.
+constexpr int kRadialThreads = 128;
+constexpr int kTrigMax = 256;  // ray angles with a cos / sin table in shared memory (4 KB)
+
+// Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients in FP64 and in
+// FP32, a reduction area, then the cell mask and the eroded mask as bytes.
 __host__ __device__ inline long long radial_cta_doubles(int hm, int wm) {
-    return (long long)(hm + 2 * kPad) * (wm + 2 * kPad) + 32 + (2LL * hm * wm + 7) / 8;
+    const long long np = (long long)(hm + 2 * kPad) * (wm + 2 * kPad);
+    return np + (np + 1) / 2 + 32 + (2LL * hm * wm + 7) / 8;
 }
 
 // Sum over the CTA's 4 warps in a fixed order (the same value on every thread). Slots of `red`
@@ -720,17 +707,26 @@ __device__ void radial_clear(const MethodOut out, int i, int n_angles) {
 }
 
 // Contour, polygon geometry and metrics of one method from its edge radii (one warp).
+// trig: cos and sin of the n_angles ray angles (interleaved), or null to evaluate them here.
 __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i, int n_angles, double cx, double cy,
-                                           double peak, int4 box) {
+                                           double peak, int4 box, const double* trig) {
     if (!out.status) return;
     const int lane = threadIdx.x & 31, nv = n_angles + 1;
     const double* edge = out.edge_px + (long long)i * n_angles;
     const double step = 2.0 * kPi / n_angles;
     auto vertex = [&](int k, double* x, double* y) {
         const int a = k % n_angles;
-        const double ang = (double)a * step;
-        *x = cx + edge[a] * cos(ang);
-        *y = cy + edge[a] * sin(ang);
+        double c, sn;
+        if (trig) {
+            c = trig[2 * a];
+            sn = trig[2 * a + 1];
+        } else {
+            const double ang = (double)a * step;
+            c = cos(ang);
+            sn = sin(ang);
+        }
+        *x = cx + edge[a] * c;
+        *y = cy + edge[a] * sn;
     };
     if (out.contours)
         for (int k = lane; k < nv; k += 32) {
@@ -772,10 +768,19 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
     int n_angles, double radial_step, int n_radii, double* coef_scratch, MethodOut half_out, MethodOut grad_out) {
     extern __shared__ double sm[];
+    __shared__ double trig_tab[2 * kTrigMax];  // cos, sin of the ray angles (n_angles <= kTrigMax)
     const int tid = threadIdx.x, warp = tid >> 5;
     const int hp = hm + 2 * kPad, wp = wm + 2 * kPad, area_px = hm * wm;
+    const double* trig = n_angles <= kTrigMax ? trig_tab : nullptr;
+    if (trig)
+        for (int a = tid; a < n_angles; a += kRadialThreads) {
+            const double ang = (double)a * (2.0 * kPi / n_angles);
+            trig_tab[2 * a] = cos(ang);
+            trig_tab[2 * a + 1] = sin(ang);
+        }
     double* coef = coef_scratch ? coef_scratch + (long long)blockIdx.x * radial_cta_doubles(hm, wm) : sm;
-    double* red = coef + (long long)hp * wp;  // 32 doubles: 8 slots of 4
+    float* coef_f = reinterpret_cast<float*>(coef + (long long)hp * wp);
+    double* red = coef + (long long)hp * wp + ((long long)hp * wp + 1) / 2;  // 32 doubles: 8 slots of 4
     uint8_t* mask = reinterpret_cast<uint8_t*>(red + 32);
     uint8_t* emask = mask + area_px;
     const double thr = fmax(0.35, 2.0 * radial_step);
@@ -832,6 +837,8 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         for (int row = tid; row < hp; row += kRadialThreads) spline_line(coef + (long long)row * wp, wp, 1);
         __syncthreads();
         const double peak = cubic_at(coef, hp, wp, cy + kPad, cx + kPad);
+        for (int k = tid; k < hp * wp; k += kRadialThreads) coef_f[k] = (float)coef[k];
+        __syncthreads();
         const double half = peak / 2.0;
         const double inv2s = 1.0 / (2.0 * radial_step);
         int j_min = 2;  // first gradient candidate: j >= 2 and j * step >= thr
@@ -841,7 +848,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
             double edge_h = dnan(), edge_g = dnan();
             if (peak > 0.0) {
                 const double ang = (double)ray * (2.0 * kPi / n_angles);
-                const double ux = cos(ang), uy = sin(ang);
+                const double ux = trig ? trig[2 * ray] : cos(ang), uy = trig ? trig[2 * ray + 1] : sin(ang);
                 // Samples are FP32 (SplineWindowF); the profile bookkeeping follows in FP32 and the
                 // edge positions are computed in FP64 from the kept samples.
                 float h1 = 0, h2 = 0, h3 = 0, h4 = 0;  // p[k-1] .. p[k-4]
@@ -852,22 +859,24 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                 SplineWindowF win;
                 int mfy = -1 << 30, mfx = -1 << 30;  // mask cell of the last sample and whether all
                 bool mfull = false;                   // four of its corners are in the eroded cell
-                for (int k = 0; k < n_radii; ++k) {
-                    const double r = (double)k * radial_step;
+                const double ymax = (double)(hm - 1), xmax = (double)(wm - 1);
+                double kd = 0.0;  // k as a double (exact), so r = k * step needs no conversion
+                for (int k = 0; k < n_radii; ++k, kd += 1.0) {
+                    const double r = kd * radial_step;
                     const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
-                    bool valid = y >= 0.0 && y <= (double)(hm - 1) && x >= 0.0 && x <= (double)(wm - 1);
-                    if (valid) {
-                        const int iy = (int)floor(y), ix = (int)floor(x);
-                        if (iy != mfy || ix != mfx) {
-                            mfy = iy;
-                            mfx = ix;
-                            const uint8_t* q = emask + iy * wm + ix;
-                            mfull = iy + 1 < hm && ix + 1 < wm && q[0] && q[1] && q[wm] && q[wm + 1];
-                        }
-                        valid = mfull || inside_bytes(emask, hm, wm, y, x);
+                    if (!(y >= 0.0 && y <= ymax && x >= 0.0 && x <= xmax)) { first_invalid = k; break; }
+                    double fyd, fxd;
+                    const int iy = floor_nonneg(y, &fyd), ix = floor_nonneg(x, &fxd);
+                    if (iy != mfy || ix != mfx) {
+                        mfy = iy;
+                        mfx = ix;
+                        const uint8_t* q = emask + iy * wm + ix;
+                        mfull = iy + 1 < hm && ix + 1 < wm && q[0] && q[1] && q[wm] && q[wm + 1];
                     }
-                    if (!valid) { first_invalid = k; break; }
-                    const float p = k == 0 ? (float)peak : (float)win.at(coef, hp, wp, y + kPad, x + kPad);
+                    if (!(mfull || inside_bytes(emask, hm, wm, y, x))) { first_invalid = k; break; }
+                    const float p = k == 0 ? (float)peak
+                                           : win.at(coef_f, wp, iy + kPad, ix + kPad, (float)(y - fyd),
+                                                    (float)(x - fxd));
                     if (k >= 1 && !crossed && h1 >= halff && p < halff) {
                         edge_h = (double)(k - 1) * radial_step +
                                  (((double)h1 - half) / ((double)h1 - (double)p)) * radial_step;
@@ -912,7 +921,8 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         const int all_h = (int)cta_sum((double)found_h, red + 20);
         const int all_g = (int)cta_sum((double)found_g, red + 24);  // also orders the edge writes
         if (warp < 2)  // warp 0: halfmax, warp 1: gradient
-            radial_finish(warp == 0 ? half_out : grad_out, warp == 0 ? all_h : all_g, i, n_angles, cx, cy, peak, c.box);
+            radial_finish(warp == 0 ? half_out : grad_out, warp == 0 ? all_h : all_g, i, n_angles, cx, cy, peak, c.box,
+                          trig);
     }
 }
 
@@ -1003,7 +1013,7 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
     double* scratch = nullptr;
     int blocks;
     if (smem) {
-        if (smem > 48 * 1024)
+        if (smem + 2 * kTrigMax * sizeof(double) > 48 * 1024)  // with the static cos / sin table
             SPX_CUDA(cudaFuncSetAttribute(k_radial_cd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
         SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd, kRadialThreads, smem));
