@@ -12,6 +12,10 @@ radial-gradient and half-height CDs, summary_only), all through the public API.
 Cells = Voronoi cells reported and measured by the LM Gaussian method. The page (134 MB) is larger
 than the 126 MB L2, so consecutive steps do not run from cache.
 
+``--tiled`` measures the tiled detection instead (one JSON line of its own): detect_centers_tiled
+(tile_h 8192, overlap 128, global Otsu) on a 32768 x 32768 uint16 square array (pitch 20, d 10,
+~2.7M holes) rendered on the device, with the graph-captured band pipeline and with the eager one.
+
 ``--impl reference`` times the CPU path (the oracle restatement of the reference algorithm, NumPy /
 SciPy on the host cores) on a crop of the same page; under torchrun only rank 0 runs it.
 Multi-GPU: one process per GPU, each measuring its own page (weak scaling, no collective on the
@@ -338,6 +342,46 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def tiled_arm(args):
+    """detect_centers_tiled on the 32768 x 32768 page: centres/s with band graphs and eagerly."""
+    import torch
+
+    from imageprocessor_new_b200 import synthetic, tiled
+
+    torch.cuda.set_device(0)
+    page_d, truth = synthetic.page_large_device(0, args.tiled_size)
+    torch.cuda.synchronize()
+    kw = dict(threshold="otsu", invert=False, area_min=1, area_max=400, pad=3, refine="auto", connectivity=8,
+              small_feature_max=12.0, tile_h=8192, overlap=128, threshold_mode="global", otsu_downsample=4,
+              thr_scale=0.8, dedupe_eps=1.5, device=0)
+    out = {}
+    for name, graphs in (("graphs", True), ("eager", False)):
+        for _ in range(max(1, args.warmup)):
+            res = tiled.detect_tiled(page_d, use_graphs=graphs, **kw)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(args.steps):
+            res = tiled.detect_tiled(page_d, use_graphs=graphs, **kw)
+        e.record()
+        torch.cuda.synchronize()
+        out[name] = (s.elapsed_time(e) / args.steps, len(res.centers_xy), res)
+    ms, n, res = out["graphs"]
+    px = args.tiled_size ** 2
+    print(json.dumps({
+        "metric": "centres/s, detect_centers_tiled", "value": round(n / (ms / 1e3), 1), "unit": "centres/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "mpix_per_s": round(px / 1e6 / (ms / 1e3), 1), "centres": n, "true_holes": int(len(truth)),
+        "band_graphs": bool(res.meta["band_graphs"]),
+        "eager": {"ms_per_step": round(out["eager"][0], 3),
+                  "value": round(out["eager"][1] / (out["eager"][0] / 1e3), 1)},
+        "graphs_equal_eager": bool(np.array_equal(res.centers_xy, out["eager"][2].centers_xy)),
+        "dtype": "u16 in, f64 centres", "data": "synthetic (rendered on the device)",
+        "config": {"workload": f"page_square_{args.tiled_size}x{args.tiled_size}_u16_pitch20_d10_tiled",
+                   "tile_h": 8192, "overlap": 128, "threshold": "otsu (global, img[::4, ::4] x 0.8)",
+                   "refine": "auto"}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -350,8 +394,12 @@ def main():
     ap.add_argument("--no-warm-start", dest="warm_start", action="store_false")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--tiled", action="store_true", help="measure detect_centers_tiled on the 32768^2 page instead")
+    ap.add_argument("--tiled-size", type=int, default=32768)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.tiled:
+        tiled_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         gpu_arm(args)

@@ -31,9 +31,16 @@ def ptr(t: torch.Tensor | None) -> int | None:
 
 
 def upload(a: np.ndarray) -> torch.Tensor:
-    """Host array -> contiguous device tensor (same dtype)."""
+    """Host array -> contiguous device tensor (same dtype), queued on the current stream.
+
+    The data goes through pinned memory: a copy from pageable memory would first synchronise the
+    stream (draining the GPU at every small upload); from pinned memory it is asynchronous, and
+    torch's host allocator keeps the pinned block until the copy has run."""
     a = np.ascontiguousarray(a)
-    return torch.from_numpy(a).to("cuda", non_blocking=False)
+    dtype = TORCH_ALL.get(a.dtype) or torch.from_numpy(np.empty(0, a.dtype)).dtype
+    pinned = torch.empty(a.shape, dtype=dtype, pin_memory=True)
+    pinned.numpy()[...] = a
+    return pinned.to("cuda", non_blocking=True)
 
 
 def start_download(t: torch.Tensor) -> np.ndarray:
@@ -59,6 +66,10 @@ def read_int(t: torch.Tensor) -> int:
 
 TORCH_DTYPES = {np.dtype(np.uint8): torch.uint8, np.dtype(np.uint16): torch.uint16,
                 np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64}
+# Every dtype the package uploads (image dtypes plus indices, flags and parameters).
+TORCH_ALL = {**TORCH_DTYPES, np.dtype(np.int8): torch.int8, np.dtype(np.int16): torch.int16,
+             np.dtype(np.int32): torch.int32, np.dtype(np.int64): torch.int64, np.dtype(np.bool_): torch.bool,
+             np.dtype(np.uint32): torch.uint32, np.dtype(np.uint64): torch.uint64}
 
 
 def dtype_code(t: torch.Tensor) -> int:

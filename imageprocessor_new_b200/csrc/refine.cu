@@ -611,10 +611,15 @@ __device__ void refine_edge(const void* img, int dtype, const int* labels, int W
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 k_refine(const void* img, int dtype, int H, int W, const int* labels, const int* rows,
-         const uint8_t* methods, int n, int pad, double* centers) {
+         const uint8_t* methods, int n, const int* n_dev, int pad, double* centers) {
     __shared__ double keys[kWarpsPerBlock][kSortCap];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int live = n_dev ? min(*n_dev, n) : n;  // rows past a device count are outputs of NaN
     for (int blob = blockIdx.x * kWarpsPerBlock + warp; blob < n; blob += gridDim.x * kWarpsPerBlock) {
+        if (blob >= live) {
+            if (lane == 0) centers[2LL * blob] = centers[2LL * blob + 1] = dnan();
+            continue;
+        }
         const Roi r = make_roi(rows + (long long)blob * 5, pad, H, W);
         const int m = methods[blob];
         double cx = dnan(), cy = dnan();
@@ -717,7 +722,21 @@ int spx_refine_centers(const void* img, int dtype, int height, int width, const 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
     k_refine<<<blocks < 148 * 16 ? blocks : 148 * 16, kWarpsPerBlock * 32, 0, s>>>(
-        img, dtype, height, width, labels, rows, methods, n, pad, centers_out);
+        img, dtype, height, width, labels, rows, methods, n, nullptr, pad, centers_out);
+    return check_launch("k_refine");
+}
+
+int spx_refine_centers_counted(const void* img, int dtype, int height, int width, const int* labels,
+                               const int* rows, const uint8_t* methods, const int* n_dev, int capacity, int pad,
+                               double* centers_out, void* stream) {
+    SPX_REQUIRE(capacity >= 0 && pad >= 0, "bad arguments");
+    if (capacity == 0) return SPX_OK;
+    SPX_REQUIRE(img && labels && rows && methods && n_dev && centers_out, "null pointer");
+    SPX_REQUIRE(dtype >= SPX_U8 && dtype <= SPX_F64, "bad dtype");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int blocks = (capacity + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    k_refine<<<blocks < 148 * 16 ? blocks : 148 * 16, kWarpsPerBlock * 32, 0, s>>>(
+        img, dtype, height, width, labels, rows, methods, capacity, n_dev, pad, centers_out);
     return check_launch("k_refine");
 }
 

@@ -99,7 +99,7 @@ def auto_tile(seeds_d: torch.Tensor, n: int, shape) -> tuple[int, float]:
 def quantiles(reqs) -> np.ndarray:
     """Run spx_quantiles on a list of _lib.QuantileReq; (len, 2) array of (value, count)."""
     arr = (_lib.QuantileReq * len(reqs))(*reqs)
-    raw = torch.frombuffer(bytearray(bytes(arr)), dtype=torch.uint8).to("cuda")
+    raw = dev.upload(np.frombuffer(bytes(arr), dtype=np.uint8))
     out = dev.empty((len(reqs), 2), torch.float64)
     _lib.call("spx_quantiles", raw.data_ptr(), len(reqs), out.data_ptr(), dev.stream_ptr())
     return out.cpu().numpy()

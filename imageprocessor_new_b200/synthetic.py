@@ -11,10 +11,9 @@ tabulated once per (R, s) and sampled at pixel centres. The named workloads:
                     3000 counts on 1000, Poisson + N(0, 20) read noise.
 * ``page_staggered`` 8192 x 8192 uint16 staggered array (pitch 24 x 24, odd rows shifted 12), d 12 +- 5 %, sigma 1.2,
                     3000 on 1000, N(0, 100) read noise (SNR ~30), ~116k holes incl. border-clipped.
-* ``page_large``    32768 x 32768 uint16 square array, pitch 20, d 10 +- 4 %, sigma 1.0, slow
-                    +-15 % sinusoidal illumination, ~2.7M holes (rendered on the GPU with torch).
-* ``stack_uneven``  4096 x 4096 pages with pitch U(16, 40), d 0.4-0.6 x pitch, 5 % missing and 2 %
-                    merged holes.
+* ``page_large_device`` 32768 x 32768 uint16 square array, pitch 20, d 10 +- 4 %, sigma 1.0, slow
+                    +-15 % sinusoidal illumination of the hole contrast, ~2.7M holes, rendered on the
+                    GPU (pixel coverage of each disc sampled 4 x 4, blurred, noise added on the device).
 * ``gaussian_lattice`` the Gaussian-spot lattice of the reference's GPU tests (amplitude 50 on 20).
 """
 
@@ -164,3 +163,50 @@ def dot_grid(rows=4, cols=4, spacing=20, dot_size=3, margin=10):
             img[y0:y0 + dot_size, x0:x0 + dot_size] = 255
             expected.append([x0 + (dot_size - 1) / 2.0, y0 + (dot_size - 1) / 2.0])
     return img, np.array(expected, dtype=np.float64)
+
+
+def page_large_device(seed: int = 0, size: int = 32768, *, pitch: float = 20.0, d: float = 10.0, sigma: float = 1.0,
+                      amplitude: float = 3000.0, background: float = 1000.0, read_noise: float = 20.0):
+    """The tiled-detection page on the device (uint16 torch tensor) and its true centres (host)."""
+    import ctypes
+
+    import torch
+
+    from . import _device as dev
+    from . import _lib
+
+    rng = np.random.default_rng(seed)
+    centers = square_grid((size, size), pitch, rng)
+    n = len(centers)
+    di = d * (1.0 + rng.uniform(-0.04, 0.04, n))
+    holes = np.column_stack((centers, di / 2, di / 2, np.zeros(n), np.full(n, 2.0)))
+    cell = float(np.ceil(pitch))
+    gw = int(np.ceil(size / cell)) + 1
+    gx = np.clip(np.floor(holes[:, 0] / cell).astype(np.int64), 0, gw - 1)
+    gy = np.clip(np.floor(holes[:, 1] / cell).astype(np.int64), 0, gw - 1)
+    key = gy * gw + gx
+    order = np.argsort(key, kind="stable")
+    start = np.zeros(gw * gw + 1, np.int64)
+    np.add.at(start, key + 1, 1)
+    start = np.cumsum(start).astype(np.int32)
+    holes_d = dev.upload(np.ascontiguousarray(holes))
+    start_d, ids_d = dev.upload(start), dev.upload(order.astype(np.int32))
+    s = dev.stream_ptr()
+    cov = dev.empty((size, size), torch.float64)
+    _lib.call("spx_hole_coverage", size, size, holes_d.data_ptr(), start_d.data_ptr(), ids_d.data_ptr(), gw, gw, cell,
+              4, cov.data_ptr(), s)
+    radius = int(4.0 * sigma + 0.5)
+    x = np.arange(-radius, radius + 1)
+    phi = np.exp(-0.5 / (sigma * sigma) * x ** 2)
+    wts = dev.upload(phi / phi.sum())
+    tmp = dev.empty((size, size), torch.float64)
+    _lib.call("spx_gaussian_filter", cov.data_ptr(), size, size, wts.data_ptr(), radius, tmp.data_ptr(),
+              cov.data_ptr(), s)
+    del tmp
+    wave = torch.sin(2.0 * np.pi / 8192.0 * torch.arange(size, dtype=torch.float64, device="cuda"))
+    for r0 in range(0, size, 1024):  # cov *= 1 + 0.15 sin(2 pi y / 8192) sin(2 pi x / 8192), in row blocks
+        cov[r0:r0 + 1024] *= 1.0 + 0.15 * wave[r0:r0 + 1024, None] * wave[None, :]
+    page = dev.empty((size, size), torch.uint16)
+    _lib.call("spx_page_finish", cov.data_ptr(), size * size, float(background), float(amplitude), float(read_noise),
+              ctypes.c_ulonglong(int(rng.integers(0, 2 ** 63))), page.data_ptr(), s)
+    return page, centers

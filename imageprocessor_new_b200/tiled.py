@@ -1,7 +1,14 @@
 """Tiled centre detection with the page resident on the device (detect_centers(tile_h=...),
 subpx/_gpu/centers.py:1778-1862): a global Otsu threshold of img[::ds, ::ds] x thr_scale, bands of
 tile_h rows stepping tile_h - overlap, the keep-band rule, then a GPU dedupe (O(N) with a bin grid)
-in place of the reference's O(N^2) Python loop."""
+in place of the reference's O(N^2) Python loop.
+
+With the global threshold, each band's pipeline (binarise, optional open / close, CCL, area filter,
+refiners) is captured once as a CUDA graph over fixed buffers and replayed for every band of the
+same height: the band is copied into the graph's input buffer, the counts stay on the device (the
+refiners run over a fixed capacity of rows, those past the selected count giving NaN centres that
+the keep rule drops), and the host reads the per-band component counts once at the end. A page
+with a band of more components than the capacity is redone by the eager path."""
 
 from __future__ import annotations
 
@@ -36,9 +43,121 @@ def _dedupe_device(pts_d: torch.Tensor, n: int, eps: float) -> torch.Tensor:
     return out[: dev.read_int(count)]
 
 
+# Component capacity of a captured band: one component per this many pixels (holes at a pitch of
+# 8 px or more fit; denser pages take the eager path).
+BAND_PX_PER_COMPONENT = 64
+
+
+def band_capacity(band_h: int, width: int) -> int:
+    return max(1024, band_h * width // BAND_PX_PER_COMPONENT)
+
+
+class BandGraph:
+    """The per-band pipeline of one band height, captured as a CUDA graph (see the module docstring)."""
+
+    def __init__(self, band_h: int, width: int, dtype: torch.dtype, *, fixed_threshold: float, invert: bool,
+                 area_min: int, area_max: int, pad: int, refine: str, connectivity: int, small_feature_max: float,
+                 morph_open: int = 0, morph_close: int = 0, capacity: int | None = None):
+        from .centers import _segmentation_source
+
+        self.shape = (int(band_h), int(width))
+        self.capacity = int(capacity) if capacity is not None else band_capacity(band_h, width)
+        h, w, cap = band_h, width, self.capacity
+        self.src = torch.zeros(self.shape, dtype=dtype, device="cuda")
+        self.labels = dev.empty((h, w), torch.int32)
+        self.count = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.kept = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.stats = dev.empty((cap + 1, 5), torch.int32)
+        self.centroids = dev.empty((cap + 1, 2), torch.float64)
+        self.rows = dev.empty((cap, 5), torch.int32)
+        self.methods = dev.empty((cap,), torch.uint8)
+        self.centers = dev.empty((cap, 2), torch.float64)
+        self.ccl_ws = dev.workspace(_lib.size("spx_ccl_workspace_bytes", h, w))
+        self.sel_ws = dev.workspace(_lib.size("spx_select_workspace_bytes", cap))
+        self._seg = _segmentation_source
+        self._seg_args = (float(fixed_threshold), bool(invert), int(morph_open), int(morph_close))
+        self._params = (int(area_min), int(area_max), int(pad), _lib.REFINE_CODES[refine], int(connectivity),
+                        float(small_feature_max))
+        self.graph = torch.cuda.CUDAGraph()
+        self._launch()  # eager once: first launches and attribute settings happen outside the capture
+        torch.cuda.synchronize()
+        with torch.cuda.graph(self.graph):
+            self._launch()
+
+    def _launch(self):
+        h, w = self.shape
+        area_min, area_max, pad, refine, conn, sfm = self._params
+        fixed, invert, mo, mc = self._seg_args
+        src, thr, fixed, inv = self._seg(self.src, None, fixed, invert, mo, mc)
+        stream = dev.stream_ptr()
+        _lib.call("spx_ccl_label", src.data_ptr(), dev.dtype_code(src), h, w, dev.ptr(thr), float(fixed),
+                  int(bool(inv)), conn, self.labels.data_ptr(), self.count.data_ptr(), self.ccl_ws.data_ptr(),
+                  self.ccl_ws.numel(), stream)
+        # Statistics for `capacity` labels: entries past the count stay empty (area 0), labels past
+        # the capacity are not counted.
+        _lib.call("spx_ccl_finish", self.labels.data_ptr(), h, w, conn, self.capacity, self.stats.data_ptr(),
+                  self.centroids.data_ptr(), self.ccl_ws.data_ptr(), self.ccl_ws.numel(), stream)
+        _lib.call("spx_select_components", self.stats.data_ptr(), self.capacity, area_min, area_max, refine, sfm,
+                  self.rows.data_ptr(), self.methods.data_ptr(), self.kept.data_ptr(), self.sel_ws.data_ptr(),
+                  self.sel_ws.numel(), stream)
+        _lib.call("spx_refine_centers_counted", self.src.data_ptr(), dev.dtype_code(self.src), h, w,
+                  self.labels.data_ptr(), self.rows.data_ptr(), self.methods.data_ptr(), self.kept.data_ptr(),
+                  self.capacity, pad, self.centers.data_ptr(), stream)
+
+    def run(self, band: torch.Tensor) -> torch.Tensor:
+        """Replays the pipeline on `band` (same shape); returns the (capacity, 2) centres (NaN rows
+        past the kept count) and leaves the band's component count in self.count."""
+        self.src.copy_(band)
+        self.graph.replay()
+        return self.centers
+
+
+_GRAPHS: dict = {}
+
+
+def _keep_bands(bands, kept_rows):
+    """The keep rule over (centres, y_offset, lo, hi) bands, appended on the device."""
+    kept = dev.empty((max(kept_rows, 1), 2), torch.float64)
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ws = dev.workspace(_lib.size("spx_keep_band_workspace_bytes", max((len(c) for c, *_ in bands), default=1)))
+    for c, y_off, lo, hi in bands:
+        if len(c):
+            _lib.call("spx_keep_band", c.data_ptr(), len(c), float(y_off), float(lo), float(hi), kept.data_ptr(),
+                      count.data_ptr(), max(kept_rows, 1), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+    return kept, count
+
+
+def _bands_with_graphs(img_d, spans, pre, common):
+    """Every band through a cached BandGraph of its height; None when a band overflows its capacity."""
+    width = img_d.shape[1]
+    graphs = {}
+    for y0, y1, _, _ in spans:
+        key = (y1 - y0, width, img_d.dtype, float(pre), tuple(sorted(common.items())), torch.cuda.current_device(),
+               band_capacity(y1 - y0, width))
+        if key not in _GRAPHS:
+            if len(_GRAPHS) >= 4:
+                _GRAPHS.clear()
+            _GRAPHS[key] = BandGraph(y1 - y0, width, img_d.dtype, fixed_threshold=pre, **common)
+        graphs[(y0, y1)] = _GRAPHS[key]
+    cap_total = sum(graphs[(y0, y1)].capacity for y0, y1, _, _ in spans)
+    kept = dev.empty((max(cap_total, 1), 2), torch.float64)
+    count = torch.zeros(1, dtype=torch.int32, device="cuda")
+    counts = torch.zeros(len(spans), dtype=torch.int32, device="cuda")
+    ws = dev.workspace(_lib.size("spx_keep_band_workspace_bytes", max(g.capacity for g in graphs.values())))
+    for b, (y0, y1, lo, hi) in enumerate(spans):
+        g = graphs[(y0, y1)]
+        centers = g.run(img_d[y0:y1])
+        counts[b:b + 1].copy_(g.count)
+        _lib.call("spx_keep_band", centers.data_ptr(), g.capacity, float(y0), float(lo), float(hi), kept.data_ptr(),
+                  count.data_ptr(), max(cap_total, 1), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+    if any(int(c) > graphs[spans[b][:2]].capacity for b, c in enumerate(counts.cpu().numpy())):
+        return None
+    return kept, count
+
+
 def detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, connectivity, small_feature_max,
                  tile_h, overlap, threshold_mode, otsu_downsample, thr_scale, dedupe_eps, device, morph_open=0,
-                 morph_close=0) -> CenterResult:
+                 morph_close=0, use_graphs=True) -> CenterResult:
     from .centers import _centers_on_device, _device_image
 
     if overlap >= tile_h:
@@ -52,34 +171,36 @@ def detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, con
         ds = max(1, int(otsu_downsample))
         pre = float(segment.otsu(img_d, step=ds).item()) * float(thr_scale)
     step = tile_h - overlap
-    bands = []
+    spans = []
     y0 = 0
     while y0 < height:
         y1 = min(height, y0 + tile_h)
-        band = img_d[y0:y1]
-        thr = segment.binarize_threshold(band, threshold, invert) if pre is None else None
-        c = _centers_on_device(band, threshold_dev=thr, fixed_threshold=pre if pre is not None else 0.0,
-                               invert=invert, area_min=area_min, area_max=area_max, pad=pad, refine=refine,
-                               connectivity=connectivity, small_feature_max=small_feature_max,
-                               morph_open=morph_open, morph_close=morph_close)
         half = overlap // 2
         lo = y0 if y0 == 0 else y0 + half
         hi = y1 if y1 == height else y1 - half
-        bands.append((c, y0, lo, hi))
+        spans.append((y0, y1, lo, hi))
         if y1 == height:
             break
         y0 += step
-    total = sum(len(c) for c, *_ in bands)
-    kept = dev.empty((max(total, 1), 2), torch.float64)
-    count = torch.zeros(1, dtype=torch.int32, device="cuda")
-    ws = dev.workspace(_lib.size("spx_keep_band_workspace_bytes", max((len(c) for c, *_ in bands), default=1)))
-    for c, y_off, lo, hi in bands:
-        if len(c):
-            _lib.call("spx_keep_band", c.data_ptr(), len(c), float(y_off), float(lo), float(hi), kept.data_ptr(),
-                      count.data_ptr(), max(total, 1), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+    common = dict(invert=invert, area_min=area_min, area_max=area_max, pad=pad, refine=refine,
+                  connectivity=connectivity, small_feature_max=small_feature_max, morph_open=morph_open,
+                  morph_close=morph_close)
+    graphed = pre is not None and use_graphs
+    out = _bands_with_graphs(img_d, spans, pre, common) if graphed else None
+    if out is None:
+        graphed = False
+        bands = []
+        for y0, y1, lo, hi in spans:
+            band = img_d[y0:y1]
+            thr = segment.binarize_threshold(band, threshold, invert) if pre is None else None
+            c = _centers_on_device(band, threshold_dev=thr, fixed_threshold=pre if pre is not None else 0.0, **common)
+            bands.append((c, y0, lo, hi))
+        out = _keep_bands(bands, sum(len(c) for c, *_ in bands))
+    kept, count = out
     n = dev.read_int(count)
     centers = _dedupe_device(kept[:n].contiguous(), n, float(dedupe_eps)).cpu().numpy() if n else np.zeros((0, 2))
     meta = {"tile_h": int(tile_h), "overlap": int(overlap), "threshold_mode": str(threshold_mode),
+            "band_graphs": bool(graphed),
             "otsu_downsample": int(otsu_downsample), "thr_scale": float(thr_scale), "dedupe_eps": float(dedupe_eps),
             "refine": str(refine), "invert": bool(invert), "area_min": int(area_min), "area_max": int(area_max),
             "device": int(device), "small_feature_max": float(small_feature_max)}

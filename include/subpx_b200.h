@@ -167,6 +167,12 @@ int spx_component_rows(const int* stats, const double* centroids, int num_compon
 int spx_refine_centers(const void* img, int dtype, int height, int width, const int* labels,
                        const int* rows, const uint8_t* methods, int n, int pad,
                        double* centers_out, void* stream);
+/* spx_refine_centers for the first min(*n_dev, capacity) of `capacity` rows, the count read on the
+ * device (rows past it get NaN centres), so a pipeline that selects and refines needs no host
+ * read-back of the count and can be captured in a CUDA graph. */
+int spx_refine_centers_counted(const void* img, int dtype, int height, int width, const int* labels,
+                               const int* rows, const uint8_t* methods, const int* n_dev, int capacity, int pad,
+                               double* centers_out, void* stream);
 
 /* ------------------------------------------------------------------------------------------------
  * Tiled detection (detect_centers(tile_h=...), subpx/_gpu/centers.py:1778-1862 and

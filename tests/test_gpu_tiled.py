@@ -98,3 +98,38 @@ def test_sharded_tiled_detection_on_one_rank_matches_detect_centers():
         dist.destroy_process_group()
     want = detect_centers(page, backend="gpu", tile_h=300, overlap=64, **kw).centers_xy
     np.testing.assert_array_equal(got, want)
+
+
+def _tiled_kwargs():
+    return dict(threshold="otsu", invert=False, area_min=1, area_max=400, pad=3, refine="logquad", connectivity=8,
+                small_feature_max=12.0, tile_h=1024, overlap=128, threshold_mode="global", otsu_downsample=4,
+                thr_scale=0.8, dedupe_eps=1.5, device=0)
+
+
+@pytest.mark.parametrize("morph", [(0, 0), (1, 1)])
+def test_band_graphs_match_the_eager_bands(morph):
+    """The graph-captured band pipeline gives the eager path's centres bit for bit (bands of two
+    heights, so two graphs), also with opening / closing, and again on a second replay."""
+    from imageprocessor_new_b200 import synthetic, tiled
+
+    page = synthetic.page_staggered(3, shape=(2900, 1536)).image
+    kw = dict(_tiled_kwargs(), morph_open=morph[0], morph_close=morph[1])
+    eager = tiled.detect_tiled(page, use_graphs=False, **kw)
+    graphs = tiled.detect_tiled(page, use_graphs=True, **kw)
+    assert graphs.meta["band_graphs"] and not eager.meta["band_graphs"]
+    assert len(eager.centers_xy) > 1000
+    np.testing.assert_array_equal(graphs.centers_xy, eager.centers_xy)
+    np.testing.assert_array_equal(tiled.detect_tiled(page, use_graphs=True, **kw).centers_xy, eager.centers_xy)
+
+
+def test_band_graph_overflow_takes_the_eager_path(monkeypatch):
+    """A band with more components than the captured capacity sends the page down the eager path."""
+    from imageprocessor_new_b200 import synthetic, tiled
+
+    page = synthetic.page_staggered(4, shape=(1500, 1024)).image
+    eager = tiled.detect_tiled(page, use_graphs=False, **_tiled_kwargs())
+    assert len(eager.centers_xy) > 2 * 1024
+    monkeypatch.setattr(tiled, "BAND_PX_PER_COMPONENT", 1 << 30)  # capacity 1024 < components per band
+    res = tiled.detect_tiled(page, use_graphs=True, **_tiled_kwargs())
+    assert not res.meta["band_graphs"]
+    np.testing.assert_array_equal(res.centers_xy, eager.centers_xy)
