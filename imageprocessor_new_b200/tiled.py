@@ -7,8 +7,9 @@ With the global threshold, each band's pipeline (binarise, optional open / close
 refiners) is captured once as a CUDA graph over fixed buffers and replayed for every band of the
 same height: the band is copied into the graph's input buffer, the counts stay on the device (the
 refiners run over a fixed capacity of rows, those past the selected count giving NaN centres that
-the keep rule drops), and the host reads the per-band component counts once at the end. A page
-with a band of more components than the capacity is redone by the eager path."""
+the keep rule drops), and the host reads the per-band component counts once at the end. The
+capacity is twice the components of the band the graph was built on; a page with a band of more
+components than that is redone by the eager path (and the graph rebuilt on the next call)."""
 
 from __future__ import annotations
 
@@ -43,13 +44,15 @@ def _dedupe_device(pts_d: torch.Tensor, n: int, eps: float) -> torch.Tensor:
     return out[: dev.read_int(count)]
 
 
-# Component capacity of a captured band: one component per this many pixels (holes at a pitch of
-# 8 px or more fit; denser pages take the eager path).
-BAND_PX_PER_COMPONENT = 64
+# Component capacity of a captured band: twice the components of the band it is built on (at least
+# 1024, at most one per this many pixels); a page with a fuller band takes the eager path and the
+# graph is rebuilt for the next call.
+BAND_PX_PER_COMPONENT = 4
 
 
-def band_capacity(band_h: int, width: int) -> int:
-    return max(1024, band_h * width // BAND_PX_PER_COMPONENT)
+def band_capacity(band_h: int, width: int, components: int | None = None) -> int:
+    most = max(1024, band_h * width // BAND_PX_PER_COMPONENT)
+    return most if components is None else min(most, max(1024, 2 * int(components)))
 
 
 class BandGraph:
@@ -57,25 +60,35 @@ class BandGraph:
 
     def __init__(self, band_h: int, width: int, dtype: torch.dtype, *, fixed_threshold: float, invert: bool,
                  area_min: int, area_max: int, pad: int, refine: str, connectivity: int, small_feature_max: float,
-                 morph_open: int = 0, morph_close: int = 0, capacity: int | None = None):
+                 morph_open: int = 0, morph_close: int = 0, capacity: int | None = None,
+                 sample: torch.Tensor | None = None):
         from .centers import _segmentation_source
 
         self.shape = (int(band_h), int(width))
-        self.capacity = int(capacity) if capacity is not None else band_capacity(band_h, width)
-        h, w, cap = band_h, width, self.capacity
+        h, w = self.shape
         self.src = torch.zeros(self.shape, dtype=dtype, device="cuda")
         self.labels = dev.empty((h, w), torch.int32)
         self.count = torch.zeros(1, dtype=torch.int32, device="cuda")
         self.kept = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.ccl_ws = dev.workspace(_lib.size("spx_ccl_workspace_bytes", h, w))
+        self._seg = _segmentation_source
+        self._seg_args = (float(fixed_threshold), bool(invert), int(morph_open), int(morph_close))
+        if capacity is None and sample is not None:
+            # Size the capacity on a real band: its component count, from the labelling alone.
+            self.src.copy_(sample)
+            src, thr, fixed, inv = self._seg(self.src, None, *self._seg_args)
+            _lib.call("spx_ccl_label", src.data_ptr(), dev.dtype_code(src), h, w, dev.ptr(thr), float(fixed),
+                      int(bool(inv)), int(connectivity), self.labels.data_ptr(), self.count.data_ptr(),
+                      self.ccl_ws.data_ptr(), self.ccl_ws.numel(), dev.stream_ptr())
+            capacity = band_capacity(h, w, dev.read_int(self.count))
+        self.capacity = int(capacity) if capacity is not None else band_capacity(h, w)
+        cap = self.capacity
         self.stats = dev.empty((cap + 1, 5), torch.int32)
         self.centroids = dev.empty((cap + 1, 2), torch.float64)
         self.rows = dev.empty((cap, 5), torch.int32)
         self.methods = dev.empty((cap,), torch.uint8)
         self.centers = dev.empty((cap, 2), torch.float64)
-        self.ccl_ws = dev.workspace(_lib.size("spx_ccl_workspace_bytes", h, w))
         self.sel_ws = dev.workspace(_lib.size("spx_select_workspace_bytes", cap))
-        self._seg = _segmentation_source
-        self._seg_args = (float(fixed_threshold), bool(invert), int(morph_open), int(morph_close))
         self._params = (int(area_min), int(area_max), int(pad), _lib.REFINE_CODES[refine], int(connectivity),
                         float(small_feature_max))
         self.graph = torch.cuda.CUDAGraph()
@@ -131,14 +144,17 @@ def _bands_with_graphs(img_d, spans, pre, common):
     """Every band through a cached BandGraph of its height; None when a band overflows its capacity."""
     width = img_d.shape[1]
     graphs = {}
+    keys = {}
     for y0, y1, _, _ in spans:
         key = (y1 - y0, width, img_d.dtype, float(pre), tuple(sorted(common.items())), torch.cuda.current_device(),
-               band_capacity(y1 - y0, width))
+               BAND_PX_PER_COMPONENT)
         if key not in _GRAPHS:
             if len(_GRAPHS) >= 4:
                 _GRAPHS.clear()
-            _GRAPHS[key] = BandGraph(y1 - y0, width, img_d.dtype, fixed_threshold=pre, **common)
+            _GRAPHS[key] = BandGraph(y1 - y0, width, img_d.dtype, fixed_threshold=pre, sample=img_d[y0:y1],
+                                     **common)
         graphs[(y0, y1)] = _GRAPHS[key]
+        keys[(y0, y1)] = key
     cap_total = sum(graphs[(y0, y1)].capacity for y0, y1, _, _ in spans)
     kept = dev.empty((max(cap_total, 1), 2), torch.float64)
     count = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -150,9 +166,10 @@ def _bands_with_graphs(img_d, spans, pre, common):
         counts[b:b + 1].copy_(g.count)
         _lib.call("spx_keep_band", centers.data_ptr(), g.capacity, float(y0), float(lo), float(hi), kept.data_ptr(),
                   count.data_ptr(), max(cap_total, 1), ws.data_ptr(), ws.numel(), dev.stream_ptr())
-    if any(int(c) > graphs[spans[b][:2]].capacity for b, c in enumerate(counts.cpu().numpy())):
-        return None
-    return kept, count
+    over = [b for b, c in enumerate(counts.cpu().numpy()) if int(c) > graphs[spans[b][:2]].capacity]
+    for b in over:  # rebuilt on the next call, sized on a band of this page
+        _GRAPHS.pop(keys[spans[b][:2]], None)
+    return None if over else (kept, count)
 
 
 def detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, connectivity, small_feature_max,

@@ -131,5 +131,6 @@ def test_band_graph_overflow_takes_the_eager_path(monkeypatch):
     assert len(eager.centers_xy) > 2 * 1024
     monkeypatch.setattr(tiled, "BAND_PX_PER_COMPONENT", 1 << 30)  # capacity 1024 < components per band
     res = tiled.detect_tiled(page, use_graphs=True, **_tiled_kwargs())
+    assert tiled.band_capacity(1024, 1024, 5000) == 1024
     assert not res.meta["band_graphs"]
     np.testing.assert_array_equal(res.centers_xy, eager.centers_xy)
