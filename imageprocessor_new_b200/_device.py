@@ -3,6 +3,7 @@
 from __future__ import annotations
 
 import contextlib
+import warnings
 
 import numpy as np
 import torch
@@ -39,7 +40,13 @@ def upload(a: np.ndarray) -> torch.Tensor:
     a = np.ascontiguousarray(a)
     dtype = TORCH_ALL.get(a.dtype) or torch.from_numpy(np.empty(0, a.dtype)).dtype
     pinned = torch.empty(a.shape, dtype=dtype, pin_memory=True)
-    pinned.numpy()[...] = a
+    if a.nbytes >= 1 << 22:
+        # torch's CPU copy splits a large copy over the host threads; the source is only read.
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", UserWarning)  # read-only arrays: torch warns on wrapping them
+            pinned.copy_(torch.from_numpy(a))
+    else:
+        pinned.numpy()[...] = a
     return pinned.to("cuda", non_blocking=True)
 
 

@@ -112,7 +112,15 @@ __device__ __forceinline__ void warp_allreduce27(double* s, int lane, double* sl
             a[j] = keep + __shfl_xor_sync(0xffffffffu, send, half);
         }
     }
-    if (slot && lane < 27) slot[lane] = a[0];
+    if (slot) {
+        // Broadcast through the shared-memory slot: 27 uniform loads instead of 27 shuffles of
+        // two halves each.
+        if (lane < 27) slot[lane] = a[0];
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < 27; ++i) s[i] = slot[i];
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < 27; ++i) s[i] = __shfl_sync(0xffffffffu, a[0], i);
 }
