@@ -516,19 +516,21 @@ struct TileSel {
     const unsigned int* d2;   // distance map (free mode)
     const uint8_t* usable;    // null: all usable
     int mode;                 // SPX_TILE_FREE: model < thr_model & dist >= thr_dist; SPX_TILE_USABLE; SPX_TILE_ALL
-    double thr_model, thr_dist;
+    double thr_model;
+    unsigned long long d2_min;  // sqrt((double)d2) >= thr_dist  <=>  d2 >= d2_min (set by the host)
+    // The pixel's residual and whether the tile's median takes it. Every load is issued whatever
+    // the tests give (the branches are uniform over the launch), so a thread's loads of several
+    // pixels overlap.
     __device__ __forceinline__ bool select(int y, int x, double* value) const {
         const long long i = (long long)y * img.W + x;
         const double m = model ? model[i] : 0.0;
+        bool ok = true;
         if (mode != SPX_TILE_ALL) {
-            if (usable && !usable[i]) return false;
-            if (mode == SPX_TILE_FREE) {
-                if (!(m < thr_model)) return false;
-                if (!(sqrt((double)d2[i]) >= thr_dist)) return false;
-            }
+            if (usable) ok = usable[i] != 0;
+            if (mode == SPX_TILE_FREE) ok = ok && m < thr_model && (unsigned long long)d2[i] >= d2_min;
         }
         *value = img.at(y, x) - m;
-        return true;
+        return ok;
     }
 };
 
@@ -604,14 +606,28 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int t
     const long long P = (long long)th * tw;
     if (threadIdx.x == 0) s_count = 0;
     __syncthreads();
-    // Pass 0: count and (when they fit) stage the keys.
-    for (int k = threadIdx.x; k < (int)P; k += blockDim.x) {
-        const int yy = k / tw, xx = k - yy * tw;
-        double v;
-        if (sel.select(y0 + yy, x0 + xx, &v)) {
-            const int slot = atomicAdd(&s_count, 1);
-            if (slot < smem_keys) keys[slot] = order_key(v);
+    // Pass 0: count and (when they fit) stage the keys, kPass0 pixels per thread at a time so
+    // that their loads are in flight together.
+    constexpr int kPass0 = 8;
+    for (int k0 = 0; k0 < (int)P; k0 += kPass0 * blockDim.x) {
+        double v[kPass0];
+        bool take[kPass0];
+#pragma unroll
+        for (int u = 0; u < kPass0; ++u) {
+            const int k = k0 + u * blockDim.x + threadIdx.x;
+            take[u] = false;
+            v[u] = 0.0;
+            if (k < (int)P) {
+                const int yy = k / tw, xx = k - yy * tw;
+                take[u] = sel.select(y0 + yy, x0 + xx, &v[u]);
+            }
         }
+#pragma unroll
+        for (int u = 0; u < kPass0; ++u)
+            if (take[u]) {
+                const int slot = atomicAdd(&s_count, 1);
+                if (slot < smem_keys) keys[slot] = order_key(v[u]);
+            }
     }
     __syncthreads();
     const int c = s_count;
@@ -1164,7 +1180,19 @@ int spx_tile_medians(const void* img, int dtype, double sign, int height, int wi
     const int smem_keys = (int)(t2 < kTileSmemKeys ? t2 : kTileSmemKeys);
     const size_t smem = (size_t)smem_keys * sizeof(unsigned long long);
     SPX_CUDA(cudaFuncSetAttribute(k_tile_median, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TileSel sel{Image{img, dtype, sign, height, width}, model, dist2, usable, mode, thr_model, thr_dist};
+    // Smallest integer squared distance whose square root reaches thr_dist (sqrt is correctly
+    // rounded here and on the device, and monotonic), so the kernel compares integers.
+    unsigned long long d2_min = 0;
+    if (thr_dist != thr_dist) {
+        d2_min = 1ull << 33;  // NaN: no distance passes
+    } else if (thr_dist > 0.0) {
+        const double t2 = ceil(thr_dist * thr_dist);
+        unsigned long long d = t2 > 8.0e9 ? (1ull << 33) : (unsigned long long)t2;
+        while (d > 0 && sqrt((double)(d - 1)) >= thr_dist) --d;
+        while (d < (1ull << 33) && !(sqrt((double)d) >= thr_dist)) ++d;
+        d2_min = d;
+    }
+    TileSel sel{Image{img, dtype, sign, height, width}, model, dist2, usable, mode, thr_model, d2_min};
     k_tile_median<<<ny * nx, kTileThreads, smem, s>>>(sel, tile, nx, smem_keys, medians, counts);
     return check_launch("k_tile_median");
 }
