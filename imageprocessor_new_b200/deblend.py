@@ -72,12 +72,14 @@ def build_cells(rows, shape, pad: int, rows_d: torch.Tensor | None = None) -> Ce
     caps = dev.empty((max(n, 1),), torch.float64)
     _lib.call("spx_cells_setup", _ptr(rows_d) if n else None, n, int(pad), h, w, vor.data_ptr(), boxes.data_ptr(),
               counts.data_ptr(), caps.data_ptr(), dev.stream_ptr())
-    host = boxes[:n].cpu().numpy()
+    host = dev.start_download(boxes[:n])
+    host_counts = dev.start_download(counts[:n])
+    torch.cuda.current_stream().synchronize()
     rows = np.asarray(rows, dtype=np.float64).reshape(-1, 6)
     seeds = np.ascontiguousarray(rows[:, 4:6])
     hm = int(host[:, 3].max()) if n else 0
     wm = int(host[:, 2].max()) if n else 0
-    max_px = int(counts[:n].max().item()) if n else 1
+    max_px = int(host_counts.max()) if n else 1
     return Cells(rows, seeds, seeds_d, vor, boxes[:n], counts[:n], caps[:n], host[:, :2].astype(np.int32),
                  host[:, 2:4].astype(np.int32), hm, wm, max(max_px, 1))
 
@@ -146,29 +148,44 @@ _INTERPOLATORS: dict = {}
 def interpolate_tiles(free_med, measured, tile, shape):
     """Unmeasured tiles from the measured ones: linear over their Delaunay triangulation, the
     nearest measured tile outside it (subpx/_cpu/deblend.py:359-385)."""
-    from scipy.interpolate import LinearNDInterpolator
     from scipy.spatial import Delaunay, cKDTree
 
-    yc, xc = tile_centers(tile, shape)
-    grid = np.stack(np.meshgrid(yc, xc, indexing="ij"), axis=-1)
-    known, values = grid[measured], free_med[measured]
-    key = (tuple(shape), tile, measured.tobytes())
+    key = (tuple(shape), tile, measured.shape, measured.tobytes())
     if key not in _INTERPOLATORS:
+        yc, xc = tile_centers(tile, shape)
+        grid = np.stack(np.meshgrid(yc, xc, indexing="ij"), axis=-1)
+        known, query = grid[measured], grid[~measured]
         try:
-            tri = Delaunay(known) if len(values) >= 3 else None
+            tri = Delaunay(known) if len(known) >= 3 else None
         except Exception:  # collinear measured tiles
             tri = None
+        # LinearNDInterpolator's barycentric weights of the unmeasured tile centres, kept for the
+        # next calls with the same measured tiles (only the values change between deblending
+        # iterations); evaluated below with its arithmetic, so the results are the same bits.
+        bary = None
+        if tri is not None:
+            simplex = tri.find_simplex(query)
+            inside = simplex >= 0
+            t = tri.transform[simplex[inside]]
+            d = query[inside] - t[:, 2]
+            c0 = t[:, 0, 0] * d[:, 0] + t[:, 0, 1] * d[:, 1]
+            c1 = t[:, 1, 0] * d[:, 0] + t[:, 1, 1] * d[:, 1]
+            bary = (inside, tri.simplices[simplex[inside]], c0, c1, 1.0 - c0 - c1)
         if len(_INTERPOLATORS) >= 32:
             _INTERPOLATORS.clear()
-        _INTERPOLATORS[key] = (tri, cKDTree(known))
-    tri, tree = _INTERPOLATORS[key]
+        _INTERPOLATORS[key] = (bary, cKDTree(known), query)
+    bary, tree, query = _INTERPOLATORS[key]
+    values = free_med[measured]
     medians = free_med.copy()
     missing = ~measured
-    medians[missing] = np.nan
-    if tri is not None:
-        medians[missing] = LinearNDInterpolator(tri, values)(grid[missing])
-    still = missing & np.isnan(medians)
-    medians[still] = values[tree.query(grid[still])[1]]
+    interp = np.full(len(query), np.nan)
+    if bary is not None:
+        inside, vert, c0, c1, c2 = bary
+        interp[inside] = values[vert[:, 0]] * c0 + values[vert[:, 1]] * c1 + values[vert[:, 2]] * c2
+    still = np.isnan(interp)
+    if still.any():
+        interp[still] = values[tree.query(query[still])[1]]
+    medians[missing] = interp
     return medians
 
 
