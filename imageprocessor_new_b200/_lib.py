@@ -96,6 +96,8 @@ SIGNATURES = {
     "spx_select_workspace_bytes": (_S, [_I]),
     "spx_select_components": (_I, [_P, _I, _I, _I, _I, _D, _P, _P, _P, _P, _S, _P]),
     "spx_component_rows": (_I, [_P, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _S, _P]),
+    "spx_status_name": (ctypes.c_char_p, [_I]),
+    "spx_status_text": (_I, [_P, _I, _P, _P]),
     "spx_refine_centers_counted": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _I, _I, _P, _P]),
     "spx_refine_centers": (_I, [_P, _I, _I, _I, _P, _P, _P, _I, _I, _P, _P]),
     "spx_keep_band_workspace_bytes": (_S, [_I]),

@@ -213,6 +213,7 @@ def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
         "eigenvalues": (m, 2) if method in ("logquad", "gaussian") else None,
         "axes": (m, 2, 2) if method in ("logquad", "gaussian") else None,
         "status": ((m + 7) // 8,),  # bytes, viewed as uint8
+        "status_text": (m * 16,),   # 32 UCS-4 code points per cell, viewed on the host as "<U32"
     }
     offsets, total = {}, 0
     for key, shape in shapes.items():
@@ -264,7 +265,9 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
     shape = shapes["metrics"]
     m = host[offsets["metrics"]:offsets["metrics"] + int(np.prod(shape))].reshape(shape)
     codes = host[offsets["status"]:].view(np.uint8)[:n]
-    status = STATUS[codes]
+    # spx_status_text wrote the names on the device; the host only views them.
+    status = host[offsets["status_text"]:offsets["status_text"] + shapes["status_text"][0]].view(
+        np.dtype("<U32"))[:n]
     metrics = {name: m[k, :n] for k, name in enumerate(names)}
     if shapes["contours"] is not None:
         contours = part("contours")
@@ -465,6 +468,9 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
     def launched(names):
         # Each method's results go to pinned host memory on a side stream as soon as its kernel is
         # done, so the host converts one method while the GPU still runs the next.
+        for name in names:
+            b = bufs[name]
+            _lib.call("spx_status_text", b["status"].data_ptr(), nr, b["status_text"].data_ptr(), stream)
         ev = torch.cuda.Event()
         ev.record(main)
         pending.append((names, [_start_download(bufs[name], ev) for name in names]))

@@ -926,6 +926,29 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     }
 }
 
+// The status names, as the reference's result arrays spell them (numpy "U32": 32 UCS-4 code
+// points per entry, zero-padded).
+#define SPX_STATUS_NAMES(X)                                                                            \
+    X("ok") X("no_signal") X("insufficient_cell_pixels") X("insufficient_fit_pixels") X("singular_fit") \
+        X("non_gaussian_fit") X("contour_outside_cell") X("incomplete_rays") X("fit_diverged")         \
+            X("center_outside_cell")
+#define SPX_NAME_ENTRY(s) s,
+constexpr int kStatusCount = 10;
+constexpr int kStatusChars = 32;
+__constant__ char c_status_names[kStatusCount][kStatusChars] = {SPX_STATUS_NAMES(SPX_NAME_ENTRY)};
+const char* const kStatusNamesHost[kStatusCount] = {SPX_STATUS_NAMES(SPX_NAME_ENTRY)};
+
+// One thread per (cell, character): the UCS-4 text of each cell's status code.
+__global__ void k_status_text(const uint8_t* codes, int n, uint32_t* out) {
+    const long long total = (long long)n * kStatusChars;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / kStatusChars), c = (int)(t % kStatusChars);
+        const int code = codes[i];
+        out[t] = code < kStatusCount ? (uint32_t)(unsigned char)c_status_names[code][c] : 0u;
+    }
+}
+
 MethodOut method_out(const spx_method_out* o) {
     MethodOut m;
     if (!o) {
@@ -965,6 +988,17 @@ int spx_gaussian_method(const double* params, const uint8_t* status_in, const do
                                                               reinterpret_cast<const int4*>(boxes), which, n, hm,
                                                               wm, width, n_angles, method_out(out));
     return check_launch("k_gaussian_method");
+}
+
+const char* spx_status_name(int code) { return code >= 0 && code < kStatusCount ? kStatusNamesHost[code] : nullptr; }
+
+int spx_status_text(const uint8_t* codes, int n, uint32_t* text, void* stream) {
+    SPX_REQUIRE(n >= 0, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(codes && text, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_status_text<<<grid_for((long long)n * kStatusChars, 256), 256, 0, s>>>(codes, n, text);
+    return check_launch("k_status_text");
 }
 
 int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, const double* seeds,

@@ -374,6 +374,13 @@ typedef struct spx_method_out {
     long long metric_col_stride;  /* 0: row-major; else metric q of cell i at metrics[i + q * stride] */
 } spx_method_out;
 
+/* Status text of per-cell result codes as the reference's "U32" string arrays hold it: 32 UCS-4
+ * code points per cell (text: n x 32 uint32), zero-padded, so a host copy can be viewed as a
+ * NumPy "<U32" array. spx_status_name(code) is the same name as a C string (null for an unknown
+ * code). No reference counterpart (the reference builds its string arrays on the host). */
+const char* spx_status_name(int code);
+int spx_status_text(const uint8_t* codes, int n, uint32_t* text, void* stream);
+
 /* Half-maximum ellipses of the deblended Gaussian fits (params of cells `which`, ROI-local). */
 int spx_gaussian_method(const double* params, const uint8_t* status_in, const double* cleaned, const int* voronoi,
                         const int* boxes, const int* which, int n, int hm, int wm, int width, int n_angles,

@@ -57,3 +57,13 @@ def test_fit_options_are_checked_before_any_device_work():
                                        None, None, None, None, opts, None, 0, None)
         assert rc != 0
         assert b"fit" in lib.spx_last_error()
+
+
+def test_status_names_match_the_binding():
+    """The library's status names (also written as UCS-4 text on the device) are the binding's."""
+    from imageprocessor_new_b200 import _lib
+
+    lib = _lib.load_library()
+    assert [lib.spx_status_name(i).decode() for i in range(len(_lib.STATUS_NAMES))] == list(_lib.STATUS_NAMES)
+    assert lib.spx_status_name(len(_lib.STATUS_NAMES)) is None
+    assert max(len(n) for n in _lib.STATUS_NAMES) < 32
