@@ -76,12 +76,13 @@ def build_cells(rows, shape, pad: int, rows_d: torch.Tensor | None = None) -> Ce
     host_counts = dev.start_download(counts[:n])
     torch.cuda.current_stream().synchronize()
     rows = np.asarray(rows, dtype=np.float64).reshape(-1, 6)
-    seeds = np.ascontiguousarray(rows[:, 4:6])
     hm = int(host[:, 3].max()) if n else 0
     wm = int(host[:, 2].max()) if n else 0
     max_px = int(host_counts.max()) if n else 1
-    return Cells(rows, seeds, seeds_d, vor, boxes[:n], counts[:n], caps[:n], host[:, :2].astype(np.int32),
-                 host[:, 2:4].astype(np.int32), hm, wm, max(max_px, 1))
+    # Seeds, origins and sizes are views of the downloaded arrays (new host arrays of this size
+    # cost more in first-touch page faults than the copies themselves).
+    return Cells(rows, rows[:, 4:6], seeds_d, vor, boxes[:n], counts[:n], caps[:n], host[:, :2], host[:, 2:4], hm,
+                 wm, max(max_px, 1))
 
 
 def auto_tile(seeds_d: torch.Tensor, n: int, shape) -> tuple[int, float]:
