@@ -326,13 +326,14 @@ def _revise_seeds(dbl: Deblender, state, seeds_xy, pitch, oversized_d, *, drop_f
     order = np.lexsort((yx[:, 1], yx[:, 0]))  # np.nonzero order: row-major
     yx = yx[order]
     new = np.column_stack((yx[:, 1], yx[:, 0])).astype(float)
-    kept = np.asarray(seeds_xy, float)[~drop]
-    if len(new) and len(kept):
-        kd = dev.upload(np.ascontiguousarray(kept))
+    n_kept = int(len(drop) - np.count_nonzero(drop))
+    if len(new) and n_kept:
+        # The kept seeds selected on the device from the cells' seeds (the same values as seeds_xy).
+        kd = dbl.cells.seeds_d[dev.upload((~drop).view(np.uint8)).bool()]
         qd = dev.upload(np.ascontiguousarray(new))
         dist = dev.empty((len(new),), torch.float64)
-        ws = dev.workspace(_lib.size("spx_voronoi_workspace_bytes", len(kept), h, w))
-        _lib.call("spx_nearest_distances", kd.data_ptr(), len(kept), qd.data_ptr(), len(new), 0, h, w,
+        ws = dev.workspace(_lib.size("spx_voronoi_workspace_bytes", n_kept, h, w))
+        _lib.call("spx_nearest_distances", kd.data_ptr(), n_kept, qd.data_ptr(), len(new), 0, h, w,
                   dist.data_ptr(), ws.data_ptr(), ws.numel(), dev.stream_ptr())
         new = new[dist.cpu().numpy() > 0.5 * pitch]
     return drop, new

@@ -481,7 +481,10 @@ class Deblender:
                 break
         bg, info = self.background_of(model, stats)
         self.check_render()
-        return DeblendState(bg, model, params_d.cpu().numpy(), params_d, status_d.cpu().numpy(), status_d, self.tile,
+        # Host copies through pinned memory (cached blocks, no fresh pageable arrays to fault in).
+        params_h, status_h = dev.start_download(params_d), dev.start_download(status_d)
+        torch.cuda.current_stream().synchronize()
+        return DeblendState(bg, model, params_h, params_d, status_h, status_d, self.tile,
                             used, info, converged, fit_iters, stats[0] if stats[4] else float("nan"))
 
     def check_render(self):
