@@ -585,22 +585,21 @@ __device__ void refine_edge(const void* img, int dtype, const int* labels, int W
             }
         }
         __syncwarp();
-        int ok = 1;
-        double e[4] = {0, 0, 0, 0};
-        if (lane == 0) {
-            const int bases[4] = {xL0 - edge_rad, xR0 - edge_rad, yT0 - edge_rad, yB0 - edge_rad};
-            for (int s = 0; s < 4; ++s) {
-                double p[32];
-                for (int i = 0; i < n; ++i) p[i] = prof_sh[s * 32 + i];
-                smooth_binom5(p, n);
-                smooth_binom5(p, n);
-                if (!edge_from_profile(p, n, (double)bases[s], &e[s])) ok = 0;
-            }
+        // Lane s < 4 smooths profile s and finds its edge.
+        int ok_s = 1;
+        double e_s = 0.0;
+        if (lane < 4) {
+            const int base = lane == 0 ? xL0 : lane == 1 ? xR0 : lane == 2 ? yT0 : yB0;
+            double p[32];
+            for (int i = 0; i < n; ++i) p[i] = prof_sh[lane * 32 + i];
+            smooth_binom5(p, n);
+            smooth_binom5(p, n);
+            ok_s = edge_from_profile(p, n, (double)(base - edge_rad), &e_s);
         }
         __syncwarp();
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (!ok) return;
-        for (int s = 0; s < 4; ++s) e[s] = __shfl_sync(0xffffffffu, e[s], 0);
+        if (__ballot_sync(0xffffffffu, lane < 4 && !ok_s)) return;
+        double e[4];
+        for (int s = 0; s < 4; ++s) e[s] = __shfl_sync(0xffffffffu, e_s, s);
         xc = __dmul_rn(0.5, __dadd_rn(e[0], e[1]));
         yc = __dmul_rn(0.5, __dadd_rn(e[2], e[3]));
     }
@@ -609,6 +608,10 @@ __device__ void refine_edge(const void* img, int dtype, const int* labels, int W
     *cy = yc;
 }
 
+// One kernel per refiner M (each sized by its own register needs): it takes the rows whose
+// method is M; the SPX_REFINE_NONE kernel also takes every other code and the rows past a device
+// count (NaN).
+template <int M>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 k_refine(const void* img, int dtype, int H, int W, const int* labels, const int* rows,
          const uint8_t* methods, int n, const int* n_dev, int pad, double* centers) {
@@ -617,18 +620,22 @@ k_refine(const void* img, int dtype, int H, int W, const int* labels, const int*
     const int live = n_dev ? min(*n_dev, n) : n;  // rows past a device count are outputs of NaN
     for (int blob = blockIdx.x * kWarpsPerBlock + warp; blob < n; blob += gridDim.x * kWarpsPerBlock) {
         if (blob >= live) {
-            if (lane == 0) centers[2LL * blob] = centers[2LL * blob + 1] = dnan();
+            if (M == SPX_REFINE_NONE && lane == 0) centers[2LL * blob] = centers[2LL * blob + 1] = dnan();
             continue;
         }
-        const Roi r = make_roi(rows + (long long)blob * 5, pad, H, W);
         const int m = methods[blob];
+        const bool mine = M == SPX_REFINE_NONE
+                              ? (m != SPX_REFINE_WEIGHTED && m != SPX_REFINE_LOGQUAD && m != SPX_REFINE_EDGE)
+                              : m == M;
+        if (!mine) continue;
+        const Roi r = make_roi(rows + (long long)blob * 5, pad, H, W);
         double cx = dnan(), cy = dnan();
         if (r.w > 0 && r.h > 0) {
-            if (m == SPX_REFINE_WEIGHTED) {
+            if constexpr (M == SPX_REFINE_WEIGHTED) {
                 refine_weighted(img, dtype, labels, W, r, keys[warp], lane, &cx, &cy);
-            } else if (m == SPX_REFINE_LOGQUAD) {
+            } else if constexpr (M == SPX_REFINE_LOGQUAD) {
                 refine_logquad(img, dtype, labels, W, r, keys[warp], lane, &cx, &cy);
-            } else if (m == SPX_REFINE_EDGE) {
+            } else if constexpr (M == SPX_REFINE_EDGE) {
                 refine_edge(img, dtype, labels, W, r, keys[warp], lane, &cx, &cy);
             } else {
                 const MaskSums ms = mask_sums(labels, W, r, lane);
@@ -644,6 +651,23 @@ k_refine(const void* img, int dtype, int H, int W, const int* labels, const int*
         }
         __syncwarp();
     }
+}
+
+int launch_refine(const void* img, int dtype, int H, int W, const int* labels, const int* rows, const uint8_t* methods,
+                  int n, const int* n_dev, int pad, double* centers, int blocks, cudaStream_t s) {
+    const int grid = blocks < 148 * 16 ? blocks : 148 * 16;
+    k_refine<SPX_REFINE_WEIGHTED><<<grid, kWarpsPerBlock * 32, 0, s>>>(img, dtype, H, W, labels, rows, methods, n,
+                                                                        n_dev, pad, centers);
+    if (int e = check_launch("k_refine")) return e;
+    k_refine<SPX_REFINE_LOGQUAD><<<grid, kWarpsPerBlock * 32, 0, s>>>(img, dtype, H, W, labels, rows, methods, n,
+                                                                       n_dev, pad, centers);
+    if (int e = check_launch("k_refine")) return e;
+    k_refine<SPX_REFINE_EDGE><<<grid, kWarpsPerBlock * 32, 0, s>>>(img, dtype, H, W, labels, rows, methods, n, n_dev,
+                                                                    pad, centers);
+    if (int e = check_launch("k_refine")) return e;
+    k_refine<SPX_REFINE_NONE><<<grid, kWarpsPerBlock * 32, 0, s>>>(img, dtype, H, W, labels, rows, methods, n, n_dev,
+                                                                    pad, centers);
+    return check_launch("k_refine");
 }
 
 }  // namespace
@@ -721,9 +745,7 @@ int spx_refine_centers(const void* img, int dtype, int height, int width, const 
     SPX_REQUIRE(dtype >= SPX_U8 && dtype <= SPX_F64, "bad dtype");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    k_refine<<<blocks < 148 * 16 ? blocks : 148 * 16, kWarpsPerBlock * 32, 0, s>>>(
-        img, dtype, height, width, labels, rows, methods, n, nullptr, pad, centers_out);
-    return check_launch("k_refine");
+    return launch_refine(img, dtype, height, width, labels, rows, methods, n, nullptr, pad, centers_out, blocks, s);
 }
 
 int spx_refine_centers_counted(const void* img, int dtype, int height, int width, const int* labels,
@@ -735,9 +757,8 @@ int spx_refine_centers_counted(const void* img, int dtype, int height, int width
     SPX_REQUIRE(dtype >= SPX_U8 && dtype <= SPX_F64, "bad dtype");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int blocks = (capacity + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    k_refine<<<blocks < 148 * 16 ? blocks : 148 * 16, kWarpsPerBlock * 32, 0, s>>>(
-        img, dtype, height, width, labels, rows, methods, capacity, n_dev, pad, centers_out);
-    return check_launch("k_refine");
+    return launch_refine(img, dtype, height, width, labels, rows, methods, capacity, n_dev, pad, centers_out, blocks,
+                         s);
 }
 
 }  // extern "C"
