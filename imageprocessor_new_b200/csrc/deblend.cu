@@ -757,14 +757,15 @@ struct QuantileReq {
 };
 
 __device__ __forceinline__ bool q_select(const QuantileReq& r, int i, double* v) {
-    if (r.mask && !r.mask[i]) return false;
+    // Both loads are issued whatever the mask says, so a thread's loads of several values overlap.
+    const bool in = !r.mask || r.mask[i];
     const double x = r.values[(long long)i * r.stride];
-    if (r.finite_only && !isfinite(x)) return false;
     *v = x;
-    return true;
+    return in && !(r.finite_only && !isfinite(x));
 }
 
 constexpr int kQuantThreads = 1024;
+constexpr int kQuantAhead = 4;
 
 // Order key of the k-th smallest selected value (0-based): a radix select over 64-bit keys with
 // 11-bit digits (six passes over the values), each digit found by a CTA-wide prefix sum.
@@ -776,11 +777,21 @@ __device__ unsigned long long cta_kth_key(const QuantileReq& r, int k, int* hist
         shift -= bits;
         for (int i = threadIdx.x; i < nb; i += kQuantThreads) hist[i] = 0;
         __syncthreads();
-        for (int i = threadIdx.x; i < r.n; i += kQuantThreads) {
-            double v;
-            if (!q_select(r, i, &v)) continue;
-            const unsigned long long key = order_key(v);
-            if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
+        // kQuantAhead values per thread loaded before their histogram updates, so the loads overlap.
+        for (int i0 = threadIdx.x; i0 < r.n; i0 += kQuantAhead * kQuantThreads) {
+            double v[kQuantAhead];
+            bool ok[kQuantAhead];
+#pragma unroll
+            for (int u = 0; u < kQuantAhead; ++u) {
+                const int i = i0 + u * kQuantThreads;
+                ok[u] = i < r.n && q_select(r, i, &v[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < kQuantAhead; ++u) {
+                if (!ok[u]) continue;
+                const unsigned long long key = order_key(v[u]);
+                if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
+            }
         }
         __syncthreads();
         cta_pick_digit<kQuantThreads>(hist, nb, kk, warp_tot, s_pick);
