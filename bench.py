@@ -49,6 +49,7 @@ CENTER_KW = dict(threshold="otsu", area_max=400)
 # DRAM bytes (read + write) per cell of one k_fit_iteration launch, from an ncu capture of one
 # launch on the 4096x4096 page (29,241 cells, 195.0 MB); traffic scales with the cells processed.
 FIT_TRAFFIC_PER_CELL = 6512.0
+FIT_FP64_PIPE_ACTIVE = 0.507
 
 
 def _dist():
@@ -260,7 +261,10 @@ def gpu_arm(args):
                      "peak": peaks.get("hbm_gbs"), "peak_source": which, "unit": "GB/s",
                      "frac": None if achieved is None else round(achieved / peaks["hbm_gbs"], 4),
                      "traffic": round(FIT_TRAFFIC_PER_CELL * fit_n / 1e9, 4), "traffic_unit": "GB per launch",
-                     "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n},
+                     "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n,
+                     # The kernel's arithmetic is FP64 (not a contraction, not HBM-bound): the FP64
+                     # pipe's busy fraction from the committed ncu capture of the same kernel.
+                     "fp64_pipe_active": FIT_FP64_PIPE_ACTIVE, "fp64_source": "profiles/k_fit_iteration_page4096.md"},
         "gpu_launches": int(launches),
         "clocks": clock_summary,
     }
