@@ -47,7 +47,7 @@ REFINERS = ("weighted", "logquad", "edge_gradmoment")
 CD_KW = dict(area_max=400, summary_only=True)
 CENTER_KW = dict(threshold="otsu", area_max=400)
 # DRAM bytes (read + write) per cell of one k_fit_iteration launch, from an ncu capture of one
-# launch on the 4096x4096 page (29,241 cells, 195.0 MB); traffic scales with the cells processed.
+# launch on the 4096x4096 page (29,241 cells, 190.4 MB); traffic scales with the cells processed.
 FIT_TRAFFIC_PER_CELL = 6512.0
 FIT_FP64_PIPE_ACTIVE = 0.507
 
