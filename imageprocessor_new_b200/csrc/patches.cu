@@ -20,7 +20,10 @@ namespace spx {
 namespace {
 
 constexpr int kPatch = 32;
-__global__ void k_extract_patches(const void* img, int dtype, double sign, int H, int W, const double* seeds, int n,
+// Templated on the pixel type so that a lane's 32 loads are straight-line code, all in flight at
+// once (a dtype switch per load can put each load behind its own branch).
+template <typename Px>
+__global__ void k_extract_patches(const Px* img, double sign, int H, int W, const double* seeds, int n,
                                   __nv_bfloat16* out, double* norm) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -32,7 +35,7 @@ __global__ void k_extract_patches(const void* img, int dtype, double sign, int H
 #pragma unroll
         for (int r = 0; r < kPatch; ++r) {
             const int y = min(max(oy + r, 0), H - 1);
-            col[r] = sign * load_px(img, dtype, (long long)y * W + x);
+            col[r] = sign * (double)img[(long long)y * W + x];
             mx = fmax(mx, col[r]);
         }
         mx = warp_max(mx);
@@ -128,8 +131,25 @@ int spx_extract_patches(const void* img, int dtype, double sign, int height, int
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && seeds && out && norm, "null pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    k_extract_patches<<<grid_for(n, 8, 148 * 32), 256, 0, s>>>(img, dtype, sign, height, width, seeds, n,
-                                                               static_cast<__nv_bfloat16*>(out), norm);
+    const int grid = grid_for(n, 8, 148 * 32);
+    auto* o = static_cast<__nv_bfloat16*>(out);
+    switch (dtype) {
+        case SPX_U8:
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const uint8_t*>(img), sign, height, width, seeds, n, o,
+                                                   norm);
+            break;
+        case SPX_U16:
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const uint16_t*>(img), sign, height, width, seeds, n,
+                                                   o, norm);
+            break;
+        case SPX_F32:
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const float*>(img), sign, height, width, seeds, n, o,
+                                                   norm);
+            break;
+        default:
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const double*>(img), sign, height, width, seeds, n,
+                                                   o, norm);
+    }
     return check_launch("k_extract_patches");
 }
 

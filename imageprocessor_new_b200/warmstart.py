@@ -233,12 +233,17 @@ def patches(image_d: torch.Tensor, sign: float, seeds_d: torch.Tensor, n: int):
 
 
 def predict_init(net: WarmStartNet, image_d: torch.Tensor, sign: float, seeds_d: torch.Tensor, boxes_d: torch.Tensor,
-                 n: int, batch: int = 32768):
-    """ROI-local LM starting params (n, 6) f64 and validity flags for the cells, on the device."""
+                 n: int, batch: int | None = None):
+    """ROI-local LM starting params (n, 6) f64 and validity flags for the cells, on the device.
+    All cells go through each layer in one GEMM launch unless `batch` bounds the rows per launch
+    (the activations take 1 KB per row); a row's outputs do not depend on the batching."""
     x, norm = patches(image_d, sign, seeds_d, n)
-    y = dev.empty((max(n, 1), OUT), torch.float32)
-    for b0 in range(0, n, batch):
-        y[b0:b0 + batch] = net.forward(x[b0:b0 + batch])
+    if n and (batch is None or batch >= n):
+        y = net.forward(x)
+    else:
+        y = dev.empty((max(n, 1), OUT), torch.float32)
+        for b0 in range(0, n, batch or 1):
+            y[b0:b0 + batch] = net.forward(x[b0:b0 + batch])
     params = dev.empty((max(n, 1), 6), torch.float64)
     ok = dev.empty((max(n, 1),), torch.uint8)
     _lib.call("spx_mlp_outputs_to_params", y.data_ptr(), net.mean_d.data_ptr(), net.std_d.data_ptr(),

@@ -100,22 +100,25 @@ def test_adamw_matches_oracle():
     assert torch.equal(out_t[:, :rows], w.t().to(torch.bfloat16))
 
 
-def test_patches_match_numpy():
+@pytest.mark.parametrize("dtype,sign", [(np.uint16, 1.0), (np.uint8, 1.0), (np.float32, -1.0), (np.float64, 1.0)])
+def test_patches_match_numpy(dtype, sign):
     import torch
 
     from imageprocessor_new_b200 import synthetic
     from imageprocessor_new_b200.warmstart import patches
 
     page = synthetic.page_square(2).image[:300, :400]
+    if dtype == np.uint8:
+        page = page >> 8
+    page = np.ascontiguousarray(page.astype(dtype))
     seeds = np.array([[200.3, 150.7], [3.0, 4.4], [398.6, 299.2], [15.5, 16.5]])
-    x, norm = patches(torch.from_numpy(np.ascontiguousarray(page)).cuda(), 1.0,
-                      torch.from_numpy(seeds).cuda(), len(seeds))
+    x, norm = patches(torch.from_numpy(page).cuda(), sign, torch.from_numpy(seeds).cuda(), len(seeds))
     x, norm = x.float().cpu().numpy(), norm.cpu().numpy()
     for i, (sx, sy) in enumerate(seeds):
         ox, oy = int(np.rint(sx)) - 16, int(np.rint(sy)) - 16
         ys = np.clip(np.arange(oy, oy + 32), 0, page.shape[0] - 1)
         xs = np.clip(np.arange(ox, ox + 32), 0, page.shape[1] - 1)
-        p = page[np.ix_(ys, xs)].astype(np.float64)
+        p = sign * page[np.ix_(ys, xs)].astype(np.float64)
         blocks = p.reshape(16, 2, 16, 2).sum(axis=(1, 3))
         border = np.concatenate([blocks[0], blocks[-1], blocks[1:-1, 0], blocks[1:-1, -1]])
         bg = border.min() / 4.0
@@ -140,3 +143,20 @@ def test_trained_network_gains_over_the_plain_start():
     assert r["warm_iterations_mean"] < r["plain_iterations_mean"]
     assert r["fallback_fraction"] < 0.2
     assert r["within_1e-3_px"] >= 0.99
+
+
+def test_predict_init_does_not_depend_on_batching():
+    """One GEMM launch per layer over all cells gives the same bits as row batches (a row's outputs
+    depend only on its own patch)."""
+    import torch
+
+    from imageprocessor_new_b200 import warmstart as ws
+
+    page, _ = ws.synth_page(3, 1024)
+    cells = ws.page_cells(page)
+    net = ws.WarmStartNet(seed=2)
+    whole = ws.predict_init(net, page, 1.0, cells.seeds_d, cells.boxes, cells.n)
+    parts = ws.predict_init(net, page, 1.0, cells.seeds_d, cells.boxes, cells.n, batch=300)
+    net.check_errors()
+    for a, b in zip(whole, parts):
+        assert torch.equal(a, b)
