@@ -125,6 +125,182 @@ __device__ int stage_cell(int4 box, int j, const int* vor, int W, T* v, int* xy,
     return base;
 }
 
+// ------------------------------------------------------------------- narrow boxes (<= 32 columns)
+
+// A box at most 32 columns wide and kMaskRowsMax rows high keeps one 32-bit in-cell mask per box
+// row (bit xx of row yy: vor(box.y + yy, box.x + xx) == j) in the warp's LM slots, which are free
+// before its fit. The border test and the staging then read the Voronoi labels once, lane xx
+// handling column xx, with four rows' loads in flight together and the pixel loads typed (no dtype
+// branch per load). Border values and staged pixels come out in the same row-major order as the
+// general path's, so the staged cell, and with it the fit, is the same.
+constexpr int kMaskRowsMax = 2 * 54;
+
+__device__ __forceinline__ void cell_row_masks(const int* vor, int W, int4 box, int j, uint32_t* rowm, int lane) {
+    for (int y0 = 0; y0 < box.w; y0 += 4) {
+        int lab[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int yy = y0 + u;
+            lab[u] = (yy < box.w && lane < box.z) ? vor[(long long)(box.y + yy) * W + (box.x + lane)] : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t m = __ballot_sync(0xffffffffu, lab[u] == j);
+            if (lane == 0 && y0 + u < box.w) rowm[y0 + u] = m;
+        }
+    }
+    __syncwarp();
+}
+
+// Image::at for a known pixel type.
+template <typename Px>
+__device__ __forceinline__ double px_at(const Image& img, int y, int x) {
+    const double v = (double)static_cast<const Px*>(img.data)[(long long)y * img.W + x];
+    return img.sign < 0 ? -v : v;
+}
+
+// Values of the cell's border pixels (mask pixels with an 8-neighbour outside the mask or the box)
+// into out[0, count), row-major; returns count.
+template <typename Px>
+__device__ int gather_border(const Image& img, int4 box, const uint32_t* rowm, double* out, int lane) {
+    // All three of columns lane - 1, lane, lane + 1 of a row in the mask (column -1 and 32 are outside).
+    auto full3 = [&](uint32_t m) { return lane >= 1 && lane <= 30 && ((m >> (lane - 1)) & 7u) == 7u; };
+    int base = 0;
+    for (int y0 = 0; y0 < box.w; y0 += 4) {
+        bool border[4];
+        double val[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int yy = y0 + u;
+            border[u] = false;
+            if (yy < box.w) {
+                const uint32_t cur = rowm[yy];
+                const uint32_t up = yy > 0 ? rowm[yy - 1] : 0u, dn = yy + 1 < box.w ? rowm[yy + 1] : 0u;
+                border[u] = ((cur >> lane) & 1u) && !(full3(up) && full3(cur) && full3(dn));
+            }
+            val[u] = border[u] ? px_at<Px>(img, box.y + yy, box.x + lane) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t m = __ballot_sync(0xffffffffu, border[u]);
+            if (border[u]) out[base + __popc(m & ((1u << lane) - 1u))] = val[u];
+            base += __popc(m);
+        }
+    }
+    __syncwarp();
+    return base;
+}
+
+// stage_cell from the row masks: v[slot] = value - bg0 (rounded to T), xy[slot] packed.
+template <typename Px, typename T>
+__device__ int stage_cell_masked(const Image& img, int4 box, const uint32_t* rowm, double bg0, T* v, int* xy,
+                                 int lane) {
+    int base = 0;
+    for (int y0 = 0; y0 < box.w; y0 += 4) {
+        bool in[4];
+        double val[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int yy = y0 + u;
+            in[u] = yy < box.w && ((rowm[yy] >> lane) & 1u);
+            val[u] = in[u] ? px_at<Px>(img, box.y + yy, box.x + lane) - bg0 : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t m = __ballot_sync(0xffffffffu, in[u]);
+            if (in[u]) {
+                const int slot = base + __popc(m & ((1u << lane) - 1u));
+                v[slot] = (T)val[u];
+                xy[slot] = lane | ((y0 + u) << 16);
+            }
+            base += __popc(m);
+        }
+    }
+    __syncwarp();
+    return base;
+}
+
+// Order statistics k1 and k2 (0-based) of n <= 128 values s[0, n), none NaN, by counting ranks
+// (ties ordered by position, so the ranks are a permutation of 0..n-1): each lane ranks its up to
+// four values against all n.
+__device__ __forceinline__ void warp_rank_select2(const double* s, int n, int k1, int k2, int lane, double* r1,
+                                                  double* r2) {
+    double mine[4];
+    int rank[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        mine[u] = lane + 32 * u < n ? s[lane + 32 * u] : 0.0;
+        rank[u] = 0;
+    }
+    for (int k = 0; k < n; ++k) {
+        const double x = s[k];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) rank[u] += (x < mine[u] || (x == mine[u] && k < lane + 32 * u)) ? 1 : 0;
+    }
+    double c1 = 0.0, c2 = 0.0;
+    bool h1 = false, h2 = false;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (lane + 32 * u < n) {
+            if (rank[u] == k1) { c1 = mine[u]; h1 = true; }
+            if (rank[u] == k2) { c2 = mine[u]; h2 = true; }
+        }
+    const unsigned b1 = __ballot_sync(0xffffffffu, h1), b2 = __ballot_sync(0xffffffffu, h2);
+    *r1 = __shfl_sync(0xffffffffu, c1, __ffs(b1) - 1);
+    *r2 = __shfl_sync(0xffffffffu, c2, __ffs(b2) - 1);
+}
+
+// Narrow-box front end of the initial fit: the 10th-percentile border background (unless a level
+// is given) and the staged cell; returns the cell's pixel count.
+template <typename Px, typename T>
+__device__ __forceinline__ int narrow_front(const Image& img, int4 box, const uint32_t* rowm, bool level, double* vbuf, T* v,
+                            int* xy, int lane, double* bg0);
+
+// NumPy's 'linear' q-th percentile of the n values s[0, n) (any order; n >= 1), which the warp may
+// reorder: rank selection of the two order statistics for n <= 128 without NaN, else a bitonic sort
+// of s padded with +inf to a power of two (s holds room for it).
+__device__ double warp_percentile(double* s, int n, double q, int lane) {
+    bool nan = false;
+    for (int i = lane; i < n; i += 32) nan = nan || isnan(s[i]);
+    if (n <= 128 && !__any_sync(0xffffffffu, nan)) {
+        // The index arithmetic of sorted_percentile.
+        const double virt = __dmul_rn((double)(n - 1), q);
+        const double below = floor(virt);
+        int lo = (int)below;
+        if (lo < 0) lo = 0;
+        if (lo > n - 1) lo = n - 1;
+        int hi = lo + 1 < n ? lo + 1 : n - 1;
+        const bool last = virt >= (double)(n - 1);
+        if (last) lo = hi = n - 1;
+        double a, b;
+        warp_rank_select2(s, n, lo, hi, lane, &a, &b);
+        __syncwarp();
+        if (last) return a;
+        const double gamma = __dsub_rn(virt, below);
+        const double diff = __dsub_rn(b, a);
+        if (gamma >= 0.5) return __dsub_rn(b, __dmul_rn(diff, __dsub_rn(1.0, gamma)));
+        return __dadd_rn(a, __dmul_rn(diff, gamma));
+    }
+    int m2 = 1;
+    while (m2 < n) m2 <<= 1;
+    for (int i = n + lane; i < m2; i += 32) s[i] = dinf();
+    __syncwarp();
+    warp_bitonic_sort(s, m2, lane);
+    const double r = sorted_percentile(s, n, q);
+    __syncwarp();
+    return r;
+}
+
+template <typename Px, typename T>
+__device__ __forceinline__ int narrow_front(const Image& img, int4 box, const uint32_t* rowm, bool level, double* vbuf, T* v,
+                            int* xy, int lane, double* bg0) {
+    if (!level) {
+        const int nb = gather_border<Px>(img, box, rowm, vbuf, lane);
+        *bg0 = nb > 0 ? warp_percentile(vbuf, nb, 0.1, lane) : 0.0;
+    }
+    return stage_cell_masked<Px, T>(img, box, rowm, *bg0, v, xy, lane);
+}
+
 // --------------------------------------------------------------------------------- kernels
 
 struct FitArgs {
@@ -155,7 +331,7 @@ struct WarmStart {
 // T: type of the staged cell values and of the LM's per-pixel arithmetic (double or float).
 // Launch bounds: at most 8 warps, two such blocks per SM, which caps registers at 128 (a few spilled
 // in the solve) so that 16 warps of 4-warp blocks fit per SM.
-template <typename T>
+template <typename T, typename Px>
 __global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a, const double* seeds, double background_level, int has_level,
                               double* params, uint8_t* status, int* iters, WarmStart warm) {
     extern __shared__ unsigned char smem[];
@@ -179,47 +355,47 @@ __global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a,
         j = __shfl_sync(0xffffffffu, j, 0);
         if (j >= a.n) break;
         const int4 box = a.boxes[j];
-        // Border pixels: mask pixels with an 8-neighbour outside the mask or the box.
+        // Border pixels: mask pixels with an 8-neighbour outside the mask or the box. Narrow boxes
+        // take the row-mask path; wider ones test the labels per pixel.
         auto in_cell = [&](int yy, int xx) {
             return yy >= 0 && xx >= 0 && yy < box.w && xx < box.z &&
                    a.vor[(long long)(box.y + yy) * a.img.W + (box.x + xx)] == j;
         };
-        double bg0;
-        if (has_level) {
-            bg0 = background_level;
+        double bg0 = background_level;
+        int n;
+        if (box.z <= 32 && box.w <= kMaskRowsMax) {
+            uint32_t* rowm = reinterpret_cast<uint32_t*>(lm_slots[warp]);
+            cell_row_masks(a.vor, a.img.W, box, j, rowm, lane);
+            n = narrow_front<Px>(a.img, box, rowm, has_level, vbuf, v, xy, lane, &bg0);
         } else {
-            // Stage border values into v (sorted below), then take the 10th percentile.
-            int base = 0;
-            const int P = box.z * box.w;
-            for (int k0 = 0; k0 < P; k0 += 32) {
-                const int k = k0 + lane;
-                bool border = false;
-                int yy = 0, xx = 0;
-                if (k < P) {
-                    yy = k / box.z;
-                    xx = k - yy * box.z;
-                    if (in_cell(yy, xx)) {
-                        for (int dy = -1; dy <= 1 && !border; ++dy)
-                            for (int dx = -1; dx <= 1; ++dx)
-                                if (!in_cell(yy + dy, xx + dx)) { border = true; break; }
+            if (!has_level) {
+                // Stage border values into v, then take the 10th percentile.
+                int base = 0;
+                const int P = box.z * box.w;
+                for (int k0 = 0; k0 < P; k0 += 32) {
+                    const int k = k0 + lane;
+                    bool border = false;
+                    int yy = 0, xx = 0;
+                    if (k < P) {
+                        yy = k / box.z;
+                        xx = k - yy * box.z;
+                        if (in_cell(yy, xx)) {
+                            for (int dy = -1; dy <= 1 && !border; ++dy)
+                                for (int dx = -1; dx <= 1; ++dx)
+                                    if (!in_cell(yy + dy, xx + dx)) { border = true; break; }
+                        }
                     }
+                    const unsigned m = __ballot_sync(0xffffffffu, border);
+                    if (border) vbuf[base + __popc(m & ((1u << lane) - 1u))] = a.img.at(box.y + yy, box.x + xx);
+                    base += __popc(m);
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, border);
-                if (border) vbuf[base + __popc(m & ((1u << lane) - 1u))] = a.img.at(box.y + yy, box.x + xx);
-                base += __popc(m);
+                __syncwarp();
+                bg0 = base > 0 ? warp_percentile(vbuf, base, 0.1, lane) : 0.0;
             }
-            __syncwarp();
-            int m2 = 1;
-            while (m2 < base) m2 <<= 1;
-            for (int i = base + lane; i < m2; i += 32) vbuf[i] = dinf();
-            __syncwarp();
-            warp_bitonic_sort(vbuf, m2, lane);
-            bg0 = base > 0 ? sorted_percentile(vbuf, base, 0.1) : 0.0;
-            __syncwarp();
+            n = stage_cell(box, j, a.vor, a.img.W, v, xy, lane, [&](int yy, int xx) {
+                return a.img.at(box.y + yy, box.x + xx) - bg0;
+            });
         }
-        const int n = stage_cell(box, j, a.vor, a.img.W, v, xy, lane, [&](int yy, int xx) {
-            return a.img.at(box.y + yy, box.x + xx) - bg0;
-        });
         // initial_params: amplitude = peak, centre = seed, sigma from the core's second moment.
         double peak = -dinf();
         for (int k = lane; k < n; k += 32) peak = fmax(peak, (double)v[k]);
@@ -1037,16 +1213,39 @@ int read_fit_options(const spx_fit_options* o, bool* f32, double* cost_tol) {
     return SPX_OK;
 }
 
+template <typename T, typename Px>
+int launch_fit_initial_px(const FitArgs& a0, FitLayout L, cudaStream_t s, const double* seeds,
+                          double background_level, int has_level, double* params, uint8_t* status, int* iterations,
+                          WarmStart warm) {
+    return launch_fit(a0, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
+        if (smem + kLmSlotBytes > 48 * 1024)
+            SPX_CUDA(cudaFuncSetAttribute(k_fit_initial<T, Px>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+        k_fit_initial<T, Px><<<blocks, warps * 32, smem, s>>>(fa, seeds, background_level, has_level, params,
+                                                               status, iterations, warm);
+        return check_launch("k_fit_initial");
+    });
+}
+
+// The pixel type is a template parameter of the initial fit (its narrow-box front end loads pixels
+// without a dtype branch per load).
 template <typename T>
 int launch_fit_initial(const FitArgs& a0, FitLayout L, cudaStream_t s, const double* seeds, double background_level,
                        int has_level, double* params, uint8_t* status, int* iterations, WarmStart warm) {
-    return launch_fit(a0, L, s, [&](const FitArgs& fa, size_t smem, int warps, int blocks) -> int {
-        if (smem + kLmSlotBytes > 48 * 1024)
-            SPX_CUDA(cudaFuncSetAttribute(k_fit_initial<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_fit_initial<T><<<blocks, warps * 32, smem, s>>>(fa, seeds, background_level, has_level, params, status,
-                                                           iterations, warm);
-        return check_launch("k_fit_initial");
-    });
+    switch (a0.img.dtype) {
+        case SPX_U8:
+            return launch_fit_initial_px<T, uint8_t>(a0, L, s, seeds, background_level, has_level, params, status,
+                                                     iterations, warm);
+        case SPX_U16:
+            return launch_fit_initial_px<T, uint16_t>(a0, L, s, seeds, background_level, has_level, params, status,
+                                                      iterations, warm);
+        case SPX_F32:
+            return launch_fit_initial_px<T, float>(a0, L, s, seeds, background_level, has_level, params, status,
+                                                   iterations, warm);
+        default:
+            return launch_fit_initial_px<T, double>(a0, L, s, seeds, background_level, has_level, params, status,
+                                                    iterations, warm);
+    }
 }
 
 template <typename T>

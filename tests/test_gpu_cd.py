@@ -51,3 +51,49 @@ def test_measure_cds_matches_reference_cpu(golden, name):
         centers = z[f"{name}_{method}_centers"]
         fin = np.isfinite(centers).all(axis=1) & np.isfinite(got.centers_xy).all(axis=1)
         assert np.abs(got.centers_xy[fin] - centers[fin]).max(initial=0) <= 1e-3, method
+
+
+def _mixed_page(dtype):
+    """288 x 288 page, 48 px pitch, holes of 30 and 12 px diameter alternating: the large holes'
+    cell boxes are wider than 32 columns (the initial fit's per-pixel border test), the small ones'
+    narrower (its row-mask path)."""
+    from imageprocessor_new_b200 import synthetic
+
+    rng = np.random.default_rng(7)
+    shape = (288, 288)
+    centers = synthetic.square_grid(shape, 48.0, rng)
+    d = np.where(np.arange(len(centers)) % 2 == 0, 30.0, 12.0)
+    clean = synthetic.render(shape, centers, d, 1.5, amplitude=3000.0, background=1000.0)
+    img = synthetic.add_noise(clean, rng, read_noise=20.0)
+    if dtype == np.uint8:
+        return (img >> 5).astype(np.uint8)
+    return img.astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.uint16, np.uint8, np.float32, np.float64])
+def test_measure_cds_wide_and_narrow_cells_match_oracle(dtype):
+    from imageprocessor_new_b200 import measure_cds
+    from oracle import cd as ocd
+
+    img = _mixed_page(dtype)
+    kw = dict(methods=("gaussian",), area_max=2000)
+    res = measure_cds(img, backend="gpu", **kw)
+    ref = ocd.measure_cds(img, **kw)
+    np.testing.assert_array_equal(res.seeds_xy, ref["seeds"])
+    assert len(ref["seeds"]) == 36
+    if dtype in (np.uint16, np.uint8):
+        # Cell boxes are the component boxes grown by pad = 3 on each side.
+        from oracle import segment as osg
+
+        binary = osg.binarize(img, osg.otsu_threshold(img), False)
+        _, _, stats, _ = osg.label_components(binary, 8)
+        box_w = stats[1:, 2] + 6
+        assert (box_w > 32).any() and (box_w <= 32).any()
+    np.testing.assert_allclose(res.deblend_model["params"], ref["params"], rtol=0, atol=1e-6)
+    got = res.measurements["gaussian"]
+    want = ref["measurements"]["gaussian"]
+    assert np.array_equal(got.status, want["status"])
+    a, b = got.metrics["cd_equivalent_px"], want["metrics"]["cd_equivalent_px"]
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    ok = ~np.isnan(a)
+    assert ok.sum() >= 30 and np.abs(a[ok] - b[ok]).max() <= 2e-3
