@@ -53,8 +53,9 @@ class GemmEpilogue(ctypes.Structure):
 
 
 class FitOptions(ctypes.Structure):
-    """spx_fit_options: LM arithmetic (FIT_F64 / FIT_F32) and the plain fits' relative cost tolerance."""
-    _fields_ = [("precision", c_int), ("cost_tol", c_double)]
+    """spx_fit_options: LM arithmetic (FIT_F64 / FIT_F32), the plain fits' relative cost tolerance and
+    the rows per image of a stack (0: one image)."""
+    _fields_ = [("precision", c_int), ("cost_tol", c_double), ("rows_per_image", c_int)]
 
 
 FIT_F64, FIT_F32 = 0, 1
@@ -83,6 +84,7 @@ SIGNATURES = {
     "spx_transpose_bf16": (_I, [_P, _I, _I, _P, _P]),
     "spx_mlp_outputs_to_params": (_I, [_P, _P, _P, _P, _P, _I, _P, _P, _P]),
     "spx_extract_patches": (_I, [_P, _I, _D, _I, _I, _P, _I, _P, _P, _P]),
+    "spx_extract_patches_stack": (_I, [_P, _I, _D, _I, _I, _I, _P, _P, _I, _P, _P, _P]),
     "spx_hole_coverage": (_I, [_I, _I, _P, _P, _P, _I, _I, _D, _I, _P, _P]),
     "spx_page_finish": (_I, [_P, c_longlong, _D, _D, _D, ctypes.c_ulonglong, _P, _P]),
     "spx_tune_set": (_I, [ctypes.c_char_p, _I]),

@@ -315,6 +315,7 @@ struct FitArgs {
     int* queue;       // work counter (reset by the host before the launch)
     double* gbuf_v;   // global staging when shared memory is too small (else null)
     int* gbuf_xy;
+    int rows_per_image;  // > 0: the image is a stack of such images; seeds are in their own image's rows
 };
 
 // Initial fit: 10th-percentile cell-border background, initial_params, LM, status.
@@ -400,7 +401,9 @@ __global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a,
         double peak = -dinf();
         for (int k = lane; k < n; k += 32) peak = fmax(peak, (double)v[k]);
         peak = warp_max(peak);
-        const double sx = seeds[2LL * j] - box.x, sy = seeds[2LL * j + 1] - box.y;
+        // Box origin in the seed's own image (a stack's boxes are in stack rows).
+        const int box_y = a.rows_per_image > 0 ? box.y % a.rows_per_image : box.y;
+        const double sx = seeds[2LL * j] - box.x, sy = seeds[2LL * j + 1] - box_y;
         double tot = 0.0, mom = 0.0, amax = 0.0;
         for (int k = lane; k < n; k += 32) {
             const double d = (double)v[k];
@@ -1205,11 +1208,14 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
 namespace {
 
 // The fit options with their defaults (FP64, the reference's 1e-12 stop rule) and checks.
-int read_fit_options(const spx_fit_options* o, bool* f32, double* cost_tol) {
+int read_fit_options(const spx_fit_options* o, bool* f32, double* cost_tol, int* rows_per_image, int height) {
     *f32 = o && o->precision == SPX_FIT_F32;
     *cost_tol = o ? o->cost_tol : 1e-12;
+    *rows_per_image = o ? o->rows_per_image : 0;
     SPX_REQUIRE(!o || o->precision == SPX_FIT_F64 || o->precision == SPX_FIT_F32, "bad fit precision");
     SPX_REQUIRE(*cost_tol > 0.0 && *cost_tol < 1.0, "fit cost_tol must be in (0, 1)");
+    SPX_REQUIRE(*rows_per_image == 0 || (*rows_per_image > 0 && height % *rows_per_image == 0),
+                "rows_per_image must be 0 or divide the image height");
     return SPX_OK;
 }
 
@@ -1276,7 +1282,8 @@ int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height
     SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
     bool f32 = false;
     double cost_tol = 1e-12;
-    if (int e = read_fit_options(options, &f32, &cost_tol)) return e;
+    int rows_per_image = 0;
+    if (int e = read_fit_options(options, &f32, &cost_tol, &rows_per_image, height)) return e;
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && voronoi && boxes && caps && seeds && params && status && workspace, "null pointer");
     SPX_REQUIRE(workspace_bytes >= spx_fit_workspace_bytes(max_cell_pixels), "workspace too small");
@@ -1284,7 +1291,7 @@ int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height
     const int cap_px = pow2_at_least(max_cell_pixels > 0 ? max_cell_pixels : 1);
     FitLayout L = fit_layout(workspace, cap_px, nullptr);
     FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
-              hm, wm, cap_px, max_iter, cost_tol, nullptr, nullptr, nullptr};
+              hm, wm, cap_px, max_iter, cost_tol, nullptr, nullptr, nullptr, rows_per_image};
     const WarmStart warm{init_params, init_ok, background_out, fallback_out, warm_cost_tol};
     return f32 ? launch_fit_initial<float>(a, L, s, seeds, background_level, has_level, params, status, iterations,
                                            warm)
@@ -1301,7 +1308,8 @@ int spx_deblend_iteration(const void* img, int dtype, double sign, int height, i
     SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
     bool f32 = false;
     double cost_tol = 1e-12;
-    if (int e = read_fit_options(options, &f32, &cost_tol)) return e;
+    int rows_per_image = 0;
+    if (int e = read_fit_options(options, &f32, &cost_tol, &rows_per_image, height)) return e;
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && voronoi && boxes && caps && background && model && params && params_out && status_out &&
                     maxstep && workspace,

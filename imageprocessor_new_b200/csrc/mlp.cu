@@ -288,7 +288,10 @@ __global__ void k_outputs_to_params(const float* y, const double* mean, const do
         for (int j = 0; j < 6; ++j) t[j] = (double)y[7LL * i + j] * stdv[j] + mean[j];
         const double* nm = norm + 4LL * i;
         const int4 b = boxes[i];
-        const double p[6] = {t[0] * nm[3], nm[0] + 16.0 + t[1] - b.x, nm[1] + 16.0 + t[2] - b.y, t[3], t[4], t[5]};
+        // Patch origin relative to the box first (exact integers), so the result does not depend on
+        // where the box sits (a stack's rows).
+        const double p[6] = {t[0] * nm[3], (nm[0] - b.x) + 16.0 + t[1], (nm[1] - b.y) + 16.0 + t[2], t[3], t[4],
+                             t[5]};
         bool good = p[0] > 0.0;
 #pragma unroll
         for (int j = 0; j < 6; ++j) {

@@ -1,7 +1,9 @@
 // Inputs of the warm-start MLP and the synthetic pages it is trained on.
 //
 // A patch is the 32 x 32 window of the signal (image x sign) whose centre pixel (16, 16) is the
-// cell seed rounded to the nearest pixel, edges replicated. It is normalised by its own level and
+// cell seed rounded to the nearest pixel, edges replicated. In a stack of images (images x H rows;
+// cell boxes in stack rows, seeds in their own image's rows) a patch replicates the edges of its
+// cell's image, so a stacked cell's patch is the one it has in that image. It is normalised by its own level and
 // scale: bg = the smallest mean of the 60 2 x 2 blocks along its border (robust to single noisy
 // pixels), amp = max - bg, and x = (v - bg) / amp, stored as bf16. One warp per patch, lane c
 // holding column c in registers, so the window is read once.
@@ -23,18 +25,20 @@ constexpr int kPatch = 32;
 // Templated on the pixel type so that a lane's 32 loads are straight-line code, all in flight at
 // once (a dtype switch per load can put each load behind its own branch).
 template <typename Px>
-__global__ void k_extract_patches(const Px* img, double sign, int H, int W, const double* seeds, int n,
-                                  __nv_bfloat16* out, double* norm) {
+__global__ void k_extract_patches(const Px* img, double sign, int images, int H, int W, const double* seeds,
+                                  const int* boxes, int n, __nv_bfloat16* out, double* norm) {
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        // First row of the cell's image (a box's y is in stack rows).
+        const int y0 = boxes ? min(max(boxes[4LL * i + 1], 0) / H, images - 1) * H : 0;
         const int ox = (int)rint(seeds[2LL * i]) - kPatch / 2, oy = (int)rint(seeds[2LL * i + 1]) - kPatch / 2;
         const int x = min(max(ox + lane, 0), W - 1);
         double col[kPatch];
         double mx = -dinf();
 #pragma unroll
         for (int r = 0; r < kPatch; ++r) {
-            const int y = min(max(oy + r, 0), H - 1);
+            const int y = y0 + min(max(oy + r, 0), H - 1);
             col[r] = sign * (double)img[(long long)y * W + x];
             mx = fmax(mx, col[r]);
         }
@@ -61,7 +65,7 @@ __global__ void k_extract_patches(const Px* img, double sign, int H, int W, cons
         for (int r = 0; r < kPatch; ++r) o[r * kPatch] = __float2bfloat16_rn((float)((col[r] - bg) * inv));
         if (lane == 0) {
             norm[4LL * i] = ox;
-            norm[4LL * i + 1] = oy;
+            norm[4LL * i + 1] = y0 + oy;
             norm[4LL * i + 2] = bg;
             norm[4LL * i + 3] = amp;
         }
@@ -125,9 +129,12 @@ using namespace spx;
 
 extern "C" {
 
-int spx_extract_patches(const void* img, int dtype, double sign, int height, int width, const double* seeds, int n,
-                        void* out, double* norm, void* stream) {
-    SPX_REQUIRE(height > 0 && width > 0 && n >= 0 && dtype >= SPX_U8 && dtype <= SPX_F64, "bad arguments");
+int spx_extract_patches_stack(const void* img, int dtype, double sign, int images, int height, int width,
+                              const double* seeds, const int* boxes, int n, void* out, double* norm, void* stream) {
+    SPX_REQUIRE(images > 0 && height > 0 && width > 0 && n >= 0 && dtype >= SPX_U8 && dtype <= SPX_F64,
+                "bad arguments");
+    SPX_REQUIRE((long long)images * height <= 0x7fffffffLL, "stack too tall");
+    SPX_REQUIRE(images == 1 || boxes, "a stack needs the cell boxes");
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(img && seeds && out && norm, "null pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -135,22 +142,27 @@ int spx_extract_patches(const void* img, int dtype, double sign, int height, int
     auto* o = static_cast<__nv_bfloat16*>(out);
     switch (dtype) {
         case SPX_U8:
-            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const uint8_t*>(img), sign, height, width, seeds, n, o,
-                                                   norm);
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const uint8_t*>(img), sign, images, height, width,
+                                                   seeds, boxes, n, o, norm);
             break;
         case SPX_U16:
-            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const uint16_t*>(img), sign, height, width, seeds, n,
-                                                   o, norm);
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const uint16_t*>(img), sign, images, height, width,
+                                                   seeds, boxes, n, o, norm);
             break;
         case SPX_F32:
-            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const float*>(img), sign, height, width, seeds, n, o,
-                                                   norm);
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const float*>(img), sign, images, height, width,
+                                                   seeds, boxes, n, o, norm);
             break;
         default:
-            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const double*>(img), sign, height, width, seeds, n,
-                                                   o, norm);
+            k_extract_patches<<<grid, 256, 0, s>>>(static_cast<const double*>(img), sign, images, height, width,
+                                                   seeds, boxes, n, o, norm);
     }
     return check_launch("k_extract_patches");
+}
+
+int spx_extract_patches(const void* img, int dtype, double sign, int height, int width, const double* seeds, int n,
+                        void* out, double* norm, void* stream) {
+    return spx_extract_patches_stack(img, dtype, sign, 1, height, width, seeds, nullptr, n, out, norm, stream);
 }
 
 int spx_hole_coverage(int height, int width, const double* holes, const int* grid_start, const int* grid_ids,

@@ -221,23 +221,31 @@ def active() -> "WarmStartNet | None":
 
 # ---------------------------------------------------------------------------------- inference
 
-def patches(image_d: torch.Tensor, sign: float, seeds_d: torch.Tensor, n: int):
-    """(n, 1024) bf16 patches and (n, 4) [origin x, origin y, bg, amp] around the seeds."""
+def patches(image_d: torch.Tensor, sign: float, seeds_d: torch.Tensor, n: int, images: int = 1,
+            boxes_d: torch.Tensor | None = None):
+    """(n, 1024) bf16 patches and (n, 4) [origin x, origin y, bg, amp] around the seeds. With
+    images > 1 the (rows, W) image is a stack of that many images of rows / images rows each, the
+    cell boxes (y in stack rows) say which image each cell is in, the seeds are in that image's rows,
+    and each patch replicates the edges of its cell's image."""
     h, w = image_d.shape
+    if images < 1 or h % images or (images > 1 and boxes_d is None):
+        raise ValueError(f"{h} rows do not split into {images} images with cell boxes")
     out = dev.empty((max(n, 1), IN), torch.bfloat16)
     norm = dev.empty((max(n, 1), 4), torch.float64)
     if n:
-        _lib.call("spx_extract_patches", image_d.data_ptr(), dev.dtype_code(image_d), float(sign), h, w,
-                  seeds_d.data_ptr(), n, out.data_ptr(), norm.data_ptr(), dev.stream_ptr())
+        _lib.call("spx_extract_patches_stack", image_d.data_ptr(), dev.dtype_code(image_d), float(sign), images,
+                  h // images, w, seeds_d.data_ptr(), None if images == 1 else boxes_d.data_ptr(), n,
+                  out.data_ptr(), norm.data_ptr(), dev.stream_ptr())
     return out[:n], norm[:n]
 
 
 def predict_init(net: WarmStartNet, image_d: torch.Tensor, sign: float, seeds_d: torch.Tensor, boxes_d: torch.Tensor,
-                 n: int, batch: int | None = None):
+                 n: int, batch: int | None = None, images: int = 1):
     """ROI-local LM starting params (n, 6) f64 and validity flags for the cells, on the device.
     All cells go through each layer in one GEMM launch unless `batch` bounds the rows per launch
-    (the activations take 1 KB per row); a row's outputs do not depend on the batching."""
-    x, norm = patches(image_d, sign, seeds_d, n)
+    (the activations take 1 KB per row); a row's outputs do not depend on the batching. `images` as
+    in `patches`."""
+    x, norm = patches(image_d, sign, seeds_d, n, images, boxes_d)
     if n and (batch is None or batch >= n):
         y = net.forward(x)
     else:
@@ -336,12 +344,14 @@ def page_cells(page_d: torch.Tensor, *, area_min: int = 10, area_max: int = 2000
 
 
 def initial_fits(page_d: torch.Tensor, cells, *, sign: float = 1.0, max_iter: int = 30, warm=None,
-                 cost_tol: float = 1e-12, precision: str = "fp64"):
+                 cost_tol: float = 1e-12, precision: str = "fp64", rows_per_image: int = 0):
     """The initial LM fits of the cells (plain, or warm-started with (params, ok)) in the given LM
-    arithmetic: params, status, iterations, cell-border backgrounds and fallback flags (device)."""
+    arithmetic: params, status, iterations, cell-border backgrounds and fallback flags (device).
+    rows_per_image > 0: the page is a stack of such images (boxes in stack rows, seeds in image rows)."""
     from .deblend import fit_options
 
     opts = fit_options(precision)
+    opts.rows_per_image = int(rows_per_image)
     cost_tol = max(float(cost_tol), opts.cost_tol)
     n = cells.n
     h, w = page_d.shape

@@ -241,6 +241,8 @@ enum { SPX_FIT_F64 = 0, SPX_FIT_F32 = 1 };
 typedef struct spx_fit_options {
     int precision;
     double cost_tol;
+    int rows_per_image; /* 0: one image; > 0: the image is a stack of images this many rows high
+                         * (boxes in stack rows, seeds in each cell's own image rows) */
 } spx_fit_options;
 
 size_t spx_fit_workspace_bytes(int max_cell_pixels);
@@ -443,7 +445,7 @@ int spx_adamw(float* param, const float* grad, float* m, float* v, int rows, int
 /* dst (cols x rows) = src (rows x cols)^T, bf16. */
 int spx_transpose_bf16(const void* src, int rows, int cols, void* dst, void* stream);
 /* Standardised MLP outputs y (n x 7 f32) -> ROI-local LM starting params (n x 6): t = y * std +
- * mean; A = t0 amp, x0 = origin x + 16 + t1 - box x, y0 = origin y + 16 + t2 - box y, u = t3..t5,
+ * mean; A = t0 amp, x0 = (origin x - box x) + 16 + t1, y0 = (origin y - box y) + 16 + t2, u = t3..t5,
  * with norm rows [origin x, origin y, bg, amp] of spx_extract_patches; ok = finite and A > 0. */
 int spx_mlp_outputs_to_params(const float* y, const double* out_mean, const double* out_std, const double* norm,
                               const int* boxes, int n, double* params, uint8_t* ok, void* stream);
@@ -452,6 +454,12 @@ int spx_mlp_outputs_to_params(const float* y, const double* out_mean, const doub
  * amp = max - bg, as bf16 (n x 1024); norm (n x 4 doubles) = [origin x, origin y, bg, amp]. */
 int spx_extract_patches(const void* img, int dtype, double sign, int height, int width, const double* seeds, int n,
                         void* out, double* norm, void* stream);
+/* spx_extract_patches over a stack of `images` images of height x width stored one after another
+ * (images * height rows): boxes (n x 4 int [x, y, w, h], y in stack rows; may be null for one image)
+ * give each cell's image, seeds are in that image's rows, each patch replicates the edges of its
+ * cell's image (the patch the cell has in its own image), and norm's origin y is in stack rows. */
+int spx_extract_patches_stack(const void* img, int dtype, double sign, int images, int height, int width,
+                              const double* seeds, const int* boxes, int n, void* out, double* norm, void* stream);
 /* Training pages: coverage (H x W doubles) of rotated superellipse holes (rows of [cx, cy, a, b,
  * theta, exponent]) sampled on samples x samples points per pixel, holes found through a CSR grid
  * of cell size `cell` (grid_start: grid_w * grid_h + 1 offsets into grid_ids). */

@@ -57,6 +57,15 @@ def test_fit_options_are_checked_before_any_device_work():
                                        None, None, None, None, opts, None, 0, None)
         assert rc != 0
         assert b"fit" in lib.spx_last_error()
+    # A stack's rows per image must divide the image height.
+    for opts in (_lib.FitOptions(_lib.FIT_F64, 1e-12, 3), _lib.FitOptions(_lib.FIT_F64, 1e-12, -8)):
+        rc = lib.spx_deblend_iteration(None, 1, 1.0, 8, 8, None, None, None, 0, 4, 4, 16, bg, None, 2, None, 0.6, 30,
+                                       None, None, None, None, opts, None, 0, None)
+        assert rc != 0
+        assert b"rows_per_image" in lib.spx_last_error()
+    # Patches of a stack need the cell boxes (they say which image a cell is in).
+    rc = lib.spx_extract_patches_stack(None, 1, 1.0, 2, 8, 8, None, None, 1, None, None, None)
+    assert rc != 0 and b"boxes" in lib.spx_last_error()
 
 
 def test_status_names_match_the_binding():
