@@ -61,6 +61,7 @@ def stack_cells(stack_d: torch.Tensor, *, area_min: int = 10, area_max: int = 20
     for i in range(n_img):
         c = ws.page_cells(stack_d[i], area_min=area_min, area_max=area_max, pad=pad)
         torch.add(c.voronoi, starts[-1], out=vor[i * h:(i + 1) * h])
+        c.voronoi = None  # the stack's copy is the one kept
         parts.append(c)
         starts.append(starts[-1] + c.n)
     shift = [i * h for i in range(n_img)]

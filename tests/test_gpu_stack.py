@@ -3,8 +3,8 @@
 Four 768 x 768 synthetic images with their own pitch, hole size, blur and noise. The one-launch
 stack fits must be the per-image fits cell for cell (plain and warm-started), and per image the
 plain fits of a sample of cells are checked against the FP64 oracle's initial fit
-(oracle/deblend.py, restating subpx/_cpu/deblend.py:152-171 and 174-254 with the border
-percentile of :330-341).
+(oracle/deblend.py, restating subpx/_cpu/deblend.py:152-171 and 174-254 with the cell-border
+10th percentile of :480-481).
 """
 
 import numpy as np
