@@ -404,6 +404,7 @@ def stack_arm(args):
     """All cells of the uneven stack in one initial-fit launch: cells/s warm-started and plain."""
     import torch
 
+    from imageprocessor_new_b200 import _lib
     from imageprocessor_new_b200 import stack as st
     from imageprocessor_new_b200 import warmstart as ws
 
@@ -420,6 +421,7 @@ def stack_arm(args):
                 fn()
         torch.cuda.synchronize()
         clocks.mark_start()
+        n0 = _lib.lib().spx_launch_count()
         for _ in range(args.steps):
             for k, fn in arms.items():
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -428,6 +430,7 @@ def stack_arm(args):
                 b.record()
                 torch.cuda.synchronize()
                 ms[k] += a.elapsed_time(b) / args.steps
+        launches = _lib.lib().spx_launch_count() - n0
         clocks.mark_end()
     net.check_errors()
     (pw, sw, iw, _, fw), (pp, sp, ip, _, _) = ([t.cpu().numpy() for t in res[k]] for k in ("warm", "plain"))
@@ -451,7 +454,7 @@ def stack_arm(args):
                    "l2": f"inputs larger than L2 ({s.numel() * 2 / 1e9:.1f} GB stack)"},
         "plain_lm": {"value": round(n / (ms["plain"] / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms["plain"], 3)},
         "speedup": round(ms["plain"] / ms["warm"], 3),
-        "gpu_launches": 7 * args.steps,  # per step: patches, 3 GEMMs, params, warm fit; plain fit
+        "gpu_launches": int(launches),
         "fallback_fraction": float(fw.mean()),
         "centre_dev_max_px": max(p["centre_dev_max_px"] for p in per_image),
         "within_1e-3_px": bool(all(p["centre_dev_max_px"] <= 1e-3 for p in per_image)),
