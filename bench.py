@@ -8,6 +8,12 @@ radial-gradient and half-height CDs, summary_only), all through the public API.
   value  cells/s with the page already in HBM (a CUDA tensor passed to the API)
   e2e    cells/s through the same API with a host (NumPy) page: host->device copy of the page and
          device->host copy of the results inside the timed region
+  accuracy_vs_oracle
+         the GPU pipeline (warm-started and plain) against the FP64 CPU oracle on the CPU-baseline
+         crop of the same page: largest centre and CD errors per method, same seeds / statuses
+  lm_stage
+         the initial-fit stage in three arms: plain LM at the reference's 1e-12 stop rule, plain LM
+         at the warm fits' 1e-7 rule (like for like), and patches + MLP + warm-started LM
 
 Cells = Voronoi cells reported and measured by the LM Gaussian method. The page (134 MB) is larger
 than the 126 MB L2, so consecutive steps do not run from cache.
@@ -52,8 +58,10 @@ METHODS = ("gaussian", "gradient", "halfmax")
 REFINERS = ("weighted", "logquad", "edge_gradmoment")
 CD_KW = dict(area_max=400, summary_only=True)
 CENTER_KW = dict(threshold="otsu", area_max=400)
-# DRAM bytes (read + write) per cell of one k_fit_iteration launch, from an ncu capture of one
-# launch on the 4096x4096 page (29,241 cells, 190.4 MB); traffic scales with the cells processed.
+# DRAM bytes (read + write) per cell of one k_fit_iteration launch and the FP64 pipe's busy
+# fraction, both constants read from one ncu capture of a launch on the 4096x4096 page (29,241
+# cells, 190.4 MB of DRAM traffic), not measured in this run; traffic scales with the cells
+# processed.
 FIT_TRAFFIC_PER_CELL = 6512.0
 FIT_FP64_PIPE_ACTIVE = 0.507
 
@@ -253,6 +261,7 @@ def gpu_arm(args):
     px_per_cell = 24 * 24
     bytes_per_cell = px_per_cell * (2 + 4 + 8 + 8) + 13 * 8
     achieved = fit_n * bytes_per_cell / (fit_avg_ms / 1e3) / 1e9 if fit_ms else None
+    mpix = world * args.page * args.page / 1e6 / (ms / 1e3 / args.steps)
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
@@ -267,10 +276,13 @@ def gpu_arm(args):
                      "peak": peaks.get("hbm_gbs"), "peak_source": which, "unit": "GB/s",
                      "frac": None if achieved is None else round(achieved / peaks["hbm_gbs"], 4),
                      "traffic": round(FIT_TRAFFIC_PER_CELL * fit_n / 1e9, 4), "traffic_unit": "GB per launch",
+                     "traffic_source": "constant per cell from one ncu capture (4096x4096 page), scaled by cells",
                      "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n,
                      # The kernel's arithmetic is FP64 (not a contraction, not HBM-bound): the FP64
-                     # pipe's busy fraction from the committed ncu capture of the same kernel.
-                     "fp64_pipe_active": FIT_FP64_PIPE_ACTIVE, "fp64_source": "profiles/k_fit_iteration_page4096.md"},
+                     # pipe's busy fraction from one ncu capture of the same kernel (a constant).
+                     "fp64_pipe_active": FIT_FP64_PIPE_ACTIVE,
+                     "fp64_source": "constant from one ncu capture of k_fit_iteration (4096x4096 page)"},
+        "mpix_per_s": round(mpix, 1),
         "gpu_launches": int(launches),
         "clocks": clock_summary,
     }
@@ -284,7 +296,13 @@ def gpu_arm(args):
         if lm_stage is not None:
             line["lm_stage"] = {k: (round(v, 6) if isinstance(v, float) else v) for k, v in lm_stage.items()}
     if args.cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(page, args.cpu_sample)
+        line["cpu_baseline"], oracle_res = cpu_baseline(page, args.cpu_sample)
+        crop = np.ascontiguousarray(page[:args.cpu_sample, :args.cpu_sample])
+        line["accuracy_vs_oracle"] = {"sample": line["cpu_baseline"]["sample"]}
+        for variant in ["plain"] + (["warm"] if net is not None else []):
+            warmstart.use(net if variant == "warm" else None)
+            line["accuracy_vs_oracle"][variant] = _accuracy_vs_oracle(crop, oracle_res)
+        warmstart.use(None)
     print(json.dumps(line), flush=True)
 
 
@@ -301,6 +319,39 @@ def _accuracy(warm, plain) -> dict:
         dcd = (float(np.abs(a.metrics["cd_equivalent_px"][both] - b.metrics["cd_equivalent_px"][both]).max())
                if both.any() else 0.0)
         out[name] = {"centre_max_px": dc, "cd_max_px": dcd, "same_validity": float((a.valid == b.valid).mean())}
+    return out
+
+
+def _accuracy_vs_oracle(crop, oracle_res) -> dict:
+    """The GPU pipeline on the crop (the three refiners' centres and measure_cds) against the FP64
+    CPU oracle's results on the same crop: same seeds and statuses, largest centre / CD errors."""
+    from imageprocessor_new_b200 import detect_centers, measure_cds
+
+    centers, cds = oracle_res
+    out = {"refiners": {}}
+    for refine in REFINERS:
+        got = detect_centers(crop, backend="gpu", refine=refine, **CENTER_KW).centers_xy
+        want = centers[refine]
+        same = got.shape == want.shape
+        out["refiners"][refine] = {"same_count": bool(same),
+                                   "centre_max_px": float(np.abs(got - want).max(initial=0.0)) if same else None}
+    res = measure_cds(crop, backend="gpu", methods=METHODS, area_max=400)
+    out["same_seeds"] = bool(np.array_equal(res.seeds_xy, cds["seeds"]))
+    out["same_cell_labels"] = bool(np.array_equal(res.cell_labels, cds["cell_labels"]))
+    if not out["same_seeds"]:
+        return out
+    for m in METHODS:
+        got, want = res.measurements[m], cds["measurements"][m]
+        both = got.valid & (want["status"] == "ok")
+        a, b = got.metrics["cd_equivalent_px"][both], want["metrics"]["cd_equivalent_px"][both]
+        dc = np.abs(got.centers_xy[both] - want["centers"][both])
+        out[m] = {"cells": int(len(got.valid)), "same_status": float((got.status == want["status"]).mean()),
+                  "centre_max_px": float(dc.max(initial=0.0)), "cd_max_px": float(np.abs(a - b).max(initial=0.0))}
+    worst_c = max([out[m]["centre_max_px"] for m in METHODS] +
+                  [r["centre_max_px"] or 0.0 for r in out["refiners"].values()])
+    worst_cd = max(out[m]["cd_max_px"] for m in METHODS)
+    out["within_1e-3_px_centres"] = bool(worst_c <= 1e-3)
+    out["within_2e-3_px_cds"] = bool(worst_cd <= 2e-3)
     return out
 
 
@@ -321,19 +372,22 @@ def _d2h_bytes(cells: int) -> int:
 
 
 def cpu_baseline(page, size):
-    """The oracle (CPU restatement of the reference path) on a crop of the page, all host cores."""
+    """The oracle (CPU restatement of the reference path) on a crop of the page, all host cores.
+    Returns the baseline entry and the oracle's results ({refiner: centres}, measure_cds dict)."""
     from oracle import cd as ocd
     from oracle import centers as oc
 
     crop = np.ascontiguousarray(page[:size, :size])
     t0 = time.perf_counter()
+    centers = {}
     for refine in REFINERS:
-        oc.detect_centers(crop, threshold="otsu", refine_method=refine, area_max=400)
+        centers[refine] = oc.detect_centers(crop, threshold="otsu", refine_method=refine, area_max=400)
     res = ocd.measure_cds(crop, methods=METHODS, area_max=400)
     dt = time.perf_counter() - t0
     n = len(res["seeds"])
-    return {"value": round(n / dt, 2), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{size}x{size} crop of the page ({n} cells), same step", "seconds": round(dt, 2)}
+    return ({"value": round(n / dt, 2), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+             "sample": f"{size}x{size} crop of the page ({n} cells), same step", "seconds": round(dt, 2)},
+            (centers, res))
 
 
 def reference_arm(args):
@@ -346,7 +400,7 @@ def reference_arm(args):
         pass
     vals, secs, cells = [], [], 0
     for _ in range(args.steps):
-        r = cpu_baseline(page, size)
+        r, _ = cpu_baseline(page, size)
         vals.append(r["value"])
         secs.append(r["seconds"])
     value = float(np.median(vals))

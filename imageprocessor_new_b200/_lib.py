@@ -76,7 +76,7 @@ SIGNATURES = {
     "spx_ccl_workspace_bytes": (_S, [_I, _I]),
     "spx_gemm_bf16": (_I, [_P, _I, _P, _I, _I, _I, _I, POINTER(GemmEpilogue), _P, _P]),
     "spx_deblend_initial_warm": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _P, _I, _I, _I, _I, _D, _I, _I, _P, _P, _D, _P,
-                                      _P, _P, _P, _P, _FO, _P, _S, _P]),
+                                      _P, _P, _P, _P, _P, _FO, _P, _S, _P]),
     "spx_mlp_loss_grad": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _P, _P]),
     "spx_rowsum_bf16": (_I, [_P, _I, _I, _P, _P]),
     "spx_adamw": (_I, [_P, _P, _P, _P, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -132,8 +132,17 @@ SIGNATURES = {
     "spx_label_mask": (_I, [_P, _P, _I, _I, _I, _P, _P, _P]),
     "spx_gaussian_method": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _MO, _P]),
     "spx_logquad_cd": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _MO, _P]),
-    "spx_radial_workspace_bytes": (_S, [_I, _I]),
-    "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _MO, _MO, _P, _S, _P]),
+    "spx_radial_workspace_bytes": (_S, [_I, _I, _I]),
+    "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _P, _I, _MO, _MO, _P, _S, _P]),
+    "spx_minimum_filter": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "spx_signal_image": (_I, [_P, _I, _D, _I, _I, _P, _P]),
+    "spx_pitch_workspace_bytes": (_S, [_I, _I, _I]),
+    "spx_pitch_crop": (_I, [_P, _I, _D, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_pitch_from_autocorrelation": (_I, [_P, _I, _I, _I, _P, _P, _S, _P]),
+    "spx_peak_workspace_bytes": (_S, [_I, _I]),
+    "spx_peak_candidates": (_I, [_P, _P, _P, _I, _I, _P, _P, _I, _P, _P, _S, _P]),
+    "spx_peak_select_workspace_bytes": (_S, [_I]),
+    "spx_peak_select": (_I, [_P, _P, _I, _P, _D, _P, _I, _I, _P, _P, _P, _S, _P]),
 }
 
 class QuantileReq(ctypes.Structure):

@@ -1,10 +1,10 @@
 """measure_cds on the device: cells, deblending and CD measurements (drop-in for
 ``subpx.measure_cds(..., backend="gpu")``, subpx/cd.py:44-380 and _measure_cds 424-784).
 
-Scope: ``background="model"`` with ``seeds="threshold"`` and the methods gaussian (deblended
-Gaussian FWHM), logquad, gradient and halfmax — the hot path. Every per-pixel and per-cell step
-runs in libsubpx_b200; the host keeps the reference's orchestration (validation, the seed revision
-bookkeeping, result assembly).
+Scope: ``background="model"`` with ``seeds="threshold"`` or ``seeds="peaks"``, ``smooth_sigma`` >= 0,
+and the methods gaussian (deblended Gaussian FWHM), logquad, gradient and halfmax — the hot path.
+Every per-pixel and per-cell step runs in libsubpx_b200; the host keeps the reference's
+orchestration (validation, the seed revision bookkeeping, result assembly).
 """
 
 from __future__ import annotations
@@ -17,7 +17,7 @@ import torch
 from . import _device as dev
 from . import _lib
 from . import segment
-from .deblend import FWHM_K, STATUS, Deblender, build_cells, sigma_major
+from .deblend import FWHM_K, STATUS, Deblender, auto_tile, build_cells, sigma_major
 from .types import CDMethodResult, CDResult, CDSummary
 
 METHOD_LABELS = {
@@ -163,13 +163,9 @@ def measure_cds(
         raise ValueError("imageprocessor_new_b200 is the GPU backend: use backend='gpu' (or 'auto')")
     if background != "model":
         raise ValueError("backend='gpu' requires background='model'; border mode runs on the CPU")
-    if seeds != "threshold":
-        raise NotImplementedError("seeds='peaks' is not part of this package yet")
     unsupported = [m for m in methods if m not in SUPPORTED]
     if unsupported:
         raise NotImplementedError("methods outside the hot path: " + ", ".join(unsupported))
-    if smooth_sigma > 0:
-        raise NotImplementedError("smooth_sigma > 0 is not part of this package yet")
     metrics_only = bool(metrics_only) or bool(summary_only)
     with dev.on_device(device):
         return _measure_cds(img, methods=methods, threshold=threshold, invert=bool(invert), area_min=int(area_min),
@@ -178,7 +174,8 @@ def measure_cds(
                             background_level=background_level, background_tile=background_tile,
                             deblend_iterations=int(deblend_iterations), deblend_tolerance=float(deblend_tolerance),
                             pixel_size=float(pixel_size), unit=unit, device=int(device), metrics_only=metrics_only,
-                            summary_only=bool(summary_only), fit_precision=fit_precision)
+                            summary_only=bool(summary_only), fit_precision=fit_precision, seeds=seeds,
+                            peak_min_distance=peak_min_distance, smooth_sigma=float(smooth_sigma))
 
 
 def _segment(img_d: torch.Tensor, threshold: str, invert: bool):
@@ -339,9 +336,22 @@ def _revise_seeds(dbl: Deblender, state, seeds_xy, pitch, oversized_d, *, drop_f
     return drop, new
 
 
+def _peak_rows(img_d, sign, peak_min_distance):
+    """Cell rows of peak seeds (subpx/cd.py:502-511): a (2 ceil(0.6 pitch) + 1)^2 box around each
+    peak, no component, every hole reported by its fitted reach."""
+    from . import peaks
+
+    xy, pitch = peaks.detect_peaks(img_d, sign, min_distance=peak_min_distance)
+    half = int(np.ceil(0.6 * pitch))
+    rows = np.column_stack((xy[:, 0] - half, xy[:, 1] - half, np.full(len(xy), 2 * half + 1.0),
+                            np.full(len(xy), 2 * half + 1.0), xy[:, 0], xy[:, 1])).reshape(-1, 6)
+    return rows, pitch
+
+
 def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_angles, radial_step, fit_fraction,
                  background_level, background_tile, deblend_iterations, deblend_tolerance, pixel_size, unit, device,
-                 metrics_only, summary_only, fit_precision="fp64"):
+                 metrics_only, summary_only, fit_precision="fp64", seeds="threshold", peak_min_distance=None,
+                 smooth_sigma=0.0):
     started = time.perf_counter()
     seconds = {}
     height, width = tuple(img.shape)
@@ -350,52 +360,72 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         img_d = img.contiguous()
     else:
         img_d = dev.upload(img if img.dtype in _lib.DTYPES else img.astype(np.float64))
-    comp, rescaled = _segment(img_d, threshold, invert)
-    k = comp.count
-    components_before_filter = k
-    # Area filter, cell rows, border flags and oversized labels on the device (subpx/cd.py:485-500).
-    rows_d = dev.empty((max(k, 1), 6), torch.float64)
-    ids_d = dev.empty((max(k, 1),), torch.int32)
-    inside_d = dev.empty((max(k, 1),), torch.uint8)
-    oversized_flags_d = dev.empty((k + 1,), torch.uint8)
-    counts_d = dev.empty((2,), torch.int32)
-    ws = dev.workspace(_lib.size("spx_select_workspace_bytes", k))
-    _lib.call("spx_component_rows", comp.stats.data_ptr(), comp.centroids.data_ptr(), k, int(area_min), int(area_max),
-              width, height, rows_d.data_ptr(), ids_d.data_ptr(), inside_d.data_ptr(), oversized_flags_d.data_ptr(),
-              counts_d.data_ptr(), ws.data_ptr(), ws.numel(), dev.stream_ptr())
-    n_keep, n_oversized = (int(v) for v in counts_d.cpu().numpy())
-    rows_d = rows_d[:n_keep]
-    # Host copies land while the Voronoi cells are built (build_cells syncs before reading them).
-    rows = dev.start_download(rows_d)
-    component_ids = dev.start_download(ids_d[:n_keep])
-    interior_u8 = dev.start_download(inside_d[:n_keep])
-    labels_d = comp.labels
-    tmp8 = dev.empty((height, width), torch.uint8)
-    oversized_d = None
-    if n_oversized:
-        oversized_d = dev.empty((height, width), torch.uint8)
-        _lib.call("spx_label_mask", labels_d.data_ptr(), oversized_flags_d.data_ptr(), height, width, 0,
-                  oversized_d.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
-
-    def exclude_for(ids):
-        flags = np.ones(k + 1, np.uint8)
-        flags[0] = 0
-        ids = ids[(ids >= 0) & (ids <= k)]
-        flags[ids] = 0
-        out = dev.empty((height, width), torch.uint8)
-        _lib.call("spx_label_mask", labels_d.data_ptr(), dev.upload(flags).data_ptr(), height, width, 2,
-                  out.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
-        return out
-
     shape = tuple(img_d.shape)
-    cells = build_cells(rows, shape, pad, rows_d=rows_d)
-    rows = cells.rows
-    interior = interior_u8.view(np.bool_)  # 0 / 1 bytes
+    if seeds == "peaks":
+        # Peak seeds (subpx/cd.py:502-511): no components, nothing excluded from the background, the
+        # deblend's own tile, every hole reported by its fitted reach.
+        rows, pitch = _peak_rows(img_d, sign, peak_min_distance)
+        comp, rescaled, k, components_before_filter = None, False, 0, 0
+        component_ids = np.full(len(rows), -1, np.int32)
+        oversized_d = None
+
+        def exclude_for(ids):
+            return None
+
+        cells = build_cells(rows, shape, pad)
+        rows = cells.rows
+        interior = np.ones(len(rows), bool)
+        by_reach = np.ones(len(rows), bool)
+        tile_px, tiled_seeds = None, None
+    else:
+        comp, rescaled = _segment(img_d, threshold, invert)
+        k = comp.count
+        components_before_filter = k
+        # Area filter, cell rows, border flags and oversized labels on the device (subpx/cd.py:485-500).
+        rows_d = dev.empty((max(k, 1), 6), torch.float64)
+        ids_d = dev.empty((max(k, 1),), torch.int32)
+        inside_d = dev.empty((max(k, 1),), torch.uint8)
+        oversized_flags_d = dev.empty((k + 1,), torch.uint8)
+        counts_d = dev.empty((2,), torch.int32)
+        ws = dev.workspace(_lib.size("spx_select_workspace_bytes", k))
+        _lib.call("spx_component_rows", comp.stats.data_ptr(), comp.centroids.data_ptr(), k, int(area_min), int(area_max),
+                  width, height, rows_d.data_ptr(), ids_d.data_ptr(), inside_d.data_ptr(), oversized_flags_d.data_ptr(),
+                  counts_d.data_ptr(), ws.data_ptr(), ws.numel(), dev.stream_ptr())
+        n_keep, n_oversized = (int(v) for v in counts_d.cpu().numpy())
+        rows_d = rows_d[:n_keep]
+        # Host copies land while the Voronoi cells are built (build_cells syncs before reading them).
+        rows = dev.start_download(rows_d)
+        component_ids = dev.start_download(ids_d[:n_keep])
+        interior_u8 = dev.start_download(inside_d[:n_keep])
+        labels_d = comp.labels
+        tmp8 = dev.empty((height, width), torch.uint8)
+        oversized_d = None
+        if n_oversized:
+            oversized_d = dev.empty((height, width), torch.uint8)
+            _lib.call("spx_label_mask", labels_d.data_ptr(), oversized_flags_d.data_ptr(), height, width, 0,
+                      oversized_d.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
+
+        def exclude_for(ids):
+            flags = np.ones(k + 1, np.uint8)
+            flags[0] = 0
+            ids = ids[(ids >= 0) & (ids <= k)]
+            flags[ids] = 0
+            out = dev.empty((height, width), torch.uint8)
+            _lib.call("spx_label_mask", labels_d.data_ptr(), dev.upload(flags).data_ptr(), height, width, 2,
+                      out.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
+            return out
+
+        cells = build_cells(rows, shape, pad, rows_d=rows_d)
+        rows = cells.rows
+        interior = interior_u8.view(np.bool_)  # 0 / 1 bytes
+        by_reach = np.zeros(len(rows), bool)
+        tile_px, pitch = auto_tile(cells.seeds_d, cells.n, shape)
+        tiled_seeds = cells
     seconds["segmentation"] = time.perf_counter() - started
     meta = {
-        "background": "model", "seeds": "threshold", "threshold": threshold, "invert": bool(invert),
+        "background": "model", "seeds": seeds, "threshold": threshold, "invert": bool(invert),
         "area_min": int(area_min), "area_max": int(area_max), "pad": int(pad), "n_angles": int(n_angles),
-        "radial_step": float(radial_step), "smooth_sigma": 0.0, "fit_fraction": float(fit_fraction),
+        "radial_step": float(radial_step), "smooth_sigma": float(smooth_sigma), "fit_fraction": float(fit_fraction),
         "cell_backend": "gpu", "measurement_backend": "gpu", "device": int(device),
         "metrics_only": bool(metrics_only), "summary_only": bool(summary_only),
         "deblend_tolerance": float(deblend_tolerance), "fit_precision": fit_precision,
@@ -404,17 +434,11 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         "coordinates": "global [x, y] pixels; images indexed [y, x]", "seconds": seconds,
     }
     start = time.perf_counter()
-    by_reach = np.zeros(len(rows), bool)
     level = None if background_level is None else sign * float(background_level)
 
     def make_deblender(cells_, tile):
         return Deblender(img_d, sign, cells_, exclude_d=exclude_for(component_ids), tile=tile,
                          background_level=level, tolerance=deblend_tolerance, fit_precision=fit_precision)
-
-    from .deblend import auto_tile
-
-    tile_px, pitch = auto_tile(cells.seeds_d, cells.n, shape)
-    tiled_seeds = cells
 
     def tile_for(cells_):
         if background_tile is not None or cells_ is not tiled_seeds:
@@ -493,9 +517,15 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
     if radial and nr:
         hb = _method_buffers(nr, n_angles, "halfmax", not metrics_only) if "halfmax" in radial else (None, None)
         gb = _method_buffers(nr, n_angles, "gradient", not metrics_only) if "gradient" in radial else (None, None)
-        ws = dev.workspace(_lib.size("spx_radial_workspace_bytes", c.hm, c.wm))
+        smooth_w, smooth_r = None, 0
+        if smooth_sigma > 0:
+            from .peaks import gaussian_weights
+
+            weights, smooth_r = gaussian_weights(smooth_sigma)
+            smooth_w = dev.upload(weights)
+        ws = dev.workspace(_lib.size("spx_radial_workspace_bytes", c.hm, c.wm, int(smooth_w is not None)))
         _lib.call("spx_radial_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(), report_d.data_ptr(),
-                  nr, c.hm, c.wm, width, n_angles, radial_step,
+                  nr, c.hm, c.wm, width, n_angles, radial_step, dev.ptr(smooth_w), smooth_r,
                   None if hb[1] is None else hb[1], None if gb[1] is None else gb[1], ws.data_ptr(), ws.numel(),
                   stream)
         if hb[0] is not None:
@@ -561,7 +591,9 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         rois = cleaned.cpu().numpy()
         masks = _mask_stack(c, report)
     result = CDResult(
-        image=img_d.cpu().numpy() if isinstance(img, torch.Tensor) else img.copy(), binary=comp.labels.cpu().numpy() > 0, component_labels=comp.labels.cpu().numpy(),
+        image=img_d.cpu().numpy() if isinstance(img, torch.Tensor) else img.copy(),
+        binary=np.zeros(shape, bool) if comp is None else comp.labels.cpu().numpy() > 0,
+        component_labels=np.zeros(shape, np.int32) if comp is None else comp.labels.cpu().numpy(),
         component_ids=np.asarray(component_ids, dtype=np.int32)[report],
         boxes_xywh=rows[report, :4].astype(np.int32), seeds_xy=c.seeds[report], cell_labels=cell_labels,
         cell_areas_px2=np.bincount(cell_labels[cell_labels >= 0], minlength=nr), origins_xy=c.origins[report],

@@ -669,9 +669,23 @@ constexpr int kTrigMax = 256;  // ray angles with a cos / sin table in shared me
 
 // Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients in FP64 and in
 // FP32, a reduction area, then the cell mask and the eroded mask as bytes.
-__host__ __device__ inline long long radial_cta_doubles(int hm, int wm) {
+// With smoothing, three more hm x wm planes follow (the two axis-0 passes and the smoothed signal).
+__host__ __device__ inline long long radial_cta_doubles(int hm, int wm, bool smooth = false) {
     const long long np = (long long)(hm + 2 * kPad) * (wm + 2 * kPad);
-    return np + (np + 1) / 2 + 32 + (2LL * hm * wm + 7) / 8;
+    return np + (np + 1) / 2 + 32 + (2LL * hm * wm + 7) / 8 + (smooth ? 3LL * hm * wm : 0);
+}
+
+// One output of scipy's correlate1d with a symmetric kernel (weights w[0..2r], centre w[r]) and
+// mode="constant" (zero outside 0..n-1): the centre term first, then the pairs outermost inwards.
+__device__ __forceinline__ double sym_correlate_zero(const double* v, int pos, int n, int stride, const double* w,
+                                                     int r) {
+    double t = __dmul_rn(v[pos * stride], w[r]);
+    for (int k = r; k >= 1; --k) {
+        const double a = pos - k >= 0 ? v[(pos - k) * stride] : 0.0;
+        const double b = pos + k < n ? v[(pos + k) * stride] : 0.0;
+        t = __dadd_rn(t, __dmul_rn(__dadd_rn(a, b), w[r - k]));
+    }
+    return t;
 }
 
 // Sum over the CTA's 4 warps in a fixed order (the same value on every thread). Slots of `red`
@@ -764,9 +778,15 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
 // crossing and the parabolic maximum of the outward decrease (halfmax / gradient methods).
 // One 128-thread CTA per cell: the cell's masks and spline coefficients are staged once in
 // shared memory and each thread walks its own rays.
+// kSmooth: the mask-normalised Gaussian smoothing of subpx/_cpu/cd.py:206-208 (smooth_sigma > 0):
+// the signal (zero outside the cell) and the mask are each filtered along y then x with zero edges
+// (scipy's gaussian_filter, mode="constant"), and the spline is fitted to their ratio over the whole
+// cell box; the centroid still comes from the unsmoothed signal.
+template <bool kSmooth>
 __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
-    int n_angles, double radial_step, int n_radii, double* coef_scratch, MethodOut half_out, MethodOut grad_out) {
+    int n_angles, double radial_step, int n_radii, const double* smooth_w, int smooth_r, double* coef_scratch,
+    MethodOut half_out, MethodOut grad_out) {
     extern __shared__ double sm[];
     __shared__ double trig_tab[2 * kTrigMax];  // cos, sin of the ray angles (n_angles <= kTrigMax)
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -778,7 +798,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
             trig_tab[2 * a] = cos(ang);
             trig_tab[2 * a + 1] = sin(ang);
         }
-    double* coef = coef_scratch ? coef_scratch + (long long)blockIdx.x * radial_cta_doubles(hm, wm) : sm;
+    double* coef = coef_scratch ? coef_scratch + (long long)blockIdx.x * radial_cta_doubles(hm, wm, kSmooth) : sm;
     float* coef_f = reinterpret_cast<float*>(coef + (long long)hp * wp);
     double* red = coef + (long long)hp * wp + ((long long)hp * wp + 1) / 2;  // 32 doubles: 8 slots of 4
     uint8_t* mask = reinterpret_cast<uint8_t*>(red + 32);
@@ -822,9 +842,41 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         const double cx = cta_sum(swx, red + 12) / sw, cy = cta_sum(swy, red + 16) / sw;
         // Spline coefficients (the cell padded by 12 edge pixels) and the eroded cell (cross
         // structure, zero outside the stack), where ray samples stay valid.
-        for (int k = tid; k < hp * wp; k += kRadialThreads) {
-            const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
-            coef[k] = mask[yy * wm + xx] ? c.roi[yy * wm + xx] : 0.0;
+        if constexpr (kSmooth) {
+            double* ts = reinterpret_cast<double*>(mask) + (2LL * area_px + 7) / 8;  // after both masks
+            double* tm = ts + area_px;
+            double* fs = tm + area_px;
+            double* sig = coef;  // the masked signal, staged in the coefficient plane (hp * wp >= hm * wm)
+            for (int k = tid; k < area_px; k += kRadialThreads) sig[k] = mask[k] ? c.roi[k] : 0.0;
+            __syncthreads();
+            for (int k = tid; k < area_px; k += kRadialThreads) {
+                const int yy = k / wm, xx = k % wm;
+                ts[k] = sym_correlate_zero(sig + xx, yy, hm, wm, smooth_w, smooth_r);
+                double t = mask[k] ? smooth_w[smooth_r] : 0.0;
+                for (int q = smooth_r; q >= 1; --q) {
+                    const double a = yy - q >= 0 && mask[k - q * wm] ? 1.0 : 0.0;
+                    const double b = yy + q < hm && mask[k + q * wm] ? 1.0 : 0.0;
+                    t = __dadd_rn(t, __dmul_rn(__dadd_rn(a, b), smooth_w[smooth_r - q]));
+                }
+                tm[k] = t;
+            }
+            __syncthreads();
+            for (int k = tid; k < area_px; k += kRadialThreads) {
+                const int yy = k / wm, xx = k % wm;
+                const double num = sym_correlate_zero(ts + yy * wm, xx, wm, 1, smooth_w, smooth_r);
+                const double den = sym_correlate_zero(tm + yy * wm, xx, wm, 1, smooth_w, smooth_r);
+                fs[k] = num / fmax(den, 1e-12);
+            }
+            __syncthreads();
+            for (int k = tid; k < hp * wp; k += kRadialThreads) {
+                const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
+                coef[k] = fs[yy * wm + xx];
+            }
+        } else {
+            for (int k = tid; k < hp * wp; k += kRadialThreads) {
+                const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
+                coef[k] = mask[yy * wm + xx] ? c.roi[yy * wm + xx] : 0.0;
+            }
         }
         for (int k = tid; k < area_px; k += kRadialThreads) {
             const int yy = k / wm, xx = k % wm;
@@ -1017,25 +1069,56 @@ int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, 
 }
 
 // Shared memory of one radial CTA, or 0 when it does not fit and the CTAs use global scratch.
-static size_t radial_smem(int hm, int wm) {
-    const size_t bytes = (size_t)radial_cta_doubles(hm, wm) * sizeof(double);
+static size_t radial_smem(int hm, int wm, bool smooth) {
+    const size_t bytes = (size_t)radial_cta_doubles(hm, wm, smooth) * sizeof(double);
     return bytes <= 220 * 1024 ? bytes : 0;
 }
 
 constexpr int kRadialScratchCtas = 148 * 4;
 
-size_t spx_radial_workspace_bytes(int hm, int wm) {
-    if (radial_smem(hm, wm)) return 256;
-    return (size_t)kRadialScratchCtas * radial_cta_doubles(hm, wm) * sizeof(double) + 256;
+size_t spx_radial_workspace_bytes(int hm, int wm, int smooth) {
+    if (radial_smem(hm, wm, smooth != 0)) return 256;
+    return (size_t)kRadialScratchCtas * radial_cta_doubles(hm, wm, smooth != 0) * sizeof(double) + 256;
 }
 
+}  // extern "C"
+
+template <bool kSmooth>
+static int launch_radial(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
+                         int wm, int width, int n_angles, double radial_step, int n_radii, const double* smooth_w,
+                         int smooth_r, const spx_method_out* halfmax, const spx_method_out* gradient, void* workspace,
+                         cudaStream_t s) {
+    const size_t smem = radial_smem(hm, wm, kSmooth);
+    double* scratch = nullptr;
+    int blocks;
+    if (smem) {
+        if (smem + 2 * kTrigMax * sizeof(double) > 48 * 1024)  // with the static cos / sin table
+            SPX_CUDA(cudaFuncSetAttribute(k_radial_cd<kSmooth>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+        int per_sm = 0;
+        SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd<kSmooth>, kRadialThreads, smem));
+        blocks = (int)std::min<long long>(n, 148LL * std::max(per_sm, 1));
+    } else {
+        scratch = static_cast<double*>(workspace);
+        blocks = std::min(n, kRadialScratchCtas);
+    }
+    k_radial_cd<kSmooth><<<blocks, kRadialThreads, smem, s>>>(
+        cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm, wm, width, n_angles, radial_step, n_radii,
+        smooth_w, smooth_r, scratch, method_out(halfmax), method_out(gradient));
+    return check_launch("k_radial_cd");
+}
+
+extern "C" {
+
 int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
-                  int wm, int width, int n_angles, double radial_step, const spx_method_out* halfmax,
-                  const spx_method_out* gradient, void* workspace, size_t workspace_bytes, void* stream) {
-    SPX_REQUIRE(n >= 0 && n_angles >= 1 && radial_step > 0, "bad arguments");
+                  int wm, int width, int n_angles, double radial_step, const double* smooth_weights,
+                  int smooth_radius, const spx_method_out* halfmax, const spx_method_out* gradient, void* workspace,
+                  size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(n >= 0 && n_angles >= 1 && radial_step > 0 && smooth_radius >= 0, "bad arguments");
     if (n == 0) return SPX_OK;
     SPX_REQUIRE(cleaned && voronoi && boxes && (halfmax || gradient), "null pointer");
-    SPX_REQUIRE(workspace_bytes >= spx_radial_workspace_bytes(hm, wm), "workspace too small");
+    const bool smooth = smooth_weights != nullptr;
+    SPX_REQUIRE(workspace_bytes >= spx_radial_workspace_bytes(hm, wm, smooth), "workspace too small");
     for (const spx_method_out* o : {halfmax, gradient})
         if (o) SPX_REQUIRE(o->centers && o->status && o->metrics && o->center_local && o->edge_px && o->n_metrics >= 8,
                            "null pointer or too few metric columns");
@@ -1043,23 +1126,11 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
     // radii = np.arange(0, hypot(hm, wm) + step, step)
     const double stop = hypot((double)hm, (double)wm) + radial_step;
     const int n_radii = (int)ceil(stop / radial_step);
-    const size_t smem = radial_smem(hm, wm);
-    double* scratch = nullptr;
-    int blocks;
-    if (smem) {
-        if (smem + 2 * kTrigMax * sizeof(double) > 48 * 1024)  // with the static cos / sin table
-            SPX_CUDA(cudaFuncSetAttribute(k_radial_cd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = 0;
-        SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd, kRadialThreads, smem));
-        blocks = (int)std::min<long long>(n, 148LL * std::max(per_sm, 1));
-    } else {
-        scratch = static_cast<double*>(workspace);
-        blocks = std::min(n, kRadialScratchCtas);
-    }
-    k_radial_cd<<<blocks, kRadialThreads, smem, s>>>(cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n,
-                                                      hm, wm, width, n_angles, radial_step, n_radii, scratch,
-                                                      method_out(halfmax), method_out(gradient));
-    return check_launch("k_radial_cd");
+    if (smooth)
+        return launch_radial<true>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles, radial_step, n_radii,
+                                   smooth_weights, smooth_radius, halfmax, gradient, workspace, s);
+    return launch_radial<false>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles, radial_step, n_radii,
+                                nullptr, 0, halfmax, gradient, workspace, s);
 }
 
 }  // extern "C"

@@ -327,6 +327,7 @@ struct WarmStart {
     double* background;
     uint8_t* fallback;
     double cost_tol;  // relative cost drop that ends a warm-started fit
+    double* cost;     // optional: the LM cost (sum of squared residuals) at each cell's returned params
 };
 
 // T: type of the staged cell values and of the LM's per-pixel arithmetic (double or float).
@@ -423,6 +424,7 @@ __global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a,
         const double cap = a.caps[j];
         const double amp_cap = 3.0 * fmax(amax, 1e-12);
         int it = 0, st = 0;
+        double final_cost = dnan();
         bool fell_back = false, done = false;
         if (warm.params && (!warm.ok || warm.ok[j])) {
             // Warm start: LM from the predicted params; kept when it meets the stop rule within
@@ -434,7 +436,8 @@ __global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a,
                 finite = finite && isfinite(q[i]);
             }
             if (finite && q[0] > 0.0) {
-                it = warp_lm_fit(q, v, xy, n, cap, amp_cap, a.max_iter, lane, lm_slots[warp], warm.cost_tol);
+                it = warp_lm_fit(q, v, xy, n, cap, amp_cap, a.max_iter, lane, lm_slots[warp], warm.cost_tol,
+                                 &final_cost);
                 st = fit_status_of(q, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
                 if (it < a.max_iter && st == SPX_ST_OK) {
                     for (int i = 0; i < 6; ++i) p[i] = q[i];
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a,
             fell_back = !done;
         }
         if (!done) {
-            it += warp_lm_fit(p, v, xy, n, cap, amp_cap, a.max_iter, lane, lm_slots[warp], a.cost_tol);
+            it += warp_lm_fit(p, v, xy, n, cap, amp_cap, a.max_iter, lane, lm_slots[warp], a.cost_tol, &final_cost);
             st = fit_status_of(p, cap, j, box, a.hm, a.wm, a.vor, a.img.W);
         }
         if (lane == 0) {
@@ -453,6 +456,7 @@ __global__ void __launch_bounds__(kFitWarpsMax * 32, 2) k_fit_initial(FitArgs a,
             if (iters) iters[j] = it;
             if (warm.background) warm.background[j] = bg0;
             if (warm.fallback) warm.fallback[j] = fell_back;
+            if (warm.cost) warm.cost[j] = final_cost;
         }
         __syncwarp();
     }
@@ -1199,7 +1203,7 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
                         size_t workspace_bytes, void* stream) {
     return spx_deblend_initial_warm(img, dtype, sign, height, width, voronoi, boxes, caps, seeds, n, hm, wm,
                                     max_cell_pixels, background_level, has_level, max_iter, nullptr, nullptr, 1e-12,
-                                    params, status, iterations, nullptr, nullptr, nullptr, workspace,
+                                    params, status, iterations, nullptr, nullptr, nullptr, nullptr, workspace,
                                     workspace_bytes, stream);
 }
 
@@ -1276,8 +1280,8 @@ int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height
                              int max_cell_pixels, double background_level, int has_level, int max_iter,
                              const double* init_params, const uint8_t* init_ok, double warm_cost_tol,
                              double* params, uint8_t* status, int* iterations, double* background_out,
-                             uint8_t* fallback_out, const spx_fit_options* options, void* workspace,
-                             size_t workspace_bytes, void* stream) {
+                             uint8_t* fallback_out, double* cost_out, const spx_fit_options* options,
+                             void* workspace, size_t workspace_bytes, void* stream) {
     SPX_REQUIRE(warm_cost_tol > 0.0, "warm_cost_tol must be positive");
     SPX_REQUIRE(n >= 0 && height > 0 && width > 0 && max_iter >= 1, "bad arguments");
     bool f32 = false;
@@ -1292,7 +1296,7 @@ int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height
     FitLayout L = fit_layout(workspace, cap_px, nullptr);
     FitArgs a{Image{img, dtype, sign, height, width}, voronoi, reinterpret_cast<const int4*>(boxes), caps, n,
               hm, wm, cap_px, max_iter, cost_tol, nullptr, nullptr, nullptr, rows_per_image};
-    const WarmStart warm{init_params, init_ok, background_out, fallback_out, warm_cost_tol};
+    const WarmStart warm{init_params, init_ok, background_out, fallback_out, warm_cost_tol, cost_out};
     return f32 ? launch_fit_initial<float>(a, L, s, seeds, background_level, has_level, params, status, iterations,
                                            warm)
                : launch_fit_initial<double>(a, L, s, seeds, background_level, has_level, params, status,

@@ -7,7 +7,8 @@
 //
 // The Gaussian filter is separable (axis 0, then axis 1) with scipy's symmetric correlate1d sum:
 // centre term first, then the pairs (in[-k] + in[k]) * w[k] from the outermost inwards, edges
-// replicated. The maximum filter is exact in any order.
+// replicated. The maximum and minimum filters (also detect_peaks' prominence window,
+// subpx/_cpu/deblend.py:620) are exact in any order.
 
 #include "common.cuh"
 
@@ -38,6 +39,15 @@ struct MaxOp {
     __device__ __forceinline__ double operator()(const double* v, int stride) const {
         double m = -dinf();
         for (int o = -r; o <= r; ++o) m = fmax(m, v[o * stride]);
+        return m;
+    }
+};
+
+struct MinOp {
+    int r;
+    __device__ __forceinline__ double operator()(const double* v, int stride) const {
+        double m = dinf();
+        for (int o = -r; o <= r; ++o) m = fmin(m, v[o * stride]);
         return m;
     }
 };
@@ -86,17 +96,18 @@ __global__ void k_gauss_1d(const double* in, int H, int W, const double* w, int 
     }
 }
 
-__global__ void k_max_1d(const double* in, int H, int W, int r, int along_y, double* out) {
+// Direct maximum (lowest = false) or minimum (lowest = true) pass.
+__global__ void k_max_1d(const double* in, int H, int W, int r, int along_y, bool lowest, double* out) {
     const long long total = (long long)H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
         int y, x;
         divmod_idx(i, W, &y, &x);
-        double m = -dinf();
+        double m = lowest ? dinf() : -dinf();
         for (int o = -r; o <= r; ++o) {
             const double v = along_y ? in[(long long)min(max(y + o, 0), H - 1) * W + x]
                                      : in[(long long)y * W + min(max(x + o, 0), W - 1)];
-            m = fmax(m, v);
+            m = lowest ? fmin(m, v) : fmax(m, v);
         }
         out[i] = m;
     }
@@ -210,9 +221,25 @@ int spx_maximum_filter(const double* in, int height, int width, int radius, doub
         if (int e = filter_pass(in, height, width, radius, 1, op, tmp, s, "k_filter_y<max>")) return e;
         return filter_pass(tmp, height, width, radius, 0, op, out, s, "k_filter_x<max>");
     }
-    k_max_1d<<<grid_for(n, 256), 256, 0, s>>>(in, height, width, radius, 1, tmp);
+    k_max_1d<<<grid_for(n, 256), 256, 0, s>>>(in, height, width, radius, 1, false, tmp);
     if (int e = check_launch("k_max_1d")) return e;
-    k_max_1d<<<grid_for(n, 256), 256, 0, s>>>(tmp, height, width, radius, 0, out);
+    k_max_1d<<<grid_for(n, 256), 256, 0, s>>>(tmp, height, width, radius, 0, false, out);
+    return check_launch("k_max_1d");
+}
+
+int spx_minimum_filter(const double* in, int height, int width, int radius, double* tmp, double* out, void* stream) {
+    SPX_REQUIRE(height > 0 && width > 0 && radius >= 0, "bad arguments");
+    SPX_REQUIRE(in && tmp && out && tmp != in && tmp != out, "null or aliased pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long n = (long long)height * width;
+    if (radius <= kFilterMaxR && height <= 65535) {
+        const MinOp op{radius};
+        if (int e = filter_pass(in, height, width, radius, 1, op, tmp, s, "k_filter_y<min>")) return e;
+        return filter_pass(tmp, height, width, radius, 0, op, out, s, "k_filter_x<min>");
+    }
+    k_max_1d<<<grid_for(n, 256), 256, 0, s>>>(in, height, width, radius, 1, true, tmp);
+    if (int e = check_launch("k_max_1d")) return e;
+    k_max_1d<<<grid_for(n, 256), 256, 0, s>>>(tmp, height, width, radius, 0, true, out);
     return check_launch("k_max_1d");
 }
 

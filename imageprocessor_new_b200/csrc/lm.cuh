@@ -226,12 +226,15 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const float*
 // arithmetic of every sum is that of separate Jacobian and cost passes.
 // `cost_tol` is the relative cost drop at or below which an accepted step ends the fit (1e-12, the
 // reference's rule, by default).
+// `final_cost` (optional) receives the cost at the returned params (the same on every lane).
 template <typename T>
 __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, double cap, double amp_cap,
-                                  int max_iter, int lane, double* slots, double cost_tol = 1e-12) {
+                                  int max_iter, int lane, double* slots, double cost_tol = 1e-12,
+                                  double* final_cost = nullptr) {
     double s[27];
     int kept = 0;
     double cost = warp_normal_pass(p, v, xy, n, lane, s, slots);
+    if (final_cost) *final_cost = cost;
     if (!isfinite(cost)) return 0;
     double lam = 1e-3;
     const double lo = -log(cap), hi = -log(kSigmaMin);
@@ -273,6 +276,7 @@ __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, d
         }
     }
     __syncwarp();
+    if (final_cost) *final_cost = cost;
     return it;
 }
 

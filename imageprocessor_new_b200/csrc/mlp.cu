@@ -102,7 +102,11 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
         const int kn = kb + kGemmStages - 1;  // block to fetch now, into the stage block kb - 1 used
         if (kn < nk) {
             const int sn = kn % kGemmStages;
-            if (kb >= 1) ok = ok && mbar_wait(&mbar[sn], ((kb - 1) / kGemmStages) & 1, kWaitLimit);
+            // Every thread polls with its own bounded wait; the outcome is made block-uniform so that
+            // either all threads refill the stage or none does (a stage the MMA may still read is
+            // never overwritten), and the loop is left by all threads together.
+            if (kb >= 1) ok = __syncthreads_and(mbar_wait(&mbar[sn], ((kb - 1) / kGemmStages) & 1, kWaitLimit)) != 0;
+            if (!ok) break;
             load_tile(stage_a(sn), A, lda, m0, kGemmBM, M, kn, K);
             load_tile(stage_b(sn), B, ldb, n0, BN, N, kn, K);
         }
@@ -121,8 +125,11 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16(const __nv_bfloat16*
             umma_commit(&mbar[s]);
         }
     }
-    // The last commit covers every MMA of the tile.
-    ok = mbar_wait(&mbar[(nk - 1) % kGemmStages], ((nk - 1) / kGemmStages) & 1, kWaitLimit) && ok;
+    // The last commit covers every MMA of the tile. `ok` is block-uniform here and after the wait, so
+    // the warp-collective tcgen05.ld of the epilogue runs with whole warps or not at all.
+    if (ok) ok = __syncthreads_and(mbar_wait(&mbar[(nk - 1) % kGemmStages], ((nk - 1) / kGemmStages) & 1,
+                                             kWaitLimit)) != 0;
+    asm volatile("cp.async.wait_all;\n" ::: "memory");  // no copy into shared memory outlives the block
     tc_fence_after();
     if (!ok && threadIdx.x == 0) atomicExch(err, 1);
 

@@ -70,7 +70,7 @@ __device__ __forceinline__ unsigned int px_u(const void* img, int dtype, long lo
 // range[0] = min, range[1] = max of the sampled pixels (range must be preset to {~0u, 0}).
 __global__ void k_minmax(const void* img, int dtype, int height, int width, int step,
                          unsigned int* range) {
-    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const int hs = (int)(((long long)height + step - 1) / step), ws = (int)(((long long)width + step - 1) / step);
     const long long n = (long long)hs * ws;
     unsigned int lo = 0xffffffffu, hi = 0;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n;
@@ -137,7 +137,7 @@ __global__ void k_histogram(const void* img, int dtype, int height, int width, i
         for (unsigned int i = threadIdx.x; i < nb; i += blockDim.x) sh[i] = 0;
         __syncthreads();
     }
-    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const int hs = (int)(((long long)height + step - 1) / step), ws = (int)(((long long)width + step - 1) / step);
     const long long n = (long long)hs * ws;
     if (dense) {
         // 16-byte loads of 8 pixels, then the ragged tail.
@@ -834,7 +834,9 @@ __global__ void k_zero_u32(unsigned int* p, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0u;
 }
 
-// Device address of g_otsu_static for the current device, looked up once per device.
+// Device address of g_otsu_static for the current device, looked up once per device and kept for the
+// life of the process: a cudaDeviceReset (which unloads this module's device copy) invalidates it,
+// so the library must not be used across one.
 int otsu_static_scratch(void** out) {
     static std::mutex mu;
     static void* cache[128] = {};
@@ -983,7 +985,7 @@ int spx_otsu(const void* img, int dtype, int height, int width, int step, double
     SPX_CUDA(cudaMemsetAsync(hist, 0, 65536 * sizeof(unsigned int), s));
     const unsigned int init[2] = {0xffffffffu, 0u};
     SPX_CUDA(cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const int hs = (int)(((long long)height + step - 1) / step), ws = (int)(((long long)width + step - 1) / step);
     const long long n = (long long)hs * ws;
     if (int e = launch_minmax(img, dtype, height, width, step, n, range, s)) return e;
     const size_t smem = kHistSmemBins * sizeof(unsigned int);
@@ -1007,7 +1009,7 @@ int spx_histogram(const void* img, int dtype, int height, int width, int step, u
     SPX_CUDA(cudaMemsetAsync(hist, 0, 65536 * sizeof(unsigned int), s));
     const unsigned int init[2] = {0xffffffffu, 0u};
     SPX_CUDA(cudaMemcpyAsync(range, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    const int hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const int hs = (int)(((long long)height + step - 1) / step), ws = (int)(((long long)width + step - 1) / step);
     const long long n = (long long)hs * ws;
     if (int e = launch_minmax(img, dtype, height, width, step, n, range, s)) return e;
     const size_t smem = kHistSmemBins * sizeof(unsigned int);
@@ -1037,7 +1039,7 @@ int spx_otsu_from_histogram(const unsigned int* hist, int dtype, const unsigned 
 int spx_otsu_static(const void* img, int dtype, int height, int width, int step, double* threshold, void* stream) {
     SPX_REQUIRE(dtype == SPX_U8 || dtype == SPX_U16, "Otsu thresholding needs a uint8 or uint16 image");
     SPX_REQUIRE(height > 0 && width > 0 && step >= 1, "bad image size or step");
-    const long long hs = (height + step - 1) / step, ws = (width + step - 1) / step;
+    const long long hs = ((long long)height + step - 1) / step, ws = ((long long)width + step - 1) / step;
     SPX_REQUIRE(hs * ws <= 0xffffffffLL,
                 "spx_otsu_static: %lld sampled pixels exceed the maximum of 4294967295 (32-bit histogram counts)",
                 hs * ws);

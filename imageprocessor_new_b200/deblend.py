@@ -99,13 +99,19 @@ def auto_tile(seeds_d: torch.Tensor, n: int, shape) -> tuple[int, float]:
     return int(np.clip(round(4 * pitch), 16, max(shape))), pitch
 
 
-def quantiles(reqs) -> np.ndarray:
-    """Run spx_quantiles on a list of _lib.QuantileReq; (len, 2) array of (value, count)."""
+def quantile_device(*reqs) -> torch.Tensor:
+    """Run spx_quantiles on _lib.QuantileReq requests; a (len, 2) device array of (value, count),
+    left on the device (nothing synchronises)."""
     arr = (_lib.QuantileReq * len(reqs))(*reqs)
     raw = dev.upload(np.frombuffer(bytes(arr), dtype=np.uint8))
     out = dev.empty((len(reqs), 2), torch.float64)
     _lib.call("spx_quantiles", raw.data_ptr(), len(reqs), out.data_ptr(), dev.stream_ptr())
-    return out.cpu().numpy()
+    return out
+
+
+def quantiles(reqs) -> np.ndarray:
+    """Run spx_quantiles on a list of _lib.QuantileReq; (len, 2) array of (value, count)."""
+    return quantile_device(*reqs).cpu().numpy()
 
 
 def sigma_major(params: np.ndarray) -> np.ndarray:
@@ -405,7 +411,7 @@ class Deblender:
                   c.boxes.data_ptr(), c.caps.data_ptr(), c.seeds_d.data_ptr(), self.n, c.hm, c.wm, c.max_px,
                   float(self.background_level) if has else 0.0, int(has), int(max_iter), _ptr(warm_params),
                   _ptr(warm_ok), float(warm_cost_tol), params.data_ptr(), status.data_ptr(), iters.data_ptr(),
-                  _ptr(bg0), _ptr(fell), self.fit_options,
+                  _ptr(bg0), _ptr(fell), None, self.fit_options,
                   self.fit_ws.data_ptr(), self.fit_ws.numel(), dev.stream_ptr())
         if extras:
             return params, status, iters, bg0, fell

@@ -135,19 +135,33 @@ def page_staggered(seed: int = 0, shape=(8192, 8192)) -> Page:
     return Page(img, centers, d, dict(name="page_staggered", pitch=24.0, sigma=1.2, seed=seed))
 
 
-def gaussian_lattice(ratio: float, *, snr: float = 20, shape=(120, 240), seed: int = 0, fwhm: float = 4.0):
-    """Staggered Gaussian spots (amplitude 50 on 20) with a 15 px margin, as the reference's GPU tests
-    build them (tests/test_cd_gpu.py:23-35). Returns (float64 image, centers)."""
+def gaussian_lattice(ratio: float, *, snr: float = 20, shape=(120, 240), seed: int = 0, fwhm: float = 4.0,
+                     missing: float = 0.0, small: int = 0, faint: int = 0, faint_amplitude: float = 0.28):
+    """Staggered Gaussian spots (amplitude 50 on 20) with a 15 px margin, as the reference's tests
+    build them (tests/test_cd_gpu.py:23-35, tests/test_deblend.py:15-33). ``missing`` drops that
+    fraction of the spots at random; ``small`` interior spots get sigma 1.1 px (thresholding misses
+    them, tests/test_deblend_variants.py:27-43) and ``faint`` others get ``faint_amplitude`` x the
+    amplitude (peak seeding finds them, seed revision drops them). Returns (float64 image, centers)."""
     rng = np.random.default_rng(seed)
-    pitch, sigma = ratio * fwhm, fwhm / (2 * np.sqrt(2 * np.log(2)))
+    pitch, sigma0 = ratio * fwhm, fwhm / (2 * np.sqrt(2 * np.log(2)))
     xx, yy = np.meshgrid(np.arange(15, shape[1] - 15, pitch), np.arange(15, shape[0] - 15, pitch))
     xx[1::2] += pitch / 2
     centers = np.column_stack((xx.ravel(), yy.ravel()))
     centers = centers[centers[:, 0] < shape[1] - 15]
+    if missing:
+        centers = centers[rng.random(len(centers)) >= missing]
+    sigma = np.full(len(centers), sigma0)
+    amp = np.full(len(centers), 50.0)
+    if small or faint:
+        inner = np.flatnonzero((np.abs(centers[:, 0] - shape[1] / 2) < shape[1] / 2 - 40)
+                               & (np.abs(centers[:, 1] - shape[0] / 2) < shape[0] / 2 - 30))
+        pick = rng.choice(inner, small + faint, replace=False)
+        sigma[pick[:small]] = 1.1
+        amp[pick[small:]] *= faint_amplitude
     y, x = np.indices(shape, dtype=float)
     image = np.full(shape, 20.0)
-    for cx, cy in centers:
-        image += 50 * np.exp(-0.5 * ((x - cx) ** 2 + (y - cy) ** 2) / sigma**2)
+    for (cx, cy), s, a in zip(centers, sigma, amp):
+        image += a * np.exp(-0.5 * ((x - cx) ** 2 + (y - cy) ** 2) / s**2)
     return image + (rng.normal(0, 50 / snr, shape) if snr else 0), centers
 
 

@@ -344,13 +344,17 @@ def page_cells(page_d: torch.Tensor, *, area_min: int = 10, area_max: int = 2000
 
 
 def initial_fits(page_d: torch.Tensor, cells, *, sign: float = 1.0, max_iter: int = 30, warm=None,
-                 cost_tol: float = 1e-12, precision: str = "fp64", rows_per_image: int = 0):
+                 cost_tol: float = 1e-12, precision: str = "fp64", rows_per_image: int = 0,
+                 plain_cost_tol: float | None = None, costs: torch.Tensor | None = None):
     """The initial LM fits of the cells (plain, or warm-started with (params, ok)) in the given LM
     arithmetic: params, status, iterations, cell-border backgrounds and fallback flags (device).
-    rows_per_image > 0: the page is a stack of such images (boxes in stack rows, seeds in image rows)."""
+    rows_per_image > 0: the page is a stack of such images (boxes in stack rows, seeds in image rows).
+    plain_cost_tol: the plain-start fits' relative cost-drop stop rule (default: the arithmetic's,
+    1e-12 in FP64, the reference's); costs: a (n,) float64 device tensor that receives each fit's
+    converged LM cost."""
     from .deblend import fit_options
 
-    opts = fit_options(precision)
+    opts = fit_options(precision, plain_cost_tol)
     opts.rows_per_image = int(rows_per_image)
     cost_tol = max(float(cost_tol), opts.cost_tol)
     n = cells.n
@@ -367,7 +371,8 @@ def initial_fits(page_d: torch.Tensor, cells, *, sign: float = 1.0, max_iter: in
               cells.hm, cells.wm, cells.max_px, 0.0, 0, int(max_iter), None if wp is None else wp.data_ptr(),
               None if wo is None else wo.data_ptr(), float(cost_tol), params.data_ptr(), status.data_ptr(),
               iters.data_ptr(),
-              bg0.data_ptr(), fell.data_ptr(), opts, ws.data_ptr(), ws.numel(), dev.stream_ptr())
+              bg0.data_ptr(), fell.data_ptr(), None if costs is None else costs.data_ptr(), opts, ws.data_ptr(),
+              ws.numel(), dev.stream_ptr())
     return params[:n], status[:n], iters[:n], bg0[:n], fell[:n]
 
 
@@ -435,26 +440,42 @@ def train(net: WarmStartNet, x: torch.Tensor, t: torch.Tensor, *, epochs: int = 
 
 def compare_on_page(net: WarmStartNet, page_d: torch.Tensor, *, max_iter: int = 30, repeats: int = 3,
                     cells=None, precision: str = "fp64") -> dict:
-    """Plain FP64 against warm-started initial fits (in `precision`) of one page's cells: LM
-    iterations, fallback share, centre deviation of the warm fits from the plain ones ("ok" in
-    both), and the device time of the LM stage (the warm time includes the patches and the MLP)."""
+    """The initial-fit stage of one page's cells in three arms, timed by CUDA events:
+
+      plain_ref   plain start, the reference's stop rule (relative cost drop 1e-12);
+      plain_loose plain start, the warm fits' stop rule (net.cost_tol, 1e-7): the like-for-like arm,
+                  so warm over plain_loose is what the network alone gains;
+      warm        patches + MLP + warm-started LM (net.cost_tol) with the plain-start fallback.
+
+    Reported: LM iterations per arm, the fallback share, centre deviations of the loose arms from
+    plain_ref ("ok" in both), and the fallback rule's miss rate: the share of kept warm fits whose
+    converged LM cost exceeds the plain-start fit's under the same stop rule by more than ten times
+    that rule's relative drop (both fits stop within about one such drop of the optimum), i.e. cells
+    where "fall back whenever the warm fit's converged residual exceeds the plain fit's" would have
+    refitted but the cheaper rule used here (stop within max_iter and end "ok") did not."""
     cells = page_cells(page_d) if cells is None else cells
     n = cells.n
+    costs = {k: dev.empty((max(n, 1),), torch.float64) for k in ("plain_ref", "plain_loose", "warm")}
 
-    def plain():
-        return initial_fits(page_d, cells, max_iter=max_iter)
+    def plain_ref():
+        return initial_fits(page_d, cells, max_iter=max_iter, costs=costs["plain_ref"])
+
+    def plain_loose():
+        return initial_fits(page_d, cells, max_iter=max_iter, plain_cost_tol=net.cost_tol,
+                            costs=costs["plain_loose"])
 
     def warm():
         p0, ok = predict_init(net, page_d, 1.0, cells.seeds_d, cells.boxes, n)
         return initial_fits(page_d, cells, max_iter=max_iter, warm=(p0, ok), cost_tol=net.cost_tol,
-                            precision=precision)
+                            precision=precision, costs=costs["warm"])
 
-    for fn in (plain, warm):
+    arms = {"plain_ref": plain_ref, "plain_loose": plain_loose, "warm": warm}
+    for fn in arms.values():
         fn()
-    t = {"plain": 0.0, "warm": 0.0}
+    t = {k: 0.0 for k in arms}
     res = {}
     for _ in range(repeats):
-        for which, fn in (("plain", plain), ("warm", warm)):
+        for which, fn in arms.items():
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record()
             res[which] = fn()
@@ -462,34 +483,57 @@ def compare_on_page(net: WarmStartNet, page_d: torch.Tensor, *, max_iter: int = 
             torch.cuda.synchronize()
             t[which] += s.elapsed_time(e) / repeats
     net.check_errors()
-    pp, sp, ip, _, _ = (a.cpu().numpy() for a in res["plain"])
-    pw, sw, iw, _, fw = (a.cpu().numpy() for a in res["warm"])
-    both = (sp == 0) & (sw == 0)
-    dc = np.abs(pw[both, 1:3] - pp[both, 1:3]).max(axis=1) if both.any() else np.zeros(0)
-    return {"cells": int(n), "plain_iterations_mean": float(ip.mean()), "warm_iterations_mean": float(iw.mean()),
-            "fallback_fraction": float(fw.mean()), "same_status": float((sp == sw).mean()),
-            "centre_dev_max_px": float(dc.max()) if len(dc) else 0.0,
-            "within_1e-3_px": float((dc <= 1e-3).mean()) if len(dc) else 1.0,
-            "plain_ms": t["plain"], "warm_ms": t["warm"], "plain_cells_per_s": n / (t["plain"] / 1e3),
-            "warm_cells_per_s": n / (t["warm"] / 1e3), "speedup": t["plain"] / t["warm"]}
+    host = {k: [a.cpu().numpy() for a in v] for k, v in res.items()}
+    cost = {k: v[:n].cpu().numpy() for k, v in costs.items()}
+    pp, sp, ip = host["plain_ref"][:3]
+    out = {"cells": int(n)}
+    for k in ("plain_loose", "warm"):
+        pk, sk = host[k][:2]
+        both = (sp == 0) & (sk == 0)
+        dc = np.abs(pk[both, 1:3] - pp[both, 1:3]).max(axis=1) if both.any() else np.zeros(0)
+        out[f"{k}_centre_dev_max_px"] = float(dc.max()) if len(dc) else 0.0
+        out[f"{k}_within_1e-3_px"] = float((dc <= 1e-3).mean()) if len(dc) else 1.0
+        out[f"{k}_same_status"] = float((sp == sk).mean())
+    fw = host["warm"][4].astype(bool)
+    kept = ~fw & (host["warm"][1] == 0) & (host["plain_loose"][1] == 0)
+    excess = (cost["warm"] - cost["plain_loose"]) / np.maximum(cost["plain_loose"], 1e-300)
+    for k in arms:
+        out[f"{k}_iterations_mean"] = float(host[k][2].mean())
+        out[f"{k}_ms"] = t[k]
+        out[f"{k}_cells_per_s"] = n / (t[k] / 1e3)
+    out.update(
+        fallback_fraction=float(fw.mean()),
+        fallback_miss_rate=float((excess[kept] > 10 * net.cost_tol).mean()) if kept.any() else 0.0,
+        fallback_miss_excess_max=float(excess[kept].max()) if kept.any() else 0.0,
+        speedup_vs_plain_ref=t["plain_ref"] / t["warm"],
+        speedup_vs_plain_loose=t["plain_loose"] / t["warm"],
+        # names kept from the two-arm report: plain = the reference's stop rule
+        plain_ms=t["plain_ref"], warm_ms=t["warm"], speedup=t["plain_ref"] / t["warm"],
+        centre_dev_max_px=out["warm_centre_dev_max_px"],
+    )
+    return out
 
 
 def evaluate(net: WarmStartNet, *, pages: int = 2, size: int = 2048, seed: int = 999, max_iter: int = 30,
              repeats: int = 3) -> dict:
-    """compare_on_page over held-out synthetic pages, pooled (times summed, means cell-weighted)."""
+    """compare_on_page over held-out synthetic pages, pooled (times summed, means cell-weighted,
+    maxima over pages)."""
     rows = [compare_on_page(net, synth_page(seed * 7919 + k, size)[0], max_iter=max_iter, repeats=repeats)
             for k in range(pages)]
     n = sum(r["cells"] for r in rows)
     out = {"cells": n}
-    for key in ("plain_iterations_mean", "warm_iterations_mean", "fallback_fraction", "same_status",
-                "within_1e-3_px"):
+    arms = ("plain_ref", "plain_loose", "warm")
+    means = [f"{k}_iterations_mean" for k in arms] + ["fallback_fraction", "fallback_miss_rate"] + [
+        f"{k}_{q}" for k in arms[1:] for q in ("within_1e-3_px", "same_status")]
+    for key in means:
         out[key] = sum(r[key] * r["cells"] for r in rows) / max(n, 1)
-    out["centre_dev_max_px"] = max(r["centre_dev_max_px"] for r in rows)
-    out["plain_ms"] = sum(r["plain_ms"] for r in rows)
-    out["warm_ms"] = sum(r["warm_ms"] for r in rows)
-    out["plain_cells_per_s"] = n / (out["plain_ms"] / 1e3)
-    out["warm_cells_per_s"] = n / (out["warm_ms"] / 1e3)
-    out["speedup"] = out["plain_ms"] / out["warm_ms"]
+    for key in ["fallback_miss_excess_max"] + [f"{k}_centre_dev_max_px" for k in arms[1:]]:
+        out[key] = max(r[key] for r in rows)
+    for k in arms:
+        out[f"{k}_ms"] = sum(r[f"{k}_ms"] for r in rows)
+        out[f"{k}_cells_per_s"] = n / (out[f"{k}_ms"] / 1e3)
+    out["speedup_vs_plain_ref"] = out["plain_ref_ms"] / out["warm_ms"]
+    out["speedup_vs_plain_loose"] = out["plain_loose_ms"] / out["warm_ms"]
     return out
 
 

@@ -85,7 +85,8 @@ int spx_otsu(const void* img, int dtype, int height, int width, int step, double
  * in a 2.3 MiB file-scope device array that every GPU loading the library holds until exit.
  * Limit: at most 4294967295 sampled pixels (ceil(H/step) * ceil(W/step)), the range of the 32-bit
  * histogram counts; larger images are rejected with SPX_ERR_ARGUMENT. The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress), so make it before any stream capture.
+ * looks up the array's device address (cudaGetSymbolAddress), so make it before any stream capture;
+ * the address is kept until the process exits, so do not call it after a cudaDeviceReset.
  * All calls share the one array: calls that overlap on the GPU (other streams, other host threads)
  * race and must be serialised by the caller. Allocates nothing (no cudaMalloc, cudaFree or
  * allocating library call). */
@@ -258,16 +259,17 @@ int spx_deblend_initial(const void* img, int dtype, double sign, int height, int
  * an accepted step lowers the cost by at most warm_cost_tol relative (1e-12 is the plain rule),
  * max |step| < 1e-7 or the damping exceeds 1e12; that fit is kept when it stops within max_iter and ends "ok", otherwise
  * the plain start runs as well (fallback_out[j] = 1; iterations counts both). background_out[j]
- * receives the cell-border background the fit subtracted. options (null: FP64, cost_tol 1e-12)
- * sets the fits' arithmetic and the plain-start fits' stop rule. No reference counterpart (learned
- * warm start). */
+ * receives the cell-border background the fit subtracted and cost_out[j] (may be null) the LM cost
+ * (sum of squared residuals) at the returned params, so that a caller can compare a warm-started
+ * fit's converged cost with the plain fit's. options (null: FP64, cost_tol 1e-12) sets the fits'
+ * arithmetic and the plain-start fits' stop rule. No reference counterpart (learned warm start). */
 int spx_deblend_initial_warm(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                              const int* boxes, const double* caps, const double* seeds, int n, int hm, int wm,
                              int max_cell_pixels, double background_level, int has_level, int max_iter,
                              const double* init_params, const uint8_t* init_ok, double warm_cost_tol,
                              double* params, uint8_t* status, int* iterations, double* background_out,
-                             uint8_t* fallback_out, const spx_fit_options* options, void* workspace,
-                             size_t workspace_bytes, void* stream);
+                             uint8_t* fallback_out, double* cost_out, const spx_fit_options* options,
+                             void* workspace, size_t workspace_bytes, void* stream);
 /* One outer iteration: clean every cell against `model` and `background`, LM from `params`,
  * params_out = params + relaxation * (fitted - params), status of params_out, and maxstep =
  * max |step[1:]| (NaN unless the cell is ok with a finite fit). The cleaning is FP64 in both
@@ -343,6 +345,9 @@ int spx_gaussian_filter(const double* in, int height, int width, const double* w
                         double* out, void* stream);
 /* Separable maximum filter of size 2 radius + 1, nearest edges. */
 int spx_maximum_filter(const double* in, int height, int width, int radius, double* tmp, double* out, void* stream);
+/* Separable minimum filter of size 2 radius + 1, nearest edges (detect_peaks' prominence window,
+ * subpx/_cpu/deblend.py:620). */
+int spx_minimum_filter(const double* in, int height, int width, int radius, double* tmp, double* out, void* stream);
 /* Pixels where smooth == maxf, smooth > level and not exclude[i] (exclude may be null), appended as
  * (y, x) int pairs in any order; *count (device) receives the total (may exceed capacity). */
 int spx_find_peaks(const double* smooth, const double* maxf, const uint8_t* exclude, int height, int width,
@@ -351,6 +356,40 @@ int spx_find_peaks(const double* smooth, const double* maxf, const uint8_t* excl
  * (zero outside the image); tmp is an H x W byte scratch. */
 int spx_label_mask(const int* labels, const uint8_t* flags, int height, int width, int dilations, uint8_t* out,
                    uint8_t* tmp, void* stream);
+
+/* ------------------------------------------------------------------------------------------------
+ * Peak seeds for arrays too dense to threshold: measure_cds(seeds="peaks") (subpx/cd.py:502-511)
+ * with estimate_pitch and detect_peaks (subpx/_cpu/deblend.py:570-630).
+ * ---------------------------------------------------------------------------------------------- */
+
+/* out = sign * img as double (H x W), the signal the peak search and the pitch read. */
+int spx_signal_image(const void* img, int dtype, double sign, int height, int width, double* out, void* stream);
+size_t spx_pitch_workspace_bytes(int height, int width, int max_size);
+/* The centred crop of estimate_pitch (at most max_size x max_size, offsets max(0, (H - max_size) / 2)
+ * and likewise in x) times sign, minus its mean, in the top-left corner of `padded`, a zero
+ * (2 ch) x (2 cw) double array (ch, cw = the crop's size): the input of the caller's FFT. */
+int spx_pitch_crop(const void* img, int dtype, double sign, int height, int width, int max_size, double* padded,
+                   void* workspace, size_t workspace_bytes, void* stream);
+/* Pitch from the autocorrelation `autoc` (height2 x width2, zero lag at [0, 0], periodic, i.e. the
+ * inverse FFT of the padded crop's power spectrum before fftshift): means of the lags in integer
+ * radius bins 0..r_max (r_max = min(ch, cw) / 2), the first bin k >= 2 above its predecessor, at
+ * least its successor and positive, refined by a parabola. *pitch (device) = NaN when none is
+ * found. Uses the workspace of spx_pitch_crop. */
+int spx_pitch_from_autocorrelation(const double* autoc, int height2, int width2, int r_max, double* pitch,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+size_t spx_peak_workspace_bytes(int height, int width);
+/* Pixels with smooth == maxf and prominence smooth - minf > 0, as (y, x) int pairs with their
+ * prominence, in row-major order; *count (device) receives the total (may exceed capacity). */
+int spx_peak_candidates(const double* smooth, const double* maxf, const double* minf, int height, int width,
+                        int* out_yx, double* out_prom, int capacity, int* count, void* workspace,
+                        size_t workspace_bytes, void* stream);
+size_t spx_peak_select_workspace_bytes(int n);
+/* Candidates with prom >= fraction * (*level) (level: a device double, e.g. the 90th percentile of
+ * spx_quantiles), kept in order as [x, y] seeds moved by the parabola vertex of their row and column
+ * neighbours in `smooth`, clipped to +-0.5 px; *count (device) = the number kept. */
+int spx_peak_select(const int* yx, const double* prom, int n, const double* level, double fraction,
+                    const double* smooth, int height, int width, double* out_xy, int* count, void* workspace,
+                    size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------------------------------
  * CD measurements of cleaned cells (an (n, hm, wm) stack, zero outside each cell; cell i is cell
@@ -391,12 +430,15 @@ int spx_gaussian_method(const double* params, const uint8_t* status_in, const do
 int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, const double* seeds,
                    int n, int hm, int wm, int width, int n_angles, double fit_fraction, const spx_method_out* out,
                    void* stream);
-size_t spx_radial_workspace_bytes(int hm, int wm);
+size_t spx_radial_workspace_bytes(int hm, int wm, int smooth);
 /* Cubic-spline radial profiles; half-height crossings (halfmax) and gradient maxima (gradient).
- * Either output may be null. */
+ * Either output may be null. smooth_weights (device, 2 smooth_radius + 1 symmetric Gaussian
+ * weights, scipy's gaussian_filter kernel for smooth_sigma) selects the mask-normalised smoothing
+ * of the profiles (subpx/_cpu/cd.py:206-208); null for smooth_sigma = 0. */
 int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
-                  int wm, int width, int n_angles, double radial_step, const spx_method_out* halfmax,
-                  const spx_method_out* gradient, void* workspace, size_t workspace_bytes, void* stream);
+                  int wm, int width, int n_angles, double radial_step, const double* smooth_weights,
+                  int smooth_radius, const spx_method_out* halfmax, const spx_method_out* gradient, void* workspace,
+                  size_t workspace_bytes, void* stream);
 
 
 /* ------------------------------------------------------------------ learned warm start (MLP) */

@@ -89,13 +89,17 @@ def _logquad(roi, mask, seed, angles, fit_fraction):
     return center, contour, extra, "ok", (ev, ax)
 
 
-def _radial(roi, mask, angles, step):
-    from scipy.ndimage import binary_erosion, map_coordinates
+def _radial(roi, mask, angles, step, smooth_sigma=0.0):
+    from scipy.ndimage import binary_erosion, gaussian_filter, map_coordinates
 
     signal = np.where(mask, roi, 0)
     wgt = np.where(mask & (signal > 0.1 * signal.max()), signal, 0)
     yy, xx = np.indices(roi.shape)
     center = np.array([(wgt * xx).sum(), (wgt * yy).sum()]) / wgt.sum()
+    if smooth_sigma > 0:
+        # Mask-normalised smoothing (subpx/_cpu/cd.py:206-208); the centre comes from the raw signal.
+        support = gaussian_filter(mask.astype(float), smooth_sigma, mode="constant")
+        signal = gaussian_filter(signal, smooth_sigma, mode="constant") / np.maximum(support, 1e-12)
     radii = np.arange(0, np.hypot(*roi.shape) + step, step)
     dirs = np.column_stack((np.cos(angles), np.sin(angles)))
     pts = center + dirs[:, None, :] * radii[None, :, None]
@@ -150,7 +154,8 @@ def _new_method(method, n, n_angles):
             "edge_px": np.full((n, n_angles), np.nan)}
 
 
-def measure_cells(rois, masks, origins, seeds, *, methods, n_angles=128, radial_step=0.1, fit_fraction=0.2):
+def measure_cells(rois, masks, origins, seeds, *, methods, n_angles=128, radial_step=0.1, fit_fraction=0.2,
+                  smooth_sigma=0.0):
     n = len(rois)
     angles = np.arange(n_angles) * (2 * np.pi / n_angles)
     res = {m: _new_method(m, n, n_angles) for m in methods}
@@ -168,7 +173,7 @@ def measure_cells(rois, masks, origins, seeds, *, methods, n_angles=128, radial_
                 center, contour, met, st, _ = _logquad(roi, mask, seed - origin, angles, fit_fraction)
             else:
                 if radial is None:
-                    radial = _radial(roi, mask, angles, radial_step)
+                    radial = _radial(roi, mask, angles, radial_step, smooth_sigma)
                 center, contour, met, st, edge = _radial_edges(m, *radial, angles)
                 r["edge_px"][i] = edge
             r["centers"][i] = center + origin
@@ -233,12 +238,19 @@ def unmodelled(binary, labels, ids):
 
 def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), threshold="otsu", invert=False,
                 area_min=3, area_max=50, pad=3, n_angles=128, radial_step=0.1, fit_fraction=0.2,
-                deblend_iterations=30, deblend_tolerance=1e-3, background_level=None):
-    """The model-background measure_cds pipeline (seeds from thresholded components)."""
+                deblend_iterations=30, deblend_tolerance=1e-3, background_level=None, seeds="threshold",
+                peak_min_distance=None, smooth_sigma=0.0):
+    """The model-background measure_cds pipeline, seeds from thresholded components or, with
+    seeds="peaks", from the smoothed signal's maxima (subpx/cd.py:502-511)."""
     img = np.asarray(img)
     h, w = img.shape
     sign = -1.0 if invert else 1.0
     signal = img.astype(np.float64) * sign
+    if seeds == "peaks":
+        return _measure_peaks(img, signal, sign, methods=methods, pad=pad, n_angles=n_angles, radial_step=radial_step,
+                              fit_fraction=fit_fraction, deblend_iterations=deblend_iterations,
+                              deblend_tolerance=deblend_tolerance, background_level=background_level,
+                              peak_min_distance=peak_min_distance, smooth_sigma=smooth_sigma)
     seg = img
     if img.dtype != np.uint8 and not (img.dtype == np.uint16 and threshold == "otsu"):
         g = img.astype(np.float64)
@@ -265,15 +277,47 @@ def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), 
 
     seeds, cell_labels, masks, origins = build(rows)
     tile_px, pitch = odb.auto_tile(seeds, img.shape)
+    return _deblend_and_measure(img, signal, sign, rows, ids, interior, np.zeros(len(rows), bool), pitch,
+                                tile_px, unmodelled(binary, labels, ids), oversized, methods=methods, pad=pad,
+                                n_angles=n_angles, radial_step=radial_step, fit_fraction=fit_fraction,
+                                deblend_iterations=deblend_iterations, deblend_tolerance=deblend_tolerance,
+                                background_level=background_level, smooth_sigma=smooth_sigma)
+
+
+def _measure_peaks(img, signal, sign, *, peak_min_distance, **kw):
+    """seeds="peaks" (subpx/cd.py:502-511): square boxes of 2 ceil(0.6 pitch) + 1 around each peak,
+    no component ids, every hole reported by its fitted reach, no excluded features, and the
+    deblend's own tile rule."""
+    peaks, pitch = odb.detect_peaks(signal, min_distance=peak_min_distance)
+    half = int(np.ceil(0.6 * pitch))
+    rows = np.array([[cx - half, cy - half, 2 * half + 1, 2 * half + 1, cx, cy] for cx, cy in peaks],
+                    dtype=np.float64).reshape(-1, 6)
+    n = len(rows)
+    return _deblend_and_measure(img, signal, sign, rows, np.full(n, -1, np.int32), np.ones(n, bool),
+                                np.ones(n, bool), pitch, None, None, None, **kw)
+
+
+def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch, tile_px, exclude_mask, oversized, *,
+                         methods, pad, n_angles, radial_step, fit_fraction, deblend_iterations, deblend_tolerance,
+                         background_level, smooth_sigma):
+    """The deblend passes with seed revision and the measurements (subpx/cd.py:581-760)."""
+    h, w = img.shape
+
+    def build(rows_):
+        seeds_ = rows_[:, 4:6].copy()
+        lab_ = ov.voronoi_labels(seeds_, img.shape)
+        masks_, origins_ = cell_stack(lab_, rows_, pad, img.shape)
+        return seeds_, lab_, masks_, origins_
+
+    seeds, cell_labels, masks, origins = build(rows)
     tiled = seeds
-    by_reach = np.zeros(len(rows), bool)
     level = None if background_level is None else sign * float(background_level)
     passes, added, dropped = [], 0, 0
     state = None
     for revision in range(3):
-        exclude = unmodelled(binary, labels, ids)
+        exclude = exclude_mask
         final = revision == 2 or not np.isfinite(pitch)
-        tile = tile_px if seeds is tiled else None
+        tile = tile_px if (seeds is tiled and tile_px is not None) else None
         state = odb.deblend(signal, seeds, masks, origins, iterations=deblend_iterations if final else
                             min(10, deblend_iterations), tile=tile, exclude=exclude, background_level=level,
                             tolerance=deblend_tolerance)
@@ -308,7 +352,7 @@ def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), 
     cleaned = state.cleaned[report]
     measured = [m for m in methods if m != "gaussian"]
     out = measure_cells(cleaned, masks[report], origins[report], seeds[report], methods=measured, n_angles=n_angles,
-                        radial_step=radial_step, fit_fraction=fit_fraction) if measured else {}
+                        radial_step=radial_step, fit_fraction=fit_fraction, smooth_sigma=smooth_sigma) if measured else {}
     if "gaussian" in methods:
         out["gaussian"] = gaussian_method(state.params[report], state.status[report], cleaned, masks[report],
                                           origins[report], n_angles)
@@ -325,4 +369,4 @@ def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), 
     return {"seeds": seeds[report], "cell_labels": remap[cell_labels], "measurements": out, "params": params_global,
             "report": report, "passes": passes, "iterations_used": sum(passes), "added": added, "dropped": dropped,
             "source": state.background_info.get("source"), "background_map": sign * state.background_map,
-            "status": state.status[report]}
+            "status": state.status[report], "pitch": pitch}

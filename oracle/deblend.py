@@ -394,3 +394,63 @@ def revise_seeds(signal, state, seeds, pitch, *, drop_fraction=0.3, add_fraction
     if len(new) and len(kept):
         new = new[cKDTree(kept).query(new)[0] > 0.5 * pitch]
     return drop, new
+
+
+def estimate_pitch(signal, *, max_size=1024):
+    """Lattice pitch from the first ring of the radially averaged autocorrelation of a centred crop
+    (subpx/_cpu/deblend.py:570-590): zero-padded FFT autocorrelation, integer radius bins
+    (np.rint of the distance to the zero lag) up to half the crop, first local maximum k >= 2 of
+    the bin means refined by a parabola through its neighbours."""
+    h, w = signal.shape
+    y0, x0 = max(0, (h - max_size) // 2), max(0, (w - max_size) // 2)
+    crop = np.asarray(signal[y0:y0 + max_size, x0:x0 + max_size], dtype=np.float64)
+    crop = crop - crop.mean()
+    size = (2 * crop.shape[0], 2 * crop.shape[1])
+    auto = np.fft.fftshift(np.fft.irfft2(np.abs(np.fft.rfft2(crop, s=size)) ** 2, s=size))
+    cy, cx = np.array(auto.shape) // 2
+    yy, xx = np.indices(auto.shape)
+    bins = np.rint(np.hypot(yy - cy, xx - cx)).astype(int)
+    keep = bins <= int(min(crop.shape) // 2)
+    prof = np.bincount(bins[keep], weights=auto[keep]) / np.maximum(np.bincount(bins[keep]), 1)
+    for k in range(2, len(prof) - 1):
+        if prof[k] > prof[k - 1] and prof[k] >= prof[k + 1] and prof[k] > 0:
+            den = prof[k - 1] - 2 * prof[k] + prof[k + 1]
+            return float(k + (0.5 * (prof[k - 1] - prof[k + 1]) / den if den < 0 else 0.0))
+    raise ValueError("could not estimate the hole pitch; pass peak_min_distance explicitly")
+
+
+def detect_peaks(signal, *, min_distance=None, smooth_sigma=None, threshold=0.25):
+    """Local-maximum seeds of a dense array (subpx/_cpu/deblend.py:593-630): maxima of the smoothed
+    signal over a (2 floor(min_distance) + 1)^2 window whose prominence over the minimum of a
+    (2 ceil(pitch) + 1)^2 window is positive and at least `threshold` x its 90th percentile over
+    all maxima, in row-major order, each moved by the clipped parabola vertex of its row and column
+    neighbours. Returns (seeds_xy, pitch)."""
+    from scipy.ndimage import gaussian_filter, maximum_filter, minimum_filter
+
+    signal = np.asarray(signal, dtype=np.float64)
+    pitch = 2.0 * float(min_distance) if min_distance is not None else estimate_pitch(signal)
+    if min_distance is None:
+        min_distance = 0.5 * pitch
+    if smooth_sigma is None:
+        smooth_sigma = max(0.5, 0.1 * pitch)
+    smooth = gaussian_filter(signal, smooth_sigma, mode="nearest")
+    rad = max(1, int(np.floor(min_distance)))
+    is_max = smooth == maximum_filter(smooth, size=2 * rad + 1, mode="nearest")
+    prom = smooth - minimum_filter(smooth, size=2 * int(np.ceil(pitch)) + 1, mode="nearest")
+    ys, xs = np.nonzero(is_max & (prom > 0))
+    if len(xs) == 0:
+        return np.zeros((0, 2)), pitch
+    pv = prom[ys, xs]
+    keep = pv >= threshold * np.percentile(pv, 90)
+    ys, xs = ys[keep], xs[keep]
+    h, w = signal.shape
+    sub = np.column_stack((xs, ys)).astype(float)
+    for axis, (dy, dx) in enumerate(((0, 1), (1, 0))):
+        ok = (ys - dy >= 0) & (ys + dy < h) & (xs - dx >= 0) & (xs + dx < w)
+        left = smooth[np.clip(ys - dy, 0, h - 1), np.clip(xs - dx, 0, w - 1)]
+        mid = smooth[ys, xs]
+        right = smooth[np.clip(ys + dy, 0, h - 1), np.clip(xs + dx, 0, w - 1)]
+        curv = left - 2 * mid + right
+        delta = np.where(ok & (curv < 0), 0.5 * (left - right) / np.where(curv < 0, curv, -1), 0.0)
+        sub[:, axis] += np.clip(delta, -0.5, 0.5)
+    return sub, pitch

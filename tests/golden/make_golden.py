@@ -13,6 +13,7 @@ tests compare the oracle (CPU) and the CUDA library against them.
 from __future__ import annotations
 
 import argparse
+import json
 import sys
 from pathlib import Path
 
@@ -211,13 +212,24 @@ def cd_cases():
     cen = S.staggered_grid((192, 256), 24.0, rng)
     stag = S.add_noise(S.render((192, 256), cen, 12.0 * (1 + rng.uniform(-0.05, 0.05, len(cen))), 1.2,
                                 amplitude=3000.0, background=1000.0), rng, read_noise=100.0, poisson=False)
+    # Seed revision: faint spots found by peak seeding and dropped after the first pass; narrow spots
+    # that thresholding misses (below area_min) and the residual check adds.
+    drop, _ = S.gaussian_lattice(2.0, faint=6, faint_amplitude=0.26, seed=3)
+    add, _ = S.gaussian_lattice(1.8, small=6, faint=6, faint_amplitude=0.26, seed=3)
+    clean20, _ = S.gaussian_lattice(2.0, snr=0)
     return {
         "lattice2": (lat2, dict(area_max=400)),
-        "lattice14": (lat14, dict(area_max=400, methods=("gaussian", "halfmax"))),
+        # pitch / FWHM 1.4: too dense to threshold; peak seeding (subpx/cd.py:502-511).
+        "lattice14": (lat14, dict(area_max=400, seeds="peaks", methods=("gaussian", "halfmax"))),
         "page": (page, dict(area_max=400)),
         "staggered": (stag, dict(area_max=400)),
         "page_invert": ((65535 - page).astype(np.uint16), dict(area_max=400, invert=True,
                                                                methods=("gaussian", "logquad"))),
+        "drop_peaks": (drop, dict(seeds="peaks", methods=("gaussian", "gradient"), area_max=400)),
+        "add_threshold": (add, dict(methods=("gaussian", "halfmax"), area_min=10, area_max=400)),
+        "dark_peaks_fixed": (100 - clean20, dict(invert=True, seeds="peaks", methods=("gaussian", "halfmax"),
+                                                  background_level=80.0)),
+        "page_smooth": (page, dict(area_max=400, smooth_sigma=1.0, methods=("gaussian", "gradient", "halfmax"))),
     }
 
 
@@ -229,6 +241,7 @@ def make_cd(out: Path, ref):
     for name, (img, kw) in cd_cases().items():
         res = measure_cds(img, backend="cpu", **kw)
         arrays[f"{name}_img"] = img
+        arrays[f"{name}_kwargs"] = np.array(json.dumps(kw))
         arrays[f"{name}_seeds"] = res.seeds_xy
         arrays[f"{name}_cell_labels"] = res.cell_labels
         arrays[f"{name}_params"] = res.deblend_model["params"]
@@ -238,6 +251,8 @@ def make_cd(out: Path, ref):
                                            res.meta["seeds_added_from_residual"],
                                            res.meta["seeds_dropped_as_insignificant"]])
         arrays[f"{name}_source"] = np.array(res.meta["background_source"])
+        arrays[f"{name}_pitch"] = np.array(np.nan if res.meta.get("pitch_px") is None else res.meta["pitch_px"])
+        arrays[f"{name}_passes"] = np.array(res.meta["deblend_pass_iterations"])
         meths = list(res.measurements)
         arrays[f"{name}_methods"] = np.array(meths)
         for m, r in res.measurements.items():

@@ -1,4 +1,12 @@
-"""measure_cds on the GPU against the reference's own CPU measure_cds (golden fixtures)."""
+"""measure_cds on the GPU against the reference's own CPU measure_cds (golden fixtures).
+
+The fixtures (tests/golden/make_golden.py) cover threshold seeding on lattices, contact-hole pages
+and an inverted page; peak seeding on a pitch / FWHM 1.4 array (lattice14) and on dark holes with a
+fixed background level; seed revision that drops seeds (drop_peaks) and adds them (add_threshold),
+each with two deblend passes; and smoothed radial profiles (page_smooth, smooth_sigma = 1).
+"""
+
+import json
 
 import numpy as np
 import pytest
@@ -7,13 +15,8 @@ from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
-CASES = {
-    "lattice2": dict(area_max=400),
-    "lattice14": dict(area_max=400, methods=("gaussian", "halfmax")),
-    "page": dict(area_max=400),
-    "staggered": dict(area_max=400),
-    "page_invert": dict(area_max=400, invert=True, methods=("gaussian", "logquad")),
-}
+CASES = ("lattice2", "lattice14", "page", "staggered", "page_invert", "drop_peaks", "add_threshold",
+         "dark_peaks_fixed", "page_smooth")
 
 
 @pytest.fixture(scope="module")
@@ -21,20 +24,38 @@ def golden():
     return np.load(GOLDEN / "cd.npz")
 
 
-@pytest.mark.parametrize("name", list(CASES))
+def _kwargs(z, name):
+    kw = json.loads(str(z[f"{name}_kwargs"]))
+    if "methods" in kw:
+        kw["methods"] = tuple(kw["methods"])
+    return kw
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_measure_cds_matches_reference_cpu(golden, name):
     from imageprocessor_new_b200 import measure_cds
 
     z = golden
     img = z[f"{name}_img"]
-    res = measure_cds(img, backend="gpu", **CASES[name])
-    # Cells: seeds and Voronoi labels bit-exact.
-    np.testing.assert_array_equal(res.seeds_xy, z[f"{name}_seeds"])
+    kw = _kwargs(z, name)
+    res = measure_cds(img, backend="gpu", **kw)
+    if kw.get("seeds") == "peaks":
+        # Peak positions come from the smoothed signal, whose width follows the pitch of an FFT
+        # autocorrelation (cuFFT here, pocketfft in the reference): same seeds to 1e-9 px.
+        assert res.meta["pitch_px"] == pytest.approx(float(z[f"{name}_pitch"]), rel=1e-9)
+        assert res.seeds_xy.shape == z[f"{name}_seeds"].shape
+        np.testing.assert_allclose(res.seeds_xy, z[f"{name}_seeds"], rtol=0, atol=1e-9)
+    else:
+        # Cells: seeds bit-exact.
+        np.testing.assert_array_equal(res.seeds_xy, z[f"{name}_seeds"])
     np.testing.assert_array_equal(res.cell_labels, z[f"{name}_cell_labels"])
-    # Deblending: same number of outer iterations and passes.
+    # Deblending: same passes, outer iterations per pass, seeds added and dropped.
     meta = z[f"{name}_meta"]
     assert res.meta["deblend_iterations_used"] == meta[0]
     assert res.meta["deblend_passes"] == meta[1]
+    assert res.meta["deblend_pass_iterations"] == list(z[f"{name}_passes"])
+    assert res.meta["seeds_added_from_residual"] == meta[2]
+    assert res.meta["seeds_dropped_as_insignificant"] == meta[3]
     assert res.meta["background_source"] == str(z[f"{name}_source"])
     np.testing.assert_allclose(res.deblend_model["params"], z[f"{name}_params"], rtol=0, atol=1e-6)
     for method in z[f"{name}_methods"]:

@@ -131,7 +131,9 @@ def test_patches_match_numpy(dtype, sign):
 
 def test_trained_network_gains_over_the_plain_start():
     """A network trained here on synthetic pages needs fewer LM iterations than the plain initialiser
-    and ends at the plain fit's optimum (centres within 1e-3 px)."""
+    under the same stop rule (relative cost drop 1e-7; the like-for-like arm) and than the
+    reference's 1e-12 rule, and ends at the plain fit's optimum (centres within 1e-3 px of the
+    1e-12 fit); kept warm fits end at the plain fit's cost (the fallback rule's misses are rare)."""
     from imageprocessor_new_b200 import warmstart as ws
 
     x, t = ws.training_set(12, size=1536, seed=11)
@@ -140,9 +142,10 @@ def test_trained_network_gains_over_the_plain_start():
     assert hist[-1] < 0.5 * hist[0]
     r = ws.evaluate(net, pages=1, size=1536, seed=5, repeats=1)
     assert r["cells"] > 1000
-    assert r["warm_iterations_mean"] < r["plain_iterations_mean"]
+    assert r["warm_iterations_mean"] < r["plain_loose_iterations_mean"] < r["plain_ref_iterations_mean"]
     assert r["fallback_fraction"] < 0.2
-    assert r["within_1e-3_px"] >= 0.99
+    assert r["warm_within_1e-3_px"] >= 0.99
+    assert r["fallback_miss_rate"] < 0.05
 
 
 def test_predict_init_does_not_depend_on_batching():

@@ -69,25 +69,32 @@ def test_tiled_rules_match_reference():
     np.testing.assert_allclose(key(got), key(want), rtol=0, atol=1e-9)
 
 
-CD_CASES = {
-    "lattice2": dict(area_max=400),
-    "lattice14": dict(area_max=400, methods=("gaussian", "halfmax")),
-    "page": dict(area_max=400),
-    "staggered": dict(area_max=400),
-    "page_invert": dict(area_max=400, invert=True, methods=("gaussian", "logquad")),
-}
+def _cd_kwargs(z, name):
+    """measure_cds keyword arguments the fixture was made with (stored beside it as JSON)."""
+    import json
+
+    kw = json.loads(str(z[f"{name}_kwargs"]))
+    if "methods" in kw:
+        kw["methods"] = tuple(kw["methods"])
+    return kw
 
 
-@pytest.mark.parametrize("name", ["lattice2", "page", "page_invert"])
+# lattice14: seeds="peaks" on a pitch / FWHM 1.4 array; drop_peaks / add_threshold: seed revision
+# dropping / adding seeds (two deblend passes); dark_peaks_fixed: inverted, fixed background level;
+# page_smooth: smooth_sigma = 1 in the radial profiles.
+@pytest.mark.parametrize("name", ["lattice2", "page", "page_invert", "lattice14", "drop_peaks", "add_threshold",
+                                  "dark_peaks_fixed", "page_smooth"])
 def test_measure_cds_oracle_matches_reference(name):
     from oracle import cd as ocd
 
     z = _load("cd")
-    kw = dict(CD_CASES[name])
+    kw = _cd_kwargs(z, name)
     got = ocd.measure_cds(z[f"{name}_img"], **kw)
     np.testing.assert_array_equal(got["seeds"], z[f"{name}_seeds"])
     np.testing.assert_array_equal(got["cell_labels"], z[f"{name}_cell_labels"])
     assert got["iterations_used"] == z[f"{name}_meta"][0]
+    assert got["passes"] == list(z[f"{name}_passes"])
+    assert (got["added"], got["dropped"]) == tuple(z[f"{name}_meta"][2:4])
     np.testing.assert_allclose(got["params"], z[f"{name}_params"], rtol=0, atol=1e-9)
     for method in z[f"{name}_methods"]:
         method = str(method)
