@@ -440,6 +440,7 @@ def tiled_arm(args):
         out[name] = (s.elapsed_time(e) / args.steps, len(res.centers_xy), res)
     ms, n, res = out["graphs"]
     px = args.tiled_size ** 2
+    cpu = tiled_cpu_baseline(page_d, res, args) if args.cpu_baseline else None
     print(json.dumps({
         "metric": "centres/s, detect_centers_tiled", "value": round(n / (ms / 1e3), 1), "unit": "centres/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
@@ -451,7 +452,44 @@ def tiled_arm(args):
         "dtype": "u16 in, f64 centres", "data": "synthetic (rendered on the device)",
         "config": {"workload": f"page_square_{args.tiled_size}x{args.tiled_size}_u16_pitch20_d10_tiled",
                    "tile_h": 8192, "overlap": 128, "threshold": "otsu (global, img[::4, ::4] x 0.8)",
-                   "refine": "auto"}}), flush=True)
+                   "refine": "auto"},
+        "cpu_baseline": cpu}), flush=True)
+
+
+def tiled_cpu_baseline(page_d, res, args, strip_rows: int = 512) -> dict:
+    """The tiled page's CPU cost by the oracle (the reference algorithm on the host cores), from
+    bounded samples: the global Otsu of img[::4, ::4]; the per-band detection timed on one strip of
+    `strip_rows` rows (fixed threshold, refine="auto") and scaled by the rows the bands cover
+    (overlaps counted twice); the reference's O(N^2) dedupe timed on 1/64 of the page's centres and
+    extrapolated by (64)^2. Centres/s = the page's centres / the extrapolated total."""
+    from imageprocessor_new_b200 import shard
+    from oracle import centers as oc
+    from oracle import segment as osg
+
+    size = int(page_d.shape[0])
+    t0 = time.perf_counter()
+    sub = page_d[::4, ::4].cpu().numpy()
+    pre = osg.otsu_threshold(np.ascontiguousarray(sub)) * 0.8
+    t_otsu = time.perf_counter() - t0
+    y0 = size // 2
+    strip = page_d[y0:y0 + strip_rows].cpu().numpy()
+    t0 = time.perf_counter()
+    oc.detect_centers(strip, threshold="otsu", area_max=400, refine_method="auto", fixed_threshold=pre)
+    t_strip = time.perf_counter() - t0
+    rows = sum(b.y1 - b.y0 for b in shard.band_plan(size, 8192, 128))
+    t_bands = t_strip * rows / strip_rows
+    pts = res.centers_xy[:: 64]
+    t0 = time.perf_counter()
+    oc.dedupe_pairwise(pts, 1.5)
+    t_dd = time.perf_counter() - t0
+    t_total = t_otsu + t_bands + t_dd * 64 ** 2
+    return {"value": round(len(res.centers_xy) / t_total, 2), "unit": "centres/s", "cores": os.cpu_count(),
+            "kind": "port", "sample": (f"global Otsu of img[::4, ::4]; one {strip_rows}-row strip of detection "
+                                       f"scaled by the {rows} band rows; O(N^2) dedupe on 1/64 of the centres "
+                                       "extrapolated by 64^2"),
+            "seconds": {"otsu": round(t_otsu, 2), "strip": round(t_strip, 2), "bands_extrapolated": round(t_bands, 1),
+                        "dedupe_1_64": round(t_dd, 2), "dedupe_extrapolated": round(t_dd * 64 ** 2, 1),
+                        "page_extrapolated": round(t_total, 1)}}
 
 
 def stack_arm(args):
@@ -498,6 +536,7 @@ def stack_arm(args):
                           "plain_iterations_mean": round(float(ip[sl].mean()), 3) if sl.stop > sl.start else 0.0,
                           "warm_iterations_mean": round(float(iw[sl].mean()), 3) if sl.stop > sl.start else 0.0})
     n = sc.n
+    cpu = stack_cpu_baseline(s, args) if args.cpu_baseline else None
     print(json.dumps({
         "metric": METRIC, "value": round(n / (ms["warm"] / 1e3), 1), "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(ms["warm"], 3),
@@ -512,7 +551,38 @@ def stack_arm(args):
         "fallback_fraction": float(fw.mean()),
         "centre_dev_max_px": max(p["centre_dev_max_px"] for p in per_image),
         "within_1e-3_px": bool(all(p["centre_dev_max_px"] <= 1e-3 for p in per_image)),
-        "per_image": per_image, "clocks": clocks.summary()}), flush=True)
+        "per_image": per_image, "clocks": clocks.summary(), "cpu_baseline": cpu}), flush=True)
+
+
+def _stack_cpu_worker(crop):
+    """One pool worker: the oracle's initial fits of one image crop's cells, timed (no GPU here)."""
+    import time as _time
+
+    from oracle import cd as ocd
+    from oracle import deblend as odb
+
+    seeds, masks, origins = ocd.threshold_cells(crop, area_min=10, area_max=2000, pad=3)
+    t0 = _time.perf_counter()
+    odb.initial_fits(crop, seeds, masks, origins)
+    return len(seeds), _time.perf_counter() - t0
+
+
+def stack_cpu_baseline(stack_d, args, crop: int = 768) -> dict:
+    """The stack's initial fits on the host cores by the oracle (the reference's NumPy LM), as the
+    reference's batch pipeline runs them: a process pool of min(64, cores) workers, one image each,
+    on a bounded sample (a crop x crop corner of the first `workers` images). cells/s = cells fitted
+    / the pool's wall time for the fits (the slowest worker bounds it)."""
+    import multiprocessing as mp
+
+    workers = max(1, min(64, os.cpu_count() or 1, int(stack_d.shape[0])))
+    crops = [np.ascontiguousarray(stack_d[i, :crop, :crop].cpu().numpy()) for i in range(workers)]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        out = pool.map(_stack_cpu_worker, crops)
+    cells = sum(c for c, _ in out)
+    wall = max(t for _, t in out)
+    return {"value": round(cells / wall, 2), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "workers": workers, "sample": f"{crop}x{crop} corner of each of {workers} images, one per worker",
+            "cells": cells, "seconds": round(wall, 2)}
 
 
 def main():

@@ -593,7 +593,7 @@ __device__ __forceinline__ void cubic_weights(double v, int n, double* w, int* i
     for (int k = 0; k < 4; ++k) idx[k] = min(max((int)f - 1 + k, 0), n - 1);
 }
 
-__device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, double y, double x) {
+__device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, int pitch, double y, double x) {
     double wy[4], wx[4];
     int iy[4], ix[4];
     cubic_weights(y, hp, wy, iy);
@@ -602,7 +602,7 @@ __device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, d
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) out += coef[iy[a] * wp + ix[b]] * wy[a] * wx[b];
+        for (int b = 0; b < 4; ++b) out += coef[iy[a] * pitch + ix[b]] * wy[a] * wx[b];
     return out;
 }
 
@@ -669,10 +669,16 @@ constexpr int kTrigMax = 256;  // ray angles with a cos / sin table in shared me
 
 // Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients in FP64 and in
 // FP32, a reduction area, then the cell mask and the eroded mask as bytes.
+// Row pitch (in doubles) of the FP64 coefficient plane: the padded width made odd, so that the
+// threads of the row pass of the spline prefilter (one row each, stepping along their rows) fall in
+// different shared-memory banks.
+__host__ __device__ inline int radial_pitch(int wm) { return (wm + 2 * kPad) | 1; }
+
 // With smoothing, three more hm x wm planes follow (the two axis-0 passes and the smoothed signal).
 __host__ __device__ inline long long radial_cta_doubles(int hm, int wm, bool smooth = false) {
-    const long long np = (long long)(hm + 2 * kPad) * (wm + 2 * kPad);
-    return np + (np + 1) / 2 + 32 + (2LL * hm * wm + 7) / 8 + (smooth ? 3LL * hm * wm : 0);
+    const long long np = (long long)(hm + 2 * kPad) * radial_pitch(wm);
+    const long long nf = (long long)(hm + 2 * kPad) * (wm + 2 * kPad);
+    return np + (nf + 1) / 2 + 32 + (2LL * hm * wm + 7) / 8 + (smooth ? 3LL * hm * wm : 0);
 }
 
 // One output of scipy's correlate1d with a symmetric kernel (weights w[0..2r], centre w[r]) and
@@ -790,7 +796,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     extern __shared__ double sm[];
     __shared__ double trig_tab[2 * kTrigMax];  // cos, sin of the ray angles (n_angles <= kTrigMax)
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int hp = hm + 2 * kPad, wp = wm + 2 * kPad, area_px = hm * wm;
+    const int hp = hm + 2 * kPad, wp = wm + 2 * kPad, dp = radial_pitch(wm), area_px = hm * wm;
     const double* trig = n_angles <= kTrigMax ? trig_tab : nullptr;
     if (trig)
         for (int a = tid; a < n_angles; a += kRadialThreads) {
@@ -799,8 +805,8 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
             trig_tab[2 * a + 1] = sin(ang);
         }
     double* coef = coef_scratch ? coef_scratch + (long long)blockIdx.x * radial_cta_doubles(hm, wm, kSmooth) : sm;
-    float* coef_f = reinterpret_cast<float*>(coef + (long long)hp * wp);
-    double* red = coef + (long long)hp * wp + ((long long)hp * wp + 1) / 2;  // 32 doubles: 8 slots of 4
+    float* coef_f = reinterpret_cast<float*>(coef + (long long)hp * dp);  // FP32 copy, row pitch wp
+    double* red = coef + (long long)hp * dp + ((long long)hp * wp + 1) / 2;  // 32 doubles: 8 slots of 4
     uint8_t* mask = reinterpret_cast<uint8_t*>(red + 32);
     uint8_t* emask = mask + area_px;
     const double thr = fmax(0.35, 2.0 * radial_step);
@@ -869,13 +875,15 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
             }
             __syncthreads();
             for (int k = tid; k < hp * wp; k += kRadialThreads) {
-                const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
-                coef[k] = fs[yy * wm + xx];
+                const int r = k / wp, q = k % wp;
+                const int yy = min(max(r - kPad, 0), hm - 1), xx = min(max(q - kPad, 0), wm - 1);
+                coef[r * dp + q] = fs[yy * wm + xx];
             }
         } else {
             for (int k = tid; k < hp * wp; k += kRadialThreads) {
-                const int yy = min(max(k / wp - kPad, 0), hm - 1), xx = min(max(k % wp - kPad, 0), wm - 1);
-                coef[k] = mask[yy * wm + xx] ? c.roi[yy * wm + xx] : 0.0;
+                const int r = k / wp, q = k % wp;
+                const int yy = min(max(r - kPad, 0), hm - 1), xx = min(max(q - kPad, 0), wm - 1);
+                coef[r * dp + q] = mask[yy * wm + xx] ? c.roi[yy * wm + xx] : 0.0;
             }
         }
         for (int k = tid; k < area_px; k += kRadialThreads) {
@@ -884,12 +892,12 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                        mask[k - 1] && mask[k + 1];
         }
         __syncthreads();
-        for (int col = tid; col < wp; col += kRadialThreads) spline_line(coef + col, hp, wp);
+        for (int col = tid; col < wp; col += kRadialThreads) spline_line(coef + col, hp, dp);
         __syncthreads();
-        for (int row = tid; row < hp; row += kRadialThreads) spline_line(coef + (long long)row * wp, wp, 1);
+        for (int row = tid; row < hp; row += kRadialThreads) spline_line(coef + (long long)row * dp, wp, 1);
         __syncthreads();
-        const double peak = cubic_at(coef, hp, wp, cy + kPad, cx + kPad);
-        for (int k = tid; k < hp * wp; k += kRadialThreads) coef_f[k] = (float)coef[k];
+        const double peak = cubic_at(coef, hp, wp, dp, cy + kPad, cx + kPad);
+        for (int k = tid; k < hp * wp; k += kRadialThreads) coef_f[k] = (float)coef[(k / wp) * dp + k % wp];
         __syncthreads();
         const double half = peak / 2.0;
         const double inv2s = 1.0 / (2.0 * radial_step);

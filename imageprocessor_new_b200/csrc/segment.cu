@@ -183,6 +183,141 @@ __global__ void k_histogram(const void* img, int dtype, int height, int width, i
     }
 }
 
+// Certified parallel Otsu: the bin that OpenCV's sequential FP64 scan chooses, found without the
+// scan whenever the exact rational between-class variances single it out.
+//
+// For bin i with integer prefix sums Q = sum_{j<=i} h_j and S = sum_{j<=i} j h_j (N pixels, grey
+// sum M), the exact variance is sigma2 = (S N - Q M)^2 / (N^2 Q (N - Q)), and mu1 - mu2 =
+// (S N - Q M) / (Q (N - Q)). OpenCV's loop computes q1 as a running FP64 sum of h_j / N (relative
+// error <= (n + 2) u for n bins, u = 2^-53), mu1 by a recurrence whose product mu1 q1 is a running
+// sum of j h_j / N (relative error <= 4 (n + 2) u), mu2 = (mu - q1 mu1) / q2 and sigma2 = q1 q2
+// (mu1 - mu2)^2. From these error terms every bin gets an interval [lo, hi] that holds OpenCV's
+// rounded sigma2 (each term inflated four times), and the skip test min(q1, q2) < FLT_EPSILON is
+// decided on the exact q1 = Q / N unless q1 or q2 lies within 1e-9 of FLT_EPSILON or of
+// 1 - FLT_EPSILON (a bin that might go either way). When the bin i* with the largest lo among the
+// surely unskipped bins has lo > 0 and lo above every other not-surely-skipped bin's hi, OpenCV's
+// strict-maximum scan must choose i*: returns true with the threshold. Otherwise (near-ties,
+// ambiguous skips) returns false and the caller runs the sequential scan. Block-uniform result;
+// needs blockDim.x == 1024.
+__device__ bool otsu_certified(const unsigned int* hist, int first, int n, long long total,
+                               unsigned long long grey_sum, double* threshold) {
+    constexpr int T = 1024;
+    __shared__ unsigned long long s_q[T], s_m[T];
+    __shared__ double s_val[32];
+    __shared__ int s_idx[32];
+    __shared__ double s_best_lo;
+    __shared__ int s_best;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int per = (n + T - 1) / T, b0 = min(n, t * per), b1 = min(n, b0 + per);
+    unsigned long long cq = 0, cm = 0;
+    for (int k = b0; k < b1; ++k) {
+        const unsigned long long h = hist[first + k];
+        cq += h;
+        cm += h * (unsigned long long)(first + k);
+    }
+    s_q[t] = cq;
+    s_m[t] = cm;
+    __syncthreads();
+    for (int o = 1; o < T; o <<= 1) {  // inclusive scan of the chunk totals
+        const unsigned long long aq = t >= o ? s_q[t - o] : 0ull, am = t >= o ? s_m[t - o] : 0ull;
+        __syncthreads();
+        s_q[t] += aq;
+        s_m[t] += am;
+        __syncthreads();
+    }
+    const unsigned long long q_start = s_q[t] - cq, m_start = s_m[t] - cm;
+    const double Nd = (double)total, invN = 1.0 / Nd;
+    const double u = 1.1102230246251565e-16;
+    const double eps = 1.1920928955078125e-07, win = 1e-9;
+    const double g = (double)(n + 2) * u;
+    const double mu = (double)grey_sum * invN;
+    // cls: 0 surely skipped, 1 surely unskipped, 2 either. lo / hi: the interval of OpenCV's sigma2.
+    auto eval = [&](unsigned long long Q, unsigned long long S, double* lo, double* hi) -> int {
+        const unsigned long long R = (unsigned long long)total - Q;
+        const double q1 = (double)Q * invN, q2 = (double)R * invN;
+        const bool amb = fabs(q1 - eps) <= win || fabs(q2 - eps) <= win || fabs(q1 - (1.0 - eps)) <= win ||
+                         fabs(q2 - (1.0 - eps)) <= win;
+        const bool skip = fmin(q1, q2) < eps || fmax(q1, q2) > 1.0 - eps;
+        if (skip && !amb) return 0;
+        if (Q == 0 || R == 0) {  // q1 or q2 exactly 0 cannot be unskipped (amb never holds here)
+            *lo = *hi = 0.0;
+            return 0;
+        }
+        const __int128 D = (__int128)S * (__int128)total - (__int128)Q * (__int128)grey_sum;
+        const double qr = (double)Q * (double)R;
+        const double d = (double)D / qr;                  // mu1 - mu2
+        const double ad = fabs(d);
+        const double mu1 = (double)S / (double)Q;
+        const double mu2 = (double)(grey_sum - S) / (double)R;
+        const double rel_q1 = 4.0 * g;
+        const double rel_q2 = 4.0 * (g * q1 + u) / q2;
+        const double num = q2 * mu2;                      // mu - q1 mu1, > 0 here
+        const double rel_mu2 = (5.0 * g + u) * mu / fmax(num, 1e-300) + (g * q1 + u) / q2 + u;
+        const double err_d = 4.0 * (4.0 * g * mu1 + mu2 * rel_mu2 + u * ad);
+        const double base = q1 * q2;
+        *hi = base * (1.0 + rel_q1) * (1.0 + rel_q2) * (ad + err_d) * (ad + err_d) * (1.0 + 16.0 * u);
+        const double dl = fmax(ad - err_d, 0.0);
+        *lo = rel_q2 >= 1.0 ? 0.0 : base * (1.0 - rel_q1) * (1.0 - rel_q2) * dl * dl * (1.0 - 16.0 * u);
+        return amb ? 2 : 1;
+    };
+    // Pass 1: the surely unskipped bin with the largest lower bound (lowest index on ties).
+    double best_lo = -1.0;
+    int best = 0x7fffffff;
+    {
+        unsigned long long Q = q_start, S = m_start;
+        for (int k = b0; k < b1; ++k) {
+            const unsigned long long h = hist[first + k];
+            Q += h;
+            S += h * (unsigned long long)(first + k);
+            double lo, hi;
+            if (eval(Q, S, &lo, &hi) == 1 && lo > best_lo) {
+                best_lo = lo;
+                best = k;
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best_lo, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, best, o);
+        if (ov > best_lo || (ov == best_lo && oi < best)) { best_lo = ov; best = oi; }
+    }
+    if (lane == 0) { s_val[warp] = best_lo; s_idx[warp] = best; }
+    __syncthreads();
+    if (t == 0) {
+        double v = -1.0;
+        int i = 0x7fffffff;
+        for (int w = 0; w < T / 32; ++w)
+            if (s_val[w] > v || (s_val[w] == v && s_idx[w] < i)) { v = s_val[w]; i = s_idx[w]; }
+        s_best_lo = v;
+        s_best = i;
+    }
+    __syncthreads();
+    const double star_lo = s_best_lo;
+    const int star = s_best;
+    // Pass 2: the largest upper bound of every other bin that may be unskipped.
+    double other_hi = 0.0;
+    {
+        unsigned long long Q = q_start, S = m_start;
+        for (int k = b0; k < b1; ++k) {
+            const unsigned long long h = hist[first + k];
+            Q += h;
+            S += h * (unsigned long long)(first + k);
+            double lo, hi;
+            if (k != star && eval(Q, S, &lo, &hi) != 0) other_hi = fmax(other_hi, hi);
+        }
+    }
+    other_hi = warp_max(other_hi);
+    __syncthreads();  // s_val is reused
+    if (lane == 0) s_val[warp] = other_hi;
+    __syncthreads();
+    double top = 0.0;
+    for (int w = 0; w < T / 32; ++w) top = fmax(top, s_val[w]);
+    const bool ok = star != 0x7fffffff && star_lo > 0.0 && star_lo > top;
+    if (ok && t == 0) *threshold = (double)(first + star);
+    return ok;
+}
+
 // OpenCV's Otsu scan (getThreshVal_Otsu) over bins [0, N), by one block in four phases:
 //   A  p_i = h[i] * scale (parallel), then q1_i = q1_{i-1} + p_i by one thread (additions only);
 //   B  y_i = RN(1 / q1_i) (parallel);
@@ -214,6 +349,7 @@ __global__ void __launch_bounds__(1024) k_otsu_scan(const unsigned int* hist, in
     __syncthreads();
     unsigned long long mu_int = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mu_int += s_mu[w];
+    if (n > 0 && otsu_certified(hist, first, n, total, mu_int, threshold)) return;
     // The reference sums i*h[i] sequentially in double: every partial sum is an integer below 2^53,
     // hence exact, and equal to this integer sum.
     const double mu = __dmul_rn((double)mu_int, scale);

@@ -205,3 +205,41 @@ def detect_tiled_sharded(image: np.ndarray, *, tile_h: int, overlap: int = 128, 
     if not kept:
         return np.zeros((0, 2))
     return ops.dedupe(np.vstack(kept), float(dedupe_eps))
+
+
+def measure_cds_sharded(pages, *, measure=None, group=None, dst: int | None = 0, **measure_kw):
+    """measure_cds of a batch of pages (a sequence or an (N, H, W) stack, e.g. the images of an
+    uneven stack or the pages of a TIFF batch) spread over the process group: rank r measures the
+    contiguous run units_of_rank(N, r, world) of pages (each page once, no exchange while
+    measuring), and the per-page results are gathered in page order, as the reference's batch
+    pipeline runs one worker process per GPU over its share of the pages and collects their
+    summaries (scripts/cd_batch.py:369-420, 705-728).
+
+    ``measure`` maps one page to its result (default: ``measure_cds(page, backend="gpu",
+    summary_only=True, **measure_kw)`` on this rank's GPU). Results are gathered to rank ``dst``
+    (other ranks return None), or to every rank when ``dst`` is None. Every rank must call this
+    with the same number of pages."""
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    if measure is None:
+        from .cd import measure_cds
+
+        kw = dict(summary_only=True, **measure_kw)
+
+        def measure(page):
+            return measure_cds(page, backend="gpu", **kw)
+
+    n = len(pages)
+    local = [(i, measure(pages[i])) for i in units_of_rank(n, rank, world)]
+    if dst is None:
+        parts = [None] * world
+        dist.all_gather_object(parts, local, group=group)
+    else:
+        parts = [None] * world if rank == dst else None
+        dist.gather_object(local, parts, dst=dst, group=group)
+        if rank != dst:
+            return None
+    out = [None] * n
+    for part in parts:
+        for i, res in part:
+            out[i] = res
+    return out

@@ -370,3 +370,17 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
             "report": report, "passes": passes, "iterations_used": sum(passes), "added": added, "dropped": dropped,
             "source": state.background_info.get("source"), "background_map": sign * state.background_map,
             "status": state.status[report], "pitch": pitch}
+
+
+def threshold_cells(img, *, threshold="otsu", invert=False, area_min=3, area_max=50, pad=3):
+    """Seeds, cell masks and origins of thresholded components (subpx/cd.py:472-538: segmentation,
+    area filter, Voronoi cells of the centroids, boxes grown by pad)."""
+    img = np.asarray(img)
+    t = osg.otsu_threshold(img) if threshold == "otsu" else osg.triangle_threshold(img)
+    num, labels, stats, cents = osg.label_components(osg.binarize(img, t, invert), 8)
+    area = stats[1:num, 4]
+    keep = (area >= area_min) & (area <= area_max)
+    rows = np.column_stack((stats[1:num, :4], cents[1:num])).astype(np.float64)[keep]
+    seeds = rows[:, 4:6].copy()
+    masks, origins = cell_stack(ov.voronoi_labels(seeds, img.shape), rows, pad, img.shape)
+    return seeds, masks, origins

@@ -259,3 +259,44 @@ def detect_tiled(image, *, tile_h, overlap=128, threshold_mode="auto", otsu_down
     if not kept:
         return np.zeros((0, 2))
     return dedupe(np.vstack(kept), dedupe_eps)
+
+
+def dedupe_pairwise(points: np.ndarray, eps: float = 1.5) -> np.ndarray:
+    """The reference's own O(N^2) dedupe (subpx/centers.py:335-380): for each point, squared
+    distances to every later point, union-find (path halving, union by rank) of pairs within eps,
+    cluster means ordered by root index. Same clusters and means as ``dedupe`` (whose order is by
+    smallest member); kept to time the reference's cost on the CPU baseline of the tiled page."""
+    pts = np.asarray(points, dtype=np.float64).reshape(-1, 2)
+    n = len(pts)
+    if n == 0:
+        return pts
+    parent = np.arange(n, dtype=np.int64)
+    rank = np.zeros(n, dtype=np.int8)
+
+    def find(a):
+        while parent[a] != a:
+            parent[a] = parent[parent[a]]
+            a = parent[a]
+        return int(a)
+
+    eps2 = float(eps) ** 2
+    for i in range(n):
+        d2 = np.sum((pts[i + 1:] - pts[i]) ** 2, axis=1)
+        for j in np.flatnonzero(d2 <= eps2) + i + 1:
+            ra, rb = find(i), find(int(j))
+            if ra == rb:
+                continue
+            if rank[ra] < rank[rb]:
+                parent[ra] = rb
+            elif rank[ra] > rank[rb]:
+                parent[rb] = ra
+            else:
+                parent[rb] = ra
+                rank[ra] += 1
+    roots = np.array([find(i) for i in range(n)])
+    _, inv = np.unique(roots, return_inverse=True)
+    sums = np.zeros((inv.max() + 1, 2))
+    counts = np.zeros(inv.max() + 1)
+    np.add.at(sums, inv, pts)
+    np.add.at(counts, inv, 1)
+    return sums / counts[:, None]

@@ -454,3 +454,21 @@ def detect_peaks(signal, *, min_distance=None, smooth_sigma=None, threshold=0.25
         delta = np.where(ok & (curv < 0), 0.5 * (left - right) / np.where(curv < 0, curv, -1), 0.0)
         sub[:, axis] += np.clip(delta, -0.5, 0.5)
     return sub, pitch
+
+
+def initial_fits(image, seeds, masks, origins, *, background_level=None, max_iter=30):
+    """The initial fits that start deblend (subpx/_cpu/deblend.py:452-480): per cell the 10th
+    percentile of its border pixels as background (or the given level), initial_params, LM and
+    fit_status. Returns (params, status) in cell-local coordinates."""
+    from scipy.ndimage import binary_erosion
+
+    image = np.asarray(image, dtype=np.float64)
+    seeds = np.asarray(seeds, float).reshape(-1, 2)
+    origins = np.asarray(origins, dtype=np.int64).reshape(-1, 2)
+    raw = windows(image, origins, masks.shape[1:])
+    border = masks & ~binary_erosion(masks, structure=np.ones((1, 3, 3)), border_value=0)
+    bg0 = np.array([np.percentile(r[b], 10) if b.any() else 0.0 for r, b in zip(raw, border)])
+    if background_level is not None:
+        bg0[:] = background_level
+    data = np.where(masks, raw - bg0[:, None, None], 0.0)
+    return fit_batch(data, masks, initial_params(data, masks, seeds - origins), max_iter)

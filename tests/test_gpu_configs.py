@@ -20,7 +20,11 @@ def _compare_cds(res, ref, methods):
     np.testing.assert_array_equal(res.seeds_xy, ref["seeds"])
     np.testing.assert_array_equal(res.cell_labels, ref["cell_labels"])
     assert res.meta["deblend_pass_iterations"] == ref["passes"]
-    np.testing.assert_allclose(res.deblend_model["params"], ref["params"], rtol=1e-9, atol=1e-6)
+    # FP64 sums in another order: positions and log-widths within 1e-6, amplitudes (thousands of
+    # counts) within 1e-7 relative (a fit ends where the 1e-12 cost rule stops it).
+    got_p, want_p = res.deblend_model["params"], ref["params"]
+    np.testing.assert_allclose(got_p[:, 1:], want_p[:, 1:], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(got_p[:, 0], want_p[:, 0], rtol=1e-7, atol=1e-6)
     for m in methods:
         got, want = res.measurements[m], ref["measurements"][m]
         np.testing.assert_array_equal(got.status, want["status"], err_msg=m)

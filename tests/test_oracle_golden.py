@@ -121,3 +121,16 @@ def test_morphology_matches_opencv(seed):
         if c:
             want = cv2.morphologyEx(want, cv2.MORPH_CLOSE, k, iterations=c)
         np.testing.assert_array_equal(osg.morphology(fg, o, c), want > 0, err_msg=f"open {o} close {c}")
+
+
+@pytest.mark.parametrize("n", [0, 1, 300, 2000])
+def test_pairwise_dedupe_equals_kdtree_dedupe(n):
+    """The reference's O(N^2) dedupe loop and the oracle's KD-tree restatement give the same clusters
+    (as sorted sets of means)."""
+    rng = np.random.default_rng(n)
+    base = rng.uniform(0, 300, (n, 2))
+    pts = np.concatenate([base, base[: n // 3] + rng.normal(0, 0.6, (n // 3, 2))]) if n else np.zeros((0, 2))
+    key = lambda a: a[np.lexsort((a[:, 1], a[:, 0]))]
+    a, b = oc.dedupe(pts, 1.5), oc.dedupe_pairwise(pts, 1.5)
+    assert a.shape == b.shape
+    np.testing.assert_allclose(key(a), key(b), rtol=0, atol=1e-12)

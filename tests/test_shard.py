@@ -92,3 +92,58 @@ def test_plans_cover_every_row_and_unit_once():
         np.testing.assert_array_equal(sampled, np.arange(1001)[::4])
     with pytest.raises(ValueError):
         shard.band_plan(100, 50, 50)
+
+
+def _cd_pages():
+    from imageprocessor_new_b200 import synthetic
+
+    return [synthetic.gaussian_lattice(r, shape=(90, 150), seed=k)[0] for k, r in enumerate((2.0, 2.67, 2.2, 2.5,
+                                                                                          3.0))]
+
+
+def _oracle_summary(page):
+    from oracle import cd as ocd
+
+    r = ocd.measure_cds(page, methods=("gaussian", "halfmax"), area_max=400)
+    return {"seeds": r["seeds"], "cd": {m: r["measurements"][m]["metrics"]["cd_equivalent_px"]
+                                        for m in ("gaussian", "halfmax")}, "passes": r["passes"]}
+
+
+def _cd_worker(rank, world, port, dst, out_dir):
+    import pickle
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=120))
+    try:
+        got = shard.measure_cds_sharded(_cd_pages(), measure=_oracle_summary, dst=dst)
+        with open(os.path.join(out_dir, f"cd{rank}.pkl"), "wb") as f:
+            pickle.dump(got, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,dst", [(2, 0), (3, None)])
+def test_sharded_measure_cds_gathers_pages_in_order(tmp_path, world, dst):
+    """Pages split into contiguous runs per rank, each measured once (the oracle stands in for each
+    rank's GPU), results gathered in page order: equal to measuring every page in one process."""
+    import pickle
+
+    import torch.multiprocessing as mp
+
+    mp.spawn(_cd_worker, args=(world, _free_port(), dst, str(tmp_path)), nprocs=world, join=True)
+    want = [_oracle_summary(p) for p in _cd_pages()]
+    for rank in range(world):
+        with open(tmp_path / f"cd{rank}.pkl", "rb") as f:
+            got = pickle.load(f)
+        if dst is not None and rank != dst:
+            assert got is None
+            continue
+        assert len(got) == len(want)
+        for g, w in zip(got, want):
+            np.testing.assert_array_equal(g["seeds"], w["seeds"])
+            assert g["passes"] == w["passes"]
+            for m in w["cd"]:
+                np.testing.assert_array_equal(g["cd"][m], w["cd"][m])
