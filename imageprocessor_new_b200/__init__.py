@@ -17,6 +17,7 @@ from .centers import (
     recommend_refine_method,
 )
 from .cd import METHOD_LABELS, measure_cds
+from .results import load_cd_results, save_cd_arrays, save_cd_results, save_cd_tables
 from .segment import connected_components_stats
 from .voronoi import compute_voronoi_labels, compute_voronoi_labels_gpu
 
@@ -24,7 +25,7 @@ __version__ = "0.1.0"
 
 __all__ = [
     "CDMethodResult", "CDResult", "CDSummary", "CenterResult", "ComponentStatsResult", "METHOD_LABELS",
-    "measure_cds",
+    "measure_cds", "load_cd_results", "save_cd_arrays", "save_cd_results", "save_cd_tables",
     "choose_refine_method_for_bbox", "compute_voronoi_labels", "compute_voronoi_labels_gpu",
     "connected_components_stats", "detect_centers", "detect_centers_batch", "detect_centers_tiled",
     "detect_centers_tiled_global_otsu", "filter_centers", "recommend_refine_method",

@@ -135,6 +135,8 @@ SIGNATURES = {
     "spx_radial_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _P, _I, _MO, _MO, _P, _S, _P]),
     "spx_minimum_filter": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "spx_clean_masked": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _BG, _P, _I, _I, _I, _P, _P]),
+    "spx_rebuild_contours": (_I, [_I, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P]),
     "spx_signal_image": (_I, [_P, _I, _D, _I, _I, _P, _P]),
     "spx_pitch_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_pitch_crop": (_I, [_P, _I, _D, _I, _I, _I, _P, _P, _S, _P]),

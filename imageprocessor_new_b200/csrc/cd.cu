@@ -986,6 +986,52 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     }
 }
 
+// Contours of stored results from their geometry (the compact result files' rebuild), with the
+// measurement kernels' own vertex arithmetic: kind 0 the deblended Gaussian's half-maximum ellipse
+// about the global centre, kind 1 the log-quadratic ellipse about the local centre plus the origin,
+// kind 2 the radial polygon center_local + edge * (cos, sin) plus the origin. NaN where the cell
+// has no ellipse or, for kind 2, no centre.
+__global__ void k_rebuild_contours(int kind, const double* centers, const double* center_local,
+                                   const double* eigenvalues, const double* axes, const double* edge_px,
+                                   const int* origins, int n, int n_angles, double* contours) {
+    const int nv = n_angles + 1;
+    const long long total = (long long)n * nv;
+    const double step = 2.0 * kPi / n_angles;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t / nv), k = (int)(t % nv), a = k % n_angles;
+        double x = dnan(), y = dnan();
+        if (kind == 2) {
+            const double cx = center_local[2LL * i], cy = center_local[2LL * i + 1];
+            const double ang = (double)a * (2.0 * kPi / n_angles);
+            const double c = cos(ang), sn = sin(ang);
+            const double e = edge_px[(long long)i * n_angles + a];
+            const double vx = cx + e * c, vy = cy + e * sn;
+            x = vx + origins[2LL * i];
+            y = vy + origins[2LL * i + 1];
+        } else {
+            Eig2 e;
+            e.w0 = eigenvalues[2LL * i];
+            e.w1 = eigenvalues[2LL * i + 1];
+            e.v00 = axes[4LL * i + 0];
+            e.v01 = axes[4LL * i + 1];
+            e.v10 = axes[4LL * i + 2];
+            e.v11 = axes[4LL * i + 3];
+            if (isfinite(e.w0) && isfinite(e.w1)) {
+                const double s0 = 1.0 / sqrt(e.w0), s1 = 1.0 / sqrt(e.w1);
+                const double* ctr = kind == 0 ? centers : center_local;
+                ellipse_vertex(ctr[2LL * i], ctr[2LL * i + 1], e, s0, s1, (double)a * step, &x, &y);
+                if (kind == 1) {
+                    x = x + origins[2LL * i];
+                    y = y + origins[2LL * i + 1];
+                }
+            }
+        }
+        contours[2 * t] = x;
+        contours[2 * t + 1] = y;
+    }
+}
+
 // The status names, as the reference's result arrays spell them (numpy "U32": 32 UCS-4 code
 // points per entry, zero-padded).
 #define SPX_STATUS_NAMES(X)                                                                            \
@@ -1083,6 +1129,20 @@ static size_t radial_smem(int hm, int wm, bool smooth) {
 }
 
 constexpr int kRadialScratchCtas = 148 * 4;
+
+int spx_rebuild_contours(int kind, const double* centers, const double* center_local, const double* eigenvalues,
+                         const double* axes, const double* edge_px, const int* origins, int n, int n_angles,
+                         double* contours, void* stream) {
+    SPX_REQUIRE(kind >= 0 && kind <= 2 && n >= 0 && n_angles >= 1, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(contours && (kind != 2 || (center_local && edge_px && origins)) &&
+                    (kind == 2 || (eigenvalues && axes && (kind == 0 ? centers != nullptr : (center_local && origins)))),
+                "null pointer");
+    const long long total = (long long)n * (n_angles + 1);
+    k_rebuild_contours<<<grid_for(total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        kind, centers, center_local, eigenvalues, axes, edge_px, origins, n, n_angles, contours);
+    return check_launch("k_rebuild_contours");
+}
 
 size_t spx_radial_workspace_bytes(int hm, int wm, int smooth) {
     if (radial_smem(hm, wm, smooth != 0)) return 256;

@@ -679,6 +679,34 @@ __global__ void k_clean_stack(Image img, const int* vor, const int4* boxes, cons
     }
 }
 
+// The measured cells from their stored masks (the compact result files' rebuild): out = image -
+// background - (model - own Gaussian) on the mask, 0 elsewhere, with global params, the same
+// arithmetic as k_clean_stack.
+__global__ void k_clean_masked(Image img, const uint8_t* masks, const int* origins, const double* params_global,
+                               int radius_cap, spx_bgmap bg, const double* model, int n, int hm, int wm,
+                               double* out) {
+    const long long total = (long long)n * hm * wm;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        int c, k;
+        divmod_idx(t, hm * wm, &c, &k);
+        double v = 0.0;
+        if (masks[t]) {
+            const int y = origins[2LL * c + 1] + k / wm, x = origins[2LL * c] + k % wm;
+            const double* p = params_global + 6LL * c;
+            const double dx = (double)x - p[1], dy = (double)y - p[2];
+            const int r = render_radius(p, radius_cap);
+            double own = 0.0;
+            if (fabs(dx) <= r && fabs(dy) <= r) {
+                const double aa = exp(p[3]) * dx + p[4] * dy, bb = exp(p[5]) * dy;
+                own = p[0] * exp(-0.5 * (aa * aa + bb * bb));
+            }
+            v = (img.at(y, x) - bg_at(bg, y, x)) - (model[(long long)y * img.W + x] - own);
+        }
+        out[t] = v;
+    }
+}
+
 // ------------------------------------------------------------------------------ tile medians
 
 constexpr int kTileThreads = 512;
@@ -1388,6 +1416,20 @@ int spx_clean_cells(const void* img, int dtype, double sign, int height, int wid
                                                        reinterpret_cast<const int4*>(boxes), params, radius_cap,
                                                        *background, model, which, n_out, hm, wm, out);
     return check_launch("k_clean_stack");
+}
+
+int spx_clean_masked(const void* img, int dtype, double sign, int height, int width, const uint8_t* masks,
+                     const int* origins, const double* params_global, int radius_cap, const spx_bgmap* background,
+                     const double* model, int n, int hm, int wm, double* out, void* stream) {
+    SPX_REQUIRE(n >= 0 && hm >= 0 && wm >= 0 && height > 0 && width > 0, "bad arguments");
+    if (n == 0 || hm == 0 || wm == 0) return SPX_OK;
+    SPX_REQUIRE(img && masks && origins && params_global && background && model && out, "null pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long total = (long long)n * hm * wm;
+    k_clean_masked<<<grid_for(total, 256), 256, 0, s>>>(Image{img, dtype, sign, height, width}, masks, origins,
+                                                        params_global, radius_cap, *background, model, n, hm, wm,
+                                                        out);
+    return check_launch("k_clean_masked");
 }
 
 int spx_tile_medians(const void* img, int dtype, double sign, int height, int width, const double* model,

@@ -441,6 +441,25 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
                   size_t workspace_bytes, void* stream);
 
 
+/* ------------------------------------------------------------------------------------------------
+ * Compact result files (save_cd_results(compact=True) / load_cd_results, subpx/cd.py:878-1131): the
+ * arrays a compact file leaves out are rebuilt on the device from what it keeps.
+ * ---------------------------------------------------------------------------------------------- */
+
+/* Measured cells from their stored masks (n x hm x wm bytes), origins (n x 2 int [x, y]) and global
+ * params (n x 6): image - background - (model - own truncated Gaussian) on the mask, 0 elsewhere
+ * (subpx/cd.py:1116-1131 _rebuild_rois; the same arithmetic as spx_clean_cells). */
+int spx_clean_masked(const void* img, int dtype, double sign, int height, int width, const uint8_t* masks,
+                     const int* origins, const double* params_global, int radius_cap, const spx_bgmap* background,
+                     const double* model, int n, int hm, int wm, double* out, void* stream);
+/* Closed contours (n x (n_angles + 1) x 2) from stored geometry with the measurement kernels'
+ * arithmetic (subpx/_cpu/cd.py:110-128 radial_contours / ellipse_contours): kind 0 gaussian
+ * (centers, eigenvalues, axes), 1 logquad (center_local, eigenvalues, axes, origins), 2 radial
+ * (center_local, edge_px, origins). */
+int spx_rebuild_contours(int kind, const double* centers, const double* center_local, const double* eigenvalues,
+                         const double* axes, const double* edge_px, const int* origins, int n, int n_angles,
+                         double* contours, void* stream);
+
 /* ------------------------------------------------------------------ learned warm start (MLP) */
 
 /* Epilogue of spx_gemm_bf16: x = scale * acc (+ bias[n]); x = 0 where mask_act[m, n] <= 0 (the

@@ -265,8 +265,22 @@ def make_cd(out: Path, ref):
     np.savez_compressed(out / "cd.npz", names=np.array(names), **arrays)
 
 
+def make_results(out: Path, ref):
+    """Result folders written by the reference's own save_cd_results (full and compact) for a small
+    lattice page measured by its CPU path: the file format the loader must read."""
+    from subpx import measure_cds
+    from subpx.cd import save_cd_results
+
+    from imageprocessor_new_b200 import synthetic as S
+
+    img, _ = S.gaussian_lattice(2.0, shape=(64, 112), seed=6)
+    res = measure_cds(img, backend="cpu", methods=("gaussian", "halfmax"), area_max=400)
+    for compact in (False, True):
+        save_cd_results(res, out / ("results_compact" if compact else "results_full"), compact=compact)
+
+
 MAKERS = {"thresholds": make_thresholds, "ccl": make_ccl, "centers": make_centers, "voronoi": make_voronoi,
-          "tiled": make_tiled, "cd": make_cd}
+          "tiled": make_tiled, "cd": make_cd, "results": make_results}
 
 
 def main():
