@@ -1,9 +1,11 @@
 """Autotuner of the launch shapes (no reference counterpart).
 
 The knobs (``spx_tune_set``): warps per block and persistent blocks per SM of the LM fit kernels,
-and the model-render tile. None of them changes a result -- the fits take cells from a device work
-queue and every cell's arithmetic is the same whatever shape runs it; the render sums each pixel's
-Gaussians in cell order in every tile shape -- so the tuner only times them. It times each
+the model-render tile, and how the radial profiles map rays to threads (one ray per thread, or one
+ray per warp with 32 samples at once). None of them changes a result -- the fits take cells from a
+device work queue and every cell's arithmetic is the same whatever shape runs it; the render sums
+each pixel's Gaussians in cell order in every tile shape; both ray mappings evaluate the same
+samples with the same arithmetic and rules -- so the tuner only times them. It times each
 candidate with CUDA events on the caller's own data (one initial fit, one deblending iteration and
 one render of a page's cells), one knob at a time in the order below, and keeps the fastest. A
 choice is cached per device name and workload size class in a JSON file (``SPX_TUNE_CACHE``, or
@@ -27,6 +29,7 @@ KNOBS = {
     "fit_warps": (2, 4, 8),
     "fit_blocks_per_sm": (4, 8, 16),
     "render_tile": (16, 32),
+    "radial_rays": (0, 1),
 }
 
 
@@ -91,10 +94,26 @@ def tune(page_d: torch.Tensor, *, sign: float = 1.0, repeats: int = 3, use_cache
     model = dbl.render(params)
     bg, _ = dbl.background_of(model, dbl.stats(params, status))
 
+    h, w = dbl.shape
+    c = dbl.cells
+    cleaned = dev.empty((max(c.n, 1), c.hm, c.wm), torch.float64)
+    if c.n:
+        _lib.call("spx_clean_cells", dbl.img.data_ptr(), dbl.dtype, dbl.sign, h, w, c.voronoi.data_ptr(),
+                  c.boxes.data_ptr(), params.data_ptr(), max(dbl.radius_cap, 2), bg.struct(), model.data_ptr(), None,
+                  c.n, c.hm, c.wm, cleaned.data_ptr(), dev.stream_ptr())
+    from .cd import _method_buffers
+
+    hb, hs = _method_buffers(c.n, 128, "halfmax", False)
+    gb, gs = _method_buffers(c.n, 128, "gradient", False)
+    rws = dev.workspace(_lib.size("spx_radial_workspace_bytes", c.hm, c.wm, 0))
+
     def workload():
         dbl.initial(dbl.max_iter)
         dbl.iteration(params, model, bg)
         dbl.render(params)
+        if c.n:
+            _lib.call("spx_radial_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(), None, c.n, c.hm,
+                      c.wm, w, 128, 0.1, None, 0, hs, gs, rws.data_ptr(), rws.numel(), dev.stream_ptr())
 
     timings = {}
     for knob, values in KNOBS.items():

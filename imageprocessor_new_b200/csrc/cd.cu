@@ -648,6 +648,24 @@ struct SplineWindowF {
     }
 };
 
+// One FP32 spline sample from the 4 x 4 window at (iy - 1, ix - 1) of the FP32 coefficient copy:
+// the arithmetic of SplineWindowF::at without the cached window.
+__device__ __forceinline__ float spline_sample_f(const float* coef, int wp, int iy, int ix, float ty, float tx) {
+    float wy[4], wx[4];
+    SplineWindowF::weights(ty, wy);
+    SplineWindowF::weights(tx, wx);
+    const float* q = coef + (iy - 1) * wp + (ix - 1);
+    float out = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        float row = 0.0f;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) row = fmaf(q[a * wp + b], wx[b], row);
+        out = fmaf(row, wy[a], out);
+    }
+    return out;
+}
+
 // floor(y) for 0 <= y < 2^51 as an int and as a double, with FP64 additions only (no conversion
 // instructions): y + 1.5 * 2^52 holds y rounded to an integer in its low mantissa bits, and one
 // comparison turns the rounding into a floor.
@@ -674,11 +692,13 @@ constexpr int kTrigMax = 256;  // ray angles with a cos / sin table in shared me
 // different shared-memory banks.
 __host__ __device__ inline int radial_pitch(int wm) { return (wm + 2 * kPad) | 1; }
 
-// With smoothing, three more hm x wm planes follow (the two axis-0 passes and the smoothed signal).
+// The masks are three byte planes (cell, eroded cell, and per pixel square whether its four corners
+// are all in the eroded cell). With smoothing, three more hm x wm doubles follow (the two axis-0
+// passes and the smoothed signal).
 __host__ __device__ inline long long radial_cta_doubles(int hm, int wm, bool smooth = false) {
     const long long np = (long long)(hm + 2 * kPad) * radial_pitch(wm);
     const long long nf = (long long)(hm + 2 * kPad) * (wm + 2 * kPad);
-    return np + (nf + 1) / 2 + 32 + (2LL * hm * wm + 7) / 8 + (smooth ? 3LL * hm * wm : 0);
+    return np + (nf + 1) / 2 + 32 + (3LL * hm * wm + 7) / 8 + (smooth ? 3LL * hm * wm : 0);
 }
 
 // One output of scipy's correlate1d with a symmetric kernel (weights w[0..2r], centre w[r]) and
@@ -788,7 +808,12 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
 // the signal (zero outside the cell) and the mask are each filtered along y then x with zero edges
 // (scipy's gaussian_filter, mode="constant"), and the spline is fitted to their ratio over the whole
 // cell box; the centroid still comes from the unsmoothed signal.
-template <bool kSmooth>
+// kWarpRays: the ray loop maps one ray to one warp, its lanes taking 32 consecutive samples at a
+// time (positions, validity and spline samples with no per-lane caching, so no divergent reloads),
+// with the halfmax crossing and the gradient maximum found by ballots and shuffles; the results are
+// bit for bit those of the one-ray-per-thread loop (same sample arithmetic, same first-crossing and
+// first-maximum rules).
+template <bool kSmooth, bool kWarpRays>
 __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
     int n_angles, double radial_step, int n_radii, const double* smooth_w, int smooth_r, double* coef_scratch,
@@ -809,6 +834,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     double* red = coef + (long long)hp * dp + ((long long)hp * wp + 1) / 2;  // 32 doubles: 8 slots of 4
     uint8_t* mask = reinterpret_cast<uint8_t*>(red + 32);
     uint8_t* emask = mask + area_px;
+    uint8_t* full = emask + area_px;  // square [iy, iy+1] x [ix, ix+1] inside the eroded cell
     const double thr = fmax(0.35, 2.0 * radial_step);
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
         const int j = which ? which[i] : i;
@@ -849,7 +875,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         // Spline coefficients (the cell padded by 12 edge pixels) and the eroded cell (cross
         // structure, zero outside the stack), where ray samples stay valid.
         if constexpr (kSmooth) {
-            double* ts = reinterpret_cast<double*>(mask) + (2LL * area_px + 7) / 8;  // after both masks
+            double* ts = reinterpret_cast<double*>(mask) + (3LL * area_px + 7) / 8;  // after the masks
             double* tm = ts + area_px;
             double* fs = tm + area_px;
             double* sig = coef;  // the masked signal, staged in the coefficient plane (hp * wp >= hm * wm)
@@ -892,6 +918,11 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                        mask[k - 1] && mask[k + 1];
         }
         __syncthreads();
+        if constexpr (kWarpRays)
+            for (int k = tid; k < area_px; k += kRadialThreads) {
+                const int yy = k / wm, xx = k % wm;
+                full[k] = yy + 1 < hm && xx + 1 < wm && emask[k] && emask[k + 1] && emask[k + wm] && emask[k + wm + 1];
+            }
         for (int col = tid; col < wp; col += kRadialThreads) spline_line(coef + col, hp, dp);
         __syncthreads();
         for (int row = tid; row < hp; row += kRadialThreads) spline_line(coef + (long long)row * dp, wp, 1);
@@ -904,7 +935,106 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         int j_min = 2;  // first gradient candidate: j >= 2 and j * step >= thr
         while ((double)j_min * radial_step < thr) ++j_min;
         int found_h = 0, found_g = 0;
-        for (int ray = tid; ray < n_angles; ray += kRadialThreads) {
+        if constexpr (kWarpRays) {
+            const int lane = tid & 31;
+            const float halff = (float)half;
+            const double ymax = (double)(hm - 1), xmax = (double)(wm - 1);
+            for (int ray = warp; ray < n_angles; ray += kRadialThreads / 32) {
+                double edge_h = dnan(), edge_g = dnan();
+                if (peak > 0.0) {
+                    const double ang = (double)ray * (2.0 * kPi / n_angles);
+                    const double ux = trig ? trig[2 * ray] : cos(ang), uy = trig ? trig[2 * ray + 1] : sin(ang);
+                    float c1 = 0, c2 = 0, c3 = 0, c4 = 0;  // p[k0-1] .. p[k0-4] of the previous chunk
+                    bool crossed = false;
+                    float best = -INFINITY, dl = 0, dm = 0, dr = 0;
+                    int best_j = -1, first_invalid = n_radii;
+                    for (int k0 = 0; k0 < n_radii; k0 += 32) {
+                        const int k = k0 + lane;
+                        bool valid = false;
+                        float p = 0.0f;
+                        if (k < n_radii) {
+                            const double r = (double)k * radial_step;
+                            const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
+                            if (y >= 0.0 && y <= ymax && x >= 0.0 && x <= xmax) {
+                                double fyd, fxd;
+                                const int iy = floor_nonneg(y, &fyd), ix = floor_nonneg(x, &fxd);
+                                valid = full[iy * wm + ix] || inside_bytes(emask, hm, wm, y, x);
+                                if (valid)
+                                    p = k == 0 ? (float)peak
+                                               : spline_sample_f(coef_f, wp, iy + kPad, ix + kPad, (float)(y - fyd),
+                                                                 (float)(x - fxd));
+                            }
+                        }
+                        const unsigned inv = __ballot_sync(0xffffffffu, k < n_radii && !valid);
+                        const int lim = inv ? k0 + __ffs(inv) - 1 : min(k0 + 32, n_radii);  // processed: k < lim
+                        if (inv) first_invalid = lim;
+                        const bool proc = k < lim;
+                        // p[k - m] for m = 1..4 (lanes below m take the previous chunk's values).
+                        float pm1 = __shfl_up_sync(0xffffffffu, p, 1), pm2 = __shfl_up_sync(0xffffffffu, p, 2);
+                        float pm3 = __shfl_up_sync(0xffffffffu, p, 3), pm4 = __shfl_up_sync(0xffffffffu, p, 4);
+                        if (lane < 1) pm1 = c1;
+                        if (lane < 2) pm2 = lane == 0 ? c2 : c1;
+                        if (lane < 3) pm3 = lane == 0 ? c3 : (lane == 1 ? c2 : c1);
+                        if (lane < 4) pm4 = lane == 0 ? c4 : (lane == 1 ? c3 : (lane == 2 ? c2 : c1));
+                        // Half-height: the first processed k >= 1 with p[k-1] >= half > p[k].
+                        if (!crossed) {
+                            const unsigned hc = __ballot_sync(0xffffffffu, proc && k >= 1 && pm1 >= halff && p < halff);
+                            if (hc) {
+                                const int f = __ffs(hc) - 1;
+                                double e = 0.0;
+                                if (lane == f)
+                                    e = (double)(k - 1) * radial_step +
+                                        (((double)pm1 - half) / ((double)pm1 - (double)p)) * radial_step;
+                                edge_h = __shfl_sync(0xffffffffu, e, f);
+                                crossed = true;
+                            }
+                        }
+                        // Gradient: candidate j = k - 2 (sample k valid) with d = p[j-1] - p[j+1]; the
+                        // first maximum over all candidates.
+                        const int jj = k - 2;
+                        const bool cand = proc && jj >= j_min && jj <= n_radii - 3;
+                        const float d = cand ? pm3 - pm1 : -INFINITY;
+                        float m = d;
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+                        if (m > best) {
+                            const int f = __ffs(__ballot_sync(0xffffffffu, cand && d == m)) - 1;
+                            const float l4 = __shfl_sync(0xffffffffu, pm4 - pm2, f);
+                            const float r2 = __shfl_sync(0xffffffffu, pm2 - p, f);
+                            best = m;
+                            best_j = k0 + f - 2;
+                            dm = m;
+                            dl = l4;
+                            dr = r2;
+                        }
+                        if (inv || k0 + 32 >= n_radii) break;
+                        c1 = __shfl_sync(0xffffffffu, p, 31);
+                        c2 = __shfl_sync(0xffffffffu, p, 30);
+                        c3 = __shfl_sync(0xffffffffu, p, 29);
+                        c4 = __shfl_sync(0xffffffffu, p, 28);
+                    }
+                    if (best_j >= 0) {
+                        const int j = best_j;
+                        const double gm = (double)dm * inv2s, gl = (double)dl * inv2s, gr = (double)dr * inv2s;
+                        const bool left_ok = j - 1 >= j_min;
+                        const bool right_ok = j + 1 <= n_radii - 3 && j + 3 < first_invalid;
+                        const double curv = gl - 2.0 * gm + gr;
+                        if (left_ok && right_ok && gm >= gl && gm >= gr && gm > 0.01 * peak && curv < -1e-12) {
+                            double delta = 0.5 * (gl - gr) / curv;
+                            delta = delta < -0.5 ? -0.5 : (delta > 0.5 ? 0.5 : delta);
+                            edge_g = (double)j * radial_step + delta * radial_step;
+                        }
+                    }
+                }
+                if (lane == 0) {
+                    if (half_out.status) half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
+                    if (grad_out.status) grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
+                    found_h += isfinite(edge_h);
+                    found_g += isfinite(edge_g);
+                }
+            }
+        }
+        for (int ray = kWarpRays ? n_angles : tid; ray < n_angles; ray += kRadialThreads) {
             double edge_h = dnan(), edge_g = dnan();
             if (peak > 0.0) {
                 const double ang = (double)ray * (2.0 * kPi / n_angles);
@@ -1151,7 +1281,7 @@ size_t spx_radial_workspace_bytes(int hm, int wm, int smooth) {
 
 }  // extern "C"
 
-template <bool kSmooth>
+template <bool kSmooth, bool kWarpRays>
 static int launch_radial(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
                          int wm, int width, int n_angles, double radial_step, int n_radii, const double* smooth_w,
                          int smooth_r, const spx_method_out* halfmax, const spx_method_out* gradient, void* workspace,
@@ -1161,16 +1291,17 @@ static int launch_radial(const double* cleaned, const int* voronoi, const int* b
     int blocks;
     if (smem) {
         if (smem + 2 * kTrigMax * sizeof(double) > 48 * 1024)  // with the static cos / sin table
-            SPX_CUDA(cudaFuncSetAttribute(k_radial_cd<kSmooth>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            SPX_CUDA(cudaFuncSetAttribute(k_radial_cd<kSmooth, kWarpRays>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
         int per_sm = 0;
-        SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd<kSmooth>, kRadialThreads, smem));
+        SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd<kSmooth, kWarpRays>, kRadialThreads,
+                                                               smem));
         blocks = (int)std::min<long long>(n, 148LL * std::max(per_sm, 1));
     } else {
         scratch = static_cast<double*>(workspace);
         blocks = std::min(n, kRadialScratchCtas);
     }
-    k_radial_cd<kSmooth><<<blocks, kRadialThreads, smem, s>>>(
+    k_radial_cd<kSmooth, kWarpRays><<<blocks, kRadialThreads, smem, s>>>(
         cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm, wm, width, n_angles, radial_step, n_radii,
         smooth_w, smooth_r, scratch, method_out(halfmax), method_out(gradient));
     return check_launch("k_radial_cd");
@@ -1194,11 +1325,18 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
     // radii = np.arange(0, hypot(hm, wm) + step, step)
     const double stop = hypot((double)hm, (double)wm) + radial_step;
     const int n_radii = (int)ceil(stop / radial_step);
+    const bool warp_rays = tuning().radial_rays == 1;
     if (smooth)
-        return launch_radial<true>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles, radial_step, n_radii,
-                                   smooth_weights, smooth_radius, halfmax, gradient, workspace, s);
-    return launch_radial<false>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles, radial_step, n_radii,
-                                nullptr, 0, halfmax, gradient, workspace, s);
+        return warp_rays ? launch_radial<true, true>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
+                                                     radial_step, n_radii, smooth_weights, smooth_radius, halfmax,
+                                                     gradient, workspace, s)
+                         : launch_radial<true, false>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
+                                                      radial_step, n_radii, smooth_weights, smooth_radius, halfmax,
+                                                      gradient, workspace, s);
+    return warp_rays ? launch_radial<false, true>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
+                                                  radial_step, n_radii, nullptr, 0, halfmax, gradient, workspace, s)
+                     : launch_radial<false, false>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
+                                                   radial_step, n_radii, nullptr, 0, halfmax, gradient, workspace, s);
 }
 
 }  // extern "C"

@@ -602,9 +602,12 @@ __global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const d
         sorted[rank] = id;
     }
     __syncthreads();
-    // Each candidate's centre, radius, amplitude and precision factors are staged once per tile
-    // (chunks of 256), so a pixel term costs one exp.
-    __shared__ double s_cx[256], s_cy[256], s_r[256], s_a[256], s_e1[256], s_u2[256], s_e3[256];
+    // Each candidate's centre, amplitude, precision factors and the integer bounds of its truncated
+    // square are staged once per tile (chunks of 256), so a pixel tests a candidate with integer
+    // compares and a term costs one exp. |x - cx| <= r <=> ceil(cx - r) <= x <= floor(cx + r) for
+    // integer x and r: x - cx and cx -+ r are exact in FP64 for coordinates below 2^16.
+    __shared__ double s_cx[256], s_cy[256], s_a[256], s_e1[256], s_u2[256], s_e3[256];
+    __shared__ int4 s_box[256];  // x lo, x hi, y lo, y hi
     constexpr int kRows = kRenderTile * kRenderTile / 256;
     const int x = tx0 + (threadIdx.x % kRenderTile), yb = ty0 + (threadIdx.x / kRenderTile);
     double acc[kRows];
@@ -615,9 +618,11 @@ __global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const d
         if ((int)threadIdx.x < cn) {
             const int id = sorted[c0 + threadIdx.x];
             const double* p = params + 6LL * id;
-            s_cx[threadIdx.x] = centres[2LL * id];
-            s_cy[threadIdx.x] = centres[2LL * id + 1];
-            s_r[threadIdx.x] = (double)radius[id];
+            const double cxv = centres[2LL * id], cyv = centres[2LL * id + 1], rv = (double)radius[id];
+            s_cx[threadIdx.x] = cxv;
+            s_cy[threadIdx.x] = cyv;
+            s_box[threadIdx.x] = make_int4((int)ceil(cxv - rv), (int)floor(cxv + rv), (int)ceil(cyv - rv),
+                                           (int)floor(cyv + rv));
             s_a[threadIdx.x] = p[0];
             s_e1[threadIdx.x] = exp(p[3]);
             s_u2[threadIdx.x] = p[4];
@@ -625,13 +630,14 @@ __global__ void __launch_bounds__(256) k_render(int H, int W, BinGrid g, const d
         }
         __syncthreads();
         for (int k = 0; k < cn; ++k) {
-            const double r = s_r[k];
+            const int4 bx = s_box[k];
+            if (x < bx.x || x > bx.y) continue;
             const double dx = (double)x - s_cx[k];
-            if (fabs(dx) > r) continue;
 #pragma unroll
             for (int q = 0; q < kRows; ++q) {
-                const double dy = (double)(yb + q * (256 / kRenderTile)) - s_cy[k];
-                if (fabs(dy) > r) continue;
+                const int yq = yb + q * (256 / kRenderTile);
+                if (yq < bx.z || yq > bx.w) continue;
+                const double dy = (double)yq - s_cy[k];
                 const double aa = s_e1[k] * dx + s_u2[k] * dy, bb = s_e3[k] * dy;
                 const double val = s_a[k] * exp(-0.5 * (aa * aa + bb * bb));
                 if (val != 0.0) acc[q] += val;

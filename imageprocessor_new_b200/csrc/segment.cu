@@ -1056,6 +1056,9 @@ int spx_tune_set(const char* knob, int value) {
     } else if (!strcmp(knob, "render_tile")) {
         SPX_REQUIRE(value == 16 || value == 32, "render_tile must be 16 or 32");
         t.render_tile = value;
+    } else if (!strcmp(knob, "radial_rays")) {
+        SPX_REQUIRE(value == 0 || value == 1, "radial_rays must be 0 or 1");
+        t.radial_rays = value;
     } else {
         set_error("unknown tuning knob '%s'", knob);
         return SPX_ERR_ARGUMENT;
@@ -1069,6 +1072,7 @@ int spx_tune_get(const char* knob, int* value) {
     if (!strcmp(knob, "fit_warps")) *value = t.fit_warps;
     else if (!strcmp(knob, "fit_blocks_per_sm")) *value = t.fit_blocks_per_sm;
     else if (!strcmp(knob, "render_tile")) *value = t.render_tile;
+    else if (!strcmp(knob, "radial_rays")) *value = t.radial_rays;
     else {
         set_error("unknown tuning knob '%s'", knob);
         return SPX_ERR_ARGUMENT;

@@ -315,8 +315,12 @@ def _rebuild_rois(arrays, model, sign) -> np.ndarray:
     else:  # a full map of one level (background_level given) or without tiles
         bg = Background((h, w), max(h, w)).set_fixed(float(sign * np.asarray(arrays["background_map"]).flat[0]))
     out = dev.empty((n, hm, wm), torch.float64)
-    _lib.call("spx_clean_masked", img_d.data_ptr(), dev.dtype_code(img_d), float(sign), h, w,
-              dev.upload(masks.astype(np.uint8)).data_ptr(), dev.upload(np.ascontiguousarray(origins, np.int32)).data_ptr(),
-              dev.upload(params[report]).data_ptr(), max(radius_cap, 2), bg.struct(), model_d.data_ptr(), n, hm, wm,
+    # Uploads held in names until the launch: a temporary's block could be reused by the next upload
+    # (enqueued before the kernel) on the same stream.
+    masks_d = dev.upload(masks.astype(np.uint8))
+    origins_d = dev.upload(np.ascontiguousarray(origins, np.int32))
+    own_d = dev.upload(params[report])
+    _lib.call("spx_clean_masked", img_d.data_ptr(), dev.dtype_code(img_d), float(sign), h, w, masks_d.data_ptr(),
+              origins_d.data_ptr(), own_d.data_ptr(), max(radius_cap, 2), bg.struct(), model_d.data_ptr(), n, hm, wm,
               out.data_ptr(), dev.stream_ptr())
     return out.cpu().numpy()

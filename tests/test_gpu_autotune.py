@@ -58,3 +58,28 @@ def test_every_setting_gives_identical_results(tmp_path, monkeypatch):
         assert again["config"] == res["config"]
     finally:
         autotune.apply(before)
+
+
+def test_radial_ray_mappings_give_identical_cds():
+    """One ray per thread and one ray per warp: the same edges, statuses and metrics bit for bit,
+    with and without profile smoothing."""
+    from imageprocessor_new_b200 import autotune, measure_cds, synthetic
+
+    before = autotune.current()
+    page = synthetic.page_staggered(2, shape=(768, 1024)).image
+    try:
+        for smooth in (0.0, 1.0):
+            res = []
+            for mode in (0, 1):
+                autotune.set("radial_rays", mode)
+                res.append(measure_cds(page, backend="gpu", methods=("gradient", "halfmax"), area_max=400,
+                                       smooth_sigma=smooth))
+            for m in ("gradient", "halfmax"):
+                a, b = res[0].measurements[m], res[1].measurements[m]
+                np.testing.assert_array_equal(a.geometry["edge_px"], b.geometry["edge_px"])
+                np.testing.assert_array_equal(a.status, b.status)
+                np.testing.assert_array_equal(a.contours_xy, b.contours_xy)
+                for k in a.metrics:
+                    np.testing.assert_array_equal(a.metrics[k], b.metrics[k], err_msg=k)
+    finally:
+        autotune.apply(before)
