@@ -268,7 +268,9 @@ def gpu_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded render + noise)",
         "config": {"workload": _workload(args.page), "image": f"{args.page}x{args.page} uint16",
                    "cells_per_step": per_step_cells,
-                   "methods": list(METHODS), "refiners": list(REFINERS), "l2": "inputs larger than L2 (134 MB page)",
+                   "methods": list(METHODS), "refiners": list(REFINERS),
+                   "l2": f"inputs {'larger' if page.nbytes > 126e6 else 'smaller'} than L2 "
+                         f"({page.nbytes / 1e6:.0f} MB page)",
                    "warm_start": "plain LM (no network)"},
         "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(page.nbytes) * (len(REFINERS) + 1),
                 "d2h_bytes_per_step": d2h},
@@ -320,6 +322,31 @@ def _accuracy(warm, plain) -> dict:
                if both.any() else 0.0)
         out[name] = {"centre_max_px": dc, "cd_max_px": dcd, "same_validity": float((a.valid == b.valid).mean())}
     return out
+
+
+def fp64_peak_tflops(repeats: int = 5) -> float:
+    """The device's FP64 rate measured here (spx_fp64_fma_rate: independent FMA chains on every SM,
+    CUDA events, best of `repeats`), the denominator of the LM kernel's FP64 roofline."""
+    import ctypes
+
+    import torch
+
+    from imageprocessor_new_b200 import _lib
+
+    lib = _lib.lib()
+    blocks = 148 * 16
+    sink = torch.empty(blocks * 256, dtype=torch.float64, device="cuda")
+    flops = ctypes.c_double(0.0)
+    stream = torch.cuda.current_stream().cuda_stream
+    best = 0.0
+    for _ in range(repeats + 1):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        _lib.call("spx_fp64_fma_rate", blocks, 4096, sink.data_ptr(), ctypes.byref(flops), stream)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, flops.value / (s.elapsed_time(e) / 1e3) / 1e12)
+    return best
 
 
 def _accuracy_vs_oracle(crop, oracle_res) -> dict:

@@ -69,6 +69,7 @@ SIGNATURES = {
     "spx_version": (_I, []),
     "spx_launch_count": (ctypes.c_ulonglong, []),
     "spx_device_info": (_I, [POINTER(c_int), POINTER(c_int)]),
+    "spx_fp64_fma_rate": (_I, [_I, _I, _P, POINTER(c_double), _P]),
     "spx_otsu_workspace_bytes": (_S, [_I]),
     "spx_otsu": (_I, [_P, _I, _I, _I, _I, _P, _P, _S, _P]),
     "spx_otsu_static": (_I, [_P, _I, _I, _I, _I, _P, _P]),
@@ -135,6 +136,7 @@ SIGNATURES = {
     "spx_radial_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _P, _I, _MO, _MO, _P, _S, _P]),
     "spx_minimum_filter": (_I, [_P, _I, _I, _I, _P, _P, _P]),
+    "spx_support_labels": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P]),
     "spx_clean_masked": (_I, [_P, _I, _D, _I, _I, _P, _P, _P, _I, _BG, _P, _I, _I, _I, _P, _P]),
     "spx_rebuild_contours": (_I, [_I, _P, _P, _P, _P, _P, _P, _I, _I, _P, _P]),
     "spx_signal_image": (_I, [_P, _I, _D, _I, _I, _P, _P]),

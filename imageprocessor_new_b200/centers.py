@@ -20,6 +20,9 @@ from .types import CenterResult
 _SUPPORTED_REFINE = ("none", "weighted", "logquad", "logquadratic", "edge_gradmoment", "edge_moment",
                      "edges_centered", "auto")
 _VORONOI_METHODS = {"radial_symmetry", "isophote_curvature"}
+# Refiners of ROI stacks, which detect_centers(background="model") can re-run on deblended cells
+# (subpx/centers.py:34; the Voronoi refiners are outside this package).
+_DEBLEND_METHODS = {"weighted", "logquad", "logquadratic", "none"}
 
 
 def choose_refine_method_for_bbox(width: float, height: float, *, small_feature_max: float = 12.0) -> str:
@@ -150,13 +153,26 @@ def detect_centers(
         raise ValueError(f"Unsupported refine method: {refine}")
     if background not in (None, "model"):
         raise ValueError("background must be None or 'model'")
-    if background == "model":
-        raise NotImplementedError("background='model' centre re-refinement is not part of this package yet")
+    if background == "model" and refine not in _DEBLEND_METHODS:
+        raise NotImplementedError(
+            f"background='model' is not supported for refine='{refine}': edge methods read the full image rather "
+            "than per-cell ROIs. Use one of " + ", ".join(sorted(_DEBLEND_METHODS)) + ".")
     if connectivity not in (4, 8):
         raise ValueError("connectivity must be 4 or 8")
     if int(morph_open) < 0 or int(morph_close) < 0:
         raise ValueError("morph_open and morph_close must be >= 0")
     img = _as_image(image)
+    if background == "model":
+        result = detect_centers(img, backend=backend, threshold=threshold, invert=invert, area_min=area_min,
+                                area_max=area_max, morph_open=morph_open, morph_close=morph_close, pad=pad,
+                                refine=refine, connectivity=connectivity, gpu_batch=gpu_batch, device=device,
+                                use_float64=use_float64, components_backend=components_backend,
+                                small_feature_max=small_feature_max, upsample_factor=upsample_factor,
+                                tile_h=tile_h, overlap=overlap, threshold_mode=threshold_mode,
+                                otsu_downsample=otsu_downsample, thr_scale=thr_scale, dedupe_eps=dedupe_eps)
+        with dev.on_device(device):
+            return _refine_deblended(img, result, refine=refine, invert=invert, pad=int(pad),
+                                     iterations=int(deblend_iterations), tile_h=tile_h, overlap=int(overlap))
     with dev.on_device(device):
         if tile_h is not None:
             return _detect_tiled(img, threshold=threshold, invert=invert, area_min=area_min, area_max=area_max,
@@ -180,6 +196,77 @@ def detect_centers(
         "small_feature_max": float(small_feature_max),
     }
     return CenterResult(centers_xy=arr, method=f"threshold={threshold}, refine={refine}", backend="gpu", meta=meta)
+
+
+def _deblended_cells_centers(img_d: torch.Tensor, sign: float, seeds: np.ndarray, *, refine: str, pad: int,
+                             iterations: int):
+    """Centres of `seeds` re-refined on deblended cells (subpx/centers.py:224-268): square cells of
+    2 ceil(0.6 pitch) + 1 around each seed cut by the Voronoi partition, a deblend of the image
+    (background map and every hole's Gaussian), then the refiner on each cleaned cell restricted to
+    its pixels above 0.2 x its peak. Returns (global centres with NaN rows, cell mask pixel counts,
+    the deblend state)."""
+    from .deblend import Deblender, auto_tile, build_cells
+
+    h, w = (int(v) for v in img_d.shape)
+    seeds_d = dev.upload(np.ascontiguousarray(seeds, dtype=np.float64))
+    pitch = auto_tile(seeds_d, len(seeds), (h, w))[1]
+    half = int(np.ceil(0.6 * pitch)) if np.isfinite(pitch) else 16
+    rows = np.column_stack((seeds[:, 0] - half, seeds[:, 1] - half, np.full(len(seeds), 2 * half + 1.0),
+                            np.full(len(seeds), 2 * half + 1.0), seeds[:, 0], seeds[:, 1])).reshape(-1, 6)
+    cells = build_cells(rows, (h, w), pad)
+    dbl = Deblender(img_d, sign, cells)
+    state = dbl.run(iterations=iterations)
+    n, hm, wm = cells.n, cells.hm, cells.wm
+    if n == 0:
+        return np.zeros((0, 2)), np.zeros(0, np.int64), state
+    cleaned = dbl.cleaned(state)
+    labels = dev.empty((n * hm, wm), torch.int32)
+    refine_rows = dev.empty((n, 5), torch.int32)
+    stream = dev.stream_ptr()
+    _lib.call("spx_support_labels", cleaned.data_ptr(), cells.voronoi.data_ptr(), cells.boxes.data_ptr(),
+              state.params_d.data_ptr(), n, hm, wm, w, labels.data_ptr(), refine_rows.data_ptr(), stream)
+    methods = torch.full((n,), _lib.REFINE_CODES[refine], dtype=torch.uint8, device="cuda")
+    local = dev.empty((n, 2), torch.float64)
+    _lib.call("spx_refine_centers", cleaned.data_ptr(), _lib.DTYPES[np.dtype(np.float64)], n * hm, wm,
+              labels.data_ptr(), refine_rows.data_ptr(), methods.data_ptr(), n, 0, local.data_ptr(), stream)
+    centres = local.cpu().numpy()
+    centres[:, 1] -= np.arange(n) * hm  # window row -> cell row
+    centres += cells.origins
+    return centres, cells.counts.cpu().numpy().astype(np.int64), state
+
+
+def _refine_deblended(img, result: CenterResult, *, refine, invert, pad, iterations, tile_h, overlap) -> CenterResult:
+    """detect_centers(background="model") (subpx/centers.py:271-314): the centres found without it
+    re-refined on deblended cells, in row strips of tile_h (with +-overlap halos) when tiled."""
+    sign = -1.0 if invert else 1.0
+    seeds = np.asarray(result.centers_xy, dtype=np.float64).reshape(-1, 2)
+    img_d = _device_image(img)
+    height = img_d.shape[0]
+    bands = [(0, height)] if not tile_h else [(y0, min(height, y0 + int(tile_h))) for y0 in range(0, height,
+                                                                                                   int(tile_h))]
+    centers, statuses, used, sources = [], [], 0, set()
+    for y0, y1 in bands:
+        lo, hi = (0, height) if not tile_h else (max(0, y0 - int(overlap)), min(height, y1 + int(overlap)))
+        own = (seeds[:, 1] >= y0) & (seeds[:, 1] < y1)
+        if not own.any():
+            continue
+        inside = (seeds[:, 1] >= lo) & (seeds[:, 1] < hi)
+        found, _, state = _deblended_cells_centers(img_d[lo:hi].contiguous(), sign, seeds[inside] - [0, lo],
+                                                   refine=refine, pad=pad, iterations=iterations)
+        keep = own[inside]
+        centers.append(found[keep] + [0, lo])
+        statuses.append(state.status[keep])
+        used = max(used, state.iterations)
+        sources.add(state.background_info.get("source"))
+    centers = np.concatenate(centers) if centers else np.zeros((0, 2))
+    finite = np.isfinite(centers).all(axis=1)
+    status = np.concatenate(statuses) if statuses else np.zeros(0, "U32")
+    names, counts = np.unique(status, return_counts=True)
+    meta = dict(result.meta)
+    meta.update(background="model", deblend_iterations=int(iterations), deblend_iterations_used=int(used),
+                deblend_status_counts=dict(zip(names.tolist(), counts.tolist())),
+                background_source=sorted(s for s in sources if s), deblend_dropped_nonfinite=int((~finite).sum()))
+    return CenterResult(centers_xy=centers[finite], method=result.method, backend=result.backend, meta=meta)
 
 
 def _detect_tiled(img, *, threshold, invert, area_min, area_max, pad, refine, connectivity, small_feature_max,

@@ -713,6 +713,40 @@ __global__ void k_clean_masked(Image img, const uint8_t* masks, const int* origi
     }
 }
 
+// Support labels of deblended cells for re-refining their centres (detect_centers with
+// background="model", subpx/centers.py:258-268): cell j's window of the (n x hm x wm) cleaned stack,
+// laid out as rows j*hm .. j*hm + hm - 1 of a tall image, gets label j + 1 where the cell's mask
+// holds and the cleaned value exceeds 0.2 x the peak (the fitted amplitude when finite and
+// positive, else the largest cleaned value on the mask); rows_out[j] = the window as a refine row
+// [0, j*hm, wm, hm, j + 1]. One warp per cell.
+__global__ void k_support_labels(const double* cleaned, const int* vor, const int4* boxes, const double* params, int n,
+                                 int hm, int wm, int W, int* labels, int* rows_out) {
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    const int area = hm * wm;
+    for (int j = blockIdx.x * warps + (threadIdx.x >> 5); j < n; j += gridDim.x * warps) {
+        const int4 b = boxes[j];
+        const double* c = cleaned + (long long)j * area;
+        auto inside = [&](int k) {
+            const int yy = k / wm, xx = k % wm;
+            return yy < b.w && xx < b.z && vor[(long long)(b.y + yy) * W + b.x + xx] == j;
+        };
+        double peak = params[6LL * j];
+        if (!(isfinite(peak) && peak > 0.0)) {
+            double m = -dinf();
+            for (int k = lane; k < area; k += 32)
+                if (inside(k)) m = fmax(m, c[k]);
+            peak = warp_max(m);
+        }
+        const double level = __dmul_rn(0.2, peak);
+        for (int k = lane; k < area; k += 32)
+            labels[(long long)j * area + k] = (inside(k) && c[k] > level) ? j + 1 : 0;
+        if (lane < 5) {
+            const int v[5] = {0, j * hm, wm, hm, j + 1};
+            rows_out[5LL * j + lane] = v[lane];
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------ tile medians
 
 constexpr int kTileThreads = 512;
@@ -1436,6 +1470,17 @@ int spx_clean_masked(const void* img, int dtype, double sign, int height, int wi
                                                         params_global, radius_cap, *background, model, n, hm, wm,
                                                         out);
     return check_launch("k_clean_masked");
+}
+
+int spx_support_labels(const double* cleaned, const int* voronoi, const int* boxes, const double* params, int n,
+                       int hm, int wm, int width, int* labels, int* rows_out, void* stream) {
+    SPX_REQUIRE(n >= 0 && hm >= 0 && wm >= 0 && width > 0, "bad arguments");
+    if (n == 0 || hm == 0 || wm == 0) return SPX_OK;
+    SPX_REQUIRE(cleaned && voronoi && boxes && params && labels && rows_out, "null pointer");
+    SPX_REQUIRE((long long)n * hm < (1LL << 31), "cell stack too tall");
+    k_support_labels<<<grid_for(n, 8, 148 * 16), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        cleaned, voronoi, reinterpret_cast<const int4*>(boxes), params, n, hm, wm, width, labels, rows_out);
+    return check_launch("k_support_labels");
 }
 
 int spx_tile_medians(const void* img, int dtype, double sign, int height, int width, const double* model,

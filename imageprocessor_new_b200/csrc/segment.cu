@@ -1082,6 +1082,37 @@ int spx_tune_get(const char* knob, int* value) {
 
 unsigned long long spx_launch_count(void) { return __atomic_load_n(&spx::g_launches, __ATOMIC_RELAXED); }
 
+}  // extern "C"
+
+namespace spx {
+namespace {
+// Eight independent FP64 FMA chains per thread (no dependency between them, so the FP64 pipe, not
+// the FMA latency, bounds the rate); the sums go to `sink` so nothing is optimised away.
+__global__ void __launch_bounds__(256) k_fp64_fma_rate(int iters, double* sink) {
+    double a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = 1.0 + 1e-3 * (threadIdx.x + q);
+    const double b = 0.9999999, c = 1e-7;
+    for (int i = 0; i < iters; ++i)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) a[q] = __fma_rn(a[q], b, c);
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t += a[q];
+    sink[blockIdx.x * blockDim.x + threadIdx.x] = t;
+}
+}  // namespace
+}  // namespace spx
+
+extern "C" {
+
+int spx_fp64_fma_rate(int blocks, int iters, double* sink, double* flops, void* stream) {
+    SPX_REQUIRE(blocks >= 1 && iters >= 1 && sink && flops, "bad arguments");
+    k_fp64_fma_rate<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(iters, sink);
+    *flops = 2.0 * 8.0 * 256.0 * (double)blocks * (double)iters;
+    return check_launch("k_fp64_fma_rate");
+}
+
 int spx_device_info(int* sm_count, int* is_sm100) {
     int dev = 0;
     SPX_CUDA(cudaGetDevice(&dev));

@@ -64,6 +64,11 @@ int spx_tune_set(const char* knob, int value);
 int spx_tune_get(const char* knob, int* value);
 /* Number of SMs of the current device, and whether it is an sm_100 part (1) or not (0). */
 int spx_device_info(int* sm_count, int* is_sm100);
+/* FP64 FMA throughput probe (no reference counterpart): `blocks` x 256 threads each run eight
+ * independent FP64 FMA chains of `iters` steps; *flops (host) = the launch's floating-point
+ * operations (2 per FMA), so that a caller timing the launch gets the device's FP64 rate, the
+ * denominator of an FP64-bound kernel's roofline. sink: blocks x 256 doubles. */
+int spx_fp64_fma_rate(int blocks, int iters, double* sink, double* flops, void* stream);
 
 /* ------------------------------------------------------------------------------------------------
  * Segmentation: Otsu threshold, binarisation, 8/4-connected components with stats.
@@ -290,6 +295,13 @@ int spx_render_model(const double* params, const int* boxes, int n, int height, 
  * one 16x16 tile leaves that tile unrendered): reset = 1 clears it, reset = 0 copies it to the host
  * int *flag_out and synchronises the stream. */
 int spx_render_overflow(void* workspace, int n, int height, int width, int* flag_out, int reset, void* stream);
+/* Centre re-refinement on deblended cells (detect_centers(background="model"), subpx/centers.py:
+ * 224-268): labels (n*hm x wm int32) marks, in cell j's window of the cleaned stack (rows j*hm ..
+ * j*hm + hm - 1), the pixels of the cell's mask above 0.2 x its peak (fitted amplitude, else the
+ * largest cleaned value) with j + 1; rows_out (n x 5) = [0, j*hm, wm, hm, j + 1], so that
+ * spx_refine_centers on the stack as an (n*hm x wm) double image with pad 0 refines every cell. */
+int spx_support_labels(const double* cleaned, const int* voronoi, const int* boxes, const double* params, int n,
+                       int hm, int wm, int width, int* labels, int* rows_out, void* stream);
 /* Cleaned cells of `which` (n_out indices; all cells when null) as an (n_out, hm, wm) stack. */
 int spx_clean_cells(const void* img, int dtype, double sign, int height, int width, const int* voronoi,
                     const int* boxes, const double* params, int radius_cap, const spx_bgmap* background,

@@ -300,3 +300,34 @@ def dedupe_pairwise(points: np.ndarray, eps: float = 1.5) -> np.ndarray:
     np.add.at(sums, inv, pts)
     np.add.at(counts, inv, 1)
     return sums / counts[:, None]
+
+
+def detect_centers_model(image, *, refine_method="logquad", invert=False, pad=3, deblend_iterations=30, **kw):
+    """detect_centers(background="model") without bands (subpx/centers.py:178-297): the centres of
+    `detect_centers`, then per centre a square cell of 2 ceil(0.6 pitch) + 1 (pitch from auto_tile;
+    16 when undefined) cut by the Voronoi partition, a deblend (background map and every other
+    hole's Gaussian removed), and the refiner again on each cleaned cell with support = the cell's
+    mask where the cleaned value exceeds 0.2 x its peak (the fitted amplitude, else the cell's
+    maximum). Returns (finite centres, deblend state, non-finite count)."""
+    from . import deblend as odb
+    from . import voronoi as ov
+
+    g = np.asarray(image)
+    seeds = detect_centers(g, refine_method=refine_method, invert=invert, pad=pad, **kw)
+    signal = g.astype(np.float64) * (-1.0 if invert else 1.0)
+    pitch = odb.auto_tile(seeds, signal.shape)[1]
+    half = int(np.ceil(0.6 * pitch)) if np.isfinite(pitch) else 16
+    rows = np.array([[x - half, y - half, 2 * half + 1, 2 * half + 1, x, y] for x, y in seeds],
+                    dtype=np.float64).reshape(-1, 6)
+    labels = ov.voronoi_labels(seeds, signal.shape)
+    origins, sizes = ov.cell_boxes(rows, signal.shape, pad)
+    masks = ov.cell_masks(labels, origins, sizes)
+    state = odb.deblend(signal, seeds, masks, origins, iterations=deblend_iterations)
+    cleaned = state.cleaned
+    p0 = state.params[:, 0]
+    peak = np.where(np.isfinite(p0) & (p0 > 0), p0, np.where(masks, cleaned, -np.inf).reshape(len(seeds), -1).max(axis=1))
+    support = masks & (cleaned > 0.2 * peak[:, None, None])
+    local = np.array([refine(c, m, refine_method) for c, m in zip(cleaned, support)], dtype=np.float64).reshape(-1, 2)
+    centres = local + origins
+    finite = np.isfinite(centres).all(axis=1)
+    return centres[finite], state, int((~finite).sum())

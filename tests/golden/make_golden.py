@@ -279,8 +279,28 @@ def make_results(out: Path, ref):
         save_cd_results(res, out / ("results_compact" if compact else "results_full"), compact=compact)
 
 
+def make_centers_model(out: Path, ref):
+    """detect_centers(background="model") of the reference's CPU path: centres re-refined on
+    deblended cells, for the refiners that support it."""
+    from subpx import detect_centers
+
+    from imageprocessor_new_b200 import synthetic as S
+
+    page = np.ascontiguousarray(S.page_square(4).image[:256, :320])
+    lat, _ = S.gaussian_lattice(2.2, shape=(96, 160), seed=8)
+    lat = np.clip(np.rint(lat), 0, 255).astype(np.uint8)
+    arrays = {"page_img": page, "lattice_img": lat}
+    for name, img, kw in (("page", page, dict(threshold="otsu", area_max=400)),
+                          ("lattice", lat, dict(threshold="otsu", area_max=400))):
+        for refine in ("weighted", "logquad", "none"):
+            res = detect_centers(img, backend="cpu", refine=refine, background="model", **kw)
+            arrays[f"{name}_{refine}"] = res.centers_xy
+            arrays[f"{name}_{refine}_used"] = np.array(res.meta["deblend_iterations_used"])
+    np.savez_compressed(out / "centers_model.npz", **arrays)
+
+
 MAKERS = {"thresholds": make_thresholds, "ccl": make_ccl, "centers": make_centers, "voronoi": make_voronoi,
-          "tiled": make_tiled, "cd": make_cd, "results": make_results}
+          "tiled": make_tiled, "cd": make_cd, "results": make_results, "centers_model": make_centers_model}
 
 
 def main():

@@ -112,3 +112,20 @@ def test_tiled_with_morphology_matches_untiled_rules():
     d = np.sqrt(((whole[:, None, :] - tiled[None, :, :]) ** 2).sum(-1)).min(axis=1)
     assert len(tiled) == len(whole)
     assert np.median(d) == 0.0
+
+
+@pytest.mark.parametrize("name", ["page", "lattice"])
+@pytest.mark.parametrize("refine", ["weighted", "logquad", "none"])
+def test_model_background_refinement_matches_reference(name, refine):
+    """detect_centers(background="model") on the GPU against the reference's CPU path (golden): the
+    same centres to 1e-6 px (deblended cells in FP64, sums in another order) and deblend iterations."""
+    from imageprocessor_new_b200 import detect_centers
+
+    z = np.load(GOLDEN / "centers_model.npz")
+    res = detect_centers(z[f"{name}_img"], backend="gpu", threshold="otsu", area_max=400, refine=refine,
+                         background="model")
+    want = z[f"{name}_{refine}"]
+    assert res.centers_xy.shape == want.shape
+    np.testing.assert_allclose(res.centers_xy, want, rtol=0, atol=1e-6)
+    assert res.meta["deblend_iterations_used"] == int(z[f"{name}_{refine}_used"])
+    assert res.meta["background"] == "model"

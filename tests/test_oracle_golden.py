@@ -134,3 +134,15 @@ def test_pairwise_dedupe_equals_kdtree_dedupe(n):
     a, b = oc.dedupe(pts, 1.5), oc.dedupe_pairwise(pts, 1.5)
     assert a.shape == b.shape
     np.testing.assert_allclose(key(a), key(b), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("name", ["page", "lattice"])
+def test_model_background_centres_match_reference(name):
+    """detect_centers(background="model"): centres re-refined on deblended cells (reference CPU path,
+    tests/golden/centers_model.npz)."""
+    z = _load("centers_model")
+    for refine in ("weighted", "logquad", "none"):
+        got, state, _ = oc.detect_centers_model(z[f"{name}_img"], refine_method=refine, threshold="otsu",
+                                                area_max=400)
+        np.testing.assert_allclose(got, z[f"{name}_{refine}"], rtol=0, atol=1e-9)
+        assert state.iterations == int(z[f"{name}_{refine}_used"])
