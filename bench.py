@@ -58,12 +58,21 @@ METHODS = ("gaussian", "gradient", "halfmax")
 REFINERS = ("weighted", "logquad", "edge_gradmoment")
 CD_KW = dict(area_max=400, summary_only=True)
 CENTER_KW = dict(threshold="otsu", area_max=400)
-# DRAM bytes (read + write) per cell of one k_fit_iteration launch and the FP64 pipe's busy
-# fraction, both constants read from one ncu capture of a launch on the 4096x4096 page (29,241
-# cells, 190.4 MB of DRAM traffic), not measured in this run; traffic scales with the cells
-# processed.
-FIT_TRAFFIC_PER_CELL = 6512.0
-FIT_FP64_PIPE_ACTIVE = 0.507
+# Algorithmic FP64 operations of one k_fit_iteration launch (adds and multiplies, an FMA counted
+# as two, exp and rsqrt as one each), counted from the cells' own work in the timed launches:
+#   per staged pixel, cleaning (own Gaussian, background, model): FIT_FLOP_CLEAN
+#   per staged pixel and LM pass (one pass at the start, one per iteration): model, residual, cost,
+#     the six Jacobian entries, 21 J^T J and 6 J^T r accumulations: FIT_FLOP_PASS
+#   per LM iteration, the damped 6x6 Cholesky solve, trial step and acceptance: FIT_FLOP_SOLVE
+FIT_FLOP_CLEAN = 16.0
+FIT_FLOP_PASS = 83.0
+FIT_FLOP_SOLVE = 185.0
+# DRAM bytes (read + write) per cell of one k_fit_iteration launch and the FP64 instructions it
+# issues per cell (dadd + dmul + 2 dfma, exp expanded), constants from one ncu capture of a launch
+# on the 4096x4096 page (29,241 cells: 190.3 MB of DRAM traffic, 15.42 GFLOP issued in 1.094 ms),
+# not measured in this run; both scale with the cells processed.
+FIT_TRAFFIC_PER_CELL = 6508.0
+FIT_ISSUED_FLOP_PER_CELL = 5.274e5
 
 
 def _dist():
@@ -128,6 +137,14 @@ class ClockSampler:
     def summary(self):
         t0, t1 = self.window
         inside = [p for t, p in self.samples if (t0 is None or t >= t0) and (t1 is None or t <= t1)]
+        where = "inside the timed region"
+        if not inside and t0 is not None:
+            # A timed region shorter than the 200 ms sampling period: the samples just before and
+            # just after it (the GPU was busy with the warm-up and the end-to-end steps then).
+            before = [(t, p) for t, p in self.samples if t < t0]
+            after = [(t, p) for t, p in self.samples if t1 is not None and t > t1]
+            inside = [q[-1][1] for q in (before, after[:1]) if q]
+            where = "adjacent to a timed region shorter than the sampling period"
         if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(s[1]) for s in inside if s[1].replace(".", "").isdigit()]
@@ -135,7 +152,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for s in inside for k in range(4) if s[5 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(inside)}
+                "reasons": reasons, "samples": len(inside), "sampled": where}
 
 
 def make_page(rank: int, size: int = 8192):
@@ -162,6 +179,7 @@ def gpu_arm(args):
     # launch each) on the launching stream, inside the timed region.
     fit_times = []
     fit_cells = []
+    fit_work = []  # (iterations, staged pixels) per cell of every timed launch, device tensors
     orig_iteration = deblend.Deblender.iteration
 
     def timed_iteration(self, params_d, model, bg):
@@ -171,6 +189,7 @@ def gpu_arm(args):
         e.record()
         fit_times.append((s, e))
         fit_cells.append(self.n)
+        fit_work.append((out[3], self.cells.counts))
         return out
 
     deblend.Deblender.iteration = timed_iteration
@@ -192,6 +211,7 @@ def gpu_arm(args):
     def run(image, k):
         fit_times.clear()
         fit_cells.clear()
+        fit_work.clear()
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -240,6 +260,7 @@ def gpu_arm(args):
             fit_ms = [a.elapsed_time(b) for a, b in fit_times]
             fit_avg_ms = float(np.mean(fit_ms)) if fit_ms else float("nan")
             fit_n = float(np.mean(fit_cells)) if fit_cells else 0.0
+            fit_flop = _fit_flops(fit_work)
             # End to end: host page, copies inside the region.
             warm(page, max(2, args.warmup))
             ms_e2e, cells_e2e, _ = run(page, args.steps)
@@ -255,12 +276,16 @@ def gpu_arm(args):
     e2e = world * (cells_e2e / args.steps) / (ms_e2e / 1e3 / args.steps)
     peaks, which = _peaks()
     d2h = _d2h_bytes(int(per_step_cells))
-    # Roofline of the dominant kernel (the LM deblending iteration, FP64, compute-bound): its
-    # algorithmic HBM bytes per launch are the cells' pixels read (image 2 B + labels 4 B + model 8 B
-    # + background rows 8 B) plus 6 params in / 6 out + status; its FP64 rate is reported beside.
+    # Roofline of the dominant kernel, the LM deblending iteration: FP64-bound (neither a tensor-core
+    # contraction nor HBM-bound), so its roofline is the FP64 rate measured here on this GPU, and the
+    # achieved rate is the launches' algorithmic FP64 operations over their CUDA-event time. Its
+    # HBM view beside it: algorithmic bytes = the cells' pixels read (image 2 B + labels 4 B + model
+    # 8 B + background rows 8 B) plus 6 params in / 6 out + status.
+    fp64_peak = fp64_peak_tflops()
+    fit_tflops = fit_flop / (sum(fit_ms) / 1e3) / 1e12 if fit_ms else None
     px_per_cell = 24 * 24
     bytes_per_cell = px_per_cell * (2 + 4 + 8 + 8) + 13 * 8
-    achieved = fit_n * bytes_per_cell / (fit_avg_ms / 1e3) / 1e9 if fit_ms else None
+    achieved_gbs = fit_n * bytes_per_cell / (fit_avg_ms / 1e3) / 1e9 if fit_ms else None
     mpix = world * args.page * args.page / 1e6 / (ms / 1e3 / args.steps)
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -274,16 +299,25 @@ def gpu_arm(args):
                    "warm_start": "plain LM (no network)"},
         "e2e": {"value": round(e2e, 1), "unit": UNIT, "h2d_bytes_per_step": int(page.nbytes) * (len(REFINERS) + 1),
                 "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": "k_fit_iteration", "achieved": None if achieved is None else round(achieved, 1),
-                     "peak": peaks.get("hbm_gbs"), "peak_source": which, "unit": "GB/s",
-                     "frac": None if achieved is None else round(achieved / peaks["hbm_gbs"], 4),
+        "roofline": {"bound": "fp64", "kernel": "k_fit_iteration<double>", "unit": "TFLOP/s",
+                     "achieved": None if fit_tflops is None else round(fit_tflops, 3),
+                     "peak": round(fp64_peak, 3),
+                     "peak_source": "measured in this run (spx_fp64_fma_rate: independent DFMA chains on "
+                                    "every SM, CUDA events)",
+                     "frac": None if fit_tflops is None else round(fit_tflops / fp64_peak, 4),
+                     "flop_per_launch": round(fit_flop / max(len(fit_ms), 1)),
+                     "flop_source": "algorithmic, from the timed launches' per-cell LM iterations and staged "
+                                    "pixels (exp and rsqrt one operation each)",
+                     "issued_frac": None if not fit_ms else
+                     round(FIT_ISSUED_FLOP_PER_CELL * fit_n / (fit_avg_ms / 1e3) / 1e12 / fp64_peak, 4),
+                     "issued_source": "FP64 instructions issued per cell (exp expanded) from one ncu capture "
+                                      "(4096x4096 page), scaled by cells",
                      "traffic": round(FIT_TRAFFIC_PER_CELL * fit_n / 1e9, 4), "traffic_unit": "GB per launch",
                      "traffic_source": "constant per cell from one ncu capture (4096x4096 page), scaled by cells",
                      "launch_ms": round(fit_avg_ms, 4), "cells_per_launch": fit_n,
-                     # The kernel's arithmetic is FP64 (not a contraction, not HBM-bound): the FP64
-                     # pipe's busy fraction from one ncu capture of the same kernel (a constant).
-                     "fp64_pipe_active": FIT_FP64_PIPE_ACTIVE,
-                     "fp64_source": "constant from one ncu capture of k_fit_iteration (4096x4096 page)"},
+                     "hbm": {"achieved": None if achieved_gbs is None else round(achieved_gbs, 1),
+                             "peak": peaks.get("hbm_gbs"), "peak_source": which, "unit": "GB/s",
+                             "frac": None if achieved_gbs is None else round(achieved_gbs / peaks["hbm_gbs"], 4)}},
         "mpix_per_s": round(mpix, 1),
         "gpu_launches": int(launches),
         "clocks": clock_summary,
@@ -322,6 +356,18 @@ def _accuracy(warm, plain) -> dict:
                if both.any() else 0.0)
         out[name] = {"centre_max_px": dc, "cd_max_px": dcd, "same_validity": float((a.valid == b.valid).mean())}
     return out
+
+
+def _fit_flops(work) -> float:
+    """Algorithmic FP64 operations of the timed k_fit_iteration launches (FIT_FLOP_* per staged
+    pixel, per pixel and LM pass, and per iteration), from each launch's per-cell iteration counts
+    and staged pixel counts (device tensors, read after the timed region)."""
+    total = 0.0
+    for iters, pixels in work:
+        it = iters.double()
+        px = pixels.double()
+        total += float((px * (FIT_FLOP_CLEAN + FIT_FLOP_PASS * (it + 1.0))).sum() + FIT_FLOP_SOLVE * it.sum())
+    return total
 
 
 def fp64_peak_tflops(repeats: int = 5) -> float:

@@ -28,8 +28,8 @@ from . import _lib
 KNOBS = {
     "fit_warps": (2, 4, 8),
     "fit_blocks_per_sm": (4, 8, 16),
-    "render_tile": (16, 32),
-    "radial_rays": (0, 1),
+    "render_tile": (16, 32, 64),
+    "radial_rays": (0, 1, 2),
 }
 
 

@@ -12,6 +12,8 @@
 // scipy.ndimage.map_coordinates(order=3, mode="nearest") does, and scipy's cubic weights.
 
 #include <algorithm>
+#include <type_traits>
+
 #include "common.cuh"
 #include "lm.cuh"
 
@@ -621,17 +623,21 @@ struct SplineWindowF {
         w[0] = s * s * s * k;
         w[3] = 1.0f - w[0] - w[1] - w[2];
     }
-    // (iy, ix): the sample's cell in padded coordinates, at least 1 and at most hp - 3 / wp - 3 for a
-    // sample inside the cell box (the padding is wider than the 4 x 4 window), so no clamping.
-    __device__ __forceinline__ float at(const float* coef, int wp, int iy, int ix, float ty, float tx) {
+    // (iy, ix): the sample's cell in box coordinates (0 <= iy < hm, 0 <= ix < wm); the window is the
+    // four float4 rows quad[(iy + a) * wm + ix], a = 0..3 (radial_quad_offset).
+    __device__ __forceinline__ float at(const float4* quad, int wm, int iy, int ix, float ty, float tx) {
         if (iy != fy || ix != fx) {
             fy = iy;
             fx = ix;
-            const float* q = coef + (iy - 1) * wp + (ix - 1);
+            const float4* q = quad + iy * wm + ix;
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) c[a * 4 + b] = q[a * wp + b];
+            for (int a = 0; a < 4; ++a) {
+                const float4 t = q[a * wm];
+                c[a * 4 + 0] = t.x;
+                c[a * 4 + 1] = t.y;
+                c[a * 4 + 2] = t.z;
+                c[a * 4 + 3] = t.w;
+            }
         }
         float wy[4], wx[4];
         weights(ty, wy);
@@ -648,19 +654,22 @@ struct SplineWindowF {
     }
 };
 
-// One FP32 spline sample from the 4 x 4 window at (iy - 1, ix - 1) of the FP32 coefficient copy:
-// the arithmetic of SplineWindowF::at without the cached window.
-__device__ __forceinline__ float spline_sample_f(const float* coef, int wp, int iy, int ix, float ty, float tx) {
+// One FP32 spline sample from the window rows of box cell (iy, ix): the arithmetic of
+// SplineWindowF::at without the cached window.
+__device__ __forceinline__ float spline_sample_f(const float4* quad, int wm, int iy, int ix, float ty, float tx) {
     float wy[4], wx[4];
     SplineWindowF::weights(ty, wy);
     SplineWindowF::weights(tx, wx);
-    const float* q = coef + (iy - 1) * wp + (ix - 1);
+    const float4* q = quad + iy * wm + ix;
     float out = 0.0f;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
+        const float4 t = q[a * wm];
         float row = 0.0f;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) row = fmaf(q[a * wp + b], wx[b], row);
+        row = fmaf(t.x, wx[0], row);
+        row = fmaf(t.y, wx[1], row);
+        row = fmaf(t.z, wx[2], row);
+        row = fmaf(t.w, wx[3], row);
         out = fmaf(row, wy[a], out);
     }
     return out;
@@ -685,20 +694,29 @@ __device__ __forceinline__ int floor_nonneg(double y, double* fl) {
 constexpr int kRadialThreads = 128;
 constexpr int kTrigMax = 256;  // ray angles with a cos / sin table in shared memory (4 KB)
 
-// Doubles of shared (or scratch) memory one radial CTA needs: spline coefficients in FP64 and in
-// FP32, a reduction area, then the cell mask and the eroded mask as bytes.
+// Shared (or scratch) memory of one radial CTA, in doubles: the FP64 spline coefficient plane, the
+// FP32 sampling windows, a reduction area, then the cell mask and the eroded mask as bytes.
 // Row pitch (in doubles) of the FP64 coefficient plane: the padded width made odd, so that the
 // threads of the row pass of the spline prefilter (one row each, stepping along their rows) fall in
 // different shared-memory banks.
 __host__ __device__ inline int radial_pitch(int wm) { return (wm + 2 * kPad) | 1; }
 
+// The FP32 sampling windows start after the FP64 plane, 16-byte aligned. A ray sample in box cell
+// (iy, ix) (0 <= iy < hm, 0 <= ix < wm) reads the 4 x 4 coefficients of padded rows iy + kPad - 1 ..
+// iy + kPad + 2 and columns ix + kPad - 1 .. ix + kPad + 2; quad[r * wm + ix] holds the four of padded
+// row r + kPad - 1 as one float4, for r = 0 .. hm + 2, so a window is four 16-byte loads.
+__host__ __device__ inline long long radial_quad_offset(int hm, int wm) {
+    return ((long long)(hm + 2 * kPad) * radial_pitch(wm) + 1) & ~1LL;
+}
+__host__ __device__ inline long long radial_quad_doubles(int hm, int wm) { return 2LL * (hm + 3) * wm; }
+
 // The masks are three byte planes (cell, eroded cell, and per pixel square whether its four corners
 // are all in the eroded cell). With smoothing, three more hm x wm doubles follow (the two axis-0
-// passes and the smoothed signal).
+// passes and the smoothed signal). The total is even, so every CTA's scratch stays 16-byte aligned.
 __host__ __device__ inline long long radial_cta_doubles(int hm, int wm, bool smooth = false) {
-    const long long np = (long long)(hm + 2 * kPad) * radial_pitch(wm);
-    const long long nf = (long long)(hm + 2 * kPad) * (wm + 2 * kPad);
-    return np + (nf + 1) / 2 + 32 + (3LL * hm * wm + 7) / 8 + (smooth ? 3LL * hm * wm : 0);
+    const long long t = radial_quad_offset(hm, wm) + radial_quad_doubles(hm, wm) + 32 + (3LL * hm * wm + 7) / 8 +
+                        (smooth ? 3LL * hm * wm : 0);
+    return (t + 1) & ~1LL;
 }
 
 // One output of scipy's correlate1d with a symmetric kernel (weights w[0..2r], centre w[r]) and
@@ -813,11 +831,15 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
 // with the halfmax crossing and the gradient maximum found by ballots and shuffles; the results are
 // bit for bit those of the one-ray-per-thread loop (same sample arithmetic, same first-crossing and
 // first-maximum rules).
-template <bool kSmooth, bool kWarpRays>
+// kRays: 0 one ray per thread with the 4 x 4 window cached in registers (reloaded when a ray enters
+// another pixel), 1 one ray per warp (kWarpRays), 2 one ray per thread reading the window's four
+// float4 rows at every sample (no per-lane reload branch) and the precomputed corner plane.
+template <bool kSmooth, int kRays>
 __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
     int n_angles, double radial_step, int n_radii, const double* smooth_w, int smooth_r, double* coef_scratch,
     MethodOut half_out, MethodOut grad_out) {
+    constexpr bool kWarpRays = kRays == 1;
     extern __shared__ double sm[];
     __shared__ double trig_tab[2 * kTrigMax];  // cos, sin of the ray angles (n_angles <= kTrigMax)
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -830,8 +852,8 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
             trig_tab[2 * a + 1] = sin(ang);
         }
     double* coef = coef_scratch ? coef_scratch + (long long)blockIdx.x * radial_cta_doubles(hm, wm, kSmooth) : sm;
-    float* coef_f = reinterpret_cast<float*>(coef + (long long)hp * dp);  // FP32 copy, row pitch wp
-    double* red = coef + (long long)hp * dp + ((long long)hp * wp + 1) / 2;  // 32 doubles: 8 slots of 4
+    float4* quad = reinterpret_cast<float4*>(coef + radial_quad_offset(hm, wm));  // FP32 window rows
+    double* red = coef + radial_quad_offset(hm, wm) + radial_quad_doubles(hm, wm);  // 32 doubles: 8 slots of 4
     uint8_t* mask = reinterpret_cast<uint8_t*>(red + 32);
     uint8_t* emask = mask + area_px;
     uint8_t* full = emask + area_px;  // square [iy, iy+1] x [ix, ix+1] inside the eroded cell
@@ -918,7 +940,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                        mask[k - 1] && mask[k + 1];
         }
         __syncthreads();
-        if constexpr (kWarpRays)
+        if constexpr (kRays != 0)
             for (int k = tid; k < area_px; k += kRadialThreads) {
                 const int yy = k / wm, xx = k % wm;
                 full[k] = yy + 1 < hm && xx + 1 < wm && emask[k] && emask[k + 1] && emask[k + wm] && emask[k + wm + 1];
@@ -928,7 +950,10 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         for (int row = tid; row < hp; row += kRadialThreads) spline_line(coef + (long long)row * dp, wp, 1);
         __syncthreads();
         const double peak = cubic_at(coef, hp, wp, dp, cy + kPad, cx + kPad);
-        for (int k = tid; k < hp * wp; k += kRadialThreads) coef_f[k] = (float)coef[(k / wp) * dp + k % wp];
+        for (int k = tid; k < (hm + 3) * wm; k += kRadialThreads) {
+            const double* q = coef + (k / wm + kPad - 1) * dp + (k % wm + kPad - 1);
+            quad[k] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+        }
         __syncthreads();
         const double half = peak / 2.0;
         const double inv2s = 1.0 / (2.0 * radial_step);
@@ -961,7 +986,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                                 valid = full[iy * wm + ix] || inside_bytes(emask, hm, wm, y, x);
                                 if (valid)
                                     p = k == 0 ? (float)peak
-                                               : spline_sample_f(coef_f, wp, iy + kPad, ix + kPad, (float)(y - fyd),
+                                               : spline_sample_f(quad, wm, iy, ix, (float)(y - fyd),
                                                                  (float)(x - fxd));
                             }
                         }
@@ -1057,16 +1082,21 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                     if (!(y >= 0.0 && y <= ymax && x >= 0.0 && x <= xmax)) { first_invalid = k; break; }
                     double fyd, fxd;
                     const int iy = floor_nonneg(y, &fyd), ix = floor_nonneg(x, &fxd);
-                    if (iy != mfy || ix != mfx) {
-                        mfy = iy;
-                        mfx = ix;
-                        const uint8_t* q = emask + iy * wm + ix;
-                        mfull = iy + 1 < hm && ix + 1 < wm && q[0] && q[1] && q[wm] && q[wm + 1];
+                    float p;
+                    if constexpr (kRays == 2) {
+                        if (!(full[iy * wm + ix] || inside_bytes(emask, hm, wm, y, x))) { first_invalid = k; break; }
+                        p = k == 0 ? (float)peak
+                                   : spline_sample_f(quad, wm, iy, ix, (float)(y - fyd), (float)(x - fxd));
+                    } else {
+                        if (iy != mfy || ix != mfx) {
+                            mfy = iy;
+                            mfx = ix;
+                            const uint8_t* q = emask + iy * wm + ix;
+                            mfull = iy + 1 < hm && ix + 1 < wm && q[0] && q[1] && q[wm] && q[wm + 1];
+                        }
+                        if (!(mfull || inside_bytes(emask, hm, wm, y, x))) { first_invalid = k; break; }
+                        p = k == 0 ? (float)peak : win.at(quad, wm, iy, ix, (float)(y - fyd), (float)(x - fxd));
                     }
-                    if (!(mfull || inside_bytes(emask, hm, wm, y, x))) { first_invalid = k; break; }
-                    const float p = k == 0 ? (float)peak
-                                           : win.at(coef_f, wp, iy + kPad, ix + kPad, (float)(y - fyd),
-                                                    (float)(x - fxd));
                     if (k >= 1 && !crossed && h1 >= halff && p < halff) {
                         edge_h = (double)(k - 1) * radial_step +
                                  (((double)h1 - half) / ((double)h1 - (double)p)) * radial_step;
@@ -1281,7 +1311,7 @@ size_t spx_radial_workspace_bytes(int hm, int wm, int smooth) {
 
 }  // extern "C"
 
-template <bool kSmooth, bool kWarpRays>
+template <bool kSmooth, int kRays>
 static int launch_radial(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
                          int wm, int width, int n_angles, double radial_step, int n_radii, const double* smooth_w,
                          int smooth_r, const spx_method_out* halfmax, const spx_method_out* gradient, void* workspace,
@@ -1291,17 +1321,18 @@ static int launch_radial(const double* cleaned, const int* voronoi, const int* b
     int blocks;
     if (smem) {
         if (smem + 2 * kTrigMax * sizeof(double) > 48 * 1024)  // with the static cos / sin table
-            SPX_CUDA(cudaFuncSetAttribute(k_radial_cd<kSmooth, kWarpRays>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            SPX_CUDA(cudaFuncSetAttribute(k_radial_cd<kSmooth, kRays>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
         int per_sm = 0;
-        SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd<kSmooth, kWarpRays>, kRadialThreads,
+        SPX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_radial_cd<kSmooth, kRays>, kRadialThreads,
                                                                smem));
         blocks = (int)std::min<long long>(n, 148LL * std::max(per_sm, 1));
     } else {
+        SPX_REQUIRE((reinterpret_cast<uintptr_t>(workspace) & 15) == 0, "workspace must be 16-byte aligned");
         scratch = static_cast<double*>(workspace);
         blocks = std::min(n, kRadialScratchCtas);
     }
-    k_radial_cd<kSmooth, kWarpRays><<<blocks, kRadialThreads, smem, s>>>(
+    k_radial_cd<kSmooth, kRays><<<blocks, kRadialThreads, smem, s>>>(
         cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm, wm, width, n_angles, radial_step, n_radii,
         smooth_w, smooth_r, scratch, method_out(halfmax), method_out(gradient));
     return check_launch("k_radial_cd");
@@ -1325,18 +1356,19 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
     // radii = np.arange(0, hypot(hm, wm) + step, step)
     const double stop = hypot((double)hm, (double)wm) + radial_step;
     const int n_radii = (int)ceil(stop / radial_step);
-    const bool warp_rays = tuning().radial_rays == 1;
-    if (smooth)
-        return warp_rays ? launch_radial<true, true>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
-                                                     radial_step, n_radii, smooth_weights, smooth_radius, halfmax,
-                                                     gradient, workspace, s)
-                         : launch_radial<true, false>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
-                                                      radial_step, n_radii, smooth_weights, smooth_radius, halfmax,
-                                                      gradient, workspace, s);
-    return warp_rays ? launch_radial<false, true>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
-                                                  radial_step, n_radii, nullptr, 0, halfmax, gradient, workspace, s)
-                     : launch_radial<false, false>(cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles,
-                                                   radial_step, n_radii, nullptr, 0, halfmax, gradient, workspace, s);
+    const int rays = tuning().radial_rays;
+    auto go = [&](auto smooth_c, auto rays_c) {
+        return launch_radial<decltype(smooth_c)::value, decltype(rays_c)::value>(
+            cleaned, voronoi, boxes, which, n, hm, wm, width, n_angles, radial_step, n_radii,
+            smooth ? smooth_weights : nullptr, smooth ? smooth_radius : 0, halfmax, gradient, workspace, s);
+    };
+    using T = std::true_type;
+    using F = std::false_type;
+    using R0 = std::integral_constant<int, 0>;
+    using R1 = std::integral_constant<int, 1>;
+    using R2 = std::integral_constant<int, 2>;
+    if (smooth) return rays == 1 ? go(T{}, R1{}) : rays == 2 ? go(T{}, R2{}) : go(T{}, R0{});
+    return rays == 1 ? go(F{}, R1{}) : rays == 2 ? go(F{}, R2{}) : go(F{}, R0{});
 }
 
 }  // extern "C"

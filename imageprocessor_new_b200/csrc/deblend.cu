@@ -554,7 +554,8 @@ __global__ void k_render_prep(const double* params, const int4* boxes, int n, in
 }
 
 // Render tiles: Tile x Tile pixels per 256-thread block (16: one pixel per thread, 32: four rows
-// per thread), chosen by tuning().render_tile.
+// per thread, 64: sixteen rows per thread, fewer tiles to gather candidates for), chosen by
+// tuning().render_tile.
 constexpr int kRenderCap = 2048;
 
 // model(y, x) = sum over cells (increasing index) whose truncated square covers the pixel, each
@@ -769,19 +770,35 @@ struct TileSel {
     int mode;                 // SPX_TILE_FREE: model < thr_model & dist >= thr_dist; SPX_TILE_USABLE; SPX_TILE_ALL
     double thr_model;
     unsigned long long d2_min;  // sqrt((double)d2) >= thr_dist  <=>  d2 >= d2_min (set by the host)
-    // The pixel's residual and whether the tile's median takes it. Every load is issued whatever
-    // the tests give (the branches are uniform over the launch), so a thread's loads of several
-    // pixels overlap.
-    __device__ __forceinline__ bool select(int y, int x, double* value) const {
-        const long long i = (long long)y * img.W + x;
-        const double m = model ? model[i] : 0.0;
+    // A pixel's loads (pixel of type Px, model, distance, usable flag), none of them conditional on
+    // another's value, so that a thread's loads of several pixels are in flight together.
+    struct Loaded {
+        double raw, m;
+        unsigned int dd;
+        uint8_t use;
+    };
+    template <typename Px>
+    __device__ __forceinline__ Loaded load(long long i) const {
+        Loaded q;
+        q.raw = (double)static_cast<const Px*>(img.data)[i];
+        q.m = model ? model[i] : 0.0;
+        q.dd = mode == SPX_TILE_FREE ? d2[i] : 0u;
+        q.use = (mode != SPX_TILE_ALL && usable) ? usable[i] : (uint8_t)1;
+        return q;
+    }
+    // The pixel's residual and whether the tile's median takes it.
+    __device__ __forceinline__ bool decide(const Loaded& q, double* value) const {
         bool ok = true;
         if (mode != SPX_TILE_ALL) {
-            if (usable) ok = usable[i] != 0;
-            if (mode == SPX_TILE_FREE) ok = ok && m < thr_model && (unsigned long long)d2[i] >= d2_min;
+            ok = q.use != 0;
+            if (mode == SPX_TILE_FREE) ok = ok && q.m < thr_model && (unsigned long long)q.dd >= d2_min;
         }
-        *value = img.at(y, x) - m;
+        *value = (img.sign < 0 ? -q.raw : q.raw) - q.m;
         return ok;
+    }
+    template <typename Px>
+    __device__ __forceinline__ bool select(int y, int x, double* value) const {
+        return decide(load<Px>((long long)y * img.W + x), value);
     }
 };
 
@@ -811,9 +828,10 @@ __device__ __forceinline__ int cta_incl_scan(int v, int* warp_tot) {
     return r;
 }
 
-// One radix pass of a CTA-wide select: hist[2048] holds the counts of the current 11-bit (last: 9-bit)
-// digit among the keys that match the prefix so far; finds the digit holding the kk-th key and
-// the rank inside it. NT threads, each owning 2048 / NT consecutive bins.
+// One radix pass of a CTA-wide select: hist[2048] holds the counts of the current digit (at most 11
+// bits) among the keys that match the prefix so far; finds the digit holding the kk-th key, the
+// rank inside it and the digit's count (s_pick[0..2]). NT threads, each owning 2048 / NT
+// consecutive bins.
 template <int NT>
 __device__ __forceinline__ void cta_pick_digit(const int* hist, int nb, int kk, int* warp_tot, int* s_pick) {
     constexpr int per = 2048 / NT;
@@ -833,6 +851,7 @@ __device__ __forceinline__ void cta_pick_digit(const int* hist, int nb, int kk, 
             if (kk < excl + c[j]) {
                 s_pick[0] = b0 + j;
                 s_pick[1] = kk - excl;
+                s_pick[2] = c[j];
                 break;
             }
             excl += c[j];
@@ -841,47 +860,157 @@ __device__ __forceinline__ void cta_pick_digit(const int* hist, int nb, int kk, 
     __syncthreads();
 }
 
+__device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// The k-th smallest (0-based) of the 64-bit keys that for_keys visits and, when want_next, the
+// (k+1)-th, by a CTA-wide radix select. kmin and kmax are the smallest and largest key: the bits
+// above the highest one where they differ are common to all keys, so the 11-bit digits start
+// below it; the passes stop as soon as the digit holding the k-th key holds no other key, and one
+// last pass fetches that key and the smallest key above it. The keys' order statistics are
+// exact, so the result does not depend on how many passes ran.
+// for_keys(fn) calls fn(key) on every key once, spread over the CTA's threads; all NT threads
+// call this function. s_pick: 3 ints, s_keys: 2 keys of shared memory.
+template <int NT, class ForKeys>
+__device__ void cta_select(ForKeys&& for_keys, int k, bool want_next, unsigned long long kmin,
+                           unsigned long long kmax, int* hist, int* warp_tot, int* s_pick,
+                           unsigned long long* s_keys, unsigned long long* key_k, unsigned long long* key_next) {
+    if (kmin == kmax) {
+        *key_k = *key_next = kmin;
+        return;
+    }
+    const int top = 63 - __clzll((long long)(kmin ^ kmax));
+    // Bits top+1..63 are common to every key (the shift of 2 by 63 is 0, so top = 63 leaves none).
+    unsigned long long pmask = ~((2ull << top) - 1ull);
+    unsigned long long prefix = kmin & pmask;
+    int shift = top + 1, kk = k, cnt = 0;
+    while (shift > 0) {
+        const int bits = shift < 11 ? shift : 11, nb = 1 << bits;
+        shift -= bits;
+        for (int i = threadIdx.x; i < nb; i += NT) hist[i] = 0;
+        __syncthreads();
+        for_keys([&](unsigned long long key) {
+            if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
+        });
+        __syncthreads();
+        cta_pick_digit<NT>(hist, nb, kk, warp_tot, s_pick);
+        prefix |= (unsigned long long)s_pick[0] << shift;
+        pmask |= (unsigned long long)(nb - 1) << shift;
+        kk = s_pick[1];
+        cnt = s_pick[2];
+        __syncthreads();
+        if (cnt == 1) break;
+    }
+    // Fully resolved (shift 0): every key with the prefix equals it, and the (k+1)-th is the same
+    // key when the digit holds it too. Otherwise the k-th is the digit's only key.
+    const bool resolved = shift == 0;
+    if (resolved && (!want_next || kk + 1 < cnt)) {
+        *key_k = *key_next = prefix;
+        return;
+    }
+    if (threadIdx.x == 0) {
+        s_keys[0] = prefix;
+        s_keys[1] = ~0ull;
+    }
+    __syncthreads();
+    unsigned long long mn = ~0ull;
+    for_keys([&](unsigned long long key) {
+        const unsigned long long m = key & pmask;
+        if (m == prefix) {
+            if (!resolved) s_keys[0] = key;
+        } else if (m > prefix && key < mn) {
+            mn = key;
+        }
+    });
+    mn = warp_min_u64(mn);
+    if ((threadIdx.x & 31) == 0 && mn != ~0ull) atomicMin(&s_keys[1], mn);
+    __syncthreads();
+    *key_k = s_keys[0];
+    *key_next = want_next ? s_keys[1] : s_keys[0];
+    __syncthreads();
+}
+
 // Median (mean of the two middle values, NaN when empty) and count of the selected residuals of
-// each tile, by an 8-pass radix select on order-preserving 64-bit keys.
-__global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int tile, int nx, int smem_keys,
+// each tile: the selected pixels' order-preserving 64-bit keys are staged in shared memory (each
+// warp reserves its slots with one atomic), with their smallest and largest key, and cta_select
+// finds the middle one(s).
+template <typename Px>
+__global__ void __launch_bounds__(kTileThreads, 2) k_tile_median(TileSel sel, int tile, int nx, int smem_keys,
                                                               double* medians, long long* counts) {
     extern __shared__ unsigned long long keys[];
     __shared__ int hist[2048];
-    __shared__ int warp_tot[32], s_pick[2];
+    __shared__ int warp_tot[32], s_pick[3];
     __shared__ int s_count;
-    __shared__ unsigned long long s_min;
-    __shared__ int s_le;
+    __shared__ unsigned long long s_keys[2], s_kmin, s_kmax;
     const int ty = blockIdx.x / nx, tx = blockIdx.x % nx;
     const int y0 = ty * tile, x0 = tx * tile;
     const int th = min(tile, sel.img.H - y0), tw = min(tile, sel.img.W - x0);
     const long long P = (long long)th * tw;
-    if (threadIdx.x == 0) s_count = 0;
+    const int lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        s_count = 0;
+        s_kmin = ~0ull;
+        s_kmax = 0;
+    }
     __syncthreads();
     // Pass 0: count and (when they fit) stage the keys, kPass0 pixels per thread at a time so
-    // that their loads are in flight together.
+    // that their loads are in flight together. The loop bounds are the same for every thread, so
+    // the warp votes are over full warps.
     constexpr int kPass0 = 8;
+    unsigned long long kmin = ~0ull, kmax = 0;
     for (int k0 = 0; k0 < (int)P; k0 += kPass0 * blockDim.x) {
         double v[kPass0];
         bool take[kPass0];
+        TileSel::Loaded q[kPass0];
 #pragma unroll
         for (int u = 0; u < kPass0; ++u) {
-            const int k = k0 + u * blockDim.x + threadIdx.x;
-            take[u] = false;
-            v[u] = 0.0;
-            if (k < (int)P) {
-                const int yy = k / tw, xx = k - yy * tw;
-                take[u] = sel.select(y0 + yy, x0 + xx, &v[u]);
-            }
+            const int k = min(k0 + u * (int)blockDim.x + (int)threadIdx.x, (int)P - 1);
+            const int yy = k / tw, xx = k - yy * tw;
+            q[u] = sel.load<Px>((long long)(y0 + yy) * sel.img.W + (x0 + xx));
         }
 #pragma unroll
-        for (int u = 0; u < kPass0; ++u)
+        for (int u = 0; u < kPass0; ++u) {
+            take[u] = sel.decide(q[u], &v[u]) && k0 + u * (int)blockDim.x + (int)threadIdx.x < (int)P;
+        }
+#pragma unroll
+        for (int u = 0; u < kPass0; ++u) {
+            const unsigned ballot = __ballot_sync(0xffffffffu, take[u]);
+            if (ballot == 0u) continue;
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&s_count, __popc(ballot));
+            base = __shfl_sync(0xffffffffu, base, 0);
             if (take[u]) {
-                const int slot = atomicAdd(&s_count, 1);
-                if (slot < smem_keys) keys[slot] = order_key(v[u]);
+                const int slot = base + __popc(ballot & ((1u << lane) - 1u));
+                const unsigned long long key = order_key(v[u]);
+                if (slot < smem_keys) keys[slot] = key;
+                kmin = min(kmin, key);
+                kmax = max(kmax, key);
             }
+        }
+    }
+    kmin = warp_min_u64(kmin);
+    kmax = warp_max_u64(kmax);
+    if (lane == 0) {
+        atomicMin(&s_kmin, kmin);
+        atomicMax(&s_kmax, kmax);
     }
     __syncthreads();
     const int c = s_count;
+    if (c == 0) {
+        if (threadIdx.x == 0) {
+            medians[blockIdx.x] = dnan();
+            counts[blockIdx.x] = 0;
+        }
+        return;
+    }
     const bool in_smem = c <= smem_keys;
     auto for_keys = [&](auto&& fn) {
         if (in_smem) {
@@ -890,57 +1019,15 @@ __global__ void __launch_bounds__(kTileThreads) k_tile_median(TileSel sel, int t
             for (int k = threadIdx.x; k < (int)P; k += blockDim.x) {
                 const int yy = k / tw, xx = k - yy * tw;
                 double v;
-                if (sel.select(y0 + yy, x0 + xx, &v)) fn(order_key(v));
+                if (sel.select<Px>(y0 + yy, x0 + xx, &v)) fn(order_key(v));
             }
         }
     };
-    if (c == 0) {
-        if (threadIdx.x == 0) {
-            medians[blockIdx.x] = dnan();
-            counts[blockIdx.x] = 0;
-        }
-        return;
-    }
-    // k-th smallest key (k = (c - 1) / 2): radix select with 11-bit digits (six passes).
-    unsigned long long prefix = 0, mask = 0;
-    int kk = (c - 1) / 2, shift = 64;
-    for (int pass = 0; pass < 6; ++pass) {
-        const int bits = pass < 5 ? 11 : 9, nb = 1 << bits;
-        shift -= bits;
-        for (int i = threadIdx.x; i < nb; i += blockDim.x) hist[i] = 0;
-        __syncthreads();
-        for_keys([&](unsigned long long key) {
-            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
-        });
-        __syncthreads();
-        cta_pick_digit<kTileThreads>(hist, nb, kk, warp_tot, s_pick);
-        prefix |= (unsigned long long)s_pick[0] << shift;
-        mask |= (unsigned long long)(nb - 1) << shift;
-        kk = s_pick[1];
-        __syncthreads();
-    }
-    const unsigned long long k1 = prefix;
-    double v2;
-    if ((c & 1) == 0) {
-        // The next order statistic: k1 again when it repeats, else the smallest key above it.
-        if (threadIdx.x == 0) { s_le = 0; s_min = ~0ull; }
-        __syncthreads();
-        int le = 0;
-        unsigned long long mn = ~0ull;
-        for_keys([&](unsigned long long key) {
-            if (key <= k1) ++le;
-            else if (key < mn) mn = key;
-        });
-        atomicAdd(&s_le, le);
-        atomicMin(&s_min, mn);
-        __syncthreads();
-        v2 = s_le > c / 2 ? key_value(k1) : key_value(s_min);
-    } else {
-        v2 = key_value(k1);
-    }
+    unsigned long long k1, k2;
+    cta_select<kTileThreads>(for_keys, (c - 1) / 2, (c & 1) == 0, s_kmin, s_kmax, hist, warp_tot, s_pick, s_keys,
+                             &k1, &k2);
     if (threadIdx.x == 0) {
-        const double v1 = key_value(k1);
-        medians[blockIdx.x] = __ddiv_rn(__dadd_rn(v1, v2), 2.0);
+        medians[blockIdx.x] = __ddiv_rn(__dadd_rn(key_value(k1), key_value(k2)), 2.0);
         counts[blockIdx.x] = c;
     }
 }
@@ -1018,17 +1105,47 @@ __device__ __forceinline__ bool q_select(const QuantileReq& r, int i, double* v)
 constexpr int kQuantThreads = 1024;
 constexpr int kQuantAhead = 4;
 
-// Order key of the k-th smallest selected value (0-based): a radix select over 64-bit keys with
-// 11-bit digits (six passes over the values), each digit found by a CTA-wide prefix sum.
-__device__ unsigned long long cta_kth_key(const QuantileReq& r, int k, int* hist, int* warp_tot, int* s_pick) {
-    unsigned long long prefix = 0, pmask = 0;
-    int kk = k, shift = 64;
-    for (int pass = 0; pass < 6; ++pass) {
-        const int bits = pass < 5 ? 11 : 9, nb = 1 << bits;
-        shift -= bits;
-        for (int i = threadIdx.x; i < nb; i += kQuantThreads) hist[i] = 0;
-        __syncthreads();
-        // kQuantAhead values per thread loaded before their histogram updates, so the loads overlap.
+// One CTA per request: out[2 * b] = result (NaN when nothing is selected), out[2 * b + 1] = count.
+// A counting pass finds the count, whether a NaN is selected and the smallest and largest key;
+// cta_select then finds the order statistics, kQuantAhead values per thread loaded before their
+// histogram updates so that the loads overlap.
+__global__ void __launch_bounds__(kQuantThreads) k_quantiles(const QuantileReq* reqs, double* out) {
+    __shared__ int hist[2048];
+    __shared__ int warp_tot[32];
+    __shared__ int s_pick[3];
+    __shared__ int s_count, s_nan;
+    __shared__ unsigned long long s_keys[2], s_kmin, s_kmax;
+    const QuantileReq r = reqs[blockIdx.x];
+    if (threadIdx.x == 0) {
+        s_count = s_nan = 0;
+        s_kmin = ~0ull;
+        s_kmax = 0;
+    }
+    __syncthreads();
+    int c = 0, nan = 0;
+    unsigned long long kmin = ~0ull, kmax = 0;
+    for (int i = threadIdx.x; i < r.n; i += kQuantThreads) {
+        double v;
+        if (q_select(r, i, &v)) {
+            ++c;
+            nan += isnan(v);
+            const unsigned long long key = order_key(v);
+            kmin = min(kmin, key);
+            kmax = max(kmax, key);
+        }
+    }
+    kmin = warp_min_u64(kmin);
+    kmax = warp_max_u64(kmax);
+    atomicAdd(&s_count, c);
+    atomicAdd(&s_nan, nan);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&s_kmin, kmin);
+        atomicMax(&s_kmax, kmax);
+    }
+    __syncthreads();
+    const int n = s_count;
+    const bool any_nan = s_nan != 0;
+    auto for_keys = [&](auto&& fn) {
         for (int i0 = threadIdx.x; i0 < r.n; i0 += kQuantAhead * kQuantThreads) {
             double v[kQuantAhead];
             bool ok[kQuantAhead];
@@ -1038,88 +1155,26 @@ __device__ unsigned long long cta_kth_key(const QuantileReq& r, int k, int* hist
                 ok[u] = i < r.n && q_select(r, i, &v[u]);
             }
 #pragma unroll
-            for (int u = 0; u < kQuantAhead; ++u) {
-                if (!ok[u]) continue;
-                const unsigned long long key = order_key(v[u]);
-                if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & (nb - 1)], 1);
-            }
+            for (int u = 0; u < kQuantAhead; ++u)
+                if (ok[u]) fn(order_key(v[u]));
         }
-        __syncthreads();
-        cta_pick_digit<kQuantThreads>(hist, nb, kk, warp_tot, s_pick);
-        prefix |= (unsigned long long)s_pick[0] << shift;
-        pmask |= (unsigned long long)(nb - 1) << shift;
-        kk = s_pick[1];
-        __syncthreads();
-    }
-    return prefix;
-}
-
-// The key of the (k+1)-th smallest given the k-th's key: itself when at least k + 2 selected keys
-// are <= it, else the smallest key above it (one pass).
-__device__ unsigned long long cta_next_key(const QuantileReq& r, int k, unsigned long long key_k, int* s_cnt,
-                                           unsigned long long* s_min) {
-    if (threadIdx.x == 0) {
-        *s_cnt = 0;
-        *s_min = ~0ull;
-    }
-    __syncthreads();
-    int cnt = 0;
-    unsigned long long mn = ~0ull;
-    for (int i = threadIdx.x; i < r.n; i += kQuantThreads) {
-        double v;
-        if (!q_select(r, i, &v)) continue;
-        const unsigned long long key = order_key(v);
-        if (key <= key_k) ++cnt;
-        else mn = min(mn, key);
-    }
-    atomicAdd(s_cnt, cnt);
-    atomicMin(s_min, mn);
-    __syncthreads();
-    const unsigned long long out = *s_cnt >= k + 2 ? key_k : *s_min;
-    __syncthreads();
-    return out;
-}
-
-// One CTA per request: out[2 * b] = result (NaN when nothing is selected), out[2 * b + 1] = count.
-__global__ void __launch_bounds__(kQuantThreads) k_quantiles(const QuantileReq* reqs, double* out) {
-    __shared__ int hist[2048];
-    __shared__ int warp_tot[32];
-    __shared__ int s_pick[2];
-    __shared__ int s_count, s_nan;
-    __shared__ unsigned long long s_min;
-    const QuantileReq r = reqs[blockIdx.x];
-    if (threadIdx.x == 0) s_count = s_nan = 0;
-    __syncthreads();
-    int c = 0, nan = 0;
-    for (int i = threadIdx.x; i < r.n; i += kQuantThreads) {
-        double v;
-        if (q_select(r, i, &v)) {
-            ++c;
-            nan += isnan(v);
-        }
-    }
-    atomicAdd(&s_count, c);
-    atomicAdd(&s_nan, nan);
-    __syncthreads();
-    const int n = s_count;
-    const bool any_nan = s_nan != 0;
-    __syncthreads();
+    };
     double res = dnan();
     if (n > 0 && !any_nan) {  // numpy: a NaN among the values makes the median / percentile NaN
+        unsigned long long ka, kb;
         if (r.mode == 0) {
-            const int k = (n - 1) / 2;
-            const unsigned long long ka = cta_kth_key(r, k, hist, warp_tot, s_pick);
-            const double a = key_value(ka);
-            const double b = (n & 1) ? a : key_value(cta_next_key(r, k, ka, &s_count, &s_min));
-            res = __ddiv_rn(__dadd_rn(a, b), 2.0);
+            cta_select<kQuantThreads>(for_keys, (n - 1) / 2, (n & 1) == 0, s_kmin, s_kmax, hist, warp_tot, s_pick,
+                                      s_keys, &ka, &kb);
+            res = __ddiv_rn(__dadd_rn(key_value(ka), key_value(kb)), 2.0);
         } else {
             // numpy 'linear': virtual index (n - 1) q, _lerp of the neighbours.
             const double virt = __dmul_rn((double)(n - 1), r.q);
             const double below = floor(virt);
             const int lo = min(max((int)below, 0), n - 1), hi = min(lo + 1, n - 1);
-            const unsigned long long ka = cta_kth_key(r, lo, hist, warp_tot, s_pick);
+            cta_select<kQuantThreads>(for_keys, lo, hi != lo, s_kmin, s_kmax, hist, warp_tot, s_pick, s_keys, &ka,
+                                      &kb);
             const double a = key_value(ka);
-            const double b = hi == lo ? a : key_value(cta_next_key(r, lo, ka, &s_count, &s_min));
+            const double b = key_value(kb);
             if (virt >= (double)(n - 1)) {
                 res = b;
             } else {
@@ -1438,6 +1493,9 @@ int spx_render_model(const double* params, const int* boxes, int n, int height, 
     if (tile == 16)
         k_render<16><<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
                                           L.overflow);
+    else if (tile == 64)
+        k_render<64><<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
+                                          L.overflow);
     else
         k_render<32><<<grid, 256, 0, s>>>(height, width, bin_view(L.bins), params, L.centres, L.radius, L.rmax, model,
                                           L.overflow);
@@ -1494,7 +1552,10 @@ int spx_tile_medians(const void* img, int dtype, double sign, int height, int wi
     const long long t2 = (long long)tile * tile;
     const int smem_keys = (int)(t2 < kTileSmemKeys ? t2 : kTileSmemKeys);
     const size_t smem = (size_t)smem_keys * sizeof(unsigned long long);
-    SPX_CUDA(cudaFuncSetAttribute(k_tile_median, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kernel = dtype == SPX_U8 ? k_tile_median<uint8_t>
+                  : dtype == SPX_U16 ? k_tile_median<uint16_t>
+                  : dtype == SPX_F32 ? k_tile_median<float> : k_tile_median<double>;
+    SPX_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // Smallest integer squared distance whose square root reaches thr_dist (sqrt is correctly
     // rounded here and on the device, and monotonic), so the kernel compares integers.
     unsigned long long d2_min = 0;
@@ -1508,7 +1569,7 @@ int spx_tile_medians(const void* img, int dtype, double sign, int height, int wi
         d2_min = d;
     }
     TileSel sel{Image{img, dtype, sign, height, width}, model, dist2, usable, mode, thr_model, d2_min};
-    k_tile_median<<<ny * nx, kTileThreads, smem, s>>>(sel, tile, nx, smem_keys, medians, counts);
+    kernel<<<ny * nx, kTileThreads, smem, s>>>(sel, tile, nx, smem_keys, medians, counts);
     return check_launch("k_tile_median");
 }
 

@@ -1054,10 +1054,10 @@ int spx_tune_set(const char* knob, int value) {
         SPX_REQUIRE(value >= 2 && value <= 32, "fit_blocks_per_sm must be in [2, 32]");
         t.fit_blocks_per_sm = value;
     } else if (!strcmp(knob, "render_tile")) {
-        SPX_REQUIRE(value == 16 || value == 32, "render_tile must be 16 or 32");
+        SPX_REQUIRE(value == 16 || value == 32 || value == 64, "render_tile must be 16, 32 or 64");
         t.render_tile = value;
     } else if (!strcmp(knob, "radial_rays")) {
-        SPX_REQUIRE(value == 0 || value == 1, "radial_rays must be 0 or 1");
+        SPX_REQUIRE(value >= 0 && value <= 2, "radial_rays must be 0, 1 or 2");
         t.radial_rays = value;
     } else {
         set_error("unknown tuning knob '%s'", knob);

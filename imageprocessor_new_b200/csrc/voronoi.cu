@@ -64,6 +64,7 @@ namespace {
 
 constexpr int kTile = 16;
 constexpr int kThreads = kTile * kTile;
+constexpr int kRowsMax = 64;  // bin rows of a search square that the one-pass candidate staging takes
 
 __device__ __forceinline__ double dist2(double px, double py, double sx, double sy) {
     const double dx = __dsub_rn(px, sx), dy = __dsub_rn(py, sy);
@@ -102,22 +103,40 @@ __device__ double warp_nearest_bound(const BinGrid& g, double cx, double cy, int
 }
 
 // labels != null: nearest-seed index; d2 != null: squared distance to the nearest seed.
-__global__ void __launch_bounds__(kThreads) k_voronoi(int H, int W, BinGrid g, int* labels,
+// The tile at (tx0, ty0): its centre and the half of its diagonal (pixel centres).
+__device__ __forceinline__ void tile_geometry(int H, int W, int tx0, int ty0, double* cx, double* cy,
+                                              double* half_diag) {
+    const int ex = min(kTile, W - tx0), ey = min(kTile, H - ty0);
+    *cx = 0.5 * (tx0 + tx0 + ex - 1);
+    *cy = 0.5 * (ty0 + ty0 + ey - 1);
+    *half_diag = 0.5 * sqrt((double)(ex - 1) * (ex - 1) + (double)(ey - 1) * (ey - 1));
+}
+
+// Per 16 x 16 tile, the radius around its centre that holds every seed that can be the nearest of
+// one of its pixels: the centre's nearest-seed distance plus the tile's diagonal, plus 1 px of
+// slack for rounding (infinite without seeds). One warp per tile, so that the ring searches'
+// dependent loads of many tiles overlap.
+__global__ void k_tile_bounds(int H, int W, BinGrid g, int tiles_x, int tiles, double* bound) {
+    const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (int t = blockIdx.x * warps + (threadIdx.x >> 5); t < tiles; t += gridDim.x * warps) {
+        double cx, cy, half_diag;
+        tile_geometry(H, W, (t % tiles_x) * kTile, (t / tiles_x) * kTile, &cx, &cy, &half_diag);
+        const double best = warp_nearest_bound(g, cx, cy, lane);
+        if (lane == 0) bound[t] = sqrt(best) + 2.0 * half_diag + 1.0;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_voronoi(int H, int W, BinGrid g, const double* bound, int* labels,
                                                        unsigned int* d2out) {
     __shared__ double2 c_xy[kThreads];
     __shared__ int c_id[kThreads];
-    __shared__ double s_bound;
+    __shared__ int row_j0[kRowsMax], row_pre[kRowsMax + 1];
+    __shared__ int s_kept;
     const int tx0 = blockIdx.x * kTile, ty0 = blockIdx.y * kTile;
     const int lane = threadIdx.x & 31;
-    const int ex = min(kTile, W - tx0), ey = min(kTile, H - ty0);
-    const double cx = 0.5 * (tx0 + tx0 + ex - 1), cy = 0.5 * (ty0 + ty0 + ey - 1);
-    const double half_diag = 0.5 * sqrt((double)(ex - 1) * (ex - 1) + (double)(ey - 1) * (ey - 1));
-    if (threadIdx.x < 32) {
-        const double best = warp_nearest_bound(g, cx, cy, lane);
-        if (lane == 0) s_bound = sqrt(best) + 2.0 * half_diag + 1.0;
-    }
-    __syncthreads();
-    const double R = s_bound;
+    double cx, cy, half_diag;
+    tile_geometry(H, W, tx0, ty0, &cx, &cy, &half_diag);
+    const double R = bound[blockIdx.y * gridDim.x + blockIdx.x];
     int gx0, gx1, gy0, gy1;
     if (isfinite(R)) {
         gx0 = bin_index(cx - R, g.cell, g.gw);
@@ -133,21 +152,89 @@ __global__ void __launch_bounds__(kThreads) k_voronoi(int H, int W, BinGrid g, i
     const double px = (double)x, py = (double)y;
     double best = dinf();
     int label = 0x7fffffff;
-    for (int gy = gy0; gy <= gy1; ++gy) {
-        const int j0 = g.start[gy * g.gw + gx0], j1 = g.start[gy * g.gw + gx1 + 1];
-        for (int base = j0; base < j1; base += kThreads) {
-            const int m = min(kThreads, j1 - base);
-            __syncthreads();
-            if ((int)threadIdx.x < m) {
-                c_xy[threadIdx.x] = g.xy[base + threadIdx.x];
-                c_id[threadIdx.x] = g.id[base + threadIdx.x];
+    auto scan = [&](int m) {
+        for (int k = 0; k < m; ++k) {
+            const double2 s = c_xy[k];
+            const double d2 = dist2(px, py, s.x, s.y);
+            const int id = c_id[k];
+            if (d2 < best || (d2 == best && id < label)) { best = d2; label = id; }
+        }
+    };
+    // The search square's seeds as runs of the bin-sorted array, one per bin row, with their
+    // prefix; warp 0 builds it (lane r takes rows r and r + 32).
+    const int n_rows = gy1 - gy0 + 1;
+    int total = kThreads + 1;
+    if (isfinite(R) && n_rows <= kRowsMax) {
+        if (threadIdx.x < 32) {
+            int len[2] = {0, 0};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = lane + 32 * h;
+                if (r < n_rows) {
+                    const int b = (gy0 + r) * g.gw;
+                    row_j0[r] = g.start[b + gx0];
+                    len[h] = g.start[b + gx1 + 1] - row_j0[r];
+                }
             }
-            __syncthreads();
-            for (int k = 0; k < m; ++k) {
-                const double2 s = c_xy[k];
-                const double d2 = dist2(px, py, s.x, s.y);
-                const int id = c_id[k];
-                if (d2 < best || (d2 == best && id < label)) { best = d2; label = id; }
+            // Inclusive scans of the two halves, the second offset by the first's total.
+            int a = len[0], c = len[1];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int ua = __shfl_up_sync(0xffffffffu, a, o), uc = __shfl_up_sync(0xffffffffu, c, o);
+                if (lane >= o) { a += ua; c += uc; }
+            }
+            const int first = __shfl_sync(0xffffffffu, a, 31);
+            row_pre[lane + 1] = a;
+            row_pre[lane + 33] = first + c;
+            if (lane == 0) {
+                row_pre[0] = 0;
+                s_kept = 0;
+            }
+        }
+        __syncthreads();
+        total = row_pre[n_rows];
+    }
+    if (total <= kThreads) {
+        // Seeds farther than R from the tile centre are no pixel's nearest (nor tied): a pixel p of
+        // the tile has a seed within |p - c| + sqrt(best) <= half_diag + sqrt(best), and a seed s
+        // with |s - c| > sqrt(best) + 2 half_diag is farther from p than that. R keeps 1 px of
+        // slack for rounding. The rest are compacted (in no particular order: the (d2, index) rule
+        // does not depend on it).
+        const int t = threadIdx.x;
+        bool keep = false;
+        double2 sxy = make_double2(0.0, 0.0);
+        int sid = 0;
+        if (t < total) {
+            int r = 0;
+            while (row_pre[r + 1] <= t) ++r;
+            const int j = row_j0[r] + (t - row_pre[r]);
+            sxy = g.xy[j];
+            sid = g.id[j];
+            keep = dist2(cx, cy, sxy.x, sxy.y) <= R * R;
+        }
+        const unsigned vote = __ballot_sync(0xffffffffu, keep);
+        int base = 0;
+        if (lane == 0 && vote) base = atomicAdd(&s_kept, __popc(vote));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (keep) {
+            const int slot = base + __popc(vote & ((1u << lane) - 1u));
+            c_xy[slot] = sxy;
+            c_id[slot] = sid;
+        }
+        __syncthreads();
+        scan(s_kept);
+    } else {
+        for (int gy = gy0; gy <= gy1; ++gy) {
+            const int j0 = g.start[gy * g.gw + gx0], j1 = g.start[gy * g.gw + gx1 + 1];
+            for (int base = j0; base < j1; base += kThreads) {
+                const int m = min(kThreads, j1 - base);
+                __syncthreads();
+                if ((int)threadIdx.x < m) {
+                    c_xy[threadIdx.x] = g.xy[base + threadIdx.x];
+                    c_id[threadIdx.x] = g.id[base + threadIdx.x];
+                }
+                __syncthreads();
+                scan(m);
             }
         }
     }
@@ -220,6 +307,7 @@ namespace {
 struct VorWs {
     BinStorage bins;
     double* seed_px;
+    double* tile_bound;  // one per 16 x 16 tile
 };
 
 VorWs vor_layout(void* ws, int n, int H, int W, size_t* bytes) {
@@ -227,8 +315,19 @@ VorWs vor_layout(void* ws, int n, int H, int W, size_t* bytes) {
     VorWs v;
     v.bins = bin_layout(a, n, H, W, bin_cell_size(n, H, W));
     v.seed_px = a.take<double>(2 * (size_t)(n > 0 ? n : 1));
+    v.tile_bound = a.take<double>((size_t)((W + kTile - 1) / kTile) * ((H + kTile - 1) / kTile));
     if (bytes) *bytes = a.used;
     return v;
+}
+
+int launch_voronoi(const VorWs& L, int H, int W, int* labels, unsigned int* d2, cudaStream_t s) {
+    const dim3 grid((W + kTile - 1) / kTile, (H + kTile - 1) / kTile);
+    const int tiles = (int)(grid.x * grid.y);
+    k_tile_bounds<<<grid_for(tiles, 8, 148 * 16), 256, 0, s>>>(H, W, bin_view(L.bins), (int)grid.x, tiles,
+                                                               L.tile_bound);
+    if (int e = check_launch("k_tile_bounds")) return e;
+    k_voronoi<<<grid, kThreads, 0, s>>>(H, W, bin_view(L.bins), L.tile_bound, labels, d2);
+    return check_launch("k_voronoi");
 }
 
 }  // namespace
@@ -255,9 +354,8 @@ int spx_voronoi_labels(const double* seeds, int n, int height, int width, int* l
     SPX_REQUIRE(workspace_bytes >= spx_voronoi_workspace_bytes(n, height, width), "workspace too small");
     VorWs L = vor_layout(workspace, n, height, width, nullptr);
     if (int e = bin_build(L.bins, seeds, 2, nullptr, nullptr, n, s)) return e;
-    const dim3 grid((width + kTile - 1) / kTile, (height + kTile - 1) / kTile);
-    k_voronoi<<<grid, kThreads, 0, s>>>(height, width, bin_view(L.bins), labels, nullptr);
-    return check_launch("k_voronoi");
+    if (int e = launch_voronoi(L, height, width, labels, nullptr, s)) return e;
+    return SPX_OK;
 }
 
 int spx_seed_distance_map(const double* seeds, int n, int height, int width, unsigned int* d2,
@@ -270,9 +368,8 @@ int spx_seed_distance_map(const double* seeds, int n, int height, int width, uns
     k_seed_pixels<<<grid_for(n, 256), 256, 0, s>>>(seeds, n, height, width, L.seed_px);
     if (int e = check_launch("k_seed_pixels")) return e;
     if (int e = bin_build(L.bins, L.seed_px, 2, nullptr, nullptr, n, s)) return e;
-    const dim3 grid((width + kTile - 1) / kTile, (height + kTile - 1) / kTile);
-    k_voronoi<<<grid, kThreads, 0, s>>>(height, width, bin_view(L.bins), nullptr, d2);
-    return check_launch("k_voronoi");
+    if (int e = launch_voronoi(L, height, width, nullptr, d2, s)) return e;
+    return SPX_OK;
 }
 
 int spx_nearest_distances(const double* points, int n, const double* queries, int nq, int exclude_self,

@@ -38,7 +38,7 @@ def test_every_setting_gives_identical_results(tmp_path, monkeypatch):
     cells = page_cells(page)
     outs = []
     try:
-        for fw, fb, rt in itertools.product((2, 4, 8), (4, 16), (16, 32)):
+        for fw, fb, rt in itertools.product((2, 4, 8), (4, 16), (16, 32, 64)):
             autotune.apply({"fit_warps": fw, "fit_blocks_per_sm": fb, "render_tile": rt})
             dbl = Deblender(page, 1.0, cells)
             p, st, it = dbl.initial(dbl.max_iter)
@@ -61,8 +61,8 @@ def test_every_setting_gives_identical_results(tmp_path, monkeypatch):
 
 
 def test_radial_ray_mappings_give_identical_cds():
-    """One ray per thread and one ray per warp: the same edges, statuses and metrics bit for bit,
-    with and without profile smoothing."""
+    """One ray per thread (cached window or window read per sample) and one ray per warp: the same
+    edges, statuses and metrics bit for bit, with and without profile smoothing."""
     from imageprocessor_new_b200 import autotune, measure_cds, synthetic
 
     before = autotune.current()
@@ -70,16 +70,17 @@ def test_radial_ray_mappings_give_identical_cds():
     try:
         for smooth in (0.0, 1.0):
             res = []
-            for mode in (0, 1):
+            for mode in (0, 1, 2):
                 autotune.set("radial_rays", mode)
                 res.append(measure_cds(page, backend="gpu", methods=("gradient", "halfmax"), area_max=400,
                                        smooth_sigma=smooth))
-            for m in ("gradient", "halfmax"):
-                a, b = res[0].measurements[m], res[1].measurements[m]
-                np.testing.assert_array_equal(a.geometry["edge_px"], b.geometry["edge_px"])
-                np.testing.assert_array_equal(a.status, b.status)
-                np.testing.assert_array_equal(a.contours_xy, b.contours_xy)
-                for k in a.metrics:
-                    np.testing.assert_array_equal(a.metrics[k], b.metrics[k], err_msg=k)
+            for other in res[1:]:
+                for m in ("gradient", "halfmax"):
+                    a, b = res[0].measurements[m], other.measurements[m]
+                    np.testing.assert_array_equal(a.geometry["edge_px"], b.geometry["edge_px"])
+                    np.testing.assert_array_equal(a.status, b.status)
+                    np.testing.assert_array_equal(a.contours_xy, b.contours_xy)
+                    for k in a.metrics:
+                        np.testing.assert_array_equal(a.metrics[k], b.metrics[k], err_msg=k)
     finally:
         autotune.apply(before)
