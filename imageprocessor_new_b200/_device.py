@@ -3,7 +3,7 @@
 from __future__ import annotations
 
 import contextlib
-import warnings
+import os
 
 import numpy as np
 import torch
@@ -31,23 +31,51 @@ def ptr(t: torch.Tensor | None) -> int | None:
     return None if t is None else t.data_ptr()
 
 
+_UPLOAD_POOL = None
+_UPLOAD_CHUNK = 8 << 20  # bytes per host copy / device copy pair of a large upload
+
+
+def _upload_pool():
+    global _UPLOAD_POOL
+    if _UPLOAD_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+
+        _UPLOAD_POOL = ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1)),
+                                          thread_name_prefix="spx-upload")
+    return _UPLOAD_POOL
+
+
 def upload(a: np.ndarray) -> torch.Tensor:
     """Host array -> contiguous device tensor (same dtype), queued on the current stream.
 
     The data goes through pinned memory: a copy from pageable memory would first synchronise the
     stream (draining the GPU at every small upload); from pinned memory it is asynchronous, and
-    torch's host allocator keeps the pinned block until the copy has run."""
+    torch's host allocator keeps the pinned block until the copy has run. A large array is copied
+    into the pinned block in 8 MB chunks by a few host threads, and each chunk's device copy is
+    queued as soon as its host copy is done, so the two overlap."""
     a = np.ascontiguousarray(a)
     dtype = TORCH_ALL.get(a.dtype) or torch.from_numpy(np.empty(0, a.dtype)).dtype
     pinned = torch.empty(a.shape, dtype=dtype, pin_memory=True)
-    if a.nbytes >= 1 << 22:
-        # torch's CPU copy splits a large copy over the host threads; the source is only read.
-        with warnings.catch_warnings():
-            warnings.simplefilter("ignore", UserWarning)  # read-only arrays: torch warns on wrapping them
-            pinned.copy_(torch.from_numpy(a))
-    else:
+    if a.nbytes < 4 * _UPLOAD_CHUNK:
         pinned.numpy()[...] = a
-    return pinned.to("cuda", non_blocking=True)
+        return pinned.to("cuda", non_blocking=True)
+    out = torch.empty(a.shape, dtype=dtype, device="cuda")
+    n = a.nbytes
+    src = a.reshape(-1).view(np.uint8)
+    host = pinned.numpy().reshape(-1).view(np.uint8)
+    host_t = pinned.view(-1).view(torch.uint8)
+    dev_t = out.view(-1).view(torch.uint8)
+    bounds = [(lo, min(lo + _UPLOAD_CHUNK, n)) for lo in range(0, n, _UPLOAD_CHUNK)]
+
+    def copy(lo, hi):
+        host[lo:hi] = src[lo:hi]  # NumPy releases the GIL for the copy
+
+    pool = _upload_pool()
+    futures = [pool.submit(copy, lo, hi) for lo, hi in bounds]
+    for (lo, hi), f in zip(bounds, futures):
+        f.result()
+        dev_t[lo:hi].copy_(host_t[lo:hi], non_blocking=True)
+    return out
 
 
 def start_download(t: torch.Tensor) -> np.ndarray:

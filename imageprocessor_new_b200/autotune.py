@@ -1,10 +1,11 @@
 """Autotuner of the launch shapes (no reference counterpart).
 
 The knobs (``spx_tune_set``): warps per block and persistent blocks per SM of the LM fit kernels,
-the model-render tile, and how the radial profiles map rays to threads (one ray per thread, or one
-ray per warp with 32 samples at once). None of them changes a result -- the fits take cells from a
+the model-render tile, and how the radial profiles map rays to threads (one ray per thread with the
+spline window cached in registers, one ray per warp with 32 samples at once, or one ray per thread
+reading the window at every sample). None of them changes a result -- the fits take cells from a
 device work queue and every cell's arithmetic is the same whatever shape runs it; the render sums
-each pixel's Gaussians in cell order in every tile shape; both ray mappings evaluate the same
+each pixel's Gaussians in cell order in every tile shape; the ray mappings evaluate the same
 samples with the same arithmetic and rules -- so the tuner only times them. It times each
 candidate with CUDA events on the caller's own data (one initial fit, one deblending iteration and
 one render of a page's cells), one knob at a time in the order below, and keeps the fastest. A

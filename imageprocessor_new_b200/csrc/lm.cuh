@@ -97,7 +97,8 @@ __device__ __forceinline__ void damped_solve(const double* nu, const double* g, 
 // partial sums meet at every level, so the totals are identical to 27 separate butterflies) but as a
 // reduce-scatter: at each level a lane keeps half of its slots, adding its partner's copy of them,
 // so 31 additions and shuffles replace 135; lane i then holds total i and broadcasts it.
-// `slot` (shared memory, 27 doubles, or null) also receives the totals (lane i writes total i).
+// With `slot` (shared memory, 27 doubles) the totals go there instead (lane i writes total i) and s is
+// left as it was; without it every lane's s receives them.
 __device__ __forceinline__ void warp_allreduce27(double* s, int lane, double* slot = nullptr) {
     double a[32];
 #pragma unroll
@@ -113,12 +114,10 @@ __device__ __forceinline__ void warp_allreduce27(double* s, int lane, double* sl
         }
     }
     if (slot) {
-        // Broadcast through the shared-memory slot: 27 uniform loads instead of 27 shuffles of
-        // two halves each.
+        // The totals stay in the shared-memory slot (lane i writes total i), where the solve reads
+        // them, instead of 27 registers on every lane.
         if (lane < 27) slot[lane] = a[0];
         __syncwarp();
-#pragma unroll
-        for (int i = 0; i < 27; ++i) s[i] = slot[i];
         return;
     }
 #pragma unroll
@@ -126,10 +125,11 @@ __device__ __forceinline__ void warp_allreduce27(double* s, int lane, double* sl
 }
 
 // One pass over the pixels at params q: the 21 upper-triangle entries of J^T J and the 6 of J^T r
-// into s[0..26] and the cost sum of r^2 with r = v - A shape (numpy's model-then-residual order),
-// as warp totals identical on all lanes.
+// as warp totals into slot[0..26] (shared memory) and the cost sum of r^2 with r = v - A shape
+// (numpy's model-then-residual order), returned on all lanes.
 __device__ __forceinline__ double warp_normal_pass(const double* q, const double* v, const int* xy, int n, int lane,
-                                                   double* s, double* slot = nullptr) {
+                                                   double* slot) {
+    double s[27];
 #pragma unroll
     for (int i = 0; i < 27; ++i) s[i] = 0.0;
     double acc = 0.0;
@@ -178,7 +178,8 @@ __device__ __forceinline__ float u16_to_float(int u) { return __int_as_float(0x4
 // The FP32 pass: as warp_normal_pass above with the per-pixel arithmetic and lane sums in FP32
 // (ROI-local coordinates keep dx, dy within a few ulp of 64) and FP64 warp totals.
 __device__ __forceinline__ double warp_normal_pass(const double* q, const float* v, const int* xy, int n, int lane,
-                                                   double* s, double* slot = nullptr) {
+                                                   double* slot) {
+    double s[27];
     float jj[21];
 #pragma unroll
     for (int i = 0; i < 21; ++i) jj[i] = 0.0f;
@@ -219,11 +220,12 @@ __device__ __forceinline__ double warp_normal_pass(const double* q, const float*
 // Fits p (ROI-local, identical on all lanes) to the n compacted pixels. Returns the number of
 // iterations run. `cap` is the cell's sigma cap, `amp_cap` 3 * max(max|v|, 1e-12).
 //
-// Each trial's cost is evaluated in the same pass as its normal equations: an accepted trial (the
-// usual case) hands its sums to the next iteration; a rejected one restores the sums of the kept
-// params, which every pass also leaves in one of the warp's two shared-memory slots (`slots`, 54
-// doubles; the pass at the kept params wrote slot `kept`, a trial writes the other one). The
-// arithmetic of every sum is that of separate Jacobian and cost passes.
+// Each trial's cost is evaluated in the same pass as its normal equations. Every pass leaves its
+// sums in one of the warp's two shared-memory slots (`slots`, 54 doubles): the pass at the kept
+// params wrote slot `kept`, which the solve reads; a trial writes the other one, which becomes the
+// kept slot when the trial is accepted (the usual case) and is overwritten by the next trial when
+// it is not. The sums never occupy registers during the solve. The arithmetic of every sum is that
+// of separate Jacobian and cost passes.
 // `cost_tol` is the relative cost drop at or below which an accepted step ends the fit (1e-12, the
 // reference's rule, by default).
 // `final_cost` (optional) receives the cost at the returned params (the same on every lane).
@@ -231,9 +233,8 @@ template <typename T>
 __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, double cap, double amp_cap,
                                   int max_iter, int lane, double* slots, double cost_tol = 1e-12,
                                   double* final_cost = nullptr) {
-    double s[27];
     int kept = 0;
-    double cost = warp_normal_pass(p, v, xy, n, lane, s, slots);
+    double cost = warp_normal_pass(p, v, xy, n, lane, slots);
     if (final_cost) *final_cost = cost;
     if (!isfinite(cost)) return 0;
     double lam = 1e-3;
@@ -241,7 +242,7 @@ __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, d
     int it = 0;
     for (; it < max_iter; ++it) {
         double step[6];
-        damped_solve(s, s + 21, lam, step);
+        damped_solve(slots + 27 * kept, slots + 27 * kept + 21, lam, step);
         double trial[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) trial[i] = p[i] + step[i];
@@ -256,7 +257,8 @@ __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, d
         bool small = smax < 1e-7;
 #pragma unroll
         for (int i = 0; i < 6; ++i) small = small && !isnan(step[i]);
-        const double new_cost = warp_normal_pass(trial, v, xy, n, lane, s, slots + 27 * (kept ^ 1));
+        // The trial's sums go to the other slot; a rejected trial leaves the kept slot as it was.
+        const double new_cost = warp_normal_pass(trial, v, xy, n, lane, slots + 27 * (kept ^ 1));
         const bool better = isfinite(new_cost) && new_cost <= cost;
         const bool done = (better && (cost - new_cost <= cost_tol * fmax(cost, 1e-300))) || small;
         if (better) {
@@ -269,11 +271,6 @@ __device__ inline int warp_lm_fit(double* p, const T* v, const int* xy, int n, d
             lam *= 4.0;
         }
         if (done || lam > 1e12) { ++it; break; }
-        if (!better && it + 1 < max_iter) {
-            __syncwarp();
-#pragma unroll
-            for (int i = 0; i < 27; ++i) s[i] = slots[27 * kept + i];
-        }
     }
     __syncwarp();
     if (final_cost) *final_cost = cost;
