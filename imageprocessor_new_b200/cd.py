@@ -25,10 +25,11 @@ METHOD_LABELS = {
     "logquad": "Gaussian FWHM",
     "gradient": "Maximum radial gradient",
     "halfmax": "Half-height contour",
+    "projection": "x/y projection max-slope width",
 }
 SUPPORTED = tuple(METHOD_LABELS)
 # Methods of the reference that are outside this package (invariant, local, outline families).
-OTHER_METHODS = ("disk", "flux_ratio", "projection", "half_area", "half_area_min", "half_area_min_avg",
+OTHER_METHODS = ("disk", "flux_ratio", "half_area", "half_area_min", "half_area_min_avg",
                  "tail_area", "tail_area_norm", "edge_area", "foot_area", "foot_area_ratio", "local_projection",
                  "local_half_area", "local_half_area_min_avg", "local_tail_area", "outline_fit", "outline_fit_fast")
 
@@ -43,7 +44,34 @@ def _metric_names(method: str) -> tuple[str, ...]:
         return _COLS + FIT_METRICS
     if method == "gaussian":
         return _COLS + FIT_METRICS[:-1] + ("fit_rmse",)
+    if method == "projection":
+        return _COLS
     return _COLS + ("ray_coverage",)
+
+
+_PROJECTION_STEP = 0.02
+_ZERO_PAD = 32
+_PROJECTION_OPS: dict = {}
+
+
+def _projection_operators(size: int):
+    """Grid length G and the (size, G) operators that give a profile's not-a-knot cubic spline and its
+    slope at the points k * 0.02 (k < G) as profile @ operator: scipy's CubicSpline of the profile
+    padded with 32 zeros on either side, as subpx/_cpu/invariant_cd.py:343-358 builds them (the spline
+    is linear in the samples). Computed once per size on the host and kept on the device."""
+    key = (int(size), torch.cuda.current_device())
+    if key not in _PROJECTION_OPS:
+        from scipy.interpolate import CubicSpline
+
+        grid = np.arange(0.0, size - 1 + _PROJECTION_STEP / 2, _PROJECTION_STEP)
+        n = size + 2 * _ZERO_PAD
+        unit = np.zeros((n, size))
+        unit[_ZERO_PAD + np.arange(size), np.arange(size)] = 1.0
+        spline = CubicSpline(np.arange(n), unit, axis=0)
+        value_op = np.ascontiguousarray(spline(grid + _ZERO_PAD).T)
+        slope_op = np.ascontiguousarray(spline(grid + _ZERO_PAD, 1).T)
+        _PROJECTION_OPS[key] = (len(grid), dev.upload(value_op), dev.upload(slope_op))
+    return _PROJECTION_OPS[key]
 
 
 def _validate(img, *, methods, background, seeds, threshold, area_min, area_max, pad, n_angles, radial_step,
@@ -206,7 +234,8 @@ def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
         "contours": (m, n_angles + 1, 2) if contours else None,
         "metrics": (max(len(names), 13), m),  # column-major: one contiguous column per metric
         "center_local": (m, 2),
-        "edge_px": (m, n_angles) if method in ("gradient", "halfmax") else None,
+        "edge_px": (m, n_angles) if method in ("gradient", "halfmax") or (method == "projection" and contours)
+        else None,
         "eigenvalues": (m, 2) if method in ("logquad", "gaussian") else None,
         "axes": (m, 2, 2) if method in ("logquad", "gaussian") else None,
         "status": ((m + 7) // 8,),  # bytes, viewed as uint8
@@ -275,6 +304,9 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
         geometry = {"center_local": part("center_local"), "eigenvalues": part("eigenvalues"), "axes": part("axes")}
     elif method in ("gradient", "halfmax"):
         geometry = {"center_local": part("center_local"), "edge_px": part("edge_px")}
+    elif method == "projection":
+        geometry = {"center_local": part("center_local"),
+                    "edge_px": part("edge_px") if shapes["edge_px"] is not None else np.empty((n, 0))}
     elif not metrics_only:
         geometry = {"eigenvalues": part("eigenvalues"), "axes": part("axes")}
     return CDMethodResult(method=method, centers_xy=part("centers"), contours_xy=contours,
@@ -534,12 +566,23 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
             bufs["gradient"] = gb[0]
         launched([m for m in ("halfmax", "gradient") if m in bufs])
     seconds["radial"] = time.perf_counter() - start - t_gauss
+    t_proj = time.perf_counter()
+    if "projection" in methods and nr:
+        pb = _method_buffers(nr, n_angles, "projection", not metrics_only)
+        gx, vx, sx = _projection_operators(c.wm)
+        gy, vy, sy = _projection_operators(c.hm)
+        _lib.call("spx_projection_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(),
+                  report_d.data_ptr(), nr, c.hm, c.wm, width, n_angles, _PROJECTION_STEP, vx.data_ptr(),
+                  sx.data_ptr(), gx, vy.data_ptr(), sy.data_ptr(), gy, pb[1], stream)
+        bufs["projection"] = pb[0]
+        launched(["projection"])
+    seconds["projection"] = time.perf_counter() - t_proj
     for names, copies in pending:
         t0 = time.perf_counter()
         for name, (host, done) in zip(names, copies):
             done.synchronize()
             found[name] = _to_result(name, nr, bufs[name], host.numpy(), metrics_only, n_angles)
-        key = "gaussian" if names == ["gaussian"] else "radial"
+        key = names[0] if names[0] in ("gaussian", "projection") else "radial"
         seconds[key] = seconds.get(key, 0.0) + time.perf_counter() - t0
     seconds["gaussian"] = seconds.get("gaussian", 0.0) + t_gauss
     for name in methods:
@@ -625,6 +668,8 @@ def _empty_result(method, n_angles, metrics_only) -> CDMethodResult:
         geometry = {"center_local": np.zeros((0, 2)), "eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}
     elif method in ("gradient", "halfmax"):
         geometry = {"center_local": np.zeros((0, 2)), "edge_px": np.zeros((0, n_angles))}
+    elif method == "projection":
+        geometry = {"center_local": np.zeros((0, 2)), "edge_px": np.zeros((0, 0 if metrics_only else n_angles))}
     elif not metrics_only:
         geometry = {"eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}
     return CDMethodResult(method=method, centers_xy=np.zeros((0, 2)),

@@ -1192,14 +1192,243 @@ __global__ void k_rebuild_contours(int kind, const double* centers, const double
     }
 }
 
+// ------------------------------------------------------------------------------ projection
+
+// numpy's sum of n values a[k * stride] along a contiguous axis (pairwise_sum): in order below 8
+// values; up to 128, eight running sums (a[j], a[j + 8], ...) combined as ((r0 + r1) + (r2 + r3)) +
+// ((r4 + r5) + (r6 + r7)), then the values past the last full eight in order; above 128, the two
+// halves (the first a multiple of 8 long) summed that way and added.
+__device__ double np_pairwise_sum(const double* a, int n, int stride) {
+    if (n < 8) {
+        double r = 0.0;
+        for (int i = 0; i < n; ++i) r = __dadd_rn(r, a[i * stride]);
+        return r;
+    }
+    if (n <= 128) {
+        double r[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) r[j] = a[j * stride];
+        int i = 8;
+        for (; i < n - (n % 8); i += 8)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) r[j] = __dadd_rn(r[j], a[(i + j) * stride]);
+        double res = __dadd_rn(__dadd_rn(__dadd_rn(r[0], r[1]), __dadd_rn(r[2], r[3])),
+                               __dadd_rn(__dadd_rn(r[4], r[5]), __dadd_rn(r[6], r[7])));
+        for (; i < n; ++i) res = __dadd_rn(res, a[i * stride]);
+        return res;
+    }
+    int n2 = n / 2;
+    n2 -= n2 % 8;
+    return __dadd_rn(np_pairwise_sum(a, n2, stride), np_pairwise_sum(a + n2 * stride, n - n2, stride));
+}
+
+constexpr int kProjWarps = 4;
+
+// The "projection" CD of each cell (subpx/_cpu/invariant_cd.py:365-421), one warp per cell: the x
+// profile (the masked cell summed over its rows, in row order as numpy reduces a strided axis) and
+// the y profile (summed along each row, numpy's pairwise order), each spline-interpolated with the
+// host's not-a-knot operators (value_op / slope_op, size x G, the profile padded with zeros) at
+// the G points k * step. Inside the profile's span [first, last] the highest value (first on ties)
+// and, before / after it, the steepest rise and fall (first on ties) give the width (their
+// distance) and the centre (their midpoint); the cell is "ok" when both axes rise and fall strictly
+// inside their span. The result is the axis-aligned ellipse of the two widths (subpx/_cpu/
+// invariant_cd.py:320-336): edge radii a b / sqrt((b cos)^2 + (a sin)^2), contour, area pi a b,
+// equivalent CD a + b, Ramanujan's perimeter. Arithmetic in FP64 without contraction where numpy
+// rounds each operation; the spline sums are FMA chains in profile order.
+// Shared memory per warp: max(hm, wm) profile values, then max(Gx, Gy) slopes.
+__global__ void __launch_bounds__(kProjWarps * 32) k_projection_cd(
+    const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
+    int n_angles, double step, const double* vx, const double* sx, int gx, const double* vy, const double* sy,
+    int gy, MethodOut out) {
+    extern __shared__ double psm[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int pmax = max(hm, wm), gmax = max(gx, gy);
+    double* prof = psm + (long long)warp * (pmax + gmax);
+    double* slope = prof + pmax;
+    const int area_px = hm * wm;
+    for (int i = blockIdx.x * kProjWarps + warp; i < n; i += gridDim.x * kProjWarps) {
+        const int j = which ? which[i] : i;
+        const CellView c{cleaned + (long long)i * area_px, vor, boxes[j], j, W, hm, wm};
+        // Peak of the masked cell (-inf when the mask is empty).
+        double peak = -INFINITY;
+        for (int k = lane; k < area_px; k += 32)
+            if (c.mask(k / wm, k % wm)) peak = fmax(peak, c.roi[k]);
+        peak = warp_max(peak);
+        double width[2], centre[2];
+        bool good[2];
+        for (int axis = 0; axis < 2; ++axis) {
+            const int size = axis == 0 ? wm : hm;
+            const int G = axis == 0 ? gx : gy;
+            const double* vop = axis == 0 ? vx : vy;
+            const double* sop = axis == 0 ? sx : sy;
+            // Profile and the span of columns (rows) that hold mask pixels.
+            int first = size, last = -1;
+            for (int q = lane; q < size; q += 32) {
+                double v = 0.0;
+                bool any = false;
+                if (axis == 0) {  // sum over rows, in row order
+                    for (int y = 0; y < hm; ++y) {
+                        const bool m = c.mask(y, q);
+                        v = y == 0 ? (m ? c.roi[q] : 0.0) : __dadd_rn(v, m ? c.roi[y * wm + q] : 0.0);
+                        any = any || m;
+                    }
+                } else {
+                    for (int x = 0; x < wm; ++x) any = any || c.mask(q, x);
+                }
+                if (axis == 0) prof[q] = v;
+                if (any) {
+                    first = min(first, q);
+                    last = max(last, q);
+                }
+            }
+            __syncwarp();
+            if (axis == 1) {
+                // Row sums in numpy's pairwise order, the masked values staged first.
+                for (int q = 0; q < size; ++q) {
+                    for (int x = lane; x < wm; x += 32) slope[x] = c.mask(q, x) ? c.roi[q * wm + x] : 0.0;
+                    __syncwarp();
+                    if (lane == 0) prof[q] = np_pairwise_sum(slope, wm, 1);
+                    __syncwarp();
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                first = min(first, __shfl_xor_sync(0xffffffffu, first, o));
+                last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+            }
+            width[axis] = centre[axis] = dnan();
+            good[axis] = false;
+            if (last < 0) continue;  // no mask pixels: the cell has no signal either
+            const double lo = (double)first, hi = (double)last;
+            // Values and slopes on the grid; the highest value inside the span (first on ties).
+            double best = -INFINITY;
+            int best_g = 0x7fffffff;
+            for (int g = lane; g < G; g += 32) {
+                double v = 0.0, d = 0.0;
+                for (int q = 0; q < size; ++q) {
+                    const double p = prof[q];
+                    v = __fma_rn(p, vop[(long long)q * G + g], v);
+                    d = __fma_rn(p, sop[(long long)q * G + g], d);
+                }
+                slope[g] = d;
+                const double t = __dmul_rn((double)g, step);
+                if (t >= lo && t <= hi && (v > best || best_g == 0x7fffffff)) {
+                    if (v > best || best_g == 0x7fffffff) {
+                        best = v;
+                        best_g = g;
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int og = __shfl_xor_sync(0xffffffffu, best_g, o);
+                if (ob > best || (ob == best && og < best_g)) {
+                    best = ob;
+                    best_g = og;
+                }
+            }
+            __syncwarp();
+            // Steepest rise at or before the peak, steepest fall at or after it (first on ties).
+            double up = -INFINITY, down = INFINITY;
+            int up_g = 0x7fffffff, down_g = 0x7fffffff;
+            for (int g = lane; g < G; g += 32) {
+                const double t = __dmul_rn((double)g, step);
+                if (!(t >= lo && t <= hi)) continue;
+                const double d = slope[g];
+                if (g <= best_g && (d > up || up_g == 0x7fffffff)) {
+                    up = d;
+                    up_g = g;
+                }
+                if (g >= best_g && (d < down || down_g == 0x7fffffff)) {
+                    down = d;
+                    down_g = g;
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ou = __shfl_xor_sync(0xffffffffu, up, o);
+                const int oug = __shfl_xor_sync(0xffffffffu, up_g, o);
+                if (oug != 0x7fffffff && (up_g == 0x7fffffff || ou > up || (ou == up && oug < up_g))) {
+                    up = ou;
+                    up_g = oug;
+                }
+                const double od = __shfl_xor_sync(0xffffffffu, down, o);
+                const int odg = __shfl_xor_sync(0xffffffffu, down_g, o);
+                if (odg != 0x7fffffff && (down_g == 0x7fffffff || od < down || (od == down && odg < down_g))) {
+                    down = od;
+                    down_g = odg;
+                }
+            }
+            const double xl = __dmul_rn((double)up_g, step), xr = __dmul_rn((double)down_g, step);
+            width[axis] = __dsub_rn(xr, xl);
+            centre[axis] = __dmul_rn(__dadd_rn(xl, xr), 0.5);
+            good[axis] = !(xl <= lo || xr >= hi || !(up > 0.0) || !(down < 0.0));
+            __syncwarp();
+        }
+        const bool signal = peak > 0.0;
+        const bool ok = signal && good[0] && good[1];
+        const MetricRow m = out.row(i);
+        if (lane == 0) {
+            for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
+            m[M_PEAK] = peak;
+            out.status[i] = (uint8_t)(ok ? SPX_ST_OK : signal ? SPX_ST_EDGE_AT_CELL_BORDER : SPX_ST_NO_SIGNAL);
+        }
+        const double a = __dmul_rn(width[0], 0.5), b = __dmul_rn(width[1], 0.5);
+        const double cx = centre[0], cy = centre[1];
+        const int nv = n_angles + 1;
+        const double ang_step = 2.0 * kPi / n_angles;
+        for (int k = lane; k < nv; k += 32) {
+            const int q = k % n_angles;
+            double e = dnan(), x = dnan(), y = dnan();
+            if (signal) {
+                const double ang = __dmul_rn((double)q, ang_step);
+                const double co = cos(ang), si = sin(ang);
+                const double bc = __dmul_rn(b, co), as = __dmul_rn(a, si);
+                e = __ddiv_rn(__dmul_rn(a, b), sqrt(__dadd_rn(__dmul_rn(bc, bc), __dmul_rn(as, as))));
+                x = __dadd_rn(__dadd_rn(cx, __dmul_rn(e, co)), (double)c.box.x);
+                y = __dadd_rn(__dadd_rn(cy, __dmul_rn(e, si)), (double)c.box.y);
+            }
+            if (k < n_angles && out.edge_px) out.edge_px[(long long)i * n_angles + k] = e;
+            if (out.contours) {
+                out.contours[((long long)i * nv + k) * 2] = x;
+                out.contours[((long long)i * nv + k) * 2 + 1] = y;
+            }
+        }
+        if (lane == 0) {
+            const double gx_ = signal ? __dadd_rn(cx, (double)c.box.x) : dnan();
+            const double gy_ = signal ? __dadd_rn(cy, (double)c.box.y) : dnan();
+            out.centers[2LL * i] = gx_;
+            out.centers[2LL * i + 1] = gy_;
+            if (out.center_local) {
+                out.center_local[2LL * i] = signal ? cx : dnan();
+                out.center_local[2LL * i + 1] = signal ? cy : dnan();
+            }
+            if (ok) {
+                m[M_CD_X] = width[0];
+                m[M_CD_Y] = width[1];
+                m[M_AREA] = __dmul_rn(__dmul_rn(kPi, a), b);
+                const double ab = __dadd_rn(a, b);
+                m[M_CD_EQ] = ab;
+                const double r = __ddiv_rn(__dsub_rn(a, b), fmax(ab, 1e-300));
+                const double h = __dmul_rn(r, r);
+                const double h3 = __dmul_rn(3.0, h);
+                m[M_PERIM] = __dmul_rn(__dmul_rn(kPi, ab),
+                                       __dadd_rn(1.0, __ddiv_rn(h3, __dadd_rn(10.0, sqrt(__dsub_rn(4.0, h3))))));
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // The status names, as the reference's result arrays spell them (numpy "U32": 32 UCS-4 code
 // points per entry, zero-padded).
 #define SPX_STATUS_NAMES(X)                                                                            \
     X("ok") X("no_signal") X("insufficient_cell_pixels") X("insufficient_fit_pixels") X("singular_fit") \
         X("non_gaussian_fit") X("contour_outside_cell") X("incomplete_rays") X("fit_diverged")         \
-            X("center_outside_cell")
+            X("center_outside_cell") X("edge_at_cell_border")
 #define SPX_NAME_ENTRY(s) s,
-constexpr int kStatusCount = 10;
+constexpr int kStatusCount = 11;
 constexpr int kStatusChars = 32;
 __constant__ char c_status_names[kStatusCount][kStatusChars] = {SPX_STATUS_NAMES(SPX_NAME_ENTRY)};
 const char* const kStatusNamesHost[kStatusCount] = {SPX_STATUS_NAMES(SPX_NAME_ENTRY)};
@@ -1280,6 +1509,26 @@ int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, 
                                                          which, seeds, n, hm, wm, width, n_angles, fit_fraction,
                                                          method_out(out));
     return check_launch("k_logquad_cd");
+}
+
+int spx_projection_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
+                      int wm, int width, int n_angles, double step, const double* value_op_x,
+                      const double* slope_op_x, int gx, const double* value_op_y, const double* slope_op_y, int gy,
+                      const spx_method_out* out, void* stream) {
+    SPX_REQUIRE(n >= 0 && n_angles >= 1 && hm >= 1 && wm >= 1 && gx >= 1 && gy >= 1 && step > 0, "bad arguments");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(cleaned && voronoi && boxes && out && out->centers && out->status && out->metrics &&
+                    value_op_x && slope_op_x && value_op_y && slope_op_y && out->n_metrics >= 7,
+                "null pointer or too few metric columns");
+    const size_t smem = (size_t)kProjWarps * (std::max(hm, wm) + std::max(gx, gy)) * sizeof(double);
+    SPX_REQUIRE(smem <= 220 * 1024, "cell stack too large for the projection kernel");
+    if (smem > 48 * 1024) SPX_CUDA(cudaFuncSetAttribute(k_projection_cd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        (int)smem));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    k_projection_cd<<<grid_for(n, kProjWarps, 148 * 16), kProjWarps * 32, smem, s>>>(
+        cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm, wm, width, n_angles, step, value_op_x,
+        slope_op_x, gx, value_op_y, slope_op_y, gy, method_out(out));
+    return check_launch("k_projection_cd");
 }
 
 // Shared memory of one radial CTA, or 0 when it does not fit and the CTAs use global scratch.

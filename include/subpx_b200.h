@@ -49,7 +49,8 @@ enum {
     SPX_ST_CONTOUR_OUTSIDE_CELL = 6,
     SPX_ST_INCOMPLETE_RAYS = 7,
     SPX_ST_FIT_DIVERGED = 8,
-    SPX_ST_CENTER_OUTSIDE_CELL = 9
+    SPX_ST_CENTER_OUTSIDE_CELL = 9,
+    SPX_ST_EDGE_AT_CELL_BORDER = 10
 };
 
 const char* spx_last_error(void);
@@ -443,6 +444,18 @@ int spx_gaussian_method(const double* params, const uint8_t* status_in, const do
 int spx_logquad_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, const double* seeds,
                    int n, int hm, int wm, int width, int n_angles, double fit_fraction, const spx_method_out* out,
                    void* stream);
+/* The "projection" CD (subpx/_cpu/invariant_cd.py:365-421 _projection; 320-336 _set_ellipses): per
+ * reported cell the x and y profiles of the cleaned cell summed over its mask, their not-a-knot
+ * cubic splines (value_op_* / slope_op_*: size x g operators from the host, size wm for x and hm for
+ * y, evaluated at k * step for k < g), the highest value inside each profile's span and the steepest
+ * rise before / fall after it: widths cd_x, cd_y and the centre; drawn as the axis-aligned ellipse of
+ * the two widths (edge_px, contours), area pi a b, cd_equivalent a + b (a, b the half widths),
+ * Ramanujan's perimeter. Status ok, edge_at_cell_border (a rise or fall not strictly inside its span,
+ * geometry metrics NaN, ellipse still drawn) or no_signal (peak <= 0). n_metrics >= 7. */
+int spx_projection_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
+                      int wm, int width, int n_angles, double step, const double* value_op_x,
+                      const double* slope_op_x, int gx, const double* value_op_y, const double* slope_op_y, int gy,
+                      const spx_method_out* out, void* stream);
 size_t spx_radial_workspace_bytes(int hm, int wm, int smooth);
 /* Cubic-spline radial profiles; half-height crossings (halfmax) and gradient maxima (gradient).
  * Either output may be null. smooth_weights (device, 2 smooth_radius + 1 symmetric Gaussian

@@ -350,12 +350,17 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
             (c[:, 1] + reach < h - 1)
     report = np.flatnonzero(interior)
     cleaned = state.cleaned[report]
-    measured = [m for m in methods if m != "gaussian"]
+    measured = [m for m in methods if m not in ("gaussian", "projection")]
     out = measure_cells(cleaned, masks[report], origins[report], seeds[report], methods=measured, n_angles=n_angles,
                         radial_step=radial_step, fit_fraction=fit_fraction, smooth_sigma=smooth_sigma) if measured else {}
     if "gaussian" in methods:
         out["gaussian"] = gaussian_method(state.params[report], state.status[report], cleaned, masks[report],
                                           origins[report], n_angles)
+    if "projection" in methods:
+        from .invariant import projection
+
+        out["projection"] = projection(cleaned, masks[report], origins[report], n_angles)
+    out = {m: out[m] for m in methods}
     from scipy.ndimage import map_coordinates
 
     local = sign * map_coordinates(state.background_map, seeds[report].T[::-1], order=1, mode="nearest") \

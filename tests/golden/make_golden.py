@@ -265,6 +265,45 @@ def make_cd(out: Path, ref):
     np.savez_compressed(out / "cd.npz", names=np.array(names), **arrays)
 
 
+def invariant_cases():
+    cases = cd_cases()
+    stag, _ = cases["staggered"]
+    page, _ = cases["page"]
+    lat2, _ = cases["lattice2"]
+    return {
+        "staggered": (stag, dict(area_max=400, methods=("projection", "gaussian"))),
+        "page": (page, dict(area_max=400, methods=("gaussian", "projection"))),
+        "lattice2": (lat2, dict(area_max=400, methods=("projection",))),
+        "page_invert": ((65535 - page).astype(np.uint16), dict(area_max=400, invert=True, methods=("projection",))),
+        # Dense holes (pitch / FWHM 1.4): profiles whose steepest points reach the cell border.
+        "lattice14": (cases["lattice14"][0], dict(area_max=400, seeds="peaks", methods=("projection", "halfmax"))),
+    }
+
+
+def make_invariant(out: Path, ref):
+    """measure_cds with the projection method (subpx/_cpu/invariant_cd.py:365-421) beside others."""
+    from subpx import measure_cds
+
+    arrays = {}
+    names = []
+    for name, (img, kw) in invariant_cases().items():
+        res = measure_cds(img, backend="cpu", **kw)
+        arrays[f"{name}_img"] = img
+        arrays[f"{name}_kwargs"] = np.array(json.dumps(kw))
+        arrays[f"{name}_seeds"] = res.seeds_xy
+        arrays[f"{name}_methods"] = np.array(list(res.measurements))
+        for m, r in res.measurements.items():
+            arrays[f"{name}_{m}_status"] = r.status
+            arrays[f"{name}_{m}_centers"] = r.centers_xy
+            arrays[f"{name}_{m}_contours"] = r.contours_xy
+            if "edge_px" in r.geometry:
+                arrays[f"{name}_{m}_edge_px"] = r.geometry["edge_px"]
+            for metric, v in r.metrics.items():
+                arrays[f"{name}_{m}_m_{metric}"] = v
+        names.append(name)
+    np.savez_compressed(out / "invariant.npz", names=np.array(names), **arrays)
+
+
 def make_results(out: Path, ref):
     """Result folders written by the reference's own save_cd_results (full and compact) for a small
     lattice page measured by its CPU path: the file format the loader must read."""
@@ -300,7 +339,8 @@ def make_centers_model(out: Path, ref):
 
 
 MAKERS = {"thresholds": make_thresholds, "ccl": make_ccl, "centers": make_centers, "voronoi": make_voronoi,
-          "tiled": make_tiled, "cd": make_cd, "results": make_results, "centers_model": make_centers_model}
+          "tiled": make_tiled, "cd": make_cd, "results": make_results, "centers_model": make_centers_model,
+          "invariant": make_invariant}
 
 
 def main():

@@ -105,6 +105,30 @@ def test_measure_cds_oracle_matches_reference(name):
         np.testing.assert_allclose(r["contours"], z[f"{name}_{method}_contours"], rtol=0, atol=1e-9, equal_nan=True)
 
 
+# The projection CD method (subpx/_cpu/invariant_cd.py:365-421) beside others: staggered and square
+# pages, a lattice, an inverted page, and a dense peak-seeded lattice where most cells' steepest
+# points reach the cell border (edge_at_cell_border).
+@pytest.mark.parametrize("name", ["staggered", "page", "lattice2", "page_invert", "lattice14"])
+def test_projection_oracle_matches_reference(name):
+    from oracle import cd as ocd
+
+    z = _load("invariant")
+    kw = _cd_kwargs(z, name)
+    got = ocd.measure_cds(z[f"{name}_img"], **kw)
+    np.testing.assert_array_equal(got["seeds"], z[f"{name}_seeds"])
+    assert list(got["measurements"]) == [str(m) for m in z[f"{name}_methods"]]
+    for method in z[f"{name}_methods"]:
+        method = str(method)
+        r = got["measurements"][method]
+        np.testing.assert_array_equal(r["status"], z[f"{name}_{method}_status"])
+        for metric, v in r["metrics"].items():
+            np.testing.assert_array_equal(v, z[f"{name}_{method}_m_{metric}"], err_msg=f"{method} {metric}")
+        np.testing.assert_array_equal(r["centers"], z[f"{name}_{method}_centers"])
+        np.testing.assert_array_equal(r["contours"], z[f"{name}_{method}_contours"])
+        if f"{name}_{method}_edge_px" in z.files:
+            np.testing.assert_array_equal(r["edge_px"], z[f"{name}_{method}_edge_px"])
+
+
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_morphology_matches_opencv(seed):
     cv2 = pytest.importorskip("cv2")
