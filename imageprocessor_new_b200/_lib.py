@@ -22,7 +22,7 @@ REFINE_CODES = {"none": 0, "weighted": 1, "logquad": 2, "logquadratic": 2, "edge
 
 STATUS_NAMES = ("ok", "no_signal", "insufficient_cell_pixels", "insufficient_fit_pixels", "singular_fit",
                 "non_gaussian_fit", "contour_outside_cell", "incomplete_rays", "fit_diverged",
-                "center_outside_cell", "edge_at_cell_border")
+                "center_outside_cell", "edge_at_cell_border", "region_at_cell_border")
 
 _P = c_void_p
 _I = c_int
@@ -134,6 +134,8 @@ SIGNATURES = {
     "spx_gaussian_method": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _MO, _P]),
     "spx_logquad_cd": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _MO, _P]),
     "spx_projection_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _P, _P, _I, _P, _P, _I, _MO, _P]),
+    "spx_half_area_workspace_bytes": (_S, [_I, _I, _I]),
+    "spx_half_area_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _I, _D, _I, _I, _I, _MO, _MO, _P, _S, _P]),
     "spx_radial_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _P, _I, _MO, _MO, _P, _S, _P]),
     "spx_minimum_filter": (_I, [_P, _I, _I, _I, _P, _P, _P]),

@@ -26,10 +26,15 @@ METHOD_LABELS = {
     "gradient": "Maximum radial gradient",
     "halfmax": "Half-height contour",
     "projection": "x/y projection max-slope width",
+    "half_area": "Area above half height",
+    "half_area_min": "Area above half height (minimum level)",
+    "half_area_min_avg": "Area above half height (minimum level, averaged peak)",
 }
+# The half_area family: local level (median or minimum of the outermost pixels), averaged peak.
+HALF_AREA = {"half_area": ("median", False), "half_area_min": ("min", False), "half_area_min_avg": ("min", True)}
 SUPPORTED = tuple(METHOD_LABELS)
 # Methods of the reference that are outside this package (invariant, local, outline families).
-OTHER_METHODS = ("disk", "flux_ratio", "half_area", "half_area_min", "half_area_min_avg",
+OTHER_METHODS = ("disk", "flux_ratio",
                  "tail_area", "tail_area_norm", "edge_area", "foot_area", "foot_area_ratio", "local_projection",
                  "local_half_area", "local_half_area_min_avg", "local_tail_area", "outline_fit", "outline_fit_fast")
 
@@ -46,6 +51,8 @@ def _metric_names(method: str) -> tuple[str, ...]:
         return _COLS + FIT_METRICS[:-1] + ("fit_rmse",)
     if method == "projection":
         return _COLS
+    if method in HALF_AREA:
+        return _COLS + ("local_level", "threshold", "mean_signal")
     return _COLS + ("ray_coverage",)
 
 
@@ -72,6 +79,28 @@ def _projection_operators(size: int):
         slope_op = np.ascontiguousarray(spline(grid + _ZERO_PAD, 1).T)
         _PROJECTION_OPS[key] = (len(grid), dev.upload(value_op), dev.upload(slope_op))
     return _PROJECTION_OPS[key]
+
+
+_ZOOM_FACTOR = 4
+_ZOOM_OPS: dict = {}
+
+
+def _zoom_operator(size: int) -> torch.Tensor:
+    """(size * 4, size) operator of the half_area family's enlargement along one axis: column i is
+    scipy.ndimage.zoom (order 3, grid mode, zero outside) of the unit profile at i padded with 32
+    zeros either side, cut back to the profile (subpx/_cpu/invariant_cd.py:424-444). On the device."""
+    key = (int(size), torch.cuda.current_device())
+    if key not in _ZOOM_OPS:
+        from scipy.ndimage import zoom
+
+        cols = []
+        for i in range(size):
+            e = np.zeros(size + 2 * _ZERO_PAD)
+            e[_ZERO_PAD + i] = 1.0
+            z = zoom(e, _ZOOM_FACTOR, order=3, mode="grid-constant", grid_mode=True)
+            cols.append(z[_ZERO_PAD * _ZOOM_FACTOR:(_ZERO_PAD + size) * _ZOOM_FACTOR])
+        _ZOOM_OPS[key] = dev.upload(np.ascontiguousarray(np.stack(cols, axis=1)))
+    return _ZOOM_OPS[key]
 
 
 def _validate(img, *, methods, background, seeds, threshold, area_min, area_max, pad, n_angles, radial_step,
@@ -158,14 +187,18 @@ def measure_cds(
     metrics_only: bool = False,
     summary_only: bool = False,
     fit_precision: str = "fp64",
+    half_area_level: float = 0.5,
+    half_area_peak_pixels: float = 4.0,
+    outlines: bool = True,
     **other,
 ) -> CDResult | CDSummary:
     """Voronoi cells and their CDs (subpx/cd.py:44-380) on the GPU.
 
     Cells, background map, Gaussian deblending and the gaussian / logquad / gradient / halfmax
     measurements follow the reference CPU path operation for operation (FP64). Parameters of the
-    reference's other method families (``nominal_cd``, ``psf_fwhm``, ``half_area_level``, ...) are
-    accepted in ``other`` and must keep their defaults.
+    reference's other method families (``nominal_cd``, ``psf_fwhm``, ``tail_area_level``, ...) are
+    accepted in ``other`` and must keep their defaults. ``projection`` and the ``half_area`` family
+    (``half_area_level``, ``half_area_peak_pixels``, ``outlines``) follow subpx/_cpu/invariant_cd.py.
 
     ``fit_precision`` (no reference counterpart) sets the deblending LM's arithmetic: "fp64" is the
     reference's; "fp32" runs the per-pixel residuals, Jacobian and sums in FP32 (compensated J^T r
@@ -180,6 +213,12 @@ def measure_cds(
                         deblend_tolerance=deblend_tolerance, pixel_size=pixel_size, unit=unit,
                         metrics_only=metrics_only, summary_only=summary_only, peak_min_distance=peak_min_distance,
                         background_tile=background_tile, background_level=background_level)
+    if not (np.isfinite(half_area_level) and 0 < half_area_level < 1):
+        raise ValueError("half_area_level must be between 0 and 1")
+    if not (np.isfinite(half_area_peak_pixels) and half_area_peak_pixels >= 1):
+        raise ValueError("half_area_peak_pixels must be at least 1")
+    if not isinstance(outlines, (bool, np.bool_)):
+        raise ValueError("outlines must be True or False")
     from .deblend import fit_options
 
     fit_options(fit_precision)  # ValueError for an unknown arithmetic
@@ -203,7 +242,9 @@ def measure_cds(
                             deblend_iterations=int(deblend_iterations), deblend_tolerance=float(deblend_tolerance),
                             pixel_size=float(pixel_size), unit=unit, device=int(device), metrics_only=metrics_only,
                             summary_only=bool(summary_only), fit_precision=fit_precision, seeds=seeds,
-                            peak_min_distance=peak_min_distance, smooth_sigma=float(smooth_sigma))
+                            peak_min_distance=peak_min_distance, smooth_sigma=float(smooth_sigma),
+                            half_area_level=float(half_area_level), half_area_peak_pixels=float(half_area_peak_pixels),
+                            outlines=bool(outlines))
 
 
 def _segment(img_d: torch.Tensor, threshold: str, invert: bool):
@@ -234,8 +275,8 @@ def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
         "contours": (m, n_angles + 1, 2) if contours else None,
         "metrics": (max(len(names), 13), m),  # column-major: one contiguous column per metric
         "center_local": (m, 2),
-        "edge_px": (m, n_angles) if method in ("gradient", "halfmax") or (method == "projection" and contours)
-        else None,
+        "edge_px": (m, n_angles) if method in ("gradient", "halfmax") or (
+            (method == "projection" or method in HALF_AREA) and contours) else None,
         "eigenvalues": (m, 2) if method in ("logquad", "gaussian") else None,
         "axes": (m, 2, 2) if method in ("logquad", "gaussian") else None,
         "status": ((m + 7) // 8,),  # bytes, viewed as uint8
@@ -304,7 +345,7 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
         geometry = {"center_local": part("center_local"), "eigenvalues": part("eigenvalues"), "axes": part("axes")}
     elif method in ("gradient", "halfmax"):
         geometry = {"center_local": part("center_local"), "edge_px": part("edge_px")}
-    elif method == "projection":
+    elif method == "projection" or method in HALF_AREA:
         geometry = {"center_local": part("center_local"),
                     "edge_px": part("edge_px") if shapes["edge_px"] is not None else np.empty((n, 0))}
     elif not metrics_only:
@@ -383,7 +424,7 @@ def _peak_rows(img_d, sign, peak_min_distance):
 def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_angles, radial_step, fit_fraction,
                  background_level, background_tile, deblend_iterations, deblend_tolerance, pixel_size, unit, device,
                  metrics_only, summary_only, fit_precision="fp64", seeds="threshold", peak_min_distance=None,
-                 smooth_sigma=0.0):
+                 smooth_sigma=0.0, half_area_level=0.5, half_area_peak_pixels=4.0, outlines=True):
     started = time.perf_counter()
     seconds = {}
     height, width = tuple(img.shape)
@@ -577,12 +618,35 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
         bufs["projection"] = pb[0]
         launched(["projection"])
     seconds["projection"] = time.perf_counter() - t_proj
+    half = [m for m in methods if m in HALF_AREA]
+    t_half = time.perf_counter()
+    if half and nr:
+        zy, zx = _zoom_operator(c.hm), _zoom_operator(c.wm)
+        ws = dev.workspace(_lib.size("spx_half_area_workspace_bytes", c.hm, c.wm, _ZOOM_FACTOR))
+        big_px = c.hm * c.wm * _ZOOM_FACTOR * _ZOOM_FACTOR
+        n_top = min(max(1, int(round(half_area_peak_pixels * _ZOOM_FACTOR * _ZOOM_FACTOR))), big_px)
+        for kind in ("median", "min"):
+            names = [m for m in half if HALF_AREA[m][0] == kind]
+            if not names:
+                continue
+            outs = {}
+            for m in names:
+                hb_ = _method_buffers(nr, n_angles, m, not metrics_only)
+                bufs[m] = hb_[0]
+                outs[HALF_AREA[m][1]] = hb_[1]
+            _lib.call("spx_half_area_cd", cleaned.data_ptr(), c.voronoi.data_ptr(), c.boxes.data_ptr(),
+                      report_d.data_ptr(), nr, c.hm, c.wm, width, n_angles, zy.data_ptr(), zx.data_ptr(), _ZOOM_FACTOR,
+                      float(half_area_level), int(kind == "median"), n_top, int(bool(outlines) and not metrics_only),
+                      outs.get(False), outs.get(True), ws.data_ptr(), ws.numel(), stream)
+            launched(names)
+    seconds["half_area"] = time.perf_counter() - t_half
     for names, copies in pending:
         t0 = time.perf_counter()
         for name, (host, done) in zip(names, copies):
             done.synchronize()
             found[name] = _to_result(name, nr, bufs[name], host.numpy(), metrics_only, n_angles)
-        key = names[0] if names[0] in ("gaussian", "projection") else "radial"
+        key = names[0] if names[0] in ("gaussian", "projection") else "half_area" if names[0] in HALF_AREA \
+            else "radial"
         seconds[key] = seconds.get(key, 0.0) + time.perf_counter() - t0
     seconds["gaussian"] = seconds.get("gaussian", 0.0) + t_gauss
     for name in methods:
@@ -668,7 +732,7 @@ def _empty_result(method, n_angles, metrics_only) -> CDMethodResult:
         geometry = {"center_local": np.zeros((0, 2)), "eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}
     elif method in ("gradient", "halfmax"):
         geometry = {"center_local": np.zeros((0, 2)), "edge_px": np.zeros((0, n_angles))}
-    elif method == "projection":
+    elif method == "projection" or method in HALF_AREA:
         geometry = {"center_local": np.zeros((0, 2)), "edge_px": np.zeros((0, 0 if metrics_only else n_angles))}
     elif not metrics_only:
         geometry = {"eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}

@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "lm.cuh"
+#include "select.cuh"
 
 namespace spx {
 namespace {
@@ -160,6 +161,8 @@ enum {
     M_AREA = 0, M_CD_EQ = 1, M_CD_X = 2, M_CD_Y = 3, M_PERIM = 4, M_BACKGROUND = 5, M_PEAK = 6,
     // ellipse methods
     M_SIG_MAJ = 7, M_SIG_MIN = 8, M_FWHM_MAJ = 9, M_FWHM_MIN = 10, M_ANGLE = 11, M_RMSE = 12,
+    // area methods
+    M_LOCAL_LEVEL = 7, M_THRESHOLD = 8, M_MEAN_SIGNAL = 9,
     // radial methods
     M_COVERAGE = 7
 };
@@ -1421,14 +1424,528 @@ __global__ void __launch_bounds__(kProjWarps * 32) k_projection_cd(
     }
 }
 
+// ------------------------------------------------------------------------------ half_area family
+
+constexpr int kHalfThreads = 256;
+constexpr int kHalfLeavesMax = 1024;  // pairwise-sum leaves of one enlarged cell (<= 128 values each)
+constexpr int kHalfCtas = 148 * 4;    // persistent CTAs (each with its own scratch)
+
+// The leaves of numpy's pairwise sum of n values (blocks of at most 128, split at half rounded down to
+// a multiple of 8), in order: starts and lengths; returns their number.
+__device__ int np_pairwise_leaves(int start, int n, int* lo, int* len, int count) {
+    if (n <= 128) {
+        lo[count] = start;
+        len[count] = n;
+        return count + 1;
+    }
+    int n2 = n / 2;
+    n2 -= n2 % 8;
+    count = np_pairwise_leaves(start, n2, lo, len, count);
+    return np_pairwise_leaves(start + n2, n - n2, lo, len, count);
+}
+
+// The pairwise sum's tree over its leaf sums (same splits as np_pairwise_leaves).
+__device__ double np_pairwise_tree(const double* leaf, int n, int* next) {
+    if (n <= 128) return leaf[(*next)++];
+    int n2 = n / 2;
+    n2 -= n2 % 8;
+    const double a = np_pairwise_tree(leaf, n2, next);
+    return __dadd_rn(a, np_pairwise_tree(leaf, n - n2, next));
+}
+
+// One leaf of numpy's pairwise sum (n <= 128 values v(i), i = 0 .. n-1).
+template <class F>
+__device__ double np_leaf_sum(F v, int n) {
+    if (n < 8) {
+        double r = 0.0;
+        for (int i = 0; i < n; ++i) r = __dadd_rn(r, v(i));
+        return r;
+    }
+    double r[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r[j] = v(j);
+    int i = 8;
+    for (; i < n - (n % 8); i += 8)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) r[j] = __dadd_rn(r[j], v(i + j));
+    double res = __dadd_rn(__dadd_rn(__dadd_rn(r[0], r[1]), __dadd_rn(r[2], r[3])),
+                           __dadd_rn(__dadd_rn(r[4], r[5]), __dadd_rn(r[6], r[7])));
+    for (; i < n; ++i) res = __dadd_rn(res, v(i));
+    return res;
+}
+
+struct HalfArgs {
+    const double* cleaned;
+    const int* vor;
+    const int4* boxes;
+    const int* which;
+    int n, hm, wm, W, n_angles;
+    const double* zy;  // (hm * f) x hm enlargement along y
+    const double* zx;  // (wm * f) x wm along x
+    int factor;
+    double level;
+    int median;   // local level: 1 median, 0 minimum of the outermost mask pixels
+    int n_top;    // sub-pixels of the averaged peak
+    int outlines;
+    double* scratch;  // per CTA: (hm f) x wm, then (hm f) x (wm f) doubles
+    MethodOut single, averaged;  // highest-pixel peak, averaged peak (status null: not wanted)
+};
+
+struct HalfCtx {
+    const uint8_t* mask;
+    const double* big;
+    const uint32_t* bmask;
+    uint32_t* above;
+    uint32_t* reg;
+    uint32_t* reg2;
+    int* rowcnt;
+    int* colcnt;
+    double* tmp;
+    double* leafsum;
+    const int* leaf_lo;
+    const int* leaf_len;
+    int n_leaves;
+    int Hb, Wb, RW, N;
+    double b;
+    int top;
+    int* s_int;
+    double* s_dbl;
+};
+
+// One output of the half_area family from the cell's enlargement: region above b + level x peak
+// around the highest pixel, its metrics and outline (see k_half_area).
+__device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, double peak, const HalfCtx& h,
+                            const CellView& c) {
+    const int tid = threadIdx.x, Hb = h.Hb, Wb = h.Wb, RW = h.RW;
+    const double cut = __dmul_rn(a.level, peak);
+    const bool signal = peak > 0.0 && isfinite(cut) && cut < peak;
+    const uint32_t last_bits = (Wb % 32) ? ((1u << (Wb % 32)) - 1u) : 0xffffffffu;
+    for (int t = tid; t < Hb * RW; t += kHalfThreads) {
+        const int Y = t / RW, w0 = (t % RW) * 32;
+        uint32_t word = 0;
+        for (int bit = 0; bit < 32 && w0 + bit < Wb; ++bit) {
+            const int X = w0 + bit;
+            word |= (uint32_t)(((h.bmask[t] >> bit) & 1u) && h.big[(long long)Y * Wb + X] > cut) << bit;
+        }
+        h.above[t] = word;
+        h.reg[t] = 0u;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const int Y = h.top / Wb, X = h.top % Wb;
+        const uint32_t bitv = 1u << (X % 32);
+        if (h.above[Y * RW + X / 32] & bitv) h.reg[Y * RW + X / 32] = bitv;
+    }
+    __syncthreads();
+    // Grow the region from the highest pixel, one 8-neighbour ring per step, inside the above-
+    // threshold pixels, until it stops changing.
+    uint32_t* cur = h.reg;
+    uint32_t* nxt = h.reg2;
+    auto vert = [&](const uint32_t* p, int Y, int w) {
+        uint32_t v = p[Y * RW + w];
+        if (Y > 0) v |= p[(Y - 1) * RW + w];
+        if (Y < Hb - 1) v |= p[(Y + 1) * RW + w];
+        return v;
+    };
+    auto dilate = [&](const uint32_t* p, int t) {
+        const int Y = t / RW, w = t % RW;
+        const uint32_t v = vert(p, Y, w);
+        const uint32_t vp = w > 0 ? vert(p, Y, w - 1) : 0u, vn = w < RW - 1 ? vert(p, Y, w + 1) : 0u;
+        uint32_t d = v | (v << 1) | (v >> 1) | (vp >> 31) | (vn << 31);
+        if (w == RW - 1) d &= last_bits;
+        return d;
+    };
+    for (int step = 0; step < h.N; ++step) {
+        int changed = 0;
+        for (int t = tid; t < Hb * RW; t += kHalfThreads) {
+            const uint32_t nw = dilate(cur, t) & h.above[t];
+            nxt[t] = nw;
+            changed |= nw != cur[t];
+        }
+        changed = __syncthreads_or(changed);
+        uint32_t* sw = cur;
+        cur = nxt;
+        nxt = sw;
+        if (!changed) break;
+    }
+    // Counts per row and column, and whether the region reaches outside the mask or the stack's edge.
+    int touch = 0;
+    for (int t = tid; t < Hb * RW; t += kHalfThreads) {
+        const int Y = t / RW, w = t % RW;
+        const uint32_t d = dilate(cur, t);
+        const uint32_t valid = w == RW - 1 ? last_bits : 0xffffffffu;
+        touch |= (d & ~h.bmask[t] & valid) != 0u;
+        if ((Y == 0 || Y == Hb - 1) && cur[t]) touch = 1;
+        if (w == 0 && (cur[t] & 1u)) touch = 1;
+        if (w == (Wb - 1) / 32 && ((cur[t] >> ((Wb - 1) % 32)) & 1u)) touch = 1;
+    }
+    for (int Y = tid; Y < Hb; Y += kHalfThreads) {
+        int cnt = 0;
+        for (int w = 0; w < RW; ++w) cnt += __popc(cur[Y * RW + w]);
+        h.rowcnt[Y] = cnt;
+    }
+    for (int X = tid; X < Wb; X += kHalfThreads) {
+        int cnt = 0;
+        for (int Y = 0; Y < Hb; ++Y) cnt += (cur[Y * RW + X / 32] >> (X % 32)) & 1u;
+        h.colcnt[X] = cnt;
+    }
+    // Leaves of the region's brightness sum (numpy's pairwise order over the enlarged cell).
+    for (int L = tid; L < h.n_leaves; L += kHalfThreads) {
+        const int lo = h.leaf_lo[L];
+        h.leafsum[L] = np_leaf_sum(
+            [&](int q) {
+                const int t = lo + q, Y = t / Wb, X = t % Wb;
+                return ((cur[Y * RW + X / 32] >> (X % 32)) & 1u) ? h.big[t] : 0.0;
+            },
+            h.leaf_len[L]);
+    }
+    touch = __syncthreads_or(touch);
+    __shared__ long long s_count;
+    if (tid == 0) {
+        long long count = 0;
+        for (int Y = 0; Y < Hb; ++Y) count += h.rowcnt[Y];
+        s_count = count;
+        int next = 0;
+        h.s_dbl[2] = np_pairwise_tree(h.leafsum, h.N, &next);
+        for (int Y = 0; Y < Hb; ++Y) h.tmp[Y] = __dmul_rn((double)h.rowcnt[Y], (double)Y);
+        h.s_dbl[0] = np_pairwise_sum(h.tmp, Hb, 1);  // sum of row counts x row
+        for (int X = 0; X < Wb; ++X) h.tmp[X] = __dmul_rn((double)h.colcnt[X], (double)X);
+        h.s_dbl[1] = np_pairwise_sum(h.tmp, Wb, 1);
+    }
+    __syncthreads();
+    const long long count = s_count;
+    const double weight = (double)(count > 1 ? count : 1);
+    const double cy = __ddiv_rn(h.s_dbl[0], weight), cx = __ddiv_rn(h.s_dbl[1], weight);
+    const double mean_signal = __ddiv_rn(h.s_dbl[2], weight);
+    __syncthreads();
+    const double sx = 1.0 / a.factor, sy = sx;
+    if (tid == 0) {
+        for (int X = 0; X < Wb; ++X) {
+            const double d = __dsub_rn((double)X, cx);
+            h.tmp[X] = __dmul_rn((double)h.colcnt[X], __dmul_rn(d, d));
+        }
+        h.s_dbl[3] = __dmul_rn(__dmul_rn(__ddiv_rn(np_pairwise_sum(h.tmp, Wb, 1), weight), sx), sx);  // var_x
+        for (int Y = 0; Y < Hb; ++Y) {
+            const double d = __dsub_rn((double)Y, cy);
+            h.tmp[Y] = __dmul_rn((double)h.rowcnt[Y], __dmul_rn(d, d));
+        }
+        h.s_dbl[2] = __dmul_rn(__dmul_rn(__ddiv_rn(np_pairwise_sum(h.tmp, Hb, 1), weight), sy), sy);  // var_y
+    }
+    __syncthreads();
+    const double var_x = h.s_dbl[3], var_y = h.s_dbl[2];
+    const double shift = (double)(a.factor - 1) / (2.0 * a.factor);
+    const double cxl = __dsub_rn(__dmul_rn(cx, sx), shift), cyl = __dsub_rn(__dmul_rn(cy, sy), shift);
+    const bool ok = signal && !touch;
+    // Display outline: along each ray from the centroid, the last 1/8 px step still in the region.
+    const int nv = a.n_angles + 1;
+    double* vx = h.tmp;
+    double* vy = h.tmp + nv;
+    if (a.outlines && signal) {
+        const int nr = (int)ceil(hypot((double)a.hm, (double)a.wm) / 0.125);
+        const double ang_step = 2.0 * kPi / a.n_angles;
+        for (int q = tid; q < a.n_angles; q += kHalfThreads) {
+            const double ang = __dmul_rn((double)q, ang_step);
+            const double co = cos(ang), si = sin(ang);
+            int first_out = nr;
+            for (int s = 0; s < nr; ++s) {
+                const double st = __dmul_rn((double)s, 0.125);
+                const double fx = rint(__dadd_rn(cx, __ddiv_rn(__dmul_rn(co, st), sx)));
+                const double fy = rint(__dadd_rn(cy, __ddiv_rn(__dmul_rn(si, st), sy)));
+                bool hit = fx >= 0.0 && fx < (double)Wb && fy >= 0.0 && fy < (double)Hb;
+                if (hit) {
+                    const int X = (int)fx, Y = (int)fy;
+                    hit = (cur[Y * RW + X / 32] >> (X % 32)) & 1u;
+                }
+                if (!hit) {
+                    first_out = s;
+                    break;
+                }
+            }
+            const double e = __dadd_rn(__dmul_rn((double)max(first_out - 1, 0), 0.125), 0.0625);
+            if (out.edge_px) out.edge_px[(long long)i * a.n_angles + q] = e;
+            vx[q] = __dadd_rn(__dadd_rn(cxl, __dmul_rn(e, co)), (double)c.box.x);
+            vy[q] = __dadd_rn(__dadd_rn(cyl, __dmul_rn(e, si)), (double)c.box.y);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            vx[a.n_angles] = vx[0];
+            vy[a.n_angles] = vy[0];
+        }
+        __syncthreads();
+        if (out.contours)
+            for (int k = tid; k < nv; k += kHalfThreads) {
+                out.contours[((long long)i * nv + k) * 2] = vx[k];
+                out.contours[((long long)i * nv + k) * 2 + 1] = vy[k];
+            }
+    } else {
+        if (out.edge_px)
+            for (int q = tid; q < a.n_angles; q += kHalfThreads) out.edge_px[(long long)i * a.n_angles + q] = dnan();
+        if (out.contours)
+            for (int k = tid; k < 2 * nv; k += kHalfThreads) out.contours[(long long)i * 2 * nv + k] = dnan();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const MetricRow m = out.row(i);
+        for (int q = 0; q < out.n_metrics; ++q) m[q] = dnan();
+        m[M_LOCAL_LEVEL] = h.b;
+        out.status[i] = (uint8_t)(!signal ? SPX_ST_NO_SIGNAL : touch ? SPX_ST_REGION_AT_CELL_BORDER : SPX_ST_OK);
+        const double nan = dnan();
+        out.centers[2LL * i] = signal ? __dadd_rn(cxl, (double)c.box.x) : nan;
+        out.centers[2LL * i + 1] = signal ? __dadd_rn(cyl, (double)c.box.y) : nan;
+        if (out.center_local) {
+            out.center_local[2LL * i] = signal ? cxl : nan;
+            out.center_local[2LL * i + 1] = signal ? cyl : nan;
+        }
+        if (signal) {
+            m[M_PEAK] = peak;
+            m[M_THRESHOLD] = __dadd_rn(h.b, cut);
+            m[M_MEAN_SIGNAL] = mean_signal;
+        }
+        if (ok) {
+            const double area = __dmul_rn((double)count, __dmul_rn(sx, sy));
+            const double cd_eq = __dmul_rn(2.0, sqrt(__ddiv_rn(area, kPi)));
+            const double ratio = sqrt(sqrt(__ddiv_rn(fmax(var_x, 1e-12), fmax(var_y, 1e-12))));
+            m[M_AREA] = area;
+            m[M_CD_EQ] = cd_eq;
+            m[M_CD_X] = __dmul_rn(cd_eq, ratio);
+            m[M_CD_Y] = __ddiv_rn(cd_eq, ratio);
+            if (a.outlines) {
+                for (int q = 0; q < a.n_angles; ++q) {
+                    const double dx = __dsub_rn(vx[q + 1], vx[q]), dy = __dsub_rn(vy[q + 1], vy[q]);
+                    h.tmp[2 * nv + q] = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+                }
+                m[M_PERIM] = np_pairwise_sum(h.tmp + 2 * nv, a.n_angles, 1);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// The half_area family (subpx/_cpu/invariant_cd.py:551-799 with 802-875 for the level backgrounds):
+// one CTA per cell. Local level b = median or minimum of the outermost mask pixels; the cell minus b
+// (zero outside its mask) enlarged f times by the host's cubic zoom operators (Zy C Zx^T, FMA chains in
+// the order of the inner index); peak = the highest enlarged pixel of the mask (or the mean of the
+// n_top highest); threshold b + level x peak; the region = the 8-connected above-threshold pixels that
+// hold the highest pixel (grown one ring per step over bit rows); area, centroid, x / y spreads (sums in
+// numpy's pairwise order), the equal-area ellipse's diameters, and the display outline (the region's
+// last pixel along each ray from the centroid, 1/8 px steps). Status no_signal / region_at_cell_border
+// (the region reaches the mask's edge or the stack's) / ok.
+__global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
+    extern __shared__ double hsm[];
+    __shared__ int hist[2048];
+    __shared__ int warp_tot[32], s_pick[3];
+    __shared__ unsigned long long s_keys[2];
+    __shared__ double s_red[2 * (kHalfThreads / 32)];
+    __shared__ int s_ired[kHalfThreads / 32];
+    __shared__ int s_int[4];
+    __shared__ double s_dbl[4];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int hm = a.hm, wm = a.wm, f = a.factor;
+    const int Hb = hm * f, Wb = wm * f, RW = (Wb + 31) / 32, N = Hb * Wb, area_px = hm * wm;
+    // Shared layout: cell values, ring values, leaf sums, small arrays (doubles); bit planes, counts,
+    // leaves (ints); mask bytes.
+    double* cell = hsm;
+    double* ring = cell + area_px;
+    double* leafsum = ring + area_px;
+    const int tmpn = max(max(Hb, Wb), 3 * (a.n_angles + 1));
+    double* tmp = leafsum + kHalfLeavesMax;
+    uint32_t* bmask = reinterpret_cast<uint32_t*>(tmp + tmpn);
+    uint32_t* above = bmask + Hb * RW;
+    uint32_t* reg = above + Hb * RW;
+    uint32_t* reg2 = reg + Hb * RW;
+    int* rowcnt = reinterpret_cast<int*>(reg2 + Hb * RW);
+    int* colcnt = rowcnt + Hb;
+    int* leaf_lo = colcnt + Wb;
+    int* leaf_len = leaf_lo + kHalfLeavesMax;
+    uint8_t* mask = reinterpret_cast<uint8_t*>(leaf_len + kHalfLeavesMax);
+    double* T = a.scratch + (long long)blockIdx.x * ((long long)Hb * wm + (long long)N);
+    double* big = T + (long long)Hb * wm;
+    const double sx = 1.0 / f, sy = 1.0 / f;
+    const double shift = (double)(f - 1) / (2.0 * f);
+    if (tid == 0) s_int[3] = np_pairwise_leaves(0, N, leaf_lo, leaf_len, 0);
+    __syncthreads();
+    const int n_leaves = s_int[3];
+    for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
+        const int j = a.which ? a.which[i] : i;
+        const CellView c{a.cleaned + (long long)i * area_px, a.vor, a.boxes[j], j, a.W, hm, wm};
+        __syncthreads();  // the previous cell's shared-memory reads are done
+        if (tid == 0) s_int[0] = 0;
+        for (int k = tid; k < area_px; k += kHalfThreads) {
+            const bool m = c.mask(k / wm, k % wm);
+            mask[k] = m;
+            cell[k] = m ? c.roi[k] : 0.0;
+        }
+        __syncthreads();
+        // Outermost mask pixels: a 4-neighbour outside the mask, or on the stack's edge.
+        double lmin = INFINITY;
+        for (int k = tid; k < area_px; k += kHalfThreads) {
+            const int y = k / wm, x = k % wm;
+            if (!mask[k]) continue;
+            const bool inner = y > 0 && x > 0 && y < hm - 1 && x < wm - 1 && mask[k - wm] && mask[k + wm] &&
+                               mask[k - 1] && mask[k + 1];
+            if (!inner) {
+                ring[atomicAdd(&s_int[0], 1)] = cell[k];
+                lmin = fmin(lmin, cell[k]);
+            }
+        }
+        lmin = warp_min(lmin);
+        if (lane == 0) s_red[warp] = lmin;
+        __syncthreads();
+        const int r = s_int[0];
+        double b;
+        if (a.median) {
+            // nanmedian: the middle value(s) by rank (ties ranked by position), their mean; NaN if none.
+            const int k1 = (r - 1) / 2, k2 = r / 2;
+            for (int t = tid; t < r; t += kHalfThreads) {
+                const double v = ring[t];
+                int rank = 0;
+                for (int q = 0; q < r; ++q) rank += ring[q] < v || (ring[q] == v && q < t);
+                if (rank == k1) s_dbl[0] = v;
+                if (rank == k2) s_dbl[1] = v;
+            }
+            __syncthreads();
+            b = r ? __ddiv_rn(__dadd_rn(s_dbl[0], s_dbl[1]), 2.0) : dnan();
+        } else {
+            b = s_red[0];
+            for (int q = 1; q < kHalfThreads / 32; ++q) b = fmin(b, s_red[q]);
+        }
+        __syncthreads();
+        for (int k = tid; k < area_px; k += kHalfThreads) cell[k] = mask[k] ? __dsub_rn(cell[k], b) : 0.0;
+        __syncthreads();
+        // Enlargement: T = Zy C (Hb x wm), then big = T Zx^T (Hb x Wb).
+        for (int t = tid; t < Hb * wm; t += kHalfThreads) {
+            const int Y = t / wm, x = t % wm;
+            double v = 0.0;
+            for (int y = 0; y < hm; ++y) v = __fma_rn(a.zy[(long long)Y * hm + y], cell[y * wm + x], v);
+            T[t] = v;
+        }
+        __syncthreads();
+        for (int t = tid; t < N; t += kHalfThreads) {
+            const int Y = t / Wb, X = t % Wb;
+            double v = 0.0;
+            for (int x = 0; x < wm; ++x) v = __fma_rn(T[(long long)Y * wm + x], a.zx[(long long)X * wm + x], v);
+            big[t] = v;
+        }
+        // Bit plane of the enlarged mask (each sub-pixel copies its pixel).
+        for (int t = tid; t < Hb * RW; t += kHalfThreads) {
+            const int Y = t / RW, w0 = (t % RW) * 32;
+            uint32_t word = 0;
+            for (int bit = 0; bit < 32 && w0 + bit < Wb; ++bit)
+                word |= (uint32_t)mask[(Y / f) * wm + (w0 + bit) / f] << bit;
+            bmask[t] = word;
+        }
+        __syncthreads();
+        // Highest enlarged pixel of the mask (first in row-major order on ties; index 0 when none).
+        double best = -INFINITY;
+        int best_i = 0x7fffffff;
+        unsigned long long kmin = ~0ull, kmax = 0;
+        for (int t = tid; t < N; t += kHalfThreads) {
+            const bool in = (bmask[(t / Wb) * RW + (t % Wb) / 32] >> ((t % Wb) % 32)) & 1u;
+            const double v = in ? big[t] : -INFINITY;
+            if (v > best || best_i == 0x7fffffff) {
+                if (v > best || best_i == 0x7fffffff) {
+                    best = v;
+                    best_i = t;
+                }
+            }
+            const unsigned long long key = order_key(v);
+            kmin = min(kmin, key);
+            kmax = max(kmax, key);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oi = __shfl_xor_sync(0xffffffffu, best_i, o);
+            if (ob > best || (ob == best && oi < best_i)) {
+                best = ob;
+                best_i = oi;
+            }
+        }
+        kmin = warp_min_u64(kmin);
+        kmax = warp_max_u64(kmax);
+        if (lane == 0) {
+            s_red[warp] = best;
+            s_ired[warp] = best_i;
+            s_red[kHalfThreads / 32 + warp] = 0.0;
+            hist[warp] = 0;  // (overwritten by the select below)
+        }
+        __shared__ unsigned long long s_kmin, s_kmax;
+        if (tid == 0) {
+            s_kmin = ~0ull;
+            s_kmax = 0;
+        }
+        __syncthreads();
+        if (lane == 0) {
+            atomicMin(&s_kmin, kmin);
+            atomicMax(&s_kmax, kmax);
+        }
+        __syncthreads();
+        double top_v = s_red[0];
+        int top = s_ired[0];
+        for (int q = 1; q < kHalfThreads / 32; ++q)
+            if (s_red[q] > top_v || (s_red[q] == top_v && s_ired[q] < top)) {
+                top_v = s_red[q];
+                top = s_ired[q];
+            }
+        if (top == 0x7fffffff) top = 0;
+        __syncthreads();
+        HalfCtx ctx{mask, big, bmask, above, reg, reg2, rowcnt, colcnt, tmp, leafsum, leaf_lo, leaf_len, n_leaves,
+                    Hb, Wb, RW, N, b, top, s_int, s_dbl};
+        if (a.single.status) half_output(a, a.single, i, top_v, ctx, c);
+        if (a.averaged.status) {
+            // Mean of the n_top highest enlarged pixels (outside the mask -inf): the n_top-th highest key
+            // by the CTA select, then the keys above it and as many copies of it as are missing.
+            double peak = -1.0;
+            if (a.n_top <= N) {
+                auto for_keys = [&](auto&& fn) {
+                    for (int t = tid; t < N; t += kHalfThreads) {
+                        const bool in = (bmask[(t / Wb) * RW + (t % Wb) / 32] >> ((t % Wb) % 32)) & 1u;
+                        fn(order_key(in ? big[t] : -INFINITY));
+                    }
+                };
+                unsigned long long kth, kth2;
+                cta_select<kHalfThreads>(for_keys, N - a.n_top, false, s_kmin, s_kmax, hist, warp_tot, s_pick,
+                                         s_keys, &kth, &kth2);
+                double sum = 0.0;
+                int cnt = 0;
+                for_keys([&](unsigned long long key) {
+                    if (key > kth) {
+                        sum += key_value(key);
+                        ++cnt;
+                    }
+                });
+                sum = warp_sum(sum);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+                if (lane == 0) {
+                    s_red[warp] = sum;
+                    s_ired[warp] = cnt;
+                }
+                __syncthreads();
+                double total = 0.0;
+                int above_cnt = 0;
+                for (int q = 0; q < kHalfThreads / 32; ++q) {
+                    total += s_red[q];
+                    above_cnt += s_ired[q];
+                }
+                total += (double)(a.n_top - above_cnt) * key_value(kth);
+                const double mean = total / a.n_top;
+                peak = isfinite(mean) ? mean : -1.0;
+                __syncthreads();
+            }
+            half_output(a, a.averaged, i, peak, ctx, c);
+        }
+    }
+}
+
 // The status names, as the reference's result arrays spell them (numpy "U32": 32 UCS-4 code
 // points per entry, zero-padded).
 #define SPX_STATUS_NAMES(X)                                                                            \
     X("ok") X("no_signal") X("insufficient_cell_pixels") X("insufficient_fit_pixels") X("singular_fit") \
         X("non_gaussian_fit") X("contour_outside_cell") X("incomplete_rays") X("fit_diverged")         \
-            X("center_outside_cell") X("edge_at_cell_border")
+            X("center_outside_cell") X("edge_at_cell_border") X("region_at_cell_border")
 #define SPX_NAME_ENTRY(s) s,
-constexpr int kStatusCount = 11;
+constexpr int kStatusCount = 12;
 constexpr int kStatusChars = 32;
 __constant__ char c_status_names[kStatusCount][kStatusChars] = {SPX_STATUS_NAMES(SPX_NAME_ENTRY)};
 const char* const kStatusNamesHost[kStatusCount] = {SPX_STATUS_NAMES(SPX_NAME_ENTRY)};
@@ -1529,6 +2046,46 @@ int spx_projection_cd(const double* cleaned, const int* voronoi, const int* boxe
         cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm, wm, width, n_angles, step, value_op_x,
         slope_op_x, gx, value_op_y, slope_op_y, gy, method_out(out));
     return check_launch("k_projection_cd");
+}
+
+// Shared memory of one half-area CTA (see the layout in k_half_area).
+static size_t half_smem(int hm, int wm, int f, int n_angles) {
+    const size_t Hb = (size_t)hm * f, Wb = (size_t)wm * f, RW = (Wb + 31) / 32, area = (size_t)hm * wm;
+    const size_t tmpn = std::max(std::max(Hb, Wb), (size_t)3 * (n_angles + 1));
+    return (2 * area + kHalfLeavesMax + tmpn) * sizeof(double) + 4 * Hb * RW * sizeof(uint32_t) +
+           (Hb + Wb + 2 * kHalfLeavesMax) * sizeof(int) + area;
+}
+
+size_t spx_half_area_workspace_bytes(int hm, int wm, int factor) {
+    const size_t Hb = (size_t)hm * factor, Wb = (size_t)wm * factor;
+    return (size_t)kHalfCtas * (Hb * wm + Hb * Wb) * sizeof(double) + 256;
+}
+
+int spx_half_area_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
+                     int wm, int width, int n_angles, const double* zoom_y, const double* zoom_x, int factor,
+                     double level, int median, int n_top, int outlines, const spx_method_out* single,
+                     const spx_method_out* averaged, void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(n >= 0 && n_angles >= 1 && hm >= 1 && wm >= 1 && factor >= 1 && n_top >= 1, "bad arguments");
+    SPX_REQUIRE(level > 0.0 && level < 1.0, "level must be between 0 and 1");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(cleaned && voronoi && boxes && zoom_y && zoom_x && workspace && (single || averaged), "null pointer");
+    for (const spx_method_out* o : {single, averaged})
+        if (o) SPX_REQUIRE(o->centers && o->status && o->metrics && o->n_metrics >= 10, "null pointer or too few metric columns");
+    // Up to 32768 sub-pixels: numpy's pairwise-sum leaves (at least 57 values each) then fit kHalfLeavesMax.
+    SPX_REQUIRE((long long)hm * factor * wm * factor <= 32768, "cell stack too large for the half-area kernel");
+    SPX_REQUIRE(workspace_bytes >= spx_half_area_workspace_bytes(hm, wm, factor), "workspace too small");
+    const size_t smem = half_smem(hm, wm, factor, n_angles);
+    SPX_REQUIRE(smem <= 200 * 1024, "cell stack too large for the half-area kernel");
+    if (smem > 48 * 1024)
+        SPX_CUDA(cudaFuncSetAttribute(k_half_area, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const uintptr_t base = (reinterpret_cast<uintptr_t>(workspace) + 255) & ~(uintptr_t)255;
+    HalfArgs a{cleaned, voronoi, reinterpret_cast<const int4*>(boxes), which, n, hm, wm, width, n_angles, zoom_y,
+               zoom_x, factor, level, median, n_top, outlines, reinterpret_cast<double*>(base), method_out(single),
+               method_out(averaged)};
+    if (!single) a.single.status = nullptr;
+    if (!averaged) a.averaged.status = nullptr;
+    k_half_area<<<std::min(n, kHalfCtas), kHalfThreads, smem, static_cast<cudaStream_t>(stream)>>>(a);
+    return check_launch("k_half_area");
 }
 
 // Shared memory of one radial CTA, or 0 when it does not fit and the CTAs use global scratch.

@@ -50,7 +50,8 @@ enum {
     SPX_ST_INCOMPLETE_RAYS = 7,
     SPX_ST_FIT_DIVERGED = 8,
     SPX_ST_CENTER_OUTSIDE_CELL = 9,
-    SPX_ST_EDGE_AT_CELL_BORDER = 10
+    SPX_ST_EDGE_AT_CELL_BORDER = 10,
+    SPX_ST_REGION_AT_CELL_BORDER = 11
 };
 
 const char* spx_last_error(void);
@@ -456,6 +457,24 @@ int spx_projection_cd(const double* cleaned, const int* voronoi, const int* boxe
                       int wm, int width, int n_angles, double step, const double* value_op_x,
                       const double* slope_op_x, int gx, const double* value_op_y, const double* slope_op_y, int gy,
                       const spx_method_out* out, void* stream);
+
+/* The half_area family (subpx/_cpu/invariant_cd.py:551-799, 802-875): half_area (median local level,
+ * highest-pixel peak), half_area_min (minimum level) and half_area_min_avg (minimum level, peak =
+ * mean of the n_top highest sub-pixels). Per reported cell the local level b (median = 1: median,
+ * else minimum of the mask pixels with a 4-neighbour outside the mask or on the stack's edge), the
+ * cell minus b enlarged factor times by zoom_y ((hm factor) x hm) and zoom_x ((wm factor) x wm),
+ * the host's cubic zoom operators; the region = the 8-connected sub-pixels above b + level x peak
+ * around the highest one; area, centroid, the equal-area ellipse's x / y diameters (cd_x, cd_y),
+ * metrics local_level, threshold, mean_signal (columns 7-9; n_metrics >= 10) and, with outlines, the
+ * display outline (edge_px, contours, perimeter). `single` gets the highest-pixel peak, `averaged`
+ * the averaged one (either may be null; both share one enlargement). Status ok,
+ * region_at_cell_border or no_signal. (hm factor) x (wm factor) <= 32768; workspace:
+ * spx_half_area_workspace_bytes. */
+size_t spx_half_area_workspace_bytes(int hm, int wm, int factor);
+int spx_half_area_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
+                     int wm, int width, int n_angles, const double* zoom_y, const double* zoom_x, int factor,
+                     double level, int median, int n_top, int outlines, const spx_method_out* single,
+                     const spx_method_out* averaged, void* workspace, size_t workspace_bytes, void* stream);
 size_t spx_radial_workspace_bytes(int hm, int wm, int smooth);
 /* Cubic-spline radial profiles; half-height crossings (halfmax) and gradient maxima (gradient).
  * Either output may be null. smooth_weights (device, 2 smooth_radius + 1 symmetric Gaussian

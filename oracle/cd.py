@@ -350,7 +350,9 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
             (c[:, 1] + reach < h - 1)
     report = np.flatnonzero(interior)
     cleaned = state.cleaned[report]
-    measured = [m for m in methods if m not in ("gaussian", "projection")]
+    from .invariant import HALF_AREA
+
+    measured = [m for m in methods if m not in ("gaussian", "projection") and m not in HALF_AREA]
     out = measure_cells(cleaned, masks[report], origins[report], seeds[report], methods=measured, n_angles=n_angles,
                         radial_step=radial_step, fit_fraction=fit_fraction, smooth_sigma=smooth_sigma) if measured else {}
     if "gaussian" in methods:
@@ -360,6 +362,11 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
         from .invariant import projection
 
         out["projection"] = projection(cleaned, masks[report], origins[report], n_angles)
+    half = [m for m in methods if m in HALF_AREA]
+    if half:
+        from .invariant import half_areas
+
+        out.update(half_areas(cleaned, masks[report], origins[report], n_angles, half))
     out = {m: out[m] for m in methods}
     from scipy.ndimage import map_coordinates
 

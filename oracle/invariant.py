@@ -95,3 +95,182 @@ def projection(cleaned, masks, origins, n_angles=128, step=0.02):
     for name in ("area_px2", "cd_equivalent_px", "cd_x_px", "cd_y_px", "perimeter_px"):
         out["metrics"][name][~ok] = np.nan
     return out
+
+
+# ---------------------------------------------------------------------------- the half_area family
+# subpx/_cpu/invariant_cd.py: _zoom_operators 424-444, _nearest_pixels 447-456, _grow 459-467,
+# _connected_to_top 470-490 (the 8-connected part of the above-threshold pixels that holds the top
+# pixel), _top_mean 493-499, _half_areas 551-799 on the CPU (one size bucket, chunks of
+# 4096 * 196 // (h * w) cells), _regions_by_arrays 802-875 for the level backgrounds.
+
+HALF_AREA = {"half_area": ("median", False), "half_area_min": ("min", False), "half_area_min_avg": ("min", True)}
+HALF_NAMES = NAMES + ("local_level", "threshold", "mean_signal")
+FACTOR = 4
+
+
+@lru_cache(maxsize=16)
+def zoom_operator(size: int, factor: int = FACTOR) -> np.ndarray:
+    """(size * factor, size): column i is scipy.ndimage.zoom (order 3, grid mode, zero outside) of
+    the unit profile at i, padded with 32 zeros either side, cut back to the profile's extent."""
+    from scipy.ndimage import zoom
+
+    cols = []
+    for i in range(size):
+        e = np.zeros(size + 2 * ZERO_PAD)
+        e[ZERO_PAD + i] = 1.0
+        z = zoom(e, factor, order=3, mode="grid-constant", grid_mode=True)
+        cols.append(z[ZERO_PAD * factor:(ZERO_PAD + size) * factor])
+    return np.stack(cols, axis=1)
+
+
+def _grow8(region):
+    """Dilation of a batch of boolean images by one pixel in the 8 directions."""
+    rows = region.copy()
+    rows[:, 1:] |= region[:, :-1]
+    rows[:, :-1] |= region[:, 1:]
+    out = rows.copy()
+    out[:, :, 1:] |= rows[:, :, :-1]
+    out[:, :, :-1] |= rows[:, :, 1:]
+    return out
+
+
+def _component_of(above, top):
+    """Per image, the 8-connected component of `above` holding its pixel `top` (flat index)."""
+    from scipy.ndimage import label
+
+    k, h, w = above.shape
+    out = np.zeros_like(above)
+    for i in range(k):
+        y, x = divmod(int(top[i]), w)
+        if above[i, y, x]:
+            lab, _ = label(above[i], structure=np.ones((3, 3), bool))
+            out[i] = lab == lab[y, x]
+    return out
+
+
+def _ring_level(mask, cell, kind):
+    """Local level: median or minimum of each cell's outermost mask pixels (mask pixels with a
+    4-neighbour outside the mask or on the stack's edge)."""
+    k = len(mask)
+    inner = mask.copy()
+    inner[:, 1:] &= mask[:, :-1]
+    inner[:, :-1] &= mask[:, 1:]
+    inner[:, :, 1:] &= mask[:, :, :-1]
+    inner[:, :, :-1] &= mask[:, :, 1:]
+    inner[:, [0, -1]] = False
+    inner[:, :, [0, -1]] = False
+    ring = mask & ~inner
+    if kind == "median":
+        import warnings
+
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)  # all-NaN rows: no ring
+            return np.nanmedian(np.where(ring, cell, np.nan).reshape(k, -1), axis=1)
+    return np.where(ring, cell, np.inf).reshape(k, -1).min(axis=1)
+
+
+def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, level=0.5, peak_pixels=4.0,
+               outlines=True):
+    """The half_area family on an (n, h, w) stack of neighbour-removed cells: for each name of
+    `names` the oracle's measurement dict with the reference's metrics (local_level, threshold,
+    mean_signal beside the geometry)."""
+    cleaned = np.asarray(cleaned, dtype=np.float64)
+    masks = np.asarray(masks, dtype=bool)
+    origins = np.asarray(origins, dtype=np.float64).reshape(-1, 2)
+    n, h, w = masks.shape
+    sy = sx = 1.0 / FACTOR
+    shift = (FACTOR - 1) / (2 * FACTOR)
+    zy, zx = zoom_operator(h), zoom_operator(w)
+    H, W = zy.shape[0], zx.shape[0]
+    iy, ix = np.arange(h).repeat(FACTOR), np.arange(w).repeat(FACTOR)
+    gy, gx = np.arange(H, dtype=float), np.arange(W, dtype=float)
+    angles = np.arange(n_angles) * (2 * np.pi / n_angles)
+    radii = np.arange(0.0, float(np.hypot(h, w)), 0.125)
+    cos_a, sin_a = np.cos(angles), np.sin(angles)
+    out = {}
+    for name in names:
+        out[name] = {"centers": np.full((n, 2), np.nan), "center_local": np.full((n, 2), np.nan),
+                     "contours": np.full((n, n_angles + 1, 2), np.nan), "edge_px": np.full((n, n_angles), np.nan),
+                     "status": np.full(n, "no_signal", dtype="U32"),
+                     "metrics": {k: np.full(n, np.nan) for k in HALF_NAMES}}
+    chunk = max(1, 4096 * 196 // (h * w))
+    for start in range(0, n, chunk):
+        rows = np.arange(start, min(n, start + chunk))
+        k = len(rows)
+        mask = masks[rows]
+        cell = np.where(mask, cleaned[rows], 0.0)
+        big_mask = mask[:, iy][:, :, ix]
+        levels, bigs = {}, {}
+        for name in names:
+            kind, averaged = HALF_AREA[name]
+            if kind not in levels:
+                b = _ring_level(mask, cell, kind)
+                levels[kind] = b
+                centered = np.where(mask, cell - b[:, None, None], 0.0)
+                bigs[kind] = zy[None] @ centered @ zx.T[None]
+            b, big = levels[kind], bigs[kind]
+            flat = np.where(big_mask, big, -np.inf).reshape(k, -1)
+            top = np.argmax(flat, axis=1)
+            peak = flat[np.arange(k), top]
+            if averaged:
+                n_top = min(max(1, int(round(peak_pixels * FACTOR * FACTOR))), H * W)
+                peak = np.partition(flat, -n_top, axis=1)[:, -n_top:].mean(axis=1)
+                peak = np.where(np.isfinite(peak), peak, -1.0)
+            cut = level * peak
+            above = big_mask & (big > cut[:, None, None])
+            region = _component_of(above, top)
+            count = region.sum(axis=(1, 2))
+            touches = ((_grow8(region) & ~big_mask).any(axis=(1, 2)) | region[:, [0, -1]].any(axis=(1, 2))
+                       | region[:, :, [0, -1]].any(axis=(1, 2)))
+            weight = np.maximum(count, 1)
+            mean_signal = np.where(region, big, 0.0).sum(axis=(1, 2)) / weight
+            cy = (region.sum(axis=2) * gy).sum(axis=1) / weight
+            cx = (region.sum(axis=1) * gx).sum(axis=1) / weight
+            var_x = (region.sum(axis=1) * (gx[None] - cx[:, None]) ** 2).sum(axis=1) / weight * sx * sx
+            var_y = (region.sum(axis=2) * (gy[None] - cy[:, None]) ** 2).sum(axis=1) / weight * sy * sy
+            cd_eq = 2 * np.sqrt(count * (sx * sy) / np.pi)
+            ratio = np.sqrt(np.sqrt(np.maximum(var_x, 1e-12) / np.maximum(var_y, 1e-12)))
+            o = out[name]
+            signal = (peak > 0) & np.isfinite(cut) & (cut < peak)
+            m = o["metrics"]
+            m["local_level"][rows] = b
+            m["peak_signal"][rows] = np.where(signal, peak, np.nan)
+            m["threshold"][rows] = np.where(signal, b + cut, np.nan)
+            m["mean_signal"][rows] = np.where(signal, mean_signal, np.nan)
+            m["area_px2"][rows] = np.where(signal, count * (sx * sy), np.nan)
+            m["cd_x_px"][rows] = np.where(signal, cd_eq * ratio, np.nan)
+            m["cd_y_px"][rows] = np.where(signal, cd_eq / ratio, np.nan)
+            o["status"][rows] = np.where(~signal, "no_signal", np.where(touches, "region_at_cell_border", "ok"))
+            o["center_local"][rows] = np.column_stack((cx * sx - shift, cy * sy - shift))
+            if outlines:
+                # The region's last pixel along each ray from its centroid, in 1/8 px steps.
+                far = ((gx[None, None] - cx[:, None, None]) * sx) ** 2 + ((gy[None, :, None] - cy[:, None, None]) * sy) ** 2
+                reach = float(np.sqrt(np.where(region, far, 0.0).max())) if k else 0.0
+                steps = radii[:min(len(radii), int(reach / 0.125) + 3)]
+                px = np.rint(cx[:, None, None] + cos_a[None, :, None] * steps[None, None] / sx).astype(np.int64)
+                py = np.rint(cy[:, None, None] + sin_a[None, :, None] * steps[None, None] / sy).astype(np.int64)
+                inside = (px >= 0) & (px < W) & (py >= 0) & (py < H)
+                index = (np.clip(py, 0, H - 1) * W + np.clip(px, 0, W - 1)).reshape(k, -1)
+                hit = np.take_along_axis(region.reshape(k, -1), index, axis=1).reshape(px.shape) & inside
+                first_out = np.where(hit.all(axis=2), len(steps), np.argmin(hit, axis=2))
+                o["edge_px"][rows] = steps[np.maximum(first_out - 1, 0)] + 0.0625
+    for name in names:
+        o = out[name]
+        m = o["metrics"]
+        m["cd_equivalent_px"][:] = 2 * np.sqrt(m["area_px2"] / np.pi)
+        rows = np.flatnonzero(o["status"] != "no_signal")
+        o["center_local"][o["status"] == "no_signal"] = np.nan
+        o["centers"][rows] = o["center_local"][rows] + origins[rows]
+        if outlines:
+            o["edge_px"][o["status"] == "no_signal"] = np.nan
+            c = o["center_local"][rows]
+            dirs = np.column_stack((cos_a, sin_a))
+            pts = c[:, None, :] + o["edge_px"][rows][:, :, None] * dirs[None]
+            o["contours"][rows] = np.concatenate((pts, pts[:, :1]), axis=1) + origins[rows][:, None, :]
+            m["perimeter_px"][rows] = np.linalg.norm(np.diff(o["contours"][rows], axis=1), axis=2).sum(axis=1)
+        else:
+            o["edge_px"][:] = np.nan
+        ok = o["status"] == "ok"
+        for metric in ("area_px2", "cd_equivalent_px", "cd_x_px", "cd_y_px", "perimeter_px"):
+            m[metric][~ok] = np.nan
+    return out

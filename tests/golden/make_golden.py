@@ -277,6 +277,12 @@ def invariant_cases():
         "page_invert": ((65535 - page).astype(np.uint16), dict(area_max=400, invert=True, methods=("projection",))),
         # Dense holes (pitch / FWHM 1.4): profiles whose steepest points reach the cell border.
         "lattice14": (cases["lattice14"][0], dict(area_max=400, seeds="peaks", methods=("projection", "halfmax"))),
+        # The half_area family: median and minimum local levels, the averaged peak.
+        "staggered_half": (stag, dict(area_max=400, methods=("half_area", "half_area_min", "half_area_min_avg",
+                                                            "projection"))),
+        "page_half": (page, dict(area_max=400, methods=("gaussian", "half_area_min_avg", "half_area"))),
+        "lattice14_half": (cases["lattice14"][0], dict(area_max=400, seeds="peaks",
+                                                       methods=("half_area", "half_area_min_avg"))),
     }
 
 

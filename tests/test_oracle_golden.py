@@ -107,8 +107,10 @@ def test_measure_cds_oracle_matches_reference(name):
 
 # The projection CD method (subpx/_cpu/invariant_cd.py:365-421) beside others: staggered and square
 # pages, a lattice, an inverted page, and a dense peak-seeded lattice where most cells' steepest
-# points reach the cell border (edge_at_cell_border).
-@pytest.mark.parametrize("name", ["staggered", "page", "lattice2", "page_invert", "lattice14"])
+# points reach the cell border (edge_at_cell_border); the half_area family (551-875) on a staggered
+# page, a square page and the dense lattice (region_at_cell_border).
+@pytest.mark.parametrize("name", ["staggered", "page", "lattice2", "page_invert", "lattice14", "staggered_half",
+                                  "page_half", "lattice14_half"])
 def test_projection_oracle_matches_reference(name):
     from oracle import cd as ocd
 
