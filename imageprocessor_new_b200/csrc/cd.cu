@@ -1225,6 +1225,36 @@ __device__ double np_pairwise_sum(const double* a, int n, int stride) {
     return __dadd_rn(np_pairwise_sum(a, n2, stride), np_pairwise_sum(a + n2 * stride, n - n2, stride));
 }
 
+// np_pairwise_sum by one warp (every lane calls it; all lanes return the sum): lanes 0-7 run the
+// eight running sums of a block of up to 128 values, every lane combines them in numpy's tree and
+// adds the tail; above 128 values the same halves as numpy's.
+__device__ double warp_np_sum(const double* a, int n) {
+    if (n > 128) {
+        int n2 = n / 2;
+        n2 -= n2 % 8;
+        const double left = warp_np_sum(a, n2);
+        return __dadd_rn(left, warp_np_sum(a + n2, n - n2));
+    }
+    if (n < 8) {
+        double r = 0.0;
+        for (int i = 0; i < n; ++i) r = __dadd_rn(r, a[i]);
+        return r;
+    }
+    const int lane = threadIdx.x & 31, full = n - n % 8;
+    double r = 0.0;
+    if (lane < 8) {
+        r = a[lane];
+        for (int i = 8; i < full; i += 8) r = __dadd_rn(r, a[i + lane]);
+    }
+    double q[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) q[j] = __shfl_sync(0xffffffffu, r, j);
+    double res = __dadd_rn(__dadd_rn(__dadd_rn(q[0], q[1]), __dadd_rn(q[2], q[3])),
+                           __dadd_rn(__dadd_rn(q[4], q[5]), __dadd_rn(q[6], q[7])));
+    for (int i = full; i < n; ++i) res = __dadd_rn(res, a[i]);
+    return res;
+}
+
 constexpr int kProjWarps = 4;
 
 // The "projection" CD of each cell (subpx/_cpu/invariant_cd.py:365-421), one warp per cell: the x
@@ -1453,25 +1483,14 @@ __device__ double np_pairwise_tree(const double* leaf, int n, int* next) {
     return __dadd_rn(a, np_pairwise_tree(leaf, n - n2, next));
 }
 
-// One leaf of numpy's pairwise sum (n <= 128 values v(i), i = 0 .. n-1).
-template <class F>
-__device__ double np_leaf_sum(F v, int n) {
-    if (n < 8) {
-        double r = 0.0;
-        for (int i = 0; i < n; ++i) r = __dadd_rn(r, v(i));
-        return r;
-    }
-    double r[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) r[j] = v(j);
-    int i = 8;
-    for (; i < n - (n % 8); i += 8)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) r[j] = __dadd_rn(r[j], v(i + j));
-    double res = __dadd_rn(__dadd_rn(__dadd_rn(r[0], r[1]), __dadd_rn(r[2], r[3])),
-                           __dadd_rn(__dadd_rn(r[4], r[5]), __dadd_rn(r[6], r[7])));
-    for (; i < n; ++i) res = __dadd_rn(res, v(i));
-    return res;
+// Doubles before the zoom operators in a half-area CTA's shared memory: cell, ring, leaf sums and
+// small arrays (doubles), four bit planes, row / column counts and leaves (ints), the mask bytes.
+__host__ __device__ inline long long half_ops_offset(int hm, int wm, int f, int n_angles) {
+    const long long Hb = (long long)hm * f, Wb = (long long)wm * f, RW = (Wb + 31) / 32, area = (long long)hm * wm;
+    const long long tmpn = std::max(Hb + Wb, 3LL * (n_angles + 1));
+    const long long bytes = (2 * area + kHalfLeavesMax + tmpn) * 8 + 4 * Hb * RW * 4 + (Hb + Wb + 2 * kHalfLeavesMax) * 4 +
+                            area;
+    return (bytes + 7) / 8;
 }
 
 struct HalfArgs {
@@ -1487,7 +1506,7 @@ struct HalfArgs {
     int median;   // local level: 1 median, 0 minimum of the outermost mask pixels
     int n_top;    // sub-pixels of the averaged peak
     int outlines;
-    double* scratch;  // per CTA: (hm f) x wm, then (hm f) x (wm f) doubles
+    double* scratch;  // per CTA: the (hm f) x (wm f) enlarged cell
     MethodOut single, averaged;  // highest-pixel peak, averaged peak (status null: not wanted)
 };
 
@@ -1520,15 +1539,15 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
     const double cut = __dmul_rn(a.level, peak);
     const bool signal = peak > 0.0 && isfinite(cut) && cut < peak;
     const uint32_t last_bits = (Wb % 32) ? ((1u << (Wb % 32)) - 1u) : 0xffffffffu;
-    for (int t = tid; t < Hb * RW; t += kHalfThreads) {
-        const int Y = t / RW, w0 = (t % RW) * 32;
-        uint32_t word = 0;
-        for (int bit = 0; bit < 32 && w0 + bit < Wb; ++bit) {
-            const int X = w0 + bit;
-            word |= (uint32_t)(((h.bmask[t] >> bit) & 1u) && h.big[(long long)Y * Wb + X] > cut) << bit;
+    const int lane = tid & 31;
+    for (int t = tid >> 5; t < Hb * RW; t += kHalfThreads / 32) {
+        const int Y = t / RW, X = (t % RW) * 32 + lane;
+        const bool in = X < Wb && h.big[(long long)Y * Wb + X] > cut;  // -inf outside the mask
+        const uint32_t word = __ballot_sync(0xffffffffu, in);
+        if (lane == 0) {
+            h.above[t] = word;
+            h.reg[t] = 0u;
         }
-        h.above[t] = word;
-        h.reg[t] = 0u;
     }
     __syncthreads();
     if (tid == 0) {
@@ -1591,45 +1610,84 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
     }
     // Leaves of the region's brightness sum (numpy's pairwise order over the enlarged cell).
     for (int L = tid; L < h.n_leaves; L += kHalfThreads) {
-        const int lo = h.leaf_lo[L];
-        h.leafsum[L] = np_leaf_sum(
-            [&](int q) {
-                const int t = lo + q, Y = t / Wb, X = t % Wb;
-                return ((cur[Y * RW + X / 32] >> (X % 32)) & 1u) ? h.big[t] : 0.0;
-            },
-            h.leaf_len[L]);
+        // The leaf's values in memory order (the order of numpy's running sums), (Y, X) stepped along.
+        const int lo = h.leaf_lo[L], n = h.leaf_len[L];
+        int Y = lo / Wb, X = lo - Y * Wb;
+        auto next = [&]() {
+            const double v = ((cur[Y * RW + (X >> 5)] >> (X & 31)) & 1u) ? h.big[(long long)Y * Wb + X] : 0.0;
+            if (++X == Wb) {
+                X = 0;
+                ++Y;
+            }
+            return v;
+        };
+        double res;
+        if (n < 8) {
+            res = 0.0;
+            for (int q = 0; q < n; ++q) res = __dadd_rn(res, next());
+        } else {
+            double r[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) r[j] = next();
+            int q = 8;
+            for (; q < n - (n % 8); q += 8)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) r[j] = __dadd_rn(r[j], next());
+            res = __dadd_rn(__dadd_rn(__dadd_rn(r[0], r[1]), __dadd_rn(r[2], r[3])),
+                            __dadd_rn(__dadd_rn(r[4], r[5]), __dadd_rn(r[6], r[7])));
+            for (; q < n; ++q) res = __dadd_rn(res, next());
+        }
+        h.leafsum[L] = res;
     }
     touch = __syncthreads_or(touch);
     __shared__ long long s_count;
-    if (tid == 0) {
+    const int warp = tid >> 5;
+    // Row / column moments (products first, by all threads; numpy's sums by one warp each).
+    double* ty = h.tmp;       // rows
+    double* tx = h.tmp + Hb;  // columns
+    for (int Y = tid; Y < Hb; Y += kHalfThreads) ty[Y] = __dmul_rn((double)h.rowcnt[Y], (double)Y);
+    for (int X = tid; X < Wb; X += kHalfThreads) tx[X] = __dmul_rn((double)h.colcnt[X], (double)X);
+    __syncthreads();
+    if (warp == 0) {
         long long count = 0;
-        for (int Y = 0; Y < Hb; ++Y) count += h.rowcnt[Y];
-        s_count = count;
-        int next = 0;
-        h.s_dbl[2] = np_pairwise_tree(h.leafsum, h.N, &next);
-        for (int Y = 0; Y < Hb; ++Y) h.tmp[Y] = __dmul_rn((double)h.rowcnt[Y], (double)Y);
-        h.s_dbl[0] = np_pairwise_sum(h.tmp, Hb, 1);  // sum of row counts x row
-        for (int X = 0; X < Wb; ++X) h.tmp[X] = __dmul_rn((double)h.colcnt[X], (double)X);
-        h.s_dbl[1] = np_pairwise_sum(h.tmp, Wb, 1);
+        for (int Y = lane; Y < Hb; Y += 32) count += h.rowcnt[Y];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
+        if (lane == 0) s_count = count;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int next = 0;
+            h.s_dbl[2] = np_pairwise_tree(h.leafsum, h.N, &next);
+        }
+    } else if (warp == 2) {
+        const double v = warp_np_sum(ty, Hb);
+        if (lane == 0) h.s_dbl[0] = v;  // sum of row counts x row
+    } else if (warp == 3) {
+        const double v = warp_np_sum(tx, Wb);
+        if (lane == 0) h.s_dbl[1] = v;
     }
     __syncthreads();
     const long long count = s_count;
     const double weight = (double)(count > 1 ? count : 1);
     const double cy = __ddiv_rn(h.s_dbl[0], weight), cx = __ddiv_rn(h.s_dbl[1], weight);
     const double mean_signal = __ddiv_rn(h.s_dbl[2], weight);
-    __syncthreads();
     const double sx = 1.0 / a.factor, sy = sx;
-    if (tid == 0) {
-        for (int X = 0; X < Wb; ++X) {
-            const double d = __dsub_rn((double)X, cx);
-            h.tmp[X] = __dmul_rn((double)h.colcnt[X], __dmul_rn(d, d));
-        }
-        h.s_dbl[3] = __dmul_rn(__dmul_rn(__ddiv_rn(np_pairwise_sum(h.tmp, Wb, 1), weight), sx), sx);  // var_x
-        for (int Y = 0; Y < Hb; ++Y) {
-            const double d = __dsub_rn((double)Y, cy);
-            h.tmp[Y] = __dmul_rn((double)h.rowcnt[Y], __dmul_rn(d, d));
-        }
-        h.s_dbl[2] = __dmul_rn(__dmul_rn(__ddiv_rn(np_pairwise_sum(h.tmp, Hb, 1), weight), sy), sy);  // var_y
+    const bool pow2 = (a.factor & (a.factor - 1)) == 0;
+    for (int X = tid; X < Wb; X += kHalfThreads) {
+        const double d = __dsub_rn((double)X, cx);
+        tx[X] = __dmul_rn((double)h.colcnt[X], __dmul_rn(d, d));
+    }
+    for (int Y = tid; Y < Hb; Y += kHalfThreads) {
+        const double d = __dsub_rn((double)Y, cy);
+        ty[Y] = __dmul_rn((double)h.rowcnt[Y], __dmul_rn(d, d));
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const double v = warp_np_sum(tx, Wb);
+        if (lane == 0) h.s_dbl[3] = __dmul_rn(__dmul_rn(__ddiv_rn(v, weight), sx), sx);  // var_x
+    } else if (warp == 1) {
+        const double v = warp_np_sum(ty, Hb);
+        if (lane == 0) h.s_dbl[2] = __dmul_rn(__dmul_rn(__ddiv_rn(v, weight), sy), sy);  // var_y
     }
     __syncthreads();
     const double var_x = h.s_dbl[3], var_y = h.s_dbl[2];
@@ -1649,8 +1707,11 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
             int first_out = nr;
             for (int s = 0; s < nr; ++s) {
                 const double st = __dmul_rn((double)s, 0.125);
-                const double fx = rint(__dadd_rn(cx, __ddiv_rn(__dmul_rn(co, st), sx)));
-                const double fy = rint(__dadd_rn(cy, __ddiv_rn(__dmul_rn(si, st), sy)));
+                // (cos x step) / sx, a multiplication by the factor when it is a power of two (exact).
+                const double ox = pow2 ? __dmul_rn(__dmul_rn(co, st), (double)a.factor) : __ddiv_rn(__dmul_rn(co, st), sx);
+                const double oy = pow2 ? __dmul_rn(__dmul_rn(si, st), (double)a.factor) : __ddiv_rn(__dmul_rn(si, st), sy);
+                const double fx = rint(__dadd_rn(cx, ox));
+                const double fy = rint(__dadd_rn(cy, oy));
                 bool hit = fx >= 0.0 && fx < (double)Wb && fy >= 0.0 && fy < (double)Hb;
                 if (hit) {
                     const int X = (int)fx, Y = (int)fy;
@@ -1677,6 +1738,17 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
                 out.contours[((long long)i * nv + k) * 2] = vx[k];
                 out.contours[((long long)i * nv + k) * 2 + 1] = vy[k];
             }
+        // Perimeter: the closed polygon's side lengths, summed in numpy's order by one warp.
+        double* side = h.tmp + 2 * nv;
+        for (int q = tid; q < a.n_angles; q += kHalfThreads) {
+            const double dx = __dsub_rn(vx[q + 1], vx[q]), dy = __dsub_rn(vy[q + 1], vy[q]);
+            side[q] = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const double v = warp_np_sum(side, a.n_angles);
+            if (lane == 0) h.s_dbl[3] = v;
+        }
     } else {
         if (out.edge_px)
             for (int q = tid; q < a.n_angles; q += kHalfThreads) out.edge_px[(long long)i * a.n_angles + q] = dnan();
@@ -1709,13 +1781,7 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
             m[M_CD_EQ] = cd_eq;
             m[M_CD_X] = __dmul_rn(cd_eq, ratio);
             m[M_CD_Y] = __ddiv_rn(cd_eq, ratio);
-            if (a.outlines) {
-                for (int q = 0; q < a.n_angles; ++q) {
-                    const double dx = __dsub_rn(vx[q + 1], vx[q]), dy = __dsub_rn(vy[q + 1], vy[q]);
-                    h.tmp[2 * nv + q] = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
-                }
-                m[M_PERIM] = np_pairwise_sum(h.tmp + 2 * nv, a.n_angles, 1);
-            }
+            if (a.outlines) m[M_PERIM] = h.s_dbl[3];
         }
     }
     __syncthreads();
@@ -1747,7 +1813,7 @@ __global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
     double* cell = hsm;
     double* ring = cell + area_px;
     double* leafsum = ring + area_px;
-    const int tmpn = max(max(Hb, Wb), 3 * (a.n_angles + 1));
+    const int tmpn = max(Hb + Wb, 3 * (a.n_angles + 1));
     double* tmp = leafsum + kHalfLeavesMax;
     uint32_t* bmask = reinterpret_cast<uint32_t*>(tmp + tmpn);
     uint32_t* above = bmask + Hb * RW;
@@ -1758,8 +1824,13 @@ __global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
     int* leaf_lo = colcnt + Wb;
     int* leaf_len = leaf_lo + kHalfLeavesMax;
     uint8_t* mask = reinterpret_cast<uint8_t*>(leaf_len + kHalfLeavesMax);
-    double* T = a.scratch + (long long)blockIdx.x * ((long long)Hb * wm + (long long)N);
-    double* big = T + (long long)Hb * wm;
+    // The zoom operators, staged once per CTA after the mask bytes (8-byte aligned).
+    double* zy = reinterpret_cast<double*>(hsm) + half_ops_offset(hm, wm, f, a.n_angles);
+    double* zxT = zy + (long long)Hb * hm;  // transposed: zxT[x * Wb + X] = zx[X * wm + x]
+    double* T = zxT + (long long)Wb * wm;    // Hb x wm
+    for (int t = tid; t < Hb * hm; t += kHalfThreads) zy[t] = a.zy[t];
+    for (int t = tid; t < Wb * wm; t += kHalfThreads) zxT[(t % wm) * Wb + t / wm] = a.zx[t];
+    double* big = a.scratch + (long long)blockIdx.x * (long long)N;
     const double sx = 1.0 / f, sy = 1.0 / f;
     const double shift = (double)(f - 1) / (2.0 * f);
     if (tid == 0) s_int[3] = np_pairwise_leaves(0, N, leaf_lo, leaf_len, 0);
@@ -1812,36 +1883,58 @@ __global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
         __syncthreads();
         for (int k = tid; k < area_px; k += kHalfThreads) cell[k] = mask[k] ? __dsub_rn(cell[k], b) : 0.0;
         __syncthreads();
-        // Enlargement: T = Zy C (Hb x wm), then big = T Zx^T (Hb x Wb).
+        // Bit plane of the enlarged mask (each sub-pixel copies its pixel), one word per warp ballot.
+        for (int t = warp; t < Hb * RW; t += kHalfThreads / 32) {
+            const int Y = t / RW, X = (t % RW) * 32 + lane;
+            const uint32_t word = __ballot_sync(0xffffffffu, X < Wb && mask[(Y / f) * wm + X / f]);
+            if (lane == 0) bmask[t] = word;
+        }
+        // Enlargement: T = Zy C (Hb x wm), then big = T Zx^T (Hb x Wb), stored -inf outside the
+        // mask (only sub-pixels of the mask take part in what follows).
         for (int t = tid; t < Hb * wm; t += kHalfThreads) {
             const int Y = t / wm, x = t % wm;
             double v = 0.0;
-            for (int y = 0; y < hm; ++y) v = __fma_rn(a.zy[(long long)Y * hm + y], cell[y * wm + x], v);
+            for (int y = 0; y < hm; ++y) v = __fma_rn(zy[Y * hm + y], cell[y * wm + x], v);
             T[t] = v;
         }
         __syncthreads();
-        for (int t = tid; t < N; t += kHalfThreads) {
-            const int Y = t / Wb, X = t % Wb;
-            double v = 0.0;
-            for (int x = 0; x < wm; ++x) v = __fma_rn(T[(long long)Y * wm + x], a.zx[(long long)X * wm + x], v);
-            big[t] = v;
-        }
-        // Bit plane of the enlarged mask (each sub-pixel copies its pixel).
-        for (int t = tid; t < Hb * RW; t += kHalfThreads) {
-            const int Y = t / RW, w0 = (t % RW) * 32;
-            uint32_t word = 0;
-            for (int bit = 0; bit < 32 && w0 + bit < Wb; ++bit)
-                word |= (uint32_t)mask[(Y / f) * wm + (w0 + bit) / f] << bit;
-            bmask[t] = word;
-        }
+        // One warp per pair of enlarged rows: lane takes columns lane + 32 q, the rows' T values
+        // broadcast, each column's operator values shared by the two rows.
+        for (int Y0 = 2 * warp; Y0 < Hb; Y0 += 2 * (kHalfThreads / 32))
+            for (int X0 = 0; X0 < Wb; X0 += 128) {
+                const bool two = Y0 + 1 < Hb;
+                double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+                for (int x = 0; x < wm; ++x) {
+                    const double t0 = T[Y0 * wm + x], t1 = two ? T[(Y0 + 1) * wm + x] : 0.0;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int X = X0 + lane + 32 * q;
+                        if (X < Wb) {
+                            const double z = zxT[x * Wb + X];
+                            v0[q] = __fma_rn(t0, z, v0[q]);
+                            v1[q] = __fma_rn(t1, z, v1[q]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int X = X0 + lane + 32 * q;
+                    if (X >= Wb) continue;
+                    const bool m0 = (bmask[Y0 * RW + (X >> 5)] >> (X & 31)) & 1u;
+                    big[(long long)Y0 * Wb + X] = m0 ? v0[q] : -INFINITY;
+                    if (two) {
+                        const bool m1 = (bmask[(Y0 + 1) * RW + (X >> 5)] >> (X & 31)) & 1u;
+                        big[(long long)(Y0 + 1) * Wb + X] = m1 ? v1[q] : -INFINITY;
+                    }
+                }
+            }
         __syncthreads();
         // Highest enlarged pixel of the mask (first in row-major order on ties; index 0 when none).
         double best = -INFINITY;
         int best_i = 0x7fffffff;
         unsigned long long kmin = ~0ull, kmax = 0;
         for (int t = tid; t < N; t += kHalfThreads) {
-            const bool in = (bmask[(t / Wb) * RW + (t % Wb) / 32] >> ((t % Wb) % 32)) & 1u;
-            const double v = in ? big[t] : -INFINITY;
+            const double v = big[t];
             if (v > best || best_i == 0x7fffffff) {
                 if (v > best || best_i == 0x7fffffff) {
                     best = v;
@@ -1898,10 +1991,7 @@ __global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
             double peak = -1.0;
             if (a.n_top <= N) {
                 auto for_keys = [&](auto&& fn) {
-                    for (int t = tid; t < N; t += kHalfThreads) {
-                        const bool in = (bmask[(t / Wb) * RW + (t % Wb) / 32] >> ((t % Wb) % 32)) & 1u;
-                        fn(order_key(in ? big[t] : -INFINITY));
-                    }
+                    for (int t = tid; t < N; t += kHalfThreads) fn(order_key(big[t]));
                 };
                 unsigned long long kth, kth2;
                 cta_select<kHalfThreads>(for_keys, N - a.n_top, false, s_kmin, s_kmax, hist, warp_tot, s_pick,
@@ -2048,17 +2138,16 @@ int spx_projection_cd(const double* cleaned, const int* voronoi, const int* boxe
     return check_launch("k_projection_cd");
 }
 
-// Shared memory of one half-area CTA (see the layout in k_half_area).
+// Shared memory of one half-area CTA (see the layout in k_half_area): the cell's arrays, then the
+// two zoom operators and the first product.
 static size_t half_smem(int hm, int wm, int f, int n_angles) {
-    const size_t Hb = (size_t)hm * f, Wb = (size_t)wm * f, RW = (Wb + 31) / 32, area = (size_t)hm * wm;
-    const size_t tmpn = std::max(std::max(Hb, Wb), (size_t)3 * (n_angles + 1));
-    return (2 * area + kHalfLeavesMax + tmpn) * sizeof(double) + 4 * Hb * RW * sizeof(uint32_t) +
-           (Hb + Wb + 2 * kHalfLeavesMax) * sizeof(int) + area;
+    return (half_ops_offset(hm, wm, f, n_angles) + (size_t)hm * f * hm + (size_t)wm * f * wm + (size_t)hm * f * wm) *
+           sizeof(double);
 }
 
 size_t spx_half_area_workspace_bytes(int hm, int wm, int factor) {
     const size_t Hb = (size_t)hm * factor, Wb = (size_t)wm * factor;
-    return (size_t)kHalfCtas * (Hb * wm + Hb * Wb) * sizeof(double) + 256;
+    return (size_t)kHalfCtas * Hb * Wb * sizeof(double) + 256;
 }
 
 int spx_half_area_cd(const double* cleaned, const int* voronoi, const int* boxes, const int* which, int n, int hm,
