@@ -26,7 +26,8 @@ than the 126 MB L2, so consecutive steps do not run from cache.
 uint16 images, each with its own pitch U(16, 40) px, hole diameter 0.4-0.6 x pitch, 5 % missing and
 2 % merged holes; the initial LM fits of all their cells run in one launch, warm-started (patches,
 MLP, LM: `value`) and plain (`plain_lm`), with the warm start's deviation from the plain FP64 fit
-per image.
+per image; `full_measure_cds` then times measure_cds of every image (image by image on the GPU) and
+checks each against the FP64 oracle on a 384 x 384 corner.
 
 ``--impl reference`` times the CPU path (the oracle restatement of the reference algorithm, NumPy /
 SciPy on the host cores) on a crop of the same page; under torchrun only rank 0 runs it.
@@ -609,6 +610,7 @@ def stack_arm(args):
                           "plain_iterations_mean": round(float(ip[sl].mean()), 3) if sl.stop > sl.start else 0.0,
                           "warm_iterations_mean": round(float(iw[sl].mean()), 3) if sl.stop > sl.start else 0.0})
     n = sc.n
+    full = stack_full_pipeline(s)
     cpu = stack_cpu_baseline(s, args) if args.cpu_baseline else None
     print(json.dumps({
         "metric": METRIC, "value": round(n / (ms["warm"] / 1e3), 1), "unit": UNIT, "n_gpus": 1,
@@ -624,7 +626,69 @@ def stack_arm(args):
         "fallback_fraction": float(fw.mean()),
         "centre_dev_max_px": max(p["centre_dev_max_px"] for p in per_image),
         "within_1e-3_px": bool(all(p["centre_dev_max_px"] <= 1e-3 for p in per_image)),
-        "per_image": per_image, "clocks": clocks.summary(), "cpu_baseline": cpu}), flush=True)
+        "per_image": per_image, "clocks": clocks.summary(), "cpu_baseline": cpu,
+        "full_measure_cds": full}), flush=True)
+
+
+STACK_CD_KW = dict(area_min=10, area_max=2000, pad=3)
+
+
+def _stack_oracle_worker(crop):
+    """One pool worker: the oracle's measure_cds of one image crop (no GPU here)."""
+    from oracle import cd as ocd
+
+    return ocd.measure_cds(crop, methods=METHODS, **STACK_CD_KW)
+
+
+def stack_full_pipeline(stack_d, crop: int = 384) -> dict:
+    """measure_cds (the bench's methods, summary_only) of every image of the stack, one after another
+    on this GPU, timed with CUDA events (the images already in HBM); and per image the GPU pipeline
+    against the FP64 oracle on a crop x crop corner (a spawn pool on the host cores): largest centre
+    and CD differences per method over the cells both report."""
+    import multiprocessing as mp
+
+    import torch
+
+    from imageprocessor_new_b200 import measure_cds
+
+    n_img = int(stack_d.shape[0])
+    measure_cds(stack_d[0], backend="gpu", methods=METHODS, summary_only=True, **STACK_CD_KW)
+    torch.cuda.synchronize()
+    per_image, cells, total = [], 0, 0.0
+    for i in range(n_img):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        res = measure_cds(stack_d[i], backend="gpu", methods=METHODS, summary_only=True, **STACK_CD_KW)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        total += ms
+        cells += len(res.seeds_xy)
+        per_image.append({"cells": int(len(res.seeds_xy)), "ms": round(ms, 3)})
+    crops = [np.ascontiguousarray(stack_d[i, :crop, :crop].cpu().numpy()) for i in range(n_img)]
+    with mp.get_context("spawn").Pool(max(1, min(n_img, os.cpu_count() or 1))) as pool:
+        oracle = pool.map(_stack_oracle_worker, crops)
+    worst_c = worst_cd = 0.0
+    same = True
+    for i, (c, ref) in enumerate(zip(crops, oracle)):
+        got = measure_cds(c, backend="gpu", methods=METHODS, **STACK_CD_KW)
+        same = same and np.array_equal(got.seeds_xy, ref["seeds"])
+        err_c = err_cd = 0.0
+        if np.array_equal(got.seeds_xy, ref["seeds"]):
+            for m in METHODS:
+                g, r = got.measurements[m], ref["measurements"][m]
+                both = (g.status == "ok") & (r["status"] == "ok")
+                if both.any():
+                    err_c = max(err_c, float(np.abs(g.centers_xy[both] - r["centers"][both]).max()))
+                    err_cd = max(err_cd, float(np.abs(g.metrics["cd_equivalent_px"][both]
+                                                      - r["metrics"]["cd_equivalent_px"][both]).max()))
+        per_image[i].update(oracle_crop_cells=int(len(ref["seeds"])), centre_max_px=err_c, cd_max_px=err_cd)
+        worst_c, worst_cd = max(worst_c, err_c), max(worst_cd, err_cd)
+    return {"value": round(cells / (total / 1e3), 1), "unit": UNIT, "ms_total": round(total, 2), "cells": cells,
+            "how": "measure_cds (gaussian, gradient, halfmax; summary_only) image by image on one GPU",
+            "accuracy_vs_oracle": {"sample": f"{crop}x{crop} corner of every image", "same_seeds": same,
+                                   "centre_max_px": worst_c, "cd_max_px": worst_cd},
+            "per_image": per_image}
 
 
 def _stack_cpu_worker(crop):

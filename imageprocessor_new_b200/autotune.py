@@ -1,9 +1,8 @@
 """Autotuner of the launch shapes (no reference counterpart).
 
 The knobs (``spx_tune_set``): warps per block and persistent blocks per SM of the LM fit kernels,
-the model-render tile, and how the radial profiles map rays to threads (one ray per thread with the
-spline window cached in registers, one ray per warp with 32 samples at once, or one ray per thread
-reading the window at every sample). None of them changes a result -- the fits take cells from a
+the model-render tile, and how the radial profiles read their spline windows (one ray per thread,
+the window cached in registers or read at every sample). None of them changes a result -- the fits take cells from a
 device work queue and every cell's arithmetic is the same whatever shape runs it; the render sums
 each pixel's Gaussians in cell order in every tile shape; the ray mappings evaluate the same
 samples with the same arithmetic and rules -- so the tuner only times them. It times each
@@ -30,7 +29,7 @@ KNOBS = {
     "fit_warps": (2, 4, 8),
     "fit_blocks_per_sm": (4, 8, 16),
     "render_tile": (16, 32, 64),
-    "radial_rays": (0, 1, 2),
+    "radial_rays": (0, 2),
 }
 
 

@@ -611,6 +611,22 @@ __device__ __forceinline__ double cubic_at(const double* coef, int hp, int wp, i
     return out;
 }
 
+// cubic_at for a position whose 4 x 4 window lies inside the plane (no index clamps needed): the same
+// weights, products and order of additions, so the same value.
+__device__ __forceinline__ double cubic_at_inner(const double* coef, int pitch, double y, double x) {
+    const double fy = floor(y), fx = floor(x);
+    double wy[4], wx[4];
+    cubic_weights_t(y - fy, wy);
+    cubic_weights_t(x - fx, wx);
+    const double* q = coef + ((int)fy - 1) * pitch + ((int)fx - 1);
+    double out = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) out += q[a * pitch + b] * wy[a] * wx[b];
+    return out;
+}
+
 // The same window evaluated in FP32 (weights, products and sums), the sampling precision the ray
 // profiles use, from an FP32 copy of the coefficients: sample positions stay FP64 and only their
 // fractional offsets inside the window are rounded to FP32, so a sample differs from the FP64
@@ -820,6 +836,183 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
     }
 }
 
+// FP64 sample k of a ray (k = 0: the peak): position centre + k step (cos, sin) rounded as the FP32
+// walk computes it, and scipy's order-3 evaluation of the FP64 coefficient plane. Not inlined: every
+// FP64 sample of the radial kernel runs this one copy of the code, which keeps the kernel's
+// instruction footprint small (the walk's loop and this function stay in the instruction cache).
+__device__ __noinline__ double ray_sample64(const double* coef, int hp, int wp, int dp, double cx, double cy,
+                                            double ux, double uy, double step, int k, double peak) {
+    if (k == 0) return peak;
+    const double r = (double)k * step;
+    const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
+    return cubic_at_inner(coef, dp, y + kPad, x + kPad);
+}
+
+// One ray walked again with FP64 samples (scipy's order-3 evaluation of the FP64 coefficient plane,
+// as the peak) and the reference's own arithmetic (subpx/_cpu/cd.py:220-264): the first half-height
+// crossing (p[j] >= half > p[j+1], radius j step + (p[j] - half) / (p[j] - p[j+1]) step) and the
+// first maximum of the outward decrease grad(j) = -((p[j+1] - p[j-1]) / (2 step)) over the
+// candidates, refined by the parabola through grad(j-1), grad(j), grad(j+1). Validity as in the FP32
+// walk. Writes the edges asked for (NaN when none).
+__device__ __noinline__ void ray_fp64(const double* coef, int hp, int wp, int dp, const uint8_t* emask, int hm, int wm,
+                                      double cx, double cy, double ux, double uy, double step, int n_radii,
+                                      int j_min, double peak, bool want_h, bool want_g, double* edge_h,
+                                      double* edge_g) {
+    const double half = peak / 2.0, two_step = 2.0 * step;
+    const double ymax = (double)(hm - 1), xmax = (double)(wm - 1);
+    double p1 = 0.0, p2 = 0.0;             // p[k-1], p[k-2]
+    double ga = 0.0, gb = 0.0;             // grad(k-3), grad(k-2)
+    double best = -INFINITY, bl = 0.0, bm = 0.0, br = 0.0;
+    int best_j = -1, first_invalid = n_radii;
+    double eh = dnan(), eg = dnan();
+    bool crossed = false;
+    for (int k = 0; k < n_radii; ++k) {
+        const double r = (double)k * step;
+        const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
+        if (!(y >= 0.0 && y <= ymax && x >= 0.0 && x <= xmax)) {
+            first_invalid = k;
+            break;
+        }
+        double fyd, fxd;
+        const int iy = floor_nonneg(y, &fyd), ix = floor_nonneg(x, &fxd);
+        const uint8_t* q = emask + iy * wm + ix;
+        const bool full4 = iy + 1 < hm && ix + 1 < wm && q[0] && q[1] && q[wm] && q[wm + 1];
+        if (!(full4 || inside_bytes(emask, hm, wm, y, x))) {
+            first_invalid = k;
+            break;
+        }
+        const double pk = ray_sample64(coef, hp, wp, dp, cx, cy, ux, uy, step, k, peak);
+        if (k >= 1 && !crossed && p1 >= half && pk < half) {
+            eh = __dadd_rn((double)(k - 1) * step, __dmul_rn(__ddiv_rn(__dsub_rn(p1, half), __dsub_rn(p1, pk)), step));
+            crossed = true;
+        }
+        if (k >= 2) {
+            const double gc = -__ddiv_rn(__dsub_rn(pk, p2), two_step);  // grad(k-1)
+            const int j = k - 2;  // candidate: samples j-2 .. j+2 valid
+            if (k >= 3 && j >= j_min && j <= n_radii - 3 && gb > best) {
+                best = gb;
+                best_j = j;
+                bl = ga;
+                bm = gb;
+                br = gc;
+            }
+            ga = gb;
+            gb = gc;
+        }
+        p2 = p1;
+        p1 = pk;
+    }
+    if (best_j >= 0) {
+        const int j = best_j;
+        const bool left_ok = j - 1 >= j_min;
+        const bool right_ok = j + 1 <= n_radii - 3 && j + 3 < first_invalid;
+        const double curv = __dadd_rn(__dsub_rn(bl, __dmul_rn(2.0, bm)), br);
+        if (left_ok && right_ok && bm >= bl && bm >= br && bm > __dmul_rn(0.01, peak) && curv < -1e-12) {
+            double delta = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(bl, br)), curv);
+            delta = delta < -0.5 ? -0.5 : (delta > 0.5 ? 0.5 : delta);
+            eg = __dadd_rn((double)j * step, __dmul_rn(delta, step));
+        }
+    }
+    if (want_h) *edge_h = eh;
+    if (want_g) *edge_g = eg;
+}
+
+// The edges of one ray from FP64 samples (scipy's order-3 evaluation of the FP64 coefficient plane)
+// at the places the FP32 walk found, with the reference's arithmetic (subpx/_cpu/cd.py:220-264):
+// * kc > 0: the half-height crossing between samples kc - 1 and kc (the walk has checked that no
+//   earlier sample and neither of these is within its error bound of half height), at radius
+//   (kc - 1) step + (p[kc-1] - half) / (p[kc-1] - p[kc]) step;
+// * j >= 0: the gradient edge around j, the maximum of the FP32 outward decreases, when every
+//   candidate three or more samples from j is clearly below it: candidates j-2 .. j+2 compete with
+//   FP64 decreases grad(k) = -((p[k+1] - p[k-1]) / (2 step)) (first maximum wins) and the winner is
+//   refined by the parabola through its neighbours, NaN when it fails a test.
+// Samples j-3 .. j+3 and the crossing pair (usually among them) are taken once each in one rolled
+// loop with the sampler inlined once (this function has one call site); when the winner is j-2 or
+// j+2, the two samples of its outer neighbour's decrease are taken again (rare).
+__device__ __forceinline__ void ray_edges64(const double* coef, int hp, int wp, int dp, double cx, double cy, double ux,
+                                         double uy, double step, double peak, int kc, int j, int j_min, int n_radii,
+                                         int first_invalid, double* edge_h, double* edge_g) {
+    const double half = peak / 2.0, two_step = 2.0 * step;
+    int lo = 1 << 30, hi = -(1 << 30);
+    if (kc > 0) {
+        lo = kc - 1;
+        hi = kc;
+    }
+    if (j >= 0) {
+        lo = min(lo, j - 3);
+        hi = max(hi, j + 3);
+    }
+    double g1 = 0.0, g2 = 0.0, g3 = 0.0, g4 = 0.0, g5 = 0.0;  // grad(j-2) .. grad(j+2)
+    double pm1 = 0.0, pm2 = 0.0;                              // p[k-1], p[k-2]
+    double c0 = 0.0, c1 = 0.0;                                // p[kc-1], p[kc]
+#pragma unroll 1
+    for (int k = lo; k <= hi; ++k) {
+        const bool in_g = j >= 0 && k >= j - 3 && k <= j + 3;
+        const bool in_h = kc > 0 && (k == kc - 1 || k == kc);
+        if (!in_g && !in_h) continue;
+        double pk = 0.0;
+        if (k == 0) {
+            pk = peak;
+        } else if (k > 0 && k < first_invalid) {
+            const double r = (double)k * step;
+            const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
+            pk = cubic_at_inner(coef, dp, y + kPad, x + kPad);
+        }
+        if (k == kc - 1) c0 = pk;
+        if (k == kc) c1 = pk;
+        if (in_g) {
+            if (k >= j - 1) {  // grad(k - 1)
+                g1 = g2;
+                g2 = g3;
+                g3 = g4;
+                g4 = g5;
+                g5 = -__ddiv_rn(__dsub_rn(pk, pm2), two_step);
+            }
+            pm2 = pm1;
+            pm1 = pk;
+        }
+    }
+    if (kc > 0) *edge_h = __dadd_rn((double)(kc - 1) * step, __dmul_rn(__ddiv_rn(__dsub_rn(c0, half), __dsub_rn(c0, c1)), step));
+    if (j < 0) return;
+    *edge_g = dnan();
+    const double gs[5] = {g1, g2, g3, g4, g5};
+    int tb = -1;
+    double mid = 0.0;
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+        const int k = j - 2 + t;
+        const bool cand = k >= j_min && k <= n_radii - 3 && k + 2 < first_invalid;
+        if (cand && (tb < 0 || gs[t] > mid)) {
+            tb = t;
+            mid = gs[t];
+        }
+    }
+    const int jb = j - 2 + tb;
+    const bool left_ok = jb - 1 >= j_min;
+    const bool right_ok = jb + 1 <= n_radii - 3 && jb + 3 < first_invalid;
+    if (!(left_ok && right_ok)) return;
+    double left, right;
+    if (tb == 0) {  // grad(j - 3) needs samples j - 4 and j - 2
+        const double pa = ray_sample64(coef, hp, wp, dp, cx, cy, ux, uy, step, j - 4, peak);
+        const double pb = ray_sample64(coef, hp, wp, dp, cx, cy, ux, uy, step, j - 2, peak);
+        left = -__ddiv_rn(__dsub_rn(pb, pa), two_step);
+        right = g2;
+    } else if (tb == 4) {  // grad(j + 3) needs samples j + 2 and j + 4
+        const double pa = ray_sample64(coef, hp, wp, dp, cx, cy, ux, uy, step, j + 2, peak);
+        const double pb = ray_sample64(coef, hp, wp, dp, cx, cy, ux, uy, step, j + 4, peak);
+        left = g4;
+        right = -__ddiv_rn(__dsub_rn(pb, pa), two_step);
+    } else {
+        left = tb == 1 ? g1 : (tb == 2 ? g2 : g3);
+        right = tb == 1 ? g3 : (tb == 2 ? g4 : g5);
+    }
+    const double curv = __dadd_rn(__dsub_rn(left, __dmul_rn(2.0, mid)), right);
+    if (!(mid >= left && mid >= right && mid > __dmul_rn(0.01, peak) && curv < -1e-12)) return;
+    double delta = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(left, right)), curv);
+    delta = delta < -0.5 ? -0.5 : (delta > 0.5 ? 0.5 : delta);
+    *edge_g = __dadd_rn((double)jb * step, __dmul_rn(delta, step));
+}
+
 // Radial profiles of each cell: weighted centroid of the pixels above 0.1 x max, cubic-spline
 // samples every radial_step along n_angles rays until the eroded cell ends, first half-height
 // crossing and the parabolic maximum of the outward decrease (halfmax / gradient methods).
@@ -829,20 +1022,20 @@ __device__ __noinline__ void radial_finish(const MethodOut out, int found, int i
 // the signal (zero outside the cell) and the mask are each filtered along y then x with zero edges
 // (scipy's gaussian_filter, mode="constant"), and the spline is fitted to their ratio over the whole
 // cell box; the centroid still comes from the unsmoothed signal.
-// kWarpRays: the ray loop maps one ray to one warp, its lanes taking 32 consecutive samples at a
-// time (positions, validity and spline samples with no per-lane caching, so no divergent reloads),
-// with the halfmax crossing and the gradient maximum found by ballots and shuffles; the results are
-// bit for bit those of the one-ray-per-thread loop (same sample arithmetic, same first-crossing and
-// first-maximum rules).
 // kRays: 0 one ray per thread with the 4 x 4 window cached in registers (reloaded when a ray enters
-// another pixel), 1 one ray per warp (kWarpRays), 2 one ray per thread reading the window's four
-// float4 rows at every sample (no per-lane reload branch) and the precomputed corner plane.
+// another pixel), 2 one ray per thread reading the window's four float4 rows at every sample (no
+// per-lane reload branch) and the precomputed corner plane; the same samples either way.
+// The walk samples in FP32 and finds the first half-height crossing and the largest outward decrease;
+// the edges come from FP64 samples at those places (the crossing pair; the decreases two samples
+// either side of the maximum, grad_edge64), so they carry the reference's FP64 arithmetic. Where an
+// FP32 sample leaves a decision elsewhere within its error bound (a sample near half height before
+// the crossing; a candidate three or more samples from the maximum level with it), ray_fp64 walks
+// the ray again with FP64 samples and that result is kept.
 template <bool kSmooth, int kRays>
 __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     const double* cleaned, const int* vor, const int4* boxes, const int* which, int n, int hm, int wm, int W,
     int n_angles, double radial_step, int n_radii, const double* smooth_w, int smooth_r, double* coef_scratch,
     MethodOut half_out, MethodOut grad_out) {
-    constexpr bool kWarpRays = kRays == 1;
     extern __shared__ double sm[];
     __shared__ double trig_tab[2 * kTrigMax];  // cos, sin of the ray angles (n_angles <= kTrigMax)
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -953,125 +1146,35 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         for (int row = tid; row < hp; row += kRadialThreads) spline_line(coef + (long long)row * dp, wp, 1);
         __syncthreads();
         const double peak = cubic_at(coef, hp, wp, dp, cy + kPad, cx + kPad);
+        float cmax = 0.0f;  // largest FP32 coefficient magnitude a sample can weigh
         for (int k = tid; k < (hm + 3) * wm; k += kRadialThreads) {
             const double* q = coef + (k / wm + kPad - 1) * dp + (k % wm + kPad - 1);
-            quad[k] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+            const float4 f = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+            quad[k] = f;
+            cmax = fmaxf(cmax, fmaxf(fmaxf(fabsf(f.x), fabsf(f.y)), fmaxf(fabsf(f.z), fabsf(f.w))));
         }
-        __syncthreads();
+        // The window weights are non-negative and sum to one per axis, so an FP32 sample is within about
+        // 45 ulps of cmax of the FP64 one (coefficient, offset and weight roundings, 20 FMAs); tol keeps
+        // a margin of nearly 3 (2^-17 cmax). Also orders the quad writes before the rays read them.
+        const float tol = (float)cta_max((double)cmax, red + 28) * 7.62939453125e-06f;
         const double half = peak / 2.0;
-        const double inv2s = 1.0 / (2.0 * radial_step);
         int j_min = 2;  // first gradient candidate: j >= 2 and j * step >= thr
         while ((double)j_min * radial_step < thr) ++j_min;
         int found_h = 0, found_g = 0;
-        if constexpr (kWarpRays) {
-            const int lane = tid & 31;
-            const float halff = (float)half;
-            const double ymax = (double)(hm - 1), xmax = (double)(wm - 1);
-            for (int ray = warp; ray < n_angles; ray += kRadialThreads / 32) {
-                double edge_h = dnan(), edge_g = dnan();
-                if (peak > 0.0) {
-                    const double ang = (double)ray * (2.0 * kPi / n_angles);
-                    const double ux = trig ? trig[2 * ray] : cos(ang), uy = trig ? trig[2 * ray + 1] : sin(ang);
-                    float c1 = 0, c2 = 0, c3 = 0, c4 = 0;  // p[k0-1] .. p[k0-4] of the previous chunk
-                    bool crossed = false;
-                    float best = -INFINITY, dl = 0, dm = 0, dr = 0;
-                    int best_j = -1, first_invalid = n_radii;
-                    for (int k0 = 0; k0 < n_radii; k0 += 32) {
-                        const int k = k0 + lane;
-                        bool valid = false;
-                        float p = 0.0f;
-                        if (k < n_radii) {
-                            const double r = (double)k * radial_step;
-                            const double x = __dadd_rn(cx, __dmul_rn(ux, r)), y = __dadd_rn(cy, __dmul_rn(uy, r));
-                            if (y >= 0.0 && y <= ymax && x >= 0.0 && x <= xmax) {
-                                double fyd, fxd;
-                                const int iy = floor_nonneg(y, &fyd), ix = floor_nonneg(x, &fxd);
-                                valid = full[iy * wm + ix] || inside_bytes(emask, hm, wm, y, x);
-                                if (valid)
-                                    p = k == 0 ? (float)peak
-                                               : spline_sample_f(quad, wm, iy, ix, (float)(y - fyd),
-                                                                 (float)(x - fxd));
-                            }
-                        }
-                        const unsigned inv = __ballot_sync(0xffffffffu, k < n_radii && !valid);
-                        const int lim = inv ? k0 + __ffs(inv) - 1 : min(k0 + 32, n_radii);  // processed: k < lim
-                        if (inv) first_invalid = lim;
-                        const bool proc = k < lim;
-                        // p[k - m] for m = 1..4 (lanes below m take the previous chunk's values).
-                        float pm1 = __shfl_up_sync(0xffffffffu, p, 1), pm2 = __shfl_up_sync(0xffffffffu, p, 2);
-                        float pm3 = __shfl_up_sync(0xffffffffu, p, 3), pm4 = __shfl_up_sync(0xffffffffu, p, 4);
-                        if (lane < 1) pm1 = c1;
-                        if (lane < 2) pm2 = lane == 0 ? c2 : c1;
-                        if (lane < 3) pm3 = lane == 0 ? c3 : (lane == 1 ? c2 : c1);
-                        if (lane < 4) pm4 = lane == 0 ? c4 : (lane == 1 ? c3 : (lane == 2 ? c2 : c1));
-                        // Half-height: the first processed k >= 1 with p[k-1] >= half > p[k].
-                        if (!crossed) {
-                            const unsigned hc = __ballot_sync(0xffffffffu, proc && k >= 1 && pm1 >= halff && p < halff);
-                            if (hc) {
-                                const int f = __ffs(hc) - 1;
-                                double e = 0.0;
-                                if (lane == f)
-                                    e = (double)(k - 1) * radial_step +
-                                        (((double)pm1 - half) / ((double)pm1 - (double)p)) * radial_step;
-                                edge_h = __shfl_sync(0xffffffffu, e, f);
-                                crossed = true;
-                            }
-                        }
-                        // Gradient: candidate j = k - 2 (sample k valid) with d = p[j-1] - p[j+1]; the
-                        // first maximum over all candidates.
-                        const int jj = k - 2;
-                        const bool cand = proc && jj >= j_min && jj <= n_radii - 3;
-                        const float d = cand ? pm3 - pm1 : -INFINITY;
-                        float m = d;
-#pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-                        if (m > best) {
-                            const int f = __ffs(__ballot_sync(0xffffffffu, cand && d == m)) - 1;
-                            const float l4 = __shfl_sync(0xffffffffu, pm4 - pm2, f);
-                            const float r2 = __shfl_sync(0xffffffffu, pm2 - p, f);
-                            best = m;
-                            best_j = k0 + f - 2;
-                            dm = m;
-                            dl = l4;
-                            dr = r2;
-                        }
-                        if (inv || k0 + 32 >= n_radii) break;
-                        c1 = __shfl_sync(0xffffffffu, p, 31);
-                        c2 = __shfl_sync(0xffffffffu, p, 30);
-                        c3 = __shfl_sync(0xffffffffu, p, 29);
-                        c4 = __shfl_sync(0xffffffffu, p, 28);
-                    }
-                    if (best_j >= 0) {
-                        const int j = best_j;
-                        const double gm = (double)dm * inv2s, gl = (double)dl * inv2s, gr = (double)dr * inv2s;
-                        const bool left_ok = j - 1 >= j_min;
-                        const bool right_ok = j + 1 <= n_radii - 3 && j + 3 < first_invalid;
-                        const double curv = gl - 2.0 * gm + gr;
-                        if (left_ok && right_ok && gm >= gl && gm >= gr && gm > 0.01 * peak && curv < -1e-12) {
-                            double delta = 0.5 * (gl - gr) / curv;
-                            delta = delta < -0.5 ? -0.5 : (delta > 0.5 ? 0.5 : delta);
-                            edge_g = (double)j * radial_step + delta * radial_step;
-                        }
-                    }
-                }
-                if (lane == 0) {
-                    if (half_out.status) half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
-                    if (grad_out.status) grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
-                    found_h += isfinite(edge_h);
-                    found_g += isfinite(edge_g);
-                }
-            }
-        }
-        for (int ray = kWarpRays ? n_angles : tid; ray < n_angles; ray += kRadialThreads) {
+        for (int ray = tid; ray < n_angles; ray += kRadialThreads) {
             double edge_h = dnan(), edge_g = dnan();
             if (peak > 0.0) {
                 const double ang = (double)ray * (2.0 * kPi / n_angles);
                 const double ux = trig ? trig[2 * ray] : cos(ang), uy = trig ? trig[2 * ray + 1] : sin(ang);
-                // Samples are FP32 (SplineWindowF); the profile bookkeeping follows in FP32 and the
-                // edge positions are computed in FP64 from the kept samples.
-                float h1 = 0, h2 = 0, h3 = 0, h4 = 0;  // p[k-1] .. p[k-4]
-                bool crossed = false;
-                float best = -INFINITY, dl = 0, dm = 0, dr = 0;  // p[j-1] - p[j+1] at the best j, j-1, j+1
+                // Samples are FP32 (SplineWindowF) and the walk's decisions are FP32; the edges are then
+                // computed from FP64 samples at the decisive positions.
+                float h1 = 0, h2 = 0, h3 = 0;  // p[k-1] .. p[k-3]
+                int kc = -1;                   // first FP32 crossing: p[kc-1] >= half > p[kc]
+                bool amb_h = false;            // a sample up to kc within tol of half height
+                // Largest outward decrease p[j-1] - p[j+1] (first maximum) and the largest of the
+                // candidates three or more samples from it; d1, d2: the decreases at jj-1, jj-2, and
+                // m3 the largest at or before jj-3, for the current candidate jj.
+                float best = -INFINITY, far = -INFINITY, d1 = -INFINITY, d2 = -INFINITY, m3 = -INFINITY;
                 int best_j = -1, first_invalid = n_radii;
                 const float halff = (float)half;
                 SplineWindowF win;
@@ -1100,10 +1203,9 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                         if (!(mfull || inside_bytes(emask, hm, wm, y, x))) { first_invalid = k; break; }
                         p = k == 0 ? (float)peak : win.at(quad, wm, iy, ix, (float)(y - fyd), (float)(x - fxd));
                     }
-                    if (k >= 1 && !crossed && h1 >= halff && p < halff) {
-                        edge_h = (double)(k - 1) * radial_step +
-                                 (((double)h1 - half) / ((double)h1 - (double)p)) * radial_step;
-                        crossed = true;
+                    if (k >= 1 && kc < 0) {
+                        amb_h |= fabsf(p - halff) <= tol;
+                        if (h1 >= halff && p < halff) kc = k;
                     }
                     // Sample k valid makes j = k - 2 a candidate (valid[j - 2] and valid[j + 2]); its
                     // outward decrease is (p[j-1] - p[j+1]) / (2 step).
@@ -1111,30 +1213,34 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                     if (jj >= j_min && jj <= n_radii - 3) {
                         const float d = h3 - h1;
                         if (d > best) {
+                            far = m3;
                             best = d;
                             best_j = jj;
-                            dm = d;
-                            dl = h4 - h2;  // j - 1
-                            dr = h2 - p;   // j + 1
+                        } else if (jj >= best_j + 3) {
+                            far = fmaxf(far, d);
                         }
+                        m3 = fmaxf(m3, d2);
+                        d2 = d1;
+                        d1 = d;
                     }
-                    h4 = h3;
                     h3 = h2;
                     h2 = h1;
                     h1 = p;
                 }
-                if (best_j >= 0) {
-                    const int jj = best_j;
-                    const double gm = (double)dm * inv2s, gl = (double)dl * inv2s, gr = (double)dr * inv2s;
-                    const bool left_ok = jj - 1 >= j_min;
-                    const bool right_ok = jj + 1 <= n_radii - 3 && jj + 3 < first_invalid;
-                    const double curv = gl - 2.0 * gm + gr;
-                    if (left_ok && right_ok && gm >= gl && gm >= gr && gm > 0.01 * peak && curv < -1e-12) {
-                        double delta = 0.5 * (gl - gr) / curv;
-                        delta = delta < -0.5 ? -0.5 : (delta > 0.5 ? 0.5 : delta);
-                        edge_g = (double)jj * radial_step + delta * radial_step;
-                    }
-                }
+                // FP64 samples settle the edges: the crossing pair, and the decreases around the FP32
+                // maximum. A decision within the FP32 samples' error bound elsewhere on the ray (a
+                // sample near half height before the crossing, a distant candidate level with the
+                // maximum) walks the ray again in FP64.
+                const bool redo_h = half_out.status && amb_h;
+                const bool redo_g = grad_out.status && best_j >= 0 && far >= best - 4.0f * tol;
+                const int fix_kc = half_out.status && !amb_h ? kc : -1;
+                const int fix_j = grad_out.status && !redo_g ? best_j : -1;
+                if (fix_kc > 0 || fix_j >= 0)
+                    ray_edges64(coef, hp, wp, dp, cx, cy, ux, uy, radial_step, peak, fix_kc, fix_j, j_min, n_radii,
+                                first_invalid, &edge_h, &edge_g);
+                if (redo_h || redo_g)
+                    ray_fp64(coef, hp, wp, dp, emask, hm, wm, cx, cy, ux, uy, radial_step, n_radii, j_min, peak,
+                             redo_h, redo_g, &edge_h, &edge_g);
             }
             if (half_out.status) half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
             if (grad_out.status) grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
@@ -1487,7 +1593,7 @@ __device__ double np_pairwise_tree(const double* leaf, int n, int* next) {
 // small arrays (doubles), four bit planes, row / column counts and leaves (ints), the mask bytes.
 __host__ __device__ inline long long half_ops_offset(int hm, int wm, int f, int n_angles) {
     const long long Hb = (long long)hm * f, Wb = (long long)wm * f, RW = (Wb + 31) / 32, area = (long long)hm * wm;
-    const long long tmpn = std::max(Hb + Wb, 3LL * (n_angles + 1));
+    const long long tmpn = Hb + Wb > 3LL * (n_angles + 1) ? Hb + Wb : 3LL * (n_angles + 1);
     const long long bytes = (2 * area + kHalfLeavesMax + tmpn) * 8 + 4 * Hb * RW * 4 + (Hb + Wb + 2 * kHalfLeavesMax) * 4 +
                             area;
     return (bytes + 7) / 8;
@@ -1831,8 +1937,6 @@ __global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
     for (int t = tid; t < Hb * hm; t += kHalfThreads) zy[t] = a.zy[t];
     for (int t = tid; t < Wb * wm; t += kHalfThreads) zxT[(t % wm) * Wb + t / wm] = a.zx[t];
     double* big = a.scratch + (long long)blockIdx.x * (long long)N;
-    const double sx = 1.0 / f, sy = 1.0 / f;
-    const double shift = (double)(f - 1) / (2.0 * f);
     if (tid == 0) s_int[3] = np_pairwise_leaves(0, N, leaf_lo, leaf_len, 0);
     __syncthreads();
     const int n_leaves = s_int[3];
@@ -2260,10 +2364,9 @@ int spx_radial_cd(const double* cleaned, const int* voronoi, const int* boxes, c
     using T = std::true_type;
     using F = std::false_type;
     using R0 = std::integral_constant<int, 0>;
-    using R1 = std::integral_constant<int, 1>;
     using R2 = std::integral_constant<int, 2>;
-    if (smooth) return rays == 1 ? go(T{}, R1{}) : rays == 2 ? go(T{}, R2{}) : go(T{}, R0{});
-    return rays == 1 ? go(F{}, R1{}) : rays == 2 ? go(F{}, R2{}) : go(F{}, R0{});
+    if (smooth) return rays == 2 ? go(T{}, R2{}) : go(T{}, R0{});
+    return rays == 2 ? go(F{}, R2{}) : go(F{}, R0{});
 }
 
 }  // extern "C"

@@ -21,8 +21,7 @@ struct Tuning {
     int fit_warps = 4;          // warps (cells in flight) per block of the LM fit kernels: 2, 4 or 8
     int fit_blocks_per_sm = 8;  // persistent fit blocks per SM: 2..32
     int render_tile = 64;       // model render tile edge: 16, 32 or 64 pixels
-    int radial_rays = 2;        // radial profiles: 0 one ray per thread (cached window), 1 one ray per warp
-                                // (32 samples at once), 2 one ray per thread (window read per sample)
+    int radial_rays = 2;        // radial profiles, one ray per thread: 0 cached spline window, 2 window read per sample
 };
 Tuning& tuning();
 

@@ -1057,7 +1057,7 @@ int spx_tune_set(const char* knob, int value) {
         SPX_REQUIRE(value == 16 || value == 32 || value == 64, "render_tile must be 16, 32 or 64");
         t.render_tile = value;
     } else if (!strcmp(knob, "radial_rays")) {
-        SPX_REQUIRE(value >= 0 && value <= 2, "radial_rays must be 0, 1 or 2");
+        SPX_REQUIRE(value == 0 || value == 2, "radial_rays must be 0 or 2");
         t.radial_rays = value;
     } else {
         set_error("unknown tuning knob '%s'", knob);

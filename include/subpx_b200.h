@@ -61,8 +61,8 @@ unsigned long long spx_launch_count(void);
 /* Launch-shape knobs (process-wide, chosen by the autotuner; none changes a result):
  * "fit_warps" (2, 4, 8 cells in flight per block of the LM fit kernels), "fit_blocks_per_sm"
  * (2..32 persistent fit blocks per SM), "render_tile" (16, 32 or 64 pixel model-render tiles),
- * "radial_rays" (0 one ray per thread with a cached spline window, 1 one ray per warp, 2 one ray
- * per thread reading the window at every sample). No reference counterpart. */
+ * "radial_rays" (one ray per thread: 0 with a cached spline window, 2 reading the window at every
+ * sample). No reference counterpart. */
 int spx_tune_set(const char* knob, int value);
 int spx_tune_get(const char* knob, int* value);
 /* Number of SMs of the current device, and whether it is an sm_100 part (1) or not (0). */
