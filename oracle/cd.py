@@ -239,7 +239,7 @@ def unmodelled(binary, labels, ids):
 def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), threshold="otsu", invert=False,
                 area_min=3, area_max=50, pad=3, n_angles=128, radial_step=0.1, fit_fraction=0.2,
                 deblend_iterations=30, deblend_tolerance=1e-3, background_level=None, seeds="threshold",
-                peak_min_distance=None, smooth_sigma=0.0):
+                peak_min_distance=None, smooth_sigma=0.0, tail_area_level=0.2, tail_window=1.2):
     """The model-background measure_cds pipeline, seeds from thresholded components or, with
     seeds="peaks", from the smoothed signal's maxima (subpx/cd.py:502-511)."""
     img = np.asarray(img)
@@ -250,7 +250,8 @@ def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), 
         return _measure_peaks(img, signal, sign, methods=methods, pad=pad, n_angles=n_angles, radial_step=radial_step,
                               fit_fraction=fit_fraction, deblend_iterations=deblend_iterations,
                               deblend_tolerance=deblend_tolerance, background_level=background_level,
-                              peak_min_distance=peak_min_distance, smooth_sigma=smooth_sigma)
+                              peak_min_distance=peak_min_distance, smooth_sigma=smooth_sigma,
+                              tail_area_level=tail_area_level, tail_window=tail_window)
     seg = img
     if img.dtype != np.uint8 and not (img.dtype == np.uint16 and threshold == "otsu"):
         g = img.astype(np.float64)
@@ -281,7 +282,8 @@ def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), 
                                 tile_px, unmodelled(binary, labels, ids), oversized, methods=methods, pad=pad,
                                 n_angles=n_angles, radial_step=radial_step, fit_fraction=fit_fraction,
                                 deblend_iterations=deblend_iterations, deblend_tolerance=deblend_tolerance,
-                                background_level=background_level, smooth_sigma=smooth_sigma)
+                                background_level=background_level, smooth_sigma=smooth_sigma,
+                                tail_area_level=tail_area_level, tail_window=tail_window)
 
 
 def _measure_peaks(img, signal, sign, *, peak_min_distance, **kw):
@@ -299,7 +301,7 @@ def _measure_peaks(img, signal, sign, *, peak_min_distance, **kw):
 
 def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch, tile_px, exclude_mask, oversized, *,
                          methods, pad, n_angles, radial_step, fit_fraction, deblend_iterations, deblend_tolerance,
-                         background_level, smooth_sigma):
+                         background_level, smooth_sigma, tail_area_level=0.2, tail_window=1.2):
     """The deblend passes with seed revision and the measurements (subpx/cd.py:581-760)."""
     h, w = img.shape
 
@@ -350,9 +352,10 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
             (c[:, 1] + reach < h - 1)
     report = np.flatnonzero(interior)
     cleaned = state.cleaned[report]
-    from .invariant import HALF_AREA
+    from .invariant import HALF_AREA, TAIL_AREA
 
-    measured = [m for m in methods if m not in ("gaussian", "projection") and m not in HALF_AREA]
+    measured = [m for m in methods if m not in ("gaussian", "projection") and m not in HALF_AREA
+                and m not in TAIL_AREA]
     out = measure_cells(cleaned, masks[report], origins[report], seeds[report], methods=measured, n_angles=n_angles,
                         radial_step=radial_step, fit_fraction=fit_fraction, smooth_sigma=smooth_sigma) if measured else {}
     if "gaussian" in methods:
@@ -367,6 +370,15 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
         from .invariant import half_areas
 
         out.update(half_areas(cleaned, masks[report], origins[report], n_angles, half))
+    tails = [m for m in methods if m in TAIL_AREA]
+    tail_info = {}
+    if tails:
+        from .invariant import tail_areas
+
+        found = tail_areas(signal, state, masks, origins, report, n_angles, tails, level=tail_area_level,
+                           window=tail_window, pitch=float(pitch) if np.isfinite(pitch) else None)
+        tail_info = found.pop("_info")
+        out.update(found)
     out = {m: out[m] for m in methods}
     from scipy.ndimage import map_coordinates
 
@@ -381,7 +393,7 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
     return {"seeds": seeds[report], "cell_labels": remap[cell_labels], "measurements": out, "params": params_global,
             "report": report, "passes": passes, "iterations_used": sum(passes), "added": added, "dropped": dropped,
             "source": state.background_info.get("source"), "background_map": sign * state.background_map,
-            "status": state.status[report], "pitch": pitch}
+            "status": state.status[report], "pitch": pitch, "tail_info": tail_info}
 
 
 def threshold_cells(img, *, threshold="otsu", invert=False, area_min=3, area_max=50, pad=3):

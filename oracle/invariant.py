@@ -169,12 +169,74 @@ def _ring_level(mask, cell, kind):
     return np.where(ring, cell, np.inf).reshape(k, -1).min(axis=1)
 
 
-def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, level=0.5, peak_pixels=4.0,
-               outlines=True):
-    """The half_area family on an (n, h, w) stack of neighbour-removed cells: for each name of
-    `names` the oracle's measurement dict with the reference's metrics (local_level, threshold,
-    mean_signal beside the geometry)."""
-    cleaned = np.asarray(cleaned, dtype=np.float64)
+def _ring_or_level(mask, cell, kind, level_mask):
+    """Local level b of each cell: `kind` 'median' / 'min' of its outermost mask pixels, or with
+    `level_mask` the median over those pixels inside the mask; 'zero' for the kinds without one."""
+    k = len(mask)
+    if kind == "zero":
+        return np.zeros(k)
+    if level_mask is None:
+        return _ring_level(mask, cell, kind)
+    import warnings
+
+    ring = level_mask & mask
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        return np.nanmedian(np.where(ring, cell, np.nan).reshape(k, -1), axis=1)
+
+
+def _core(big_mask, d):
+    """Pixels whose +-d difference stencil lies in the enlarged mask, none within d of the edge."""
+    core = big_mask.copy()
+    for axis in (1, 2):
+        for shift in (d, -d):
+            core &= np.roll(big_mask, shift, axis=axis)
+    core[:, :d] = core[:, -d:] = False
+    core[:, :, :d] = core[:, :, -d:] = False
+    return core
+
+
+def _edge_cut(big, big_mask, d):
+    """edge_area's threshold (subpx/_cpu/invariant_cd.py:818-833): the enlarged cell's mean with each
+    pixel weighted by its steepness (central differences +-d sub-pixels, one original pixel)."""
+    pad = np.pad(big, ((0, 0), (d, d), (d, d)), mode="edge")
+    steep = np.sqrt(((pad[:, 2 * d:, d:-d] - pad[:, :-2 * d, d:-d]) / (2 * d * (1.0 / d))) ** 2
+                    + ((pad[:, d:-d, 2 * d:] - pad[:, d:-d, :-2 * d]) / (2 * d * (1.0 / d))) ** 2)
+    wgt = np.where(_core(big_mask, d), steep, 0.0)
+    total = wgt.sum(axis=(1, 2))
+    return np.where(total > 0, (wgt * big).sum(axis=(1, 2)) / np.where(total > 0, total, 1.0), np.inf)
+
+
+def _foot_cut(big, big_mask, d, zone):
+    """foot_area's threshold and steepest level (subpx/_cpu/invariant_cd.py:834-857): below the
+    steepness-weighted mean (the steepest level), the mean weighted by the signed curvature."""
+    s = 1.0 / d
+    pad = np.pad(big, ((0, 0), (d, d), (d, d)), mode="edge")
+    up, down = pad[:, 2 * d:, d:-d], pad[:, :-2 * d, d:-d]
+    right, left = pad[:, d:-d, 2 * d:], pad[:, d:-d, :-2 * d]
+    steep = np.sqrt(((up - down) / (2 * d * s)) ** 2 + ((right - left) / (2 * d * s)) ** 2)
+    curve = (up + down - 2 * big) / (d * s) ** 2 + (right + left - 2 * big) / (d * s) ** 2
+    core = _core(big_mask, d)
+    if zone is not None:
+        core &= zone
+    wgt = np.where(core, steep, 0.0)
+    total = wgt.sum(axis=(1, 2))
+    steepest = (wgt * big).sum(axis=(1, 2)) / np.where(total > 0, total, 1.0)
+    outer = core & (big < steepest[:, None, None])
+    bend = np.where(outer, curve, 0.0).sum(axis=(1, 2))
+    cut = np.where((total > 0) & (bend > 0),
+                   np.where(outer, curve * big, 0.0).sum(axis=(1, 2)) / np.where(bend > 0, bend, 1.0), np.inf)
+    return cut, steepest
+
+
+def areas(cells, masks, origins, n_angles, specs, *, level_masks=None, zone_masks=None, outlines=True):
+    """The area methods of subpx/_cpu/invariant_cd.py:551-875 on an (n, h, w) stack of cells (CPU
+    path, one size bucket): `specs` are dicts of name, level, background ('median', 'min', 'zero',
+    'edge', 'foot' or 'given'), peak_pixels (None: the highest enlarged pixel) and cuts (per-cell
+    thresholds for 'given'). `level_masks`: per cell, the pixels the median local level is taken over
+    (instead of the outermost pixels); `zone_masks`: foot's territory. Returns per name the oracle's
+    measurement dict (metrics: the half_area names, plus steepest_level for 'foot')."""
+    cells = np.asarray(cells, dtype=np.float64)
     masks = np.asarray(masks, dtype=bool)
     origins = np.asarray(origins, dtype=np.float64).reshape(-1, 2)
     n, h, w = masks.shape
@@ -188,23 +250,27 @@ def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, l
     radii = np.arange(0.0, float(np.hypot(h, w)), 0.125)
     cos_a, sin_a = np.cos(angles), np.sin(angles)
     out = {}
-    for name in names:
-        out[name] = {"centers": np.full((n, 2), np.nan), "center_local": np.full((n, 2), np.nan),
-                     "contours": np.full((n, n_angles + 1, 2), np.nan), "edge_px": np.full((n, n_angles), np.nan),
-                     "status": np.full(n, "no_signal", dtype="U32"),
-                     "metrics": {k: np.full(n, np.nan) for k in HALF_NAMES}}
+    for spec in specs:
+        names = HALF_NAMES + (("steepest_level",) if spec["background"] == "foot" else ())
+        out[spec["name"]] = {"centers": np.full((n, 2), np.nan), "center_local": np.full((n, 2), np.nan),
+                             "contours": np.full((n, n_angles + 1, 2), np.nan),
+                             "edge_px": np.full((n, n_angles), np.nan),
+                             "status": np.full(n, "no_signal", dtype="U32"),
+                             "metrics": {k: np.full(n, np.nan) for k in names}}
     chunk = max(1, 4096 * 196 // (h * w))
     for start in range(0, n, chunk):
         rows = np.arange(start, min(n, start + chunk))
         k = len(rows)
         mask = masks[rows]
-        cell = np.where(mask, cleaned[rows], 0.0)
+        cell = np.where(mask, cells[rows], 0.0)
         big_mask = mask[:, iy][:, :, ix]
-        levels, bigs = {}, {}
-        for name in names:
-            kind, averaged = HALF_AREA[name]
+        lm = None if level_masks is None else np.asarray(level_masks, bool)[rows]
+        levels, bigs, peaks = {}, {}, {}
+        for spec in specs:
+            name, level, background = spec["name"], spec["level"], spec["background"]
+            kind = background if background in ("median", "min") else "zero"
             if kind not in levels:
-                b = _ring_level(mask, cell, kind)
+                b = _ring_or_level(mask, cell, kind, lm)
                 levels[kind] = b
                 centered = np.where(mask, cell - b[:, None, None], 0.0)
                 bigs[kind] = zy[None] @ centered @ zx.T[None]
@@ -212,11 +278,22 @@ def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, l
             flat = np.where(big_mask, big, -np.inf).reshape(k, -1)
             top = np.argmax(flat, axis=1)
             peak = flat[np.arange(k), top]
-            if averaged:
-                n_top = min(max(1, int(round(peak_pixels * FACTOR * FACTOR))), H * W)
-                peak = np.partition(flat, -n_top, axis=1)[:, -n_top:].mean(axis=1)
-                peak = np.where(np.isfinite(peak), peak, -1.0)
-            cut = level * peak
+            if spec["peak_pixels"] is not None:
+                n_top = min(max(1, int(round(spec["peak_pixels"] * FACTOR * FACTOR))), H * W)
+                if (kind, n_top) not in peaks:
+                    p = np.partition(flat, -n_top, axis=1)[:, -n_top:].mean(axis=1)
+                    peaks[kind, n_top] = np.where(np.isfinite(p), p, -1.0)
+                peak = peaks[kind, n_top]
+            steepest = None
+            if background == "edge":
+                cut = _edge_cut(big, big_mask, FACTOR)
+            elif background == "foot":
+                zone = None if zone_masks is None else np.asarray(zone_masks, bool)[rows][:, iy][:, :, ix]
+                cut, steepest = _foot_cut(big, big_mask, FACTOR, zone)
+            elif background == "given":
+                cut = np.asarray(spec["cuts"], dtype=float)[rows]
+            else:
+                cut = level * peak
             above = big_mask & (big > cut[:, None, None])
             region = _component_of(above, top)
             count = region.sum(axis=(1, 2))
@@ -237,6 +314,8 @@ def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, l
             m["peak_signal"][rows] = np.where(signal, peak, np.nan)
             m["threshold"][rows] = np.where(signal, b + cut, np.nan)
             m["mean_signal"][rows] = np.where(signal, mean_signal, np.nan)
+            if steepest is not None:
+                m["steepest_level"][rows] = np.where(signal, steepest, np.nan)
             m["area_px2"][rows] = np.where(signal, count * (sx * sy), np.nan)
             m["cd_x_px"][rows] = np.where(signal, cd_eq * ratio, np.nan)
             m["cd_y_px"][rows] = np.where(signal, cd_eq / ratio, np.nan)
@@ -254,8 +333,8 @@ def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, l
                 hit = np.take_along_axis(region.reshape(k, -1), index, axis=1).reshape(px.shape) & inside
                 first_out = np.where(hit.all(axis=2), len(steps), np.argmin(hit, axis=2))
                 o["edge_px"][rows] = steps[np.maximum(first_out - 1, 0)] + 0.0625
-    for name in names:
-        o = out[name]
+    for spec in specs:
+        o = out[spec["name"]]
         m = o["metrics"]
         m["cd_equivalent_px"][:] = 2 * np.sqrt(m["area_px2"] / np.pi)
         rows = np.flatnonzero(o["status"] != "no_signal")
@@ -273,4 +352,139 @@ def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, l
         ok = o["status"] == "ok"
         for metric in ("area_px2", "cd_equivalent_px", "cd_x_px", "cd_y_px", "perimeter_px"):
             m[metric][~ok] = np.nan
+    return out
+
+
+def half_areas(cleaned, masks, origins, n_angles=128, names=("half_area",), *, level=0.5, peak_pixels=4.0,
+               outlines=True):
+    """The half_area family on an (n, h, w) stack of neighbour-removed cells: for each name of
+    `names` the oracle's measurement dict with the reference's metrics (local_level, threshold,
+    mean_signal beside the geometry)."""
+    specs = [{"name": name, "level": level, "background": HALF_AREA[name][0],
+              "peak_pixels": peak_pixels if HALF_AREA[name][1] else None, "cuts": None} for name in names]
+    return areas(cleaned, masks, origins, n_angles, specs, outlines=outlines)
+
+
+# ---------------------------------------------------------------------------- the tail family
+# subpx/_cpu/invariant_cd.py: _wide_cells 878-964 (CPU branch) and measure_invariant's tail branch
+# 1009-1068: each reported hole on a square window of half-width ceil(tail_window * pitch) around its
+# rounded fitted centre, holding its own share of the light, measured by the area methods with a low
+# threshold.
+
+TAIL_AREA = {"tail_area": "median", "tail_area_norm": "zero", "edge_area": "edge", "foot_area": "foot",
+             "foot_area_ratio": "given"}
+
+
+def wide_cells(signal, state, masks, origins, report, pitch, radius_pitches):
+    """(cells as float32, inside the image, level pixels, own territory, window origins): the image
+    minus the background map, each pixel shared among the holes in proportion to their models (own
+    model / (model image + 1e-3 x the median amplitude)); territory = closer to the hole than to its
+    8 nearest modelled holes; level pixels = the farthest tenth (at least 4) of the territory."""
+    from scipy.spatial import cKDTree
+
+    from .deblend import render_radius
+
+    n_all, h, w = masks.shape
+    cap = int(max(h, w))
+    params = np.asarray(state.params, dtype=float).copy()
+    params[:, 1:3] += origins
+    fallback = origins + np.array([(w - 1) / 2, (h - 1) / 2])
+    centers_all = np.where(np.isfinite(params[:, 1:3]), params[:, 1:3], fallback)
+    rows_rep = np.arange(n_all)[report]
+    centers = centers_all[rows_rep]
+    radius = int(np.ceil(radius_pitches * pitch))
+    size = 2 * radius + 1
+    win_origins = np.rint(centers).astype(np.int64) - radius
+    n = len(rows_rep)
+    if not n:
+        shape = (0, size, size)
+        return (np.empty(shape, np.float32), np.empty(shape, bool), np.empty(shape, bool), np.empty(shape, bool),
+                win_origins.astype(float))
+    k = min(9, n_all)
+    neighbours = cKDTree(centers_all).query(centers, k=k)[1].reshape(n, k)
+    neighbours[:, 0] = rows_rep
+    data = signal - state.background_map
+    model = state.model_image
+    good_amp = params[np.isfinite(params).all(axis=1), 0]
+    floor = 1e-3 * float(np.median(good_amp)) if good_amp.size else 1e-12
+    height, width = signal.shape
+    offsets = np.arange(size)
+    o = win_origins
+    ys = o[:, 1, None] + offsets[None]
+    xs = o[:, 0, None] + offsets[None]
+    inside = ((ys >= 0) & (ys < height))[:, :, None] & ((xs >= 0) & (xs < width))[:, None, :]
+    pick = (np.clip(ys, 0, height - 1)[:, :, None], np.clip(xs, 0, width - 1)[:, None, :])
+    win, total = data[pick], model[pick]
+    gp = params[rows_rep]
+    good = np.isfinite(gp).all(axis=1)
+    gp = np.where(good[:, None], gp, 0.0)
+    render = render_radius(np.where(np.isfinite(params[rows_rep]), params[rows_rep], 0.0), cap)
+    gx = xs[:, None, :].astype(float)
+    gy = ys[:, :, None].astype(float)
+    dx = gx - gp[:, 1, None, None]
+    dy = gy - gp[:, 2, None, None]
+    a = np.exp(gp[:, 3, None, None]) * dx + gp[:, 4, None, None] * dy
+    b = np.exp(gp[:, 5, None, None]) * dy
+    box = (np.abs(dx) <= render[:, None, None]) & (np.abs(dy) <= render[:, None, None]) & good[:, None, None]
+    own = np.where(box, gp[:, 0, None, None] * np.exp(-0.5 * (a * a + b * b)), 0.0)
+    near = centers_all[neighbours]
+    dist = np.sqrt((gx[:, None] - near[:, :, 0, None, None]) ** 2 + (gy[:, None] - near[:, :, 1, None, None]) ** 2)
+    mine = dist[:, 0] <= dist[:, 1:].min(axis=1) if k > 1 else np.ones_like(dist[:, 0], dtype=bool)
+    own_area = inside & mine
+    far = np.sort(np.where(own_area, dist[:, 0], -np.inf).reshape(n, -1), axis=1)[:, ::-1]
+    count = own_area.reshape(n, -1).sum(axis=1)
+    keep = np.clip(np.maximum(count // 10, 4), 1, far.shape[1]) - 1
+    level = own_area & (dist[:, 0] >= far[np.arange(n), keep][:, None, None])
+    cells = np.where(inside, win * own / (total + floor), 0.0).astype(np.float32)
+    return cells, inside, level, own_area, win_origins.astype(float)
+
+
+def median_pitch(state, origins):
+    """The median nearest-neighbour distance of the fitted centres (measure_invariant's default pitch)."""
+    from scipy.spatial import cKDTree
+
+    centers = np.asarray(state.params)[:, 1:3] + origins
+    centers = centers[np.isfinite(centers).all(axis=1)]
+    return float(np.median(cKDTree(centers).query(centers, k=2)[0][:, 1])) if len(centers) > 1 else None
+
+
+def tail_areas(signal, state, masks, origins, report, n_angles=128, names=("tail_area",), *, level=0.2,
+               peak_pixels=4.0, window=1.2, pitch=None, outlines=True):
+    """The tail family for the reported holes of a converged deblend state: per name the oracle's
+    measurement dict (center_local relative to the hole's own cell), plus "_info" with the window
+    size in pixels and foot_area_ratio's ratio."""
+    masks = np.asarray(masks, dtype=bool)
+    origins = np.asarray(origins, dtype=np.float64).reshape(-1, 2)
+    if pitch is None or not np.isfinite(pitch):
+        pitch = median_pitch(state, origins)
+        if pitch is None:
+            pitch = float(max(masks.shape[1:]))
+    cells, inside, level_masks, territory, win_origins = wide_cells(signal, state, masks, origins, report, pitch,
+                                                                    window)
+    first = [name for name in names if name != "foot_area_ratio"]
+    if "foot_area_ratio" in names and "foot_area" not in first:
+        first.append("foot_area")
+    specs = [{"name": name, "level": level, "background": TAIL_AREA[name], "peak_pixels": peak_pixels, "cuts": None}
+             for name in first]
+    found = areas(cells, inside, win_origins, n_angles, specs, level_masks=level_masks, zone_masks=territory,
+                  outlines=outlines)
+    info = {"tail_window_px": int(cells.shape[1])}
+    if "foot_area_ratio" in names:
+        foot = found["foot_area"]
+        steepest = foot["metrics"]["steepest_level"]
+        valid = foot["status"] == "ok"
+        ratio = float(np.nanmedian((foot["metrics"]["threshold"] / steepest)[valid])) if valid.any() else np.nan
+        info["foot_ratio"] = ratio
+        found.update(areas(cells, inside, win_origins, n_angles,
+                           [{"name": "foot_area_ratio", "level": level, "background": "given",
+                             "peak_pixels": peak_pixels, "cuts": ratio * steepest}],
+                           level_masks=level_masks, zone_masks=territory, outlines=outlines))
+    rep_origins = origins[np.arange(len(origins))[report]]
+    out = {}
+    for name in names:
+        o = found[name]
+        local = o["centers"] - rep_origins
+        o["center_local"] = np.where(np.isfinite(local), local, np.nan)
+        out[name] = o
+    out["_info"] = info
     return out

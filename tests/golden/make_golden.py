@@ -344,9 +344,55 @@ def make_centers_model(out: Path, ref):
     np.savez_compressed(out / "centers_model.npz", **arrays)
 
 
+TAIL = ("tail_area", "tail_area_norm", "edge_area", "foot_area", "foot_area_ratio")
+
+
+def tail_cases():
+    cases = cd_cases()
+    stag, _ = cases["staggered"]
+    page, _ = cases["page"]
+    lat2, _ = cases["lattice2"]
+    return {
+        # Windows of 1.2 pitches holding each hole's share of the light; the five threshold rules.
+        "staggered_tail": (stag, dict(area_max=400, methods=TAIL)),
+        "lattice2_tail": (lat2, dict(area_max=400, methods=TAIL + ("half_area_min_avg",))),
+        # Options: a lower level on narrower windows, no display outlines.
+        "page_tail": (page, dict(area_max=400, methods=("tail_area", "foot_area_ratio", "edge_area"),
+                                 tail_area_level=0.3, tail_window=0.8, outlines=False)),
+        # Dense holes seeded by peaks: windows reaching past several neighbours.
+        "lattice14_tail": (cases["lattice14"][0], dict(area_max=400, seeds="peaks",
+                                                       methods=("tail_area", "tail_area_norm", "foot_area"))),
+    }
+
+
+def make_tail(out: Path, ref):
+    """measure_cds with the tail family (subpx/_cpu/invariant_cd.py:878-1068)."""
+    from subpx import measure_cds
+
+    arrays = {}
+    names = []
+    for name, (img, kw) in tail_cases().items():
+        res = measure_cds(img, backend="cpu", **kw)
+        arrays[f"{name}_img"] = img
+        arrays[f"{name}_kwargs"] = np.array(json.dumps(kw))
+        arrays[f"{name}_seeds"] = res.seeds_xy
+        arrays[f"{name}_meta"] = np.array(json.dumps({k: res.meta.get(k) for k in ("tail_window_px", "foot_ratio")}))
+        for m, r in res.measurements.items():
+            arrays[f"{name}_{m}_status"] = r.status
+            arrays[f"{name}_{m}_centers"] = r.centers_xy
+            arrays[f"{name}_{m}_center_local"] = r.geometry["center_local"]
+            # Outline radii are k / 8 + 1 / 16 px: exact in float32. Contours are centre + radius x
+            # (cos, sin) + origin and are not stored.
+            arrays[f"{name}_{m}_edge_px"] = r.geometry["edge_px"].astype(np.float32)
+            for metric, v in r.metrics.items():
+                arrays[f"{name}_{m}_m_{metric}"] = v
+        names.append(name)
+    np.savez_compressed(out / "tail.npz", names=np.array(names), **arrays)
+
+
 MAKERS = {"thresholds": make_thresholds, "ccl": make_ccl, "centers": make_centers, "voronoi": make_voronoi,
           "tiled": make_tiled, "cd": make_cd, "results": make_results, "centers_model": make_centers_model,
-          "invariant": make_invariant}
+          "invariant": make_invariant, "tail": make_tail}
 
 
 def main():

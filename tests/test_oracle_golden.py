@@ -131,6 +131,38 @@ def test_projection_oracle_matches_reference(name):
             np.testing.assert_array_equal(r["edge_px"], z[f"{name}_{method}_edge_px"])
 
 
+# The tail family (subpx/_cpu/invariant_cd.py:878-1068): windows of tail_window pitches holding each
+# hole's share of the light, measured with the median of the territory's farthest tenth as the level
+# (tail_area), none (tail_area_norm), the steepness-weighted mean (edge_area), the foot of the edge
+# (foot_area) and the image's median foot ratio (foot_area_ratio); options on a square page, and a
+# dense peak-seeded lattice.
+@pytest.mark.parametrize("name", ["staggered_tail", "lattice2_tail", "page_tail", "lattice14_tail"])
+def test_tail_oracle_matches_reference(name):
+    import json
+
+    from oracle import cd as ocd
+
+    z = _load("tail")
+    kw = _cd_kwargs(z, name)
+    outlines = kw.pop("outlines", True)
+    got = ocd.measure_cds(z[f"{name}_img"], **kw)
+    np.testing.assert_array_equal(got["seeds"], z[f"{name}_seeds"])
+    meta = json.loads(str(z[f"{name}_meta"]))
+    assert got["tail_info"]["tail_window_px"] == meta["tail_window_px"]
+    assert got["tail_info"].get("foot_ratio") == meta["foot_ratio"]
+    for method in kw["methods"]:
+        r = got["measurements"][method]
+        np.testing.assert_array_equal(r["status"], z[f"{name}_{method}_status"])
+        for metric, v in r["metrics"].items():
+            if metric == "background" or (metric == "perimeter_px" and not outlines):
+                continue
+            np.testing.assert_array_equal(v, z[f"{name}_{method}_m_{metric}"], err_msg=f"{method} {metric}")
+        np.testing.assert_array_equal(r["centers"], z[f"{name}_{method}_centers"])
+        np.testing.assert_array_equal(r["center_local"], z[f"{name}_{method}_center_local"])
+        if outlines:
+            np.testing.assert_array_equal(r["edge_px"], z[f"{name}_{method}_edge_px"].astype(np.float64))
+
+
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_morphology_matches_opencv(seed):
     cv2 = pytest.importorskip("cv2")
