@@ -136,6 +136,12 @@ SIGNATURES = {
     "spx_projection_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _P, _P, _I, _P, _P, _I, _MO, _P]),
     "spx_half_area_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_half_area_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P, _I, _D, _I, _I, _I, _MO, _MO, _P, _S, _P]),
+    "spx_wide_cells_workspace_bytes": (_S, [_I, _I, _I, _I, _D]),
+    "spx_wide_cells": (_I, [_P, _I, _D, _I, _I, _BG, _P, _P, _P, _I, _I, _I, _P, _I, _I, _D, _D, _P, _P, _P, _P, _P,
+                            _P, _P, _S, _P]),
+    "spx_tail_area_workspace_bytes": (_S, [_I, _I, _I]),
+    "spx_tail_area_cd": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _P, _P, _I, _D, _I, _I, _P, _MO, _MO, _MO, _MO, _MO,
+                              _P, _S, _P]),
     "spx_radial_workspace_bytes": (_S, [_I, _I, _I]),
     "spx_radial_cd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _D, _P, _I, _MO, _MO, _P, _S, _P]),
     "spx_minimum_filter": (_I, [_P, _I, _I, _I, _P, _P, _P]),

@@ -29,14 +29,22 @@ METHOD_LABELS = {
     "half_area": "Area above half height",
     "half_area_min": "Area above half height (minimum level)",
     "half_area_min_avg": "Area above half height (minimum level, averaged peak)",
+    "tail_area": "Area above a low threshold near the background",
+    "tail_area_norm": "Area above a fraction of the peak (no background step)",
+    "edge_area": "Area inside the steepest edge (no peak, no background step)",
+    "foot_area": "Area inside the foot of the edge, a tail boundary (no peak, no background step)",
+    "foot_area_ratio": "Area inside the foot of the edge, foot found once per image (no peak, no background step)",
 }
 # The half_area family: local level (median or minimum of the outermost pixels), averaged peak.
 HALF_AREA = {"half_area": ("median", False), "half_area_min": ("min", False), "half_area_min_avg": ("min", True)}
+# The tail family on windows of tail_window pitches: each one's threshold rule.
+TAIL_AREA = {"tail_area": "median", "tail_area_norm": "zero", "edge_area": "edge", "foot_area": "foot",
+             "foot_area_ratio": "given"}
+AREA_METHODS = tuple(HALF_AREA) + tuple(TAIL_AREA)
 SUPPORTED = tuple(METHOD_LABELS)
 # Methods of the reference that are outside this package (invariant, local, outline families).
-OTHER_METHODS = ("disk", "flux_ratio",
-                 "tail_area", "tail_area_norm", "edge_area", "foot_area", "foot_area_ratio", "local_projection",
-                 "local_half_area", "local_half_area_min_avg", "local_tail_area", "outline_fit", "outline_fit_fast")
+OTHER_METHODS = ("disk", "flux_ratio", "local_projection", "local_half_area", "local_half_area_min_avg",
+                 "local_tail_area", "outline_fit", "outline_fit_fast")
 
 GEOMETRY_METRICS = ("area_px2", "cd_equivalent_px", "cd_x_px", "cd_y_px", "perimeter_px")
 FIT_METRICS = ("sigma_major_px", "sigma_minor_px", "fwhm_major_px", "fwhm_minor_px", "angle_deg", "log_fit_rmse")
@@ -51,8 +59,9 @@ def _metric_names(method: str) -> tuple[str, ...]:
         return _COLS + FIT_METRICS[:-1] + ("fit_rmse",)
     if method == "projection":
         return _COLS
-    if method in HALF_AREA:
-        return _COLS + ("local_level", "threshold", "mean_signal")
+    if method in AREA_METHODS:
+        return _COLS + ("local_level", "threshold", "mean_signal") + (("steepest_level",) if method == "foot_area"
+                                                                     else ())
     return _COLS + ("ray_coverage",)
 
 
@@ -189,6 +198,8 @@ def measure_cds(
     fit_precision: str = "fp64",
     half_area_level: float = 0.5,
     half_area_peak_pixels: float = 4.0,
+    tail_area_level: float = 0.2,
+    tail_window: float = 1.2,
     outlines: bool = True,
     **other,
 ) -> CDResult | CDSummary:
@@ -197,8 +208,10 @@ def measure_cds(
     Cells, background map, Gaussian deblending and the gaussian / logquad / gradient / halfmax
     measurements follow the reference CPU path operation for operation (FP64). Parameters of the
     reference's other method families (``nominal_cd``, ``psf_fwhm``, ``tail_area_level``, ...) are
-    accepted in ``other`` and must keep their defaults. ``projection`` and the ``half_area`` family
-    (``half_area_level``, ``half_area_peak_pixels``, ``outlines``) follow subpx/_cpu/invariant_cd.py.
+    accepted in ``other`` and must keep their defaults. ``projection``, the ``half_area`` family
+    (``half_area_level``, ``half_area_peak_pixels``, ``outlines``) and the tail family (``tail_area``,
+    ``tail_area_norm``, ``edge_area``, ``foot_area``, ``foot_area_ratio``; ``tail_area_level``,
+    ``tail_window``) follow subpx/_cpu/invariant_cd.py; tail windows are limited to 64 px.
 
     ``fit_precision`` (no reference counterpart) sets the deblending LM's arithmetic: "fp64" is the
     reference's; "fp32" runs the per-pixel residuals, Jacobian and sums in FP32 (compensated J^T r
@@ -217,6 +230,10 @@ def measure_cds(
         raise ValueError("half_area_level must be between 0 and 1")
     if not (np.isfinite(half_area_peak_pixels) and half_area_peak_pixels >= 1):
         raise ValueError("half_area_peak_pixels must be at least 1")
+    if not (np.isfinite(tail_area_level) and 0 < tail_area_level < 1):
+        raise ValueError("tail_area_level must be between 0 and 1")
+    if not (np.isfinite(tail_window) and 0.5 <= tail_window <= 2):
+        raise ValueError("tail_window must be between 0.5 and 2 pitches")
     if not isinstance(outlines, (bool, np.bool_)):
         raise ValueError("outlines must be True or False")
     from .deblend import fit_options
@@ -244,6 +261,7 @@ def measure_cds(
                             summary_only=bool(summary_only), fit_precision=fit_precision, seeds=seeds,
                             peak_min_distance=peak_min_distance, smooth_sigma=float(smooth_sigma),
                             half_area_level=float(half_area_level), half_area_peak_pixels=float(half_area_peak_pixels),
+                            tail_area_level=float(tail_area_level), tail_window=float(tail_window),
                             outlines=bool(outlines))
 
 
@@ -276,7 +294,7 @@ def _method_buffers(n: int, n_angles: int, method: str, contours: bool):
         "metrics": (max(len(names), 13), m),  # column-major: one contiguous column per metric
         "center_local": (m, 2),
         "edge_px": (m, n_angles) if method in ("gradient", "halfmax") or (
-            (method == "projection" or method in HALF_AREA) and contours) else None,
+            (method == "projection" or method in AREA_METHODS) and contours) else None,
         "eigenvalues": (m, 2) if method in ("logquad", "gaussian") else None,
         "axes": (m, 2, 2) if method in ("logquad", "gaussian") else None,
         "status": ((m + 7) // 8,),  # bytes, viewed as uint8
@@ -345,7 +363,7 @@ def _to_result(method: str, n: int, b: dict, host: np.ndarray, metrics_only: boo
         geometry = {"center_local": part("center_local"), "eigenvalues": part("eigenvalues"), "axes": part("axes")}
     elif method in ("gradient", "halfmax"):
         geometry = {"center_local": part("center_local"), "edge_px": part("edge_px")}
-    elif method == "projection" or method in HALF_AREA:
+    elif method == "projection" or method in AREA_METHODS:
         geometry = {"center_local": part("center_local"),
                     "edge_px": part("edge_px") if shapes["edge_px"] is not None else np.empty((n, 0))}
     elif not metrics_only:
@@ -424,7 +442,8 @@ def _peak_rows(img_d, sign, peak_min_distance):
 def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_angles, radial_step, fit_fraction,
                  background_level, background_tile, deblend_iterations, deblend_tolerance, pixel_size, unit, device,
                  metrics_only, summary_only, fit_precision="fp64", seeds="threshold", peak_min_distance=None,
-                 smooth_sigma=0.0, half_area_level=0.5, half_area_peak_pixels=4.0, outlines=True):
+                 smooth_sigma=0.0, half_area_level=0.5, half_area_peak_pixels=4.0, tail_area_level=0.2,
+                 tail_window=1.2, outlines=True):
     started = time.perf_counter()
     seconds = {}
     height, width = tuple(img.shape)
@@ -484,7 +503,8 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
             ids = ids[(ids >= 0) & (ids <= k)]
             flags[ids] = 0
             out = dev.empty((height, width), torch.uint8)
-            _lib.call("spx_label_mask", labels_d.data_ptr(), dev.upload(flags).data_ptr(), height, width, 2,
+            flags_d = dev.upload(flags)  # held until the launch is queued (an upload freed earlier could be reused)
+            _lib.call("spx_label_mask", labels_d.data_ptr(), flags_d.data_ptr(), height, width, 2,
                       out.data_ptr(), tmp8.data_ptr(), dev.stream_ptr())
             return out
 
@@ -640,13 +660,22 @@ def _measure_cds(img, *, methods, threshold, invert, area_min, area_max, pad, n_
                       outs.get(False), outs.get(True), ws.data_ptr(), ws.numel(), stream)
             launched(names)
     seconds["half_area"] = time.perf_counter() - t_half
+    tails = [m for m in methods if m in TAIL_AREA]
+    if tails and nr:
+        t_tail = time.perf_counter()
+        tail_bufs = _tail_areas(img_d, sign, state, c, report, report_d, pitch, tails, n_angles=n_angles,
+                                level=tail_area_level, peak_pixels=half_area_peak_pixels, window=tail_window,
+                                outlines=bool(outlines) and not metrics_only, metrics_only=metrics_only, meta=meta)
+        bufs.update(tail_bufs)
+        launched(tails)
+        seconds["tail_area"] = time.perf_counter() - t_tail
     for names, copies in pending:
         t0 = time.perf_counter()
         for name, (host, done) in zip(names, copies):
             done.synchronize()
             found[name] = _to_result(name, nr, bufs[name], host.numpy(), metrics_only, n_angles)
         key = names[0] if names[0] in ("gaussian", "projection") else "half_area" if names[0] in HALF_AREA \
-            else "radial"
+            else "tail_area" if names[0] in TAIL_AREA else "radial"
         seconds[key] = seconds.get(key, 0.0) + time.perf_counter() - t0
     seconds["gaussian"] = seconds.get("gaussian", 0.0) + t_gauss
     for name in methods:
@@ -725,6 +754,102 @@ def _mask_stack(c, report) -> np.ndarray:
     return (inside & (c.voronoi.to(torch.int64)[ys, xs] == rep[:, None, None])).cpu().numpy()
 
 
+_TAIL_CHUNK_BYTES = 512 * 2**20  # window arrays (float32 share + three byte masks) per chunk of holes
+
+
+def _method_out_rows(b: dict, start: int) -> _lib.MethodOut:
+    """A method's output struct shifted to row `start` (metrics stay column-major with the full stride)."""
+    def at(key):
+        t = b[key]
+        if t is None:
+            return None
+        return (t[:, start:] if key == "metrics" else t[start:]).data_ptr()
+
+    return _lib.MethodOut(at("centers"), at("contours"), at("status"), at("metrics"), at("center_local"),
+                          at("edge_px"), None, None, b["metrics"].shape[0], b["metrics"].shape[1])
+
+
+def _nanmedian_device(v: torch.Tensor) -> float:
+    """numpy's nanmedian of a device vector: the middle value, or the mean of the two middle ones."""
+    v = v[~torch.isnan(v)]
+    n = int(v.numel())
+    if n == 0:
+        return float("nan")
+    v = torch.sort(v).values
+    if n % 2:
+        return float(v[n // 2])
+    return float((v[n // 2 - 1] + v[n // 2]) / 2)
+
+
+def _tail_areas(img_d, sign, state, c, report, report_d, pitch, names, *, n_angles, level, peak_pixels, window,
+                outlines, metrics_only, meta):
+    """The tail family of the reported holes (subpx/_cpu/invariant_cd.py:1009-1068): windows of
+    ceil(window x pitch) px half-width holding each hole's share of the light (spx_wide_cells), then
+    spx_tail_area_cd on them, in chunks of holes; foot_area_ratio takes a second pass with the median
+    foot ratio of the first. Returns the methods' device buffers."""
+    nr = len(report)
+    # measure_invariant's pitch: the deblend's, else (fewer than two holes) the stack's larger side.
+    pitch_t = float(pitch) if np.isfinite(pitch) else float(max(c.hm, c.wm))
+    radius = int(np.ceil(window * pitch_t))
+    side = 2 * radius + 1
+    if side > 64:
+        raise NotImplementedError(f"tail windows of {side} px (tail_window x pitch): at most 64 px are supported")
+    params = state.params
+    good_amp = params[np.isfinite(params).all(axis=1), 0]
+    floor = 1e-3 * float(np.median(good_amp)) if good_amp.size else 1e-12
+    zy = _zoom_operator(side)
+    zx_t = zy.t().contiguous()  # one operator per axis (square windows)
+    big_px = side * side * _ZOOM_FACTOR * _ZOOM_FACTOR
+    n_top = min(max(1, int(round(peak_pixels * _ZOOM_FACTOR * _ZOOM_FACTOR))), big_px)
+    first = [m for m in names if m != "foot_area_ratio"]
+    if "foot_area_ratio" in names and "foot_area" not in first:
+        first.append("foot_area")
+    bufs = {m: _method_buffers(nr, n_angles, m, not metrics_only) for m in first + [m for m in names if m not in first]}
+    h, w = state.model.shape
+    n_all = c.n
+    cell_org = c.boxes[report_d.to(torch.int64), :2].contiguous()
+    chunk = max(1, min(nr, _TAIL_CHUNK_BYTES // (7 * side * side)))
+    ws_wide = dev.workspace(_lib.size("spx_wide_cells_workspace_bytes", n_all, chunk, h, w, pitch_t))
+    ws_tail = dev.workspace(_lib.size("spx_tail_area_workspace_bytes", side, _ZOOM_FACTOR, n_angles))
+    win_cells = dev.empty((chunk, side, side), torch.float32)
+    inside = dev.empty((chunk, side, side), torch.uint8)
+    level_px = dev.empty((chunk, side, side), torch.uint8)
+    territory = dev.empty((chunk, side, side), torch.uint8)
+    win_org = dev.empty((chunk, 2), torch.int32)
+    bg = state.background.struct()
+    stream = dev.stream_ptr()
+
+    def run(kinds, cuts=None):
+        for s0 in range(0, nr, chunk):
+            m = min(chunk, nr - s0)
+            _lib.call("spx_wide_cells", img_d.data_ptr(), dev.dtype_code(img_d), float(sign), h, w, bg,
+                      state.model.data_ptr(), state.params_d.data_ptr(), c.boxes.data_ptr(), n_all, c.hm, c.wm,
+                      report_d[s0:].data_ptr(), m, radius, pitch_t, floor, win_cells.data_ptr(), inside.data_ptr(),
+                      level_px.data_ptr(), territory.data_ptr(), win_org.data_ptr(), None, ws_wide.data_ptr(),
+                      ws_wide.numel(), stream)
+            outs = [(_method_out_rows(bufs[k][0], s0) if k in kinds else None)
+                    for k in ("tail_area", "tail_area_norm", "edge_area", "foot_area", "foot_area_ratio")]
+            _lib.call("spx_tail_area_cd", win_cells.data_ptr(), inside.data_ptr(), level_px.data_ptr(),
+                      territory.data_ptr(), win_org.data_ptr(), cell_org[s0:].data_ptr(), m, side, n_angles,
+                      zy.data_ptr(), zx_t.data_ptr(), _ZOOM_FACTOR, float(level), n_top, int(outlines),
+                      None if cuts is None else cuts[s0:].data_ptr(), *outs, ws_tail.data_ptr(), ws_tail.numel(),
+                      stream)
+
+    run(first)
+    meta["tail_window_px"] = int(side)
+    if "foot_area_ratio" in names:
+        fb = bufs["foot_area"][0]
+        cols = _metric_names("foot_area")
+        threshold = fb["metrics"][cols.index("threshold"), :nr]
+        steepest = fb["metrics"][cols.index("steepest_level"), :nr]
+        valid = fb["status"][:nr] == 0
+        ratio = _nanmedian_device((threshold / steepest)[valid])
+        meta["foot_ratio"] = ratio
+        cuts = (ratio * steepest).contiguous()
+        run(["foot_area_ratio"], cuts)
+    return {m: bufs[m][0] for m in names}
+
+
 def _empty_result(method, n_angles, metrics_only) -> CDMethodResult:
     names = _metric_names(method)
     geometry = {}
@@ -732,7 +857,7 @@ def _empty_result(method, n_angles, metrics_only) -> CDMethodResult:
         geometry = {"center_local": np.zeros((0, 2)), "eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}
     elif method in ("gradient", "halfmax"):
         geometry = {"center_local": np.zeros((0, 2)), "edge_px": np.zeros((0, n_angles))}
-    elif method == "projection" or method in HALF_AREA:
+    elif method == "projection" or method in AREA_METHODS:
         geometry = {"center_local": np.zeros((0, 2)), "edge_px": np.zeros((0, 0 if metrics_only else n_angles))}
     elif not metrics_only:
         geometry = {"eigenvalues": np.zeros((0, 2)), "axes": np.zeros((0, 2, 2))}

@@ -162,7 +162,7 @@ enum {
     // ellipse methods
     M_SIG_MAJ = 7, M_SIG_MIN = 8, M_FWHM_MAJ = 9, M_FWHM_MIN = 10, M_ANGLE = 11, M_RMSE = 12,
     // area methods
-    M_LOCAL_LEVEL = 7, M_THRESHOLD = 8, M_MEAN_SIGNAL = 9,
+    M_LOCAL_LEVEL = 7, M_THRESHOLD = 8, M_MEAN_SIGNAL = 9, M_STEEPEST = 10,
     // radial methods
     M_COVERAGE = 7
 };
@@ -1637,12 +1637,19 @@ struct HalfCtx {
     double* s_dbl;
 };
 
-// One output of the half_area family from the cell's enlargement: region above b + level x peak
-// around the highest pixel, its metrics and outline (see k_half_area).
-__device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, double peak, const HalfCtx& h,
-                            const CellView& c) {
+// Where an area output's positions go: centres and contours are the enlargement's local positions
+// plus (ox, oy); center_local is the local position itself, or with a finite lx the global centre
+// minus (lx, ly) (the tail windows report it relative to the hole's own cell).
+struct AreaPlace {
+    double ox, oy, lx, ly;
+};
+
+// One output of the area methods from the cell's enlargement: region above b + cut around the
+// highest pixel, its metrics and outline (see k_half_area); steepest (foot_area) goes to the
+// metric after mean_signal when the output has that column.
+__device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, double peak, double cut, double steepest,
+                            const HalfCtx& h, const AreaPlace& at) {
     const int tid = threadIdx.x, Hb = h.Hb, Wb = h.Wb, RW = h.RW;
-    const double cut = __dmul_rn(a.level, peak);
     const bool signal = peak > 0.0 && isfinite(cut) && cut < peak;
     const uint32_t last_bits = (Wb % 32) ? ((1u << (Wb % 32)) - 1u) : 0xffffffffu;
     const int lane = tid & 31;
@@ -1830,8 +1837,8 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
             }
             const double e = __dadd_rn(__dmul_rn((double)max(first_out - 1, 0), 0.125), 0.0625);
             if (out.edge_px) out.edge_px[(long long)i * a.n_angles + q] = e;
-            vx[q] = __dadd_rn(__dadd_rn(cxl, __dmul_rn(e, co)), (double)c.box.x);
-            vy[q] = __dadd_rn(__dadd_rn(cyl, __dmul_rn(e, si)), (double)c.box.y);
+            vx[q] = __dadd_rn(__dadd_rn(cxl, __dmul_rn(e, co)), at.ox);
+            vy[q] = __dadd_rn(__dadd_rn(cyl, __dmul_rn(e, si)), at.oy);
         }
         __syncthreads();
         if (tid == 0) {
@@ -1868,16 +1875,19 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
         m[M_LOCAL_LEVEL] = h.b;
         out.status[i] = (uint8_t)(!signal ? SPX_ST_NO_SIGNAL : touch ? SPX_ST_REGION_AT_CELL_BORDER : SPX_ST_OK);
         const double nan = dnan();
-        out.centers[2LL * i] = signal ? __dadd_rn(cxl, (double)c.box.x) : nan;
-        out.centers[2LL * i + 1] = signal ? __dadd_rn(cyl, (double)c.box.y) : nan;
+        const double gcx = __dadd_rn(cxl, at.ox), gcy = __dadd_rn(cyl, at.oy);
+        out.centers[2LL * i] = signal ? gcx : nan;
+        out.centers[2LL * i + 1] = signal ? gcy : nan;
         if (out.center_local) {
-            out.center_local[2LL * i] = signal ? cxl : nan;
-            out.center_local[2LL * i + 1] = signal ? cyl : nan;
+            const bool rel = isfinite(at.lx);
+            out.center_local[2LL * i] = signal ? (rel ? __dsub_rn(gcx, at.lx) : cxl) : nan;
+            out.center_local[2LL * i + 1] = signal ? (rel ? __dsub_rn(gcy, at.ly) : cyl) : nan;
         }
         if (signal) {
             m[M_PEAK] = peak;
             m[M_THRESHOLD] = __dadd_rn(h.b, cut);
             m[M_MEAN_SIGNAL] = mean_signal;
+            if (out.n_metrics > M_STEEPEST) m[M_STEEPEST] = steepest;
         }
         if (ok) {
             const double area = __dmul_rn((double)count, __dmul_rn(sx, sy));
@@ -2088,7 +2098,8 @@ __global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
         __syncthreads();
         HalfCtx ctx{mask, big, bmask, above, reg, reg2, rowcnt, colcnt, tmp, leafsum, leaf_lo, leaf_len, n_leaves,
                     Hb, Wb, RW, N, b, top, s_int, s_dbl};
-        if (a.single.status) half_output(a, a.single, i, top_v, ctx, c);
+        const AreaPlace at{(double)c.box.x, (double)c.box.y, dnan(), dnan()};
+        if (a.single.status) half_output(a, a.single, i, top_v, __dmul_rn(a.level, top_v), dnan(), ctx, at);
         if (a.averaged.status) {
             // Mean of the n_top highest enlarged pixels (outside the mask -inf): the n_top-th highest key
             // by the CTA select, then the keys above it and as many copies of it as are missing.
@@ -2127,7 +2138,388 @@ __global__ void __launch_bounds__(kHalfThreads) k_half_area(HalfArgs a) {
                 peak = isfinite(mean) ? mean : -1.0;
                 __syncthreads();
             }
-            half_output(a, a.averaged, i, peak, ctx, c);
+            half_output(a, a.averaged, i, peak, __dmul_rn(a.level, peak), dnan(), ctx, at);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ tail family
+
+// Two of numpy's pairwise sums over an enlargement's N sub-pixels in memory order (leaves of at most
+// 128 values with eight running sums each, then the tree), of val(Y, X, &v0, &v1); the results on
+// every thread. All threads call it.
+template <class F>
+__device__ void np_sums2(F&& val, int Wb, int N, const int* leaf_lo, const int* leaf_len, int n_leaves,
+                         double* leafsum, double* s_out, double* r0, double* r1) {
+    const int tid = threadIdx.x;
+    for (int L = tid; L < n_leaves; L += kHalfThreads) {
+        const int lo = leaf_lo[L], n = leaf_len[L];
+        int Y = lo / Wb, X = lo - Y * Wb;
+        auto next = [&](double* a, double* b) {
+            val(Y, X, a, b);
+            if (++X == Wb) {
+                X = 0;
+                ++Y;
+            }
+        };
+        double res0, res1;
+        if (n < 8) {
+            res0 = res1 = 0.0;
+            for (int q = 0; q < n; ++q) {
+                double a, b;
+                next(&a, &b);
+                res0 = __dadd_rn(res0, a);
+                res1 = __dadd_rn(res1, b);
+            }
+        } else {
+            double u[8], w[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) next(&u[j], &w[j]);
+            int q = 8;
+            for (; q < n - (n % 8); q += 8)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    double a, b;
+                    next(&a, &b);
+                    u[j] = __dadd_rn(u[j], a);
+                    w[j] = __dadd_rn(w[j], b);
+                }
+            res0 = __dadd_rn(__dadd_rn(__dadd_rn(u[0], u[1]), __dadd_rn(u[2], u[3])),
+                             __dadd_rn(__dadd_rn(u[4], u[5]), __dadd_rn(u[6], u[7])));
+            res1 = __dadd_rn(__dadd_rn(__dadd_rn(w[0], w[1]), __dadd_rn(w[2], w[3])),
+                             __dadd_rn(__dadd_rn(w[4], w[5]), __dadd_rn(w[6], w[7])));
+            for (; q < n; ++q) {
+                double a, b;
+                next(&a, &b);
+                res0 = __dadd_rn(res0, a);
+                res1 = __dadd_rn(res1, b);
+            }
+        }
+        leafsum[L] = res0;
+        leafsum[kHalfLeavesMax + L] = res1;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int next = 0;
+        s_out[0] = np_pairwise_tree(leafsum, N, &next);
+        next = 0;
+        s_out[1] = np_pairwise_tree(leafsum + kHalfLeavesMax, N, &next);
+    }
+    __syncthreads();
+    *r0 = s_out[0];
+    *r1 = s_out[1];
+    __syncthreads();
+}
+
+struct TailArgs {
+    HalfArgs h;              // factor, level, n_top, outlines, n_angles; hm = wm = the window side
+    const float* cells;      // (n, S, S) each hole's share of the light
+    const uint8_t* inside;   // (n, S, S) the window inside the image: the mask
+    const uint8_t* levelm;   // level pixels (tail_area's local level)
+    const uint8_t* zone;     // own territory (foot_area)
+    const int* win_org;      // (n, 2) window origins
+    const int* cell_org;     // (n, 2) the holes' own cell origins (center_local)
+    const double* zxT;       // (S, S f) the x zoom operator transposed
+    const double* cuts;      // (n) foot_area_ratio's thresholds
+    MethodOut med, norm, edge, foot, given;  // status null: not wanted
+};
+
+__host__ __device__ inline long long tail_smem_bytes(int S, int f, int n_angles) {
+    const long long Hb = (long long)S * f, RW = (Hb + 31) / 32, area = (long long)S * S;
+    const long long tmpn = 2 * Hb > 3LL * (n_angles + 1) ? 2 * Hb : 3LL * (n_angles + 1);
+    return (2 * area + 2 * kHalfLeavesMax + tmpn) * 8 + 5 * Hb * RW * 4 + (2 * Hb + 2 * kHalfLeavesMax) * 4 + 3 * area;
+}
+
+// The tail family on hole windows (subpx/_cpu/invariant_cd.py:551-875 with the windows of 878-964):
+// one CTA per window. Local level b: the median of the level pixels (tail_area) or none (the others,
+// which share one enlargement); the window minus b inside the image, enlarged f times by the host's
+// zoom operators (read from global memory: windows are up to 64 px); averaged peak; the threshold
+// per method: level x peak (tail_area, tail_area_norm), the steepness-weighted mean of the core
+// sub-pixels (edge_area), the curvature-weighted mean below the steepest level inside the territory
+// (foot_area), or given (foot_area_ratio). The region, its metrics and outline as the half_area
+// family; positions in the image, center_local relative to the hole's own cell.
+__global__ void __launch_bounds__(kHalfThreads) k_tail_area(TailArgs t) {
+    extern __shared__ double hsm[];
+    __shared__ int hist[2048];
+    __shared__ int warp_tot[32], s_pick[3];
+    __shared__ unsigned long long s_keys[2], s_kmin, s_kmax;
+    __shared__ double s_red[2 * (kHalfThreads / 32)];
+    __shared__ int s_ired[kHalfThreads / 32];
+    __shared__ int s_int[4];
+    __shared__ double s_dbl[8];
+    const HalfArgs& a = t.h;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int S = a.hm, f = a.factor;
+    const int Hb = S * f, Wb = Hb, RW = (Wb + 31) / 32, N = Hb * Wb, area = S * S;
+    const int tmpn = max(2 * Hb, 3 * (a.n_angles + 1));
+    double* cell = hsm;
+    double* lv = cell + area;
+    double* leafsum = lv + area;
+    double* tmp = leafsum + 2 * kHalfLeavesMax;
+    uint32_t* bmask = reinterpret_cast<uint32_t*>(tmp + tmpn);
+    uint32_t* above = bmask + Hb * RW;
+    uint32_t* reg = above + Hb * RW;
+    uint32_t* reg2 = reg + Hb * RW;
+    uint32_t* zplane = reg2 + Hb * RW;
+    int* rowcnt = reinterpret_cast<int*>(zplane + Hb * RW);
+    int* colcnt = rowcnt + Hb;
+    int* leaf_lo = colcnt + Wb;
+    int* leaf_len = leaf_lo + kHalfLeavesMax;
+    uint8_t* mask = reinterpret_cast<uint8_t*>(leaf_len + kHalfLeavesMax);
+    uint8_t* lmask = mask + area;
+    uint8_t* zmask = lmask + area;
+    double* big = a.scratch + (long long)blockIdx.x * ((long long)N + (long long)Hb * S);
+    double* T = big + N;
+    if (tid == 0) s_int[3] = np_pairwise_leaves(0, N, leaf_lo, leaf_len, 0);
+    __syncthreads();
+    const int n_leaves = s_int[3];
+    const bool want_zero = t.norm.status || t.edge.status || t.foot.status || t.given.status;
+    const double sy = 1.0 / f;
+    const double den_g = __dmul_rn((double)(2 * f), sy);  // 2 d sy: central differences over +-d
+    const double den_c = __dmul_rn(__dmul_rn((double)f, sy), __dmul_rn((double)f, sy));  // (d sy)^2
+    auto bit = [&](const uint32_t* p, int Y, int X) { return (p[Y * RW + (X >> 5)] >> (X & 31)) & 1u; };
+    for (int i = blockIdx.x; i < a.n; i += gridDim.x) {
+        __syncthreads();  // the previous window's shared-memory reads are done
+        const long long base = (long long)i * area;
+        for (int k = tid; k < area; k += kHalfThreads) {
+            const bool m = t.inside[base + k];
+            mask[k] = m;
+            cell[k] = m ? (double)t.cells[base + k] : 0.0;
+            lmask[k] = t.levelm ? t.levelm[base + k] : 0;
+            zmask[k] = t.zone ? t.zone[base + k] : 1;
+        }
+        __syncthreads();
+        for (int w = warp; w < Hb * RW; w += kHalfThreads / 32) {
+            const int Y = w / RW, X = (w % RW) * 32 + lane;
+            const int src = (Y / f) * S + X / f;
+            const uint32_t mw = __ballot_sync(0xffffffffu, X < Wb && mask[src]);
+            const uint32_t zw = __ballot_sync(0xffffffffu, X < Wb && zmask[src]);
+            if (lane == 0) {
+                bmask[w] = mw;
+                zplane[w] = zw;
+            }
+        }
+        const AreaPlace at{(double)t.win_org[2LL * i], (double)t.win_org[2LL * i + 1],
+                           (double)t.cell_org[2LL * i], (double)t.cell_org[2LL * i + 1]};
+        for (int kind = 0; kind < 2; ++kind) {
+            if (kind == 0 ? !t.med.status : !want_zero) continue;
+            double b = 0.0;
+            if (kind == 0) {
+                // nanmedian of the level pixels inside the window (ranks, ties by position; NaN if none).
+                if (tid == 0) s_int[0] = 0;
+                __syncthreads();
+                for (int k = tid; k < area; k += kHalfThreads)
+                    if (mask[k] && lmask[k]) lv[atomicAdd(&s_int[0], 1)] = cell[k];
+                __syncthreads();
+                const int r = s_int[0], k1 = (r - 1) / 2, k2 = r / 2;
+                for (int q0 = tid; q0 < r; q0 += kHalfThreads) {
+                    const double v = lv[q0];
+                    int rank = 0;
+                    for (int q = 0; q < r; ++q) rank += lv[q] < v || (lv[q] == v && q < q0);
+                    if (rank == k1) s_dbl[0] = v;
+                    if (rank == k2) s_dbl[1] = v;
+                }
+                __syncthreads();
+                b = r ? __ddiv_rn(__dadd_rn(s_dbl[0], s_dbl[1]), 2.0) : dnan();
+                __syncthreads();
+            }
+            // T = Zy (window - b, zero outside the image) (Hb x S), then big = T Zx^T, -inf outside.
+            for (int q = tid; q < Hb * S; q += kHalfThreads) {
+                const int Y = q / S, x = q % S;
+                const double* zr = a.zy + (long long)Y * S;
+                double v = 0.0;
+                for (int y = 0; y < S; ++y) {
+                    const double c = mask[y * S + x] ? __dsub_rn(cell[y * S + x], b) : 0.0;
+                    v = __fma_rn(__ldg(zr + y), c, v);
+                }
+                T[q] = v;
+            }
+            __syncthreads();
+            for (int Y0 = 2 * warp; Y0 < Hb; Y0 += 2 * (kHalfThreads / 32))
+                for (int X0 = 0; X0 < Wb; X0 += 128) {
+                    const bool two = Y0 + 1 < Hb;
+                    double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+                    for (int x = 0; x < S; ++x) {
+                        const double t0 = T[(long long)Y0 * S + x], t1 = two ? T[(long long)(Y0 + 1) * S + x] : 0.0;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int X = X0 + lane + 32 * q;
+                            if (X < Wb) {
+                                const double z = __ldg(t.zxT + (long long)x * Wb + X);
+                                v0[q] = __fma_rn(t0, z, v0[q]);
+                                v1[q] = __fma_rn(t1, z, v1[q]);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int X = X0 + lane + 32 * q;
+                        if (X >= Wb) continue;
+                        big[(long long)Y0 * Wb + X] = bit(bmask, Y0, X) ? v0[q] : -INFINITY;
+                        if (two) big[(long long)(Y0 + 1) * Wb + X] = bit(bmask, Y0 + 1, X) ? v1[q] : -INFINITY;
+                    }
+                }
+            __syncthreads();
+            // Highest enlarged pixel (first on ties) and the key range for the averaged peak.
+            double best = -INFINITY;
+            int best_i = 0x7fffffff;
+            unsigned long long kmin = ~0ull, kmax = 0;
+            for (int q = tid; q < N; q += kHalfThreads) {
+                const double v = big[q];
+                if (v > best || best_i == 0x7fffffff) {
+                    best = v;
+                    best_i = q;
+                }
+                const unsigned long long key = order_key(v);
+                kmin = min(kmin, key);
+                kmax = max(kmax, key);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, best_i, o);
+                if (ob > best || (ob == best && oi < best_i)) {
+                    best = ob;
+                    best_i = oi;
+                }
+            }
+            kmin = warp_min_u64(kmin);
+            kmax = warp_max_u64(kmax);
+            if (lane == 0) {
+                s_red[warp] = best;
+                s_ired[warp] = best_i;
+            }
+            if (tid == 0) {
+                s_kmin = ~0ull;
+                s_kmax = 0;
+            }
+            __syncthreads();
+            if (lane == 0) {
+                atomicMin(&s_kmin, kmin);
+                atomicMax(&s_kmax, kmax);
+            }
+            __syncthreads();
+            double top_v = s_red[0];
+            int top = s_ired[0];
+            for (int q = 1; q < kHalfThreads / 32; ++q)
+                if (s_red[q] > top_v || (s_red[q] == top_v && s_ired[q] < top)) {
+                    top_v = s_red[q];
+                    top = s_ired[q];
+                }
+            if (top == 0x7fffffff) top = 0;
+            __syncthreads();
+            // Averaged peak: the mean of the n_top highest sub-pixels (-inf outside the mask).
+            double peak = -1.0;
+            if (a.n_top <= N) {
+                auto for_keys = [&](auto&& fn) {
+                    for (int q = tid; q < N; q += kHalfThreads) fn(order_key(big[q]));
+                };
+                unsigned long long kth, kth2;
+                cta_select<kHalfThreads>(for_keys, N - a.n_top, false, s_kmin, s_kmax, hist, warp_tot, s_pick, s_keys,
+                                         &kth, &kth2);
+                double sum = 0.0;
+                int cnt = 0;
+                for_keys([&](unsigned long long key) {
+                    if (key > kth) {
+                        sum += key_value(key);
+                        ++cnt;
+                    }
+                });
+                sum = warp_sum(sum);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+                if (lane == 0) {
+                    s_red[warp] = sum;
+                    s_ired[warp] = cnt;
+                }
+                __syncthreads();
+                double total = 0.0;
+                int above_cnt = 0;
+                for (int q = 0; q < kHalfThreads / 32; ++q) {
+                    total += s_red[q];
+                    above_cnt += s_ired[q];
+                }
+                total += (double)(a.n_top - above_cnt) * key_value(kth);
+                const double mean = total / a.n_top;
+                peak = isfinite(mean) ? mean : -1.0;
+                __syncthreads();
+            }
+            HalfCtx ctx{mask, big, bmask, above, reg, reg2, rowcnt, colcnt, tmp, leafsum, leaf_lo, leaf_len, n_leaves,
+                        Hb, Wb, RW, N, b, top, s_int, s_dbl};
+            if (kind == 0) {
+                half_output(a, t.med, i, peak, __dmul_rn(a.level, peak), dnan(), ctx, at);
+                continue;
+            }
+            if (t.norm.status) half_output(a, t.norm, i, peak, __dmul_rn(a.level, peak), dnan(), ctx, at);
+            // Core sub-pixels: inside the enlarged mask with their +-f stencil, none within f of the edge.
+            auto core = [&](int Y, int X, bool zoned) {
+                if (Y < f || Y >= Hb - f || X < f || X >= Wb - f) return false;
+                if (!(bit(bmask, Y, X) && bit(bmask, Y - f, X) && bit(bmask, Y + f, X) && bit(bmask, Y, X - f) &&
+                      bit(bmask, Y, X + f)))
+                    return false;
+                return !zoned || bit(zplane, Y, X) != 0u;
+            };
+            auto steep_at = [&](int Y, int X) {
+                const double* r = big + (long long)Y * Wb + X;
+                const double gy = __ddiv_rn(__dsub_rn(r[(long long)f * Wb], r[-(long long)f * Wb]), den_g);
+                const double gx = __ddiv_rn(__dsub_rn(r[f], r[-f]), den_g);
+                return sqrt(__dadd_rn(__dmul_rn(gy, gy), __dmul_rn(gx, gx)));
+            };
+            if (t.edge.status) {
+                double total, num;
+                np_sums2(
+                    [&](int Y, int X, double* w, double* wb) {
+                        if (core(Y, X, false)) {
+                            const double s = steep_at(Y, X);
+                            *w = s;
+                            *wb = __dmul_rn(s, big[(long long)Y * Wb + X]);
+                        } else {
+                            *w = 0.0;
+                            *wb = 0.0;
+                        }
+                    },
+                    Wb, N, leaf_lo, leaf_len, n_leaves, leafsum, s_dbl + 4, &total, &num);
+                const double cut = total > 0.0 ? __ddiv_rn(num, total) : INFINITY;
+                half_output(a, t.edge, i, peak, cut, dnan(), ctx, at);
+            }
+            if (t.foot.status) {
+                const bool zoned = t.zone != nullptr;
+                double total, num;
+                np_sums2(
+                    [&](int Y, int X, double* w, double* wb) {
+                        if (core(Y, X, zoned)) {
+                            const double s = steep_at(Y, X);
+                            *w = s;
+                            *wb = __dmul_rn(s, big[(long long)Y * Wb + X]);
+                        } else {
+                            *w = 0.0;
+                            *wb = 0.0;
+                        }
+                    },
+                    Wb, N, leaf_lo, leaf_len, n_leaves, leafsum, s_dbl + 4, &total, &num);
+                const double steepest = __ddiv_rn(num, total > 0.0 ? total : 1.0);
+                double bend, num2;
+                np_sums2(
+                    [&](int Y, int X, double* c, double* cb) {
+                        const double v = big[(long long)Y * Wb + X];
+                        if (core(Y, X, zoned) && v < steepest) {
+                            const double* r = big + (long long)Y * Wb + X;
+                            const double v2 = __dmul_rn(2.0, v);
+                            const double cy = __ddiv_rn(__dsub_rn(__dadd_rn(r[(long long)f * Wb], r[-(long long)f * Wb]), v2), den_c);
+                            const double cx = __ddiv_rn(__dsub_rn(__dadd_rn(r[f], r[-f]), v2), den_c);
+                            const double curve = __dadd_rn(cy, cx);
+                            *c = curve;
+                            *cb = __dmul_rn(curve, v);
+                        } else {
+                            *c = 0.0;
+                            *cb = 0.0;
+                        }
+                    },
+                    Wb, N, leaf_lo, leaf_len, n_leaves, leafsum, s_dbl + 4, &bend, &num2);
+                const double cut = total > 0.0 && bend > 0.0 ? __ddiv_rn(num2, bend) : INFINITY;
+                half_output(a, t.foot, i, peak, cut, steepest, ctx, at);
+            }
+            if (t.given.status) half_output(a, t.given, i, peak, t.cuts[i], dnan(), ctx, at);
         }
     }
 }
@@ -2279,6 +2671,58 @@ int spx_half_area_cd(const double* cleaned, const int* voronoi, const int* boxes
     if (!averaged) a.averaged.status = nullptr;
     k_half_area<<<std::min(n, kHalfCtas), kHalfThreads, smem, static_cast<cudaStream_t>(stream)>>>(a);
     return check_launch("k_half_area");
+}
+
+// Persistent CTAs of the tail kernel (each with its own enlargement scratch): up to four per SM as
+// its shared memory allows.
+static int tail_ctas(int side, int factor, int n_angles) {
+    const size_t smem = (size_t)tail_smem_bytes(side, factor, n_angles);
+    if (smem > 48 * 1024)
+        if (cudaFuncSetAttribute(k_tail_area, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return 0;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tail_area, kHalfThreads, smem) != cudaSuccess) return 0;
+    return 148 * std::min(std::max(per_sm, 1), 4);
+}
+
+size_t spx_tail_area_workspace_bytes(int side, int factor, int n_angles) {
+    if (side < 1 || factor < 1 || n_angles < 1) return 0;
+    const long long Hb = (long long)side * factor;
+    return (size_t)(148LL * 4 * (Hb * Hb + Hb * side) * sizeof(double) + 256);
+}
+
+int spx_tail_area_cd(const float* cells, const uint8_t* inside, const uint8_t* level_pixels, const uint8_t* territory,
+                     const int* window_origins, const int* cell_origins, int n, int side, int n_angles,
+                     const double* zoom_y, const double* zoom_x_t, int factor, double level, int n_top, int outlines,
+                     const double* cuts, const spx_method_out* tail, const spx_method_out* norm,
+                     const spx_method_out* edge, const spx_method_out* foot, const spx_method_out* given,
+                     void* workspace, size_t workspace_bytes, void* stream) {
+    SPX_REQUIRE(n >= 0 && n_angles >= 1 && side >= 1 && factor >= 1 && n_top >= 1, "bad arguments");
+    SPX_REQUIRE(level > 0.0 && level < 1.0, "level must be between 0 and 1");
+    if (n == 0) return SPX_OK;
+    SPX_REQUIRE(cells && inside && window_origins && cell_origins && zoom_y && zoom_x_t && workspace &&
+                    (tail || norm || edge || foot || given),
+                "null pointer");
+    SPX_REQUIRE(!tail || level_pixels, "tail_area needs the level pixels");
+    SPX_REQUIRE(!given || cuts, "foot_area_ratio needs its thresholds");
+    for (const spx_method_out* o : {tail, norm, edge, given})
+        if (o) SPX_REQUIRE(o->centers && o->status && o->metrics && o->n_metrics >= 10, "null pointer or too few metric columns");
+    if (foot) SPX_REQUIRE(foot->centers && foot->status && foot->metrics && foot->n_metrics >= 11,
+                          "null pointer or too few metric columns");
+    // numpy's pairwise-sum leaves (at least 64 values each) of up to 65536 sub-pixels fit kHalfLeavesMax.
+    SPX_REQUIRE((long long)side * factor * side * factor <= 65536, "tail window too large for the tail kernel");
+    SPX_REQUIRE(tail_smem_bytes(side, factor, n_angles) <= 200 * 1024, "tail window too large for the tail kernel");
+    SPX_REQUIRE(workspace_bytes >= spx_tail_area_workspace_bytes(side, factor, n_angles), "workspace too small");
+    const int ctas = tail_ctas(side, factor, n_angles);
+    SPX_REQUIRE(ctas > 0, "tail kernel launch configuration failed");
+    const uintptr_t base = (reinterpret_cast<uintptr_t>(workspace) + 255) & ~(uintptr_t)255;
+    HalfArgs h{nullptr, nullptr, nullptr, nullptr, n, side, side, 0, n_angles, zoom_y, nullptr, factor, level, 0, n_top,
+               outlines, reinterpret_cast<double*>(base), method_out(nullptr), method_out(nullptr)};
+    TailArgs t{h, cells, inside, level_pixels, territory, window_origins, cell_origins, zoom_x_t, cuts,
+               method_out(tail), method_out(norm), method_out(edge), method_out(foot), method_out(given)};
+    const size_t smem = (size_t)tail_smem_bytes(side, factor, n_angles);
+    k_tail_area<<<std::min(n, ctas), kHalfThreads, smem, static_cast<cudaStream_t>(stream)>>>(t);
+    return check_launch("k_tail_area");
 }
 
 // Shared memory of one radial CTA, or 0 when it does not fit and the CTAs use global scratch.

@@ -14,6 +14,7 @@
 // so it is deterministic without atomics.
 
 #include "bins.cuh"
+#include "image.cuh"
 #include "lm.cuh"
 #include "select.cuh"
 
@@ -23,28 +24,6 @@ namespace {
 constexpr int kFitWarpsMax = 8;  // largest tuning().fit_warps (sizes the global staging fallback)
 // Static shared memory of the fit kernels: two 27-double LM sum slots per warp.
 constexpr int kLmSlotBytes = kFitWarpsMax * 54 * (int)sizeof(double);
-
-// Background map: bg(y, x) = (1 - t[y]) rows[j1[y]-1][x] + t[y] rows[j1[y]][x] (ny > 1),
-// rows[0][x] (ny == 1), or a constant.
-__device__ __forceinline__ double bg_at(const spx_bgmap& m, int y, int x) {
-    if (m.mode == SPX_BG_FIXED) return m.fixed;
-    if (m.ny == 1) return m.rows[x];
-    const int j = m.j1[y];
-    const double t = m.t[y];
-    return __dadd_rn(__dmul_rn(__dsub_rn(1.0, t), m.rows[(long long)(j - 1) * m.width + x]),
-                     __dmul_rn(t, m.rows[(long long)j * m.width + x]));
-}
-
-struct Image {
-    const void* data;
-    int dtype;
-    double sign;
-    int H, W;
-    __device__ __forceinline__ double at(int y, int x) const {
-        const double v = load_px(data, dtype, (long long)y * W + x);
-        return sign < 0 ? -v : v;
-    }
-};
 
 __device__ __forceinline__ int render_radius(const double* p, int cap) {
     double r = ceil(4.0 * sigma_major(p));

@@ -475,6 +475,40 @@ int spx_half_area_cd(const double* cleaned, const int* voronoi, const int* boxes
                      int wm, int width, int n_angles, const double* zoom_y, const double* zoom_x, int factor,
                      double level, int median, int n_top, int outlines, const spx_method_out* single,
                      const spx_method_out* averaged, void* workspace, size_t workspace_bytes, void* stream);
+/* Windows of the tail family (subpx/_cpu/invariant_cd.py:878-964, _wide_cells; replaces its CPU
+ * branch and subpx/_gpu/windows.py wide_cells): for each reported hole rows[i] (of n_all modelled holes
+ * with ROI-local Gaussian params (n_all, 6) and cell boxes (n_all, 4) of an hm x wm stack) the
+ * (2 radius + 1)^2 window around its rounded fitted centre (box centre when not finite): cells =
+ * float32((sign img - background) x own model / (model + floor)) inside the image, 0 outside; inside;
+ * territory = inside and no farther from the hole than from its 8 nearest modelled holes (ties in
+ * distance to the lower index; neighbours found in buckets of `bucket` px); level = the territory
+ * pixels at or beyond the keep-th largest distance, keep = clip(max(count // 10, 4), 1, area) - 1;
+ * origins = window origins (x, y). neighbours_out (optional, (n_rep, 9) ints) receives each row's hole
+ * and its neighbours (-1 where fewer). 2 radius + 1 <= 64; workspace: spx_wide_cells_workspace_bytes. */
+size_t spx_wide_cells_workspace_bytes(int n_all, int n_rep, int height, int width, double bucket);
+int spx_wide_cells(const void* img, int dtype, double sign, int height, int width, const spx_bgmap* background,
+                   const double* model, const double* params, const int* boxes, int n_all, int hm, int wm,
+                   const int* rows, int n_rep, int radius, double bucket, double floor, float* cells, uint8_t* inside,
+                   uint8_t* level, uint8_t* territory, int* origins, int* neighbours_out, void* workspace,
+                   size_t workspace_bytes, void* stream);
+/* The tail family on those windows (subpx/_cpu/invariant_cd.py:551-875 with measure_invariant's
+ * tail branch 1009-1068): per window the local level (tail: median of the level pixels inside the
+ * window; the others none), the window minus it enlarged factor times by zoom_y ((side factor) x side)
+ * and zoom_x_t (side x (side factor), the x operator transposed), the averaged peak (n_top highest
+ * sub-pixels), and the threshold: level x peak (tail = tail_area, norm = tail_area_norm), the
+ * steepness-weighted mean of the core sub-pixels (edge = edge_area), the curvature-weighted mean below
+ * the steepest level inside the territory (foot = foot_area; its steepest level in metric column 10,
+ * n_metrics >= 11), or cuts[i] (given = foot_area_ratio). Region, metrics (columns 7-9: local_level,
+ * threshold, mean_signal) and outline as spx_half_area_cd; centres and contours in image pixels,
+ * center_local relative to cell_origins. Outputs may be null; (side factor)^2 <= 65536; workspace:
+ * spx_tail_area_workspace_bytes. */
+size_t spx_tail_area_workspace_bytes(int side, int factor, int n_angles);
+int spx_tail_area_cd(const float* cells, const uint8_t* inside, const uint8_t* level_pixels, const uint8_t* territory,
+                     const int* window_origins, const int* cell_origins, int n, int side, int n_angles,
+                     const double* zoom_y, const double* zoom_x_t, int factor, double level, int n_top, int outlines,
+                     const double* cuts, const spx_method_out* tail, const spx_method_out* norm,
+                     const spx_method_out* edge, const spx_method_out* foot, const spx_method_out* given,
+                     void* workspace, size_t workspace_bytes, void* stream);
 size_t spx_radial_workspace_bytes(int hm, int wm, int smooth);
 /* Cubic-spline radial profiles; half-height crossings (halfmax) and gradient maxima (gradient).
  * Either output may be null. smooth_weights (device, 2 smooth_radius + 1 symmetric Gaussian
