@@ -712,6 +712,7 @@ __device__ __forceinline__ int floor_nonneg(double y, double* fl) {
 
 constexpr int kRadialThreads = 128;
 constexpr int kTrigMax = 256;  // ray angles with a cos / sin table in shared memory (4 KB)
+constexpr int kRewalkQueue = 64;  // rays per cell queued for the warps' FP64 re-walk
 
 // Shared (or scratch) memory of one radial CTA, in doubles: the FP64 spline coefficient plane, the
 // FP32 sampling windows, a reduction area, then the cell mask and the eroded mask as bytes.
@@ -917,6 +918,104 @@ __device__ __noinline__ void ray_fp64(const double* coef, int hp, int wp, int dp
     if (want_g) *edge_g = eg;
 }
 
+// ray_fp64 by one warp: the lanes take 32 consecutive samples at a time into `buf` (the warp's part of
+// the CTA's FP32 window rows, free once every ray's FP32 walk is done), then find the first
+// half-height crossing by ballot and the first maximum of the outward decrease by a warp reduction
+// (largest value, lowest index), with ray_fp64's arithmetic. Returns false (nothing written) when the
+// valid samples do not fit `cap`; the caller then walks the ray on one thread.
+__device__ __noinline__ bool ray_fp64_warp(const double* coef, int hp, int wp, int dp, const uint8_t* emask, int hm,
+                                           int wm, double cx, double cy, double ux, double uy, double step,
+                                           int n_radii, int j_min, double peak, bool want_h, bool want_g,
+                                           double* buf, int cap, double* edge_h, double* edge_g) {
+    const int lane = threadIdx.x & 31;
+    const double half = peak / 2.0, two_step = 2.0 * step;
+    const double ymax = (double)(hm - 1), xmax = (double)(wm - 1);
+    int first_invalid = n_radii;
+    for (int base = 0; base < n_radii; base += 32) {
+        const int k = base + lane;
+        bool valid = false;
+        double x = 0.0, y = 0.0;
+        if (k < n_radii) {
+            const double r = (double)k * step;
+            x = __dadd_rn(cx, __dmul_rn(ux, r));
+            y = __dadd_rn(cy, __dmul_rn(uy, r));
+            if (y >= 0.0 && y <= ymax && x >= 0.0 && x <= xmax) {
+                double fyd, fxd;
+                const int iy = floor_nonneg(y, &fyd), ix = floor_nonneg(x, &fxd);
+                const uint8_t* q = emask + iy * wm + ix;
+                const bool full4 = iy + 1 < hm && ix + 1 < wm && q[0] && q[1] && q[wm] && q[wm + 1];
+                valid = full4 || inside_bytes(emask, hm, wm, y, x);
+            }
+        }
+        const unsigned bad = __ballot_sync(0xffffffffu, !valid);
+        const int stop = bad ? base + __ffs(bad) - 1 : n_radii;
+        if (min(stop, base + 32) > cap) return false;  // this chunk's valid samples do not fit
+        if (valid && k < stop) buf[k] = k == 0 ? peak : cubic_at(coef, hp, wp, dp, y + kPad, x + kPad);
+        if (bad) {
+            first_invalid = min(stop, n_radii);
+            break;
+        }
+    }
+    __syncwarp();
+    if (want_h) {
+        double e = dnan();
+        for (int base = 1; base < first_invalid; base += 32) {
+            const int k = base + lane;
+            const bool cross = k < first_invalid && buf[k - 1] >= half && buf[k] < half;
+            const unsigned hit = __ballot_sync(0xffffffffu, cross);
+            if (hit) {
+                const int kc = base + __ffs(hit) - 1;
+                const double p1 = buf[kc - 1], pk = buf[kc];
+                e = __dadd_rn((double)(kc - 1) * step, __dmul_rn(__ddiv_rn(__dsub_rn(p1, half), __dsub_rn(p1, pk)), step));
+                break;
+            }
+        }
+        *edge_h = e;
+    }
+    if (want_g) {
+        // Candidates j: j >= max(j_min, 1), j <= n_radii - 3 and sample j + 2 valid.
+        const int jlo = max(j_min, 1), jhi = min(n_radii - 3, first_invalid - 3);
+        double best = -INFINITY;
+        int best_j = 0x7fffffff;
+        for (int j = jlo + lane; j <= jhi; j += 32) {
+            const double g = -__ddiv_rn(__dsub_rn(buf[j + 1], buf[j - 1]), two_step);
+            if (g > best) {
+                best = g;
+                best_j = j;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int oj = __shfl_xor_sync(0xffffffffu, best_j, o);
+            if (ob > best || (ob == best && oj < best_j)) {
+                best = ob;
+                best_j = oj;
+            }
+        }
+        double e = dnan();
+        if (best_j != 0x7fffffff) {
+            const int j = best_j;
+            const bool left_ok = j - 1 >= j_min;
+            const bool right_ok = j + 1 <= n_radii - 3 && j + 3 < first_invalid;
+            if (left_ok && right_ok) {
+                const double bl = -__ddiv_rn(__dsub_rn(buf[j], buf[j - 2]), two_step);
+                const double bm = best;
+                const double br = -__ddiv_rn(__dsub_rn(buf[j + 2], buf[j]), two_step);
+                const double curv = __dadd_rn(__dsub_rn(bl, __dmul_rn(2.0, bm)), br);
+                if (bm >= bl && bm >= br && bm > __dmul_rn(0.01, peak) && curv < -1e-12) {
+                    double delta = __ddiv_rn(__dmul_rn(0.5, __dsub_rn(bl, br)), curv);
+                    delta = delta < -0.5 ? -0.5 : (delta > 0.5 ? 0.5 : delta);
+                    e = __dadd_rn((double)j * step, __dmul_rn(delta, step));
+                }
+            }
+        }
+        *edge_g = e;
+    }
+    __syncwarp();
+    return true;
+}
+
 // The edges of one ray from FP64 samples (scipy's order-3 evaluation of the FP64 coefficient plane)
 // at the places the FP32 walk found, with the reference's arithmetic (subpx/_cpu/cd.py:220-264):
 // * kc > 0: the half-height crossing between samples kc - 1 and kc (the walk has checked that no
@@ -1038,7 +1137,8 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
     MethodOut half_out, MethodOut grad_out) {
     extern __shared__ double sm[];
     __shared__ double trig_tab[2 * kTrigMax];  // cos, sin of the ray angles (n_angles <= kTrigMax)
-    const int tid = threadIdx.x, warp = tid >> 5;
+    __shared__ int s_queue[kRewalkQueue], s_nq;  // rays to walk again in FP64, by warps
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int hp = hm + 2 * kPad, wp = wm + 2 * kPad, dp = radial_pitch(wm), area_px = hm * wm;
     const double* trig = n_angles <= kTrigMax ? trig_tab : nullptr;
     if (trig)
@@ -1156,6 +1256,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         // The window weights are non-negative and sum to one per axis, so an FP32 sample is within about
         // 45 ulps of cmax of the FP64 one (coefficient, offset and weight roundings, 20 FMAs); tol keeps
         // a margin of nearly 3 (2^-17 cmax). Also orders the quad writes before the rays read them.
+        if (tid == 0) s_nq = 0;  // before the barrier in cta_max; read after the barrier that follows the rays
         const float tol = (float)cta_max((double)cmax, red + 28) * 7.62939453125e-06f;
         const double half = peak / 2.0;
         int j_min = 2;  // first gradient candidate: j >= 2 and j * step >= thr
@@ -1163,6 +1264,7 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
         int found_h = 0, found_g = 0;
         for (int ray = tid; ray < n_angles; ray += kRadialThreads) {
             double edge_h = dnan(), edge_g = dnan();
+            bool pend_h = false, pend_g = false;  // queued for the warps' FP64 re-walk
             if (peak > 0.0) {
                 const double ang = (double)ray * (2.0 * kPi / n_angles);
                 const double ux = trig ? trig[2 * ray] : cos(ang), uy = trig ? trig[2 * ray + 1] : sin(ang);
@@ -1238,14 +1340,57 @@ __global__ void __launch_bounds__(kRadialThreads, 6) k_radial_cd(
                 if (fix_kc > 0 || fix_j >= 0)
                     ray_edges64(coef, hp, wp, dp, cx, cy, ux, uy, radial_step, peak, fix_kc, fix_j, j_min, n_radii,
                                 first_invalid, &edge_h, &edge_g);
-                if (redo_h || redo_g)
-                    ray_fp64(coef, hp, wp, dp, emask, hm, wm, cx, cy, ux, uy, radial_step, n_radii, j_min, peak,
-                             redo_h, redo_g, &edge_h, &edge_g);
+                if (redo_h || redo_g) {
+                    // Queued for a warp after the ray loop, or walked here when the queue is full.
+                    const int slot = atomicAdd(&s_nq, 1);
+                    if (slot < kRewalkQueue) {
+                        s_queue[slot] = ray | (redo_h ? 1 << 16 : 0) | (redo_g ? 1 << 17 : 0);
+                        pend_h = redo_h;
+                        pend_g = redo_g;
+                    } else {
+                        ray_fp64(coef, hp, wp, dp, emask, hm, wm, cx, cy, ux, uy, radial_step, n_radii, j_min, peak,
+                                 redo_h, redo_g, &edge_h, &edge_g);
+                    }
+                }
             }
-            if (half_out.status) half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
-            if (grad_out.status) grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
-            found_h += isfinite(edge_h);
-            found_g += isfinite(edge_g);
+            if (half_out.status && !pend_h) {
+                half_out.edge_px[(long long)i * n_angles + ray] = edge_h;
+                found_h += isfinite(edge_h);
+            }
+            if (grad_out.status && !pend_g) {
+                grad_out.edge_px[(long long)i * n_angles + ray] = edge_g;
+                found_g += isfinite(edge_g);
+            }
+        }
+        // The queued rays, one warp each, 32 FP64 samples at a time (the FP32 window rows are free now).
+        __syncthreads();
+        const int nq = min(s_nq, kRewalkQueue);
+        if (nq > 0) {
+            const int cap = (int)(2LL * (hm + 3) * wm / (kRadialThreads / 32));
+            double* buf = reinterpret_cast<double*>(quad) + (long long)warp * cap;
+            for (int q = warp; q < nq; q += kRadialThreads / 32) {
+                const int e = s_queue[q], ray = e & 0xffff;
+                const bool wh = (e >> 16) & 1, wg = (e >> 17) & 1;
+                const double ang = (double)ray * (2.0 * kPi / n_angles);
+                const double ux = trig ? trig[2 * ray] : cos(ang), uy = trig ? trig[2 * ray + 1] : sin(ang);
+                double eh = dnan(), eg = dnan();
+                if (!ray_fp64_warp(coef, hp, wp, dp, emask, hm, wm, cx, cy, ux, uy, radial_step, n_radii, j_min, peak,
+                                   wh, wg, buf, cap, &eh, &eg)) {
+                    if (lane == 0)
+                        ray_fp64(coef, hp, wp, dp, emask, hm, wm, cx, cy, ux, uy, radial_step, n_radii, j_min, peak,
+                                 wh, wg, &eh, &eg);
+                }
+                if (lane == 0) {
+                    if (wh) {
+                        half_out.edge_px[(long long)i * n_angles + ray] = eh;
+                        found_h += isfinite(eh);
+                    }
+                    if (wg) {
+                        grad_out.edge_px[(long long)i * n_angles + ray] = eg;
+                        found_g += isfinite(eg);
+                    }
+                }
+            }
         }
         const int all_h = (int)cta_sum((double)found_h, red + 20);
         const int all_g = (int)cta_sum((double)found_g, red + 24);  // also orders the edge writes
