@@ -2369,10 +2369,20 @@ struct TailArgs {
     MethodOut med, norm, edge, foot, given;  // status null: not wanted
 };
 
+// Shared memory of a tail CTA: the window (doubles), leaf sums and small arrays, five bit planes,
+// row / column counts, the three masks. The enlargement, its first product (whose space also holds
+// the level pixels' values before it) and the pairwise-sum leaves live in the CTA's global scratch,
+// so that two CTAs fit an SM for windows up to 59 px.
 __host__ __device__ inline long long tail_smem_bytes(int S, int f, int n_angles) {
     const long long Hb = (long long)S * f, RW = (Hb + 31) / 32, area = (long long)S * S;
     const long long tmpn = 2 * Hb > 3LL * (n_angles + 1) ? 2 * Hb : 3LL * (n_angles + 1);
-    return (2 * area + 2 * kHalfLeavesMax + tmpn) * 8 + 5 * Hb * RW * 4 + (2 * Hb + 2 * kHalfLeavesMax) * 4 + 3 * area;
+    return (area + 2 * kHalfLeavesMax + tmpn) * 8 + 5 * Hb * RW * 4 + 2 * Hb * 4 + 3 * area;
+}
+
+// Doubles of one tail CTA's global scratch: enlargement (Hb^2), first product (Hb S), leaves.
+__host__ __device__ inline long long tail_scratch_doubles(int S, int f) {
+    const long long Hb = (long long)S * f;
+    return Hb * Hb + Hb * S + kHalfLeavesMax;
 }
 
 // The tail family on hole windows (subpx/_cpu/invariant_cd.py:551-875 with the windows of 878-964):
@@ -2398,8 +2408,7 @@ __global__ void __launch_bounds__(kHalfThreads) k_tail_area(TailArgs t) {
     const int Hb = S * f, Wb = Hb, RW = (Wb + 31) / 32, N = Hb * Wb, area = S * S;
     const int tmpn = max(2 * Hb, 3 * (a.n_angles + 1));
     double* cell = hsm;
-    double* lv = cell + area;
-    double* leafsum = lv + area;
+    double* leafsum = cell + area;
     double* tmp = leafsum + 2 * kHalfLeavesMax;
     uint32_t* bmask = reinterpret_cast<uint32_t*>(tmp + tmpn);
     uint32_t* above = bmask + Hb * RW;
@@ -2408,16 +2417,18 @@ __global__ void __launch_bounds__(kHalfThreads) k_tail_area(TailArgs t) {
     uint32_t* zplane = reg2 + Hb * RW;
     int* rowcnt = reinterpret_cast<int*>(zplane + Hb * RW);
     int* colcnt = rowcnt + Hb;
-    int* leaf_lo = colcnt + Wb;
-    int* leaf_len = leaf_lo + kHalfLeavesMax;
-    uint8_t* mask = reinterpret_cast<uint8_t*>(leaf_len + kHalfLeavesMax);
+    uint8_t* mask = reinterpret_cast<uint8_t*>(colcnt + Wb);
     uint8_t* lmask = mask + area;
     uint8_t* zmask = lmask + area;
-    double* big = a.scratch + (long long)blockIdx.x * ((long long)N + (long long)Hb * S);
+    double* big = a.scratch + (long long)blockIdx.x * tail_scratch_doubles(S, f);
     double* T = big + N;
+    double* lv = T;  // the level pixels' values, used before T is computed
+    int* leaf_lo = reinterpret_cast<int*>(T + (long long)Hb * S);
+    int* leaf_len = leaf_lo + kHalfLeavesMax;
     if (tid == 0) s_int[3] = np_pairwise_leaves(0, N, leaf_lo, leaf_len, 0);
     __syncthreads();
     const int n_leaves = s_int[3];
+    __syncthreads();  // s_int is reused below
     const bool want_zero = t.norm.status || t.edge.status || t.foot.status || t.given.status;
     const double sy = 1.0 / f;
     const double den_g = __dmul_rn((double)(2 * f), sy);  // 2 d sy: central differences over +-d
@@ -2832,8 +2843,7 @@ static int tail_ctas(int side, int factor, int n_angles) {
 
 size_t spx_tail_area_workspace_bytes(int side, int factor, int n_angles) {
     if (side < 1 || factor < 1 || n_angles < 1) return 0;
-    const long long Hb = (long long)side * factor;
-    return (size_t)(148LL * 4 * (Hb * Hb + Hb * side) * sizeof(double) + 256);
+    return (size_t)(148LL * 4 * tail_scratch_doubles(side, factor) * sizeof(double) + 256);
 }
 
 int spx_tail_area_cd(const float* cells, const uint8_t* inside, const uint8_t* level_pixels, const uint8_t* territory,
