@@ -175,3 +175,40 @@ def test_window_neighbours_match_kdtree(case):
         cand = [(d, j) for d, j in zip(d_ref[r], i_ref[r]) if j != report[r]][:8]
         np.testing.assert_allclose(d_got, np.sort([d for d, _ in cand]), rtol=0, atol=1e-9)
     np.testing.assert_array_equal(org.cpu().numpy(), np.rint(glob[report]).astype(np.int64) - radius)
+
+
+def test_tail_few_holes_and_options():
+    """Fewer modelled holes than the 8 neighbours a window looks at (the reference's k-d tree query
+    then asks for fewer), against the oracle on the same models; the reference's argument checks;
+    windows wider than the kernel's 64 px refused; a page without holes gives empty results."""
+    from imageprocessor_new_b200 import measure_cds, synthetic
+    from oracle import deblend as odb
+    from oracle import invariant as oi
+
+    img, _ = synthetic.gaussian_lattice(2.0, shape=(40, 60), seed=0)  # 8 holes, windows past the edges
+    level = float(np.percentile(img, 10))
+    res = measure_cds(img, backend="gpu", methods=TAIL, area_max=400, background_level=level)
+    dm = res.deblend_model
+    params, report = dm["params"], dm["report"]
+    assert 1 < len(params) <= 8
+    hm, wm = res.meta["cell_stack_shape"]
+    state = odb.State.__new__(odb.State)
+    state.params = params
+    state.background_map = np.full(img.shape, level)
+    state.model_image = odb.render(params, img.shape, max(hm, wm))
+    want = oi.tail_areas(img.astype(np.float64), state, np.zeros((len(params), hm, wm), bool),
+                         np.zeros((len(params), 2)), report, 128, TAIL, pitch=res.meta["pitch_px"])
+    for m in TAIL:
+        np.testing.assert_array_equal(res.measurements[m].status, want[m]["status"], err_msg=m)
+        _close(res.measurements[m].metrics["area_px2"], want[m]["metrics"]["area_px2"], frac=1.0, atol=1e-9)
+    with pytest.raises(ValueError, match="tail_area_level"):
+        measure_cds(img, backend="gpu", methods=("tail_area",), tail_area_level=1.0)
+    with pytest.raises(ValueError, match="tail_window"):
+        measure_cds(img, backend="gpu", methods=("tail_area",), tail_window=2.5)
+    page = synthetic.page_staggered(0, shape=(256, 256)).image
+    with pytest.raises(NotImplementedError, match="64 px"):
+        measure_cds(page, backend="gpu", methods=("tail_area",), area_max=400, tail_window=1.5)
+    empty = measure_cds(np.full((64, 64), 1000, np.uint16), backend="gpu", methods=TAIL)
+    for m in TAIL:
+        assert len(empty.measurements[m].status) == 0
+        assert "steepest_level" in empty.measurements[m].metrics or m != "foot_area"
