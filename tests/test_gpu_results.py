@@ -44,3 +44,28 @@ def test_own_compact_export_round_trip(tmp_path, methods):
         np.testing.assert_array_equal(a, b, err_msg=m)
         np.testing.assert_array_equal(back.measurements[m].metrics["cd_equivalent_px"],
                                       res.measurements[m].metrics["cd_equivalent_px"])
+
+
+def test_compact_round_trip_area_methods(tmp_path):
+    """Compact files of the projection, half_area and tail methods: contours rebuilt from center_local,
+    edge_px and the cell origins. The tail methods measure on windows around the holes and report
+    center_local relative to the hole's cell, so their rebuilt contours agree to rounding (as the
+    reference's own loader's do); the others bit for bit; metrics unchanged."""
+    from imageprocessor_new_b200 import measure_cds, synthetic
+    from imageprocessor_new_b200.results import load_cd_results, save_cd_results
+
+    methods = ("projection", "half_area_min_avg", "tail_area", "foot_area", "foot_area_ratio")
+    page = np.ascontiguousarray(synthetic.page_square(3).image[:200, :260])
+    # tail_window 0.8: windows of 53 px on this page (pitch about 32 px; the kernel takes up to 64 px).
+    res = measure_cds(page, backend="gpu", methods=methods, area_max=400, tail_window=0.8)
+    save_cd_results(res, tmp_path / "c", compact=True)
+    back = load_cd_results(tmp_path / "c")
+    for m in methods:
+        a, b = back.measurements[m].contours_xy, res.measurements[m].contours_xy
+        if m in ("tail_area", "foot_area", "foot_area_ratio"):
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-9, equal_nan=True, err_msg=m)
+        else:
+            np.testing.assert_array_equal(a, b, err_msg=m)
+        for metric, v in res.measurements[m].metrics.items():
+            np.testing.assert_array_equal(back.measurements[m].metrics[metric], v, err_msg=f"{m} {metric}")
+        np.testing.assert_array_equal(back.measurements[m].status, res.measurements[m].status)
