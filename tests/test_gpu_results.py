@@ -48,9 +48,10 @@ def test_own_compact_export_round_trip(tmp_path, methods):
 
 def test_compact_round_trip_area_methods(tmp_path):
     """Compact files of the projection, half_area and tail methods: contours rebuilt from center_local,
-    edge_px and the cell origins. The tail methods measure on windows around the holes and report
-    center_local relative to the hole's cell, so their rebuilt contours agree to rounding (as the
-    reference's own loader's do); the others bit for bit; metrics unchanged."""
+    edge_px and the cell origins (as the reference's loader rebuilds them). The measuring kernels
+    draw projection's ellipse and the tail outlines (on windows around the holes, center_local then
+    relative to the hole's cell) with other roundings, so the rebuilt vertices agree to 1e-9 px;
+    metrics and statuses are unchanged."""
     from imageprocessor_new_b200 import measure_cds, synthetic
     from imageprocessor_new_b200.results import load_cd_results, save_cd_results
 
@@ -62,10 +63,7 @@ def test_compact_round_trip_area_methods(tmp_path):
     back = load_cd_results(tmp_path / "c")
     for m in methods:
         a, b = back.measurements[m].contours_xy, res.measurements[m].contours_xy
-        if m in ("tail_area", "foot_area", "foot_area_ratio"):
-            np.testing.assert_allclose(a, b, rtol=0, atol=1e-9, equal_nan=True, err_msg=m)
-        else:
-            np.testing.assert_array_equal(a, b, err_msg=m)
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-9, equal_nan=True, err_msg=m)
         for metric, v in res.measurements[m].metrics.items():
             np.testing.assert_array_equal(back.measurements[m].metrics[metric], v, err_msg=f"{m} {metric}")
         np.testing.assert_array_equal(back.measurements[m].status, res.measurements[m].status)
