@@ -2393,7 +2393,7 @@ __host__ __device__ inline long long tail_scratch_doubles(int S, int f) {
 // sub-pixels (edge_area), the curvature-weighted mean below the steepest level inside the territory
 // (foot_area), or given (foot_area_ratio). The region, its metrics and outline as the half_area
 // family; positions in the image, center_local relative to the hole's own cell.
-__global__ void __launch_bounds__(kHalfThreads) k_tail_area(TailArgs t) {
+__global__ void __launch_bounds__(kHalfThreads, 2) k_tail_area(TailArgs t) {
     extern __shared__ double hsm[];
     __shared__ int hist[2048];
     __shared__ int warp_tot[32], s_pick[3];
@@ -2484,6 +2484,7 @@ __global__ void __launch_bounds__(kHalfThreads) k_tail_area(TailArgs t) {
                 const int Y = q / S, x = q % S;
                 const double* zr = a.zy + (long long)Y * S;
                 double v = 0.0;
+#pragma unroll 4
                 for (int y = 0; y < S; ++y) {
                     const double c = mask[y * S + x] ? __dsub_rn(cell[y * S + x], b) : 0.0;
                     v = __fma_rn(__ldg(zr + y), c, v);
@@ -2491,19 +2492,27 @@ __global__ void __launch_bounds__(kHalfThreads) k_tail_area(TailArgs t) {
                 T[q] = v;
             }
             __syncthreads();
-            for (int Y0 = 2 * warp; Y0 < Hb; Y0 += 2 * (kHalfThreads / 32))
+            // Four enlarged rows per warp step (each operator load feeds four rows), lanes across
+            // columns, the products summed in the order of x as before.
+            for (int Y0 = 4 * warp; Y0 < Hb; Y0 += 4 * (kHalfThreads / 32))
                 for (int X0 = 0; X0 < Wb; X0 += 128) {
-                    const bool two = Y0 + 1 < Hb;
-                    double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+                    double v[4][4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) v[r][q] = 0.0;
+#pragma unroll 2
                     for (int x = 0; x < S; ++x) {
-                        const double t0 = T[(long long)Y0 * S + x], t1 = two ? T[(long long)(Y0 + 1) * S + x] : 0.0;
+                        double tr[4];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) tr[r] = Y0 + r < Hb ? T[(long long)(Y0 + r) * S + x] : 0.0;
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
                             const int X = X0 + lane + 32 * q;
                             if (X < Wb) {
                                 const double z = __ldg(t.zxT + (long long)x * Wb + X);
-                                v0[q] = __fma_rn(t0, z, v0[q]);
-                                v1[q] = __fma_rn(t1, z, v1[q]);
+#pragma unroll
+                                for (int r = 0; r < 4; ++r) v[r][q] = __fma_rn(tr[r], z, v[r][q]);
                             }
                         }
                     }
@@ -2511,8 +2520,9 @@ __global__ void __launch_bounds__(kHalfThreads) k_tail_area(TailArgs t) {
                     for (int q = 0; q < 4; ++q) {
                         const int X = X0 + lane + 32 * q;
                         if (X >= Wb) continue;
-                        big[(long long)Y0 * Wb + X] = bit(bmask, Y0, X) ? v0[q] : -INFINITY;
-                        if (two) big[(long long)(Y0 + 1) * Wb + X] = bit(bmask, Y0 + 1, X) ? v1[q] : -INFINITY;
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (Y0 + r < Hb) big[(long long)(Y0 + r) * Wb + X] = bit(bmask, Y0 + r, X) ? v[r][q] : -INFINITY;
                     }
                 }
             __syncthreads();
