@@ -1805,6 +1805,7 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
         if (lane == 0) {
             h.above[t] = word;
             h.reg[t] = 0u;
+            h.reg2[t] = 0u;
         }
     }
     __syncthreads();
@@ -1815,7 +1816,9 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
     }
     __syncthreads();
     // Grow the region from the highest pixel, one 8-neighbour ring per step, inside the above-
-    // threshold pixels, until it stops changing.
+    // threshold pixels, until it stops changing. After s steps the region lies within s rows of the
+    // highest pixel's row, so step s + 1 only computes the rows within s + 1 of it (the others of both
+    // planes stay zero).
     uint32_t* cur = h.reg;
     uint32_t* nxt = h.reg2;
     auto vert = [&](const uint32_t* p, int Y, int w) {
@@ -1832,9 +1835,11 @@ __device__ void half_output(const HalfArgs& a, const MethodOut& out, int i, doub
         if (w == RW - 1) d &= last_bits;
         return d;
     };
+    const int top_row = h.top / Wb;
     for (int step = 0; step < h.N; ++step) {
         int changed = 0;
-        for (int t = tid; t < Hb * RW; t += kHalfThreads) {
+        const int r0 = max(top_row - step - 1, 0), r1 = min(top_row + step + 1, Hb - 1);
+        for (int t = r0 * RW + tid; t < (r1 + 1) * RW; t += kHalfThreads) {
             const uint32_t nw = dilate(cur, t) & h.above[t];
             nxt[t] = nw;
             changed |= nw != cur[t];
