@@ -239,7 +239,8 @@ def unmodelled(binary, labels, ids):
 def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), threshold="otsu", invert=False,
                 area_min=3, area_max=50, pad=3, n_angles=128, radial_step=0.1, fit_fraction=0.2,
                 deblend_iterations=30, deblend_tolerance=1e-3, background_level=None, seeds="threshold",
-                peak_min_distance=None, smooth_sigma=0.0, tail_area_level=0.2, tail_window=1.2):
+                peak_min_distance=None, smooth_sigma=0.0, tail_area_level=0.2, tail_window=1.2, psf_fwhm=None,
+                nominal_cd=None, dark_level=0.0, flux_ratio_scale=None):
     """The model-background measure_cds pipeline, seeds from thresholded components or, with
     seeds="peaks", from the smoothed signal's maxima (subpx/cd.py:502-511)."""
     img = np.asarray(img)
@@ -251,7 +252,9 @@ def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), 
                               fit_fraction=fit_fraction, deblend_iterations=deblend_iterations,
                               deblend_tolerance=deblend_tolerance, background_level=background_level,
                               peak_min_distance=peak_min_distance, smooth_sigma=smooth_sigma,
-                              tail_area_level=tail_area_level, tail_window=tail_window)
+                              tail_area_level=tail_area_level, tail_window=tail_window,
+                              psf_fwhm=psf_fwhm, nominal_cd=nominal_cd, dark_level=sign * float(dark_level),
+                              flux_ratio_scale=flux_ratio_scale)
     seg = img
     if img.dtype != np.uint8 and not (img.dtype == np.uint16 and threshold == "otsu"):
         g = img.astype(np.float64)
@@ -283,7 +286,9 @@ def measure_cds(img, *, methods=("gaussian", "logquad", "gradient", "halfmax"), 
                                 n_angles=n_angles, radial_step=radial_step, fit_fraction=fit_fraction,
                                 deblend_iterations=deblend_iterations, deblend_tolerance=deblend_tolerance,
                                 background_level=background_level, smooth_sigma=smooth_sigma,
-                                tail_area_level=tail_area_level, tail_window=tail_window)
+                                tail_area_level=tail_area_level, tail_window=tail_window,
+                                psf_fwhm=psf_fwhm, nominal_cd=nominal_cd, dark_level=sign * float(dark_level),
+                                flux_ratio_scale=flux_ratio_scale)
 
 
 def _measure_peaks(img, signal, sign, *, peak_min_distance, **kw):
@@ -301,7 +306,8 @@ def _measure_peaks(img, signal, sign, *, peak_min_distance, **kw):
 
 def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch, tile_px, exclude_mask, oversized, *,
                          methods, pad, n_angles, radial_step, fit_fraction, deblend_iterations, deblend_tolerance,
-                         background_level, smooth_sigma, tail_area_level=0.2, tail_window=1.2):
+                         background_level, smooth_sigma, tail_area_level=0.2, tail_window=1.2, psf_fwhm=None,
+                         nominal_cd=None, dark_level=0.0, flux_ratio_scale=None):
     """The deblend passes with seed revision and the measurements (subpx/cd.py:581-760)."""
     h, w = img.shape
 
@@ -354,8 +360,8 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
     cleaned = state.cleaned[report]
     from .invariant import HALF_AREA, TAIL_AREA
 
-    measured = [m for m in methods if m not in ("gaussian", "projection") and m not in HALF_AREA
-                and m not in TAIL_AREA]
+    measured = [m for m in methods if m not in ("gaussian", "projection", "disk", "flux_ratio")
+                and m not in HALF_AREA and m not in TAIL_AREA]
     out = measure_cells(cleaned, masks[report], origins[report], seeds[report], methods=measured, n_angles=n_angles,
                         radial_step=radial_step, fit_fraction=fit_fraction, smooth_sigma=smooth_sigma) if measured else {}
     if "gaussian" in methods:
@@ -378,6 +384,14 @@ def _deblend_and_measure(img, signal, sign, rows, ids, interior, by_reach, pitch
         found = tail_areas(signal, state, masks, origins, report, n_angles, tails, level=tail_area_level,
                            window=tail_window, pitch=float(pitch) if np.isfinite(pitch) else None)
         tail_info = found.pop("_info")
+        out.update(found)
+    disks = [m for m in methods if m in ("disk", "flux_ratio")]
+    if disks:
+        from .disk import disk_methods
+
+        found = disk_methods(signal, state, masks, origins, report, n_angles, disks, psf_fwhm_px=psf_fwhm,
+                             nominal_cd_px=nominal_cd, dark_level=dark_level, flux_ratio_scale=flux_ratio_scale)
+        tail_info.update(found.pop("_info"))
         out.update(found)
     out = {m: out[m] for m in methods}
     from scipy.ndimage import map_coordinates

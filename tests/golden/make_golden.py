@@ -390,9 +390,49 @@ def make_tail(out: Path, ref):
     np.savez_compressed(out / "tail.npz", names=np.array(names), **arrays)
 
 
+def disk_cases():
+    from imageprocessor_new_b200 import synthetic as S
+
+    small, _ = S.gaussian_lattice(2.0, shape=(60, 120))
+    stag, _ = cd_cases()["staggered"]
+    return {
+        # Blur given: the disk table of that Airy FWHM, two rounds of fits.
+        "lattice_psf": (small, dict(area_max=400, methods=("disk", "flux_ratio"), psf_fwhm=2.0)),
+        # Blur calibrated by bisection so that the median disk diameter equals nominal_cd; flux ratios
+        # scaled to it.
+        "lattice_nominal": (small, dict(area_max=400, methods=("disk", "flux_ratio"), nominal_cd=3.0)),
+        # Wide holes of a staggered page; dark level and a given flux-ratio scale.
+        "staggered_disk": (stag, dict(area_max=400, methods=("flux_ratio", "disk"), psf_fwhm=3.0, dark_level=100.0,
+                                      flux_ratio_scale=1.5)),
+    }
+
+
+def make_disk(out: Path, ref):
+    """measure_cds with the disk and flux_ratio methods (subpx/_cpu/invariant_cd.py:94-306, 1069-1206)."""
+    from subpx import measure_cds
+
+    arrays = {}
+    names = []
+    for name, (img, kw) in disk_cases().items():
+        res = measure_cds(img, backend="cpu", **kw)
+        arrays[f"{name}_img"] = img
+        arrays[f"{name}_kwargs"] = np.array(json.dumps(kw))
+        arrays[f"{name}_seeds"] = res.seeds_xy
+        arrays[f"{name}_meta"] = np.array(json.dumps({k: res.meta.get(k) for k in (
+            "psf_fwhm_px", "psf_source", "disk_median_cd_px", "flux_ratio_scale")}))
+        for m, r in res.measurements.items():
+            arrays[f"{name}_{m}_status"] = r.status
+            arrays[f"{name}_{m}_centers"] = r.centers_xy
+            arrays[f"{name}_{m}_edge_px"] = r.geometry["edge_px"]
+            for metric, v in r.metrics.items():
+                arrays[f"{name}_{m}_m_{metric}"] = v
+        names.append(name)
+    np.savez_compressed(out / "disk.npz", names=np.array(names), **arrays)
+
+
 MAKERS = {"thresholds": make_thresholds, "ccl": make_ccl, "centers": make_centers, "voronoi": make_voronoi,
           "tiled": make_tiled, "cd": make_cd, "results": make_results, "centers_model": make_centers_model,
-          "invariant": make_invariant, "tail": make_tail}
+          "invariant": make_invariant, "tail": make_tail, "disk": make_disk}
 
 
 def main():

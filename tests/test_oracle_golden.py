@@ -163,6 +163,35 @@ def test_tail_oracle_matches_reference(name):
             np.testing.assert_array_equal(r["edge_px"], z[f"{name}_{method}_edge_px"].astype(np.float64))
 
 
+# The disk and flux_ratio methods (subpx/_cpu/invariant_cd.py:94-306, 1069-1206): the Airy-blurred,
+# pixel-averaged disk table, the batched LM of each hole's disk, a second round with the neighbours
+# re-rendered from the disk fits (near and far field), the blur given or calibrated by bisection on
+# nominal_cd, the flux ratios with a dark level and scale.
+@pytest.mark.parametrize("name", ["lattice_psf", "lattice_nominal", "staggered_disk"])
+def test_disk_oracle_matches_reference(name):
+    import json
+
+    from oracle import cd as ocd
+
+    z = _load("disk")
+    kw = _cd_kwargs(z, name)
+    got = ocd.measure_cds(z[f"{name}_img"], **kw)
+    np.testing.assert_array_equal(got["seeds"], z[f"{name}_seeds"])
+    meta = json.loads(str(z[f"{name}_meta"]))
+    for key in ("psf_fwhm_px", "psf_source", "disk_median_cd_px", "flux_ratio_scale"):
+        if meta.get(key) is not None:
+            assert got["tail_info"][key] == meta[key], key
+    for method in kw["methods"]:
+        r = got["measurements"][method]
+        np.testing.assert_array_equal(r["status"], z[f"{name}_{method}_status"])
+        for metric, v in r["metrics"].items():
+            if metric == "background":
+                continue
+            np.testing.assert_array_equal(v, z[f"{name}_{method}_m_{metric}"], err_msg=f"{method} {metric}")
+        np.testing.assert_array_equal(r["centers"], z[f"{name}_{method}_centers"])
+        np.testing.assert_array_equal(r["edge_px"], z[f"{name}_{method}_edge_px"])
+
+
 @pytest.mark.parametrize("seed", [0, 1, 2])
 def test_morphology_matches_opencv(seed):
     cv2 = pytest.importorskip("cv2")
